@@ -1,0 +1,94 @@
+/*
+ * oracle.h -- TEST INFRASTRUCTURE. Not part of the product.
+ *
+ * CPU restatement of the reference contact-solve hot path, used only as the
+ * checker by tests/, __graft_entry__.smoke() and the cpu_baseline leg of
+ * bench.py. The product (solfec-1.0_b200/) never links or calls it.
+ *
+ * Pinning: the restated solver is compared against the reference's own
+ * GAUSS_SEIDEL_Solve compiled from its sources (oracle/_ref, built by
+ * oracle/Makefile) and against committed golden vectors produced by that build
+ * (tests/golden/, script tests/golden/make_golden.py).
+ *
+ * Layout conventions (shared with the product's C ABI):
+ *  - 3x3 matrices are column-major, A[3*j+i] = A(i,j) (alg.h:948-953);
+ *  - row arrays are indexed by row (contact) in the caller's list order;
+ *  - off-diagonal blocks of row i are adjptr[i]..adjptr[i+1]-1 with the
+ *    neighbour row in adjcol[] and the 9 entries of W_ij in Woff[9*k..].
+ */
+#ifndef ORC_ORACLE_H
+#define ORC_ORACLE_H
+
+#include <stdint.h>
+
+/* reference THROW codes (err.h enum values) reported by a FAILURE_EXIT solve */
+#define ORC_ERR_GAUSS_SEIDEL_DIAGONAL_DIVERGED 44
+#define ORC_ERR_GAUSS_SEIDEL_DIVERGED 45
+
+/* Restatement of the serial GAUSS_SEIDEL_Solve (bgs.c:913-1069) over a flat
+ * local-dynamics description; same argument list as ref_gs_solve in
+ * oracle/ref/ref_harness.c so a test can call either. Returns 0, or the THROW
+ * code a FAILURE_EXIT solve raised. */
+int orc_gs_solve (int n, const int *adjptr, const int *adjcol, const double *Woff,
+                  const double *W, const double *A, const double *rho, const double *B, const double *V,
+                  const double *gap, const double *friction, const double *restitution, const double *cohesion,
+                  double *R, double *U, double *conmerit,
+                  double free_energy, int dynamic, double step,
+                  double epsilon, int maxiter, double meritval, int failure,
+                  double diagepsilon, int diagmaxiter, int diagsolver, int reverse,
+                  int *out_iters, int *out_error, double *out_merit,
+                  double *rerhist, double *merhist, int *out_ncallbacks);
+
+/* Restatement of MERIT_Function (mrf.c:35-185) with update_U = 1: recomputes U
+ * for every row and returns the merit value; conmerit (may be NULL) receives
+ * the per-constraint merit. */
+double orc_merit (int n, const int *adjptr, const int *adjcol, const double *Woff,
+                  const double *W, const double *A, const double *B, const double *V,
+                  const double *gap, const double *friction, const double *restitution, const double *cohesion,
+                  const double *R, double *U, double *conmerit, double free_energy, int dynamic, double step);
+
+/* One diagonal block solve (dbs.c:492-550, CONTACT + SIGNORINI_COULOMB). */
+int orc_diagonal_solve (int diagsolver, double diagepsilon, int diagmaxiter, int dynamic, double step,
+                        double friction, double restitution, double cohesion, double gap, double rho,
+                        const double *W, const double *B, const double *V, double *U, double *R);
+
+/* ---------------- local dynamics assembly (ldy.c, bod.c) ---------------- */
+
+/* Number of off-diagonal blocks LOCDYN_Insert (ldy.c:492-568) creates for the
+ * contact list: per row, per non-obstacle body of the row, one block per other
+ * row touching that body. Fills adjptr[ncon+1]. */
+int64_t orc_count_blocks (int nbod, const int *obstacle, int ncon, const int *master, const int *slave, int *adjptr);
+
+/* Restatement of update_V_and_B (ldy.c:364-474) and LOCDYN_Update_Begin
+ * (ldy.c:626-876) for rigid bodies and obstacles (bod.c:216-258,1817-1871).
+ * Body arrays: rot[9] (column-major rotation), x0[3] (referential mass centre),
+ * jinv[9] (inverse referential inertia), minv (1/mass), velo[6] ([Omega; v] at
+ * t+h after the free step) and velo0[6] (at t), obstacle flag.
+ * Contact arrays: master, slave (-1 = none), mpnt[3]/spnt[3] referential
+ * points, base[9] local frame (normal = third column).
+ * Outputs per row W[9], A[9], rho, B[3], V[3]; blocks adjcol, adjbod (shared
+ * body), Woff[9] in the order adjptr from orc_count_blocks; free energy.
+ * Block order inside a row: master-body neighbours then slave-body neighbours,
+ * each by ascending row index. Returns 0, or -1 for an unsupported input
+ * (self-contact master == slave). */
+int orc_assemble (int nbod, const double *rot, const double *x0, const double *jinv, const double *minv,
+                  const double *velo, const double *velo0, const int *obstacle,
+                  int ncon, const int *master, const int *slave, const double *mpnt, const double *spnt,
+                  const double *base, double step,
+                  double *W, double *A, double *rho, double *B, double *V, double *free_energy,
+                  const int *adjptr, int *adjcol, int *adjbod, double *Woff);
+
+/* ---------------- contact-graph colouring ---------------- */
+
+/* Counter-based priority of row i for a colouring seed (shared definition with
+ * the device Jones-Plassmann kernel). */
+uint64_t orc_jp_priority (uint64_t seed, int i);
+
+/* Greedy colouring in decreasing priority order: each row takes the smallest
+ * colour not used by an already coloured neighbour. This is the fixed point of
+ * Jones-Plassmann with smallest-available-colour selection, so the device
+ * kernel must reproduce it bit for bit. Returns the number of colours, or -1
+ * when more than maxcolours are needed. */
+int orc_colour (int n, const int *adjptr, const int *adjcol, uint64_t seed, int maxcolours, int *colour);
+
+#endif

@@ -1,0 +1,178 @@
+"""oracle.py -- TEST INFRASTRUCTURE. Not part of the product.
+
+ctypes binding of the CPU oracle (lib/liboracle.so, the C restatement) and of
+the reference's own solver compiled from its sources (_ref/libref_bgs.so).
+Only tests/, __graft_entry__.smoke() and the cpu_baseline leg of bench.py
+import this module, and only as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBS = {}
+
+DS = {'PROJECTED_GRADIENT': 0, 'DE_SAXCE_FENG': 1, 'SEMISMOOTH_NEWTON': 2, 'PROJECTED_NEWTON': 3}
+FAIL = {'CONTINUE': 0, 'EXIT': 1, 'CALLBACK': 2}
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags='C_CONTIGUOUS')
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags='C_CONTIGUOUS')
+
+
+def build():
+    """Compile the restatement and, where the reference tree is present, the
+    reference solver (oracle/Makefile)."""
+    subprocess.run(['make', '-s', '-C', HERE], check=True)
+
+
+def _load(name):
+    if name in _LIBS:
+        return _LIBS[name]
+    path = os.path.join(HERE, {'oracle': 'lib/liboracle.so', 'ref': '_ref/libref_bgs.so'}[name])
+    if not os.path.exists(path):
+        build()
+    lib = C.CDLL(path)
+    solve = lib.orc_gs_solve if name == 'oracle' else lib.ref_gs_solve
+    solve.restype = C.c_int
+    solve.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                      _dp, _dp, _dp, C.c_double, C.c_int, C.c_double,
+                      C.c_double, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+                      C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double), _dp, _dp, C.POINTER(C.c_int)]
+    if name == 'oracle':
+        lib.orc_count_blocks.restype = C.c_int64
+        lib.orc_count_blocks.argtypes = [C.c_int, _ip, C.c_int, _ip, _ip, _ip]
+        lib.orc_assemble.restype = C.c_int
+        lib.orc_assemble.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _ip, C.c_int, _ip, _ip, _dp, _dp, _dp,
+                                     C.c_double, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_double), _ip, _ip, _ip, _dp]
+        lib.orc_colour.restype = C.c_int
+        lib.orc_colour.argtypes = [C.c_int, _ip, _ip, C.c_uint64, C.c_int, _ip]
+        lib.orc_jp_priority.restype = C.c_uint64
+        lib.orc_jp_priority.argtypes = [C.c_uint64, C.c_int]
+        lib.orc_merit.restype = C.c_double
+        lib.orc_merit.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                  C.c_double, C.c_int, C.c_double]
+    _LIBS[name] = lib
+    return lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(HERE, '_ref/libref_bgs.so')) or os.path.isdir('/root/reference')
+
+
+class LocalDynamics:
+    """Flat local dynamics (the LOCDYN content the solver reads): rows in list
+    order with W, A, rho, B, V and contact parameters, plus per-row
+    off-diagonal blocks (adjptr/adjcol/Woff)."""
+
+    def __init__(self, W, A, rho, B, V, gap, friction, restitution, cohesion, adjptr, adjcol, Woff,
+                 free_energy, step, dynamic=1, adjbod=None):
+        c = np.ascontiguousarray
+        self.W, self.A, self.rho, self.B, self.V = c(W, float), c(A, float), c(rho, float), c(B, float), c(V, float)
+        self.gap, self.friction = c(gap, float), c(friction, float)
+        self.restitution, self.cohesion = c(restitution, float), c(cohesion, float)
+        self.adjptr, self.adjcol, self.Woff = c(adjptr, np.int32), c(adjcol, np.int32), c(Woff, float)
+        self.adjbod = None if adjbod is None else c(adjbod, np.int32)
+        self.free_energy, self.step, self.dynamic = float(free_energy), float(step), int(dynamic)
+
+    @property
+    def n(self):
+        return int(self.rho.shape[0])
+
+    @property
+    def nblocks(self):
+        return int(self.adjptr[-1])
+
+    def permuted(self, order):
+        """Rows re-listed in the given order (order[p] = old row at position p),
+        block columns renumbered, each row's blocks kept in their order."""
+        order = np.asarray(order, np.int64)
+        inv = np.empty_like(order); inv[order] = np.arange(order.size)
+        deg = np.diff(self.adjptr)[order]
+        ptr = np.zeros(order.size + 1, np.int64); np.cumsum(deg, out=ptr[1:])
+        src = np.concatenate([np.arange(self.adjptr[i], self.adjptr[i + 1]) for i in order]) if order.size else np.zeros(0, np.int64)
+        src = src.astype(np.int64)
+        rows = lambda a, w: a.reshape(-1, w)[order].reshape(-1)  # noqa: E731
+        return LocalDynamics(rows(self.W, 9), rows(self.A, 9), self.rho[order], rows(self.B, 3), rows(self.V, 3),
+                             self.gap[order], self.friction[order], self.restitution[order], self.cohesion[order],
+                             ptr.astype(np.int32), inv[self.adjcol[src]].astype(np.int32),
+                             self.Woff.reshape(-1, 9)[src].reshape(-1), self.free_energy, self.step, self.dynamic,
+                             None if self.adjbod is None else self.adjbod[src])
+
+
+def assemble(scene) -> LocalDynamics:
+    """Oracle assembly of a scenes.Scene (restated LOCDYN_Update_Begin)."""
+    lib = _load('oracle')
+    n = scene.ncon
+    adjptr = np.zeros(n + 1, np.int32)
+    nblk = lib.orc_count_blocks(scene.nbod, scene.obstacle, n, scene.master, scene.slave, adjptr)
+    W = np.zeros(9 * n); A = np.zeros(9 * n); rho = np.zeros(n); B = np.zeros(3 * n); V = np.zeros(3 * n)
+    adjcol = np.zeros(max(nblk, 1), np.int32); adjbod = np.zeros(max(nblk, 1), np.int32)
+    Woff = np.zeros(9 * max(nblk, 1))
+    fe = C.c_double(0.0)
+    rc = lib.orc_assemble(scene.nbod, scene.rot.ravel(), scene.x0.ravel(), scene.jinv.ravel(), scene.minv,
+                          scene.velo.ravel(), scene.velo0.ravel(), scene.obstacle, n, scene.master, scene.slave,
+                          scene.mpnt.ravel(), scene.spnt.ravel(), scene.base.ravel(), scene.step,
+                          W, A, rho, B, V, C.byref(fe), adjptr, adjcol, adjbod, Woff)
+    if rc != 0:
+        raise ValueError('oracle assembly rejected the scene (rc=%d)' % rc)
+    return LocalDynamics(W, A, rho, B, V, scene.gap, scene.friction, scene.restitution, scene.cohesion,
+                         adjptr, adjcol[:nblk], Woff[:9 * nblk], fe.value, scene.step, scene.dynamic, adjbod[:nblk])
+
+
+def colour(ld: LocalDynamics, seed: int, maxcolours: int = 256):
+    lib = _load('oracle')
+    col = np.zeros(ld.n, np.int32)
+    nc = lib.orc_colour(ld.n, ld.adjptr, ld.adjcol if ld.nblocks else np.zeros(1, np.int32), seed, maxcolours, col)
+    return nc, col
+
+
+def colour_order(col):
+    """Rows sorted by (colour, row index): the processing order of a
+    colour-by-colour sweep."""
+    return np.lexsort((np.arange(col.size), col)).astype(np.int64)
+
+
+def solve(ld: LocalDynamics, R=None, U=None, epsilon=1e-4, maxiter=1000, meritval=1.0, failure='CONTINUE',
+          diagepsilon=None, diagmaxiter=None, diagsolver='SEMISMOOTH_NEWTON', reverse=False, impl='oracle'):
+    """Run the restated (impl='oracle') or the compiled reference
+    (impl='ref') Gauss-Seidel solve on ld in list order. Defaults of
+    diagepsilon / diagmaxiter follow lng.c:4335-4342."""
+    if diagepsilon is None:
+        diagepsilon = max(2.220446049250313e-16, 0.01 * min(epsilon, min(meritval, 1e-4)))
+    if diagmaxiter is None:
+        diagmaxiter = max(100, maxiter // 100)
+    lib = _load(impl)
+    fn = lib.orc_gs_solve if impl == 'oracle' else lib.ref_gs_solve
+    n = ld.n
+    R = np.zeros(3 * n) if R is None else np.ascontiguousarray(R, float).copy().reshape(-1)
+    U = np.zeros(3 * n) if U is None else np.ascontiguousarray(U, float).copy().reshape(-1)
+    conmerit = np.zeros(max(n, 1))
+    rer = np.zeros(max(maxiter, 1)); mer = np.zeros(max(maxiter, 1))
+    iters, err, ncb = C.c_int(0), C.c_int(0), C.c_int(0)
+    merit = C.c_double(0.0)
+    adjcol = ld.adjcol if ld.nblocks else np.zeros(1, np.int32)
+    Woff = ld.Woff if ld.nblocks else np.zeros(9)
+    thrown = fn(n, ld.adjptr, adjcol, Woff, ld.W if n else np.zeros(9), ld.A if n else np.zeros(9),
+                ld.rho if n else np.zeros(1), ld.B if n else np.zeros(3), ld.V if n else np.zeros(3),
+                ld.gap if n else np.zeros(1), ld.friction if n else np.zeros(1),
+                ld.restitution if n else np.zeros(1), ld.cohesion if n else np.zeros(1),
+                R if n else np.zeros(3), U if n else np.zeros(3), conmerit, ld.free_energy, ld.dynamic, ld.step,
+                epsilon, maxiter, meritval, FAIL[failure], diagepsilon, diagmaxiter, DS[diagsolver], int(reverse),
+                C.byref(iters), C.byref(err), C.byref(merit), rer, mer, C.byref(ncb))
+    k = iters.value
+    return dict(R=R, U=U, conmerit=conmerit[:n], iters=k, error=err.value, merit=merit.value,
+                rerhist=rer[:k].copy(), merhist=mer[:k].copy(), thrown=thrown, ncallbacks=ncb.value)
+
+
+def merit(ld: LocalDynamics, R):
+    lib = _load('oracle')
+    U = np.zeros(3 * ld.n); cm = np.zeros(max(ld.n, 1))
+    m = lib.orc_merit(ld.n, ld.adjptr, ld.adjcol if ld.nblocks else np.zeros(1, np.int32),
+                      ld.Woff if ld.nblocks else np.zeros(9), ld.W, ld.A, ld.B, ld.V, ld.gap, ld.friction,
+                      ld.restitution, ld.cohesion, np.ascontiguousarray(R, float).reshape(-1), U, cm,
+                      ld.free_energy, ld.dynamic, ld.step)
+    return m, U, cm[:ld.n]

@@ -1,0 +1,461 @@
+"""Seeded synthetic rigid-body contact scenes.
+
+The reference builds its contact problems inside a full simulation
+(SOLFEC_Run, sol.c:665-842: body time stepping, contact detection in goc.c and
+LOCDYN_Insert). That pipeline is outside the solver path, so the scenes here
+are generated directly in the form the solver path consumes:
+
+* rigid bodies: rotation R (3x3, column-major), referential mass centre X0,
+  inverse referential inertia J^-1, 1/mass, velocity [Omega (body frame); v]
+  at time t (``velo0``) and after the free step t+h (``velo``), obstacle flag
+  (bod.c:53-74 layout);
+* contacts: master/slave body, referential points on both bodies, local frame
+  ``base`` (column-major, normal = third column, pointing from slave to
+  master), gap, Coulomb friction, restitution and cohesion (dom.h:77-129).
+
+Every generator is deterministic for a given seed. Contact detection follows
+the reference threshold: a pair is a contact when gap < GEOMETRIC_EPSILON
+(alg.c:24, goc.c:431).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+GEOMETRIC_EPSILON = 1e-6  # alg.c:24
+GRAVITY = np.array([0.0, 0.0, -9.81])
+
+
+@dataclasses.dataclass
+class Scene:
+    name: str
+    step: float
+    dynamic: int
+    # bodies
+    rot: np.ndarray        # (nb, 9) column-major rotation
+    x: np.ndarray          # (nb, 3) current mass centre
+    x0: np.ndarray         # (nb, 3) referential mass centre
+    jinv: np.ndarray       # (nb, 9) inverse referential inertia, column-major
+    minv: np.ndarray       # (nb,)
+    velo: np.ndarray       # (nb, 6) [Omega; v] after the free step (t+h)
+    velo0: np.ndarray      # (nb, 6) [Omega; v] at t
+    obstacle: np.ndarray   # (nb,) int32, 1 for obstacles (walls)
+    # contacts
+    master: np.ndarray     # (nc,) int32
+    slave: np.ndarray      # (nc,) int32, -1 for none
+    mpnt: np.ndarray       # (nc, 3) master referential point
+    spnt: np.ndarray       # (nc, 3) slave referential point
+    base: np.ndarray       # (nc, 9) column-major [t1 t2 n]
+    gap: np.ndarray        # (nc,)
+    friction: np.ndarray   # (nc,)
+    restitution: np.ndarray
+    cohesion: np.ndarray   # (nc,) cohesion * area, as dbs.c:500 forms it
+    mass: np.ndarray = None  # (nb,) for diagnostics
+
+    @property
+    def nbod(self) -> int:
+        return int(self.rot.shape[0])
+
+    @property
+    def ncon(self) -> int:
+        return int(self.master.shape[0])
+
+    def body_arrays(self):
+        return dict(rot=self.rot, x0=self.x0, jinv=self.jinv, minv=self.minv,
+                    velo=self.velo, velo0=self.velo0, obstacle=self.obstacle)
+
+    def contact_arrays(self):
+        return dict(master=self.master, slave=self.slave, mpnt=self.mpnt, spnt=self.spnt,
+                    base=self.base, gap=self.gap, friction=self.friction,
+                    restitution=self.restitution, cohesion=self.cohesion)
+
+
+# ----------------------------------------------------------------------------- helpers
+
+def _random_rotations(rng: np.random.Generator, n: int) -> np.ndarray:
+    """Uniform random rotations (Shoemake quaternions), column-major (n, 9)."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    q = np.stack([np.sqrt(1 - u1) * np.sin(2 * np.pi * u2), np.sqrt(1 - u1) * np.cos(2 * np.pi * u2),
+                  np.sqrt(u1) * np.sin(2 * np.pi * u3), np.sqrt(u1) * np.cos(2 * np.pi * u3)], axis=1)
+    x, y, z, w = q.T
+    R = np.empty((n, 3, 3))
+    R[:, 0, 0] = 1 - 2 * (y * y + z * z); R[:, 0, 1] = 2 * (x * y - z * w); R[:, 0, 2] = 2 * (x * z + y * w)
+    R[:, 1, 0] = 2 * (x * y + z * w); R[:, 1, 1] = 1 - 2 * (x * x + z * z); R[:, 1, 2] = 2 * (y * z - x * w)
+    R[:, 2, 0] = 2 * (x * z - y * w); R[:, 2, 1] = 2 * (y * z + x * w); R[:, 2, 2] = 1 - 2 * (x * x + y * y)
+    return R.transpose(0, 2, 1).reshape(n, 9)  # column-major flattening
+
+
+def _colmajor(M: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(M.transpose(0, 2, 1).reshape(M.shape[0], 9))
+
+
+def local_base(normal: np.ndarray) -> np.ndarray:
+    """Right-handed frame [t1 t2 n] per normal, column-major (nc, 9)."""
+    n = normal / np.linalg.norm(normal, axis=1, keepdims=True)
+    e = np.zeros_like(n)
+    idx = np.argmin(np.abs(n), axis=1)
+    e[np.arange(n.shape[0]), idx] = 1.0
+    t1 = np.cross(n, e)
+    t1 /= np.linalg.norm(t1, axis=1, keepdims=True)
+    t2 = np.cross(n, t1)
+    return np.ascontiguousarray(np.concatenate([t1, t2, n], axis=1))
+
+
+def _referential(rot: np.ndarray, x: np.ndarray, x0: np.ndarray, p: np.ndarray) -> np.ndarray:
+    """Referential point X with R (X - X0) = p - x."""
+    R = rot.reshape(-1, 3, 3).transpose(0, 2, 1)  # row-major view of column-major storage
+    return x0 + np.einsum('nji,nj->ni', R, p - x)
+
+
+def _walls(lo, hi):
+    """Six obstacle walls of an axis-aligned box: (outward-into-box normal, plane point)."""
+    lo = np.asarray(lo, float); hi = np.asarray(hi, float)
+    normals = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]], float)
+    points = np.array([lo, hi, lo, hi, lo, hi], float)
+    return normals, points
+
+
+def _settle_spheres(x, r, lo, hi, iters, drop, overlap, rng, relax=200, shake=0.15):
+    """Gravity compaction by position projection: every iteration lowers all
+    spheres by a drop that decays to zero and then pushes overlapping pairs
+    apart until they interpenetrate by at most ``overlap``, with a decaying
+    lateral shake (a fraction ``shake`` of the radius) that lets spheres roll
+    off unstable columns into the hollows below; a final run of
+    projection passes without drop relaxes the packing. Produces a dense
+    resting packing in which touching spheres overlap slightly (so they are
+    detected contacts)."""
+    from scipy.spatial import cKDTree
+    rmax = float(r.max())
+    skin = 4 * drop + 0.1 * rmax
+    pairs = None
+    total = iters + relax
+    for it in range(total):
+        if it % 5 == 0:
+            pairs = cKDTree(x).query_pairs(2 * rmax + skin, output_type='ndarray')
+        if it < iters:
+            decay = (1.0 - it / float(iters)) ** 2
+            x[:, 2] -= drop * decay
+            x[:, 0:2] += rng.uniform(-shake, shake, (x.shape[0], 2)) * decay * r[:, None]
+        for _ in range(4):
+            if pairs.shape[0]:
+                i, j = pairs[:, 0], pairs[:, 1]
+                d = x[i] - x[j]
+                dist = np.sqrt(np.einsum('ij,ij->i', d, d))
+                pen = (r[i] + r[j] - overlap) - dist
+                m = pen > 0
+                if np.any(m):
+                    dd = d[m] / np.maximum(dist[m], 1e-12)[:, None]
+                    corr = 0.5 * pen[m][:, None] * dd
+                    np.add.at(x, i[m], corr)
+                    np.add.at(x, j[m], -corr)
+            x[:] = np.clip(x, lo + r[:, None] - overlap, hi - r[:, None] + overlap)
+    return x
+
+
+def _sphere_contacts(x, r, walls_n, walls_p, nsph, threshold=0.0):
+    """Sphere-sphere and sphere-wall contacts with gap < threshold.
+
+    The reference detects contacts at gap < GEOMETRIC_EPSILON (goc.c:431), but
+    the diagonal solvers force R = 0 on rows with gap > 0 (dbs.c:43-48,149-154)
+    while the merit function still counts their approach velocity (mrf.c:84),
+    which puts a floor under the merit that no sweep removes. The settled
+    scenes therefore keep touching pairs only (threshold 0)."""
+    from scipy.spatial import cKDTree
+    pairs = cKDTree(x).query_pairs(2 * float(r.max()) + GEOMETRIC_EPSILON, output_type='ndarray')
+    masters, slaves, points, normals, gaps = [], [], [], [], []
+    if pairs.shape[0]:
+        a, b = pairs[:, 0], pairs[:, 1]   # master a, slave b; normal from b to a
+        d = x[a] - x[b]
+        dist = np.linalg.norm(d, axis=1)
+        g = dist - r[a] - r[b]
+        m = g < threshold
+        a, b, d, dist, g = a[m], b[m], d[m], dist[m], g[m]
+        n = d / dist[:, None]
+        p = x[b] + n * (r[b] + 0.5 * g)[:, None]
+        masters.append(a); slaves.append(b); points.append(p); normals.append(n); gaps.append(g)
+    for w in range(walls_n.shape[0]):   # sphere is master, wall obstacle is slave
+        n = walls_n[w]
+        dist = (x - walls_p[w]) @ n
+        g = dist - r
+        idx = np.nonzero(g < threshold)[0]
+        if idx.size:
+            nn = np.repeat(n[None], idx.size, axis=0)
+            p = x[idx] - nn * (r[idx] + 0.5 * g[idx])[:, None]
+            masters.append(idx); slaves.append(np.full(idx.size, nsph + w)); points.append(p)
+            normals.append(nn); gaps.append(g[idx])
+    cat = lambda L, shape: np.concatenate(L) if L else np.zeros(shape)
+    return (cat(masters, (0,)).astype(np.int32), cat(slaves, (0,)).astype(np.int32),
+            cat(points, (0, 3)), cat(normals, (0, 3)), cat(gaps, (0,)))
+
+
+def _assemble_scene(name, step, x_b, rot, x0, jinv, minv, mass, velo0, obstacle, master, slave, points, normals,
+                    gaps, friction, restitution, cohesion, gravity=GRAVITY):
+    velo = velo0.copy()
+    movable = obstacle == 0
+    velo[movable, 3:6] += step * gravity  # free step: u_free = u + h M^-1 f_ext (gravity on v)
+    base = local_base(normals)
+    mpnt = _referential(rot[master], x_b[master], x0[master], points)
+    spnt = _referential(rot[slave], x_b[slave], x0[slave], points)
+    nc = master.shape[0]
+    full = lambda v: np.ascontiguousarray(np.broadcast_to(np.asarray(v, float), (nc,)).copy())
+    return Scene(name=name, step=step, dynamic=1, rot=np.ascontiguousarray(rot), x=np.ascontiguousarray(x_b),
+                 x0=np.ascontiguousarray(x0), jinv=np.ascontiguousarray(jinv), minv=np.ascontiguousarray(minv),
+                 velo=np.ascontiguousarray(velo), velo0=np.ascontiguousarray(velo0),
+                 obstacle=np.ascontiguousarray(obstacle.astype(np.int32)),
+                 master=np.ascontiguousarray(master.astype(np.int32)), slave=np.ascontiguousarray(slave.astype(np.int32)),
+                 mpnt=np.ascontiguousarray(mpnt), spnt=np.ascontiguousarray(spnt), base=base,
+                 gap=np.ascontiguousarray(gaps.astype(float)), friction=full(friction), restitution=full(restitution),
+                 cohesion=full(cohesion), mass=mass)
+
+
+def _sphere_scene(name, rng, x, r, density, lo, hi, step, friction, restitution, vel_sigma, settle_iters,
+                  drop, overlap):
+    n = x.shape[0]
+    x = _settle_spheres(x, r, np.asarray(lo, float), np.asarray(hi, float), settle_iters, drop, overlap, rng)
+    walls_n, walls_p = _walls(lo, hi)
+    master, slave, points, normals, gaps = _sphere_contacts(x, r, walls_n, walls_p, n)
+    nb = n + 6
+    mass = np.empty(nb); mass[:n] = density * 4.0 / 3.0 * math.pi * r ** 3; mass[n:] = 1.0
+    J = 0.4 * mass[:n] * r ** 2                      # solid sphere inertia
+    jinv = np.zeros((nb, 9)); jinv[:n, 0] = jinv[:n, 4] = jinv[:n, 8] = 1.0 / J
+    minv = np.zeros(nb); minv[:n] = 1.0 / mass[:n]
+    rot = np.zeros((nb, 9)); rot[:, 0] = rot[:, 4] = rot[:, 8] = 1.0
+    rot[:n] = _random_rotations(rng, n)
+    xb = np.concatenate([x, walls_p], axis=0)
+    x0 = xb.copy()
+    velo0 = np.zeros((nb, 6))
+    if vel_sigma > 0:
+        velo0[:n, 3:6] = rng.normal(0.0, vel_sigma, (n, 3))
+        velo0[:n, 0:3] = rng.normal(0.0, vel_sigma, (n, 3)) / r[:, None]
+    obstacle = np.zeros(nb, np.int32); obstacle[n:] = 1
+    fr = friction(master.shape[0]) if callable(friction) else friction
+    return _assemble_scene(name, step, xb, rot, x0, jinv, minv, mass, velo0, obstacle, master, slave, points,
+                           normals, gaps, fr, restitution, 0.0)
+
+
+# ----------------------------------------------------------------------------- configurations
+
+def spheres_lattice(seed: int = 1, n_side: int = 10, radius: float = 0.05, pitch: float = 0.11,
+                    jitter: float = 0.005, density: float = 2000.0, box: float = 1.2, friction: float = 0.3,
+                    step: float = 1e-3, settle_iters: int = 200) -> Scene:
+    """1000 spheres of radius 0.05 m on a 10^3 lattice (0.11 m pitch, +-0.005 m
+    jitter) in a 1.2 m box, settled under gravity; friction 0.3, e = 0, h = 1e-3."""
+    rng = np.random.default_rng(seed)
+    g = (np.arange(n_side) - (n_side - 1) / 2.0) * pitch
+    X, Y, Z = np.meshgrid(g, g, g + box / 2.0, indexing='ij')
+    x = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    x += rng.uniform(-jitter, jitter, x.shape)
+    r = np.full(x.shape[0], radius)
+    lo = [-box / 2, -box / 2, 0.0]; hi = [box / 2, box / 2, box]
+    return _sphere_scene('spheres-lattice-%d' % x.shape[0], rng, x, r, density, lo, hi, step, friction, 0.0, 0.0,
+                         settle_iters, 0.01, 1e-5)
+
+
+def spheres_polydisperse(seed: int = 2, n: int = 20000, rmin: float = 0.03, rmax: float = 0.06,
+                         density: float = 2500.0, box=(2.0, 2.0, 4.0), friction: float = 0.5, step: float = 5e-4,
+                         vel_sigma: float = 0.1, settle_iters: int = 200) -> Scene:
+    """Polydisperse packing: radius U[rmin, rmax], density 2500, footprint 2x2 m,
+    friction 0.5, h = 5e-4, initial velocities N(0, 0.1) m/s. Initial positions
+    by seeded random sequential addition in a column twice the box height (at
+    the box height the solid fraction would be ~0.53, beyond the jamming limit
+    of sequential addition), then settled under gravity into the 2x2x4 box."""
+    from scipy.spatial import cKDTree
+    rng = np.random.default_rng(seed)
+    r = np.sort(rng.uniform(rmin, rmax, n))[::-1].copy()   # large first
+    lo = np.array([-box[0] / 2, -box[1] / 2, 0.0]); hi = np.array([box[0] / 2, box[1] / 2, 2.0 * box[2]])
+    placed = np.zeros((0, 3)); pr = np.zeros(0)
+    k = 0
+    while k < n:
+        m = min(4096, n - k)
+        cand_r = r[k:k + m]
+        cand = rng.uniform(lo + rmax, hi - rmax, (4 * m, 3))
+        cr = np.resize(cand_r, 4 * m)
+        ok = np.ones(4 * m, bool)
+        if placed.shape[0]:
+            d, _ = cKDTree(placed).query(cand, k=1)
+            ok &= d > cr + rmax
+        acc_idx = []
+        tree_new = []
+        for c in np.nonzero(ok)[0]:
+            if len(acc_idx) >= m:
+                break
+            p = cand[c]
+            if tree_new:
+                q = np.asarray(tree_new)
+                if np.any(np.linalg.norm(q - p, axis=1) < 2 * rmax):
+                    continue
+            tree_new.append(p); acc_idx.append(c)
+        if acc_idx:
+            placed = np.concatenate([placed, cand[acc_idx]], axis=0)
+            pr = np.concatenate([pr, r[k:k + len(acc_idx)]])
+            k += len(acc_idx)
+    hi_box = np.array([box[0] / 2, box[1] / 2, 2.0 * box[2]])
+    return _sphere_scene('spheres-polydisperse-%d' % n, rng, placed, pr, density, lo, hi_box, step, friction, 0.0,
+                         vel_sigma, settle_iters, 0.02, 1e-5)
+
+
+def spheres_small(seed: int, n: int, rmin: float = 0.02, rmax: float = 0.05, friction: float = 0.4,
+                  step: float = 1e-3, density: float = 2000.0, settle_iters: int = 80) -> Scene:
+    """A small uneven sphere scene (batched-solve workload): n spheres on a
+    jittered lattice in a square column, settled under gravity."""
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(rmin, rmax, n)
+    side = max(2, int(round((n / 2.0) ** (1.0 / 3.0))))
+    layers = int(math.ceil(n / float(side * side)))
+    pitch = 2.2 * rmax
+    g = (np.arange(side) - (side - 1) / 2.0) * pitch
+    X, Y, Z = np.meshgrid(g, g, (np.arange(layers) + 0.5) * pitch, indexing='ij')
+    x = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)[:n]
+    x += rng.uniform(-0.1 * rmax, 0.1 * rmax, x.shape)
+    half = side * pitch / 2.0 + rmax
+    lo = [-half, -half, 0.0]; hi = [half, half, layers * pitch + 2 * rmax]
+    return _sphere_scene('spheres-small-%d' % n, rng, x, r, density, lo, hi, step, friction, 0.0, 0.0,
+                         settle_iters, 0.004, 1e-5)
+
+
+def _hexahedron_mass(verts: np.ndarray, density: float):
+    """Volume, mass centre and inertia (about the centre) of hexahedra given by
+    8 vertices each, by tetrahedra from the vertex mean over the 12 surface
+    triangles. verts: (n, 8, 3) ordered as the unit-cube corners (x fastest)."""
+    faces = np.array([[0, 2, 3, 1], [4, 5, 7, 6], [0, 1, 5, 4], [2, 6, 7, 3], [0, 4, 6, 2], [1, 3, 7, 5]])
+    tris = np.concatenate([faces[:, [0, 1, 2]], faces[:, [0, 2, 3]]], axis=0)
+    o = verts.mean(axis=1)
+    vol = np.zeros(verts.shape[0]); first = np.zeros((verts.shape[0], 3)); second = np.zeros((verts.shape[0], 3, 3))
+    for t in tris:
+        a, b, c = verts[:, t[0]] - o, verts[:, t[1]] - o, verts[:, t[2]] - o
+        v = np.einsum('ij,ij->i', a, np.cross(b, c)) / 6.0
+        s = a + b + c
+        vol += v
+        first += v[:, None] * s / 4.0
+        second += (v / 20.0)[:, None, None] * (np.einsum('ni,nj->nij', a, a) + np.einsum('ni,nj->nij', b, b)
+                                               + np.einsum('ni,nj->nij', c, c) + np.einsum('ni,nj->nij', s, s))
+    c_rel = first / vol[:, None]
+    cov = second - vol[:, None, None] * np.einsum('ni,nj->nij', c_rel, c_rel)
+    J = density * (np.trace(cov, axis1=1, axis2=2)[:, None, None] * np.eye(3)[None] - cov)
+    return vol, o + c_rel, J, density * vol
+
+
+def hexahedra_lattice(seed: int = 3, nx: int = 100, ny: int = 100, nz: int = 10, side: float = 0.04,
+                      perturb: float = 0.1, density: float = 2000.0, friction: float = 0.4, step: float = 5e-4,
+                      vel_sigma: float = 0.02) -> Scene:
+    """Rigid convex hexahedra: unit cubes of side 0.04 m whose 8 vertices get
+    seeded uniform perturbations of +-10% of the side, density 2000, stacked
+    face to face on a jittered nx x ny x nz lattice resting on the floor of a
+    4x4x3 m box; friction 0.4, h = 5e-4.
+
+    Contacts (a simplified convex-convex generator; the reference uses the
+    polyhedral intersection of cvi.c): one contact per face-adjacent pair and
+    per face resting on a wall, at the mid-point of the two facing face
+    centroids, with the normal the normalised mean of the two facing face
+    normals and a settled interpenetration gap drawn from -|N(0, 2e-5)| m."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    corners = np.array([[i, j, k] for k in (0, 1) for j in (0, 1) for i in (0, 1)], float) - 0.5
+    I, J_, K = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing='ij')
+    idx = np.stack([I.ravel(), J_.ravel(), K.ravel()], axis=1)
+    lat = np.stack([(idx[:, 0] - (nx - 1) / 2.0) * side, (idx[:, 1] - (ny - 1) / 2.0) * side,
+                    (idx[:, 2] + 0.5) * side], axis=1)
+    verts = lat[:, None, :] + side * (corners[None] + rng.uniform(-perturb, perturb, (n, 8, 3)))
+    vol, xc, Jt, mass_b = _hexahedron_mass(verts, density)
+    # face vertex sets (outward): -x, +x, -y, +y, -z, +z
+    fv = {0: [0, 2, 6, 4], 1: [1, 5, 7, 3], 2: [0, 4, 5, 1], 3: [2, 3, 7, 6], 4: [0, 1, 3, 2], 5: [4, 6, 7, 5]}
+
+    def face(f):
+        q = verts[:, fv[f]]
+        cen = q.mean(axis=1)
+        nrm = np.cross(q[:, 2] - q[:, 0], q[:, 3] - q[:, 1])
+        nrm *= np.sign(np.einsum('ij,ij->i', nrm, cen - xc))[:, None]   # orient outward
+        return cen, nrm / np.linalg.norm(nrm, axis=1, keepdims=True)
+
+    F = [face(f) for f in range(6)]
+    body_of = np.empty((nx, ny, nz), np.int64)
+    body_of[idx[:, 0], idx[:, 1], idx[:, 2]] = np.arange(n)
+    masters, slaves, points, normals = [], [], [], []
+    for axis, (fneg, fpos) in enumerate(((0, 1), (2, 3), (4, 5))):
+        sl_lo = [slice(None)] * 3; sl_hi = [slice(None)] * 3
+        sl_lo[axis] = slice(0, -1); sl_hi[axis] = slice(1, None)
+        a = body_of[tuple(sl_lo)].ravel(); b = body_of[tuple(sl_hi)].ravel()   # a below/left, b above/right
+        nrm = F[fpos][1][a] - F[fneg][1][b]
+        nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+        p = 0.5 * (F[fpos][0][a] + F[fneg][0][b])
+        masters.append(b); slaves.append(a); points.append(p); normals.append(nrm)   # normal from slave a to master b
+    # walls: floor and four sides of the box around the lattice
+    halfx, halfy = nx * side / 2.0 + 0.5 * side * perturb, ny * side / 2.0 + 0.5 * side * perturb
+    walls_n = np.array([[0, 0, 1], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0]], float)
+    walls_p = np.array([[0, 0, 0], [-halfx, 0, 0], [halfx, 0, 0], [0, -halfy, 0], [0, halfy, 0]], float)
+    wall_faces = [(4, body_of[:, :, 0].ravel()), (0, body_of[0, :, :].ravel()), (1, body_of[-1, :, :].ravel()),
+                  (2, body_of[:, 0, :].ravel()), (3, body_of[:, -1, :].ravel())]
+    for w, (f, bodies) in enumerate(wall_faces):
+        cen = F[f][0][bodies]
+        nn = np.repeat(walls_n[w][None], bodies.size, axis=0)
+        p = cen.copy()
+        p -= nn * ((cen - walls_p[w]) @ walls_n[w])[:, None] * 0.5
+        masters.append(bodies); slaves.append(np.full(bodies.size, n + w)); points.append(p); normals.append(nn)
+    master = np.concatenate(masters).astype(np.int32); slave = np.concatenate(slaves).astype(np.int32)
+    points = np.concatenate(points); normals = np.concatenate(normals)
+    gaps = -np.abs(rng.normal(0.0, 2e-5, master.shape[0]))
+    nb = n + walls_n.shape[0]
+    xb = np.concatenate([xc, walls_p], axis=0)
+    rot = np.zeros((nb, 9)); rot[:, 0] = rot[:, 4] = rot[:, 8] = 1.0
+    x0 = xb.copy()
+    jinv = np.zeros((nb, 9)); jinv[:n] = _colmajor(np.linalg.inv(Jt))
+    minv = np.zeros(nb); minv[:n] = 1.0 / mass_b
+    mass = np.ones(nb); mass[:n] = mass_b
+    velo0 = np.zeros((nb, 6))
+    if vel_sigma > 0:
+        velo0[:n, 3:6] = rng.normal(0.0, vel_sigma, (n, 3))
+        velo0[:n, 0:3] = rng.normal(0.0, vel_sigma / side, (n, 3))
+    obstacle = np.zeros(nb, np.int32); obstacle[n:] = 1
+    return _assemble_scene('hexahedra-lattice-%d' % n, step, xb, rot, x0, jinv, minv, mass, velo0, obstacle,
+                           master, slave, points, normals, gaps, friction, 0.0, 0.0)
+
+
+def batched_scenes(seed: int = 4, count: int = 256, nmin: int = 50, nmax: int = 2000):
+    """Uneven independent sphere scenes: body count log-uniform in [nmin, nmax],
+    radius U[0.02, 0.05], friction U[0.2, 0.6], h = 1e-3."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(math.log(nmin), math.log(nmax), count)).astype(int)
+    fr = rng.uniform(0.2, 0.6, count)
+    return [spheres_small(seed * 100003 + s, int(sizes[s]), friction=float(fr[s])) for s in range(count)]
+
+
+def advance_velocities(scene: Scene, R: np.ndarray) -> Scene:
+    """One velocity step of the rigid bodies with the solved reactions: the new
+    velocity at t is u = u_free + h M^-1 sum H^T R (bod.c:418-439 force
+    accumulation, bod.c:1425-1493 second half step), then a new free velocity
+    u_free' = u + h M^-1 f_ext. Geometry is kept (a one-step snapshot), so the
+    returned scene is the next solve of the same contact set, warm-started by R."""
+    nb = scene.nbod
+    imp = np.zeros((nb, 6))
+    Rw = np.einsum('nij,nj->ni', scene.base.reshape(-1, 3, 3).transpose(0, 2, 1), R)
+    for side, pnt, sign in ((scene.master, scene.mpnt, 1.0), (scene.slave, scene.spnt, -1.0)):
+        ok = side >= 0
+        b = side[ok]
+        rot = scene.rot[b].reshape(-1, 3, 3).transpose(0, 2, 1)
+        lever = np.einsum('nij,nj->ni', rot, pnt[ok] - scene.x0[b])          # spatial lever arm
+        f = sign * Rw[ok]
+        torque_w = np.cross(lever, f)
+        torque_b = np.einsum('nji,nj->ni', rot, torque_w)                  # body-frame torque
+        np.add.at(imp, b, np.concatenate([torque_b, f], axis=1))
+    J = scene.jinv.reshape(-1, 3, 3).transpose(0, 2, 1)
+    du = np.zeros((nb, 6))
+    du[:, 0:3] = np.einsum('nij,nj->ni', J, imp[:, 0:3])
+    du[:, 3:6] = scene.minv[:, None] * imp[:, 3:6]
+    movable = scene.obstacle == 0
+    u = scene.velo.copy()
+    u[movable] += scene.step * du[movable]
+    nxt = dataclasses.replace(scene)
+    nxt.velo0 = np.ascontiguousarray(u)
+    uf = u.copy()
+    uf[movable, 3:6] += scene.step * GRAVITY
+    nxt.velo = np.ascontiguousarray(uf)
+    return nxt
+
+
+CONFIGS = {
+    'spheres1k': spheres_lattice,
+    'spheres20k': spheres_polydisperse,
+    'hexahedra100k': hexahedra_lattice,
+}
