@@ -1,0 +1,138 @@
+/*
+ * b2_device.h -- thin C ABI of the sm_100a device layer (libsolfec_b200.so).
+ *
+ * The host code in C (solfec-1.0_b200/host/b2gs.c, declared in solfec_b200.h)
+ * drives the GPU only through these entry points: plain pointers, sizes and
+ * integer status codes, no C++ or torch types. Every function returns
+ * B2DEV_OK (0) or a negative B2DEV_E* code; b2dev_last_error() gives the text.
+ *
+ * A context holds one local-dynamics problem resident in HBM in the layout the
+ * kernels stream (rows sorted by colour, 3x3 off-diagonal blocks in a CSR of
+ * nine coefficient planes, R/U double-buffered), plus the CUDA stream all its
+ * work is queued on. It is the device mirror of the reference LOCDYN (ldy.h:81-90)
+ * together with the R/U state of its constraints (dom.h:79-81).
+ *
+ * Pointer arguments are host pointers unless the call takes an `on_device`
+ * flag that is non-zero, in which case they are device pointers on the
+ * context's device.
+ */
+#ifndef B2_DEVICE_H
+#define B2_DEVICE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum b2dev_status {
+  B2DEV_OK = 0,
+  B2DEV_EINVAL = -1,        /* invalid argument or size */
+  B2DEV_ECUDA = -2,         /* CUDA runtime error (out of memory, launch failure) */
+  B2DEV_ETIMEOUT = -3,      /* a bounded device-side wait gave up */
+  B2DEV_ECOLOURS = -4,      /* the contact graph needs more colours than supported */
+  B2DEV_EUNSUPPORTED = -5,  /* input outside the rigid contact path (e.g. self-contact) */
+  B2DEV_ESTATE = -6         /* call out of order (e.g. solve before assembly) */
+};
+
+enum b2dev_precision { B2DEV_FP64 = 0, B2DEV_MIXED = 1 };
+
+typedef struct b2dev_ctx b2dev_ctx;
+
+/* Options of one solve; meaning as struct gs (bgs.h:64-111). */
+typedef struct b2dev_solve_opts {
+  double epsilon, meritval, diagepsilon;
+  int maxiter, diagmaxiter, diagsolver, failure, reverse, nomerit;
+  int precision;   /* b2dev_precision; MIXED = FP32 off-diagonal sweeps + closing FP64 refinement */
+  int grid;        /* persistent grid size in blocks; 0 = chosen from occupancy and size */
+} b2dev_solve_opts;
+
+/* Outcome of one solve. Histories are written to caller buffers of maxiter. */
+typedef struct b2dev_solve_report {
+  int iters;                /* iterations (gs->iters) */
+  int thrown;               /* FAILURE_EXIT raised (reference THROW) */
+  int last_fail_kind;       /* 0 none, 1 DIAGONAL_DIVERGED, 2 DIAGONAL_FAILED (last failing row) */
+  int nfailures;            /* diagonal failures over the returned iterations */
+  int sweeps;               /* sweeps run (includes discarded speculative sweeps) */
+  int iters_mixed;          /* iterations spent in FP32 sweeps (mixed precision) */
+  double merit;             /* merit of the returned iterate (dom->merit) */
+  double error;             /* relative error of the returned iterate */
+  double merit_input;       /* merit of the initial reactions (0 without merit) */
+  float ms_device;          /* device time of the solve (CUDA events) */
+} b2dev_solve_report;
+
+const char* b2dev_last_error(void);
+
+/* Create a context on a CUDA device; stream may be NULL (a stream is created)
+ * or a cudaStream_t to queue all work on. */
+b2dev_ctx* b2dev_create(int device, void* stream);
+void b2dev_destroy(b2dev_ctx* ctx);
+void* b2dev_stream(b2dev_ctx* ctx);
+
+/* Rigid bodies and contacts of one step (layout documented in solfec_b200.h,
+ * b2gs_bodies / b2gs_contacts). */
+int b2dev_upload_scene(b2dev_ctx* ctx, int nbod, const double* rot, const double* x0, const double* jinv,
+                       const double* minv, const double* velo, const double* velo0, const int* obstacle,
+                       int ncon, const int* master, const int* slave, const double* mpnt, const double* spnt,
+                       const double* base, const double* gap, const double* friction, const double* restitution,
+                       const double* cohesion, int on_device);
+
+/* LOCDYN_Update_Begin: assemble W_ii, A, rho, B, V, free energy and the
+ * off-diagonal blocks of the uploaded scene, colour the contact graph and lay
+ * the rows out colour by colour. */
+int b2dev_assemble(b2dev_ctx* ctx, double step, int dynamic, uint64_t colour_seed);
+
+/* Load an already assembled local dynamics (rows in caller order, blocks of
+ * row i at adjptr[i]..adjptr[i+1]-1, Woff 9 doubles per block), colour it and
+ * lay it out; the same data the reference solver reads from LOCDYN. */
+int b2dev_upload_locdyn(b2dev_ctx* ctx, int n, const double* W, const double* A, const double* rho,
+                        const double* B, const double* V, const double* gap, const double* friction,
+                        const double* restitution, const double* cohesion, const int* adjptr, const int* adjcol,
+                        const double* Woff, double free_energy, double step, int dynamic, uint64_t colour_seed,
+                        int on_device);
+
+/* Reactions and relative velocities (3 per row, caller order): initial
+ * values before a solve, results after it. conmerit (may be NULL) receives
+ * the per-constraint merit of the last merit evaluation. */
+int b2dev_set_state(b2dev_ctx* ctx, const double* R, const double* U, int on_device);
+int b2dev_get_state(b2dev_ctx* ctx, double* R, double* U, double* conmerit, int on_device);
+
+/* Run the Gauss-Seidel solve on the resident problem. rerhist / merhist may
+ * be NULL or host buffers of opts->maxiter doubles. */
+int b2dev_solve(b2dev_ctx* ctx, const b2dev_solve_opts* opts, b2dev_solve_report* rep, double* rerhist,
+                double* merhist);
+
+/* Introspection: sizes, processing order and the assembled data (caller order). */
+int b2dev_sizes(b2dev_ctx* ctx, int* n, long long* nblocks, int* ncolours, double* free_energy);
+int b2dev_get_order(b2dev_ctx* ctx, int* order);         /* order[p] = caller row swept p-th */
+int b2dev_get_colours(b2dev_ctx* ctx, int* colour);      /* colour per caller row */
+int b2dev_get_locdyn(b2dev_ctx* ctx, double* W, double* A, double* rho, double* B, double* V,
+                     int* adjptr, int* adjcol, double* Woff, double* free_energy);
+
+/* Events-timed device duration of the last b2dev_assemble (assembly +
+ * colouring + layout), in milliseconds. */
+float b2dev_last_assemble_ms(b2dev_ctx* ctx);
+
+/* Tracing: record, for every row, the inputs and outputs of its diagonal
+ * solve in sweep `sweep` (0-based; -1 switches tracing off) of the next
+ * solves; b2dev_get_trace copies the last record out in caller row order,
+ * 16 doubles per row: B'[3], U in[3], R in[3], U out[3], R out[3], failure kind. */
+int b2dev_trace_sweep(b2dev_ctx* ctx, int sweep);
+int b2dev_get_trace(b2dev_ctx* ctx, double* out);
+
+/* One diagonal block solve (dbs.c:492-550 with the FAILURE_CONTINUE fallback
+ * chain of bgs.c:976-1003) per caller-given row, on the device: W[9], B[3]
+ * (the local free velocity B' including the off-diagonal sum), V[3], rho,
+ * gap, friction, restitution, cohesion per row; U and R (3 per row) are read
+ * as the starting point and overwritten; kind[i] = 0 ok, 1 diverged,
+ * 2 failed. Host arrays. */
+int b2dev_diag_solve_batch(b2dev_ctx* ctx, int n, int diagsolver, int failure, double diagepsilon, int diagmaxiter,
+                           int dynamic, double step, const double* W, const double* B, const double* V,
+                           const double* rho, const double* gap, const double* friction, const double* restitution,
+                           const double* cohesion, double* U, double* R, int* kind);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,249 @@
+// b2_colour.cuh -- contact-graph colouring and the colour-sorted layout.
+//
+// The reference sweeps rows in list order (bgs.c:950). Rows that share no
+// non-obstacle body are uncoupled (W_ij = 0), so any colouring of the contact
+// graph gives an order whose colours can be swept in parallel. The colouring
+// is Jones-Plassmann with smallest-available colour: in every round each
+// uncoloured row whose priority beats all uncoloured neighbours takes the
+// smallest colour no coloured neighbour holds. Priorities come from
+// jp_priority(seed, row), so the result equals the sequential greedy
+// colouring in decreasing priority order and is reproducible bit for bit on
+// the host.
+#pragma once
+
+#include <cuda_runtime.h>
+#include "b2_common.cuh"
+#include "b2_solve.cuh"
+
+namespace b2 {
+
+constexpr int kMaxColours = 256;
+
+struct ColourControl {
+  unsigned bar_count;
+  int timeout;
+  int overflow;      // more than kMaxColours colours needed
+  int ncolours;
+  int rounds;
+  unsigned remaining[3];
+};
+
+__device__ __forceinline__ bool colour_barrier(ColourControl* ctrl, unsigned nblocks, unsigned& epoch) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    epoch++;
+    __threadfence();
+    atomicAdd(&ctrl->bar_count, 1u);
+    const unsigned target = nblocks * epoch;
+    volatile unsigned* cnt = &ctrl->bar_count;
+    volatile int* to = &ctrl->timeout;
+    uint64_t t0 = globaltimer_ns();
+    while (*cnt < target) {
+      if (*to) { ok = 0; break; }
+      if (globaltimer_ns() - t0 > kBarrierLimitNs) { *to = 1; ok = 0; break; }
+      __nanosleep(32);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Persistent cooperative Jones-Plassmann colouring of the graph (adjptr,
+// adjcol). colour[] must be -1 on entry.
+__global__ void k_jp_colour(int n, const int* adjptr, const int* adjcol, unsigned long long seed, int* colour,
+                            int* sel, ColourControl* ctrl) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthreads = gridDim.x * blockDim.x;
+  const unsigned nblocks = gridDim.x;
+  unsigned epoch = 0;
+  for (int r = 0;; r++) {
+    if (tid == 0) ctrl->remaining[(r + 1) % 3] = 0u;
+    // phase 1: local maxima among uncoloured neighbours
+    for (int i = tid; i < n; i += nthreads) {
+      int s = 0;
+      if (__ldcg(colour + i) < 0) {
+        s = 1;
+        const uint64_t pi = jp_priority(seed, i);
+        for (int k = adjptr[i]; k < adjptr[i + 1]; k++) {
+          const int j = adjcol[k];
+          if (__ldcg(colour + j) < 0 && jp_priority(seed, j) > pi) { s = 0; break; }
+        }
+      }
+      sel[i] = s;
+    }
+    if (!colour_barrier(ctrl, nblocks, epoch)) return;
+    // phase 2: selected rows take the smallest colour unused by coloured neighbours
+    unsigned left = 0;
+    for (int i = tid; i < n; i += nthreads) {
+      if (__ldcg(sel + i)) {
+        unsigned long long used[kMaxColours / 64] = {0ull, 0ull, 0ull, 0ull};
+        for (int k = adjptr[i]; k < adjptr[i + 1]; k++) {
+          const int cj = __ldcg(colour + adjcol[k]);
+          if (cj >= 0) used[cj >> 6] |= 1ull << (cj & 63);
+        }
+        int c = -1;
+#pragma unroll
+        for (int w = 0; w < kMaxColours / 64; w++) {
+          if (c < 0 && ~used[w] != 0ull) c = w * 64 + __ffsll((long long)~used[w]) - 1;
+        }
+        if (c < 0) { atomicExch(&ctrl->overflow, 1); c = kMaxColours - 1; }
+        colour[i] = c;
+        atomicMax(&ctrl->ncolours, c + 1);
+      } else if (__ldcg(colour + i) < 0) {
+        left++;
+      }
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) left += __shfl_down_sync(0xffffffffu, left, d);
+    if ((threadIdx.x & 31) == 0 && left) atomicAdd(&ctrl->remaining[r % 3], left);
+    if (!colour_barrier(ctrl, nblocks, epoch)) return;
+    const unsigned rem = *(volatile unsigned*)&ctrl->remaining[r % 3];
+    if (rem == 0u || *(volatile int*)&ctrl->overflow) {
+      if (tid == 0) ctrl->rounds = r + 1;
+      return;
+    }
+  }
+}
+
+// colour offsets from the colour-sorted keys
+__global__ void k_colptr(int n, const int* sorted_colour, int ncolours, int* colptr) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p > n) return;
+  const int cur = p < n ? sorted_colour[p] : ncolours;
+  const int prev = p > 0 ? sorted_colour[p - 1] : -1;
+  for (int c = prev + 1; c <= cur; c++) colptr[c] = p;
+}
+
+__global__ void k_inverse_perm(int n, const int* perm, int* iperm) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) iperm[perm[p]] = p;
+}
+
+__global__ void k_sorted_degree(int n, const int* perm, const int* adjptr, int* deg) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) { const int i = perm[p]; deg[p] = adjptr[i + 1] - adjptr[i]; }
+}
+
+// Off-diagonal blocks in the colour-sorted CSR computed from the row factors:
+// W_ij = h H_i^b M_b^-1 H_j^b^T for j > i (ldy.c:738-794, serial form
+// left = H_i, right = M^-1 H_j^T) and the transposed block of the pair for
+// j < i (ldy.c:829-844); the transposed block is recomputed with identical
+// operands and order, so it is bitwise the transpose. Warp per sorted row.
+__global__ void k_offdiag_assembled(int n, const int* perm, const int* iperm, const int* adjptr, const int* adjcol,
+                                    const int* adjbod, const int* master, const double* factors, double step,
+                                    const int* rowptr, int* col, double* W64, float* W32, long long kstride) {
+  const int p = blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
+  const int lane = threadIdx.x & (kWarp - 1);
+  if (p >= n) return;
+  const int i = perm[p];
+  const int kb = adjptr[i], d = adjptr[i + 1] - kb, qb = rowptr[p];
+  for (int t = lane; t < d; t += kWarp) {
+    const int j = adjcol[kb + t], b = adjbod[kb + t];
+    const int lo = j > i ? i : j, hi = j > i ? j : i;
+    const double* left = factors + (size_t)lo * kFactorStride + (master[lo] == b ? 0 : 36);
+    const double* right = factors + (size_t)hi * kFactorStride + (master[hi] == b ? 18 : 54);
+    double Lr[18], Pr[18], W[9];
+#pragma unroll
+    for (int q = 0; q < 18; q++) { Lr[q] = left[q]; Pr[q] = right[q]; }
+#pragma unroll
+    for (int q = 0; q < 9; q++) W[q] = 0.0;
+    hp_add(Lr, Pr, W);
+#pragma unroll
+    for (int q = 0; q < 9; q++) W[q] *= step;
+    const long long qo = qb + t;
+    col[qo] = iperm[j];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const double v = j > i ? W[3 * c + r] : W[3 * r + c];  // (r, c) of W_ij
+        W64[(3 * c + r) * kstride + qo] = v;
+        W32[(3 * c + r) * kstride + qo] = (float)v;
+      }
+  }
+}
+
+// Off-diagonal blocks handed in by the caller (AoS, 9 doubles per block in
+// caller CSR order) gathered into the colour-sorted plane layout.
+__global__ void k_offdiag_copy(int n, const int* perm, const int* iperm, const int* adjptr, const int* adjcol,
+                               const double* Woff, const int* rowptr, int* col, double* W64, float* W32,
+                               long long kstride) {
+  const int p = blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
+  const int lane = threadIdx.x & (kWarp - 1);
+  if (p >= n) return;
+  const int i = perm[p];
+  const int kb = adjptr[i], d = adjptr[i + 1] - kb, qb = rowptr[p];
+  for (int t = lane; t < d; t += kWarp) {
+    const long long qo = qb + t;
+    col[qo] = iperm[adjcol[kb + t]];
+    const double* w = Woff + (size_t)9 * (kb + t);
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+      const double v = w[q];
+      W64[q * kstride + qo] = v;
+      W32[q * kstride + qo] = (float)v;
+    }
+  }
+}
+
+// Row quantities (caller order, AoS) into the colour-sorted plane layout.
+__global__ void k_rows_permute(int n, const int* perm, const double* Wii, const double* Aii, const double* rho_in,
+                               const double* Bi, const double* Vi, const double* gap_in, const double* fric_in,
+                               const double* rest_in, const double* coh_in, double* Wd, double* Ad, double* Bv,
+                               double* Vv, double* rho, double* gap, double* fric, double* rest, double* coh) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int i = perm[p];
+#pragma unroll
+  for (int q = 0; q < 9; q++) {
+    Wd[(size_t)q * n + p] = Wii[(size_t)9 * i + q];
+    Ad[(size_t)q * n + p] = Aii[(size_t)9 * i + q];
+  }
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    Bv[(size_t)q * n + p] = Bi[(size_t)3 * i + q];
+    Vv[(size_t)q * n + p] = Vi[(size_t)3 * i + q];
+  }
+  rho[p] = rho_in[i];
+  gap[p] = gap_in[i];
+  fric[p] = fric_in[i];
+  rest[p] = rest_in[i];
+  coh[p] = coh_in[i];
+}
+
+// Initial R and U (caller order, 3 doubles per row) into the sorted buffers.
+__global__ void k_state_in(int n, const int* perm, const double* R, const double* U, double4* R64, float4* R32,
+                           double4* Us) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int i = perm[p];
+  const double r0 = R[3 * (size_t)i], r1 = R[3 * (size_t)i + 1], r2 = R[3 * (size_t)i + 2];
+  R64[p] = make_double4(r0, r1, r2, 0.0);
+  R32[p] = make_float4((float)r0, (float)r1, (float)r2, 0.f);
+  Us[p] = make_double4(U[3 * (size_t)i], U[3 * (size_t)i + 1], U[3 * (size_t)i + 2], 0.0);
+}
+
+// Final R, U and per-constraint merit back into caller order.
+__global__ void k_state_out(int n, const int* perm, const double4* R64, const double4* Usrc, const double* conmerit,
+                            double merit_denom, double* R, double* U, double* cm) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int i = perm[p];
+  const double4 r = R64[p], u = Usrc[p];
+  R[3 * (size_t)i] = r.x; R[3 * (size_t)i + 1] = r.y; R[3 * (size_t)i + 2] = r.z;
+  U[3 * (size_t)i] = u.x; U[3 * (size_t)i + 1] = u.y; U[3 * (size_t)i + 2] = u.z;
+  if (cm && conmerit) cm[i] = conmerit[p] / merit_denom;
+}
+
+// Shadow copy of a double buffer into its float buffer (start of a mixed solve).
+__global__ void k_shadow(int n, const double4* R64, float4* R32) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double4 r = R64[p];
+  R32[p] = make_float4((float)r.x, (float)r.y, (float)r.z, 0.f);
+}
+
+}  // namespace b2

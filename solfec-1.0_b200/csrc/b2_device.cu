@@ -1,0 +1,874 @@
+// b2_device.cu -- device layer of the B200 contact-solve path: context, memory,
+// kernel orchestration and the thin C ABI declared in include/b2_device.h.
+//
+// Per step the path is: upload (optional) -> row factors, W_ii, rho, A, B, V,
+// free energy -> contact graph through shared bodies -> Jones-Plassmann
+// colouring -> colour-sorted CSR of 3x3 blocks in nine coefficient planes ->
+// persistent Gauss-Seidel solve with the merit fused into the next sweep ->
+// results scattered back to the caller's row order.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <cfloat>
+#include <vector>
+#include <algorithm>
+
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include "../../include/b2_device.h"
+#include "b2_common.cuh"
+#include "b2_diag.cuh"
+#include "b2_solve.cuh"
+#include "b2_assemble.cuh"
+#include "b2_colour.cuh"
+
+using namespace b2;
+
+namespace {
+
+thread_local char g_err[1024] = "";
+
+void set_err(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+}
+
+#define B2_CK(call)                                                                  \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      set_err("%s failed at %s:%d: %s", #call, __FILE__, __LINE__, cudaGetErrorString(e_)); \
+      return B2DEV_ECUDA;                                                            \
+    }                                                                                \
+  } while (0)
+
+#define B2_TRY(expr)             \
+  do {                           \
+    int rc_ = (expr);            \
+    if (rc_ != B2DEV_OK) return rc_; \
+  } while (0)
+
+struct Buf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+// Grow-only device buffer of at least `bytes` (contents not preserved).
+int ensure(Buf& b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.cap >= bytes) return B2DEV_OK;
+  if (b.p) { cudaFree(b.p); b.p = nullptr; b.cap = 0; }
+  size_t want = bytes + bytes / 8;  // headroom for growing problems
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) {
+    set_err("cudaMalloc(%zu bytes) failed: %s", want, cudaGetErrorString(e));
+    return B2DEV_ECUDA;
+  }
+  b.cap = want;
+  return B2DEV_OK;
+}
+
+template <class T>
+T* ptr(Buf& b) { return static_cast<T*>(b.p); }
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+inline int blocks_for(long long n, int t) { return (int)std::max<long long>(1, (n + t - 1) / t); }
+
+__global__ void k_iota(int n, int* v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = i;
+}
+
+// adjptr monotone within [0, K] and every adjcol in [0, n)
+__global__ void k_check_graph(int n, long long K, const int* adjptr, const int* adjcol, int* bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int a = adjptr[i], b = adjptr[i + 1];
+  if (a < 0 || b < a || b > K || (i == 0 && a != 0)) { atomicExch(bad, 1); return; }
+  for (int k = a; k < b; k++)
+    if (adjcol[k] < 0 || adjcol[k] >= n) { atomicExch(bad, 1); return; }
+}
+
+__global__ void k_set_last_zero(int* a, int n) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) a[n] = 0;
+}
+
+// one diagonal block solve per thread on caller-given rows (unit parity of the
+// device diagonal solvers)
+__global__ void k_diag_batch(int n, int solver, int failure, double diagepsilon, int diagmaxiter, int dynamic,
+                             double step, const double* W, const double* B, const double* V, const double* rho,
+                             const double* gap, const double* fric, const double* rest, const double* coh, double* U,
+                             double* R, int* kind) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  ContactParams cp;
+  cp.friction = fric[i]; cp.restitution = rest[i]; cp.cohesion = coh[i]; cp.gap = gap[i]; cp.step = step;
+  cp.dynamic = dynamic;
+  double w[9], b[3], v[3], u[3], r[3];
+  for (int q = 0; q < 9; q++) w[q] = W[9 * (size_t)i + q];
+  for (int q = 0; q < 3; q++) { b[q] = B[3 * (size_t)i + q]; v[q] = V[3 * (size_t)i + q]; u[q] = U[3 * (size_t)i + q]; r[q] = R[3 * (size_t)i + q]; }
+  kind[i] = diagonal_solve_row(solver, failure, cp, diagepsilon, diagmaxiter, rho[i], w, b, v, u, r);
+  for (int q = 0; q < 3; q++) { U[3 * (size_t)i + q] = u[q]; R[3 * (size_t)i + q] = r[q]; }
+}
+
+// caller-order blocks back out of the sorted plane layout (introspection)
+__global__ void k_offdiag_out(int n, const int* iperm, const int* adjptr, const int* rowptr, const double* W64,
+                              long long kstride, double* Woff) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int kb = adjptr[i], d = adjptr[i + 1] - kb, qb = rowptr[iperm[i]];
+  for (int t = 0; t < d; t++)
+    for (int q = 0; q < 9; q++) Woff[(size_t)9 * (kb + t) + q] = W64[q * kstride + qb + t];
+}
+
+}  // namespace
+
+struct b2dev_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sms = 0;
+
+  // scene (caller order)
+  int nbod = 0, ncon = 0;
+  Buf rot, x0, jinv, minv, velo, velo0, obst, master, slave, mpnt, spnt, base;
+  Buf gap_c, fric_c, rest_c, coh_c;
+  bool have_scene = false;
+
+  // caller-order row data and graph
+  Buf factors, Wii, Aii, rho_c, B_c, V_c, fe_part, fe_dev, bad;
+  Buf bdeg, bptr, cursor, brow, deg, adjptr, adjcol, adjbod, Woff_c;
+  bool assembled_mode = false;
+
+  // colouring and layout
+  Buf colour, sel, cctrl, keys_out, iota, perm, iperm, colptr, sdeg;
+  Buf rowptr, col, W64, W32, Wd, Ad, Bv, Vv, rho, gap, fric, rest, coh;
+  std::vector<int> colptr_h;
+
+  // state and solve scratch
+  Buf R64[2], R32[2], Us, Um, conmerit, part, rer, mer, failkey, failcount, sctrl, io, cub_tmp, trace;
+  int trace_sweep = -1;  // sweep of the next solve whose diagonal solves are recorded
+
+  int n = 0;
+  long long K = 0, kstride = 0;
+  int ncolours = 0;
+  double free_energy = 0.0, step = 0.0;
+  int dynamic = 1;
+  bool ready = false;
+  int state_parity = 0;        // R64 buffer holding the current reactions
+  bool state_u_merit = false;  // current U lives in Um (true) or Us
+  bool have_conmerit = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  float assemble_ms = 0.f;
+};
+
+namespace {
+
+int scan_exclusive(b2dev_ctx* c, const int* in, int* out, int count) {
+  size_t bytes = 0;
+  B2_CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, count, c->stream));
+  B2_TRY(ensure(c->cub_tmp, bytes));
+  B2_CK(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, bytes, in, out, count, c->stream));
+  return B2DEV_OK;
+}
+
+int cooperative_grid(const void* func, int threads, int sms, int want, int* grid, size_t smem = 0) {
+  int per_sm = 0;
+  if (smem > 0) B2_CK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  B2_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem));
+  if (per_sm < 1) {
+    set_err("kernel cannot be resident with %d threads per block", threads);
+    return B2DEV_ECUDA;
+  }
+  int cap = per_sm * sms;
+  *grid = std::max(1, std::min(cap, want > 0 ? want : cap));
+  return B2DEV_OK;
+}
+
+// Colour the caller-order graph (adjptr/adjcol) and build the colour-sorted
+// layout; row data must already sit in the caller-order buffers.
+int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
+  const int n = c->n;
+  cudaStream_t st = c->stream;
+  const int T = 256;
+  B2_TRY(ensure(c->colour, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->sel, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->cctrl, sizeof(ColourControl)));
+  B2_TRY(ensure(c->keys_out, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->iota, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->perm, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->iperm, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->colptr, sizeof(int) * (kMaxColours + 2)));
+  B2_TRY(ensure(c->sdeg, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->rowptr, sizeof(int) * (n + 1)));
+
+  ColourControl cc;
+  B2_CK(cudaMemsetAsync(c->colour.p, 0xff, sizeof(int) * (n + 1), st));
+  B2_CK(cudaMemsetAsync(c->cctrl.p, 0, sizeof(ColourControl), st));
+  if (n > 0) {
+    int grid = 0;
+    B2_TRY(cooperative_grid((const void*)k_jp_colour, T, c->sms, blocks_for(n, T), &grid));
+    int nn = n;
+    const int* ap = ptr<int>(c->adjptr);
+    const int* ac = ptr<int>(c->adjcol);
+    unsigned long long sd = seed;
+    int* colp = ptr<int>(c->colour);
+    int* selp = ptr<int>(c->sel);
+    ColourControl* ctl = ptr<ColourControl>(c->cctrl);
+    void* args[] = {&nn, &ap, &ac, &sd, &colp, &selp, &ctl};
+    B2_CK(cudaLaunchCooperativeKernel((const void*)k_jp_colour, grid, T, args, 0, st));
+  }
+  B2_CK(cudaMemcpyAsync(&cc, c->cctrl.p, sizeof cc, cudaMemcpyDeviceToHost, st));
+  B2_CK(cudaStreamSynchronize(st));
+  if (cc.timeout) { set_err("colouring: grid barrier wait timed out"); return B2DEV_ETIMEOUT; }
+  if (cc.overflow) { set_err("colouring: more than %d colours needed", kMaxColours); return B2DEV_ECOLOURS; }
+  c->ncolours = n > 0 ? cc.ncolours : 0;
+
+  // rows sorted by colour, ascending row index inside a colour (stable radix sort)
+  k_iota<<<blocks_for(n, T), T, 0, st>>>(n, ptr<int>(c->iota));
+  if (n > 0) {
+    size_t bytes = 0;
+    B2_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, ptr<int>(c->colour), ptr<int>(c->keys_out),
+                                          ptr<int>(c->iota), ptr<int>(c->perm), n, 0, 9, st));
+    B2_TRY(ensure(c->cub_tmp, bytes));
+    B2_CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, bytes, ptr<int>(c->colour), ptr<int>(c->keys_out),
+                                          ptr<int>(c->iota), ptr<int>(c->perm), n, 0, 9, st));
+  }
+  k_colptr<<<blocks_for(n + 1, T), T, 0, st>>>(n, ptr<int>(c->keys_out), c->ncolours, ptr<int>(c->colptr));
+  k_inverse_perm<<<blocks_for(n, T), T, 0, st>>>(n, ptr<int>(c->perm), ptr<int>(c->iperm));
+  k_sorted_degree<<<blocks_for(n, T), T, 0, st>>>(n, ptr<int>(c->perm), ptr<int>(c->adjptr), ptr<int>(c->sdeg));
+  k_set_last_zero<<<1, 32, 0, st>>>(ptr<int>(c->sdeg), n);
+  B2_TRY(scan_exclusive(c, ptr<int>(c->sdeg), ptr<int>(c->rowptr), n + 1));
+
+  c->colptr_h.assign(c->ncolours + 1, 0);
+  if (c->ncolours > 0)
+    B2_CK(cudaMemcpyAsync(c->colptr_h.data(), c->colptr.p, sizeof(int) * (c->ncolours + 1), cudaMemcpyDeviceToHost, st));
+
+  const long long K = c->K;
+  c->kstride = ((K + 31) / 32) * 32;
+  B2_TRY(ensure(c->col, sizeof(int) * (K + 1)));
+  B2_TRY(ensure(c->W64, sizeof(double) * 9 * (c->kstride + 1)));
+  B2_TRY(ensure(c->W32, sizeof(float) * 9 * (c->kstride + 1)));
+  const int wpb = 8;
+  if (n > 0 && K > 0) {
+    if (assembled) {
+      k_offdiag_assembled<<<blocks_for(n, wpb), wpb * kWarp, 0, st>>>(
+          n, ptr<int>(c->perm), ptr<int>(c->iperm), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<int>(c->adjbod),
+          ptr<int>(c->master), ptr<double>(c->factors), c->step, ptr<int>(c->rowptr), ptr<int>(c->col),
+          ptr<double>(c->W64), ptr<float>(c->W32), c->kstride);
+    } else {
+      k_offdiag_copy<<<blocks_for(n, wpb), wpb * kWarp, 0, st>>>(
+          n, ptr<int>(c->perm), ptr<int>(c->iperm), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<double>(c->Woff_c),
+          ptr<int>(c->rowptr), ptr<int>(c->col), ptr<double>(c->W64), ptr<float>(c->W32), c->kstride);
+    }
+  }
+  B2_TRY(ensure(c->Wd, sizeof(double) * 9 * (n + 1)));
+  B2_TRY(ensure(c->Ad, sizeof(double) * 9 * (n + 1)));
+  B2_TRY(ensure(c->Bv, sizeof(double) * 3 * (n + 1)));
+  B2_TRY(ensure(c->Vv, sizeof(double) * 3 * (n + 1)));
+  B2_TRY(ensure(c->rho, sizeof(double) * (n + 1)));
+  B2_TRY(ensure(c->gap, sizeof(double) * (n + 1)));
+  B2_TRY(ensure(c->fric, sizeof(double) * (n + 1)));
+  B2_TRY(ensure(c->rest, sizeof(double) * (n + 1)));
+  B2_TRY(ensure(c->coh, sizeof(double) * (n + 1)));
+  k_rows_permute<<<blocks_for(n, T), T, 0, st>>>(
+      n, ptr<int>(c->perm), ptr<double>(c->Wii), ptr<double>(c->Aii), ptr<double>(c->rho_c), ptr<double>(c->B_c),
+      ptr<double>(c->V_c), ptr<double>(c->gap_c), ptr<double>(c->fric_c), ptr<double>(c->rest_c),
+      ptr<double>(c->coh_c), ptr<double>(c->Wd), ptr<double>(c->Ad), ptr<double>(c->Bv), ptr<double>(c->Vv),
+      ptr<double>(c->rho), ptr<double>(c->gap), ptr<double>(c->fric), ptr<double>(c->rest), ptr<double>(c->coh));
+
+  for (int b = 0; b < 2; b++) {
+    B2_TRY(ensure(c->R64[b], sizeof(double4) * (n + 1)));
+    B2_TRY(ensure(c->R32[b], sizeof(float4) * (n + 1)));
+  }
+  B2_TRY(ensure(c->Us, sizeof(double4) * (n + 1)));
+  B2_TRY(ensure(c->Um, sizeof(double4) * (n + 1)));
+  B2_TRY(ensure(c->conmerit, sizeof(double) * (n + 1)));
+  // new contacts start from R = U = 0 (MEM_Alloc zeroes, mem.c:64-86)
+  B2_CK(cudaMemsetAsync(c->R64[0].p, 0, sizeof(double4) * (n + 1), st));
+  B2_CK(cudaMemsetAsync(c->R32[0].p, 0, sizeof(float4) * (n + 1), st));
+  B2_CK(cudaMemsetAsync(c->Us.p, 0, sizeof(double4) * (n + 1), st));
+  B2_CK(cudaMemsetAsync(c->conmerit.p, 0, sizeof(double) * (n + 1), st));
+  c->state_parity = 0;
+  c->state_u_merit = false;
+  c->have_conmerit = false;
+  B2_CK(cudaGetLastError());
+  B2_CK(cudaStreamSynchronize(st));
+  c->ready = true;
+  return B2DEV_OK;
+}
+
+template <class T>
+int upload(b2dev_ctx* c, Buf& b, const T* src, size_t count, int on_device) {
+  B2_TRY(ensure(b, sizeof(T) * (count + 1)));
+  if (count == 0) return B2DEV_OK;
+  if (!src) { set_err("null input array"); return B2DEV_EINVAL; }
+  B2_CK(cudaMemcpyAsync(b.p, src, sizeof(T) * count, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                        c->stream));
+  return B2DEV_OK;
+}
+
+int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter, int iter0, int in_parity,
+                 int u0_from_merit, int grid_req, SolveControl* out) {
+  const int n = c->n;
+  cudaStream_t st = c->stream;
+  const void* fn = mixed ? (const void*)k_solve<true> : (const void*)k_solve<false>;
+  // blocks needed for the largest colour (8 row tiles of 32 per block)
+  int maxc = 0;
+  for (int k = 0; k < c->ncolours; k++) maxc = std::max(maxc, c->colptr_h[k + 1] - c->colptr_h[k]);
+  const int want = grid_req > 0 ? grid_req : blocks_for(blocks_for(maxc, kWarp), kSolveWarps);
+  int grid = 0;
+  const size_t smem = mixed ? solve_smem_bytes<true>() : solve_smem_bytes<false>();
+  B2_TRY(cooperative_grid(fn, kSolveThreads, c->sms, want, &grid, smem));
+  B2_TRY(ensure(c->part, sizeof(double) * 2 * 4 * grid));
+  B2_CK(cudaMemsetAsync(c->sctrl.p, 0, sizeof(SolveControl), st));
+  B2_CK(cudaMemsetAsync(ptr<unsigned long long>(c->failkey) + iter0, 0, sizeof(unsigned long long) * (maxiter + 1), st));
+  B2_CK(cudaMemsetAsync(ptr<unsigned>(c->failcount) + iter0, 0, sizeof(unsigned) * (maxiter + 1), st));
+
+  SolveArgs a;
+  memset(&a, 0, sizeof a);
+  a.n = n;
+  a.ncolours = c->ncolours;
+  a.colptr = ptr<int>(c->colptr);
+  a.rowptr = ptr<int>(c->rowptr);
+  a.col = ptr<int>(c->col);
+  a.W64 = ptr<double>(c->W64);
+  a.W32 = ptr<float>(c->W32);
+  a.kstride = c->kstride;
+  a.Wd = ptr<double>(c->Wd);
+  a.Ad = ptr<double>(c->Ad);
+  a.Bv = ptr<double>(c->Bv);
+  a.Vv = ptr<double>(c->Vv);
+  a.rho = ptr<double>(c->rho);
+  a.gap = ptr<double>(c->gap);
+  a.fric = ptr<double>(c->fric);
+  a.rest = ptr<double>(c->rest);
+  a.coh = ptr<double>(c->coh);
+  a.R64[0] = ptr<double4>(c->R64[0]);
+  a.R64[1] = ptr<double4>(c->R64[1]);
+  a.R32[0] = ptr<float4>(c->R32[0]);
+  a.R32[1] = ptr<float4>(c->R32[1]);
+  a.Us = ptr<double4>(c->Us);
+  a.Um = ptr<double4>(c->Um);
+  a.conmerit = ptr<double>(c->conmerit);
+  a.part = ptr<double>(c->part);
+  a.rerhist = ptr<double>(c->rer);
+  a.merhist = ptr<double>(c->mer);
+  a.failkey = ptr<unsigned long long>(c->failkey);
+  a.failcount = ptr<unsigned>(c->failcount);
+  a.ctrl = ptr<SolveControl>(c->sctrl);
+  a.epsilon = o->epsilon;
+  a.meritval = o->meritval;
+  a.diagepsilon = o->diagepsilon;
+  a.step = c->step;
+  double lo = c->free_energy < DBL_EPSILON ? 1.0 : c->free_energy;  // mrf.c:45
+  a.merit_denom = lo == 0.0 ? 1.0 : lo;                             // mrf.c:177
+  a.maxiter = maxiter;
+  a.diagmaxiter = o->diagmaxiter;
+  a.diagsolver = o->diagsolver;
+  a.failure = o->failure;
+  a.dynamic = c->dynamic;
+  a.reverse = o->reverse;
+  a.nomerit = o->nomerit;
+  a.iter0 = iter0;
+  a.in_parity = in_parity;
+  a.u0_from_merit = u0_from_merit;
+  if (c->trace_sweep >= 0 && iter0 == 0) {
+    B2_TRY(ensure(c->trace, sizeof(double) * kTraceStride * (n + 1)));
+    B2_CK(cudaMemsetAsync(c->trace.p, 0, sizeof(double) * kTraceStride * (n + 1), st));
+    a.trace = ptr<double>(c->trace);
+    a.trace_sweep = c->trace_sweep;
+  }
+  void* args[] = {&a};
+  B2_CK(cudaLaunchCooperativeKernel(fn, grid, kSolveThreads, args, smem, st));
+  B2_CK(cudaMemcpyAsync(out, c->sctrl.p, sizeof(SolveControl), cudaMemcpyDeviceToHost, st));
+  B2_CK(cudaStreamSynchronize(st));
+  if (out->timeout) { set_err("solve: grid barrier wait timed out"); return B2DEV_ETIMEOUT; }
+  return B2DEV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* b2dev_last_error(void) { return g_err; }
+
+b2dev_ctx* b2dev_create(int device, void* stream) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    set_err("no CUDA device %d (found %d)", device, ndev);
+    return nullptr;
+  }
+  DeviceGuard g(device);
+  b2dev_ctx* c = new b2dev_ctx();
+  c->device = device;
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+  if (!coop) {
+    set_err("device %d does not support cooperative launches", device);
+    delete c;
+    return nullptr;
+  }
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      set_err("cudaStreamCreate failed");
+      delete c;
+      return nullptr;
+    }
+    c->own_stream = true;
+  }
+  for (int k = 0; k < 4; k++) cudaEventCreate(&c->ev[k]);
+  if (ensure(c->sctrl, sizeof(SolveControl)) != B2DEV_OK || ensure(c->fe_dev, sizeof(double)) != B2DEV_OK ||
+      ensure(c->bad, sizeof(int)) != B2DEV_OK) {
+    b2dev_destroy(c);
+    return nullptr;
+  }
+  return c;
+}
+
+void b2dev_destroy(b2dev_ctx* c) {
+  if (!c) return;
+  DeviceGuard g(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  Buf* all[] = {&c->rot, &c->x0, &c->jinv, &c->minv, &c->velo, &c->velo0, &c->obst, &c->master, &c->slave,
+                &c->mpnt, &c->spnt, &c->base, &c->gap_c, &c->fric_c, &c->rest_c, &c->coh_c, &c->factors, &c->Wii,
+                &c->Aii, &c->rho_c, &c->B_c, &c->V_c, &c->fe_part, &c->fe_dev, &c->bad, &c->bdeg, &c->bptr,
+                &c->cursor, &c->brow, &c->deg, &c->adjptr, &c->adjcol, &c->adjbod, &c->Woff_c, &c->colour, &c->sel,
+                &c->cctrl, &c->keys_out, &c->iota, &c->perm, &c->iperm, &c->colptr, &c->sdeg, &c->rowptr, &c->col,
+                &c->W64, &c->W32, &c->Wd, &c->Ad, &c->Bv, &c->Vv, &c->rho, &c->gap, &c->fric, &c->rest, &c->coh,
+                &c->R64[0], &c->R64[1], &c->R32[0], &c->R32[1], &c->Us, &c->Um, &c->conmerit, &c->part, &c->rer,
+                &c->mer, &c->failkey, &c->failcount, &c->sctrl, &c->io, &c->cub_tmp, &c->trace};
+  for (Buf* b : all)
+    if (b->p) cudaFree(b->p);
+  for (int k = 0; k < 4; k++)
+    if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+void* b2dev_stream(b2dev_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int b2dev_upload_scene(b2dev_ctx* c, int nbod, const double* rot, const double* x0, const double* jinv,
+                       const double* minv, const double* velo, const double* velo0, const int* obstacle, int ncon,
+                       const int* master, const int* slave, const double* mpnt, const double* spnt,
+                       const double* base, const double* gap, const double* friction, const double* restitution,
+                       const double* cohesion, int on_device) {
+  if (!c || nbod < 0 || ncon < 0) { set_err("invalid scene sizes"); return B2DEV_EINVAL; }
+  DeviceGuard g(c->device);
+  c->nbod = nbod;
+  c->ncon = ncon;
+  B2_TRY(upload(c, c->rot, rot, (size_t)9 * nbod, on_device));
+  B2_TRY(upload(c, c->x0, x0, (size_t)3 * nbod, on_device));
+  B2_TRY(upload(c, c->jinv, jinv, (size_t)9 * nbod, on_device));
+  B2_TRY(upload(c, c->minv, minv, (size_t)nbod, on_device));
+  B2_TRY(upload(c, c->velo, velo, (size_t)6 * nbod, on_device));
+  B2_TRY(upload(c, c->velo0, velo0, (size_t)6 * nbod, on_device));
+  B2_TRY(upload(c, c->obst, obstacle, (size_t)nbod, on_device));
+  B2_TRY(upload(c, c->master, master, (size_t)ncon, on_device));
+  B2_TRY(upload(c, c->slave, slave, (size_t)ncon, on_device));
+  B2_TRY(upload(c, c->mpnt, mpnt, (size_t)3 * ncon, on_device));
+  B2_TRY(upload(c, c->spnt, spnt, (size_t)3 * ncon, on_device));
+  B2_TRY(upload(c, c->base, base, (size_t)9 * ncon, on_device));
+  B2_TRY(upload(c, c->gap_c, gap, (size_t)ncon, on_device));
+  B2_TRY(upload(c, c->fric_c, friction, (size_t)ncon, on_device));
+  B2_TRY(upload(c, c->rest_c, restitution, (size_t)ncon, on_device));
+  B2_TRY(upload(c, c->coh_c, cohesion, (size_t)ncon, on_device));
+  c->have_scene = true;
+  c->ready = false;
+  return B2DEV_OK;
+}
+
+int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed) {
+  if (!c || !c->have_scene) { set_err("assemble: no scene uploaded"); return B2DEV_ESTATE; }
+  if (!(step > 0.0)) { set_err("assemble: step must be positive"); return B2DEV_EINVAL; }
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  const int T = 256;
+  const int n = c->ncon, nb = c->nbod;
+  c->n = n;
+  c->step = step;
+  c->dynamic = dynamic ? 1 : 0;
+  c->assembled_mode = true;
+  B2_CK(cudaEventRecord(c->ev[0], st));
+
+  B2_TRY(ensure(c->factors, sizeof(double) * kFactorStride * (n + 1)));
+  B2_TRY(ensure(c->Wii, sizeof(double) * 9 * (n + 1)));
+  B2_TRY(ensure(c->Aii, sizeof(double) * 9 * (n + 1)));
+  B2_TRY(ensure(c->rho_c, sizeof(double) * (n + 1)));
+  B2_TRY(ensure(c->B_c, sizeof(double) * 3 * (n + 1)));
+  B2_TRY(ensure(c->V_c, sizeof(double) * 3 * (n + 1)));
+  const int rb = blocks_for(n, T);
+  B2_TRY(ensure(c->fe_part, sizeof(double) * rb));
+  B2_CK(cudaMemsetAsync(c->bad.p, 0, sizeof(int), st));
+
+  SceneDev sc;
+  sc.nbod = nb; sc.ncon = n;
+  sc.rot = ptr<double>(c->rot); sc.x0 = ptr<double>(c->x0); sc.jinv = ptr<double>(c->jinv);
+  sc.minv = ptr<double>(c->minv); sc.velo = ptr<double>(c->velo); sc.velo0 = ptr<double>(c->velo0);
+  sc.obstacle = ptr<int>(c->obst); sc.master = ptr<int>(c->master); sc.slave = ptr<int>(c->slave);
+  sc.mpnt = ptr<double>(c->mpnt); sc.spnt = ptr<double>(c->spnt); sc.base = ptr<double>(c->base);
+  k_row_factors<<<rb, T, 0, st>>>(sc, step, ptr<double>(c->factors), ptr<double>(c->Wii), ptr<double>(c->Aii),
+                                  ptr<double>(c->rho_c), ptr<double>(c->B_c), ptr<double>(c->V_c),
+                                  ptr<double>(c->fe_part), ptr<int>(c->bad));
+  k_sum_partials<<<1, 1024, 0, st>>>(ptr<double>(c->fe_part), rb, ptr<double>(c->fe_dev));
+  {  // body indices are checked before any kernel indexes per-body arrays with them
+    int bad0 = 0;
+    B2_CK(cudaMemcpyAsync(&bad0, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaStreamSynchronize(st));
+    if (bad0) { set_err("assemble: self-contact or invalid body index (outside the rigid contact path)"); return B2DEV_EUNSUPPORTED; }
+  }
+
+  // contact graph through shared non-obstacle bodies
+  B2_TRY(ensure(c->bdeg, sizeof(int) * (nb + 1)));
+  B2_TRY(ensure(c->bptr, sizeof(int) * (nb + 1)));
+  B2_TRY(ensure(c->cursor, sizeof(int) * (nb + 1)));
+  B2_CK(cudaMemsetAsync(c->bdeg.p, 0, sizeof(int) * (nb + 1), st));
+  B2_CK(cudaMemsetAsync(c->cursor.p, 0, sizeof(int) * (nb + 1), st));
+  k_body_count<<<rb, T, 0, st>>>(n, ptr<int>(c->master), ptr<int>(c->slave), ptr<int>(c->obst), ptr<int>(c->bdeg));
+  B2_TRY(scan_exclusive(c, ptr<int>(c->bdeg), ptr<int>(c->bptr), nb + 1));
+  B2_TRY(ensure(c->brow, sizeof(int) * (2 * (size_t)n + 1)));
+  k_body_fill<<<rb, T, 0, st>>>(n, ptr<int>(c->master), ptr<int>(c->slave), ptr<int>(c->obst), ptr<int>(c->bptr),
+                                ptr<int>(c->cursor), ptr<int>(c->brow));
+  k_body_sort<<<blocks_for(nb, T), T, 0, st>>>(nb, ptr<int>(c->bptr), ptr<int>(c->brow));
+  B2_TRY(ensure(c->deg, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->adjptr, sizeof(int) * (n + 1)));
+  k_row_degree<<<rb, T, 0, st>>>(n, ptr<int>(c->master), ptr<int>(c->slave), ptr<int>(c->obst), ptr<int>(c->bptr),
+                                 ptr<int>(c->deg));
+  k_set_last_zero<<<1, 32, 0, st>>>(ptr<int>(c->deg), n);
+  B2_TRY(scan_exclusive(c, ptr<int>(c->deg), ptr<int>(c->adjptr), n + 1));
+  int K = 0, bad = 0;
+  B2_CK(cudaMemcpyAsync(&K, ptr<int>(c->adjptr) + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+  B2_CK(cudaMemcpyAsync(&bad, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  B2_CK(cudaMemcpyAsync(&c->free_energy, c->fe_dev.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+  B2_CK(cudaStreamSynchronize(st));
+  if (bad) { set_err("assemble: self-contact or invalid body index (outside the rigid contact path)"); return B2DEV_EUNSUPPORTED; }
+  if (K < 0) { set_err("assemble: block count overflows 32-bit indexing"); return B2DEV_EINVAL; }
+  c->K = K;
+  B2_TRY(ensure(c->adjcol, sizeof(int) * ((size_t)K + 1)));
+  B2_TRY(ensure(c->adjbod, sizeof(int) * ((size_t)K + 1)));
+  k_adj_fill<<<rb, T, 0, st>>>(n, ptr<int>(c->master), ptr<int>(c->slave), ptr<int>(c->obst), ptr<int>(c->bptr),
+                               ptr<int>(c->brow), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<int>(c->adjbod));
+  B2_TRY(prepare_layout(c, colour_seed, true));
+  B2_CK(cudaEventRecord(c->ev[1], st));
+  B2_CK(cudaEventSynchronize(c->ev[1]));
+  cudaEventElapsedTime(&c->assemble_ms, c->ev[0], c->ev[1]);
+  return B2DEV_OK;
+}
+
+int b2dev_upload_locdyn(b2dev_ctx* c, int n, const double* W, const double* A, const double* rho, const double* B,
+                        const double* V, const double* gap, const double* friction, const double* restitution,
+                        const double* cohesion, const int* adjptr, const int* adjcol, const double* Woff,
+                        double free_energy, double step, int dynamic, uint64_t colour_seed, int on_device) {
+  if (!c || n < 0 || !adjptr) { set_err("invalid local dynamics"); return B2DEV_EINVAL; }
+  DeviceGuard g(c->device);
+  int K = 0;
+  if (on_device) {
+    if (n > 0) B2_CK(cudaMemcpy(&K, adjptr + n, sizeof(int), cudaMemcpyDeviceToHost));
+    if (K < 0) { set_err("adjptr[n] negative"); return B2DEV_EINVAL; }
+  } else {
+    K = adjptr[n];
+    if (adjptr[0] != 0) { set_err("adjptr[0] must be 0"); return B2DEV_EINVAL; }
+    for (int i = 0; i < n; i++)
+      if (adjptr[i + 1] < adjptr[i]) { set_err("adjptr not monotone at row %d", i); return B2DEV_EINVAL; }
+    for (int k = 0; k < K; k++)
+      if (adjcol[k] < 0 || adjcol[k] >= n) { set_err("adjcol[%d] = %d out of range", k, adjcol[k]); return B2DEV_EINVAL; }
+  }
+  c->n = n;
+  c->K = K;
+  c->step = step;
+  c->dynamic = dynamic ? 1 : 0;
+  c->free_energy = free_energy;
+  c->assembled_mode = false;
+  B2_TRY(upload(c, c->Wii, W, (size_t)9 * n, on_device));
+  B2_TRY(upload(c, c->Aii, A, (size_t)9 * n, on_device));
+  B2_TRY(upload(c, c->rho_c, rho, (size_t)n, on_device));
+  B2_TRY(upload(c, c->B_c, B, (size_t)3 * n, on_device));
+  B2_TRY(upload(c, c->V_c, V, (size_t)3 * n, on_device));
+  B2_TRY(upload(c, c->gap_c, gap, (size_t)n, on_device));
+  B2_TRY(upload(c, c->fric_c, friction, (size_t)n, on_device));
+  B2_TRY(upload(c, c->rest_c, restitution, (size_t)n, on_device));
+  B2_TRY(upload(c, c->coh_c, cohesion, (size_t)n, on_device));
+  B2_TRY(upload(c, c->adjptr, adjptr, (size_t)n + 1, on_device));
+  B2_TRY(upload(c, c->adjcol, adjcol, (size_t)K, on_device));
+  B2_TRY(upload(c, c->Woff_c, Woff, (size_t)9 * K, on_device));
+  if (on_device && n > 0) {  // device-resident graph: check it before the colouring walks it
+    B2_CK(cudaMemsetAsync(c->bad.p, 0, sizeof(int), c->stream));
+    k_check_graph<<<blocks_for(n, 256), 256, 0, c->stream>>>(n, K, ptr<int>(c->adjptr), ptr<int>(c->adjcol),
+                                                             ptr<int>(c->bad));
+    int bad = 0;
+    B2_CK(cudaMemcpyAsync(&bad, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    B2_CK(cudaStreamSynchronize(c->stream));
+    if (bad) { set_err("adjptr/adjcol out of range"); return B2DEV_EINVAL; }
+  }
+  return prepare_layout(c, colour_seed, false);
+}
+
+int b2dev_set_state(b2dev_ctx* c, const double* R, const double* U, int on_device) {
+  if (!c || !c->ready) { set_err("set_state: no local dynamics"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  const int n = c->n;
+  cudaStream_t st = c->stream;
+  B2_TRY(ensure(c->io, sizeof(double) * 6 * (n + 1)));
+  double* dR = ptr<double>(c->io);
+  double* dU = dR + 3 * (size_t)(n + 1);
+  if (n > 0) {
+    const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (R) B2_CK(cudaMemcpyAsync(dR, R, sizeof(double) * 3 * n, kd, st));
+    else B2_CK(cudaMemsetAsync(dR, 0, sizeof(double) * 3 * n, st));
+    if (U) B2_CK(cudaMemcpyAsync(dU, U, sizeof(double) * 3 * n, kd, st));
+    else B2_CK(cudaMemsetAsync(dU, 0, sizeof(double) * 3 * n, st));
+    k_state_in<<<blocks_for(n, 256), 256, 0, st>>>(n, ptr<int>(c->perm), dR, dU, ptr<double4>(c->R64[0]),
+                                                   ptr<float4>(c->R32[0]), ptr<double4>(c->Us));
+  }
+  c->state_parity = 0;
+  c->state_u_merit = false;
+  B2_CK(cudaGetLastError());
+  return B2DEV_OK;
+}
+
+int b2dev_get_state(b2dev_ctx* c, double* R, double* U, double* conmerit, int on_device) {
+  if (!c || !c->ready) { set_err("get_state: no local dynamics"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  const int n = c->n;
+  cudaStream_t st = c->stream;
+  if (n == 0) return B2DEV_OK;
+  B2_TRY(ensure(c->io, sizeof(double) * 7 * (n + 1)));
+  double* dR = ptr<double>(c->io);
+  double* dU = dR + 3 * (size_t)(n + 1);
+  double* dC = dU + 3 * (size_t)(n + 1);
+  double lo = c->free_energy < DBL_EPSILON ? 1.0 : c->free_energy;
+  lo = lo == 0.0 ? 1.0 : lo;
+  k_state_out<<<blocks_for(n, 256), 256, 0, st>>>(n, ptr<int>(c->perm), ptr<double4>(c->R64[c->state_parity]),
+                                                  c->state_u_merit ? ptr<double4>(c->Um) : ptr<double4>(c->Us),
+                                                  c->have_conmerit ? ptr<double>(c->conmerit) : nullptr, lo, dR, dU,
+                                                  c->have_conmerit ? dC : nullptr);
+  const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (R) B2_CK(cudaMemcpyAsync(R, dR, sizeof(double) * 3 * n, kd, st));
+  if (U) B2_CK(cudaMemcpyAsync(U, dU, sizeof(double) * 3 * n, kd, st));
+  if (conmerit) {
+    if (c->have_conmerit) B2_CK(cudaMemcpyAsync(conmerit, dC, sizeof(double) * n, kd, st));
+    else if (on_device) B2_CK(cudaMemsetAsync(conmerit, 0, sizeof(double) * n, st));
+    else memset(conmerit, 0, sizeof(double) * n);
+  }
+  B2_CK(cudaStreamSynchronize(st));
+  return B2DEV_OK;
+}
+
+int b2dev_solve(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_solve_report* rep, double* rerhist, double* merhist) {
+  if (!c || !o || !rep) { set_err("solve: null argument"); return B2DEV_EINVAL; }
+  if (!c->ready) { set_err("solve: no local dynamics (assemble or upload first)"); return B2DEV_ESTATE; }
+  if (o->maxiter <= 0 || o->diagmaxiter <= 0 || o->diagsolver < 0 || o->diagsolver > 3 || o->failure < 0 ||
+      o->failure > 2 || (o->precision != B2DEV_FP64 && o->precision != B2DEV_MIXED)) {
+    set_err("solve: invalid options");
+    return B2DEV_EINVAL;
+  }
+  if (o->precision == B2DEV_MIXED && o->maxiter < 2) { set_err("solve: mixed precision needs maxiter >= 2"); return B2DEV_EINVAL; }
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  memset(rep, 0, sizeof *rep);
+  const int maxiter = o->maxiter;
+  B2_TRY(ensure(c->rer, sizeof(double) * (maxiter + 2)));
+  B2_TRY(ensure(c->mer, sizeof(double) * (maxiter + 2)));
+  B2_TRY(ensure(c->failkey, sizeof(unsigned long long) * (maxiter + 2)));
+  B2_TRY(ensure(c->failcount, sizeof(unsigned) * (maxiter + 2)));
+  B2_CK(cudaEventRecord(c->ev[2], st));
+
+  SolveControl s1, s2;
+  memset(&s1, 0, sizeof s1);
+  memset(&s2, 0, sizeof s2);
+  int parity = c->state_parity;
+  int iters = 0, final_global = 0;
+  bool thrown = false;
+  double merit = 0.0, error = 0.0;
+  std::vector<std::pair<int, int>> ranges;  // [first, last] global sweep indices of returned iterates
+  if (o->precision == B2DEV_MIXED) {
+    k_shadow<<<blocks_for(c->n, 256), 256, 0, st>>>(c->n, ptr<double4>(c->R64[parity]), ptr<float4>(c->R32[parity]));
+    B2_TRY(solve_launch(c, true, o, maxiter - 1, 0, parity, 0, o->grid, &s1));
+    rep->merit_input = s1.merit_input;
+    iters = s1.iters;
+    thrown = s1.thrown != 0;
+    ranges.push_back({0, s1.final_iter});
+    parity = (parity + 1 + s1.final_iter) & 1;
+    merit = s1.merit;
+    error = s1.error;
+    rep->iters_mixed = iters;
+    rep->sweeps = s1.sweeps;
+    if (!thrown) {  // closing FP64 refinement, continuing the iteration count
+      B2_TRY(solve_launch(c, false, o, maxiter - iters, iters, parity, o->nomerit ? 0 : 1, o->grid, &s2));
+      ranges.push_back({iters, iters + s2.final_iter});
+      parity = (parity + 1 + s2.final_iter) & 1;
+      iters += s2.iters;
+      thrown = s2.thrown != 0;
+      merit = s2.merit;
+      error = s2.error;
+      rep->sweeps += s2.sweeps;
+    }
+  } else {
+    B2_TRY(solve_launch(c, false, o, maxiter, 0, parity, 0, o->grid, &s1));
+    rep->merit_input = s1.merit_input;
+    iters = s1.iters;
+    thrown = s1.thrown != 0;
+    ranges.push_back({0, s1.final_iter});
+    parity = (parity + 1 + s1.final_iter) & 1;
+    merit = s1.merit;
+    error = s1.error;
+    rep->sweeps = s1.sweeps;
+  }
+  B2_CK(cudaEventRecord(c->ev[3], st));
+  final_global = iters;
+
+  // failure bookkeeping over the sweeps that produced the returned iterates
+  std::vector<unsigned long long> fk(maxiter + 2, 0ull);
+  std::vector<unsigned> fc(maxiter + 2, 0u);
+  B2_CK(cudaMemcpyAsync(fk.data(), c->failkey.p, sizeof(unsigned long long) * (maxiter + 1), cudaMemcpyDeviceToHost, st));
+  B2_CK(cudaMemcpyAsync(fc.data(), c->failcount.p, sizeof(unsigned) * (maxiter + 1), cudaMemcpyDeviceToHost, st));
+  if (rerhist && iters > 0) B2_CK(cudaMemcpyAsync(rerhist, c->rer.p, sizeof(double) * iters, cudaMemcpyDeviceToHost, st));
+  if (merhist && iters > 0) B2_CK(cudaMemcpyAsync(merhist, c->mer.p, sizeof(double) * iters, cudaMemcpyDeviceToHost, st));
+  B2_CK(cudaStreamSynchronize(st));
+  int last_kind = 0, nfail = 0;
+  for (auto& r : ranges)
+    for (int s = r.first; s <= r.second && s <= maxiter; s++) {
+      if (fk[s]) last_kind = (int)(fk[s] & 3ull);
+      nfail += (int)fc[s];
+    }
+  cudaEventElapsedTime(&rep->ms_device, c->ev[2], c->ev[3]);
+  rep->iters = final_global;
+  rep->thrown = thrown ? 1 : 0;
+  rep->last_fail_kind = last_kind;
+  rep->nfailures = nfail;
+  rep->merit = o->nomerit ? 0.0 : merit;
+  rep->error = error;
+  c->state_parity = parity;
+  c->state_u_merit = !o->nomerit;
+  c->have_conmerit = !o->nomerit;
+  return B2DEV_OK;
+}
+
+int b2dev_sizes(b2dev_ctx* c, int* n, long long* nblocks, int* ncolours, double* free_energy) {
+  if (!c) return B2DEV_EINVAL;
+  if (n) *n = c->n;
+  if (nblocks) *nblocks = c->K;
+  if (ncolours) *ncolours = c->ncolours;
+  if (free_energy) *free_energy = c->free_energy;
+  return B2DEV_OK;
+}
+
+int b2dev_get_order(b2dev_ctx* c, int* order) {
+  if (!c || !c->ready) { set_err("get_order: no local dynamics"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  if (c->n) B2_CK(cudaMemcpy(order, c->perm.p, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
+  return B2DEV_OK;
+}
+
+int b2dev_get_colours(b2dev_ctx* c, int* colour) {
+  if (!c || !c->ready) { set_err("get_colours: no local dynamics"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  if (c->n) B2_CK(cudaMemcpy(colour, c->colour.p, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
+  return B2DEV_OK;
+}
+
+int b2dev_get_locdyn(b2dev_ctx* c, double* W, double* A, double* rho, double* B, double* V, int* adjptr, int* adjcol,
+                     double* Woff, double* free_energy) {
+  if (!c || !c->ready) { set_err("get_locdyn: no local dynamics"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  const int n = c->n;
+  const long long K = c->K;
+  if (W) B2_CK(cudaMemcpy(W, c->Wii.p, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost));
+  if (A) B2_CK(cudaMemcpy(A, c->Aii.p, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost));
+  if (rho) B2_CK(cudaMemcpy(rho, c->rho_c.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (B) B2_CK(cudaMemcpy(B, c->B_c.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+  if (V) B2_CK(cudaMemcpy(V, c->V_c.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+  if (adjptr) B2_CK(cudaMemcpy(adjptr, c->adjptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+  if (adjcol && K) B2_CK(cudaMemcpy(adjcol, c->adjcol.p, sizeof(int) * K, cudaMemcpyDeviceToHost));
+  if (Woff && K) {
+    B2_TRY(ensure(c->io, sizeof(double) * 9 * (K + 1)));
+    k_offdiag_out<<<blocks_for(n, 256), 256, 0, c->stream>>>(n, ptr<int>(c->iperm), ptr<int>(c->adjptr),
+                                                             ptr<int>(c->rowptr), ptr<double>(c->W64), c->kstride,
+                                                             ptr<double>(c->io));
+    B2_CK(cudaMemcpyAsync(Woff, c->io.p, sizeof(double) * 9 * K, cudaMemcpyDeviceToHost, c->stream));
+    B2_CK(cudaStreamSynchronize(c->stream));
+  }
+  if (free_energy) *free_energy = c->free_energy;
+  return B2DEV_OK;
+}
+
+float b2dev_last_assemble_ms(b2dev_ctx* c) { return c ? c->assemble_ms : 0.f; }
+
+int b2dev_trace_sweep(b2dev_ctx* c, int sweep) {
+  if (!c) return B2DEV_EINVAL;
+  c->trace_sweep = sweep;
+  return B2DEV_OK;
+}
+
+int b2dev_get_trace(b2dev_ctx* c, double* out) {
+  if (!c || !c->ready || !c->trace.p) { set_err("get_trace: no trace recorded"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  const int n = c->n;
+  std::vector<double> tmp((size_t)kTraceStride * n);
+  std::vector<int> perm(n);
+  if (n) {
+    B2_CK(cudaMemcpy(tmp.data(), c->trace.p, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost));
+    B2_CK(cudaMemcpy(perm.data(), c->perm.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  }
+  for (int p = 0; p < n; p++)
+    memcpy(out + (size_t)kTraceStride * perm[p], tmp.data() + (size_t)kTraceStride * p, sizeof(double) * kTraceStride);
+  return B2DEV_OK;
+}
+
+int b2dev_diag_solve_batch(b2dev_ctx* c, int n, int solver, int failure, double diagepsilon, int diagmaxiter,
+                           int dynamic, double step, const double* W, const double* B, const double* V,
+                           const double* rho, const double* gap, const double* friction, const double* restitution,
+                           const double* cohesion, double* U, double* R, int* kind) {
+  if (!c || n < 0 || solver < 0 || solver > 3 || failure < 0 || failure > 2 || diagmaxiter <= 0) {
+    set_err("diag_solve_batch: invalid arguments");
+    return B2DEV_EINVAL;
+  }
+  if (n == 0) return B2DEV_OK;
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  const size_t per = 9 + 3 + 3 + 1 + 1 + 1 + 1 + 1 + 3 + 3;  // doubles per row
+  B2_TRY(ensure(c->io, sizeof(double) * per * n + sizeof(int) * (n + 1)));
+  double* d = ptr<double>(c->io);
+  double *dW = d, *dB = dW + 9 * (size_t)n, *dV = dB + 3 * (size_t)n, *drho = dV + 3 * (size_t)n, *dgap = drho + n;
+  double *dfr = dgap + n, *dre = dfr + n, *dco = dre + n, *dU = dco + n, *dR = dU + 3 * (size_t)n;
+  int* dk = reinterpret_cast<int*>(dR + 3 * (size_t)n);
+  const cudaMemcpyKind h2d = cudaMemcpyHostToDevice, d2h = cudaMemcpyDeviceToHost;
+  B2_CK(cudaMemcpyAsync(dW, W, sizeof(double) * 9 * n, h2d, st));
+  B2_CK(cudaMemcpyAsync(dB, B, sizeof(double) * 3 * n, h2d, st));
+  B2_CK(cudaMemcpyAsync(dV, V, sizeof(double) * 3 * n, h2d, st));
+  B2_CK(cudaMemcpyAsync(drho, rho, sizeof(double) * n, h2d, st));
+  B2_CK(cudaMemcpyAsync(dgap, gap, sizeof(double) * n, h2d, st));
+  B2_CK(cudaMemcpyAsync(dfr, friction, sizeof(double) * n, h2d, st));
+  B2_CK(cudaMemcpyAsync(dre, restitution, sizeof(double) * n, h2d, st));
+  B2_CK(cudaMemcpyAsync(dco, cohesion, sizeof(double) * n, h2d, st));
+  B2_CK(cudaMemcpyAsync(dU, U, sizeof(double) * 3 * n, h2d, st));
+  B2_CK(cudaMemcpyAsync(dR, R, sizeof(double) * 3 * n, h2d, st));
+  k_diag_batch<<<blocks_for(n, 128), 128, 0, st>>>(n, solver, failure, diagepsilon, diagmaxiter, dynamic, step, dW,
+                                                   dB, dV, drho, dgap, dfr, dre, dco, dU, dR, dk);
+  B2_CK(cudaGetLastError());
+  B2_CK(cudaMemcpyAsync(U, dU, sizeof(double) * 3 * n, d2h, st));
+  B2_CK(cudaMemcpyAsync(R, dR, sizeof(double) * 3 * n, d2h, st));
+  if (kind) B2_CK(cudaMemcpyAsync(kind, dk, sizeof(int) * n, d2h, st));
+  B2_CK(cudaStreamSynchronize(st));
+  return B2DEV_OK;
+}
+
+}  // extern "C"

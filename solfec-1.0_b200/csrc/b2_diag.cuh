@@ -1,0 +1,451 @@
+// b2_diag.cuh -- per-contact Signorini-Coulomb diagonal solvers in FP64.
+//
+// Device forms of the reference's CONTACT + SIGNORINI_COULOMB diagonal block
+// solvers (dbs.c:35-326) and of the smoothed contact formulation they use
+// (scf.c:28-174). One thread solves one contact; every function works on
+// register arrays. The 3x3 linear solve is LU with partial pivoting in the
+// LAPACK dgetf2/dgetrs arithmetic (pivot = first largest |a(i,j)|, column
+// scaled by the pivot reciprocal, unit-lower forward and upper back solves).
+#pragma once
+
+#include <cmath>
+#include "b2_common.cuh"
+
+namespace b2 {
+
+// Parameters of one contact row, gathered once per solve.
+struct ContactParams {
+  double friction, restitution, cohesion, gap, step;
+  int dynamic;
+};
+
+// Solve A x = b (3x3, column-major, one right-hand side). Returns 0, or k > 0
+// when U(k,k) is exactly zero (b untouched), as LAPACK dgesv reports.
+__device__ __forceinline__ int lu3_solve(double* a, double* b) {
+  int ipiv[3];
+  int info = 0;
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    int p = j;
+    double amax = fabs(a[j + 3 * j]);
+#pragma unroll
+    for (int i = j + 1; i < 3; i++) {
+      double v = fabs(a[i + 3 * j]);
+      if (v > amax) { amax = v; p = i; }
+    }
+    ipiv[j] = p;
+    if (a[p + 3 * j] != 0.0) {
+      if (p != j) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          // p is a runtime index; select-based swap keeps the array in registers
+          double tj = a[j + 3 * c];
+          double tp = (p == 1) ? a[1 + 3 * c] : a[2 + 3 * c];
+          a[j + 3 * c] = tp;
+          if (p == 1) a[1 + 3 * c] = tj; else a[2 + 3 * c] = tj;
+        }
+      }
+      double piv = a[j + 3 * j];
+      if (fabs(piv) >= 2.2250738585072014e-308) {
+        double r = 1.0 / piv;
+#pragma unroll
+        for (int i = j + 1; i < 3; i++) a[i + 3 * j] *= r;
+      } else {
+#pragma unroll
+        for (int i = j + 1; i < 3; i++) a[i + 3 * j] /= piv;
+      }
+    } else if (info == 0) {
+      info = j + 1;
+    }
+#pragma unroll
+    for (int c = j + 1; c < 3; c++) {
+      double u = a[j + 3 * c];
+      if (u != 0.0) {
+        double t = -u;
+#pragma unroll
+        for (int i = j + 1; i < 3; i++) a[i + 3 * c] += a[i + 3 * j] * t;
+      }
+    }
+  }
+  if (info) return info;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    int p = ipiv[i];
+    if (p != i) {
+      double t = b[i];
+      double bp = (p == 1) ? b[1] : b[2];
+      b[i] = bp;
+      if (p == 1) b[1] = t; else b[2] = t;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    if (b[k] != 0.0) {
+#pragma unroll
+      for (int i = k + 1; i < 3; i++) b[i] -= b[k] * a[i + 3 * k];
+    }
+  }
+#pragma unroll
+  for (int k = 2; k >= 0; k--) {
+    if (b[k] != 0.0) {
+      b[k] /= a[k + 3 * k];
+#pragma unroll
+      for (int i = 0; i < k; i++) b[i] -= b[k] * a[i + 3 * k];
+    }
+  }
+  return 0;
+}
+
+// dashed normal velocity (dbs.c:52-53; scf.c:43-44)
+__device__ __forceinline__ double dashed_un(const ContactParams& cp, const double* U, const double* V) {
+  if (cp.dynamic) return U[2] + cp.restitution * B2_MIN(V[2], 0);
+  return (B2_MAX(cp.gap, 0) / cp.step) + U[2];
+}
+
+// SCF_Project (scf.c:136-174); S is read-only here (the reference adds and
+// removes the cohesion in place, which leaves it unchanged up to rounding of
+// (S2 + c) - c; that rounding is reproduced).
+__device__ __forceinline__ void scf_project(double fri, double coh, double* S, double* R) {
+  S[2] += coh;
+  double fri2 = fri * fri;
+  double slen = sqrt(S[0] * S[0] + S[1] * S[1]);
+  double l1 = -(S[2] + fri * slen) / (1.0 + fri2);
+  double l2 = (slen - fri * S[2]) / (1.0 + fri2);
+  double u1[3], u2[3];
+  if (slen != 0.0) {
+    u2[0] = S[0] / slen; u2[1] = S[1] / slen; u2[2] = -fri;
+    u1[0] = -fri * u2[0]; u1[1] = -fri * u2[1]; u1[2] = -1.0;
+  } else {
+    u2[0] = 1.0; u2[1] = 0.0; u2[2] = -fri;
+    u1[0] = -fri; u1[1] = 0.0; u1[2] = -1.0;
+  }
+  double g1 = B2_MAX(l1, 0.0), g2 = B2_MAX(l2, 0.0);
+  double m0 = g1 * u1[0] + g2 * u2[0];
+  double m1 = g1 * u1[1] + g2 * u2[1];
+  double m2 = g1 * u1[2] + g2 * u2[2];
+  S[2] -= coh;
+  R[0] = S[0] - m0; R[1] = S[1] - m1; R[2] = S[2] - m2;
+}
+
+// SCF_Linearize (scf.c:28-133) with UT = -1 and zero smoothing, the values
+// every caller on the path passes. X, Y (Jacobians) only when WITHXY.
+template <bool WITHXY>
+__device__ __forceinline__ void scf_linearize(const ContactParams& cp, const double* V, const double* U,
+                                              const double* R, double* C, double* X, double* Y) {
+  const double fri = cp.friction;
+  double fri2 = fri * fri, onefri2 = 1.0 + fri2;
+  double udash = dashed_un(cp, U, V);
+  double ulen = sqrt(U[0] * U[0] + U[1] * U[1]);
+  double F0 = U[0], F1 = U[1], F2 = udash + fri * ulen;
+  double S[3] = {R[0] - F0, R[1] - F1, R[2] - F2};
+  S[2] += cp.cohesion;
+  double sdot = S[0] * S[0] + S[1] * S[1];
+  double slen = sqrt(sdot);
+  double l1 = -(S[2] + fri * slen) / onefri2;
+  double l2 = (slen - fri * S[2]) / onefri2;
+  double u1[3], u2[3];
+  if (slen != 0.0) {
+    u2[0] = S[0] / slen; u2[1] = S[1] / slen; u2[2] = -fri;
+    u1[0] = -fri * u2[0]; u1[1] = -fri * u2[1]; u1[2] = -1.0;
+  } else {
+    u2[0] = 1.0; u2[1] = 0.0; u2[2] = -fri;
+    u1[0] = -fri; u1[1] = 0.0; u1[2] = -1.0;
+  }
+  double sq1 = sqrt(l1 * l1), sq2 = sqrt(l2 * l2);
+  double g1 = 0.5 * (sq1 + l1), g2 = 0.5 * (sq2 + l2);
+  C[0] = F0 + (g1 * u1[0] + g2 * u2[0]);
+  C[1] = F1 + (g1 * u1[1] + g2 * u2[1]);
+  C[2] = F2 + (g1 * u1[2] + g2 * u2[2]);
+  if constexpr (WITHXY) {
+    double dF[9] = {1.0, 0.0, fri * U[0] / ulen, 0.0, 1.0, fri * U[1] / ulen, 0.0, 0.0, 1.0};
+    double dg1 = 0.5 * (1.0 + l1 / sq1);
+    if (slen != 0.0) {
+      double dg2 = 0.5 * (1.0 + l2 / sq2);
+      double a = 0.5 * (1.0 + (l2 + fri * l1) / (sq2 + fri * sq1));
+      double b = (fri2 * dg1 + dg2) / onefri2;
+      double c = (fri * (dg1 - dg2)) / onefri2;
+      double d = (dg1 + fri2 * dg2) / onefri2;
+      Y[0] = a + (b - a) * S[0] * S[0] / sdot;
+      Y[1] = (b - a) * S[1] * S[0] / sdot;
+      Y[2] = c * S[0] / slen;
+      Y[3] = Y[1];
+      Y[4] = a + (b - a) * S[1] * S[1] / sdot;
+      Y[5] = c * S[1] / slen;
+      Y[6] = Y[2];
+      Y[7] = Y[5];
+      Y[8] = d;
+    } else {
+      Y[1] = Y[2] = Y[3] = Y[5] = Y[6] = Y[7] = 0.0;
+      Y[0] = Y[4] = Y[8] = dg1;
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+        X[3 * j + i] = dF[3 * j + i] - (Y[i] * dF[3 * j] + Y[3 + i] * dF[3 * j + 1] + Y[6 + i] * dF[3 * j + 2]);
+  }
+}
+
+// projected_gradient (dbs.c:35-94)
+__device__ __noinline__ int projected_gradient(const ContactParams& cp, double epsilon, int maxiter, double rho,
+                                               const double* W, const double* B, const double* V, double* U,
+                                               double* R) {
+  if (cp.dynamic && cp.gap > 0) {
+    R[0] = R[1] = R[2] = 0.0;
+    U[0] = B[0]; U[1] = B[1]; U[2] = B[2];
+    return 0;
+  }
+  int iter = 0;
+  double scalar;
+  do {
+    double v0 = R[0], v1 = R[1], v2 = R[2];
+    nvaddmul(B, W, R, U);
+    double UN = dashed_un(cp, U, V);
+    R[0] -= rho * U[0];
+    R[1] -= rho * U[1];
+    R[2] -= rho * UN - cp.cohesion;
+    R[2] = B2_MAX(0, R[2]);
+    scalar = sqrt(R[0] * R[0] + R[1] * R[1]);
+    if (scalar >= cp.friction * R[2]) {
+      if (scalar > 0.0) scalar = cp.friction * R[2] / scalar;
+      R[0] *= scalar;
+      R[1] *= scalar;
+    }
+    R[2] -= cp.cohesion;
+    double d[3] = {R[0] - v0, R[1] - v1, R[2] - v2};
+    scalar = dot3(R, R);
+    scalar = sqrt(dot3(d, d) / B2_MAX(scalar, 1.0));
+  } while (++iter < maxiter && scalar > epsilon);
+  return iter;
+}
+
+// de_saxce_feng (dbs.c:96-140)
+__device__ __noinline__ int de_saxce_feng(const ContactParams& cp, double epsilon, int maxiter, double rho,
+                                          const double* W, const double* B, const double* V, double* U, double* R) {
+  if (cp.dynamic && cp.gap > 0) {
+    R[0] = R[1] = R[2] = 0.0;
+    U[0] = B[0]; U[1] = B[1]; U[2] = B[2];
+    return 0;
+  }
+  int iter = 0;
+  double scalar;
+  do {
+    double v0 = R[0], v1 = R[1], v2 = R[2];
+    nvaddmul(B, W, R, U);
+    double UN = dashed_un(cp, U, V);
+    double tau[3];
+    tau[0] = R[0] - rho * U[0];
+    tau[1] = R[1] - rho * U[1];
+    tau[2] = R[2] - rho * (UN + cp.friction * sqrt(U[0] * U[0] + U[1] * U[1]));
+    scf_project(cp.friction, cp.cohesion, tau, R);
+    double d[3] = {R[0] - v0, R[1] - v1, R[2] - v2};
+    scalar = dot3(R, R);
+    scalar = sqrt(dot3(d, d) / B2_MAX(scalar, 1.0));
+  } while (++iter < maxiter && scalar > epsilon);
+  return iter;
+}
+
+// semismooth_newton (dbs.c:142-303): the default diagonal solver.
+__device__ __forceinline__ int semismooth_newton(const ContactParams& cp, double epsilon, int maxiter, double rho,
+                                                 const double* W, const double* B, const double* V, double* U,
+                                                 double* R) {
+  if (cp.dynamic && cp.gap > 0) {
+    R[0] = R[1] = R[2] = 0.0;
+    U[0] = B[0]; U[1] = B[1]; U[2] = B[2];
+    return 0;
+  }
+  const double friction = cp.friction, cohesion = cp.cohesion;
+  int divi = maxiter / 10;
+  int iter = 0;
+  double error;
+  do {
+    double R00 = R[0], R01 = R[1], R02 = R[2];
+    double UN = dashed_un(cp, U, V);
+    double d0 = R[0] - rho * U[0];
+    double d1 = R[1] - rho * U[1];
+    double d2 = (R[2] + cohesion) - rho * UN;
+    double RES[3];
+    nvaddmul(B, W, R, RES);
+    RES[0] -= U[0]; RES[1] -= U[1]; RES[2] -= U[2];
+    double a[9], b[3];
+    if (d2 >= 0) {
+      double norm = sqrt(d0 * d0 + d1 * d1);
+      double lim = friction * B2_MAX(0, d2);
+      if (norm >= lim) {  // slip
+        if (lim > 0.0) {
+          double len = sqrt(R[0] * R[0] + R[1] * R[1]);
+          double den = B2_MAX(lim, len) * norm;
+          double e = lim / norm;
+          double beta;
+          if (len == 0.0) beta = 1.0;
+          else {
+            double alfa = (R[0] * d0 + R[1] * d1) / (len * norm);
+            double delta = B2_MIN(len / lim, 1.0);
+            beta = (alfa < 0.0 ? 1.0 / (1.0 - alfa * delta) : 1.0);
+          }
+          double F0 = (R[0] * d0) / den, F1 = (R[1] * d0) / den, F2 = (R[0] * d1) / den, F3 = (R[1] * d1) / den;
+          double M0 = e * (1.0 - F0), M1 = -e * F1, M2 = -e * F2, M3 = e * (1.0 - F3);
+          double H0 = 1.0 - beta * M0, H1 = -beta * M1, H2 = -beta * M2, H3 = 1.0 - beta * M3;
+          a[0] = H0 + rho * (M0 * W[0] + M2 * W[1]);
+          a[1] = H1 + rho * (M1 * W[0] + M3 * W[1]);
+          a[2] = W[2];
+          a[3] = H2 + rho * (M0 * W[3] + M2 * W[4]);
+          a[4] = H3 + rho * (M1 * W[3] + M3 * W[4]);
+          a[5] = W[5];
+          a[6] = rho * (M0 * W[6] + M2 * W[7]) - friction * (d0 / norm);
+          a[7] = rho * (M1 * W[6] + M3 * W[7]) - friction * (d1 / norm);
+          a[8] = W[8];
+          b[0] = friction * (d0 / norm) * (R[2] + cohesion) - R[0] - rho * (M0 * RES[0] + M2 * RES[1]);
+          b[1] = friction * (d1 / norm) * (R[2] + cohesion) - R[1] - rho * (M1 * RES[0] + M3 * RES[1]);
+          b[2] = -UN - RES[2];
+        } else {  // degenerate: homogeneous tangential tractions
+          a[0] = 1.0; a[1] = 0.0; a[2] = W[2];
+          a[3] = 0.0; a[4] = 1.0; a[5] = W[5];
+          a[6] = 0.0; a[7] = 0.0; a[8] = W[8];
+          b[0] = -R[0] - RES[0];
+          b[1] = -R[1] - RES[1];
+          b[2] = -UN - RES[2];
+        }
+      } else {  // stick
+        a[0] = W[0]; a[1] = W[1]; a[2] = W[2];
+        a[3] = W[3]; a[4] = W[4]; a[5] = W[5];
+        a[6] = W[6] + U[0] / d2;
+        a[7] = W[7] + U[1] / d2;
+        a[8] = W[8];
+        b[0] = -(1.0 + rho * U[2] / d2) * U[0] - RES[0];
+        b[1] = -(1.0 + rho * U[2] / d2) * U[1] - RES[1];
+        b[2] = -UN - RES[2];
+      }
+    } else {  // separation
+      a[0] = 1.0; a[1] = 0.0; a[2] = 0.0;
+      a[3] = 0.0; a[4] = 1.0; a[5] = 0.0;
+      a[6] = 0.0; a[7] = 0.0; a[8] = 1.0;
+      b[0] = -R[0]; b[1] = -R[1]; b[2] = -R[2];
+    }
+    if (lu3_solve(a, b)) return -1;
+    if (!isfinite(b[0] + b[1] + b[2])) return -1;
+    double c[3];
+    nvaddmul(RES, W, b, c);
+    R[0] += b[0]; R[1] += b[1]; R[2] += b[2];
+    U[0] += c[0]; U[1] += c[1]; U[2] += c[2];
+    double e0 = R[0] - R00, e1 = R[1] - R01, e2 = R[2] - R02;
+    error = dot3(R, R);
+    error = sqrt((e0 * e0 + e1 * e1 + e2 * e2) / B2_MAX(error, 1.0));
+    iter++;
+    if ((iter % divi) == 0) {
+      rho *= 10.0;
+      if (isinf(rho)) return -1;
+    }
+  } while (iter < maxiter && error > epsilon);
+  return iter;
+}
+
+// projected_newton (dbs.c:305-326)
+__device__ __noinline__ int projected_newton(const ContactParams& cp, double epsilon, int maxiter, const double* W,
+                                             const double* B, const double* V, double* U, double* R) {
+  double T[9], X[9], Y[9], Cv[3];
+  int iter = 0;
+  double merit;
+  nvaddmul(B, W, R, U);
+  scf_linearize<true>(cp, V, U, R, Cv, X, Y);
+  do {
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+        T[3 * j + i] = (X[i] * W[3 * j] + X[3 + i] * W[3 * j + 1] + X[6 + i] * W[3 * j + 2]) + Y[3 * j + i];
+    if (lu3_solve(T, Cv)) return -1;
+    R[0] -= Cv[0]; R[1] -= Cv[1]; R[2] -= Cv[2];
+    scf_project(cp.friction, cp.cohesion, R, R);
+    nvaddmul(B, W, R, U);
+    scf_linearize<true>(cp, V, U, R, Cv, X, Y);
+    merit = sqrt(dot3(Cv, Cv));
+  } while (merit > epsilon && ++iter < maxiter);
+  return iter;
+}
+
+__device__ __forceinline__ int diagonal_solve(int solver, const ContactParams& cp, double epsilon, int maxiter,
+                                              double rho, const double* W, const double* B, const double* V,
+                                              double* U, double* R) {
+  switch (solver) {  // dbs.c:507-521
+    case DS_PROJECTED_GRADIENT: return projected_gradient(cp, epsilon, maxiter, rho, W, B, V, U, R);
+    case DS_DE_SAXCE_FENG: return de_saxce_feng(cp, epsilon, maxiter, rho, W, B, V, U, R);
+    case DS_SEMISMOOTH_NEWTON: return semismooth_newton(cp, epsilon, maxiter, rho, W, B, V, U, R);
+    case DS_PROJECTED_NEWTON: return projected_newton(cp, epsilon, maxiter, W, B, V, U, R);
+  }
+  return 0;
+}
+
+// State of one row handed to the out-of-line solvers (rare path only, so the
+// arrays of the common path stay in registers).
+struct RowState {
+  double W[9], B[3], V[3], U[3], R[3];
+};
+
+__device__ __noinline__ int diagonal_solve_slow(int solver, const ContactParams& cp, double epsilon, int maxiter,
+                                                double rho, RowState& st) {
+  return diagonal_solve(solver, cp, epsilon, maxiter, rho, st.W, st.B, st.V, st.U, st.R);
+}
+
+// FAILURE_CONTINUE fallback chain (bgs.c:976-1003): the other solvers in the
+// order SSN, PG, DSF, PN, each from the previous reaction R0; if all fail the
+// previous reaction is kept (U keeps the last attempt's value).
+__device__ __noinline__ void fallback_chain(int solver, const ContactParams& cp, double epsilon, int maxiter,
+                                            double rho, RowState& st, const double* R0) {
+  const int chain[4] = {DS_SEMISMOOTH_NEWTON, DS_PROJECTED_GRADIENT, DS_DE_SAXCE_FENG, DS_PROJECTED_NEWTON};
+  int it = maxiter;
+  for (int t = 0; t < 4; t++) {
+    if (chain[t] != solver) {
+      st.R[0] = R0[0]; st.R[1] = R0[1]; st.R[2] = R0[2];
+      it = diagonal_solve(chain[t], cp, epsilon, maxiter, rho, st.W, st.B, st.V, st.U, st.R);
+      if (it < maxiter && it >= 0) break;
+    }
+  }
+  if (it >= maxiter || it < 0) { st.R[0] = R0[0]; st.R[1] = R0[1]; st.R[2] = R0[2]; }
+}
+
+// Diagonal solve of one row with the reference's failure handling
+// (bgs.c:969-1013). Returns the failure kind of the first attempt: 0 none,
+// 1 diverged (iterations >= maxiter), 2 failed (< 0).
+__device__ __forceinline__ int diagonal_solve_row(int solver, int failure, const ContactParams& cp, double epsilon,
+                                                  int maxiter, double rho, const double* W, const double* B,
+                                                  const double* V, double* U, double* R) {
+  const double R0[3] = {R[0], R[1], R[2]};
+  int it;
+  if (solver == DS_SEMISMOOTH_NEWTON) {
+    it = semismooth_newton(cp, epsilon, maxiter, rho, W, B, V, U, R);
+    if (it < maxiter && it >= 0) return 0;
+  }
+  RowState st;
+#pragma unroll
+  for (int q = 0; q < 9; q++) st.W[q] = W[q];
+#pragma unroll
+  for (int q = 0; q < 3; q++) { st.B[q] = B[q]; st.V[q] = V[q]; st.U[q] = U[q]; st.R[q] = R[q]; }
+  if (solver != DS_SEMISMOOTH_NEWTON) {
+    it = diagonal_solve_slow(solver, cp, epsilon, maxiter, rho, st);
+    if (it < maxiter && it >= 0) {
+#pragma unroll
+      for (int q = 0; q < 3; q++) { U[q] = st.U[q]; R[q] = st.R[q]; }
+      return 0;
+    }
+  }
+  const int kind = it < 0 ? 2 : 1;
+  if (failure == FAIL_CONTINUE) fallback_chain(solver, cp, epsilon, maxiter, rho, st, R0);
+#pragma unroll
+  for (int q = 0; q < 3; q++) { U[q] = st.U[q]; R[q] = st.R[q]; }
+  return kind;
+}
+
+// Merit numerator of one CONTACT row (mrf.c:81-87): C = SCF_Linearize(U, R),
+// up = <A C, C>.
+__device__ __forceinline__ double merit_row(const ContactParams& cp, const double* A, const double* V,
+                                            const double* U, const double* R) {
+  double P[3];
+  scf_linearize<false>(cp, V, U, R, P, nullptr, nullptr);
+  double Q0 = A[0] * P[0] + A[3] * P[1] + A[6] * P[2];
+  double Q1 = A[1] * P[0] + A[4] * P[1] + A[7] * P[2];
+  double Q2 = A[2] * P[0] + A[5] * P[1] + A[8] * P[2];
+  return Q0 * P[0] + Q1 * P[1] + Q2 * P[2];
+}
+
+}  // namespace b2
