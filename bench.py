@@ -1,0 +1,375 @@
+"""Benchmark of the B200 contact-solve path (one JSON line on rank 0).
+
+Workload: the 100,000-body perturbed-hexahedra scene (rigid convex hexahedra,
+side 0.04 m, vertices +-10%, density 2000, friction 0.4, h = 5e-4), one
+contact step = LOCDYN_Update_Begin (W_ii, rho, A, B, V, W_ij, colouring,
+colour-sorted layout) + GAUSS_SEIDEL_Solve to merit 1e-4
+(epsilon = meritval = 1e-4, maxiter 1000, SEMISMOOTH_NEWTON), warm-started
+from the reactions of the previous step, as a time-stepping run does.
+
+`value` is the per-step time of the product mode (mixed precision: FP32
+off-diagonal sweeps, FP64 diagonal solves / merit / closing refinement) with
+all inputs resident in HBM; the FP64 mode is reported beside it. `e2e` is the
+same step through the C ABI with host (pinned) buffers: scene upload, assembly,
+warm-start upload, solve and the read-back of R, U and the per-contact merit.
+
+With --gpus N > 1 (torchrun), every rank solves its own replica scene (the
+path has no exchange step for independent scenes): per-step time is the max
+over ranks.
+
+--impl reference times the reference's own serial GAUSS_SEIDEL_Solve
+(compiled from its sources into oracle/_ref) on the same local dynamics
+(assembled by the C restatement of LOCDYN_Update_Begin) on one host core.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, 'solfec-1.0_b200'))
+
+METRIC = 'per-step contact-solve time to merit 1e-4 (GPU plain vs mixed+NN) and sweep HBM GB/s'
+# time to merit 1e-4: the merit test decides (the relative-error test is made
+# non-binding with epsilon = 1; diagepsilon keeps its default 0.01 * 1e-4)
+SOLVE = dict(epsilon=1.0, maxiter=1000, meritval=1e-4)
+SCENE = dict(nx=100, ny=100, nz=10)
+WORKLOAD = 'hexahedra-100k: 100x100x10 perturbed rigid hexahedra (side 0.04 m, +-10% vertices), friction 0.4, h=5e-4'
+
+# algorithmic bytes of one fused sweep+merit pass (per off-diagonal block, per row)
+BYTES_BLOCK = {'fp64': 100, 'mixed': 52}
+BYTES_ROW = {'fp64': 316, 'mixed': 328}
+
+
+def _dist():
+    ws = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    return ws, rank, local
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            p = json.load(f)
+        return float(p['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+         'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, 'gpurun_out', 'clocks_bench.csv') if os.path.isdir(
+            os.path.join(ROOT, 'gpurun_out')) else '/tmp/b2_clocks_%d.csv' % os.getpid()
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, 'w')
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), '--query-gpu=' + self.Q,
+                                          '--format=csv,noheader,nounits', '-lms', '200'], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(',')]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1])); mx = max(mx, float(f[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower() == 'active':
+                        reasons.add(nm)
+        except Exception:
+            pass
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': mx or None,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def make_step_inputs(rank):
+    """Scene of the timed step and the warm start from the previous step.
+    The previous step is solved once (FP64, untimed) and the bodies advanced
+    by one velocity step with its reactions."""
+    from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN, scenes
+    sc0 = scenes.hexahedra_lattice(seed=3 + rank, **SCENE)
+    ldy = LOCDYN()
+    ldy.update_begin(sc0)
+    gs = GAUSS_SEIDEL_SOLVER(**SOLVE)
+    gs.solve(ldy)
+    R0, U0, _ = ldy.get_state()
+    sc1 = scenes.advance_velocities(sc0, R0)
+    ldy.close()
+    return sc1, R0, U0, gs.iters
+
+
+def bench_product(args, ws, rank, local):
+    import torch
+    import ctypes as C
+    from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN
+    from solfec_b200._lib import b2gs_bodies, b2gs_contacts, lib
+
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    sc, R0, U0, iters_prev = make_step_inputs(rank)
+    stream = torch.cuda.current_stream()
+
+    def tens(a, dtype):
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype))
+
+    host = [tens(sc.rot, np.float64), tens(sc.x0, np.float64), tens(sc.jinv, np.float64), tens(sc.minv, np.float64),
+            tens(sc.velo, np.float64), tens(sc.velo0, np.float64), tens(sc.obstacle, np.int32),
+            tens(sc.master, np.int32), tens(sc.slave, np.int32), tens(sc.mpnt, np.float64), tens(sc.spnt, np.float64),
+            tens(sc.base, np.float64), tens(sc.gap, np.float64), tens(sc.friction, np.float64),
+            tens(sc.restitution, np.float64), tens(sc.cohesion, np.float64)]
+    pinned = [t.pin_memory() for t in host]
+    devt = [t.to(dev) for t in host]
+    Rd, Ud = tens(R0, np.float64).to(dev), tens(U0, np.float64).to(dev)
+    Rh, Uh = tens(R0, np.float64).pin_memory(), tens(U0, np.float64).pin_memory()
+    n = sc.ncon
+    Rout_h = torch.empty(3 * n, dtype=torch.float64).pin_memory()
+    Uout_h = torch.empty(3 * n, dtype=torch.float64).pin_memory()
+    Cout_h = torch.empty(n, dtype=torch.float64).pin_memory()
+    h2d_bytes = sum(t.numel() * t.element_size() for t in host) + 2 * Rh.numel() * 8
+    d2h_bytes = (Rout_h.numel() + Uout_h.numel() + Cout_h.numel()) * 8
+
+    def structs(ts, on_device):
+        p = [C.c_void_p(t.data_ptr()) for t in ts]
+        return (b2gs_bodies(sc.nbod, *p[:7], on_device), b2gs_contacts(sc.ncon, *p[7:], on_device))
+
+    bd, cd = structs(devt, 1)
+    bh, ch = structs(pinned, 0)
+    ldy = LOCDYN(device=local, stream=stream.cuda_stream)
+    ctx = ldy.device_context
+
+    def step_device(gs):
+        ldy.update_begin_arrays(bd, cd, sc.step, sc.dynamic)
+        ldy.set_state_ptr(C.c_void_p(Rd.data_ptr()), C.c_void_p(Ud.data_ptr()), 1)
+        gs.solve(ldy)
+
+    def step_e2e(gs):
+        ldy.update_begin_arrays(bh, ch, sc.step, sc.dynamic)
+        ldy.set_state_ptr(C.c_void_p(Rh.data_ptr()), C.c_void_p(Uh.data_ptr()), 0)
+        gs.solve(ldy)
+        ldy.get_state_ptr(C.c_void_p(Rout_h.data_ptr()), C.c_void_p(Uout_h.data_ptr()),
+                          C.c_void_p(Cout_h.data_ptr()), 0)
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, gs, steps, warmup):
+        for _ in range(warmup):
+            fn(gs)
+        barrier()
+        l0 = lib().b2dev_launch_count(ctx)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = []
+        ev0.record(stream)
+        for _ in range(steps):
+            fn(gs)
+            reps.append(gs.report)
+        ev1.record(stream)
+        barrier()
+        ms = ev0.elapsed_time(ev1) / steps
+        launches = lib().b2dev_launch_count(ctx) - l0
+        if ws > 1:
+            t = torch.tensor([ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, reps, launches
+
+    results = {}
+    with ClockSampler(local) as clk:
+        for mode in ('fp64', 'mixed'):
+            gs = GAUSS_SEIDEL_SOLVER(**SOLVE)
+            gs.precision = 'MIXED' if mode == 'mixed' else 'FP64'
+            ms, reps, launches = timed(step_device, gs, args.steps, args.warmup)
+            r = reps[-1]
+            results[mode] = dict(ms=ms, iters=gs.iters, iters_mixed=gs.iters_mixed, merit=ldy.merit, report=r,
+                                 launches=launches, assemble_ms=ldy.assemble_ms, error=gs.error)
+        gs = GAUSS_SEIDEL_SOLVER(**SOLVE)
+        gs.precision = 'MIXED'
+        e2e_ms, _, _ = timed(step_e2e, gs, args.steps, args.warmup)
+    nrows, K, ncol, fe = ldy.sizes()
+    return dict(results=results, e2e_ms=e2e_ms, h2d=h2d_bytes, d2h=d2h_bytes, n=nrows, K=K, ncolours=ncol,
+                clocks=clk.summary(), iters_prev=iters_prev, nbod=sc.nbod)
+
+
+def roofline(mode, r, n, K, peak):
+    rep = r['report']
+    sweeps = rep['sweeps_launch'][0]
+    ms = rep['ms_kernel'][0]
+    bytes_launch = sweeps * (K * BYTES_BLOCK[mode] + n * BYTES_ROW[mode])
+    gbs = bytes_launch / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+    return dict(bound='hbm', achieved=round(gbs, 1), peak=peak, unit='GB/s', frac=round(gbs / peak, 3),
+                traffic=None, kernel='k_solve<%s>' % ('true' if mode == 'mixed' else 'false'),
+                bytes_per_launch=int(bytes_launch), sweeps_per_launch=sweeps, kernel_ms=round(ms, 4))
+
+
+def cpu_reference_step(sc, R0, U0, seed=0x5EEDC0105):
+    """Reference GAUSS_SEIDEL_Solve (oracle/_ref, one core) on the restated
+    assembly of the same step, rows in the GPU's colour order."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import oracle as O
+    t0 = time.perf_counter()
+    ld = O.assemble(sc)
+    t1 = time.perf_counter()
+    nc, col = O.colour(ld, seed)
+    order = O.colour_order(col)
+    lp = ld.permuted(order)
+    R0 = np.asarray(R0).reshape(-1, 3); U0 = np.asarray(U0).reshape(-1, 3)
+    impl = 'ref' if O.ref_available() else 'oracle'
+    t2 = time.perf_counter()
+    res = O.solve(lp, R=R0[order].ravel(), U=U0[order].ravel(), impl=impl, **SOLVE)
+    t3 = time.perf_counter()
+    return dict(ms=1e3 * ((t1 - t0) + (t3 - t2)), assemble_ms=1e3 * (t1 - t0), solve_ms=1e3 * (t3 - t2),
+                iters=res['iters'], merit=res['merit'], impl=impl)
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from solfec_b200 import scenes
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import oracle as O
+    sc0 = scenes.hexahedra_lattice(seed=3, **SCENE)
+    ld0 = O.assemble(sc0)
+    nc, col = O.colour(ld0, 0x5EEDC0105)
+    order = O.colour_order(col)
+    impl = 'ref' if O.ref_available() else 'oracle'
+    r0 = O.solve(ld0.permuted(order), impl=impl, **SOLVE)
+    R0 = np.empty((ld0.n, 3)); U0 = np.empty((ld0.n, 3))
+    R0[order] = r0['R'].reshape(-1, 3); U0[order] = r0['U'].reshape(-1, 3)
+    sc = scenes.advance_velocities(sc0, R0)
+    for _ in range(args.warmup):
+        cpu_reference_step(sc, R0, U0)
+    times = [cpu_reference_step(sc, R0, U0) for _ in range(args.steps)]
+    ms = statistics.mean(t['ms'] for t in times)
+    kind = 'reference' if impl == 'ref' else 'port'
+    sample = ('one full step per timed step: restated assembly (oracle/oracle_ldy.c) + the reference serial '
+              'GAUSS_SEIDEL_Solve (bgs.c, compiled unmodified) to merit 1e-4 on %d contacts, %d iterations'
+              % (ld0.n, times[-1]['iters']))
+    line = {'metric': METRIC, 'value': round(ms, 3), 'unit': 'ms', 'n_gpus': ws, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': round(ms, 3), 'higher_is_better': False, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded scene generator)',
+            'config': {'workload': WORKLOAD, 'contacts': ld0.n, 'blocks': ld0.nblocks, 'mode': 'reference FP64',
+                       'parallelism': 'replicas'},
+            'impl': 'reference',
+            'cpu_baseline': {'value': round(ms, 3), 'unit': 'ms', 'cores': 1, 'kind': kind, 'sample': sample,
+                             'assemble_ms': round(statistics.mean(t['assemble_ms'] for t in times), 3),
+                             'solve_ms': round(statistics.mean(t['solve_ms'] for t in times), 3)},
+            'e2e': {'value': round(ms, 3), 'unit': 'ms', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='product', choices=['product', 'reference'])
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--scene', default=None, help='NXxNYxNZ lattice of a smaller case (profiling)')
+    ap.add_argument('--maxiter', type=int, default=None, help='iteration cap of a smaller case (profiling)')
+    args = ap.parse_args()
+    global WORKLOAD
+    if args.scene:
+        nx, ny, nz = (int(v) for v in args.scene.lower().split('x'))
+        SCENE.update(nx=nx, ny=ny, nz=nz)
+        WORKLOAD = 'hexahedra %dx%dx%d (profiling case)' % (nx, ny, nz)
+    if args.maxiter:
+        SOLVE['maxiter'] = args.maxiter
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local = _dist()
+    if args.impl == 'reference':
+        run_reference(args, ws, rank)
+        return
+    import torch
+    if ws > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    out = bench_product(args, ws, rank, local)
+    peak, peak_kind = _peaks()
+    if rank == 0:
+        res = out['results']
+        mixed, fp64 = res['mixed'], res['fp64']
+        roof = roofline('mixed', mixed, out['n'], out['K'], peak)
+        roof64 = roofline('fp64', fp64, out['n'], out['K'], peak)
+        roof['peak_kind'] = peak_kind
+        cpu = None
+        if not args.no_cpu_baseline:
+            from solfec_b200 import scenes
+            sc, R0, U0, _ = make_step_inputs(0)
+            t = cpu_reference_step(sc, R0, U0)
+            cpu = {'value': round(t['ms'], 3), 'unit': 'ms', 'cores': 1,
+                   'kind': 'reference' if t['impl'] == 'ref' else 'port',
+                   'sample': 'one full step of the bench workload (%d contacts): restated assembly + reference '
+                             'GAUSS_SEIDEL_Solve, %d iterations, merit %.2e' % (out['n'], t['iters'], t['merit']),
+                   'assemble_ms': round(t['assemble_ms'], 3), 'solve_ms': round(t['solve_ms'], 3)}
+        line = {
+            'metric': METRIC, 'value': round(mixed['ms'], 4), 'unit': 'ms', 'n_gpus': ws, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': round(mixed['ms'], 4), 'higher_is_better': False,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64+f32 (mixed)',
+            'data': 'synthetic (seeded scene generator)',
+            'config': {'workload': WORKLOAD, 'contacts': out['n'], 'blocks': out['K'], 'bodies': out['nbod'],
+                       'colours': out['ncolours'], 'mode': 'mixed (FP32 sweeps, FP64 diagonal/merit/refinement)',
+                       'solver': 'GAUSS_SEIDEL_SOLVER(epsilon=%g, maxiter=%d, meritval=%g, SEMISMOOTH_NEWTON), '
+                                 'warm start from the previous step' % (SOLVE['epsilon'], SOLVE['maxiter'],
+                                                                         SOLVE['meritval']),
+                       'l2': 'sweep working set > 126 MB L2 (W planes %.0f MB FP64 / %.0f MB FP32)'
+                             % (out['K'] * 72 / 1e6, out['K'] * 36 / 1e6),
+                       'parallelism': 'replicas' if ws > 1 else 'single GPU'},
+            'modes': {m: {'ms_per_step': round(r['ms'], 4), 'iters': r['iters'], 'iters_fp32': r['iters_mixed'],
+                          'merit': r['merit'], 'error': r['error'], 'assemble_ms': round(r['assemble_ms'], 4),
+                          'solve_kernel_ms': [round(x, 4) for x in r['report']['ms_kernel']],
+                          'sweeps': r['report']['sweeps_launch'], 'grid': r['report']['grid']}
+                      for m, r in res.items()},
+            'speedup_mixed_vs_fp64': round(fp64['ms'] / mixed['ms'], 3),
+            'roofline': roof, 'roofline_fp64': roof64,
+            'cpu_baseline': cpu,
+            'e2e': {'value': round(out['e2e_ms'], 4), 'unit': 'ms', 'h2d_bytes_per_step': out['h2d'],
+                    'd2h_bytes_per_step': out['d2h']},
+            'gpu_launches': int(mixed['launches']),
+            'clocks': out['clocks'],
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -59,6 +59,9 @@ typedef struct b2dev_solve_report {
   double error;             /* relative error of the returned iterate */
   double merit_input;       /* merit of the initial reactions (0 without merit) */
   float ms_device;          /* device time of the solve (CUDA events) */
+  float ms_kernel[2];       /* solver kernel time per launch: [0] FP64 or mixed FP32 phase, [1] FP64 refinement */
+  int sweeps_launch[2];     /* sweeps run by each launch */
+  int grid;                 /* persistent grid size (blocks) of the last launch */
 } b2dev_solve_report;
 
 const char* b2dev_last_error(void);
@@ -112,6 +115,9 @@ int b2dev_get_locdyn(b2dev_ctx* ctx, double* W, double* A, double* rho, double* 
 /* Events-timed device duration of the last b2dev_assemble (assembly +
  * colouring + layout), in milliseconds. */
 float b2dev_last_assemble_ms(b2dev_ctx* ctx);
+
+/* Number of this library's kernels launched on the context so far. */
+long long b2dev_launch_count(b2dev_ctx* ctx);
 
 /* Tracing: record, for every row, the inputs and outputs of its diagonal
  * solve in sweep `sweep` (0-based; -1 switches tracing off) of the next

@@ -119,6 +119,8 @@ void b2gs_set_grid (b2gs_solver *gs, int blocks);      /* persistent grid size (
 int b2gs_get_iters_mixed (b2gs_solver *gs);           /* FP32 iterations of the last mixed solve */
 double b2gs_get_solve_ms (b2gs_solver *gs);           /* device time of the last solve */
 double b2gs_get_merit_input (b2gs_solver *gs);        /* merit of the reactions the last solve started from */
+/* the device report of the last solve (struct b2dev_solve_report of b2_device.h) */
+int b2gs_get_report (b2gs_solver *gs, void *report, int nbytes);
 
 /* ---- local dynamics (LOCDYN) and constraint state ---- */
 

@@ -161,7 +161,9 @@ struct b2dev_ctx {
   std::vector<int> colptr_h;
 
   // state and solve scratch
-  Buf R64[2], R32[2], Us, Um, conmerit, part, rer, mer, failkey, failcount, sctrl, io, cub_tmp, trace;
+  Buf R64[3], R32[3], Us[2], Um[2], conmerit[2], done, decided, tilebase, part, rer, mer, failkey, failcount, sctrl, io,
+      cub_tmp, trace;
+  int ntiles = 0;
   int trace_sweep = -1;  // sweep of the next solve whose diagonal solves are recorded
 
   int n = 0;
@@ -170,10 +172,11 @@ struct b2dev_ctx {
   double free_energy = 0.0, step = 0.0;
   int dynamic = 1;
   bool ready = false;
-  int state_parity = 0;        // R64 buffer holding the current reactions
-  bool state_u_merit = false;  // current U lives in Um (true) or Us
-  bool have_conmerit = false;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  int state_r = 0;             // R64 buffer holding the current reactions
+  Buf* state_u = nullptr;      // buffer holding the current U (one of Us[], Um[])
+  Buf* state_cm = nullptr;     // buffer holding the per-row merit numerators of the last merit pass
+  cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  long long launches = 0;  // kernels of this library launched on this context
   float assemble_ms = 0.f;
 };
 
@@ -231,6 +234,7 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
     int* selp = ptr<int>(c->sel);
     ColourControl* ctl = ptr<ColourControl>(c->cctrl);
     void* args[] = {&nn, &ap, &ac, &sd, &colp, &selp, &ctl};
+    c->launches++;
     B2_CK(cudaLaunchCooperativeKernel((const void*)k_jp_colour, grid, T, args, 0, st));
   }
   B2_CK(cudaMemcpyAsync(&cc, c->cctrl.p, sizeof cc, cudaMemcpyDeviceToHost, st));
@@ -240,6 +244,7 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   c->ncolours = n > 0 ? cc.ncolours : 0;
 
   // rows sorted by colour, ascending row index inside a colour (stable radix sort)
+  c->launches++;
   k_iota<<<blocks_for(n, T), T, 0, st>>>(n, ptr<int>(c->iota));
   if (n > 0) {
     size_t bytes = 0;
@@ -249,15 +254,21 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
     B2_CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, bytes, ptr<int>(c->colour), ptr<int>(c->keys_out),
                                           ptr<int>(c->iota), ptr<int>(c->perm), n, 0, 9, st));
   }
+  c->launches++;
   k_colptr<<<blocks_for(n + 1, T), T, 0, st>>>(n, ptr<int>(c->keys_out), c->ncolours, ptr<int>(c->colptr));
+  c->launches++;
   k_inverse_perm<<<blocks_for(n, T), T, 0, st>>>(n, ptr<int>(c->perm), ptr<int>(c->iperm));
+  c->launches++;
   k_sorted_degree<<<blocks_for(n, T), T, 0, st>>>(n, ptr<int>(c->perm), ptr<int>(c->adjptr), ptr<int>(c->sdeg));
+  c->launches++;
   k_set_last_zero<<<1, 32, 0, st>>>(ptr<int>(c->sdeg), n);
   B2_TRY(scan_exclusive(c, ptr<int>(c->sdeg), ptr<int>(c->rowptr), n + 1));
 
   c->colptr_h.assign(c->ncolours + 1, 0);
-  if (c->ncolours > 0)
+  if (c->ncolours > 0) {
     B2_CK(cudaMemcpyAsync(c->colptr_h.data(), c->colptr.p, sizeof(int) * (c->ncolours + 1), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaStreamSynchronize(st));
+  }
 
   const long long K = c->K;
   c->kstride = ((K + 31) / 32) * 32;
@@ -267,11 +278,13 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   const int wpb = 8;
   if (n > 0 && K > 0) {
     if (assembled) {
+      c->launches++;
       k_offdiag_assembled<<<blocks_for(n, wpb), wpb * kWarp, 0, st>>>(
           n, ptr<int>(c->perm), ptr<int>(c->iperm), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<int>(c->adjbod),
           ptr<int>(c->master), ptr<double>(c->factors), c->step, ptr<int>(c->rowptr), ptr<int>(c->col),
           ptr<double>(c->W64), ptr<float>(c->W32), c->kstride);
     } else {
+      c->launches++;
       k_offdiag_copy<<<blocks_for(n, wpb), wpb * kWarp, 0, st>>>(
           n, ptr<int>(c->perm), ptr<int>(c->iperm), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<double>(c->Woff_c),
           ptr<int>(c->rowptr), ptr<int>(c->col), ptr<double>(c->W64), ptr<float>(c->W32), c->kstride);
@@ -286,27 +299,37 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   B2_TRY(ensure(c->fric, sizeof(double) * (n + 1)));
   B2_TRY(ensure(c->rest, sizeof(double) * (n + 1)));
   B2_TRY(ensure(c->coh, sizeof(double) * (n + 1)));
+  c->launches++;
   k_rows_permute<<<blocks_for(n, T), T, 0, st>>>(
       n, ptr<int>(c->perm), ptr<double>(c->Wii), ptr<double>(c->Aii), ptr<double>(c->rho_c), ptr<double>(c->B_c),
       ptr<double>(c->V_c), ptr<double>(c->gap_c), ptr<double>(c->fric_c), ptr<double>(c->rest_c),
       ptr<double>(c->coh_c), ptr<double>(c->Wd), ptr<double>(c->Ad), ptr<double>(c->Bv), ptr<double>(c->Vv),
       ptr<double>(c->rho), ptr<double>(c->gap), ptr<double>(c->fric), ptr<double>(c->rest), ptr<double>(c->coh));
 
-  for (int b = 0; b < 2; b++) {
+  for (int b = 0; b < 3; b++) {
     B2_TRY(ensure(c->R64[b], sizeof(double4) * (n + 1)));
     B2_TRY(ensure(c->R32[b], sizeof(float4) * (n + 1)));
   }
-  B2_TRY(ensure(c->Us, sizeof(double4) * (n + 1)));
-  B2_TRY(ensure(c->Um, sizeof(double4) * (n + 1)));
-  B2_TRY(ensure(c->conmerit, sizeof(double) * (n + 1)));
+  for (int b = 0; b < 2; b++) {
+    B2_TRY(ensure(c->Us[b], sizeof(double4) * (n + 1)));
+    B2_TRY(ensure(c->Um[b], sizeof(double4) * (n + 1)));
+    B2_TRY(ensure(c->conmerit[b], sizeof(double) * (n + 1)));
+  }
+  B2_TRY(ensure(c->done, sizeof(int) * (n + 1)));
+  // tiles of 32 rows per colour, numbered in forward colour order
+  std::vector<int> tb(c->ncolours + 1, 0);
+  for (int k = 0; k < c->ncolours; k++) tb[k + 1] = tb[k] + (c->colptr_h[k + 1] - c->colptr_h[k] + kWarp - 1) / kWarp;
+  c->ntiles = tb[c->ncolours];
+  B2_TRY(ensure(c->tilebase, sizeof(int) * (c->ncolours + 2)));
+  B2_CK(cudaMemcpyAsync(c->tilebase.p, tb.data(), sizeof(int) * (c->ncolours + 1), cudaMemcpyHostToDevice, st));
   // new contacts start from R = U = 0 (MEM_Alloc zeroes, mem.c:64-86)
   B2_CK(cudaMemsetAsync(c->R64[0].p, 0, sizeof(double4) * (n + 1), st));
   B2_CK(cudaMemsetAsync(c->R32[0].p, 0, sizeof(float4) * (n + 1), st));
-  B2_CK(cudaMemsetAsync(c->Us.p, 0, sizeof(double4) * (n + 1), st));
-  B2_CK(cudaMemsetAsync(c->conmerit.p, 0, sizeof(double) * (n + 1), st));
-  c->state_parity = 0;
-  c->state_u_merit = false;
-  c->have_conmerit = false;
+  B2_CK(cudaMemsetAsync(c->Us[0].p, 0, sizeof(double4) * (n + 1), st));
+  B2_CK(cudaMemsetAsync(c->conmerit[0].p, 0, sizeof(double) * (n + 1), st));
+  c->state_r = 0;
+  c->state_u = &c->Us[0];
+  c->state_cm = nullptr;
   B2_CK(cudaGetLastError());
   B2_CK(cudaStreamSynchronize(st));
   c->ready = true;
@@ -323,20 +346,23 @@ int upload(b2dev_ctx* c, Buf& b, const T* src, size_t count, int on_device) {
   return B2DEV_OK;
 }
 
-int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter, int iter0, int in_parity,
-                 int u0_from_merit, int grid_req, SolveControl* out) {
+int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter, int iter0, int in,
+                 int u0_from_merit, int grid_req, SolveControl* out, float* kernel_ms, int* grid_used) {
   const int n = c->n;
   cudaStream_t st = c->stream;
   const void* fn = mixed ? (const void*)k_solve<true> : (const void*)k_solve<false>;
-  // blocks needed for the largest colour (8 row tiles of 32 per block)
-  int maxc = 0;
-  for (int k = 0; k < c->ncolours; k++) maxc = std::max(maxc, c->colptr_h[k + 1] - c->colptr_h[k]);
-  const int want = grid_req > 0 ? grid_req : blocks_for(blocks_for(maxc, kWarp), kSolveWarps);
+  // enough warps for the tiles of about two sweeps in flight, capped by residency
+  const int want = grid_req > 0 ? grid_req : blocks_for(2LL * c->ntiles, kSolveWarps);
   int grid = 0;
   const size_t smem = mixed ? solve_smem_bytes<true>() : solve_smem_bytes<false>();
   B2_TRY(cooperative_grid(fn, kSolveThreads, c->sms, want, &grid, smem));
-  B2_TRY(ensure(c->part, sizeof(double) * 2 * 4 * grid));
+  B2_TRY(ensure(c->part, sizeof(double) * (3 * 4 * (size_t)c->ntiles + 4)));
+  B2_TRY(ensure(c->decided, sizeof(int) * (maxiter + 2)));
   B2_CK(cudaMemsetAsync(c->sctrl.p, 0, sizeof(SolveControl), st));
+  B2_CK(cudaMemsetAsync(c->done.p, 0, sizeof(int) * (n + 1), st));
+  B2_CK(cudaMemsetAsync(c->decided.p, 0, sizeof(int) * (maxiter + 2), st));
+  if (!u0_from_merit && c->state_u != &c->Us[0])  // the first sweep reads its U from Us[0]
+    B2_CK(cudaMemcpyAsync(c->Us[0].p, c->state_u->p, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st));
   B2_CK(cudaMemsetAsync(ptr<unsigned long long>(c->failkey) + iter0, 0, sizeof(unsigned long long) * (maxiter + 1), st));
   B2_CK(cudaMemsetAsync(ptr<unsigned>(c->failcount) + iter0, 0, sizeof(unsigned) * (maxiter + 1), st));
 
@@ -344,6 +370,10 @@ int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxite
   memset(&a, 0, sizeof a);
   a.n = n;
   a.ncolours = c->ncolours;
+  a.ntiles = c->ntiles;
+  a.tilebase = ptr<int>(c->tilebase);
+  a.done = ptr<int>(c->done);
+  a.decided = ptr<int>(c->decided);
   a.colptr = ptr<int>(c->colptr);
   a.rowptr = ptr<int>(c->rowptr);
   a.col = ptr<int>(c->col);
@@ -359,13 +389,15 @@ int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxite
   a.fric = ptr<double>(c->fric);
   a.rest = ptr<double>(c->rest);
   a.coh = ptr<double>(c->coh);
-  a.R64[0] = ptr<double4>(c->R64[0]);
-  a.R64[1] = ptr<double4>(c->R64[1]);
-  a.R32[0] = ptr<float4>(c->R32[0]);
-  a.R32[1] = ptr<float4>(c->R32[1]);
-  a.Us = ptr<double4>(c->Us);
-  a.Um = ptr<double4>(c->Um);
-  a.conmerit = ptr<double>(c->conmerit);
+  for (int b = 0; b < 3; b++) {
+    a.R64[b] = ptr<double4>(c->R64[b]);
+    a.R32[b] = ptr<float4>(c->R32[b]);
+  }
+  for (int b = 0; b < 2; b++) {
+    a.Us[b] = ptr<double4>(c->Us[b]);
+    a.Um[b] = ptr<double4>(c->Um[b]);
+    a.conmerit[b] = ptr<double>(c->conmerit[b]);
+  }
   a.part = ptr<double>(c->part);
   a.rerhist = ptr<double>(c->rer);
   a.merhist = ptr<double>(c->mer);
@@ -386,7 +418,7 @@ int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxite
   a.reverse = o->reverse;
   a.nomerit = o->nomerit;
   a.iter0 = iter0;
-  a.in_parity = in_parity;
+  a.in = in;
   a.u0_from_merit = u0_from_merit;
   if (c->trace_sweep >= 0 && iter0 == 0) {
     B2_TRY(ensure(c->trace, sizeof(double) * kTraceStride * (n + 1)));
@@ -395,10 +427,26 @@ int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxite
     a.trace_sweep = c->trace_sweep;
   }
   void* args[] = {&a};
+  B2_CK(cudaEventRecord(c->ev[4], st));
+  c->launches++;
   B2_CK(cudaLaunchCooperativeKernel(fn, grid, kSolveThreads, args, smem, st));
+  B2_CK(cudaEventRecord(c->ev[5], st));
   B2_CK(cudaMemcpyAsync(out, c->sctrl.p, sizeof(SolveControl), cudaMemcpyDeviceToHost, st));
   B2_CK(cudaStreamSynchronize(st));
-  if (out->timeout) { set_err("solve: grid barrier wait timed out"); return B2DEV_ETIMEOUT; }
+  if (kernel_ms) cudaEventElapsedTime(kernel_ms, c->ev[4], c->ev[5]);
+  if (grid_used) *grid_used = grid;
+  if (out->timeout) { set_err("solve: a bounded device-side wait timed out"); return B2DEV_ETIMEOUT; }
+  // where the returned iterate's R, U and per-row merit live
+  const int f = out->final_iter;
+  c->state_r = (in + 1 + f) % 3;
+  if (o->nomerit) {
+    c->state_u = &c->Us[(f + 1) & 1];
+    c->state_cm = nullptr;
+  } else {
+    const int msweep = out->thrown ? f : f + 1;  // sweep that evaluated the merit of the returned iterate
+    c->state_u = &c->Um[msweep & 1];
+    c->state_cm = &c->conmerit[msweep & 1];
+  }
   return B2DEV_OK;
 }
 
@@ -435,7 +483,7 @@ b2dev_ctx* b2dev_create(int device, void* stream) {
     }
     c->own_stream = true;
   }
-  for (int k = 0; k < 4; k++) cudaEventCreate(&c->ev[k]);
+  for (int k = 0; k < 8; k++) cudaEventCreate(&c->ev[k]);
   if (ensure(c->sctrl, sizeof(SolveControl)) != B2DEV_OK || ensure(c->fe_dev, sizeof(double)) != B2DEV_OK ||
       ensure(c->bad, sizeof(int)) != B2DEV_OK) {
     b2dev_destroy(c);
@@ -454,11 +502,13 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->cursor, &c->brow, &c->deg, &c->adjptr, &c->adjcol, &c->adjbod, &c->Woff_c, &c->colour, &c->sel,
                 &c->cctrl, &c->keys_out, &c->iota, &c->perm, &c->iperm, &c->colptr, &c->sdeg, &c->rowptr, &c->col,
                 &c->W64, &c->W32, &c->Wd, &c->Ad, &c->Bv, &c->Vv, &c->rho, &c->gap, &c->fric, &c->rest, &c->coh,
-                &c->R64[0], &c->R64[1], &c->R32[0], &c->R32[1], &c->Us, &c->Um, &c->conmerit, &c->part, &c->rer,
+                &c->R64[0], &c->R64[1], &c->R64[2], &c->R32[0], &c->R32[1], &c->R32[2], &c->Us[0], &c->Us[1],
+                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tilebase,
+                &c->part, &c->rer,
                 &c->mer, &c->failkey, &c->failcount, &c->sctrl, &c->io, &c->cub_tmp, &c->trace};
   for (Buf* b : all)
     if (b->p) cudaFree(b->p);
-  for (int k = 0; k < 4; k++)
+  for (int k = 0; k < 8; k++)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   if (c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -525,9 +575,11 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
   sc.minv = ptr<double>(c->minv); sc.velo = ptr<double>(c->velo); sc.velo0 = ptr<double>(c->velo0);
   sc.obstacle = ptr<int>(c->obst); sc.master = ptr<int>(c->master); sc.slave = ptr<int>(c->slave);
   sc.mpnt = ptr<double>(c->mpnt); sc.spnt = ptr<double>(c->spnt); sc.base = ptr<double>(c->base);
+  c->launches++;
   k_row_factors<<<rb, T, 0, st>>>(sc, step, ptr<double>(c->factors), ptr<double>(c->Wii), ptr<double>(c->Aii),
                                   ptr<double>(c->rho_c), ptr<double>(c->B_c), ptr<double>(c->V_c),
                                   ptr<double>(c->fe_part), ptr<int>(c->bad));
+  c->launches++;
   k_sum_partials<<<1, 1024, 0, st>>>(ptr<double>(c->fe_part), rb, ptr<double>(c->fe_dev));
   {  // body indices are checked before any kernel indexes per-body arrays with them
     int bad0 = 0;
@@ -542,16 +594,21 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
   B2_TRY(ensure(c->cursor, sizeof(int) * (nb + 1)));
   B2_CK(cudaMemsetAsync(c->bdeg.p, 0, sizeof(int) * (nb + 1), st));
   B2_CK(cudaMemsetAsync(c->cursor.p, 0, sizeof(int) * (nb + 1), st));
+  c->launches++;
   k_body_count<<<rb, T, 0, st>>>(n, ptr<int>(c->master), ptr<int>(c->slave), ptr<int>(c->obst), ptr<int>(c->bdeg));
   B2_TRY(scan_exclusive(c, ptr<int>(c->bdeg), ptr<int>(c->bptr), nb + 1));
   B2_TRY(ensure(c->brow, sizeof(int) * (2 * (size_t)n + 1)));
+  c->launches++;
   k_body_fill<<<rb, T, 0, st>>>(n, ptr<int>(c->master), ptr<int>(c->slave), ptr<int>(c->obst), ptr<int>(c->bptr),
                                 ptr<int>(c->cursor), ptr<int>(c->brow));
+  c->launches++;
   k_body_sort<<<blocks_for(nb, T), T, 0, st>>>(nb, ptr<int>(c->bptr), ptr<int>(c->brow));
   B2_TRY(ensure(c->deg, sizeof(int) * (n + 1)));
   B2_TRY(ensure(c->adjptr, sizeof(int) * (n + 1)));
+  c->launches++;
   k_row_degree<<<rb, T, 0, st>>>(n, ptr<int>(c->master), ptr<int>(c->slave), ptr<int>(c->obst), ptr<int>(c->bptr),
                                  ptr<int>(c->deg));
+  c->launches++;
   k_set_last_zero<<<1, 32, 0, st>>>(ptr<int>(c->deg), n);
   B2_TRY(scan_exclusive(c, ptr<int>(c->deg), ptr<int>(c->adjptr), n + 1));
   int K = 0, bad = 0;
@@ -564,6 +621,7 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
   c->K = K;
   B2_TRY(ensure(c->adjcol, sizeof(int) * ((size_t)K + 1)));
   B2_TRY(ensure(c->adjbod, sizeof(int) * ((size_t)K + 1)));
+  c->launches++;
   k_adj_fill<<<rb, T, 0, st>>>(n, ptr<int>(c->master), ptr<int>(c->slave), ptr<int>(c->obst), ptr<int>(c->bptr),
                                ptr<int>(c->brow), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<int>(c->adjbod));
   B2_TRY(prepare_layout(c, colour_seed, true));
@@ -611,6 +669,7 @@ int b2dev_upload_locdyn(b2dev_ctx* c, int n, const double* W, const double* A, c
   B2_TRY(upload(c, c->Woff_c, Woff, (size_t)9 * K, on_device));
   if (on_device && n > 0) {  // device-resident graph: check it before the colouring walks it
     B2_CK(cudaMemsetAsync(c->bad.p, 0, sizeof(int), c->stream));
+    c->launches++;
     k_check_graph<<<blocks_for(n, 256), 256, 0, c->stream>>>(n, K, ptr<int>(c->adjptr), ptr<int>(c->adjcol),
                                                              ptr<int>(c->bad));
     int bad = 0;
@@ -635,11 +694,13 @@ int b2dev_set_state(b2dev_ctx* c, const double* R, const double* U, int on_devic
     else B2_CK(cudaMemsetAsync(dR, 0, sizeof(double) * 3 * n, st));
     if (U) B2_CK(cudaMemcpyAsync(dU, U, sizeof(double) * 3 * n, kd, st));
     else B2_CK(cudaMemsetAsync(dU, 0, sizeof(double) * 3 * n, st));
+    c->launches++;
     k_state_in<<<blocks_for(n, 256), 256, 0, st>>>(n, ptr<int>(c->perm), dR, dU, ptr<double4>(c->R64[0]),
-                                                   ptr<float4>(c->R32[0]), ptr<double4>(c->Us));
+                                                   ptr<float4>(c->R32[0]), ptr<double4>(c->Us[0]));
   }
-  c->state_parity = 0;
-  c->state_u_merit = false;
+  c->state_r = 0;
+  c->state_u = &c->Us[0];
+  c->state_cm = nullptr;
   B2_CK(cudaGetLastError());
   return B2DEV_OK;
 }
@@ -656,15 +717,16 @@ int b2dev_get_state(b2dev_ctx* c, double* R, double* U, double* conmerit, int on
   double* dC = dU + 3 * (size_t)(n + 1);
   double lo = c->free_energy < DBL_EPSILON ? 1.0 : c->free_energy;
   lo = lo == 0.0 ? 1.0 : lo;
-  k_state_out<<<blocks_for(n, 256), 256, 0, st>>>(n, ptr<int>(c->perm), ptr<double4>(c->R64[c->state_parity]),
-                                                  c->state_u_merit ? ptr<double4>(c->Um) : ptr<double4>(c->Us),
-                                                  c->have_conmerit ? ptr<double>(c->conmerit) : nullptr, lo, dR, dU,
-                                                  c->have_conmerit ? dC : nullptr);
+  c->launches++;
+  k_state_out<<<blocks_for(n, 256), 256, 0, st>>>(n, ptr<int>(c->perm), ptr<double4>(c->R64[c->state_r]),
+                                                  ptr<double4>(*c->state_u),
+                                                  c->state_cm ? ptr<double>(*c->state_cm) : nullptr, lo, dR, dU,
+                                                  c->state_cm ? dC : nullptr);
   const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   if (R) B2_CK(cudaMemcpyAsync(R, dR, sizeof(double) * 3 * n, kd, st));
   if (U) B2_CK(cudaMemcpyAsync(U, dU, sizeof(double) * 3 * n, kd, st));
   if (conmerit) {
-    if (c->have_conmerit) B2_CK(cudaMemcpyAsync(conmerit, dC, sizeof(double) * n, kd, st));
+    if (c->state_cm) B2_CK(cudaMemcpyAsync(conmerit, dC, sizeof(double) * n, kd, st));
     else if (on_device) B2_CK(cudaMemsetAsync(conmerit, 0, sizeof(double) * n, st));
     else memset(conmerit, 0, sizeof(double) * n);
   }
@@ -694,27 +756,37 @@ int b2dev_solve(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_solve_report* rep
   SolveControl s1, s2;
   memset(&s1, 0, sizeof s1);
   memset(&s2, 0, sizeof s2);
-  int parity = c->state_parity;
+  if (c->n == 0) {  // no rows: one iteration with zero error and merit, as the reference loop does
+    rep->iters = 1;
+    B2_CK(cudaEventRecord(c->ev[3], st));
+    B2_CK(cudaEventSynchronize(c->ev[3]));
+    if (rerhist) rerhist[0] = 0.0;
+    if (merhist) merhist[0] = 0.0;
+    return B2DEV_OK;
+  }
   int iters = 0, final_global = 0;
   bool thrown = false;
   double merit = 0.0, error = 0.0;
   std::vector<std::pair<int, int>> ranges;  // [first, last] global sweep indices of returned iterates
   if (o->precision == B2DEV_MIXED) {
-    k_shadow<<<blocks_for(c->n, 256), 256, 0, st>>>(c->n, ptr<double4>(c->R64[parity]), ptr<float4>(c->R32[parity]));
-    B2_TRY(solve_launch(c, true, o, maxiter - 1, 0, parity, 0, o->grid, &s1));
+    c->launches++;
+    k_shadow<<<blocks_for(c->n, 256), 256, 0, st>>>(c->n, ptr<double4>(c->R64[c->state_r]),
+                                                    ptr<float4>(c->R32[c->state_r]));
+    B2_TRY(solve_launch(c, true, o, maxiter - 1, 0, c->state_r, 0, o->grid, &s1, &rep->ms_kernel[0], &rep->grid));
+    rep->sweeps_launch[0] = s1.sweeps;
     rep->merit_input = s1.merit_input;
     iters = s1.iters;
     thrown = s1.thrown != 0;
     ranges.push_back({0, s1.final_iter});
-    parity = (parity + 1 + s1.final_iter) & 1;
     merit = s1.merit;
     error = s1.error;
     rep->iters_mixed = iters;
     rep->sweeps = s1.sweeps;
     if (!thrown) {  // closing FP64 refinement, continuing the iteration count
-      B2_TRY(solve_launch(c, false, o, maxiter - iters, iters, parity, o->nomerit ? 0 : 1, o->grid, &s2));
+      B2_TRY(solve_launch(c, false, o, maxiter - iters, iters, c->state_r, o->nomerit ? 0 : 1, o->grid, &s2,
+                          &rep->ms_kernel[1], &rep->grid));
+      rep->sweeps_launch[1] = s2.sweeps;
       ranges.push_back({iters, iters + s2.final_iter});
-      parity = (parity + 1 + s2.final_iter) & 1;
       iters += s2.iters;
       thrown = s2.thrown != 0;
       merit = s2.merit;
@@ -722,12 +794,12 @@ int b2dev_solve(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_solve_report* rep
       rep->sweeps += s2.sweeps;
     }
   } else {
-    B2_TRY(solve_launch(c, false, o, maxiter, 0, parity, 0, o->grid, &s1));
+    B2_TRY(solve_launch(c, false, o, maxiter, 0, c->state_r, 0, o->grid, &s1, &rep->ms_kernel[0], &rep->grid));
+    rep->sweeps_launch[0] = s1.sweeps;
     rep->merit_input = s1.merit_input;
     iters = s1.iters;
     thrown = s1.thrown != 0;
     ranges.push_back({0, s1.final_iter});
-    parity = (parity + 1 + s1.final_iter) & 1;
     merit = s1.merit;
     error = s1.error;
     rep->sweeps = s1.sweeps;
@@ -756,9 +828,6 @@ int b2dev_solve(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_solve_report* rep
   rep->nfailures = nfail;
   rep->merit = o->nomerit ? 0.0 : merit;
   rep->error = error;
-  c->state_parity = parity;
-  c->state_u_merit = !o->nomerit;
-  c->have_conmerit = !o->nomerit;
   return B2DEV_OK;
 }
 
@@ -800,6 +869,7 @@ int b2dev_get_locdyn(b2dev_ctx* c, double* W, double* A, double* rho, double* B,
   if (adjcol && K) B2_CK(cudaMemcpy(adjcol, c->adjcol.p, sizeof(int) * K, cudaMemcpyDeviceToHost));
   if (Woff && K) {
     B2_TRY(ensure(c->io, sizeof(double) * 9 * (K + 1)));
+    c->launches++;
     k_offdiag_out<<<blocks_for(n, 256), 256, 0, c->stream>>>(n, ptr<int>(c->iperm), ptr<int>(c->adjptr),
                                                              ptr<int>(c->rowptr), ptr<double>(c->W64), c->kstride,
                                                              ptr<double>(c->io));
@@ -811,6 +881,8 @@ int b2dev_get_locdyn(b2dev_ctx* c, double* W, double* A, double* rho, double* B,
 }
 
 float b2dev_last_assemble_ms(b2dev_ctx* c) { return c ? c->assemble_ms : 0.f; }
+
+long long b2dev_launch_count(b2dev_ctx* c) { return c ? c->launches : 0; }
 
 int b2dev_trace_sweep(b2dev_ctx* c, int sweep) {
   if (!c) return B2DEV_EINVAL;
@@ -861,6 +933,7 @@ int b2dev_diag_solve_batch(b2dev_ctx* c, int n, int solver, int failure, double 
   B2_CK(cudaMemcpyAsync(dco, cohesion, sizeof(double) * n, h2d, st));
   B2_CK(cudaMemcpyAsync(dU, U, sizeof(double) * 3 * n, h2d, st));
   B2_CK(cudaMemcpyAsync(dR, R, sizeof(double) * 3 * n, h2d, st));
+  c->launches++;
   k_diag_batch<<<blocks_for(n, 128), 128, 0, st>>>(n, solver, failure, diagepsilon, diagmaxiter, dynamic, step, dW,
                                                    dB, dV, drho, dgap, dfr, dre, dco, dU, dR, dk);
   B2_CK(cudaGetLastError());

@@ -1,5 +1,5 @@
-// b2_solve.cuh -- colour-by-colour block Gauss-Seidel with the merit pass fused
-// into the next sweep.
+// b2_solve.cuh -- block Gauss-Seidel in colour order with dataflow scheduling
+// and the merit pass fused into the next sweep.
 //
 // Reference loop (bgs.c:913-1069): every iteration sweeps the rows in list
 // order (each row: B' = B + sum_j W_ij R_j, diagonal solve, error sums), then
@@ -7,18 +7,33 @@
 // every row and the merit; the loop stops when error <= epsilon and merit <=
 // meritval, or at maxiter.
 //
-// Here the rows are stored sorted by colour (rows of one colour share no
-// non-obstacle body, so W_ij = 0 inside a colour) and processed colour after
-// colour, which is the reference loop run on the colour-permuted list. The
-// merit of iterate s is evaluated inside sweep s+1: R is double-buffered, so
-// while row i gathers R_j for its Gauss-Seidel sum (the new value for rows of
-// colours already swept, the old one otherwise) it also gathers the old value
-// of every neighbour and forms U_merit = B + W_ii R_i^s + sum_j W_ij R_j^s. The
-// merit row term, the U handed to the diagonal solver (the reference starts
-// iteration s+1 from the U the merit pass wrote) and the stopping decision for
-// iterate s are therefore exactly the reference's, while W is streamed once per
-// iteration instead of twice. The sweep after the final iterate is discarded;
-// the final R and U are those of the iterate that met the rule.
+// Order. Rows are stored sorted by colour (rows of one colour share no
+// non-obstacle body, so W_ij = 0 inside a colour); the sweep is the reference
+// loop run on this colour-permuted list (colours in reverse on the backward
+// sweeps of the reverse option).
+//
+// Fused merit. The merit of iterate s is evaluated inside sweep s+1: while a
+// row gathers its neighbours' reactions for the Gauss-Seidel sum (the new
+// value for rows earlier in the sweep, the previous one otherwise) it also
+// forms U_merit = B + W_ii R_i^s + sum_j W_ij R_j^s from the previous values.
+// The merit, the U handed to the diagonal solver (the reference starts
+// iteration s+1 from the U its merit pass wrote) and the stopping decision for
+// iterate s are the reference's, while W is streamed once per iteration.
+//
+// Scheduling. Instead of a grid-wide barrier per colour, warps claim tiles of
+// 32 rows from one counter in (sweep, colour, tile) order and wait only for
+// the rows a tile reads: for sweep s, a neighbour earlier in the sweep must
+// have completed sweep s, a later one sweep s-1 (per-row completion counters).
+// Reactions are triple-buffered, so a tile of sweep s+1 may run while sweep s
+// is being decided; sweep s+2 waits for that decision. Every wait is bounded.
+// Progress: a tile only waits for rows of tiles claimed before it, so the
+// earliest unfinished tile can always proceed (all blocks are co-resident,
+// cooperative launch).
+//
+// Reductions. Each tile writes its error and merit partial sums; the warp that
+// completes the last tile of a sweep adds them in tile order and takes the
+// stopping decision, decisions being taken in sweep order. Results therefore
+// do not depend on which warp ran which tile.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -29,25 +44,31 @@ namespace b2 {
 
 constexpr int kSolveThreads = 256;
 constexpr int kSolveWarps = kSolveThreads / kWarp;
-constexpr int kChunkUnroll = 4;           // 32-block chunks whose loads are issued together
-constexpr uint64_t kBarrierLimitNs = 2000000000ull;  // 2 s per grid barrier wait
+constexpr int kChunkUnroll = 4;                      // 32-block chunks whose loads are issued together
+constexpr uint64_t kBarrierLimitNs = 2000000000ull;  // 2 s per bounded wait
+
+enum { DECIDE_NONE = 0, DECIDE_CONTINUE = 1, DECIDE_STOP = 2 };
 
 // Device-side control block of one solve launch (zeroed before launch).
 struct SolveControl {
-  unsigned bar_count;       // monotone arrival counter of the grid barrier
-  int timeout;              // a barrier wait gave up (device error)
+  unsigned next_tile;       // tile counter in (sweep, colour, tile) order
+  unsigned tiles_done[3];   // completed tiles of sweep s, slot s % 3
+  int stop;                 // set once the final decision is taken
+  int timeout;              // a bounded wait gave up (device error)
   int final_iter;           // launch-local index of the returned iterate
   int iters;                // iterations completed in this launch
   int thrown;               // FAILURE_EXIT raised
-  int sweeps;               // sweeps executed (including the discarded one)
+  int sweeps;               // sweeps started (including discarded speculative ones)
   double merit;             // merit of the returned iterate (0 with nomerit)
   double error;             // relative error of the returned iterate
   double merit_input;       // merit of the input iterate (merit mode)
+  double prev_error;        // relative error of the latest iterate, kept between decisions
 };
 
 struct SolveArgs {
-  int n, ncolours;
+  int n, ncolours, ntiles;
   const int* colptr;        // [ncolours+1] colour offsets in sorted order
+  const int* tilebase;      // [ncolours+1] first tile of each colour (forward order)
   const int* rowptr;        // [n+1]
   const int* col;           // [K] neighbour (sorted index)
   const double* W64;        // 9 planes of K doubles (plane stride kstride)
@@ -62,57 +83,58 @@ struct SolveArgs {
   const double* fric;       // [n]
   const double* rest;       // [n]
   const double* coh;        // [n]
-  double4* R64[2];          // double-buffered reactions
-  float4* R32[2];           // float shadows (mixed precision)
-  double4* Us;              // U state (input U; diagonal-solver output without merit)
-  double4* Um;              // U of the merit pass (final U with merit)
-  double* conmerit;         // per-row merit numerator of the last merit pass (may be null)
-  double* part;             // [2][gridDim][4] per-block partial sums
+  double4* R64[3];          // triple-buffered reactions: iterate k in R64[(in + 1 + k) % 3]
+  float4* R32[3];           // float shadows (mixed precision)
+  double4* Us[2];           // U state without merit: sweep s reads Us[s%2], writes Us[(s+1)%2]
+  double4* Um[2];           // merit U computed in sweep s: Um[s%2]
+  double* conmerit[2];      // per-row merit numerator computed in sweep s: conmerit[s%2] (may be null)
+  int* done;                // [n] sweeps completed per row (zeroed before launch)
+  int* decided;             // [maxiter+2] decision after each sweep (zeroed before launch)
+  double* part;             // [3][ntiles][4] per-tile partial sums
   double* rerhist;          // global history arrays (indexed by iter0 + k)
   double* merhist;
   unsigned long long* failkey;  // per sweep: max (order position + 1) << 2 | kind of a diagonal failure
   unsigned* failcount;          // per sweep: number of diagonal failures
   SolveControl* ctrl;
+  double* trace;            // per-row diagonal-solve record of one sweep (null: off)
+  int trace_sweep;
   double epsilon, meritval, diagepsilon, step, merit_denom;
   int maxiter, diagmaxiter, diagsolver, failure, dynamic, reverse, nomerit;
   int iter0;                // global index of this launch's first iteration
-  int in_parity;            // R64/R32 buffer holding the input iterate
+  int in;                   // R64/R32 buffer holding the input iterate
   int u0_from_merit;        // sweep 0 hands the merit U (not Us) to the diagonal solver
-  double* trace;            // per-row diagonal-solve record of one sweep (null: off)
-  int trace_sweep;          // launch-local sweep whose rows are recorded
 };
 
 // trace record per row: B'[3], U in[3], R in[3], U out[3], R out[3], kind
 constexpr int kTraceStride = 16;
 
-__device__ __forceinline__ bool grid_barrier(SolveControl* ctrl, unsigned nblocks, unsigned& epoch) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ok = 1;
-    epoch++;
-    __threadfence();
-    atomicAdd(&ctrl->bar_count, 1u);
-    const unsigned target = nblocks * epoch;
-    volatile unsigned* cnt = &ctrl->bar_count;
-    volatile int* to = &ctrl->timeout;
-    uint64_t t0 = globaltimer_ns();
-    while (*cnt < target) {
-      if (*to) { ok = 0; break; }
-      if (globaltimer_ns() - t0 > kBarrierLimitNs) { *to = 1; ok = 0; break; }
-      __nanosleep(32);
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return ok != 0;
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
 
-template <typename T>
-__device__ __forceinline__ T shfl_down(T v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
-// 32-byte load that bypasses L1 (the R buffers are rewritten by other SMs
-// between grid barriers, so a line cached in L1 could be stale).
+// Bounded wait until *p >= need. Returns false when the solve has stopped or
+// the wait ran out (the timeout is recorded in ctrl).
+__device__ __noinline__ bool wait_at_least(const int* p, int need, SolveControl* ctrl) {
+  if (ld_acquire(p) >= need) return true;
+  const uint64_t t0 = globaltimer_ns();
+  volatile int* stop = &ctrl->stop;
+  volatile int* to = &ctrl->timeout;
+  while (ld_acquire(p) < need) {
+    if (*stop || *to) return false;
+    if (globaltimer_ns() - t0 > kBarrierLimitNs) { *to = 1; return false; }
+    __nanosleep(64);
+  }
+  return true;
+}
+
+// 32-byte load that bypasses L1 (reaction buffers are rewritten by other SMs
+// while the kernel runs, so a line cached in L1 could be stale).
 __device__ __forceinline__ double4 ldcg4(const double4* p) {
   const double2* q = reinterpret_cast<const double2*>(p);
   const double2 lo = __ldcg(q), hi = __ldcg(q + 1);
@@ -129,15 +151,16 @@ struct SweepFlags {
 
 // One tile of up to 32 consecutive rows of one colour, owned by one warp.
 // Lanes stride over the tile's contiguous CSR range (lane per block, coalesced
-// plane loads) and form the W_ij R_j products, which are staged in shared
-// memory; lane r then adds the products of row r0 + r in list order onto its
-// running sums, which start from B (Gauss-Seidel, bgs.c:957-963) and from
-// B + W_ii R_i (merit U, mrf.c:61-68). Together with the build's disabled
-// multiply-add contraction this reproduces the reference's NVADDMUL chains
-// operation for operation in FP64. Lane r then solves its row (diagonal
-// solve and merit term in FP64).
+// plane loads), wait for the neighbour rows they read, and form the W_ij R_j
+// products, which are staged in shared memory; lane r then adds the products
+// of row r0 + r in list order onto its running sums, which start from B
+// (Gauss-Seidel, bgs.c:957-963) and from B + W_ii R_i (merit U, mrf.c:61-68).
+// With the build's disabled multiply-add contraction this reproduces the
+// reference's NVADDMUL chains operation for operation in FP64. Lane r then
+// solves its row (diagonal solve and merit term in FP64). Returns false if a
+// wait gave up or the solve has stopped.
 template <bool MIXED>
-__device__ __forceinline__ void solve_tile(const SolveArgs& a, const SweepFlags& f, int r0, int nr, int cs, int ce,
+__device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags& f, int r0, int nr, int cs, int ce,
                                            int s, int rin, int rout, void* stage_raw, int* tp, double& errup,
                                            double& errlo, double& mnum) {
   typedef typename std::conditional<MIXED, float, double>::type real;
@@ -149,9 +172,11 @@ __device__ __forceinline__ void solve_tile(const SolveArgs& a, const SweepFlags&
   const int p = r0 + lane;
   if (lane <= nr) tp[lane] = __ldg(a.rowptr + r0 + lane);
   if (lane == 0 && nr == kWarp) tp[kWarp] = __ldg(a.rowptr + r0 + kWarp);
+  bool ok = true;
+  if (own) ok = wait_at_least(a.done + p, s, a.ctrl);  // this row's previous sweep is complete
 
   double B[3] = {0.0, 0.0, 0.0}, W[9], Rold[3] = {0.0, 0.0, 0.0}, ag[3], am[3] = {0.0, 0.0, 0.0};
-  if (own) {
+  if (own && ok) {
 #pragma unroll
     for (int q = 0; q < 3; q++) B[q] = __ldg(a.Bv + (size_t)q * n + p);
     const double4 ro = ldcg4(a.R64[rin] + p);
@@ -192,6 +217,9 @@ __device__ __forceinline__ void solve_tile(const SolveArgs& a, const SweepFlags&
       const int slot = u * kWarp + lane;
       if (j >= 0) {
         const bool earlier = f.backward ? (j >= ce) : (j < cs);
+        // a neighbour earlier in this sweep must have completed it, a later
+        // one the previous sweep
+        ok = wait_at_least(a.done + j, (earlier && f.gs) ? s + 1 : s, a.ctrl) && ok;
         real ro0, ro1, ro2;
         if constexpr (MIXED) {
           const float4 v = __ldcg(a.R32[rin] + j);
@@ -252,6 +280,8 @@ __device__ __forceinline__ void solve_tile(const SolveArgs& a, const SweepFlags&
     }
     __syncwarp();
   }
+  ok = __all_sync(0xffffffffu, ok);
+  if (!ok) return false;
 
   // ---- lane per row: merit term and diagonal solve
   if (own) {
@@ -271,14 +301,14 @@ __device__ __forceinline__ void solve_tile(const SolveArgs& a, const SweepFlags&
       for (int q = 0; q < 9; q++) A[q] = __ldg(a.Ad + (size_t)q * n + p);
       const double up = merit_row(cp, A, V, am, Rold);
       mnum += up;
-      a.Um[p] = make_double4(am[0], am[1], am[2], 0.0);
-      if (a.conmerit) a.conmerit[p] = up;
+      a.Um[s & 1][p] = make_double4(am[0], am[1], am[2], 0.0);
+      if (a.conmerit[0]) a.conmerit[s & 1][p] = up;
     }
     if (f.gs) {
       double R[3] = {Rold[0], Rold[1], Rold[2]};
       double U[3];
       if (f.u_merit) { U[0] = am[0]; U[1] = am[1]; U[2] = am[2]; }
-      else { const double4 us = ldcg4(a.Us + p); U[0] = us.x; U[1] = us.y; U[2] = us.z; }
+      else { const double4 us = ldcg4(a.Us[s & 1] + p); U[0] = us.x; U[1] = us.y; U[2] = us.z; }
       double* tr = (a.trace && s == a.trace_sweep) ? a.trace + (size_t)kTraceStride * p : nullptr;
       if (tr) {
 #pragma unroll
@@ -298,32 +328,15 @@ __device__ __forceinline__ void solve_tile(const SolveArgs& a, const SweepFlags&
       }
       a.R64[rout][p] = make_double4(R[0], R[1], R[2], 0.0);
       if constexpr (MIXED) a.R32[rout][p] = make_float4((float)R[0], (float)R[1], (float)R[2], 0.f);
-      if (a.nomerit) a.Us[p] = make_double4(U[0], U[1], U[2], 0.0);
+      if (a.nomerit) a.Us[(s + 1) & 1][p] = make_double4(U[0], U[1], U[2], 0.0);
       const double d0 = R[0] - Rold[0], d1 = R[1] - Rold[1], d2 = R[2] - Rold[2];
       errup += d0 * d0 + d1 * d1 + d2 * d2;
       errlo += R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
     }
+    st_release(a.done + p, s + 1);  // publishes this row's writes of sweep s
   }
   __syncwarp();
-}
-
-// Deterministic block reduction of three per-thread values (fixed shuffle
-// tree, then warps in order). Result valid in thread 0.
-__device__ __forceinline__ void block_sum3(double& x, double& y, double& z, double (*red)[3]) {
-#pragma unroll
-  for (int d = 16; d >= 1; d >>= 1) {
-    x += __shfl_down_sync(0xffffffffu, x, d);
-    y += __shfl_down_sync(0xffffffffu, y, d);
-    z += __shfl_down_sync(0xffffffffu, z, d);
-  }
-  const int warp = threadIdx.x / kWarp, lane = threadIdx.x & (kWarp - 1);
-  if (lane == 0) { red[warp][0] = x; red[warp][1] = y; red[warp][2] = z; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double sx = 0, sy = 0, sz = 0;
-    for (int w = 0; w < (int)(blockDim.x / kWarp); w++) { sx += red[w][0]; sy += red[w][1]; sz += red[w][2]; }
-    x = sx; y = sy; z = sz;
-  }
+  return true;
 }
 
 // dynamic shared memory of k_solve: per warp 6 x (32 * kChunkUnroll) staged products
@@ -332,101 +345,145 @@ __host__ __device__ constexpr size_t solve_smem_bytes() {
   return (size_t)kSolveWarps * 6 * kWarp * kChunkUnroll * (MIXED ? sizeof(float) : sizeof(double));
 }
 
+// Decision after sweep s, taken by the warp that completed the sweep's last
+// tile: sums the tile partials in tile order and applies the reference's
+// stopping rule (bgs.c:1028-1036, mrf.c:176-184). Decisions are taken in
+// sweep order.
+__device__ __noinline__ void finalize_sweep(const SolveArgs& a, int s) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  volatile int* decided = a.decided;
+  int prev = DECIDE_CONTINUE;
+  if (s >= 1) {
+    bool ok = true;
+    if (lane == 0) ok = wait_at_least(a.decided + s - 1, DECIDE_CONTINUE, a.ctrl);
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (!ok) return;
+    prev = decided[s - 1];
+  }
+  if (prev == DECIDE_STOP) {
+    if (lane == 0) { a.ctrl->tiles_done[s % 3] = 0; __threadfence(); decided[s] = DECIDE_STOP; }
+    return;
+  }
+  double su = 0.0, sl = 0.0, sm = 0.0;
+  const double* base = a.part + (size_t)(s % 3) * a.ntiles * 4;
+  for (int t = lane; t < a.ntiles; t += kWarp) {
+    su += __ldcg(base + 4 * t); sl += __ldcg(base + 4 * t + 1); sm += __ldcg(base + 4 * t + 2);
+  }
+#pragma unroll
+  for (int d = 16; d >= 1; d >>= 1) {
+    su += __shfl_down_sync(0xffffffffu, su, d);
+    sl += __shfl_down_sync(0xffffffffu, sl, d);
+    sm += __shfl_down_sync(0xffffffffu, sm, d);
+  }
+  if (lane != 0) return;
+  const bool merit_mode = !a.nomerit;
+  const double error = sqrt(su) / sqrt(sl == 0.0 ? 1.0 : sl);                // bgs.c:1028
+  const double merit_prev = merit_mode ? (0.5 * sm) / a.merit_denom : 0.0;   // mrf.c:176-184
+  const bool gs_sweep = !(merit_mode && s == a.maxiter);
+  const bool failed = __ldcg(a.failkey + a.iter0 + s) != 0ull;
+  volatile double* perr_slot = &a.ctrl->prev_error;
+  const double perr = *perr_slot;  // error of iterate s-1
+  int final_iter = -2, thrown = 0;
+  double fm = 0.0, fe = 0.0;
+  if (merit_mode) {
+    if (s == 0) a.ctrl->merit_input = merit_prev;
+    if (s >= 1) {
+      a.rerhist[a.iter0 + s - 1] = perr;
+      a.merhist[a.iter0 + s - 1] = merit_prev;
+      const bool meets = !(perr > a.epsilon || merit_prev > a.meritval);  // bgs.c:1036
+      if (meets || s == a.maxiter) { final_iter = s - 1; fm = merit_prev; fe = perr; }
+      else if (gs_sweep && failed && a.failure == FAIL_EXIT) { final_iter = s; thrown = 1; fm = merit_prev; fe = error; }
+    } else if (failed && a.failure == FAIL_EXIT) {
+      final_iter = 0; thrown = 1; fe = error;
+    }
+  } else {
+    a.rerhist[a.iter0 + s] = error;
+    a.merhist[a.iter0 + s] = 0.0;
+    if (failed && a.failure == FAIL_EXIT) { final_iter = s; thrown = 1; fe = error; }
+    else if (!(error > a.epsilon) || s + 1 >= a.maxiter) { final_iter = s; fe = error; }
+  }
+  *perr_slot = error;
+  a.ctrl->tiles_done[s % 3] = 0;
+  if (final_iter >= -1) {
+    a.ctrl->final_iter = final_iter;
+    a.ctrl->iters = thrown ? final_iter : final_iter + 1;
+    a.ctrl->thrown = thrown;
+    a.ctrl->merit = fm;
+    a.ctrl->error = fe;
+    __threadfence();
+    decided[s] = DECIDE_STOP;
+    *(volatile int*)&a.ctrl->stop = 1;
+  } else {
+    __threadfence();
+    decided[s] = DECIDE_CONTINUE;
+  }
+}
+
 template <bool MIXED>
 __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(SolveArgs a) {
   extern __shared__ __align__(16) unsigned char solve_smem[];
   __shared__ int tp[kSolveWarps][kWarp + 1];
-  __shared__ double red[kSolveWarps][3];
   const int warp = threadIdx.x / kWarp;
-  const int gwarp = blockIdx.x * kSolveWarps + warp;
-  const int nwarps = gridDim.x * kSolveWarps;
-  const unsigned nblocks = gridDim.x;
-  unsigned epoch = 0;
-  double prev_error = 0.0;
+  const int lane = threadIdx.x & (kWarp - 1);
+  void* stage = solve_smem + (size_t)warp * (solve_smem_bytes<MIXED>() / kSolveWarps);
   const bool merit_mode = !a.nomerit;
+  const int maxsweep = merit_mode ? a.maxiter : a.maxiter - 1;  // last sweep that can run
+  volatile int* stop = &a.ctrl->stop;
+  volatile int* decided = a.decided;
+  const int T = a.ntiles;
 
-  for (int s = 0;; s++) {
+  while (true) {
+    unsigned t = 0;
+    if (lane == 0) t = atomicAdd(&a.ctrl->next_tile, 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    const int s = (int)(t / (unsigned)T);
+    const int w = (int)(t % (unsigned)T);
+    if (s > maxsweep || *stop) break;
+    if (s >= 2) {  // sweep s reuses the buffers of iterate s-3: wait for the decision after sweep s-2
+      bool ok = true;
+      if (lane == 0) ok = wait_at_least(a.decided + s - 2, DECIDE_CONTINUE, a.ctrl);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok || decided[s - 2] == DECIDE_STOP) break;
+    }
     SweepFlags f;
     f.gs = !(merit_mode && s == a.maxiter);
     f.merit = merit_mode;
     f.u_merit = merit_mode && (s >= 1 || a.u0_from_merit);
     f.backward = a.reverse && ((a.iter0 + s) & 1);
-    const int rin = (a.in_parity + s) & 1;        // iterate s-1
-    const int rout = (a.in_parity + s + 1) & 1;   // iterate s
+    const int rin = (a.in + s) % 3;       // iterate s-1
+    const int rout = (a.in + s + 1) % 3;  // iterate s
+    // tile w of the sweep -> colour (in sweep order) and tile inside it
+    int cc = 0;
+    while (cc + 1 < a.ncolours) {
+      const int c_next = f.backward ? a.ncolours - 2 - cc : cc + 1;
+      const int start = f.backward ? (T - __ldg(a.tilebase + c_next + 1)) : __ldg(a.tilebase + c_next);
+      if (w >= start) cc++; else break;
+    }
+    const int c = f.backward ? a.ncolours - 1 - cc : cc;
+    const int first = f.backward ? (T - __ldg(a.tilebase + c + 1)) : __ldg(a.tilebase + c);
+    const int cs = __ldg(a.colptr + c), ce = __ldg(a.colptr + c + 1);
+    const int r0 = cs + (w - first) * kWarp;
+    const int nr = min(kWarp, ce - r0);
     double errup = 0.0, errlo = 0.0, mnum = 0.0;
-
-    for (int cc = 0; cc < a.ncolours; cc++) {
-      const int c = f.backward ? a.ncolours - 1 - cc : cc;
-      const int cs = __ldg(a.colptr + c), ce = __ldg(a.colptr + c + 1);
-      const int ntiles = (ce - cs + kWarp - 1) / kWarp;
-      for (int t = gwarp; t < ntiles; t += nwarps) {
-        const int r0 = cs + t * kWarp;
-        const int nr = min(kWarp, ce - r0);
-        void* stage = solve_smem + (size_t)warp * (solve_smem_bytes<MIXED>() / kSolveWarps);
-        solve_tile<MIXED>(a, f, r0, nr, cs, ce, s, rin, rout, stage, tp[warp], errup, errlo, mnum);
-      }
-      if (cc == a.ncolours - 1) {
-        block_sum3(errup, errlo, mnum, red);
-        if (threadIdx.x == 0) {
-          double* pp = a.part + ((size_t)(s & 1) * nblocks + blockIdx.x) * 4;
-          pp[0] = errup; pp[1] = errlo; pp[2] = mnum;
-        }
-      }
-      if (!grid_barrier(a.ctrl, nblocks, epoch)) return;
+    if (!solve_tile<MIXED>(a, f, r0, nr, cs, ce, s, rin, rout, stage, tp[warp], errup, errlo, mnum)) break;
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+      errup += __shfl_down_sync(0xffffffffu, errup, d);
+      errlo += __shfl_down_sync(0xffffffffu, errlo, d);
+      mnum += __shfl_down_sync(0xffffffffu, mnum, d);
     }
-    if (a.ncolours == 0) {
-      if (threadIdx.x == 0) {
-        double* pp = a.part + ((size_t)(s & 1) * nblocks + blockIdx.x) * 4;
-        pp[0] = pp[1] = pp[2] = 0.0;
-      }
-      if (!grid_barrier(a.ctrl, nblocks, epoch)) return;
+    unsigned prev = 0;
+    if (lane == 0) {
+      double* pp = a.part + ((size_t)(s % 3) * T + w) * 4;
+      pp[0] = errup; pp[1] = errlo; pp[2] = mnum;
+      __threadfence();
+      prev = atomicAdd(&a.ctrl->tiles_done[s % 3], 1u);
+      atomicMax(&a.ctrl->sweeps, s + 1);
     }
-
-    // every block sums the partials in the same order and takes the same decision
-    double su = 0.0, sl = 0.0, sm = 0.0;
-    for (unsigned b = 0; b < nblocks; b++) {
-      const double* pp = a.part + ((size_t)(s & 1) * nblocks + b) * 4;
-      su += __ldcg(pp); sl += __ldcg(pp + 1); sm += __ldcg(pp + 2);
-    }
-    const double error = sqrt(su) / sqrt(sl == 0.0 ? 1.0 : sl);  // bgs.c:1028
-    const double merit_prev = merit_mode ? (0.5 * sm) / a.merit_denom : 0.0;  // mrf.c:176-184
-    const bool failed = __ldcg(a.failkey + a.iter0 + s) != 0ull;
-    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
-    int final_iter = -2, thrown = 0;
-    double final_merit = 0.0, final_error = 0.0;
-
-    if (merit_mode) {
-      if (s == 0 && lead) a.ctrl->merit_input = merit_prev;
-      if (s >= 1) {
-        if (lead) { a.rerhist[a.iter0 + s - 1] = prev_error; a.merhist[a.iter0 + s - 1] = merit_prev; }
-        const bool meets = !(prev_error > a.epsilon || merit_prev > a.meritval);  // bgs.c:1036
-        if (meets || s == a.maxiter) {
-          final_iter = s - 1; final_merit = merit_prev; final_error = prev_error;
-        } else if (f.gs && failed && a.failure == FAIL_EXIT) {
-          final_iter = s; thrown = 1; final_merit = merit_prev; final_error = error;
-        }
-      } else if (f.gs && failed && a.failure == FAIL_EXIT) {
-        final_iter = 0; thrown = 1; final_merit = 0.0; final_error = error;
-      }
-    } else {
-      if (lead) { a.rerhist[a.iter0 + s] = error; a.merhist[a.iter0 + s] = 0.0; }
-      if (failed && a.failure == FAIL_EXIT) {
-        final_iter = s; thrown = 1; final_error = error;
-      } else if (!(error > a.epsilon) || s + 1 >= a.maxiter) {
-        final_iter = s; final_error = error;
-      }
-    }
-    prev_error = error;
-    if (final_iter >= -1) {
-      if (lead) {
-        a.ctrl->final_iter = final_iter;
-        a.ctrl->iters = thrown ? final_iter : final_iter + 1;
-        a.ctrl->thrown = thrown;
-        a.ctrl->sweeps = s + 1;
-        a.ctrl->merit = final_merit;
-        a.ctrl->error = final_error;
-      }
-      return;
+    prev = __shfl_sync(0xffffffffu, prev, 0);
+    if (prev == (unsigned)T - 1) {
+      __threadfence();
+      finalize_sweep(a, s);
     }
   }
 }

@@ -38,6 +38,7 @@ struct b2gs_solver
   double *rerhist, *merhist;
   int iters_mixed;
   double solve_ms, merit_input;
+  b2dev_solve_report last;
 };
 
 struct b2gs_locdyn
@@ -126,6 +127,7 @@ int b2gs_solve (b2gs_solver *gs, b2gs_locdyn *ldy)
   rc = b2dev_solve (ldy->dev, &o, &rep, gs->rerhist, gs->merhist);
   if (rc != B2DEV_OK) return rc;
 
+  gs->last = rep;
   gs->iters = rep.iters;
   gs->iters_mixed = rep.iters_mixed;
   gs->solve_ms = rep.ms_device;
@@ -258,6 +260,12 @@ void b2gs_set_grid (b2gs_solver *gs, int blocks) { gs->grid = blocks > 0 ? block
 int b2gs_get_iters_mixed (b2gs_solver *gs) { return gs->iters_mixed; }
 double b2gs_get_solve_ms (b2gs_solver *gs) { return gs->solve_ms; }
 double b2gs_get_merit_input (b2gs_solver *gs) { return gs->merit_input; }
+int b2gs_get_report (b2gs_solver *gs, void *report, int nbytes)
+{
+  if (!gs || !report || nbytes < (int) sizeof (b2dev_solve_report)) return B2DEV_EINVAL;
+  memcpy (report, &gs->last, sizeof (b2dev_solve_report));
+  return 0;
+}
 
 /* ---- local dynamics ---- */
 

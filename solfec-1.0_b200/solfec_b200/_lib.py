@@ -34,7 +34,8 @@ class b2dev_solve_opts(C.Structure):
 class b2dev_solve_report(C.Structure):
     _fields_ = [('iters', C.c_int), ('thrown', C.c_int), ('last_fail_kind', C.c_int), ('nfailures', C.c_int),
                 ('sweeps', C.c_int), ('iters_mixed', C.c_int), ('merit', C.c_double), ('error', C.c_double),
-                ('merit_input', C.c_double), ('ms_device', C.c_float)]
+                ('merit_input', C.c_double), ('ms_device', C.c_float), ('ms_kernel', C.c_float * 2),
+                ('sweeps_launch', C.c_int * 2), ('grid', C.c_int)]
 
 
 class b2gs_bodies(C.Structure):
@@ -72,6 +73,7 @@ _SIGNATURES = {
     'b2dev_get_colours': (C.c_int, [C.c_void_p, C.c_void_p]),
     'b2dev_get_locdyn': (C.c_int, [C.c_void_p] + [C.c_void_p] * 8 + [C.POINTER(C.c_double)]),
     'b2dev_last_assemble_ms': (C.c_float, [C.c_void_p]),
+    'b2dev_launch_count': (C.c_longlong, [C.c_void_p]),
     'b2dev_trace_sweep': (C.c_int, [C.c_void_p, C.c_int]),
     'b2dev_get_trace': (C.c_int, [C.c_void_p, C.c_void_p]),
     'b2dev_diag_solve_batch': (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
@@ -102,6 +104,7 @@ _SIGNATURES = {
     'b2gs_get_iters_mixed': (C.c_int, [C.c_void_p]),
     'b2gs_get_solve_ms': (C.c_double, [C.c_void_p]),
     'b2gs_get_merit_input': (C.c_double, [C.c_void_p]),
+    'b2gs_get_report': (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     'b2gs_locdyn_create': (C.c_void_p, [C.c_int, C.c_void_p]),
     'b2gs_locdyn_destroy': (None, [C.c_void_p]),
     'b2gs_locdyn_update_begin': (C.c_int, [C.c_void_p, C.POINTER(b2gs_bodies), C.POINTER(b2gs_contacts),

@@ -20,7 +20,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import CALLBACK, b2gs_bodies, b2gs_contacts, last_error, lib, ptr
+from ._lib import CALLBACK, b2dev_solve_report, b2gs_bodies, b2gs_contacts, last_error, lib, ptr
 
 DIAGSOLVERS = ('PROJECTED_GRADIENT', 'DE_SAXCE_FENG', 'SEMISMOOTH_NEWTON', 'PROJECTED_NEWTON')
 FAILURES = ('CONTINUE', 'EXIT', 'CALLBACK')
@@ -114,6 +114,13 @@ class LOCDYN:
         rc = lib().b2gs_locdyn_set(self._h, n, *[ptr(a) for a in arrs], float(ld.free_energy), float(ld.step),
                                    int(ld.dynamic), 0)
         _check(rc, 'b2gs_locdyn_set')
+
+    def set_state_ptr(self, R_ptr, U_ptr, on_device=1):
+        """Initial R/U from raw pointers (device pointers when on_device)."""
+        _check(lib().b2gs_locdyn_set_state(self._h, R_ptr, U_ptr, int(on_device)), 'b2gs_locdyn_set_state')
+
+    def get_state_ptr(self, R_ptr, U_ptr, cm_ptr=None, on_device=1):
+        _check(lib().b2gs_locdyn_get_state(self._h, R_ptr, U_ptr, cm_ptr, int(on_device)), 'b2gs_locdyn_get_state')
 
     def set_state(self, R=None, U=None):
         n = self.sizes()[0]
@@ -361,6 +368,14 @@ class GAUSS_SEIDEL_SOLVER:
     @property
     def merit_input(self):
         return float(lib().b2gs_get_merit_input(self._h))
+
+    @property
+    def report(self) -> dict:
+        """Device report of the last solve (kernel times, sweeps, grid)."""
+        r = b2dev_solve_report()
+        _check(lib().b2gs_get_report(self._h, C.byref(r), C.sizeof(r)), 'b2gs_get_report')
+        return {k: (list(getattr(r, k)) if k in ('ms_kernel', 'sweeps_launch') else getattr(r, k))
+                for k, _ in r._fields_}
 
     def write_state(self) -> str:
         buf = C.create_string_buffer(64)
