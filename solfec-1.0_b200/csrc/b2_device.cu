@@ -164,6 +164,7 @@ struct b2dev_ctx {
   Buf R64[3], R32[3], Us[2], Um[2], conmerit[2], done, decided, tilebase, part, rer, mer, failkey, failcount, sctrl, io,
       cub_tmp, trace;
   int ntiles = 0;
+  int max_tile_blocks = 0;  // most off-diagonal blocks of one 32-row tile
   int trace_sweep = -1;  // sweep of the next solve whose diagonal solves are recorded
 
   int n = 0;
@@ -320,6 +321,18 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   std::vector<int> tb(c->ncolours + 1, 0);
   for (int k = 0; k < c->ncolours; k++) tb[k + 1] = tb[k] + (c->colptr_h[k + 1] - c->colptr_h[k] + kWarp - 1) / kWarp;
   c->ntiles = tb[c->ncolours];
+  {  // largest number of blocks of one tile (sizes the per-warp staging)
+    std::vector<int> rp(n + 1);
+    B2_CK(cudaMemcpyAsync(rp.data(), c->rowptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaStreamSynchronize(st));
+    int mx = 0;
+    for (int k = 0; k < c->ncolours; k++)
+      for (int r = c->colptr_h[k]; r < c->colptr_h[k + 1]; r += kWarp) {
+        const int e = std::min(r + kWarp, c->colptr_h[k + 1]);
+        mx = std::max(mx, rp[e] - rp[r]);
+      }
+    c->max_tile_blocks = mx;
+  }
   B2_TRY(ensure(c->tilebase, sizeof(int) * (c->ncolours + 2)));
   B2_CK(cudaMemcpyAsync(c->tilebase.p, tb.data(), sizeof(int) * (c->ncolours + 1), cudaMemcpyHostToDevice, st));
   // new contacts start from R = U = 0 (MEM_Alloc zeroes, mem.c:64-86)
@@ -354,7 +367,13 @@ int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxite
   // enough warps for the tiles of about two sweeps in flight, capped by residency
   const int want = grid_req > 0 ? grid_req : blocks_for(2LL * c->ntiles, kSolveWarps);
   int grid = 0;
-  const size_t smem = mixed ? solve_smem_bytes<true>() : solve_smem_bytes<false>();
+  // staging for the largest tile, within the shared memory of one block
+  const int max_smem = 200 * 1024;
+  const size_t per_word = mixed ? sizeof(float) : sizeof(double);
+  const int gfit = (int)((max_smem / kSolveWarps - kTileHeader) / per_word / 3) - kWarp * kChunkUnroll;
+  int gcap = std::max(kWarp, std::min(((c->max_tile_blocks + kWarp - 1) / kWarp) * kWarp, (gfit / kWarp) * kWarp));
+  const size_t wsm = mixed ? solve_warp_smem<true>(gcap) : solve_warp_smem<false>(gcap);
+  const size_t smem = wsm * kSolveWarps;
   B2_TRY(cooperative_grid(fn, kSolveThreads, c->sms, want, &grid, smem));
   B2_TRY(ensure(c->part, sizeof(double) * (3 * 4 * (size_t)c->ntiles + 4)));
   B2_TRY(ensure(c->decided, sizeof(int) * (maxiter + 2)));
@@ -420,6 +439,8 @@ int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxite
   a.iter0 = iter0;
   a.in = in;
   a.u0_from_merit = u0_from_merit;
+  a.gcap = gcap;
+  a.warp_smem = (int)wsm;
   if (c->trace_sweep >= 0 && iter0 == 0) {
     B2_TRY(ensure(c->trace, sizeof(double) * kTraceStride * (n + 1)));
     B2_CK(cudaMemsetAsync(c->trace.p, 0, sizeof(double) * kTraceStride * (n + 1), st));

@@ -45,6 +45,7 @@ namespace b2 {
 constexpr int kSolveThreads = 256;
 constexpr int kSolveWarps = kSolveThreads / kWarp;
 constexpr int kChunkUnroll = 4;                      // 32-block chunks whose loads are issued together
+constexpr int kTileHeader = 256;                     // bytes of per-warp shared memory before the staging
 constexpr uint64_t kBarrierLimitNs = 2000000000ull;  // 2 s per bounded wait
 
 enum { DECIDE_NONE = 0, DECIDE_CONTINUE = 1, DECIDE_STOP = 2 };
@@ -103,6 +104,8 @@ struct SolveArgs {
   int iter0;                // global index of this launch's first iteration
   int in;                   // R64/R32 buffer holding the input iterate
   int u0_from_merit;        // sweep 0 hands the merit U (not Us) to the diagonal solver
+  int gcap;                 // Gauss-Seidel products staged per tile window
+  int warp_smem;            // bytes of dynamic shared memory per warp
 };
 
 // trace record per row: B'[3], U in[3], R in[3], U out[3], R out[3], kind
@@ -149,23 +152,77 @@ struct SweepFlags {
   bool backward;  // colours in reverse order
 };
 
+// Loads of one 32-block chunk: column indices and the nine coefficients of
+// each block (lane per block, coalesced plane loads).
+template <bool MIXED, typename real>
+__device__ __forceinline__ void load_chunk(const SolveArgs& a, int base, int ke, int lane, int (&jj)[kChunkUnroll],
+                                           real (&w)[kChunkUnroll][9]) {
+#pragma unroll
+  for (int u = 0; u < kChunkUnroll; u++) {
+    const int k = base + u * kWarp + lane;
+    jj[u] = k < ke ? __ldg(a.col + k) : -1;
+  }
+#pragma unroll
+  for (int u = 0; u < kChunkUnroll; u++) {
+    const int k = base + u * kWarp + lane;
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+      if (k < ke) {
+        if constexpr (MIXED) w[u][q] = __ldg(a.W32 + q * a.kstride + k);
+        else w[u][q] = __ldg(a.W64 + q * a.kstride + k);
+      } else {
+        w[u][q] = real(0);
+      }
+    }
+  }
+}
+
+template <bool MIXED, typename real>
+__device__ __forceinline__ void load_r(const SolveArgs& a, int buf, int j, real& r0, real& r1, real& r2) {
+  if constexpr (MIXED) {
+    const float4 v = __ldcg(a.R32[buf] + j);
+    r0 = v.x; r1 = v.y; r2 = v.z;
+  } else {
+    const double4 v = ldcg4(a.R64[buf] + j);
+    r0 = v.x; r1 = v.y; r2 = v.z;
+  }
+}
+
+// shared memory of one warp of k_solve: tile row offsets, merit products of
+// one chunk, and the Gauss-Seidel products of up to gcap blocks of the tile
+template <bool MIXED>
+__host__ __device__ constexpr size_t solve_warp_smem(int gcap) {
+  return (size_t)kTileHeader + (size_t)(3 * kWarp * kChunkUnroll + 3 * gcap) * (MIXED ? sizeof(float) : sizeof(double));
+}
+
 // One tile of up to 32 consecutive rows of one colour, owned by one warp.
-// Lanes stride over the tile's contiguous CSR range (lane per block, coalesced
-// plane loads), wait for the neighbour rows they read, and form the W_ij R_j
-// products, which are staged in shared memory; lane r then adds the products
-// of row r0 + r in list order onto its running sums, which start from B
-// (Gauss-Seidel, bgs.c:957-963) and from B + W_ii R_i (merit U, mrf.c:61-68).
-// With the build's disabled multiply-add contraction this reproduces the
+//
+// Pass 1 needs only values of the previous sweep: lanes stride over the
+// tile's contiguous CSR range (lane per block, coalesced plane loads), form
+// the merit products W_ij R_j^old and the Gauss-Seidel products of neighbours
+// later in the sweep, and the merit term of each row is evaluated. Pass 2
+// waits for the neighbours earlier in the sweep and forms their products with
+// the new reactions. Only pass 2 and the diagonal solves lie on the chain of
+// colours, so the streaming of W and the merit overlap the waits.
+//
+// The products are staged in shared memory and lane r adds those of row
+// r0 + r in list order onto its running sums, which start from B
+// (Gauss-Seidel, bgs.c:957-963) and from B + W_ii R_i (merit U, mrf.c:61-68);
+// with the build's disabled multiply-add contraction this reproduces the
 // reference's NVADDMUL chains operation for operation in FP64. Lane r then
-// solves its row (diagonal solve and merit term in FP64). Returns false if a
-// wait gave up or the solve has stopped.
+// solves its row (diagonal solve in FP64). Tiles with more blocks than the
+// staging holds are processed in windows. Returns false if a wait gave up or
+// the solve has stopped.
 template <bool MIXED>
 __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags& f, int r0, int nr, int cs, int ce,
-                                           int s, int rin, int rout, void* stage_raw, int* tp, double& errup,
+                                           int s, int rin, int rout, unsigned char* wsm, double& errup,
                                            double& errlo, double& mnum) {
   typedef typename std::conditional<MIXED, float, double>::type real;
   constexpr int kSlots = kWarp * kChunkUnroll;
-  real(*stage)[kSlots] = reinterpret_cast<real(*)[kSlots]>(stage_raw);  // [6][kSlots]
+  int* tp = reinterpret_cast<int*>(wsm);                                              // [kWarp + 1]
+  real(*mst)[kSlots] = reinterpret_cast<real(*)[kSlots]>(wsm + kTileHeader);          // [3][kSlots]
+  real* gst = reinterpret_cast<real*>(wsm + kTileHeader + 3 * kSlots * sizeof(real));  // [3][gcap]
+  const int gcap = a.gcap;
   const int lane = threadIdx.x & (kWarp - 1);
   const int n = a.n;
   const bool own = lane < nr;
@@ -176,6 +233,11 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   if (own) ok = wait_at_least(a.done + p, s, a.ctrl);  // this row's previous sweep is complete
 
   double B[3] = {0.0, 0.0, 0.0}, W[9], Rold[3] = {0.0, 0.0, 0.0}, ag[3], am[3] = {0.0, 0.0, 0.0};
+  double V[3] = {0.0, 0.0, 0.0};
+  ContactParams cp;
+  cp.step = a.step;
+  cp.dynamic = a.dynamic;
+  cp.friction = cp.restitution = cp.cohesion = cp.gap = 0.0;
   if (own && ok) {
 #pragma unroll
     for (int q = 0; q < 3; q++) B[q] = __ldg(a.Bv + (size_t)q * n + p);
@@ -184,118 +246,64 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
 #pragma unroll
     for (int q = 0; q < 9; q++) W[q] = __ldg(a.Wd + (size_t)q * n + p);
     if (f.merit) nvaddmul(B, W, Rold, am);
+    cp.friction = __ldg(a.fric + p);
+    cp.restitution = __ldg(a.rest + p);
+    cp.cohesion = __ldg(a.coh + p);
+    cp.gap = __ldg(a.gap + p);
+#pragma unroll
+    for (int q = 0; q < 3; q++) V[q] = __ldg(a.Vv + (size_t)q * n + p);
   }
   ag[0] = B[0]; ag[1] = B[1]; ag[2] = B[2];
   __syncwarp();
   const int kb = tp[0], ke = tp[nr];
   const int mb = own ? tp[lane] : 0, me = own ? tp[lane + 1] : 0;
+  const int nwin = ke > kb ? (ke - kb + gcap - 1) / gcap : 1;
 
-  for (int base = kb; base < ke; base += kSlots) {
-    int jj[kChunkUnroll];
-    real w[kChunkUnroll][9];
+  for (int win = 0; win < nwin; win++) {
+    const int wb = kb + win * gcap, we = min(ke, wb + gcap);
+    // ---- pass 1: previous-sweep values (merit products, later neighbours)
+    for (int base = wb; base < we; base += kSlots) {
+      int jj[kChunkUnroll];
+      real w[kChunkUnroll][9];
+      load_chunk<MIXED, real>(a, base, we, lane, jj, w);
 #pragma unroll
-    for (int u = 0; u < kChunkUnroll; u++) {
-      const int k = base + u * kWarp + lane;
-      jj[u] = k < ke ? __ldg(a.col + k) : -1;
-    }
-#pragma unroll
-    for (int u = 0; u < kChunkUnroll; u++) {
-      const int k = base + u * kWarp + lane;
-#pragma unroll
-      for (int q = 0; q < 9; q++) {
-        if (k < ke) {
-          if constexpr (MIXED) w[u][q] = __ldg(a.W32 + q * a.kstride + k);
-          else w[u][q] = __ldg(a.W64 + q * a.kstride + k);
-        } else {
-          w[u][q] = real(0);
-        }
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kChunkUnroll; u++) {
-      const int j = jj[u];
-      const int slot = u * kWarp + lane;
-      if (j >= 0) {
-        const bool earlier = f.backward ? (j >= ce) : (j < cs);
-        // a neighbour earlier in this sweep must have completed it, a later
-        // one the previous sweep
-        ok = wait_at_least(a.done + j, (earlier && f.gs) ? s + 1 : s, a.ctrl) && ok;
-        real ro0, ro1, ro2;
-        if constexpr (MIXED) {
-          const float4 v = __ldcg(a.R32[rin] + j);
-          ro0 = v.x; ro1 = v.y; ro2 = v.z;
-        } else {
-          const double4 v = ldcg4(a.R64[rin] + j);
-          ro0 = v.x; ro1 = v.y; ro2 = v.z;
-        }
-        const real* Wk = w[u];
-        real m0 = 0, m1 = 0, m2 = 0;
-        if (f.merit) {
-          m0 = Wk[0] * ro0 + Wk[3] * ro1 + Wk[6] * ro2;
-          m1 = Wk[1] * ro0 + Wk[4] * ro1 + Wk[7] * ro2;
-          m2 = Wk[2] * ro0 + Wk[5] * ro1 + Wk[8] * ro2;
-          stage[3][slot] = m0; stage[4][slot] = m1; stage[5][slot] = m2;
-        }
-        if (f.gs) {
-          real g0, g1, g2;
-          if (earlier) {
-            real rn0, rn1, rn2;
-            if constexpr (MIXED) {
-              const float4 v = __ldcg(a.R32[rout] + j);
-              rn0 = v.x; rn1 = v.y; rn2 = v.z;
-            } else {
-              const double4 v = ldcg4(a.R64[rout] + j);
-              rn0 = v.x; rn1 = v.y; rn2 = v.z;
-            }
-            g0 = Wk[0] * rn0 + Wk[3] * rn1 + Wk[6] * rn2;
-            g1 = Wk[1] * rn0 + Wk[4] * rn1 + Wk[7] * rn2;
-            g2 = Wk[2] * rn0 + Wk[5] * rn1 + Wk[8] * rn2;
-          } else if (f.merit) {
-            g0 = m0; g1 = m1; g2 = m2;
-          } else {
-            g0 = Wk[0] * ro0 + Wk[3] * ro1 + Wk[6] * ro2;
-            g1 = Wk[1] * ro0 + Wk[4] * ro1 + Wk[7] * ro2;
-            g2 = Wk[2] * ro0 + Wk[5] * ro1 + Wk[8] * ro2;
+      for (int u = 0; u < kChunkUnroll; u++) {
+        const int j = jj[u];
+        const int slot = u * kWarp + lane;
+        if (j >= 0) {
+          const bool earlier = f.backward ? (j >= ce) : (j < cs);
+          ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
+          real ro0, ro1, ro2;
+          load_r<MIXED, real>(a, rin, j, ro0, ro1, ro2);
+          const real* Wk = w[u];
+          real m0 = 0, m1 = 0, m2 = 0;
+          if (f.merit || (f.gs && !earlier)) {
+            m0 = Wk[0] * ro0 + Wk[3] * ro1 + Wk[6] * ro2;
+            m1 = Wk[1] * ro0 + Wk[4] * ro1 + Wk[7] * ro2;
+            m2 = Wk[2] * ro0 + Wk[5] * ro1 + Wk[8] * ro2;
           }
-          stage[0][slot] = g0; stage[1][slot] = g1; stage[2][slot] = g2;
+          if (f.merit) { mst[0][slot] = m0; mst[1][slot] = m1; mst[2][slot] = m2; }
+          if (f.gs && !earlier) {
+            const int g = base + slot - wb;
+            gst[g] = m0; gst[gcap + g] = m1; gst[2 * gcap + g] = m2;
+          }
         }
       }
-    }
-    __syncwarp();
-    // each row adds its own products, in list order
-    const int lo = mb > base ? mb : base;
-    const int hi = me < base + kSlots ? me : base + kSlots;
-    for (int k = lo; k < hi; k++) {
-      const int slot = k - base;
-      if (f.gs) {
-        ag[0] = ag[0] + (double)stage[0][slot];
-        ag[1] = ag[1] + (double)stage[1][slot];
-        ag[2] = ag[2] + (double)stage[2][slot];
+      __syncwarp();
+      if (f.merit) {  // each row adds its own merit products, in list order
+        const int lo = mb > base ? mb : base;
+        const int hi = me < base + kSlots ? me : base + kSlots;
+        for (int k = lo; k < hi; k++) {
+          const int slot = k - base;
+          am[0] = am[0] + (double)mst[0][slot];
+          am[1] = am[1] + (double)mst[1][slot];
+          am[2] = am[2] + (double)mst[2][slot];
+        }
       }
-      if (f.merit) {
-        am[0] = am[0] + (double)stage[3][slot];
-        am[1] = am[1] + (double)stage[4][slot];
-        am[2] = am[2] + (double)stage[5][slot];
-      }
+      __syncwarp();
     }
-    __syncwarp();
-  }
-  ok = __all_sync(0xffffffffu, ok);
-  if (!ok) return false;
-
-  // ---- lane per row: merit term and diagonal solve
-  if (own) {
-    ContactParams cp;
-    cp.friction = __ldg(a.fric + p);
-    cp.restitution = __ldg(a.rest + p);
-    cp.cohesion = __ldg(a.coh + p);
-    cp.gap = __ldg(a.gap + p);
-    cp.step = a.step;
-    cp.dynamic = a.dynamic;
-    double V[3];
-#pragma unroll
-    for (int q = 0; q < 3; q++) V[q] = __ldg(a.Vv + (size_t)q * n + p);
-    if (f.merit) {
+    // ---- merit term of each row (mrf.c:81-87), once its U is complete
+    if (win == nwin - 1 && f.merit && own) {
       double A[9];
 #pragma unroll
       for (int q = 0; q < 9; q++) A[q] = __ldg(a.Ad + (size_t)q * n + p);
@@ -304,6 +312,51 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
       a.Um[s & 1][p] = make_double4(am[0], am[1], am[2], 0.0);
       if (a.conmerit[0]) a.conmerit[s & 1][p] = up;
     }
+    if (!f.gs) continue;
+    // ---- pass 2: neighbours earlier in this sweep (their new reactions)
+    for (int base = wb; base < we; base += kSlots) {
+#pragma unroll
+      for (int u = 0; u < kChunkUnroll; u++) {
+        const int k = base + u * kWarp + lane;
+        if (k < we) {
+          const int j = __ldg(a.col + k);
+          const bool earlier = f.backward ? (j >= ce) : (j < cs);
+          if (earlier) {
+            ok = wait_at_least(a.done + j, s + 1, a.ctrl) && ok;
+            real Wk[9];
+#pragma unroll
+            for (int q = 0; q < 9; q++) {
+              if constexpr (MIXED) Wk[q] = __ldg(a.W32 + q * a.kstride + k);
+              else Wk[q] = __ldg(a.W64 + q * a.kstride + k);
+            }
+            real rn0, rn1, rn2;
+            load_r<MIXED, real>(a, rout, j, rn0, rn1, rn2);
+            const int g = k - wb;
+            gst[g] = Wk[0] * rn0 + Wk[3] * rn1 + Wk[6] * rn2;
+            gst[gcap + g] = Wk[1] * rn0 + Wk[4] * rn1 + Wk[7] * rn2;
+            gst[2 * gcap + g] = Wk[2] * rn0 + Wk[5] * rn1 + Wk[8] * rn2;
+          }
+        }
+      }
+    }
+    __syncwarp();
+    {  // each row adds its own Gauss-Seidel products, in list order
+      const int lo = mb > wb ? mb : wb;
+      const int hi = me < we ? me : we;
+      for (int k = lo; k < hi; k++) {
+        const int g = k - wb;
+        ag[0] = ag[0] + (double)gst[g];
+        ag[1] = ag[1] + (double)gst[gcap + g];
+        ag[2] = ag[2] + (double)gst[2 * gcap + g];
+      }
+    }
+    __syncwarp();
+  }
+  ok = __all_sync(0xffffffffu, ok);
+  if (!ok) return false;
+
+  // ---- lane per row: diagonal solve
+  if (own) {
     if (f.gs) {
       double R[3] = {Rold[0], Rold[1], Rold[2]};
       double U[3];
@@ -337,12 +390,6 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   }
   __syncwarp();
   return true;
-}
-
-// dynamic shared memory of k_solve: per warp 6 x (32 * kChunkUnroll) staged products
-template <bool MIXED>
-__host__ __device__ constexpr size_t solve_smem_bytes() {
-  return (size_t)kSolveWarps * 6 * kWarp * kChunkUnroll * (MIXED ? sizeof(float) : sizeof(double));
 }
 
 // Decision after sweep s, taken by the warp that completed the sweep's last
@@ -422,10 +469,9 @@ __device__ __noinline__ void finalize_sweep(const SolveArgs& a, int s) {
 template <bool MIXED>
 __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(SolveArgs a) {
   extern __shared__ __align__(16) unsigned char solve_smem[];
-  __shared__ int tp[kSolveWarps][kWarp + 1];
   const int warp = threadIdx.x / kWarp;
   const int lane = threadIdx.x & (kWarp - 1);
-  void* stage = solve_smem + (size_t)warp * (solve_smem_bytes<MIXED>() / kSolveWarps);
+  unsigned char* wsm = solve_smem + (size_t)warp * a.warp_smem;
   const bool merit_mode = !a.nomerit;
   const int maxsweep = merit_mode ? a.maxiter : a.maxiter - 1;  // last sweep that can run
   volatile int* stop = &a.ctrl->stop;
@@ -465,7 +511,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(SolveArgs a) {
     const int r0 = cs + (w - first) * kWarp;
     const int nr = min(kWarp, ce - r0);
     double errup = 0.0, errlo = 0.0, mnum = 0.0;
-    if (!solve_tile<MIXED>(a, f, r0, nr, cs, ce, s, rin, rout, stage, tp[warp], errup, errlo, mnum)) break;
+    if (!solve_tile<MIXED>(a, f, r0, nr, cs, ce, s, rin, rout, wsm, errup, errlo, mnum)) break;
 #pragma unroll
     for (int d = 16; d >= 1; d >>= 1) {
       errup += __shfl_down_sync(0xffffffffu, errup, d);
