@@ -126,6 +126,30 @@ long long b2dev_launch_count(b2dev_ctx* ctx);
 int b2dev_trace_sweep(b2dev_ctx* ctx, int sweep);
 int b2dev_get_trace(b2dev_ctx* ctx, double* out);
 
+/* Contact-graph colouring that allocates nothing. No counterpart in the
+ * reference (it sweeps rows in list order and never colours them).
+ *
+ * For callers that must not allocate device memory: code running while a
+ * CUDA stream is being captured into a graph, solvers embedded in a host
+ * application whose device memory is owned by its own allocator or memory
+ * pool, and real-time loops where cudaMalloc/cudaFree would synchronise the
+ * device. It runs the same Jones-Plassmann kernel as b2dev_assemble /
+ * b2dev_upload_locdyn, on the given stream, and gives the same colours for
+ * the same seed; its scratch is a fixed array inside the library (one flag per
+ * row plus a control block, at most 1,048,576 rows, about 4 MB held on every
+ * GPU that loads the library until the process exits).
+ *
+ * Device pointers: adjptr[n+1], adjcol[adjptr[n]] (the graph, as in
+ * b2dev_upload_locdyn), colour[n] (output), info[4] (output, may be NULL:
+ * timeout flag, colour-overflow flag, number of colours, rounds). n above the
+ * maximum is rejected with B2DEV_EINVAL before anything is queued.
+ * The first call on a device looks up the array's device address and the
+ * kernel's residency; make that first call before any stream capture. Every
+ * call shares the one array, so calls whose work overlaps on the GPU (other
+ * streams, other threads) race: queue them on one stream or serialise them. */
+int b2dev_colour_noalloc(int device, void* stream, int n, const int* adjptr, const int* adjcol, uint64_t seed,
+                         int* colour, int* info);
+
 /* One diagonal block solve (dbs.c:492-550 with the FAILURE_CONTINUE fallback
  * chain of bgs.c:976-1003) per caller-given row, on the device: W[9], B[3]
  * (the local free velocity B' including the off-diagonal sum), V[3], rho,

@@ -12,6 +12,7 @@
 #include <cfloat>
 #include <vector>
 #include <algorithm>
+#include <mutex>
 
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
@@ -905,6 +906,28 @@ float b2dev_last_assemble_ms(b2dev_ctx* c) { return c ? c->assemble_ms : 0.f; }
 
 long long b2dev_launch_count(b2dev_ctx* c) { return c ? c->launches : 0; }
 
+// ---- contact-graph colouring for callers that cannot allocate device memory
+//
+// b2dev_colour_noalloc runs the same Jones-Plassmann kernel as the context
+// path, but its scratch (the control block and one selection flag per row)
+// lives in this file-scope device array instead of memory obtained with
+// cudaMalloc. Every GPU that loads the library keeps the array until exit.
+constexpr int kNoAllocMaxRows = 1 << 20;  // rows of the largest graph the entry point accepts
+constexpr size_t kNoAllocCtrlBytes = 256;  // control block, padded
+static __device__ __align__(256) unsigned char g_colour_scratch[kNoAllocCtrlBytes + sizeof(int) * kNoAllocMaxRows];
+static_assert(sizeof(ColourControl) <= kNoAllocCtrlBytes, "colour control block must fit its slot");
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocSetup {
+  bool ready = false;
+  unsigned char* scratch = nullptr;  // device address of g_colour_scratch on this device
+  int grid = 0;                      // co-resident blocks of the colouring kernel
+};
+NoAllocSetup g_noalloc[kNoAllocMaxDevices];
+std::mutex g_noalloc_mutex;
+}  // namespace
+
 int b2dev_trace_sweep(b2dev_ctx* c, int sweep) {
   if (!c) return B2DEV_EINVAL;
   c->trace_sweep = sweep;
@@ -923,6 +946,60 @@ int b2dev_get_trace(b2dev_ctx* c, double* out) {
   }
   for (int p = 0; p < n; p++)
     memcpy(out + (size_t)kTraceStride * perm[p], tmp.data() + (size_t)kTraceStride * p, sizeof(double) * kTraceStride);
+  return B2DEV_OK;
+}
+
+int b2dev_colour_noalloc(int device, void* stream, int n, const int* adjptr, const int* adjcol, uint64_t seed,
+                         int* colour, int* info) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev || device >= kNoAllocMaxDevices) {
+    set_err("colour_noalloc: no CUDA device %d", device);
+    return B2DEV_EINVAL;
+  }
+  if (n < 0 || n > kNoAllocMaxRows) {
+    set_err("colour_noalloc: %d rows exceed the fixed scratch of %d rows this entry point holds", n, kNoAllocMaxRows);
+    return B2DEV_EINVAL;
+  }
+  if (n > 0 && (!adjptr || !adjcol || !colour)) {
+    set_err("colour_noalloc: null graph or output pointer");
+    return B2DEV_EINVAL;
+  }
+  DeviceGuard g(device);
+  cudaStream_t st = (cudaStream_t)stream;
+  NoAllocSetup& su = g_noalloc[device];
+  {  // set-up, once per device, with the device current
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!su.ready) {
+      void* addr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&addr, g_colour_scratch);
+      if (e != cudaSuccess) {
+        set_err("colour_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        return B2DEV_ECUDA;
+      }
+      int sms = 0, per_sm = 0;
+      B2_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+      B2_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_jp_colour, 256, 0));
+      if (per_sm < 1) { set_err("colour_noalloc: colouring kernel cannot be resident"); return B2DEV_ECUDA; }
+      su.scratch = static_cast<unsigned char*>(addr);
+      su.grid = per_sm * sms;
+      su.ready = true;
+    }
+  }
+  ColourControl* ctl = reinterpret_cast<ColourControl*>(su.scratch);
+  int* sel = reinterpret_cast<int*>(su.scratch + kNoAllocCtrlBytes);
+  // the control block starts at zero and every row uncoloured; the selection
+  // flags are written before they are read, so the previous call's values are harmless
+  B2_CK(cudaMemsetAsync(ctl, 0, sizeof(ColourControl), st));
+  if (n > 0) {
+    B2_CK(cudaMemsetAsync(colour, 0xff, sizeof(int) * n, st));
+    int nn = n;
+    unsigned long long sd = seed;
+    void* args[] = {&nn, (void*)&adjptr, (void*)&adjcol, &sd, &colour, &sel, &ctl};
+    const int grid = std::max(1, std::min(su.grid, blocks_for(n, 256)));
+    B2_CK(cudaLaunchCooperativeKernel((const void*)k_jp_colour, grid, 256, args, 0, st));
+  }
+  if (info)  // timeout flag, overflow flag, number of colours, rounds
+    B2_CK(cudaMemcpyAsync(info, &ctl->timeout, 4 * sizeof(int), cudaMemcpyDeviceToDevice, st));
   return B2DEV_OK;
 }
 

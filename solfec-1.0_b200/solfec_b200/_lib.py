@@ -74,6 +74,8 @@ _SIGNATURES = {
     'b2dev_get_locdyn': (C.c_int, [C.c_void_p] + [C.c_void_p] * 8 + [C.POINTER(C.c_double)]),
     'b2dev_last_assemble_ms': (C.c_float, [C.c_void_p]),
     'b2dev_launch_count': (C.c_longlong, [C.c_void_p]),
+    'b2dev_colour_noalloc': (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                                       C.c_void_p]),
     'b2dev_trace_sweep': (C.c_int, [C.c_void_p, C.c_int]),
     'b2dev_get_trace': (C.c_int, [C.c_void_p, C.c_void_p]),
     'b2dev_diag_solve_batch': (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
