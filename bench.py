@@ -55,6 +55,23 @@ def _dist():
     return ws, rank, local
 
 
+def replica_seed(rank: int) -> int:
+    """Scene seed of a rank's replica (independent scenes, no exchange step)."""
+    return 3 + rank
+
+
+def max_over_ranks(value: float, device=None) -> float:
+    """Per-step time of the slowest rank (all ranks take this collective in
+    the same order); identity without a process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
@@ -122,7 +139,7 @@ def make_step_inputs(rank):
     The previous step is solved once (FP64, untimed) and the bodies advanced
     by one velocity step with its reactions."""
     from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN, scenes
-    sc0 = scenes.hexahedra_lattice(seed=3 + rank, **SCENE)
+    sc0 = scenes.hexahedra_lattice(seed=replica_seed(rank), **SCENE)
     ldy = LOCDYN()
     ldy.update_begin(sc0)
     gs = GAUSS_SEIDEL_SOLVER(**SOLVE)
@@ -202,12 +219,8 @@ def bench_product(args, ws, rank, local):
             reps.append(gs.report)
         ev1.record(stream)
         barrier()
-        ms = ev0.elapsed_time(ev1) / steps
+        ms = max_over_ranks(ev0.elapsed_time(ev1) / steps, dev)
         launches = lib().b2dev_launch_count(ctx) - l0
-        if ws > 1:
-            t = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
         return ms, reps, launches
 
     results = {}
