@@ -42,7 +42,7 @@
 
 namespace b2 {
 
-constexpr int kSolveThreads = 256;
+constexpr int kSolveThreads = 64;
 constexpr int kSolveWarps = kSolveThreads / kWarp;
 constexpr int kChunkUnroll = 4;                      // 32-block chunks whose loads are issued together
 constexpr int kTileHeader = 256;                     // bytes of per-warp shared memory before the staging
