@@ -161,6 +161,54 @@ int b2dev_diag_solve_batch(b2dev_ctx* ctx, int n, int diagsolver, int failure, d
                            const double* rho, const double* gap, const double* friction, const double* restitution,
                            const double* cohesion, double* U, double* R, int* kind);
 
+/* ---- learned warm start --------------------------------------------------
+ *
+ * No counterpart in the reference, which starts each solve from the reactions
+ * of the previous step (con->R, zero for new contacts: mem.c:64-86). A small
+ * network (BF16 MLP 32 -> 128 -> 128 -> 16, GELU, FP32 accumulation; 25
+ * per-contact features plus a constant input, 3 outputs used) predicts the
+ * change of each contact's reaction from local quantities; the plain start
+ * remains the fallback, chosen by the merit function (mrf.c:35-185).
+ * Training and inference run on sm_100a tensor cores (tcgen05.mma with TMEM
+ * accumulators). Parameter vector (FP32, b2dev_mlp_nparams() values):
+ * W1[128][32] (column 25 = bias of layer 1), W2[128][128], b2[128],
+ * W3[16][128] (rows 3..15 zero), b3[16]. */
+typedef struct b2dev_mlp b2dev_mlp;
+
+typedef struct b2dev_nn_report {
+  double merit_nn;     /* merit of the network's initial reactions */
+  double merit_plain;  /* merit of the reactions held before (previous step) */
+  int used_nn;         /* 1: the network's reactions became the initial iterate */
+  float ms;            /* device time: features, network, the two merit passes */
+} b2dev_nn_report;
+
+int b2dev_mlp_nparams(void);
+/* stream NULL: the network gets its own stream */
+int b2dev_mlp_create(int device, void* stream, b2dev_mlp** out);
+void b2dev_mlp_destroy(b2dev_mlp* net);
+/* host arrays of b2dev_mlp_nparams() floats; set also clears the Adam moments */
+int b2dev_mlp_set_params(b2dev_mlp* net, const float* params);
+int b2dev_mlp_get_params(b2dev_mlp* net, float* params);
+/* Mean-squared loss over the 3 outputs and its gradient with respect to every
+ * parameter, over all nrows samples (device arrays feat[nrows][32],
+ * target[nrows][3]); grad (host, nparams) and loss (host) out. */
+int b2dev_mlp_grad(b2dev_mlp* net, int nrows, const float* feat, const float* target, float* grad, double* loss);
+/* Adam (beta 0.9/0.999, eps 1e-8) over `epochs` passes of minibatches of
+ * batch_tiles x 128 samples in a seeded random order; epoch_loss (host,
+ * `epochs` values, may be NULL) = mean loss per sample of each epoch. */
+int b2dev_mlp_train(b2dev_mlp* net, int nrows, const float* feat, const float* target, int epochs, int batch_tiles,
+                    double lr, uint64_t seed, double* epoch_loss);
+/* network outputs out[nrows][3] for features feat[nrows][32] (device arrays) */
+int b2dev_mlp_forward(b2dev_mlp* net, int nrows, const float* feat, float* out);
+/* Features of every row of the context's problem with its current reactions
+ * as the previous-step reactions, in caller order (device arrays):
+ * feat[n][32], scale[n] (= rho v_s: the prediction is R_prev + scale y) and
+ * rprev[n][3]. Used to build training sets. */
+int b2dev_nn_features(b2dev_ctx* ctx, float* feat, double* scale, double* rprev);
+/* Replace the context's initial reactions by the network's prediction when
+ * its merit is lower than that of the reactions held; U is left as it is. */
+int b2dev_nn_warm_start(b2dev_ctx* ctx, b2dev_mlp* net, b2dev_nn_report* rep);
+
 #ifdef __cplusplus
 }
 #endif

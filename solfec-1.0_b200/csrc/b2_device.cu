@@ -1043,3 +1043,5 @@ int b2dev_diag_solve_batch(b2dev_ctx* c, int n, int solver, int failure, double 
 }
 
 }  // extern "C"
+
+#include "b2_learn.cuh"

@@ -80,6 +80,17 @@ _SIGNATURES = {
     'b2dev_get_trace': (C.c_int, [C.c_void_p, C.c_void_p]),
     'b2dev_diag_solve_batch': (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
                                          C.c_double] + [C.c_void_p] * 11),
+    'b2dev_mlp_nparams': (C.c_int, []),
+    'b2dev_mlp_create': (C.c_int, [C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    'b2dev_mlp_destroy': (None, [C.c_void_p]),
+    'b2dev_mlp_set_params': (C.c_int, [C.c_void_p, C.c_void_p]),
+    'b2dev_mlp_get_params': (C.c_int, [C.c_void_p, C.c_void_p]),
+    'b2dev_mlp_grad': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
+    'b2dev_mlp_train': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double,
+                                  C.c_uint64, C.c_void_p]),
+    'b2dev_mlp_forward': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    'b2dev_nn_features': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    'b2dev_nn_warm_start': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     # include/solfec_b200.h
     'b2gs_create': (C.c_void_p, [C.c_double, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int,
                                  C.c_void_p, CALLBACK]),

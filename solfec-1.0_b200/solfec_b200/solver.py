@@ -62,6 +62,7 @@ class LOCDYN:
         self._h = L.b2gs_locdyn_create(int(device), stream)
         if not self._h:
             raise DeviceError('b2gs_locdyn_create: %s' % last_error())
+        self.device = int(device)
         self._keep = []
 
     def close(self):
