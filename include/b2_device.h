@@ -45,6 +45,7 @@ typedef struct b2dev_solve_opts {
   int maxiter, diagmaxiter, diagsolver, failure, reverse, nomerit;
   int precision;   /* b2dev_precision; MIXED = FP32 off-diagonal sweeps + closing FP64 refinement */
   int grid;        /* persistent grid size in blocks; 0 = chosen from occupancy and size */
+  int stage_blocks; /* off-diagonal blocks staged per warp window; 0 = the largest tile if it fits */
 } b2dev_solve_opts;
 
 /* Outcome of one solve. Histories are written to caller buffers of maxiter. */

@@ -274,7 +274,7 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
 
   const long long K = c->K;
   c->kstride = ((K + 31) / 32) * 32;
-  B2_TRY(ensure(c->col, sizeof(int) * (K + 1)));
+  B2_TRY(ensure(c->col, sizeof(int) * (c->kstride + 32)));
   B2_TRY(ensure(c->W64, sizeof(double) * 9 * (c->kstride + 1)));
   B2_TRY(ensure(c->W32, sizeof(float) * 9 * (c->kstride + 1)));
   const int wpb = 8;
@@ -368,11 +368,20 @@ int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxite
   // enough warps for the tiles of about two sweeps in flight, capped by residency
   const int want = grid_req > 0 ? grid_req : blocks_for(2LL * c->ntiles, kSolveWarps);
   int grid = 0;
-  // staging for the largest tile, within the shared memory of one block
-  const int max_smem = 200 * 1024;
-  const size_t per_word = mixed ? sizeof(float) : sizeof(double);
-  const int gfit = (int)((max_smem / kSolveWarps - kTileHeader) / per_word / 3) - kWarp * kChunkUnroll;
-  int gcap = std::max(kWarp, std::min(((c->max_tile_blocks + kWarp - 1) / kWarp) * kWarp, (gfit / kWarp) * kWarp));
+  // staging window: the largest tile (plus alignment slack) if the shared
+  // memory of the blocks that registers allow per SM holds it, else windows
+  int per_sm_regs = 0;
+  B2_CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
+  B2_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_regs, fn, kSolveThreads, 0));
+  per_sm_regs = std::max(1, per_sm_regs);
+  const int smem_sm = 227 * 1024 - per_sm_regs * 1024;  // per-block reserve of the runtime
+  const size_t per_block = mixed ? solve_smem_per_block<true>() : solve_smem_per_block<false>();
+  const size_t fixed = mixed ? solve_smem_fixed<true>() : solve_smem_fixed<false>();
+  const size_t per_warp = (size_t)smem_sm / per_sm_regs / kSolveWarps;
+  const int gfit = per_warp > fixed + 64 * per_block ? (int)((per_warp - fixed) / per_block) & ~3 : 64;
+  const int gwant = ((c->max_tile_blocks + 8) + 3) & ~3;
+  int gcap = std::max(64, std::min(gwant, gfit));
+  if (o->stage_blocks > 0) gcap = std::max(64, std::min(gcap, o->stage_blocks & ~3));
   const size_t wsm = mixed ? solve_warp_smem<true>(gcap) : solve_warp_smem<false>(gcap);
   const size_t smem = wsm * kSolveWarps;
   B2_TRY(cooperative_grid(fn, kSolveThreads, c->sms, want, &grid, smem));

@@ -194,6 +194,11 @@ template <bool MIXED>
 __host__ __device__ constexpr size_t solve_warp_smem(int gcap) {
   return (size_t)kTileHeader + (size_t)(3 * kWarp * kChunkUnroll + 3 * gcap) * (MIXED ? sizeof(float) : sizeof(double));
 }
+// shared memory of a warp: fixed part and bytes per staged block
+template <bool MIXED>
+__host__ __device__ constexpr size_t solve_smem_fixed() { return solve_warp_smem<MIXED>(0); }
+template <bool MIXED>
+__host__ __device__ constexpr size_t solve_smem_per_block() { return 3 * (MIXED ? sizeof(float) : sizeof(double)); }
 
 // One tile of up to 32 consecutive rows of one colour, owned by one warp.
 //

@@ -33,7 +33,7 @@ struct b2gs_solver
   int maxiter, diagmaxiter, diagsolver, failure;
   void *data;
   b2gs_callback callback;
-  int error, iters, reverse, variant, nomerit, precision, grid;
+  int error, iters, reverse, variant, nomerit, precision, grid, stage_blocks;
   int *itershist, itershistcount, itershistsize;
   double *rerhist, *merhist;
   int iters_mixed;
@@ -117,6 +117,7 @@ int b2gs_solve (b2gs_solver *gs, b2gs_locdyn *ldy)
   o.nomerit = nomerit;
   o.precision = gs->precision;
   o.grid = gs->grid;
+  o.stage_blocks = gs->stage_blocks;
 
   free (gs->rerhist);
   free (gs->merhist);
@@ -257,6 +258,7 @@ void b2gs_set_params (b2gs_solver *gs, double epsilon, int maxiter, double merit
 }
 void b2gs_set_precision (b2gs_solver *gs, int precision) { gs->precision = precision == B2GS_MIXED ? B2GS_MIXED : B2GS_FP64; }
 void b2gs_set_grid (b2gs_solver *gs, int blocks) { gs->grid = blocks > 0 ? blocks : 0; }
+void b2gs_set_stage_blocks (b2gs_solver *gs, int blocks) { gs->stage_blocks = blocks > 0 ? blocks : 0; }
 int b2gs_get_iters_mixed (b2gs_solver *gs) { return gs->iters_mixed; }
 double b2gs_get_solve_ms (b2gs_solver *gs) { return gs->solve_ms; }
 double b2gs_get_merit_input (b2gs_solver *gs) { return gs->merit_input; }

@@ -28,7 +28,8 @@ def build(force: bool = False) -> str:
 class b2dev_solve_opts(C.Structure):
     _fields_ = [('epsilon', C.c_double), ('meritval', C.c_double), ('diagepsilon', C.c_double),
                 ('maxiter', C.c_int), ('diagmaxiter', C.c_int), ('diagsolver', C.c_int), ('failure', C.c_int),
-                ('reverse', C.c_int), ('nomerit', C.c_int), ('precision', C.c_int), ('grid', C.c_int)]
+                ('reverse', C.c_int), ('nomerit', C.c_int), ('precision', C.c_int), ('grid', C.c_int),
+                ('stage_blocks', C.c_int)]
 
 
 class b2dev_solve_report(C.Structure):
@@ -114,6 +115,7 @@ _SIGNATURES = {
     'b2gs_set_params': (None, [C.c_void_p, C.c_double, C.c_int, C.c_double, C.c_double, C.c_int]),
     'b2gs_set_precision': (None, [C.c_void_p, C.c_int]),
     'b2gs_set_grid': (None, [C.c_void_p, C.c_int]),
+    'b2gs_set_stage_blocks': (None, [C.c_void_p, C.c_int]),
     'b2gs_get_iters_mixed': (C.c_int, [C.c_void_p]),
     'b2gs_get_solve_ms': (C.c_double, [C.c_void_p]),
     'b2gs_get_merit_input': (C.c_double, [C.c_void_p]),

@@ -358,6 +358,11 @@ class GAUSS_SEIDEL_SOLVER:
     def set_grid(self, blocks: int):
         lib().b2gs_set_grid(self._h, int(blocks))
 
+    def set_stage_blocks(self, blocks: int):
+        """Off-diagonal blocks staged per warp window (0: automatic); small values
+        force tiles to be processed in several windows."""
+        lib().b2gs_set_stage_blocks(self._h, int(blocks))
+
     @property
     def iters_mixed(self):
         return int(lib().b2gs_get_iters_mixed(self._h))

@@ -43,7 +43,7 @@ def same_bits(a, b):
     return a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))
 
 
-def gpu_solve(ld, R0=None, U0=None, precision='FP64', reverse=False, nomerit=False, **kw):
+def gpu_solve(ld, R0=None, U0=None, precision='FP64', reverse=False, nomerit=False, stage_blocks=0, **kw):
     ldy = LOCDYN()
     ldy.set_colour_seed(SEED)
     ldy.set(ld)
@@ -55,6 +55,8 @@ def gpu_solve(ld, R0=None, U0=None, precision='FP64', reverse=False, nomerit=Fal
         gs.reverse = 'ON'
     if nomerit:
         gs.nomerit = True
+    if stage_blocks:
+        gs.set_stage_blocks(stage_blocks)
     exc = None
     try:
         gs.solve(ldy)
@@ -112,6 +114,24 @@ def test_fp64_parity_nomerit_reverse(ld1k):
     assert g['gs'].iters == o['iters']
     assert same_bits(g['R'], o['R']) and same_bits(g['U'], o['U'])
     assert g['merit'] == 0.0
+
+
+@pytest.mark.parametrize('precision', ['FP64', 'MIXED'])
+def test_staging_windows_parity(ld1k, precision):
+    # a 64-block staging window splits every tile of the pile (up to ~270
+    # blocks) into several windows; the result must not change
+    kw = dict(epsilon=1e-4, maxiter=1000, meritval=1e-4)
+    g = gpu_solve(ld1k, precision=precision, stage_blocks=64, **kw)
+    h = gpu_solve(ld1k, precision=precision, **kw)
+    assert g['gs'].iters == h['gs'].iters
+    assert same_bits(g['R'], h['R']) and same_bits(g['U'], h['U'])
+    if precision == 'FP64':
+        o = oracle_in_order(ld1k, g['order'], **kw)
+        assert same_bits(g['R'], o['R']) and same_bits(g['U'], o['U'])
+    kw = dict(epsilon=1e-6, maxiter=300)
+    g = gpu_solve(ld1k, precision=precision, stage_blocks=64, reverse=True, **kw)
+    h = gpu_solve(ld1k, precision=precision, reverse=True, **kw)
+    assert g['gs'].iters == h['gs'].iters and same_bits(g['R'], h['R'])
 
 
 def test_warm_start_parity(ld1k, scene_cache):
