@@ -162,6 +162,50 @@ int b2dev_diag_solve_batch(b2dev_ctx* ctx, int n, int diagsolver, int failure, d
                            const double* rho, const double* gap, const double* friction, const double* restitution,
                            const double* cohesion, double* U, double* R, int* kind);
 
+/* ---- batches of independent problems --------------------------------------
+ *
+ * No counterpart in the reference (one GAUSS_SEIDEL_Solve per call,
+ * bgs.c:913). Many small scenes are solved by one persistent launch: the
+ * caller uploads the union of their bodies and contacts (contacts of problem k
+ * are caller rows row_offsets[k] .. row_offsets[k+1]-1 and touch only that
+ * problem's bodies), and every problem keeps its own stopping decision,
+ * merit, histories and failure bookkeeping, with the reference semantics
+ * (bgs.c:1028-1069). */
+typedef struct b2dev_batch_report {
+  int iters, thrown, last_fail_kind, nfailures;
+  double merit, error, merit_input;
+  double ms_to_decision;  /* device time from the launch's start to this problem's final decision */
+  int rows;               /* contacts of the problem */
+} b2dev_batch_report;
+
+/* Problems of the next b2dev_assemble (nprob = 1: one problem, offsets unused). */
+int b2dev_set_problems(b2dev_ctx* ctx, int nprob, const int* row_offsets);
+/* free energy of every problem (ldy.c:739), nprob doubles */
+int b2dev_problem_free_energy(b2dev_ctx* ctx, double* out);
+/* Rows per tile (1..32) of the current layout: smaller tiles give more
+ * parallel work to small problems; the autotuner chooses it. */
+int b2dev_set_tile_rows(b2dev_ctx* ctx, int rows);
+int b2dev_tile_rows(b2dev_ctx* ctx);
+/* Solve every problem (FP64 sweeps). use_graph: capture the launch sequence
+ * into a CUDA graph and replay it while its arguments are unchanged.
+ * reps[nprob]; rerhist/merhist NULL or nprob * opts->maxiter doubles;
+ * total (may be NULL): iterations and merit maxima, sweeps, device time. */
+int b2dev_solve_batch(b2dev_ctx* ctx, const b2dev_solve_opts* opts, b2dev_batch_report* reps, double* rerhist,
+                      double* merhist, b2dev_solve_report* total, int use_graph);
+
+/* Autotuner of the batched solve: one timed solve of the current problems per
+ * combination of rows per tile {32, 16, 8}, staging window {automatic, 128
+ * blocks} and persistent grid {full residency, 3/4, 1/2}, each from the
+ * current initial state (restored afterwards). The fastest rows per tile stay
+ * in the layout; pass grid and stage_blocks in the options of later solves. */
+typedef struct b2dev_tune_result {
+  int tile_rows, grid, stage_blocks, ntrials;
+  float ms;                                  /* device time of the fastest trial */
+  int trial_rows[32], trial_grid[32], trial_stage[32];
+  float trial_ms[32];
+} b2dev_tune_result;
+int b2dev_autotune_batch(b2dev_ctx* ctx, const b2dev_solve_opts* opts, b2dev_tune_result* res);
+
 /* ---- learned warm start --------------------------------------------------
  *
  * No counterpart in the reference, which starts each solve from the reactions

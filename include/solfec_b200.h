@@ -117,6 +117,8 @@ void b2gs_set_params (b2gs_solver *gs, double epsilon, int maxiter, double merit
 void b2gs_set_precision (b2gs_solver *gs, int precision);
 void b2gs_set_grid (b2gs_solver *gs, int blocks);      /* persistent grid size (0 = automatic) */
 void b2gs_set_stage_blocks (b2gs_solver *gs, int blocks); /* staging window per warp (0 = automatic) */
+/* device options of the next solve (b2dev_solve_opts of b2_device.h), e.g. for b2dev_solve_batch */
+int b2gs_get_opts (b2gs_solver *gs, struct b2dev_solve_opts *opts);
 int b2gs_get_iters_mixed (b2gs_solver *gs);           /* FP32 iterations of the last mixed solve */
 double b2gs_get_solve_ms (b2gs_solver *gs);           /* device time of the last solve */
 double b2gs_get_merit_input (b2gs_solver *gs);        /* merit of the reactions the last solve started from */

@@ -252,6 +252,32 @@ __global__ void k_sum_partials(const double* part, int n, double* out) {
   }
 }
 
+// Free energy of each problem of a batch (ldy.c:739 per problem): block k
+// sums 1/2 B^T A B over the caller rows off[k] .. off[k+1]-1.
+__global__ void k_problem_free_energy(const int* __restrict__ off, const double* __restrict__ Aii,
+                                      const double* __restrict__ Bc, double* __restrict__ out) {
+  __shared__ double red[32];
+  const int k = blockIdx.x;
+  double t = 0.0;
+  for (int i = off[k] + threadIdx.x; i < off[k + 1]; i += blockDim.x) {
+    const double* A = Aii + (size_t)9 * i;
+    const double* B = Bc + (size_t)3 * i;
+    const double Q0 = A[0] * B[0] + A[3] * B[1] + A[6] * B[2];
+    const double Q1 = A[1] * B[0] + A[4] * B[1] + A[7] * B[2];
+    const double Q2 = A[2] * B[0] + A[5] * B[1] + A[8] * B[2];
+    t += Q0 * B[0] + Q1 * B[1] + Q2 * B[2];
+  }
+#pragma unroll
+  for (int d = 16; d >= 1; d >>= 1) t += __shfl_down_sync(0xffffffffu, t, d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
+    out[k] = 0.5 * s;
+  }
+}
+
 // ---- contact graph (LOCDYN_Insert adjacency) ----
 
 __device__ __forceinline__ bool graph_body(const int* obstacle, int b) { return b >= 0 && !obstacle[b]; }

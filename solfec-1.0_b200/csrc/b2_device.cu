@@ -160,12 +160,22 @@ struct b2dev_ctx {
   Buf colour, sel, cctrl, keys_out, iota, perm, iperm, colptr, sdeg;
   Buf rowptr, col, W64, W32, Wd, Ad, Bv, Vv, rho, gap, fric, rest, coh;
   std::vector<int> colptr_h;
+  std::vector<int> rowptr_h;   // sorted CSR offsets (host copy, sizes the tiles)
+  std::vector<int> rprob_h;    // problem of each sorted row
 
   // state and solve scratch
-  Buf R64[3], R32[3], Us[2], Um[2], conmerit[2], done, decided, tilebase, part, rer, mer, failkey, failcount, sctrl, io,
+  Buf R64[3], R32[3], Us[2], Um[2], conmerit[2], done, decided, part, rer, mer, failkey, failcount, sctrl, io,
       cub_tmp, trace;
   int ntiles = 0;
-  int max_tile_blocks = 0;  // most off-diagonal blocks of one 32-row tile
+  int max_tile_blocks = 0;  // most off-diagonal blocks of one tile
+  int tile_rows = kWarp;    // rows per tile (at most one warp)
+
+  // independent problems solved together (one GAUSS_SEIDEL_Solve each); rows
+  // of problem k are caller rows prob_off[k] .. prob_off[k+1]-1
+  int nprob = 1;
+  std::vector<int> prob_off;
+  Buf tiles, tile_prob, ptile_ptr, ptile, row_prob, pctl, pfe, pvec;
+  std::vector<int> ptile_count;  // tiles per problem
   int trace_sweep = -1;  // sweep of the next solve whose diagonal solves are recorded
 
   int n = 0;
@@ -180,6 +190,12 @@ struct b2dev_ctx {
   cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   long long launches = 0;  // kernels of this library launched on this context
   float assemble_ms = 0.f;
+
+  // CUDA graph of the batched solve (rebuilt when its captured arguments change)
+  cudaGraphExec_t graph = nullptr;
+  std::vector<uintptr_t> graph_key;
+  void* pinned = nullptr;  // SolveControl + nprob ProblemControl written by the graph
+  size_t pinned_cap = 0;
 };
 
 namespace {
@@ -202,6 +218,54 @@ int cooperative_grid(const void* func, int threads, int sms, int want, int* grid
   }
   int cap = per_sm * sms;
   *grid = std::max(1, std::min(cap, want > 0 ? want : cap));
+  return B2DEV_OK;
+}
+
+// Tile table: runs of at most `rows` consecutive sorted rows of one colour and
+// one problem, numbered in forward colour order (problems ascending inside a
+// colour); per problem, its tiles in ascending order.
+int build_tiles(b2dev_ctx* c, int rows) {
+  cudaStream_t st = c->stream;
+  rows = std::max(1, std::min(kWarp, rows));
+  c->tile_rows = rows;
+  std::vector<int4> tl;
+  std::vector<int> tp;
+  int mx = 0;
+  for (int k = 0; k < c->ncolours; k++) {
+    const int cb = c->colptr_h[k], ce = c->colptr_h[k + 1];
+    for (int r = cb; r < ce;) {
+      const int pr = c->rprob_h[r];
+      int e = r + 1;
+      while (e < ce && e - r < rows && c->rprob_h[e] == pr) e++;
+      tl.push_back(make_int4(r, (e - r) | (pr << 6), cb, ce));  // rows | problem << 6
+      tp.push_back(pr);
+      mx = std::max(mx, c->rowptr_h[e] - c->rowptr_h[r]);
+      r = e;
+    }
+  }
+  const int T = (int)tl.size();
+  c->ntiles = T;
+  c->max_tile_blocks = mx;
+  std::vector<int> pptr(c->nprob + 1, 0), plist(std::max(T, 1));
+  for (int t = 0; t < T; t++) pptr[tp[t] + 1]++;
+  for (int k = 0; k < c->nprob; k++) pptr[k + 1] += pptr[k];
+  c->ptile_count.assign(c->nprob, 0);
+  for (int k = 0; k < c->nprob; k++) c->ptile_count[k] = pptr[k + 1] - pptr[k];
+  {
+    std::vector<int> cur(pptr.begin(), pptr.end() - 1);
+    for (int t = 0; t < T; t++) plist[cur[tp[t]]++] = t;
+  }
+  B2_TRY(ensure(c->tiles, sizeof(int4) * (T + 1)));
+  B2_TRY(ensure(c->tile_prob, sizeof(int) * (T + 1)));
+  B2_TRY(ensure(c->ptile_ptr, sizeof(int) * (c->nprob + 1)));
+  B2_TRY(ensure(c->ptile, sizeof(int) * (T + 1)));
+  if (T > 0) {
+    B2_CK(cudaMemcpyAsync(c->tiles.p, tl.data(), sizeof(int4) * T, cudaMemcpyHostToDevice, st));
+    B2_CK(cudaMemcpyAsync(c->tile_prob.p, tp.data(), sizeof(int) * T, cudaMemcpyHostToDevice, st));
+    B2_CK(cudaMemcpyAsync(c->ptile.p, plist.data(), sizeof(int) * T, cudaMemcpyHostToDevice, st));
+  }
+  B2_CK(cudaMemcpyAsync(c->ptile_ptr.p, pptr.data(), sizeof(int) * (c->nprob + 1), cudaMemcpyHostToDevice, st));
+  B2_CK(cudaStreamSynchronize(st));  // the host vectors above go out of scope
   return B2DEV_OK;
 }
 
@@ -318,24 +382,22 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
     B2_TRY(ensure(c->conmerit[b], sizeof(double) * (n + 1)));
   }
   B2_TRY(ensure(c->done, sizeof(int) * (n + 1)));
-  // tiles of 32 rows per colour, numbered in forward colour order
-  std::vector<int> tb(c->ncolours + 1, 0);
-  for (int k = 0; k < c->ncolours; k++) tb[k + 1] = tb[k] + (c->colptr_h[k + 1] - c->colptr_h[k] + kWarp - 1) / kWarp;
-  c->ntiles = tb[c->ncolours];
-  {  // largest number of blocks of one tile (sizes the per-warp staging)
-    std::vector<int> rp(n + 1);
-    B2_CK(cudaMemcpyAsync(rp.data(), c->rowptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, st));
+  {  // sorted CSR offsets and the problem of every sorted row, kept on the host for the tile table
+    c->rowptr_h.assign(n + 1, 0);
+    B2_CK(cudaMemcpyAsync(c->rowptr_h.data(), c->rowptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, st));
+    c->rprob_h.assign(n, 0);
+    if (c->nprob > 1 && n > 0) {
+      std::vector<int> perm(n);
+      B2_CK(cudaMemcpyAsync(perm.data(), c->perm.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+      B2_CK(cudaStreamSynchronize(st));
+      for (int q = 0; q < n; q++)
+        c->rprob_h[q] = (int)(std::upper_bound(c->prob_off.begin(), c->prob_off.end(), perm[q]) - c->prob_off.begin()) - 1;
+    }
     B2_CK(cudaStreamSynchronize(st));
-    int mx = 0;
-    for (int k = 0; k < c->ncolours; k++)
-      for (int r = c->colptr_h[k]; r < c->colptr_h[k + 1]; r += kWarp) {
-        const int e = std::min(r + kWarp, c->colptr_h[k + 1]);
-        mx = std::max(mx, rp[e] - rp[r]);
-      }
-    c->max_tile_blocks = mx;
+    B2_TRY(ensure(c->row_prob, sizeof(int) * (n + 1)));
+    if (n > 0) B2_CK(cudaMemcpyAsync(c->row_prob.p, c->rprob_h.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
   }
-  B2_TRY(ensure(c->tilebase, sizeof(int) * (c->ncolours + 2)));
-  B2_CK(cudaMemcpyAsync(c->tilebase.p, tb.data(), sizeof(int) * (c->ncolours + 1), cudaMemcpyHostToDevice, st));
+  B2_TRY(build_tiles(c, c->tile_rows));
   // new contacts start from R = U = 0 (MEM_Alloc zeroes, mem.c:64-86)
   B2_CK(cudaMemsetAsync(c->R64[0].p, 0, sizeof(double4) * (n + 1), st));
   B2_CK(cudaMemsetAsync(c->R32[0].p, 0, sizeof(float4) * (n + 1), st));
@@ -360,18 +422,43 @@ int upload(b2dev_ctx* c, Buf& b, const T* src, size_t count, int on_device) {
   return B2DEV_OK;
 }
 
-int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter, int iter0, int in,
-                 int u0_from_merit, int grid_req, SolveControl* out, float* kernel_ms, int* grid_used) {
+// Final iterate of every row into the state buffers R64[0], Us[0] and
+// conmerit[0] (the problems of a batch return different iterates). Each row is
+// read and written by one thread, so the copy may read its own destination.
+__global__ void k_state_gather(int n, const int* __restrict__ row_prob, const ProblemControl* __restrict__ pc, int in,
+                               int nomerit, double4* R0, double4* R1, double4* R2, double4* Us0, double4* Us1,
+                               double4* Um0, double4* Um1, double* cm0, double* cm1) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const ProblemControl& q = pc[row_prob[p]];
+  const int f = q.final_iter;
+  double4* Rb[3] = {R0, R1, R2};
+  const double4 r = Rb[(in + 1 + f) % 3][p];
+  double4 u;
+  double cm = 0.0;
+  if (nomerit) {
+    u = ((f + 1) & 1) ? Us1[p] : Us0[p];
+  } else {
+    const int ms = q.thrown ? f : f + 1;
+    u = (ms & 1) ? Um1[p] : Um0[p];
+    cm = (ms & 1) ? cm1[p] : cm0[p];
+  }
+  R0[p] = r;
+  Us0[p] = u;
+  if (!nomerit) cm0[p] = cm;
+}
+
+// Kernel arguments and launch shape of one persistent solve (nothing queued).
+int solve_setup(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter, int iter0, int in,
+                int u0_from_merit, int grid_req, SolveArgs* a, int* grid, size_t* smem) {
   const int n = c->n;
-  cudaStream_t st = c->stream;
+  const int P = c->nprob;
   const void* fn = mixed ? (const void*)k_solve<true> : (const void*)k_solve<false>;
   // enough warps for the tiles of about two sweeps in flight, capped by residency
   const int want = grid_req > 0 ? grid_req : blocks_for(2LL * c->ntiles, kSolveWarps);
-  int grid = 0;
-  // staging window: the largest tile (plus alignment slack) if the shared
-  // memory of the blocks that registers allow per SM holds it, else windows
+  // staging window: the largest tile if the shared memory of the blocks that
+  // registers allow per SM holds it, else windows
   int per_sm_regs = 0;
-  B2_CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
   B2_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_regs, fn, kSolveThreads, 0));
   per_sm_regs = std::max(1, per_sm_regs);
   const int smem_sm = 227 * 1024 - per_sm_regs * 1024;  // per-block reserve of the runtime
@@ -383,100 +470,164 @@ int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxite
   int gcap = std::max(64, std::min(gwant, gfit));
   if (o->stage_blocks > 0) gcap = std::max(64, std::min(gcap, o->stage_blocks & ~3));
   const size_t wsm = mixed ? solve_warp_smem<true>(gcap) : solve_warp_smem<false>(gcap);
-  const size_t smem = wsm * kSolveWarps;
-  B2_TRY(cooperative_grid(fn, kSolveThreads, c->sms, want, &grid, smem));
+  *smem = wsm * kSolveWarps;
+  B2_TRY(cooperative_grid(fn, kSolveThreads, c->sms, want, grid, *smem));
+  const int pstride = o->maxiter + 2;
   B2_TRY(ensure(c->part, sizeof(double) * (3 * 4 * (size_t)c->ntiles + 4)));
-  B2_TRY(ensure(c->decided, sizeof(int) * (maxiter + 2)));
-  B2_CK(cudaMemsetAsync(c->sctrl.p, 0, sizeof(SolveControl), st));
-  B2_CK(cudaMemsetAsync(c->done.p, 0, sizeof(int) * (n + 1), st));
-  B2_CK(cudaMemsetAsync(c->decided.p, 0, sizeof(int) * (maxiter + 2), st));
-  if (!u0_from_merit && c->state_u != &c->Us[0])  // the first sweep reads its U from Us[0]
-    B2_CK(cudaMemcpyAsync(c->Us[0].p, c->state_u->p, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st));
-  B2_CK(cudaMemsetAsync(ptr<unsigned long long>(c->failkey) + iter0, 0, sizeof(unsigned long long) * (maxiter + 1), st));
-  B2_CK(cudaMemsetAsync(ptr<unsigned>(c->failcount) + iter0, 0, sizeof(unsigned) * (maxiter + 1), st));
+  B2_TRY(ensure(c->decided, sizeof(int) * (size_t)P * pstride));
+  B2_TRY(ensure(c->rer, sizeof(double) * (size_t)P * pstride));
+  B2_TRY(ensure(c->mer, sizeof(double) * (size_t)P * pstride));
+  B2_TRY(ensure(c->failkey, sizeof(unsigned long long) * (size_t)P * pstride));
+  B2_TRY(ensure(c->failcount, sizeof(unsigned) * (size_t)P * pstride));
+  B2_TRY(ensure(c->pctl, sizeof(ProblemControl) * P));
+  if (c->trace_sweep >= 0 && iter0 == 0) B2_TRY(ensure(c->trace, sizeof(double) * kTraceStride * (n + 1)));
 
-  SolveArgs a;
-  memset(&a, 0, sizeof a);
-  a.n = n;
-  a.ncolours = c->ncolours;
-  a.ntiles = c->ntiles;
-  a.tilebase = ptr<int>(c->tilebase);
-  a.done = ptr<int>(c->done);
-  a.decided = ptr<int>(c->decided);
-  a.colptr = ptr<int>(c->colptr);
-  a.rowptr = ptr<int>(c->rowptr);
-  a.col = ptr<int>(c->col);
-  a.W64 = ptr<double>(c->W64);
-  a.W32 = ptr<float>(c->W32);
-  a.kstride = c->kstride;
-  a.Wd = ptr<double>(c->Wd);
-  a.Ad = ptr<double>(c->Ad);
-  a.Bv = ptr<double>(c->Bv);
-  a.Vv = ptr<double>(c->Vv);
-  a.rho = ptr<double>(c->rho);
-  a.gap = ptr<double>(c->gap);
-  a.fric = ptr<double>(c->fric);
-  a.rest = ptr<double>(c->rest);
-  a.coh = ptr<double>(c->coh);
+  SolveArgs& A = *a;
+  memset(&A, 0, sizeof A);
+  A.n = n;
+  A.ntiles = c->ntiles;
+  A.nprob = P;
+  A.nactive = 0;
+  for (int k = 0; k < P; k++) A.nactive += c->ptile_count[k] > 0 ? 1 : 0;
+  A.tiles = ptr<int4>(c->tiles);
+  A.ptile_ptr = ptr<int>(c->ptile_ptr);
+  A.ptile = ptr<int>(c->ptile);
+  A.done = ptr<int>(c->done);
+  A.decided = ptr<int>(c->decided);
+  A.rowptr = ptr<int>(c->rowptr);
+  A.col = ptr<int>(c->col);
+  A.W64 = ptr<double>(c->W64);
+  A.W32 = ptr<float>(c->W32);
+  A.kstride = c->kstride;
+  A.Wd = ptr<double>(c->Wd);
+  A.Ad = ptr<double>(c->Ad);
+  A.Bv = ptr<double>(c->Bv);
+  A.Vv = ptr<double>(c->Vv);
+  A.rho = ptr<double>(c->rho);
+  A.gap = ptr<double>(c->gap);
+  A.fric = ptr<double>(c->fric);
+  A.rest = ptr<double>(c->rest);
+  A.coh = ptr<double>(c->coh);
   for (int b = 0; b < 3; b++) {
-    a.R64[b] = ptr<double4>(c->R64[b]);
-    a.R32[b] = ptr<float4>(c->R32[b]);
+    A.R64[b] = ptr<double4>(c->R64[b]);
+    A.R32[b] = ptr<float4>(c->R32[b]);
   }
   for (int b = 0; b < 2; b++) {
-    a.Us[b] = ptr<double4>(c->Us[b]);
-    a.Um[b] = ptr<double4>(c->Um[b]);
-    a.conmerit[b] = ptr<double>(c->conmerit[b]);
+    A.Us[b] = ptr<double4>(c->Us[b]);
+    A.Um[b] = ptr<double4>(c->Um[b]);
+    A.conmerit[b] = ptr<double>(c->conmerit[b]);
   }
-  a.part = ptr<double>(c->part);
-  a.rerhist = ptr<double>(c->rer);
-  a.merhist = ptr<double>(c->mer);
-  a.failkey = ptr<unsigned long long>(c->failkey);
-  a.failcount = ptr<unsigned>(c->failcount);
-  a.ctrl = ptr<SolveControl>(c->sctrl);
-  a.epsilon = o->epsilon;
-  a.meritval = o->meritval;
-  a.diagepsilon = o->diagepsilon;
-  a.step = c->step;
-  double lo = c->free_energy < DBL_EPSILON ? 1.0 : c->free_energy;  // mrf.c:45
-  a.merit_denom = lo == 0.0 ? 1.0 : lo;                             // mrf.c:177
-  a.maxiter = maxiter;
-  a.diagmaxiter = o->diagmaxiter;
-  a.diagsolver = o->diagsolver;
-  a.failure = o->failure;
-  a.dynamic = c->dynamic;
-  a.reverse = o->reverse;
-  a.nomerit = o->nomerit;
-  a.iter0 = iter0;
-  a.in = in;
-  a.u0_from_merit = u0_from_merit;
-  a.gcap = gcap;
-  a.warp_smem = (int)wsm;
+  A.part = ptr<double>(c->part);
+  A.rerhist = ptr<double>(c->rer);
+  A.merhist = ptr<double>(c->mer);
+  A.failkey = ptr<unsigned long long>(c->failkey);
+  A.failcount = ptr<unsigned>(c->failcount);
+  A.pstride = pstride;
+  A.free_energy = ptr<double>(c->pfe);
+  A.ctrl = ptr<SolveControl>(c->sctrl);
+  A.pctl = ptr<ProblemControl>(c->pctl);
+  A.epsilon = o->epsilon;
+  A.meritval = o->meritval;
+  A.diagepsilon = o->diagepsilon;
+  A.step = c->step;
+  A.maxiter = maxiter;
+  A.diagmaxiter = o->diagmaxiter;
+  A.diagsolver = o->diagsolver;
+  A.failure = o->failure;
+  A.dynamic = c->dynamic;
+  A.reverse = o->reverse;
+  A.nomerit = o->nomerit;
+  A.iter0 = iter0;
+  A.in = in;
+  A.u0_from_merit = u0_from_merit;
+  A.gcap = gcap;
+  A.warp_smem = (int)wsm;
   if (c->trace_sweep >= 0 && iter0 == 0) {
-    B2_TRY(ensure(c->trace, sizeof(double) * kTraceStride * (n + 1)));
-    B2_CK(cudaMemsetAsync(c->trace.p, 0, sizeof(double) * kTraceStride * (n + 1), st));
-    a.trace = ptr<double>(c->trace);
-    a.trace_sweep = c->trace_sweep;
+    A.trace = ptr<double>(c->trace);
+    A.trace_sweep = c->trace_sweep;
   }
-  void* args[] = {&a};
-  B2_CK(cudaEventRecord(c->ev[4], st));
+  return B2DEV_OK;
+}
+
+// Queue the control resets and the cooperative launch (no synchronisation,
+// so the sequence can be captured into a CUDA graph).
+int solve_enqueue(b2dev_ctx* c, bool mixed, const SolveArgs& a, int grid, size_t smem) {
+  cudaStream_t st = c->stream;
+  const int n = c->n, P = c->nprob;
+  B2_CK(cudaMemsetAsync(c->sctrl.p, 0, sizeof(SolveControl), st));
+  B2_CK(cudaMemsetAsync(c->pctl.p, 0, sizeof(ProblemControl) * P, st));
+  B2_CK(cudaMemsetAsync(c->done.p, 0, sizeof(int) * (n + 1), st));
+  B2_CK(cudaMemsetAsync(c->decided.p, 0, sizeof(int) * (size_t)P * a.pstride, st));
+  if (a.iter0 == 0) {
+    B2_CK(cudaMemsetAsync(c->failkey.p, 0, sizeof(unsigned long long) * (size_t)P * a.pstride, st));
+    B2_CK(cudaMemsetAsync(c->failcount.p, 0, sizeof(unsigned) * (size_t)P * a.pstride, st));
+  } else {  // a continuation launch (one problem): its own sweeps only
+    B2_CK(cudaMemsetAsync(ptr<unsigned long long>(c->failkey) + a.iter0, 0,
+                          sizeof(unsigned long long) * (a.pstride - a.iter0), st));
+    B2_CK(cudaMemsetAsync(ptr<unsigned>(c->failcount) + a.iter0, 0, sizeof(unsigned) * (a.pstride - a.iter0), st));
+  }
+  if (a.trace) B2_CK(cudaMemsetAsync(a.trace, 0, sizeof(double) * kTraceStride * (n + 1), st));
+  const void* fn = mixed ? (const void*)k_solve<true> : (const void*)k_solve<false>;
+  SolveArgs arg = a;
+  void* args[] = {&arg};
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof cfg);
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kSolveThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   c->launches++;
-  B2_CK(cudaLaunchCooperativeKernel(fn, grid, kSolveThreads, args, smem, st));
+  B2_CK(cudaLaunchKernelExC(&cfg, fn, args));
+  return B2DEV_OK;
+}
+
+// One persistent solve launch, synchronised: per-problem outcomes in pc.
+int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter, int iter0, int in,
+                 int u0_from_merit, int grid_req, SolveControl* g, std::vector<ProblemControl>& pc, float* kernel_ms,
+                 int* grid_used) {
+  cudaStream_t st = c->stream;
+  if (!u0_from_merit && c->state_u != &c->Us[0])  // the first sweep reads its U from Us[0]
+    B2_CK(cudaMemcpyAsync(c->Us[0].p, c->state_u->p, sizeof(double4) * c->n, cudaMemcpyDeviceToDevice, st));
+  SolveArgs a;
+  int grid = 0;
+  size_t smem = 0;
+  B2_TRY(solve_setup(c, mixed, o, maxiter, iter0, in, u0_from_merit, grid_req, &a, &grid, &smem));
+  B2_CK(cudaEventRecord(c->ev[4], st));
+  B2_TRY(solve_enqueue(c, mixed, a, grid, smem));
   B2_CK(cudaEventRecord(c->ev[5], st));
-  B2_CK(cudaMemcpyAsync(out, c->sctrl.p, sizeof(SolveControl), cudaMemcpyDeviceToHost, st));
+  pc.assign(c->nprob, ProblemControl());
+  B2_CK(cudaMemcpyAsync(g, c->sctrl.p, sizeof(SolveControl), cudaMemcpyDeviceToHost, st));
+  B2_CK(cudaMemcpyAsync(pc.data(), c->pctl.p, sizeof(ProblemControl) * c->nprob, cudaMemcpyDeviceToHost, st));
   B2_CK(cudaStreamSynchronize(st));
   if (kernel_ms) cudaEventElapsedTime(kernel_ms, c->ev[4], c->ev[5]);
   if (grid_used) *grid_used = grid;
-  if (out->timeout) { set_err("solve: a bounded device-side wait timed out"); return B2DEV_ETIMEOUT; }
-  // where the returned iterate's R, U and per-row merit live
-  const int f = out->final_iter;
-  c->state_r = (in + 1 + f) % 3;
-  if (o->nomerit) {
-    c->state_u = &c->Us[(f + 1) & 1];
-    c->state_cm = nullptr;
-  } else {
-    const int msweep = out->thrown ? f : f + 1;  // sweep that evaluated the merit of the returned iterate
-    c->state_u = &c->Um[msweep & 1];
-    c->state_cm = &c->conmerit[msweep & 1];
+  if (g->timeout) { set_err("solve: a bounded device-side wait timed out"); return B2DEV_ETIMEOUT; }
+  if (c->nprob == 1) {  // where the returned iterate's R, U and per-row merit live
+    const int f = pc[0].final_iter;
+    c->state_r = (in + 1 + f) % 3;
+    if (o->nomerit) {
+      c->state_u = &c->Us[(f + 1) & 1];
+      c->state_cm = nullptr;
+    } else {
+      const int msweep = pc[0].thrown ? f : f + 1;  // sweep that evaluated the merit of the returned iterate
+      c->state_u = &c->Um[msweep & 1];
+      c->state_cm = &c->conmerit[msweep & 1];
+    }
+  } else {  // every problem's final iterate into the canonical buffers
+    c->launches++;
+    k_state_gather<<<blocks_for(c->n, 256), 256, 0, st>>>(
+        c->n, ptr<int>(c->row_prob), ptr<ProblemControl>(c->pctl), in, o->nomerit, ptr<double4>(c->R64[0]),
+        ptr<double4>(c->R64[1]), ptr<double4>(c->R64[2]), ptr<double4>(c->Us[0]), ptr<double4>(c->Us[1]),
+        ptr<double4>(c->Um[0]), ptr<double4>(c->Um[1]), ptr<double>(c->conmerit[0]), ptr<double>(c->conmerit[1]));
+    B2_CK(cudaGetLastError());
+    c->state_r = 0;
+    c->state_u = &c->Us[0];
+    c->state_cm = o->nomerit ? nullptr : &c->conmerit[0];
   }
   return B2DEV_OK;
 }
@@ -534,11 +685,13 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->cctrl, &c->keys_out, &c->iota, &c->perm, &c->iperm, &c->colptr, &c->sdeg, &c->rowptr, &c->col,
                 &c->W64, &c->W32, &c->Wd, &c->Ad, &c->Bv, &c->Vv, &c->rho, &c->gap, &c->fric, &c->rest, &c->coh,
                 &c->R64[0], &c->R64[1], &c->R64[2], &c->R32[0], &c->R32[1], &c->R32[2], &c->Us[0], &c->Us[1],
-                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tilebase,
+                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec,
                 &c->part, &c->rer,
                 &c->mer, &c->failkey, &c->failcount, &c->sctrl, &c->io, &c->cub_tmp, &c->trace};
   for (Buf* b : all)
     if (b->p) cudaFree(b->p);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->pinned) cudaFreeHost(c->pinned);
   for (int k = 0; k < 8; k++)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   if (c->own_stream) cudaStreamDestroy(c->stream);
@@ -584,6 +737,10 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
   cudaStream_t st = c->stream;
   const int T = 256;
   const int n = c->ncon, nb = c->nbod;
+  if (c->nprob > 1 && ((int)c->prob_off.size() != c->nprob + 1 || c->prob_off.back() != n)) {
+    set_err("assemble: the problem offsets do not cover the %d contacts", n);
+    return B2DEV_EINVAL;
+  }
   c->n = n;
   c->step = step;
   c->dynamic = dynamic ? 1 : 0;
@@ -612,6 +769,16 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
                                   ptr<double>(c->fe_part), ptr<int>(c->bad));
   c->launches++;
   k_sum_partials<<<1, 1024, 0, st>>>(ptr<double>(c->fe_part), rb, ptr<double>(c->fe_dev));
+  B2_TRY(ensure(c->pfe, sizeof(double) * (c->nprob + 1)));
+  if (c->nprob == 1) {
+    B2_CK(cudaMemcpyAsync(c->pfe.p, c->fe_dev.p, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  } else {  // free energy of every problem (rows of each problem in caller order)
+    B2_TRY(ensure(c->pvec, sizeof(int) * (c->nprob + 1)));
+    B2_CK(cudaMemcpyAsync(c->pvec.p, c->prob_off.data(), sizeof(int) * (c->nprob + 1), cudaMemcpyHostToDevice, st));
+    c->launches++;
+    k_problem_free_energy<<<c->nprob, 256, 0, st>>>(ptr<int>(c->pvec), ptr<double>(c->Aii), ptr<double>(c->B_c),
+                                                    ptr<double>(c->pfe));
+  }
   {  // body indices are checked before any kernel indexes per-body arrays with them
     int bad0 = 0;
     B2_CK(cudaMemcpyAsync(&bad0, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -685,6 +852,8 @@ int b2dev_upload_locdyn(b2dev_ctx* c, int n, const double* W, const double* A, c
   c->step = step;
   c->dynamic = dynamic ? 1 : 0;
   c->free_energy = free_energy;
+  B2_TRY(ensure(c->pfe, sizeof(double) * 2));
+  B2_CK(cudaMemcpyAsync(c->pfe.p, &c->free_energy, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   c->assembled_mode = false;
   B2_TRY(upload(c, c->Wii, W, (size_t)9 * n, on_device));
   B2_TRY(upload(c, c->Aii, A, (size_t)9 * n, on_device));
@@ -778,15 +947,13 @@ int b2dev_solve(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_solve_report* rep
   cudaStream_t st = c->stream;
   memset(rep, 0, sizeof *rep);
   const int maxiter = o->maxiter;
-  B2_TRY(ensure(c->rer, sizeof(double) * (maxiter + 2)));
-  B2_TRY(ensure(c->mer, sizeof(double) * (maxiter + 2)));
-  B2_TRY(ensure(c->failkey, sizeof(unsigned long long) * (maxiter + 2)));
-  B2_TRY(ensure(c->failcount, sizeof(unsigned) * (maxiter + 2)));
   B2_CK(cudaEventRecord(c->ev[2], st));
 
-  SolveControl s1, s2;
-  memset(&s1, 0, sizeof s1);
-  memset(&s2, 0, sizeof s2);
+  if (c->nprob != 1) { set_err("solve: the context holds %d problems (use b2dev_solve_batch)", c->nprob); return B2DEV_ESTATE; }
+  SolveControl g1, g2;
+  memset(&g1, 0, sizeof g1);
+  memset(&g2, 0, sizeof g2);
+  std::vector<ProblemControl> q1, q2;
   if (c->n == 0) {  // no rows: one iteration with zero error and merit, as the reference loop does
     rep->iters = 1;
     B2_CK(cudaEventRecord(c->ev[3], st));
@@ -803,8 +970,9 @@ int b2dev_solve(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_solve_report* rep
     c->launches++;
     k_shadow<<<blocks_for(c->n, 256), 256, 0, st>>>(c->n, ptr<double4>(c->R64[c->state_r]),
                                                     ptr<float4>(c->R32[c->state_r]));
-    B2_TRY(solve_launch(c, true, o, maxiter - 1, 0, c->state_r, 0, o->grid, &s1, &rep->ms_kernel[0], &rep->grid));
-    rep->sweeps_launch[0] = s1.sweeps;
+    B2_TRY(solve_launch(c, true, o, maxiter - 1, 0, c->state_r, 0, o->grid, &g1, q1, &rep->ms_kernel[0], &rep->grid));
+    const ProblemControl& s1 = q1[0];
+    rep->sweeps_launch[0] = g1.sweeps;
     rep->merit_input = s1.merit_input;
     iters = s1.iters;
     thrown = s1.thrown != 0;
@@ -812,28 +980,30 @@ int b2dev_solve(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_solve_report* rep
     merit = s1.merit;
     error = s1.error;
     rep->iters_mixed = iters;
-    rep->sweeps = s1.sweeps;
+    rep->sweeps = g1.sweeps;
     if (!thrown) {  // closing FP64 refinement, continuing the iteration count
-      B2_TRY(solve_launch(c, false, o, maxiter - iters, iters, c->state_r, o->nomerit ? 0 : 1, o->grid, &s2,
+      B2_TRY(solve_launch(c, false, o, maxiter - iters, iters, c->state_r, o->nomerit ? 0 : 1, o->grid, &g2, q2,
                           &rep->ms_kernel[1], &rep->grid));
-      rep->sweeps_launch[1] = s2.sweeps;
+      const ProblemControl& s2 = q2[0];
+      rep->sweeps_launch[1] = g2.sweeps;
       ranges.push_back({iters, iters + s2.final_iter});
       iters += s2.iters;
       thrown = s2.thrown != 0;
       merit = s2.merit;
       error = s2.error;
-      rep->sweeps += s2.sweeps;
+      rep->sweeps += g2.sweeps;
     }
   } else {
-    B2_TRY(solve_launch(c, false, o, maxiter, 0, c->state_r, 0, o->grid, &s1, &rep->ms_kernel[0], &rep->grid));
-    rep->sweeps_launch[0] = s1.sweeps;
+    B2_TRY(solve_launch(c, false, o, maxiter, 0, c->state_r, 0, o->grid, &g1, q1, &rep->ms_kernel[0], &rep->grid));
+    const ProblemControl& s1 = q1[0];
+    rep->sweeps_launch[0] = g1.sweeps;
     rep->merit_input = s1.merit_input;
     iters = s1.iters;
     thrown = s1.thrown != 0;
     ranges.push_back({0, s1.final_iter});
     merit = s1.merit;
     error = s1.error;
-    rep->sweeps = s1.sweeps;
+    rep->sweeps = g1.sweeps;
   }
   B2_CK(cudaEventRecord(c->ev[3], st));
   final_global = iters;
@@ -860,6 +1030,267 @@ int b2dev_solve(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_solve_report* rep
   rep->merit = o->nomerit ? 0.0 : merit;
   rep->error = error;
   return B2DEV_OK;
+}
+
+
+// ---- batches of independent problems ------------------------------------------
+
+int b2dev_set_problems(b2dev_ctx* c, int nprob, const int* row_offsets) {
+  if (!c || nprob < 1 || (nprob > 1 && !row_offsets)) { set_err("set_problems: invalid arguments"); return B2DEV_EINVAL; }
+  std::vector<int> off(nprob + 1, 0);
+  if (nprob > 1) {
+    for (int k = 0; k <= nprob; k++) off[k] = row_offsets[k];
+    if (off[0] != 0) { set_err("set_problems: offsets must start at 0"); return B2DEV_EINVAL; }
+    for (int k = 0; k < nprob; k++)
+      if (off[k + 1] < off[k]) { set_err("set_problems: offsets must not decrease"); return B2DEV_EINVAL; }
+  }
+  c->nprob = nprob;
+  c->prob_off = nprob > 1 ? off : std::vector<int>();
+  c->ready = false;  // the next assembly lays the problems out
+  return B2DEV_OK;
+}
+
+int b2dev_problem_free_energy(b2dev_ctx* c, double* out) {
+  if (!c || !c->ready || !out) { set_err("problem_free_energy: no local dynamics"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  B2_CK(cudaMemcpy(out, c->pfe.p, sizeof(double) * c->nprob, cudaMemcpyDeviceToHost));
+  return B2DEV_OK;
+}
+
+int b2dev_set_tile_rows(b2dev_ctx* c, int rows) {
+  if (!c || !c->ready || rows < 1 || rows > kWarp) { set_err("set_tile_rows: invalid arguments or no layout"); return B2DEV_EINVAL; }
+  DeviceGuard g(c->device);
+  return build_tiles(c, rows);
+}
+
+int b2dev_tile_rows(b2dev_ctx* c) { return c ? c->tile_rows : 0; }
+
+// Batched solve: one persistent launch over every problem of the context, each
+// an independent GAUSS_SEIDEL_Solve with its own stopping decision (FP64
+// sweeps). With use_graph the launch sequence (control resets, the
+// cooperative solve kernel, the gather of final iterates and the copy of the
+// outcomes) is captured once into a CUDA graph and replayed while its
+// arguments are unchanged. reps: nprob entries; rerhist/merhist: NULL or
+// nprob * opts->maxiter doubles; total: aggregate (may be NULL).
+int b2dev_solve_batch(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_batch_report* reps, double* rerhist,
+                      double* merhist, b2dev_solve_report* total, int use_graph) {
+  if (!c || !o || !reps) { set_err("solve_batch: null argument"); return B2DEV_EINVAL; }
+  if (!c->ready) { set_err("solve_batch: no local dynamics (assemble first)"); return B2DEV_ESTATE; }
+  if (o->maxiter <= 0 || o->diagmaxiter <= 0 || o->diagsolver < 0 || o->diagsolver > 3 || o->failure < 0 ||
+      o->failure > 2 || o->precision != B2DEV_FP64) {
+    set_err("solve_batch: invalid options (batched solves run FP64 sweeps)");
+    return B2DEV_EINVAL;
+  }
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  const int P = c->nprob, n = c->n;
+  memset(reps, 0, sizeof(b2dev_batch_report) * P);
+  if (total) memset(total, 0, sizeof *total);
+  if (n == 0) {
+    for (int k = 0; k < P; k++) reps[k].iters = 1;
+    return B2DEV_OK;
+  }
+  // the canonical state buffers hold the initial iterate
+  if (c->state_r != 0) B2_CK(cudaMemcpyAsync(c->R64[0].p, c->R64[c->state_r].p, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st));
+  if (c->state_u != &c->Us[0]) B2_CK(cudaMemcpyAsync(c->Us[0].p, c->state_u->p, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st));
+  c->state_r = 0;
+  c->state_u = &c->Us[0];
+  SolveArgs a;
+  int grid = 0;
+  size_t smem = 0;
+  B2_TRY(solve_setup(c, false, o, o->maxiter, 0, 0, 0, o->grid, &a, &grid, &smem));
+  const size_t outb = sizeof(SolveControl) + sizeof(ProblemControl) * P;
+  if (c->pinned_cap < outb) {
+    if (c->pinned) cudaFreeHost(c->pinned);
+    c->pinned = nullptr;
+    c->pinned_cap = 0;
+    B2_CK(cudaMallocHost(&c->pinned, outb));
+    c->pinned_cap = outb;
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+  }
+  SolveControl* gout = static_cast<SolveControl*>(c->pinned);
+  ProblemControl* pout = reinterpret_cast<ProblemControl*>(static_cast<char*>(c->pinned) + sizeof(SolveControl));
+  auto enqueue_all = [&]() -> int {
+    B2_TRY(solve_enqueue(c, false, a, grid, smem));
+    c->launches++;
+    k_state_gather<<<blocks_for(n, 256), 256, 0, st>>>(
+        n, ptr<int>(c->row_prob), ptr<ProblemControl>(c->pctl), 0, o->nomerit, ptr<double4>(c->R64[0]),
+        ptr<double4>(c->R64[1]), ptr<double4>(c->R64[2]), ptr<double4>(c->Us[0]), ptr<double4>(c->Us[1]),
+        ptr<double4>(c->Um[0]), ptr<double4>(c->Um[1]), ptr<double>(c->conmerit[0]), ptr<double>(c->conmerit[1]));
+    B2_CK(cudaGetLastError());
+    B2_CK(cudaMemcpyAsync(gout, c->sctrl.p, sizeof(SolveControl), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaMemcpyAsync(pout, c->pctl.p, sizeof(ProblemControl) * P, cudaMemcpyDeviceToHost, st));
+    return B2DEV_OK;
+  };
+  B2_CK(cudaEventRecord(c->ev[4], st));
+  if (use_graph) {
+    std::vector<uintptr_t> key;
+    const unsigned char* ab = reinterpret_cast<const unsigned char*>(&a);
+    for (size_t i = 0; i + sizeof(uintptr_t) <= sizeof a; i += sizeof(uintptr_t)) {
+      uintptr_t v;
+      memcpy(&v, ab + i, sizeof v);
+      key.push_back(v);
+    }
+    key.push_back((uintptr_t)grid);
+    key.push_back((uintptr_t)smem);
+    key.push_back((uintptr_t)c->pinned);
+    key.push_back((uintptr_t)c->row_prob.p);
+    key.push_back((uintptr_t)n);
+    key.push_back((uintptr_t)P);
+    if (!c->graph || key != c->graph_key) {
+      if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+      cudaGraph_t gr = nullptr;
+      B2_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      const int rc = enqueue_all();
+      const cudaError_t ec = cudaStreamEndCapture(st, &gr);
+      if (rc != B2DEV_OK) { if (gr) cudaGraphDestroy(gr); return rc; }
+      if (ec != cudaSuccess) { set_err("solve_batch: graph capture failed: %s", cudaGetErrorString(ec)); return B2DEV_ECUDA; }
+      const cudaError_t ei = cudaGraphInstantiate(&c->graph, gr, 0);
+      cudaGraphDestroy(gr);
+      if (ei != cudaSuccess) { c->graph = nullptr; set_err("solve_batch: graph instantiation failed: %s", cudaGetErrorString(ei)); return B2DEV_ECUDA; }
+      c->graph_key = key;
+    }
+    B2_CK(cudaGraphLaunch(c->graph, st));
+  } else {
+    B2_TRY(enqueue_all());
+  }
+  B2_CK(cudaEventRecord(c->ev[5], st));
+  B2_CK(cudaStreamSynchronize(st));
+  c->state_r = 0;
+  c->state_u = &c->Us[0];
+  c->state_cm = o->nomerit ? nullptr : &c->conmerit[0];
+  if (gout->timeout) { set_err("solve_batch: a bounded device-side wait timed out"); return B2DEV_ETIMEOUT; }
+  const int pstride = a.pstride, maxiter = o->maxiter;
+  std::vector<unsigned long long> fk((size_t)P * pstride);
+  std::vector<unsigned> fc((size_t)P * pstride);
+  B2_CK(cudaMemcpy(fk.data(), c->failkey.p, sizeof(unsigned long long) * fk.size(), cudaMemcpyDeviceToHost));
+  B2_CK(cudaMemcpy(fc.data(), c->failcount.p, sizeof(unsigned) * fc.size(), cudaMemcpyDeviceToHost));
+  std::vector<double> rh, mh;
+  if (rerhist || merhist) {
+    rh.resize((size_t)P * pstride);
+    mh.resize((size_t)P * pstride);
+    B2_CK(cudaMemcpy(rh.data(), c->rer.p, sizeof(double) * rh.size(), cudaMemcpyDeviceToHost));
+    B2_CK(cudaMemcpy(mh.data(), c->mer.p, sizeof(double) * mh.size(), cudaMemcpyDeviceToHost));
+  }
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
+  int maxit = 0, anythrown = 0, nfail_all = 0;
+  double mmax = 0.0, emax = 0.0;
+  for (int k = 0; k < P; k++) {
+    const ProblemControl& q = pout[k];
+    b2dev_batch_report& r = reps[k];
+    r.iters = q.iters;
+    r.thrown = q.thrown;
+    r.merit = o->nomerit ? 0.0 : q.merit;
+    r.error = q.error;
+    r.merit_input = q.merit_input;
+    r.ms_to_decision = q.t_stop > gout->t_start ? (double)(q.t_stop - gout->t_start) * 1e-6 : 0.0;
+    r.rows = c->prob_off.empty() ? n : c->prob_off[k + 1] - c->prob_off[k];
+    if (r.rows == 0) r.iters = 1;  // no rows: one iteration with zero error and merit, as the reference loop does
+    int last = 0, nf = 0;
+    for (int s = 0; s <= q.final_iter && s <= maxiter; s++) {
+      const size_t i = (size_t)k * pstride + s;
+      if (fk[i]) last = (int)(fk[i] & 3ull);
+      nf += (int)fc[i];
+    }
+    r.last_fail_kind = last;
+    r.nfailures = nf;
+    if (rerhist) memcpy(rerhist + (size_t)k * maxiter, rh.data() + (size_t)k * pstride, sizeof(double) * std::min(q.iters, maxiter));
+    if (merhist) memcpy(merhist + (size_t)k * maxiter, mh.data() + (size_t)k * pstride, sizeof(double) * std::min(q.iters, maxiter));
+    maxit = std::max(maxit, q.iters);
+    anythrown |= q.thrown;
+    nfail_all += nf;
+    mmax = std::max(mmax, r.merit);
+    emax = std::max(emax, r.error);
+  }
+  if (total) {
+    total->iters = maxit;
+    total->thrown = anythrown;
+    total->nfailures = nfail_all;
+    total->sweeps = gout->sweeps;
+    total->merit = mmax;
+    total->error = emax;
+    total->ms_device = ms;
+    total->ms_kernel[0] = ms;
+    total->sweeps_launch[0] = gout->sweeps;
+    total->grid = grid;
+  }
+  return B2DEV_OK;
+}
+
+// Autotuner of the batched solve: times one solve of the current problems
+// (from the current initial state, restored after every trial) for every
+// combination of rows per tile, persistent grid size and staging window, and
+// keeps the fastest tile rows in the layout. The chosen grid and staging
+// window are returned for the caller's options.
+int b2dev_autotune_batch(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_tune_result* res) {
+  if (!c || !o || !res) { set_err("autotune_batch: null argument"); return B2DEV_EINVAL; }
+  if (!c->ready) { set_err("autotune_batch: no local dynamics"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  const int n = c->n, P = c->nprob;
+  memset(res, 0, sizeof *res);
+  if (n == 0) { res->tile_rows = c->tile_rows; return B2DEV_OK; }
+  // initial state into a scratch copy
+  Buf save;
+  B2_TRY(ensure(save, sizeof(double4) * 2 * (size_t)n));
+  double4* sv = ptr<double4>(save);
+  B2_CK(cudaMemcpyAsync(sv, c->R64[c->state_r].p, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st));
+  B2_CK(cudaMemcpyAsync(sv + n, c->state_u->p, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st));
+  const int rows_c[3] = {32, 16, 8};
+  const int stage_c[2] = {0, 128};
+  std::vector<b2dev_batch_report> reps(P);
+  float best = 1e30f;
+  int nt = 0, rc = B2DEV_OK;
+  for (int ir = 0; ir < 3 && rc == B2DEV_OK; ir++) {
+    rc = build_tiles(c, rows_c[ir]);
+    for (int is = 0; is < 2 && rc == B2DEV_OK; is++) {
+      b2dev_solve_opts oo = *o;
+      oo.stage_blocks = stage_c[is];
+      oo.grid = 0;
+      SolveArgs a;
+      int gmax = 0;
+      size_t smem = 0;
+      rc = solve_setup(c, false, &oo, oo.maxiter, 0, 0, 0, 0, &a, &gmax, &smem);
+      const int grids[3] = {gmax, std::max(1, gmax * 3 / 4), std::max(1, gmax / 2)};
+      for (int ig = 0; ig < 3 && rc == B2DEV_OK; ig++) {
+        if (ig > 0 && grids[ig] == grids[ig - 1]) continue;
+        oo.grid = grids[ig];
+        B2_CK(cudaMemcpyAsync(c->R64[0].p, sv, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st));
+        B2_CK(cudaMemcpyAsync(c->Us[0].p, sv + n, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st));
+        c->state_r = 0;
+        c->state_u = &c->Us[0];
+        b2dev_solve_report tot;
+        rc = b2dev_solve_batch(c, &oo, reps.data(), nullptr, nullptr, &tot, 0);
+        if (rc != B2DEV_OK) break;
+        if (nt < 32) {
+          res->trial_rows[nt] = rows_c[ir];
+          res->trial_grid[nt] = oo.grid;
+          res->trial_stage[nt] = oo.stage_blocks;
+          res->trial_ms[nt] = tot.ms_device;
+        }
+        nt++;
+        if (tot.ms_device < best) {
+          best = tot.ms_device;
+          res->tile_rows = rows_c[ir];
+          res->grid = oo.grid;
+          res->stage_blocks = oo.stage_blocks;
+          res->ms = tot.ms_device;
+        }
+      }
+    }
+  }
+  res->ntrials = std::min(nt, 32);
+  // the chosen tile rows and the initial state back in place
+  if (rc == B2DEV_OK) rc = build_tiles(c, res->tile_rows);
+  cudaMemcpyAsync(c->R64[0].p, sv, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(c->Us[0].p, sv + n, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st);
+  cudaStreamSynchronize(st);
+  cudaFree(save.p);
+  c->state_r = 0;
+  c->state_u = &c->Us[0];
+  c->state_cm = nullptr;
+  return rc;
 }
 
 int b2dev_sizes(b2dev_ctx* c, int* n, long long* nblocks, int* ncolours, double* free_energy) {

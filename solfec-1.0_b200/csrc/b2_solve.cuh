@@ -53,23 +53,36 @@ enum { DECIDE_NONE = 0, DECIDE_CONTINUE = 1, DECIDE_STOP = 2 };
 // Device-side control block of one solve launch (zeroed before launch).
 struct SolveControl {
   unsigned next_tile;       // tile counter in (sweep, colour, tile) order
-  unsigned tiles_done[3];   // completed tiles of sweep s, slot s % 3
-  int stop;                 // set once the final decision is taken
+  int stop;                 // set once every problem has taken its final decision
   int timeout;              // a bounded wait gave up (device error)
+  int nstopped;             // problems that have taken their final decision
+  int sweeps;               // sweeps started (including discarded speculative ones)
+  int pad;
+  unsigned long long t_start;  // global timer at launch (ns)
+};
+
+// Per-problem control block: one independent GAUSS_SEIDEL_Solve each
+// (zeroed before launch).
+struct ProblemControl {
+  unsigned tiles_done[3];   // completed tiles of sweep s, slot s % 3
+  int stop;                 // the final decision is taken
   int final_iter;           // launch-local index of the returned iterate
   int iters;                // iterations completed in this launch
   int thrown;               // FAILURE_EXIT raised
-  int sweeps;               // sweeps started (including discarded speculative ones)
+  int pad;
   double merit;             // merit of the returned iterate (0 with nomerit)
   double error;             // relative error of the returned iterate
   double merit_input;       // merit of the input iterate (merit mode)
   double prev_error;        // relative error of the latest iterate, kept between decisions
+  unsigned long long t_stop;  // global timer at the final decision (ns)
 };
 
 struct SolveArgs {
-  int n, ncolours, ntiles;
-  const int* colptr;        // [ncolours+1] colour offsets in sorted order
-  const int* tilebase;      // [ncolours+1] first tile of each colour (forward order)
+  int n, ntiles, nprob;
+  int nactive;              // problems with at least one row (the launch ends when all have decided)
+  const int4* tiles;        // [ntiles] first row, rows | problem << 6, first and end row of its colour (forward order)
+  const int* ptile_ptr;     // [nprob+1] the tiles of each problem ...
+  const int* ptile;         // [ntiles]  ... in ascending order (fixed summation order)
   const int* rowptr;        // [n+1]
   const int* col;           // [K] neighbour (sorted index)
   const double* W64;        // 9 planes of K doubles (plane stride kstride)
@@ -90,16 +103,19 @@ struct SolveArgs {
   double4* Um[2];           // merit U computed in sweep s: Um[s%2]
   double* conmerit[2];      // per-row merit numerator computed in sweep s: conmerit[s%2] (may be null)
   int* done;                // [n] sweeps completed per row (zeroed before launch)
-  int* decided;             // [maxiter+2] decision after each sweep (zeroed before launch)
+  int* decided;             // [nprob][pstride] decision after each sweep (zeroed before launch)
   double* part;             // [3][ntiles][4] per-tile partial sums
-  double* rerhist;          // global history arrays (indexed by iter0 + k)
+  double* rerhist;          // [nprob][pstride] history arrays (indexed by iter0 + k)
   double* merhist;
-  unsigned long long* failkey;  // per sweep: max (order position + 1) << 2 | kind of a diagonal failure
-  unsigned* failcount;          // per sweep: number of diagonal failures
+  unsigned long long* failkey;  // [nprob][pstride] per sweep: max (order position + 1) << 2 | kind of a diagonal failure
+  unsigned* failcount;          // [nprob][pstride] per sweep: number of diagonal failures
+  int pstride;              // per-problem stride of the arrays above (>= maxiter + 2)
+  const double* free_energy;  // [nprob] free energy of each problem (ldy.c:739)
   SolveControl* ctrl;
+  ProblemControl* pctl;     // [nprob]
   double* trace;            // per-row diagonal-solve record of one sweep (null: off)
   int trace_sweep;
-  double epsilon, meritval, diagepsilon, step, merit_denom;
+  double epsilon, meritval, diagepsilon, step;
   int maxiter, diagmaxiter, diagsolver, failure, dynamic, reverse, nomerit;
   int iter0;                // global index of this launch's first iteration
   int in;                   // R64/R32 buffer holding the input iterate
@@ -134,6 +150,25 @@ __device__ __noinline__ bool wait_at_least(const int* p, int need, SolveControl*
     __nanosleep(64);
   }
   return true;
+}
+
+// Gate of a tile of sweep s >= 2 of one problem: 1 = run (the decision after
+// sweep s-2 is to continue), 2 = skip (the problem has taken its final
+// decision, so later sweeps are discarded), 0 = the solve is ending or the
+// bounded wait gave up.
+__device__ __noinline__ int gate_wait(const int* decided_s2, const int* pstop, SolveControl* ctrl) {
+  const uint64_t t0 = globaltimer_ns();
+  volatile int* stop = &ctrl->stop;
+  volatile int* to = &ctrl->timeout;
+  while (true) {
+    const int d = ld_acquire(decided_s2);
+    if (d == DECIDE_CONTINUE) return 1;
+    if (d == DECIDE_STOP) return 2;
+    if (*(volatile const int*)pstop) return 2;
+    if (*stop || *to) return 0;
+    if (globaltimer_ns() - t0 > kBarrierLimitNs) { *to = 1; return 0; }
+    __nanosleep(64);
+  }
 }
 
 // 32-byte load that bypasses L1 (reaction buffers are rewritten by other SMs
@@ -220,8 +255,8 @@ __host__ __device__ constexpr size_t solve_smem_per_block() { return 3 * (MIXED 
 // the solve has stopped.
 template <bool MIXED>
 __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags& f, int r0, int nr, int cs, int ce,
-                                           int s, int rin, int rout, unsigned char* wsm, double& errup,
-                                           double& errlo, double& mnum) {
+                                           int s, int rin, int rout, int prob, unsigned char* wsm,
+                                           double& errup, double& errlo, double& mnum) {
   typedef typename std::conditional<MIXED, float, double>::type real;
   constexpr int kSlots = kWarp * kChunkUnroll;
   int* tp = reinterpret_cast<int*>(wsm);                                              // [kWarp + 1]
@@ -297,7 +332,8 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
       __syncwarp();
       if (f.merit) {  // each row adds its own merit products, in list order
         const int lo = mb > base ? mb : base;
-        const int hi = me < base + kSlots ? me : base + kSlots;
+        const int cend = base + kSlots < we ? base + kSlots : we;  // this chunk, inside this window
+        const int hi = me < cend ? me : cend;
         for (int k = lo; k < hi; k++) {
           const int slot = k - base;
           am[0] = am[0] + (double)mst[0][slot];
@@ -381,8 +417,9 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
       }
       if (kind) {
         const unsigned long long pos = f.backward ? (unsigned long long)(n - 1 - p) : (unsigned long long)p;
-        atomicMax(a.failkey + a.iter0 + s, ((pos + 1ull) << 2) | (unsigned long long)kind);
-        atomicAdd(a.failcount + a.iter0 + s, 1u);
+        const size_t fo = (size_t)prob * a.pstride + a.iter0 + s;
+        atomicMax(a.failkey + fo, ((pos + 1ull) << 2) | (unsigned long long)kind);
+        atomicAdd(a.failcount + fo, 1u);
       }
       a.R64[rout][p] = make_double4(R[0], R[1], R[2], 0.0);
       if constexpr (MIXED) a.R32[rout][p] = make_float4((float)R[0], (float)R[1], (float)R[2], 0.f);
@@ -397,29 +434,40 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   return true;
 }
 
-// Decision after sweep s, taken by the warp that completed the sweep's last
-// tile: sums the tile partials in tile order and applies the reference's
-// stopping rule (bgs.c:1028-1036, mrf.c:176-184). Decisions are taken in
-// sweep order.
-__device__ __noinline__ void finalize_sweep(const SolveArgs& a, int s) {
+// Decision after sweep s of problem `prob`, taken by the warp that completed
+// the problem's last tile of the sweep: sums the problem's tile partials in
+// tile order and applies the reference's stopping rule (bgs.c:1028-1036,
+// mrf.c:176-184). Decisions of a problem are taken in sweep order.
+__device__ __noinline__ void finalize_sweep(const SolveArgs& a, int prob, int s) {
   const int lane = threadIdx.x & (kWarp - 1);
-  volatile int* decided = a.decided;
+  ProblemControl* pc = a.pctl + prob;
+  volatile int* decided = a.decided + (size_t)prob * a.pstride;
   int prev = DECIDE_CONTINUE;
   if (s >= 1) {
     bool ok = true;
-    if (lane == 0) ok = wait_at_least(a.decided + s - 1, DECIDE_CONTINUE, a.ctrl);
+    if (lane == 0) ok = wait_at_least((const int*)decided + s - 1, DECIDE_CONTINUE, a.ctrl);
     ok = __shfl_sync(0xffffffffu, ok, 0);
     if (!ok) return;
     prev = decided[s - 1];
   }
   if (prev == DECIDE_STOP) {
-    if (lane == 0) { a.ctrl->tiles_done[s % 3] = 0; __threadfence(); decided[s] = DECIDE_STOP; }
+    if (lane == 0) { pc->tiles_done[s % 3] = 0; __threadfence(); decided[s] = DECIDE_STOP; }
     return;
   }
   double su = 0.0, sl = 0.0, sm = 0.0;
   const double* base = a.part + (size_t)(s % 3) * a.ntiles * 4;
-  for (int t = lane; t < a.ntiles; t += kWarp) {
-    su += __ldcg(base + 4 * t); sl += __ldcg(base + 4 * t + 1); sm += __ldcg(base + 4 * t + 2);
+  const int t0 = __ldg(a.ptile_ptr + prob), t1 = __ldg(a.ptile_ptr + prob + 1);
+  if (a.nprob == 1) {  // tiles 0 .. ntiles-1
+#pragma unroll 8
+    for (int t = lane; t < t1; t += kWarp) {
+      su += __ldcg(base + 4 * t); sl += __ldcg(base + 4 * t + 1); sm += __ldcg(base + 4 * t + 2);
+    }
+  } else {
+#pragma unroll 8
+    for (int i = t0 + lane; i < t1; i += kWarp) {
+      const int t = __ldg(a.ptile + i);
+      su += __ldcg(base + 4 * t); sl += __ldcg(base + 4 * t + 1); sm += __ldcg(base + 4 * t + 2);
+    }
   }
 #pragma unroll
   for (int d = 16; d >= 1; d >>= 1) {
@@ -428,20 +476,23 @@ __device__ __noinline__ void finalize_sweep(const SolveArgs& a, int s) {
     sm += __shfl_down_sync(0xffffffffu, sm, d);
   }
   if (lane != 0) return;
+  const size_t ho = (size_t)prob * a.pstride + a.iter0;
   const bool merit_mode = !a.nomerit;
-  const double error = sqrt(su) / sqrt(sl == 0.0 ? 1.0 : sl);                // bgs.c:1028
-  const double merit_prev = merit_mode ? (0.5 * sm) / a.merit_denom : 0.0;   // mrf.c:176-184
+  const double error = sqrt(su) / sqrt(sl == 0.0 ? 1.0 : sl);                         // bgs.c:1028
+  double lo = __ldg(a.free_energy + prob);
+  lo = lo < 2.220446049250313e-16 ? 1.0 : lo;                                           // mrf.c:45
+  const double merit_prev = merit_mode ? (0.5 * sm) / (lo == 0.0 ? 1.0 : lo) : 0.0;     // mrf.c:176-184
   const bool gs_sweep = !(merit_mode && s == a.maxiter);
-  const bool failed = __ldcg(a.failkey + a.iter0 + s) != 0ull;
-  volatile double* perr_slot = &a.ctrl->prev_error;
+  const bool failed = __ldcg(a.failkey + ho + s) != 0ull;
+  volatile double* perr_slot = &pc->prev_error;
   const double perr = *perr_slot;  // error of iterate s-1
   int final_iter = -2, thrown = 0;
   double fm = 0.0, fe = 0.0;
   if (merit_mode) {
-    if (s == 0) a.ctrl->merit_input = merit_prev;
+    if (s == 0) pc->merit_input = merit_prev;
     if (s >= 1) {
-      a.rerhist[a.iter0 + s - 1] = perr;
-      a.merhist[a.iter0 + s - 1] = merit_prev;
+      a.rerhist[ho + s - 1] = perr;
+      a.merhist[ho + s - 1] = merit_prev;
       const bool meets = !(perr > a.epsilon || merit_prev > a.meritval);  // bgs.c:1036
       if (meets || s == a.maxiter) { final_iter = s - 1; fm = merit_prev; fe = perr; }
       else if (gs_sweep && failed && a.failure == FAIL_EXIT) { final_iter = s; thrown = 1; fm = merit_prev; fe = error; }
@@ -449,28 +500,35 @@ __device__ __noinline__ void finalize_sweep(const SolveArgs& a, int s) {
       final_iter = 0; thrown = 1; fe = error;
     }
   } else {
-    a.rerhist[a.iter0 + s] = error;
-    a.merhist[a.iter0 + s] = 0.0;
+    a.rerhist[ho + s] = error;
+    a.merhist[ho + s] = 0.0;
     if (failed && a.failure == FAIL_EXIT) { final_iter = s; thrown = 1; fe = error; }
     else if (!(error > a.epsilon) || s + 1 >= a.maxiter) { final_iter = s; fe = error; }
   }
   *perr_slot = error;
-  a.ctrl->tiles_done[s % 3] = 0;
+  pc->tiles_done[s % 3] = 0;
   if (final_iter >= -1) {
-    a.ctrl->final_iter = final_iter;
-    a.ctrl->iters = thrown ? final_iter : final_iter + 1;
-    a.ctrl->thrown = thrown;
-    a.ctrl->merit = fm;
-    a.ctrl->error = fe;
+    pc->final_iter = final_iter;
+    pc->iters = thrown ? final_iter : final_iter + 1;
+    pc->thrown = thrown;
+    pc->merit = fm;
+    pc->error = fe;
+    pc->t_stop = globaltimer_ns();
     __threadfence();
     decided[s] = DECIDE_STOP;
-    *(volatile int*)&a.ctrl->stop = 1;
+    *(volatile int*)&pc->stop = 1;
+    if (atomicAdd(&a.ctrl->nstopped, 1) + 1 == a.nactive) *(volatile int*)&a.ctrl->stop = 1;
   } else {
     __threadfence();
     decided[s] = DECIDE_CONTINUE;
   }
 }
 
+// Persistent solve of all problems of the layout. Tiles are numbered by
+// colour (forward order) and, inside a colour, by problem; every sweep claims
+// them in that order (reversed on backward sweeps). A problem's tiles of a
+// sweep after its final decision are skipped. The launch ends when every
+// problem has decided.
 template <bool MIXED>
 __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(SolveArgs a) {
   extern __shared__ __align__(16) unsigned char solve_smem[];
@@ -480,8 +538,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(SolveArgs a) {
   const bool merit_mode = !a.nomerit;
   const int maxsweep = merit_mode ? a.maxiter : a.maxiter - 1;  // last sweep that can run
   volatile int* stop = &a.ctrl->stop;
-  volatile int* decided = a.decided;
   const int T = a.ntiles;
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.ctrl->t_start = globaltimer_ns();
 
   while (true) {
     unsigned t = 0;
@@ -490,33 +548,27 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(SolveArgs a) {
     const int s = (int)(t / (unsigned)T);
     const int w = (int)(t % (unsigned)T);
     if (s > maxsweep || *stop) break;
-    if (s >= 2) {  // sweep s reuses the buffers of iterate s-3: wait for the decision after sweep s-2
-      bool ok = true;
-      if (lane == 0) ok = wait_at_least(a.decided + s - 2, DECIDE_CONTINUE, a.ctrl);
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      if (!ok || decided[s - 2] == DECIDE_STOP) break;
-    }
     SweepFlags f;
     f.gs = !(merit_mode && s == a.maxiter);
     f.merit = merit_mode;
     f.u_merit = merit_mode && (s >= 1 || a.u0_from_merit);
     f.backward = a.reverse && ((a.iter0 + s) & 1);
+    const int tile = f.backward ? T - 1 - w : w;
+    const int4 ti = __ldg(a.tiles + tile);  // first row, rows | problem << 6, colour bounds
+    const int prob = ti.y >> 6, nr = ti.y & 63;
+    const unsigned ntp = a.nprob == 1 ? (unsigned)T : (unsigned)(__ldg(a.ptile_ptr + prob + 1) - __ldg(a.ptile_ptr + prob));
+    volatile int* decided = a.decided + (size_t)prob * a.pstride;
+    if (s >= 2) {  // sweep s reuses the buffers of iterate s-3: wait for the decision after sweep s-2
+      int gate = 0;
+      if (lane == 0) gate = gate_wait((const int*)decided + s - 2, &a.pctl[prob].stop, a.ctrl);
+      gate = __shfl_sync(0xffffffffu, gate, 0);
+      if (gate == 0) break;
+      if (gate == 2) continue;  // this problem has finished: its later sweeps are not run
+    }
     const int rin = (a.in + s) % 3;       // iterate s-1
     const int rout = (a.in + s + 1) % 3;  // iterate s
-    // tile w of the sweep -> colour (in sweep order) and tile inside it
-    int cc = 0;
-    while (cc + 1 < a.ncolours) {
-      const int c_next = f.backward ? a.ncolours - 2 - cc : cc + 1;
-      const int start = f.backward ? (T - __ldg(a.tilebase + c_next + 1)) : __ldg(a.tilebase + c_next);
-      if (w >= start) cc++; else break;
-    }
-    const int c = f.backward ? a.ncolours - 1 - cc : cc;
-    const int first = f.backward ? (T - __ldg(a.tilebase + c + 1)) : __ldg(a.tilebase + c);
-    const int cs = __ldg(a.colptr + c), ce = __ldg(a.colptr + c + 1);
-    const int r0 = cs + (w - first) * kWarp;
-    const int nr = min(kWarp, ce - r0);
     double errup = 0.0, errlo = 0.0, mnum = 0.0;
-    if (!solve_tile<MIXED>(a, f, r0, nr, cs, ce, s, rin, rout, wsm, errup, errlo, mnum)) break;
+    if (!solve_tile<MIXED>(a, f, ti.x, nr, ti.z, ti.w, s, rin, rout, prob, wsm, errup, errlo, mnum)) break;
 #pragma unroll
     for (int d = 16; d >= 1; d >>= 1) {
       errup += __shfl_down_sync(0xffffffffu, errup, d);
@@ -525,16 +577,16 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(SolveArgs a) {
     }
     unsigned prev = 0;
     if (lane == 0) {
-      double* pp = a.part + ((size_t)(s % 3) * T + w) * 4;
+      double* pp = a.part + ((size_t)(s % 3) * T + tile) * 4;
       pp[0] = errup; pp[1] = errlo; pp[2] = mnum;
       __threadfence();
-      prev = atomicAdd(&a.ctrl->tiles_done[s % 3], 1u);
-      atomicMax(&a.ctrl->sweeps, s + 1);
+      prev = atomicAdd(&a.pctl[prob].tiles_done[s % 3], 1u);
+      if (w == 0) atomicMax(&a.ctrl->sweeps, s + 1);
     }
     prev = __shfl_sync(0xffffffffu, prev, 0);
-    if (prev == (unsigned)T - 1) {
+    if (prev == ntp - 1) {
       __threadfence();
-      finalize_sweep(a, s);
+      finalize_sweep(a, prob, s);
     }
   }
 }

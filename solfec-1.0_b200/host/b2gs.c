@@ -95,6 +95,25 @@ b2gs_solver* b2gs_create (double epsilon, int maxiter, double meritval, int fail
   return gs;
 }
 
+int b2gs_get_opts (b2gs_solver *gs, b2dev_solve_opts *o)
+{
+  if (!gs || !o) return B2DEV_EINVAL;
+  memset (o, 0, sizeof *o);
+  o->epsilon = gs->epsilon;
+  o->meritval = gs->meritval;
+  o->diagepsilon = gs->diagepsilon;
+  o->maxiter = gs->maxiter;
+  o->diagmaxiter = gs->diagmaxiter;
+  o->diagsolver = gs->diagsolver;
+  o->failure = gs->failure;
+  o->reverse = gs->reverse;
+  o->nomerit = gs->nomerit ? 1 : gs->meritval >= 1.0 ? 1 : 0;  /* bgs.c:927 */
+  o->precision = gs->precision;
+  o->grid = gs->grid;
+  o->stage_blocks = gs->stage_blocks;
+  return 0;
+}
+
 int b2gs_solve (b2gs_solver *gs, b2gs_locdyn *ldy)
 {
   b2dev_solve_opts o;
@@ -103,21 +122,8 @@ int b2gs_solve (b2gs_solver *gs, b2gs_locdyn *ldy)
 
   host_err[0] = '\0';
   if (!gs || !ldy) return B2DEV_EINVAL;
-  nomerit = gs->nomerit ? 1 : gs->meritval >= 1.0 ? 1 : 0;  /* bgs.c:927 */
-
-  memset (&o, 0, sizeof o);
-  o.epsilon = gs->epsilon;
-  o.meritval = gs->meritval;
-  o.diagepsilon = gs->diagepsilon;
-  o.maxiter = gs->maxiter;
-  o.diagmaxiter = gs->diagmaxiter;
-  o.diagsolver = gs->diagsolver;
-  o.failure = gs->failure;
-  o.reverse = gs->reverse;
-  o.nomerit = nomerit;
-  o.precision = gs->precision;
-  o.grid = gs->grid;
-  o.stage_blocks = gs->stage_blocks;
+  b2gs_get_opts (gs, &o);
+  nomerit = o.nomerit;
 
   free (gs->rerhist);
   free (gs->merhist);

@@ -51,6 +51,18 @@ class b2gs_contacts(C.Structure):
                 ('restitution', C.c_void_p), ('cohesion', C.c_void_p), ('on_device', C.c_int)]
 
 
+class b2dev_batch_report(C.Structure):
+    _fields_ = [('iters', C.c_int), ('thrown', C.c_int), ('last_fail_kind', C.c_int), ('nfailures', C.c_int),
+                ('merit', C.c_double), ('error', C.c_double), ('merit_input', C.c_double),
+                ('ms_to_decision', C.c_double), ('rows', C.c_int)]
+
+
+class b2dev_tune_result(C.Structure):
+    _fields_ = [('tile_rows', C.c_int), ('grid', C.c_int), ('stage_blocks', C.c_int), ('ntrials', C.c_int),
+                ('ms', C.c_float), ('trial_rows', C.c_int * 32), ('trial_grid', C.c_int * 32),
+                ('trial_stage', C.c_int * 32), ('trial_ms', C.c_float * 32)]
+
+
 CALLBACK = C.CFUNCTYPE(None, C.c_void_p)
 
 # exported symbols declared in include/*.h with their ctypes signatures
@@ -81,6 +93,13 @@ _SIGNATURES = {
     'b2dev_get_trace': (C.c_int, [C.c_void_p, C.c_void_p]),
     'b2dev_diag_solve_batch': (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
                                          C.c_double] + [C.c_void_p] * 11),
+    'b2dev_set_problems': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    'b2dev_problem_free_energy': (C.c_int, [C.c_void_p, C.c_void_p]),
+    'b2dev_set_tile_rows': (C.c_int, [C.c_void_p, C.c_int]),
+    'b2dev_tile_rows': (C.c_int, [C.c_void_p]),
+    'b2dev_solve_batch': (C.c_int, [C.c_void_p, C.POINTER(b2dev_solve_opts), C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.POINTER(b2dev_solve_report), C.c_int]),
+    'b2dev_autotune_batch': (C.c_int, [C.c_void_p, C.POINTER(b2dev_solve_opts), C.POINTER(b2dev_tune_result)]),
     'b2dev_mlp_nparams': (C.c_int, []),
     'b2dev_mlp_create': (C.c_int, [C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
     'b2dev_mlp_destroy': (None, [C.c_void_p]),
@@ -116,6 +135,7 @@ _SIGNATURES = {
     'b2gs_set_precision': (None, [C.c_void_p, C.c_int]),
     'b2gs_set_grid': (None, [C.c_void_p, C.c_int]),
     'b2gs_set_stage_blocks': (None, [C.c_void_p, C.c_int]),
+    'b2gs_get_opts': (C.c_int, [C.c_void_p, C.POINTER(b2dev_solve_opts)]),
     'b2gs_get_iters_mixed': (C.c_int, [C.c_void_p]),
     'b2gs_get_solve_ms': (C.c_double, [C.c_void_p]),
     'b2gs_get_merit_input': (C.c_double, [C.c_void_p]),
