@@ -8,11 +8,21 @@ the relative-error test non-binding, epsilon = 1; maxiter 1000,
 SEMISMOOTH_NEWTON), warm-started from the reactions of the previous step, as
 a time-stepping run does.
 
-`value` is the per-step time of the product mode (mixed precision: FP32
-off-diagonal sweeps, FP64 diagonal solves / merit / closing refinement) with
-all inputs resident in HBM; the FP64 mode is reported beside it. `e2e` is the
-same step through the C ABI with host (pinned) buffers: scene upload, assembly,
-warm-start upload, solve and the read-back of R, U and the per-contact merit.
+`value` is the per-step time of the product mode named by the metric: mixed
+precision (FP32 off-diagonal sweeps, FP64 diagonal solves / merit / closing
+refinement) started from the learned warm start (BF16 network on the tensor
+cores, kept only when its merit is below the previous-step start's), with all
+inputs resident in HBM; the plain FP64 and plain mixed modes are reported
+beside it. `e2e` is the same step through the C ABI with host (pinned)
+buffers: scene upload, assembly, warm-start upload, network start, solve and
+the read-back of R, U and the per-contact merit.
+
+--workload batched runs the batched workload instead: 256 independent uneven
+sphere scenes (bodies log-uniform in [50, 2000], radius U[0.02, 0.05],
+friction U[0.2, 0.6], h = 1e-3, epsilon = meritval = 1e-4) solved by one
+persistent launch replayed from a CUDA graph, launch shape autotuned; it
+reports contacts solved per second and the per-scene time to the final
+decision (p50, p99).
 
 With --gpus N > 1 (torchrun), every rank solves its own replica scene (the
 path has no exchange step for independent scenes): per-step time is the max
@@ -196,9 +206,20 @@ def bench_product(args, ws, rank, local):
         ldy.set_state_ptr(C.c_void_p(Rd.data_ptr()), C.c_void_p(Ud.data_ptr()), 1)
         gs.solve(ldy)
 
+    from solfec_b200 import learn
+    net = learn.WarmStartNet.load(device=local)
+    nn_reps = []
+
+    def step_device_nn(gs):
+        ldy.update_begin_arrays(bd, cd, sc.step, sc.dynamic)
+        ldy.set_state_ptr(C.c_void_p(Rd.data_ptr()), C.c_void_p(Ud.data_ptr()), 1)
+        nn_reps.append(learn.warm_start(ldy, net))
+        gs.solve(ldy)
+
     def step_e2e(gs):
         ldy.update_begin_arrays(bh, ch, sc.step, sc.dynamic)
         ldy.set_state_ptr(C.c_void_p(Rh.data_ptr()), C.c_void_p(Uh.data_ptr()), 0)
+        learn.warm_start(ldy, net)
         gs.solve(ldy)
         ldy.get_state_ptr(C.c_void_p(Rout_h.data_ptr()), C.c_void_p(Uout_h.data_ptr()),
                           C.c_void_p(Cout_h.data_ptr()), 0)
@@ -227,10 +248,11 @@ def bench_product(args, ws, rank, local):
 
     results = {}
     with ClockSampler(local) as clk:
-        for mode in ('fp64', 'mixed'):
+        for mode in ('fp64', 'mixed', 'mixed_nn'):
             gs = GAUSS_SEIDEL_SOLVER(**SOLVE)
-            gs.precision = 'MIXED' if mode == 'mixed' else 'FP64'
-            ms, reps, launches = timed(step_device, gs, args.steps, args.warmup)
+            gs.precision = 'FP64' if mode == 'fp64' else 'MIXED'
+            ms, reps, launches = timed(step_device_nn if mode == 'mixed_nn' else step_device, gs, args.steps,
+                                       args.warmup)
             r = reps[-1]
             results[mode] = dict(ms=ms, iters=gs.iters, iters_mixed=gs.iters_mixed, merit=ldy.merit, report=r,
                                  launches=launches, assemble_ms=ldy.assemble_ms, error=gs.error)
@@ -238,8 +260,121 @@ def bench_product(args, ws, rank, local):
         gs.precision = 'MIXED'
         e2e_ms, _, _ = timed(step_e2e, gs, args.steps, args.warmup)
     nrows, K, ncol, fe = ldy.sizes()
+    results['mixed_nn']['nn'] = nn_reps[-1] if nn_reps else None
+    results['mixed_nn']['nn_used_steps'] = sum(1 for r in nn_reps if r['used_nn'])
+    results['mixed_nn']['nn_steps'] = len(nn_reps)
+    net.close()
     return dict(results=results, e2e_ms=e2e_ms, h2d=h2d_bytes, d2h=d2h_bytes, n=nrows, K=K, ncolours=ncol,
                 clocks=clk.summary(), iters_prev=iters_prev, nbod=sc.nbod, scene=sc, R0=R0, U0=U0)
+
+
+BATCH = dict(seed=4, count=256, nmin=50, nmax=2000, settle_iters=300)
+BATCH_SOLVE = dict(epsilon=1e-4, maxiter=1000, meritval=1e-4)
+BATCH_METRIC = 'batched contact solve: contacts solved per second (256 uneven sphere scenes, one persistent launch)'
+
+
+def bench_batched(args, ws, rank, local):
+    """Config of the batched workload: every rank solves its own batch."""
+    import ctypes as C
+    import torch
+    from solfec_b200 import GAUSS_SEIDEL_SOLVER, scenes
+    from solfec_b200.batch import BatchSolver, concat_scenes
+    from solfec_b200._lib import lib
+    kw = dict(BATCH)
+    kw['seed'] = BATCH['seed'] + 1000 * rank
+    t0 = time.perf_counter()
+    scs = scenes.batched_scenes(workers=min(32, os.cpu_count() or 1), **kw)
+    gen_s = time.perf_counter() - t0
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    bs = BatchSolver(scs, device=local)
+    gs = GAUSS_SEIDEL_SOLVER(**BATCH_SOLVE)
+    bs.solve(gs, use_graph=False)                  # the previous step, from rest
+    R0, U0, _ = bs.state()
+    off = bs.offsets
+    nxt = [scenes.advance_velocities(sc, R0[off[k]:off[k + 1]]) for k, sc in enumerate(scs)]
+    bs.update(nxt)
+    bs.set_state(R0, U0)
+    tune = bs.autotune(gs)
+    n = int(off[-1])
+    Rd = torch.from_numpy(np.ascontiguousarray(R0.ravel())).to(dev)
+    Ud = torch.from_numpy(np.ascontiguousarray(U0.ravel())).to(dev)
+
+    def step():
+        bs.ldy.set_state_ptr(C.c_void_p(Rd.data_ptr()), C.c_void_p(Ud.data_ptr()), 1)
+        return bs.solve(gs, use_graph=True)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    l0 = lib().b2dev_launch_count(bs.ctx)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    outs = []
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            outs.append(step())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dev)
+    launches = lib().b2dev_launch_count(bs.ctx) - l0
+    # end to end: host scene arrays in, assembly and layout, warm start from the host, solve, results out
+    u, _ = concat_scenes(nxt)
+    h2d = sum(getattr(u, f).nbytes for f in ('rot', 'x0', 'jinv', 'minv', 'velo', 'velo0', 'obstacle', 'master',
+                                             'slave', 'mpnt', 'spnt', 'base', 'gap', 'friction', 'restitution',
+                                             'cohesion')) + 2 * R0.nbytes
+    d2h = 2 * R0.nbytes + n * 8
+    te = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        bs.update(nxt)
+        bs.set_state(R0, U0)
+        bs.solve(gs, use_graph=True)
+        bs.state()
+        te.append(1e3 * (time.perf_counter() - t1))
+    last = outs[-1]
+    td = last.ms_to_decision
+    res = dict(ms=ms, contacts=n, scenes=len(scs), iters=last.iters, td=td, tune=tune, launches=launches,
+               clocks=clk.summary(), gen_s=gen_s, e2e_ms=max_over_ranks(statistics.median(te), dev), h2d=h2d,
+               d2h=d2h, grid=last.grid, sweeps=last.sweeps, ms_device=last.ms_device,
+               merit_max=float(last.merit.max()), thrown=int(last.thrown.sum()))
+    bs.close()
+    return res
+
+
+def batched_line(args, ws, out):
+    td, it = out['td'], out['iters']
+    cps = out['contacts'] * ws / (out['ms'] * 1e-3)
+    return {
+        'metric': BATCH_METRIC, 'value': round(cps, 1), 'unit': 'contacts/s', 'n_gpus': ws, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': round(out['ms'], 4), 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded scene generator)',
+        'config': {'workload': 'batched: %d independent sphere scenes, bodies log-uniform in [%d, %d], radius '
+                               'U[0.02, 0.05], friction U[0.2, 0.6], h=1e-3' % (out['scenes'], BATCH['nmin'],
+                                                                                  BATCH['nmax']),
+                   'contacts': out['contacts'], 'solver': 'GAUSS_SEIDEL_SOLVER(epsilon=1e-4, maxiter=1000, '
+                                                          'meritval=1e-4), warm start from the previous step',
+                   'launch': 'one persistent cooperative launch per step, replayed from a CUDA graph',
+                   'autotuned': {k: out['tune'][k] for k in ('tile_rows', 'grid', 'stage_blocks', 'ms')},
+                   'autotune_trials': len(out['tune']['trials']),
+                   'l2': 'working set < 126 MB L2 (no flush between steps)',
+                   'parallelism': 'replicas' if ws > 1 else 'single GPU'},
+        'per_scene_ms_to_decision': {'p50': round(float(np.percentile(td, 50)), 4),
+                                     'p99': round(float(np.percentile(td, 99)), 4),
+                                     'max': round(float(td.max()), 4)},
+        'per_scene_iters': {'p50': int(np.percentile(it, 50)), 'p99': int(np.percentile(it, 99)),
+                            'max': int(it.max())},
+        'merit_max': out['merit_max'], 'thrown': out['thrown'],
+        'e2e': {'value': round(out['contacts'] * ws / (out['e2e_ms'] * 1e-3), 1), 'unit': 'contacts/s',
+                'ms_per_step': round(out['e2e_ms'], 3), 'h2d_bytes_per_step': int(out['h2d']),
+                'd2h_bytes_per_step': int(out['d2h'])},
+        'gpu_launches': int(out['launches']), 'clocks': out['clocks'],
+        'scene_generation_s': round(out['gen_s'], 1),
+    }
 
 
 def roofline(mode, r, n, K, peak):
@@ -324,6 +459,7 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--scene', default=None, help='NXxNYxNZ lattice of a smaller case (profiling)')
     ap.add_argument('--maxiter', type=int, default=None, help='iteration cap of a smaller case (profiling)')
+    ap.add_argument('--workload', default='hexahedra', choices=['hexahedra', 'batched'])
     args = ap.parse_args()
     global WORKLOAD
     if args.scene:
@@ -342,12 +478,20 @@ def main():
         import datetime
         torch.cuda.set_device(local)
         torch.distributed.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    if args.workload == 'batched':
+        out = bench_batched(args, ws, rank, local)
+        if rank == 0:
+            print(json.dumps(batched_line(args, ws, out)), flush=True)
+        if ws > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return
     out = bench_product(args, ws, rank, local)
     peak, peak_kind = _peaks()
     if rank == 0:
         res = out['results']
-        mixed, fp64 = res['mixed'], res['fp64']
-        roof = roofline('mixed', mixed, out['n'], out['K'], peak)
+        mixed, fp64, mnn = res['mixed'], res['fp64'], res['mixed_nn']
+        roof = roofline('mixed', mnn, out['n'], out['K'], peak)
         roof64 = roofline('fp64', fp64, out['n'], out['K'], peak)
         roof['peak_kind'] = peak_kind
         cpu = None
@@ -361,12 +505,14 @@ def main():
                              % (out['n'], t['sample_iters'], fp64['iters']),
                    'assemble_ms': round(t['assemble_ms'], 3), 'per_iteration_ms': round(t['per_iter_ms'], 3)}
         line = {
-            'metric': METRIC, 'value': round(mixed['ms'], 4), 'unit': 'ms', 'n_gpus': ws, 'steps': args.steps,
-            'warmup': args.warmup, 'ms_per_step': round(mixed['ms'], 4), 'higher_is_better': False,
+            'metric': METRIC, 'value': round(mnn['ms'], 4), 'unit': 'ms', 'n_gpus': ws, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': round(mnn['ms'], 4), 'higher_is_better': False,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64+f32 (mixed)',
             'data': 'synthetic (seeded scene generator)',
             'config': {'workload': WORKLOAD, 'contacts': out['n'], 'blocks': out['K'], 'bodies': out['nbod'],
-                       'colours': out['ncolours'], 'mode': 'mixed (FP32 sweeps, FP64 diagonal/merit/refinement)',
+                       'colours': out['ncolours'],
+                       'mode': 'mixed+NN: learned warm start (kept when its merit is lower), FP32 sweeps, '
+                               'FP64 diagonal/merit/refinement',
                        'solver': 'GAUSS_SEIDEL_SOLVER(epsilon=%g, maxiter=%d, meritval=%g, SEMISMOOTH_NEWTON), '
                                  'warm start from the previous step' % (SOLVE['epsilon'], SOLVE['maxiter'],
                                                                          SOLVE['meritval']),
@@ -379,11 +525,16 @@ def main():
                           'sweeps': r['report']['sweeps_launch'], 'grid': r['report']['grid']}
                       for m, r in res.items()},
             'speedup_mixed_vs_fp64': round(fp64['ms'] / mixed['ms'], 3),
+            'speedup_mixed_nn_vs_fp64': round(fp64['ms'] / mnn['ms'], 3),
+            'warm_start': None if not mnn.get('nn') else {
+                'network_start_used_steps': mnn['nn_used_steps'], 'steps': mnn['nn_steps'],
+                'merit_network_start': mnn['nn']['merit_nn'], 'merit_previous_step_start': mnn['nn']['merit_plain'],
+                'network_and_merit_ms': round(mnn['nn']['ms'], 4)},
             'roofline': roof, 'roofline_fp64': roof64,
             'cpu_baseline': cpu,
             'e2e': {'value': round(out['e2e_ms'], 4), 'unit': 'ms', 'h2d_bytes_per_step': out['h2d'],
                     'd2h_bytes_per_step': out['d2h']},
-            'gpu_launches': int(mixed['launches']),
+            'gpu_launches': int(mnn['launches']),
             'clocks': out['clocks'],
         }
         print(json.dumps(line), flush=True)

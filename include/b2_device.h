@@ -251,8 +251,10 @@ int b2dev_mlp_forward(b2dev_mlp* net, int nrows, const float* feat, float* out);
  * rprev[n][3]. Used to build training sets. */
 int b2dev_nn_features(b2dev_ctx* ctx, float* feat, double* scale, double* rprev);
 /* Replace the context's initial reactions by the network's prediction when
- * its merit is lower than that of the reactions held; U is left as it is. */
-int b2dev_nn_warm_start(b2dev_ctx* ctx, b2dev_mlp* net, b2dev_nn_report* rep);
+ * its merit is below accept_ratio (0 < accept_ratio <= 1) times the merit of
+ * the reactions held (the previous step's); otherwise, and whenever the
+ * prediction's merit is higher, the plain start stays. U is left as it is. */
+int b2dev_nn_warm_start(b2dev_ctx* ctx, b2dev_mlp* net, double accept_ratio, b2dev_nn_report* rep);
 
 #ifdef __cplusplus
 }

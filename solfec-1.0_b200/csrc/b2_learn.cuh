@@ -457,9 +457,12 @@ int b2dev_nn_features(b2dev_ctx* c, float* feat, double* scale, double* rprev) {
   return B2DEV_OK;
 }
 
-int b2dev_nn_warm_start(b2dev_ctx* c, b2dev_mlp* net, b2dev_nn_report* rep) {
+int b2dev_nn_warm_start(b2dev_ctx* c, b2dev_mlp* net, double accept_ratio, b2dev_nn_report* rep) {
   using namespace b2::mlp;
-  if (!c || !c->ready || !net || !rep) { set_err("nn_warm_start: invalid arguments"); return B2DEV_EINVAL; }
+  if (!c || !c->ready || !net || !rep || !(accept_ratio > 0.0 && accept_ratio <= 1.0)) {
+    set_err("nn_warm_start: invalid arguments");
+    return B2DEV_EINVAL;
+  }
   if (net->device != c->device) { set_err("nn_warm_start: network and context on different devices"); return B2DEV_EINVAL; }
   memset(rep, 0, sizeof *rep);
   const int n = c->n;
@@ -489,8 +492,9 @@ int b2dev_nn_warm_start(b2dev_ctx* c, b2dev_mlp* net, b2dev_nn_report* rep) {
   B2_TRY(merit_of(c, ptr<double4>(c->R64[cand]), &rep->merit_nn));
   if (err) { set_err("nn_warm_start: a bounded tensor-core wait timed out"); return B2DEV_ETIMEOUT; }
   B2_TRY(merit_of(c, ptr<double4>(c->R64[c->state_r]), &rep->merit_plain));
-  // the plain start stays unless the network's reactions have the lower merit
-  rep->used_nn = rep->merit_nn < rep->merit_plain ? 1 : 0;
+  // the plain start stays unless the network's reactions have a merit below
+  // accept_ratio times the plain start's (1: any improvement)
+  rep->used_nn = rep->merit_nn < accept_ratio * rep->merit_plain ? 1 : 0;
   if (rep->used_nn) c->state_r = cand;
   B2_CK(cudaEventRecord(c->ev[7], st));
   B2_CK(cudaEventSynchronize(c->ev[7]));

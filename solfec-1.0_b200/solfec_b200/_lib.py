@@ -110,7 +110,7 @@ _SIGNATURES = {
                                   C.c_uint64, C.c_void_p]),
     'b2dev_mlp_forward': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     'b2dev_nn_features': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
-    'b2dev_nn_warm_start': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    'b2dev_nn_warm_start': (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
     # include/solfec_b200.h
     'b2gs_create': (C.c_void_p, [C.c_double, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int,
                                  C.c_void_p, CALLBACK]),

@@ -158,10 +158,19 @@ def features(ldy):
     return feat[:n], scale[:n], rprev[:n]
 
 
-def warm_start(ldy, net: WarmStartNet) -> dict:
-    """Network start with the plain start as the fallback (by merit)."""
+ACCEPT_RATIO = 0.5  # the network start must at least halve the merit of the plain start
+
+
+def warm_start(ldy, net: WarmStartNet, accept_ratio: float = ACCEPT_RATIO) -> dict:
+    """Network start with the plain start as the fallback, by merit: the
+    prediction replaces the previous-step reactions only when its merit is
+    below accept_ratio times theirs. A start with a somewhat lower merit can
+    still need more iterations (the network corrects local residuals, while
+    the iteration count follows the slowly converging global modes), hence
+    the margin."""
     rep = b2dev_nn_report()
-    _check(lib().b2dev_nn_warm_start(ldy.device_context, net.handle, C.addressof(rep)), 'b2dev_nn_warm_start')
+    _check(lib().b2dev_nn_warm_start(ldy.device_context, net.handle, float(accept_ratio), C.addressof(rep)),
+           'b2dev_nn_warm_start')
     return dict(merit_nn=rep.merit_nn, merit_plain=rep.merit_plain, used_nn=bool(rep.used_nn), ms=rep.ms)
 
 

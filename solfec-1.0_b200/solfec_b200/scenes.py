@@ -412,13 +412,31 @@ def hexahedra_lattice(seed: int = 3, nx: int = 100, ny: int = 100, nz: int = 10,
                            master, slave, points, normals, gaps, friction, 0.0, 0.0)
 
 
-def batched_scenes(seed: int = 4, count: int = 256, nmin: int = 50, nmax: int = 2000):
-    """Uneven independent sphere scenes: body count log-uniform in [nmin, nmax],
-    radius U[0.02, 0.05], friction U[0.2, 0.6], h = 1e-3."""
+def batched_scene_specs(seed: int = 4, count: int = 256, nmin: int = 50, nmax: int = 2000, settle_iters: int = 300):
+    """Arguments of spheres_small for each scene of the batched workload: body
+    count log-uniform in [nmin, nmax], radius U[0.02, 0.05], friction
+    U[0.2, 0.6], h = 1e-3."""
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.uniform(math.log(nmin), math.log(nmax), count)).astype(int)
     fr = rng.uniform(0.2, 0.6, count)
-    return [spheres_small(seed * 100003 + s, int(sizes[s]), friction=float(fr[s])) for s in range(count)]
+    return [(seed * 100003 + s, int(sizes[s]), float(fr[s]), settle_iters) for s in range(count)]
+
+
+def batched_scene(spec) -> Scene:
+    seed, n, friction, settle_iters = spec
+    return spheres_small(seed, n, friction=friction, settle_iters=settle_iters)
+
+
+def batched_scenes(seed: int = 4, count: int = 256, nmin: int = 50, nmax: int = 2000, settle_iters: int = 300,
+                   workers: int = 1):
+    """Uneven independent sphere scenes (see batched_scene_specs); with
+    workers > 1 they are generated by a spawned process pool."""
+    specs = batched_scene_specs(seed, count, nmin, nmax, settle_iters)
+    if workers > 1:
+        import multiprocessing as mp
+        with mp.get_context('spawn').Pool(workers) as pool:
+            return pool.map(batched_scene, specs, chunksize=1)
+    return [batched_scene(sp) for sp in specs]
 
 
 def advance_velocities(scene: Scene, R: np.ndarray) -> Scene:

@@ -130,7 +130,13 @@ def test_warm_start_fallback_and_convergence():
         net = learn.WarmStartNet.load()
         ldy.set_state(R0, U0)
         rep = learn.warm_start(ldy, net)
-        assert min(rep['merit_nn'], rep['merit_plain']) == (rep['merit_nn'] if rep['used_nn'] else rep['merit_plain'])
+        assert rep['used_nn'] == (rep['merit_nn'] < learn.ACCEPT_RATIO * rep['merit_plain'])
+        # with the bare fallback rule (any lower merit) the network start is taken whenever it is better
+        ldy.set_state(R0, U0)
+        rep1 = learn.warm_start(ldy, net, accept_ratio=1.0)
+        assert rep1['used_nn'] == (rep1['merit_nn'] < rep1['merit_plain'])
+        ldy.set_state(R0, U0)
+        rep = learn.warm_start(ldy, net)
         gs_nn = GAUSS_SEIDEL_SOLVER(**kw)
         gs_nn.solve(ldy)
         assert ldy.merit <= 1e-4
