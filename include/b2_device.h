@@ -162,6 +162,15 @@ int b2dev_diag_solve_batch(b2dev_ctx* ctx, int n, int diagsolver, int failure, d
                            const double* rho, const double* gap, const double* friction, const double* restitution,
                            const double* cohesion, double* U, double* R, int* kind);
 
+/* Colouring priority of the next layouts: list_order = 1 (default) colours in
+ * the greedy order of the caller's row list; 0 uses the seeded priorities of
+ * the colour_seed argument (b2gs_locdyn_set_colour_seed selects 0). Both are
+ * reproduced bit for bit by the host greedy colouring in that order. A layout
+ * whose contact graph equals the previous one reuses its colours
+ * (b2dev_colour_reuse_count counts the reuses). */
+int b2dev_set_colour_order(b2dev_ctx* ctx, int list_order);
+long long b2dev_colour_reuse_count(b2dev_ctx* ctx);
+
 /* ---- batches of independent problems --------------------------------------
  *
  * No counterpart in the reference (one GAUSS_SEIDEL_Solve per call,

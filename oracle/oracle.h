@@ -83,6 +83,7 @@ int orc_assemble (int nbod, const double *rot, const double *x0, const double *j
 /* Counter-based priority of row i for a colouring seed (shared definition with
  * the device Jones-Plassmann kernel). */
 uint64_t orc_jp_priority (uint64_t seed, int i);
+int orc_colour_ordered (int n, const int *adjptr, const int *adjcol, const int *order, int maxcolours, int *colour);
 
 /* Greedy colouring in decreasing priority order: each row takes the smallest
  * colour not used by an already coloured neighbour. This is the fixed point of

@@ -50,6 +50,8 @@ def _load(name):
                                      C.c_double, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_double), _ip, _ip, _ip, _dp]
         lib.orc_colour.restype = C.c_int
         lib.orc_colour.argtypes = [C.c_int, _ip, _ip, C.c_uint64, C.c_int, _ip]
+        lib.orc_colour_ordered.restype = C.c_int
+        lib.orc_colour_ordered.argtypes = [C.c_int, _ip, _ip, _ip, C.c_int, _ip]
         lib.orc_jp_priority.restype = C.c_uint64
         lib.orc_jp_priority.argtypes = [C.c_uint64, C.c_int]
         lib.orc_merit.restype = C.c_double
@@ -123,10 +125,17 @@ def assemble(scene) -> LocalDynamics:
                          adjptr, adjcol[:nblk], Woff[:9 * nblk], fe.value, scene.step, scene.dynamic, adjbod[:nblk])
 
 
-def colour(ld: LocalDynamics, seed: int, maxcolours: int = 256):
+def colour(ld: LocalDynamics, seed=None, maxcolours: int = 256):
+    """Greedy colouring in decreasing Jones-Plassmann priority (seeded) order,
+    or in list order when seed is None (the device's default mode)."""
     lib = _load('oracle')
     col = np.zeros(ld.n, np.int32)
-    nc = lib.orc_colour(ld.n, ld.adjptr, ld.adjcol if ld.nblocks else np.zeros(1, np.int32), seed, maxcolours, col)
+    adjcol = ld.adjcol if ld.nblocks else np.zeros(1, np.int32)
+    if seed is None:
+        order = np.arange(max(ld.n, 1), dtype=np.int32)
+        nc = lib.orc_colour_ordered(ld.n, ld.adjptr, adjcol, order, maxcolours, col)
+    else:
+        nc = lib.orc_colour(ld.n, ld.adjptr, adjcol, seed, maxcolours, col)
     return nc, col
 
 

@@ -292,6 +292,26 @@ static int by_priority_desc (const void *a, const void *b)
   return x < y ? 1 : x > y ? -1 : 0;
 }
 
+/* greedy colouring in the given row order (smallest colour no coloured neighbour holds) */
+int orc_colour_ordered (int n, const int *adjptr, const int *adjcol, const int *order, int maxcolours, int *colour)
+{
+  unsigned char *used = calloc ((size_t) maxcolours + 1, 1);
+  int ncolours = 0;
+  for (int i = 0; i < n; i ++) colour[i] = -1;
+  for (int t = 0; t < n; t ++)
+  {
+    int i = order[t], c;
+    for (int k = adjptr[i]; k < adjptr[i+1]; k ++) { int cj = colour[adjcol[k]]; if (cj >= 0) used[cj] = 1; }
+    for (c = 0; c < maxcolours && used[c]; c ++);
+    if (c >= maxcolours) { ncolours = -1; break; }
+    colour[i] = c;
+    if (c + 1 > ncolours) ncolours = c + 1;
+    for (int k = adjptr[i]; k < adjptr[i+1]; k ++) { int cj = colour[adjcol[k]]; if (cj >= 0) used[cj] = 0; }
+  }
+  free (used);
+  return ncolours;
+}
+
 int orc_colour (int n, const int *adjptr, const int *adjcol, uint64_t seed, int maxcolours, int *colour)
 {
   uint64_t *key = malloc (((size_t) n + 1) * sizeof (uint64_t));

@@ -6,9 +6,14 @@
 // is Jones-Plassmann with smallest-available colour: in every round each
 // uncoloured row whose priority beats all uncoloured neighbours takes the
 // smallest colour no coloured neighbour holds. Priorities come from
-// jp_priority(seed, row), so the result equals the sequential greedy
-// colouring in decreasing priority order and is reproducible bit for bit on
-// the host.
+// jp_priority(seed, row) (seeded hash) or, in the list-order mode, from the
+// row index (earlier rows win); either way the result equals the sequential
+// greedy colouring in decreasing priority order and is reproducible bit for
+// bit on the host. The list order needs more rounds (the longest chain of
+// neighbours in increasing index) but, on meshes and lattices whose contacts
+// are listed in geometric order, reaches the fewest colours (6 instead of 10
+// on the hexahedra lattice, where the contact graph is the line graph of a
+// bipartite graph of degree 6); on random piles both reach the same count.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -53,8 +58,8 @@ __device__ __forceinline__ bool colour_barrier(ColourControl* ctrl, unsigned nbl
 
 // Persistent cooperative Jones-Plassmann colouring of the graph (adjptr,
 // adjcol). colour[] must be -1 on entry.
-__global__ void k_jp_colour(int n, const int* adjptr, const int* adjcol, unsigned long long seed, int* colour,
-                            int* sel, ColourControl* ctrl) {
+__global__ void k_jp_colour(int n, const int* adjptr, const int* adjcol, unsigned long long seed, int list_order,
+                            int* colour, int* sel, ColourControl* ctrl) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int nthreads = gridDim.x * blockDim.x;
   const unsigned nblocks = gridDim.x;
@@ -66,10 +71,10 @@ __global__ void k_jp_colour(int n, const int* adjptr, const int* adjcol, unsigne
       int s = 0;
       if (__ldcg(colour + i) < 0) {
         s = 1;
-        const uint64_t pi = jp_priority(seed, i);
+        const uint64_t pi = list_order ? jp_list_priority(i) : jp_priority(seed, i);
         for (int k = adjptr[i]; k < adjptr[i + 1]; k++) {
           const int j = adjcol[k];
-          if (__ldcg(colour + j) < 0 && jp_priority(seed, j) > pi) { s = 0; break; }
+          if (__ldcg(colour + j) < 0 && (list_order ? jp_list_priority(j) : jp_priority(seed, j)) > pi) { s = 0; break; }
         }
       }
       sel[i] = s;
@@ -106,6 +111,18 @@ __global__ void k_jp_colour(int n, const int* adjptr, const int* adjcol, unsigne
       return;
     }
   }
+}
+
+// Sets *diff if the graph (adjptr[n+1], adjcol[K]) differs from the copy kept
+// with the last colouring.
+__global__ void k_graph_diff(int n, long long K, const int* adjptr, const int* adjcol, const int* pptr,
+                             const int* pcol, int* diff) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  bool d = false;
+  for (long long i = t; i <= n; i += stride) d |= adjptr[i] != pptr[i];
+  for (long long k = t; k < K; k += stride) d |= adjcol[k] != pcol[k];
+  if (__any_sync(0xffffffffu, d) && (threadIdx.x & 31) == 0) atomicExch(diff, 1);
 }
 
 // colour offsets from the colour-sorted keys

@@ -44,6 +44,10 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 // splitmix64 finaliser of (seed + golden * (i+1)), high 32 bits, with the row
 // index in the low 32 bits so priorities are unique. The host colouring in the
 // test oracle uses the same definition.
+// Priority of row i in the list-order mode: rows earlier in the list win, so
+// Jones-Plassmann reproduces the sequential greedy colouring in list order.
+__host__ __device__ __forceinline__ uint64_t jp_list_priority(int i) { return ~(uint64_t)(uint32_t)i; }
+
 __host__ __device__ __forceinline__ uint64_t jp_priority(uint64_t seed, int i) {
   uint64_t z = seed + 0x9E3779B97F4A7C15ull * ((uint64_t)i + 1ull);
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;

@@ -158,6 +158,13 @@ struct b2dev_ctx {
 
   // colouring and layout
   Buf colour, sel, cctrl, keys_out, iota, perm, iperm, colptr, sdeg;
+  int colour_list = 1;            // 1: greedy order = list order, 0: seeded Jones-Plassmann priorities
+  Buf gptr_prev, gcol_prev;       // graph of the last colouring (reused while the graph is unchanged)
+  bool colour_valid = false;
+  int colour_n = -1, colour_mode = -1, ncolours_prev = 0;
+  long long colour_K = -1;
+  uint64_t colour_seed_prev = 0;
+  long long colour_reuse = 0;     // colourings skipped because the graph was unchanged
   Buf rowptr, col, W64, W32, Wd, Ad, Bv, Vv, rho, gap, fric, rest, coh;
   std::vector<int> colptr_h;
   std::vector<int> rowptr_h;   // sorted CSR offsets (host copy, sizes the tiles)
@@ -287,6 +294,24 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   B2_TRY(ensure(c->rowptr, sizeof(int) * (n + 1)));
 
   ColourControl cc;
+  memset(&cc, 0, sizeof cc);
+  bool reuse = false;
+  if (c->colour_valid && c->colour_n == n && c->colour_K == c->K && c->colour_mode == c->colour_list &&
+      (c->colour_list || c->colour_seed_prev == seed) && n > 0) {  // same graph as the last colouring?
+    B2_CK(cudaMemsetAsync(c->bad.p, 0, sizeof(int), st));
+    c->launches++;
+    k_graph_diff<<<std::max(1, std::min(4 * c->sms, blocks_for(std::max<long long>(c->K, n + 1), T))), T, 0, st>>>(
+        n, c->K, ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<int>(c->gptr_prev), ptr<int>(c->gcol_prev),
+        ptr<int>(c->bad));
+    int diff = 1;
+    B2_CK(cudaMemcpyAsync(&diff, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaStreamSynchronize(st));
+    reuse = diff == 0;
+  }
+  if (reuse) {
+    c->colour_reuse++;
+    cc.ncolours = c->ncolours_prev;
+  } else {
   B2_CK(cudaMemsetAsync(c->colour.p, 0xff, sizeof(int) * (n + 1), st));
   B2_CK(cudaMemsetAsync(c->cctrl.p, 0, sizeof(ColourControl), st));
   if (n > 0) {
@@ -296,10 +321,11 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
     const int* ap = ptr<int>(c->adjptr);
     const int* ac = ptr<int>(c->adjcol);
     unsigned long long sd = seed;
+    int lo = c->colour_list;
     int* colp = ptr<int>(c->colour);
     int* selp = ptr<int>(c->sel);
     ColourControl* ctl = ptr<ColourControl>(c->cctrl);
-    void* args[] = {&nn, &ap, &ac, &sd, &colp, &selp, &ctl};
+    void* args[] = {&nn, &ap, &ac, &sd, &lo, &colp, &selp, &ctl};
     c->launches++;
     B2_CK(cudaLaunchCooperativeKernel((const void*)k_jp_colour, grid, T, args, 0, st));
   }
@@ -307,6 +333,21 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   B2_CK(cudaStreamSynchronize(st));
   if (cc.timeout) { set_err("colouring: grid barrier wait timed out"); return B2DEV_ETIMEOUT; }
   if (cc.overflow) { set_err("colouring: more than %d colours needed", kMaxColours); return B2DEV_ECOLOURS; }
+  // keep the graph this colouring belongs to
+  c->colour_valid = false;
+  if (n > 0) {
+    B2_TRY(ensure(c->gptr_prev, sizeof(int) * (n + 1)));
+    B2_TRY(ensure(c->gcol_prev, sizeof(int) * (c->K + 1)));
+    B2_CK(cudaMemcpyAsync(c->gptr_prev.p, c->adjptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice, st));
+    if (c->K > 0) B2_CK(cudaMemcpyAsync(c->gcol_prev.p, c->adjcol.p, sizeof(int) * c->K, cudaMemcpyDeviceToDevice, st));
+    c->colour_valid = true;
+    c->colour_n = n;
+    c->colour_K = c->K;
+    c->colour_mode = c->colour_list;
+    c->colour_seed_prev = seed;
+    c->ncolours_prev = cc.ncolours;
+  }
+  }
   c->ncolours = n > 0 ? cc.ncolours : 0;
 
   // rows sorted by colour, ascending row index inside a colour (stable radix sort)
@@ -685,7 +726,7 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->cctrl, &c->keys_out, &c->iota, &c->perm, &c->iperm, &c->colptr, &c->sdeg, &c->rowptr, &c->col,
                 &c->W64, &c->W32, &c->Wd, &c->Ad, &c->Bv, &c->Vv, &c->rho, &c->gap, &c->fric, &c->rest, &c->coh,
                 &c->R64[0], &c->R64[1], &c->R64[2], &c->R32[0], &c->R32[1], &c->R32[2], &c->Us[0], &c->Us[1],
-                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec,
+                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec, &c->gptr_prev, &c->gcol_prev,
                 &c->part, &c->rer,
                 &c->mer, &c->failkey, &c->failcount, &c->sctrl, &c->io, &c->cub_tmp, &c->trace};
   for (Buf* b : all)
@@ -1034,6 +1075,14 @@ int b2dev_solve(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_solve_report* rep
 
 
 // ---- batches of independent problems ------------------------------------------
+
+int b2dev_set_colour_order(b2dev_ctx* c, int list_order) {
+  if (!c) { set_err("set_colour_order: null context"); return B2DEV_EINVAL; }
+  c->colour_list = list_order ? 1 : 0;
+  return B2DEV_OK;
+}
+
+long long b2dev_colour_reuse_count(b2dev_ctx* c) { return c ? c->colour_reuse : 0; }
 
 int b2dev_set_problems(b2dev_ctx* c, int nprob, const int* row_offsets) {
   if (!c || nprob < 1 || (nprob > 1 && !row_offsets)) { set_err("set_problems: invalid arguments"); return B2DEV_EINVAL; }
@@ -1434,7 +1483,8 @@ int b2dev_colour_noalloc(int device, void* stream, int n, const int* adjptr, con
     B2_CK(cudaMemsetAsync(colour, 0xff, sizeof(int) * n, st));
     int nn = n;
     unsigned long long sd = seed;
-    void* args[] = {&nn, (void*)&adjptr, (void*)&adjcol, &sd, &colour, &sel, &ctl};
+    int lo = 0;  // seeded priorities
+    void* args[] = {&nn, (void*)&adjptr, (void*)&adjcol, &sd, &lo, &colour, &sel, &ctl};
     const int grid = std::max(1, std::min(su.grid, blocks_for(n, 256)));
     B2_CK(cudaLaunchCooperativeKernel((const void*)k_jp_colour, grid, 256, args, 0, st));
   }

@@ -298,7 +298,11 @@ void b2gs_locdyn_destroy (b2gs_locdyn *ldy)
   free (ldy);
 }
 
-void b2gs_locdyn_set_colour_seed (b2gs_locdyn *ldy, uint64_t seed) { ldy->colour_seed = seed; }
+void b2gs_locdyn_set_colour_seed (b2gs_locdyn *ldy, uint64_t seed)
+{
+  ldy->colour_seed = seed;
+  b2dev_set_colour_order (ldy->dev, 0);  /* seeded Jones-Plassmann priorities */
+}
 
 void* b2gs_locdyn_device (b2gs_locdyn *ldy) { return ldy ? (void*) ldy->dev : NULL; }
 

@@ -93,6 +93,8 @@ _SIGNATURES = {
     'b2dev_get_trace': (C.c_int, [C.c_void_p, C.c_void_p]),
     'b2dev_diag_solve_batch': (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
                                          C.c_double] + [C.c_void_p] * 11),
+    'b2dev_set_colour_order': (C.c_int, [C.c_void_p, C.c_int]),
+    'b2dev_colour_reuse_count': (C.c_longlong, [C.c_void_p]),
     'b2dev_set_problems': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     'b2dev_problem_free_energy': (C.c_int, [C.c_void_p, C.c_void_p]),
     'b2dev_set_tile_rows': (C.c_int, [C.c_void_p, C.c_int]),

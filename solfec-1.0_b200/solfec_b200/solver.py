@@ -85,7 +85,16 @@ class LOCDYN:
         return lib().b2gs_locdyn_device(self._h)
 
     def set_colour_seed(self, seed: int):
+        """Seeded Jones-Plassmann priorities for the next layouts."""
         lib().b2gs_locdyn_set_colour_seed(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF)
+
+    def set_colour_list_order(self):
+        """Greedy colouring in list order for the next layouts (the default)."""
+        _check(lib().b2dev_set_colour_order(self.device_context, 1), 'b2dev_set_colour_order')
+
+    def colour_reuse_count(self) -> int:
+        """Layouts that reused the previous colouring (unchanged contact graph)."""
+        return int(lib().b2dev_colour_reuse_count(self.device_context))
 
     def update_begin(self, scene, step=None, dynamic=None):
         """LOCDYN_Update_Begin on a scenes.Scene (host numpy arrays)."""

@@ -266,3 +266,37 @@ def test_hexahedra_assembly_and_solve(scene_cache):
     o = oracle_in_order(ld, ldy.order(), epsilon=1e-4, maxiter=1000, meritval=1e-4)
     assert gs.iters == o['iters']
     assert same_bits(R, o['R']) and same_bits(U, o['U'])
+
+
+def test_list_order_colouring_and_reuse(scene_cache):
+    # default mode: greedy colouring in list order, bit-exact against the host
+    for sc in (scene_cache('spheres_lattice'), scene_cache('hexahedra_lattice', nx=20, ny=20, nz=6)):
+        ld = O.assemble(sc)
+        ldy = LOCDYN()
+        ldy.update_begin(sc)
+        nc, col = O.colour(ld, None)
+        assert np.array_equal(ldy.colours(), col)
+        assert ldy.sizes()[2] == nc
+        order0 = ldy.order()
+        # same contact graph: the colouring is reused, the layout is the same
+        reuse0 = ldy.colour_reuse_count()
+        ldy.update_begin(scenes.advance_velocities(sc, np.zeros((sc.ncon, 3))))
+        assert ldy.colour_reuse_count() == reuse0 + 1
+        assert np.array_equal(ldy.order(), order0) and np.array_equal(ldy.colours(), col)
+        # and the solve is the oracle's in that order
+        gs = GAUSS_SEIDEL_SOLVER(1e-4, 1000, 1e-4)
+        gs.solve(ldy)
+        R, U, _ = ldy.get_state()
+        ld2 = O.assemble(scenes.advance_velocities(sc, np.zeros((sc.ncon, 3))))
+        o = oracle_in_order(ld2, ldy.order(), epsilon=1e-4, maxiter=1000, meritval=1e-4)
+        assert gs.iters == o['iters'] and same_bits(R, o['R']) and same_bits(U, o['U'])
+        ldy.close()
+    # the lattice's contact graph is the line graph of a degree-6 bipartite graph: 6 colours in list order
+    ld = O.assemble(scene_cache('hexahedra_lattice', nx=20, ny=20, nz=6))
+    assert O.colour(ld, None)[0] == 6
+    # another graph is coloured again
+    ldy = LOCDYN()
+    ldy.update_begin(scene_cache('spheres_lattice'))
+    ldy.update_begin(scene_cache('hexahedra_lattice', nx=20, ny=20, nz=6))
+    assert ldy.colour_reuse_count() == 0
+    ldy.close()

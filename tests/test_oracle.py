@@ -190,3 +190,16 @@ def test_lu_small_against_lapack():
         assert info == info2 == 0
         np.testing.assert_array_equal(ipiv, piv + 1)
         np.testing.assert_allclose(x, y, rtol=1e-12, atol=1e-13)
+
+
+def test_list_order_colouring_is_greedy_in_list_order(pile):
+    sc, ld, _ = pile
+    nc, col = O.colour(ld, None)
+    ref = -np.ones(ld.n, int)
+    for i in range(ld.n):
+        used = set(ref[ld.adjcol[ld.adjptr[i]:ld.adjptr[i + 1]]].tolist())
+        c = 0
+        while c in used:
+            c += 1
+        ref[i] = c
+    assert np.array_equal(col, ref) and nc == ref.max() + 1
