@@ -529,8 +529,11 @@ __device__ __noinline__ void finalize_sweep(const SolveArgs& a, int prob, int s)
 // them in that order (reversed on backward sweeps). A problem's tiles of a
 // sweep after its final decision are skipped. The launch ends when every
 // problem has decided.
+// Six blocks of two warps per SM (at most 168 registers a thread): with the
+// list-order colouring a sweep has about six levels of ~1.5k tiles each, so
+// 1,776 resident warps hold a whole level in one wave.
 template <bool MIXED>
-__global__ void __launch_bounds__(kSolveThreads, 1) k_solve(SolveArgs a) {
+__global__ void __launch_bounds__(kSolveThreads, 6) k_solve(SolveArgs a) {
   extern __shared__ __align__(16) unsigned char solve_smem[];
   const int warp = threadIdx.x / kWarp;
   const int lane = threadIdx.x & (kWarp - 1);
