@@ -58,6 +58,9 @@ WORKLOAD = 'hexahedra-100k: 100x100x10 perturbed rigid hexahedra (side 0.04 m, +
 # algorithmic bytes of one fused sweep+merit pass (per off-diagonal block, per row)
 BYTES_BLOCK = {'fp64': 100, 'mixed': 52}
 BYTES_ROW = {'fp64': 316, 'mixed': 328}
+# DRAM bytes (read + write) per algorithmic byte of k_solve, measured by ncu on the 100x100x6 lattice
+# (profiles/k_solve_hexahedra100k.md); DRAM traffic grows in proportion to blocks, rows and passes
+TRAFFIC_RATIO = {'fp64': 1293.8 / 1363.6, 'mixed': 700.1 / 739.2}
 
 
 def _dist():
@@ -384,7 +387,8 @@ def roofline(mode, r, n, K, peak):
     bytes_launch = sweeps * (K * BYTES_BLOCK[mode] + n * BYTES_ROW[mode])
     gbs = bytes_launch / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
     return dict(bound='hbm', achieved=round(gbs, 1), peak=peak, unit='GB/s', frac=round(gbs / peak, 3),
-                traffic=None, kernel='k_solve<%s>' % ('true' if mode == 'mixed' else 'false'),
+                traffic=int(bytes_launch * TRAFFIC_RATIO[mode]), traffic_source='ncu, 100x100x6 lattice, scaled',
+                kernel='k_solve<%s>' % ('true' if mode == 'mixed' else 'false'),
                 bytes_per_launch=int(bytes_launch), sweeps_per_launch=sweeps, kernel_ms=round(ms, 4))
 
 
