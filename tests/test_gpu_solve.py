@@ -300,3 +300,28 @@ def test_list_order_colouring_and_reuse(scene_cache):
     ldy.update_begin(scene_cache('hexahedra_lattice', nx=20, ny=20, nz=6))
     assert ldy.colour_reuse_count() == 0
     ldy.close()
+
+
+def test_polydisperse_pile_against_compiled_reference():
+    """Config 2 shape (polydisperse spheres, friction 0.5, h = 5e-4, epsilon =
+    meritval = 1e-6), scaled to 4,000 bodies: the FP64 GPU solve against the
+    reference's own GAUSS_SEIDEL_Solve (oracle/_ref, compiled from its sources)
+    on identical W and B in the GPU's row order; falls back to the oracle where
+    the compiled reference is absent."""
+    sc = scenes.spheres_polydisperse(seed=2, n=4000)
+    ld = O.assemble(sc)
+    kw = dict(epsilon=1e-6, maxiter=1000, meritval=1e-6)
+    ldy = LOCDYN()
+    ldy.set(ld)
+    gs = GAUSS_SEIDEL_SOLVER(**kw)
+    gs.solve(ldy)
+    R, U, _ = ldy.get_state()
+    impl = 'ref' if O.ref_available() else 'oracle'
+    order = ldy.order()
+    res = O.solve(ld.permuted(order), impl=impl, **kw)
+    Rr = np.empty((ld.n, 3)); Ur = np.empty((ld.n, 3))
+    Rr[order] = res['R'].reshape(-1, 3); Ur[order] = res['U'].reshape(-1, 3)
+    assert gs.iters == res['iters']
+    assert same_bits(R, Rr) and same_bits(U, Ur)
+    assert ldy.merit <= 1e-6 or gs.iters == 1000
+    ldy.close()
