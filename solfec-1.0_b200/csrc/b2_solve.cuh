@@ -44,7 +44,10 @@ namespace b2 {
 
 constexpr int kSolveThreads = 64;
 constexpr int kSolveWarps = kSolveThreads / kWarp;
-constexpr int kChunkUnroll = 4;                      // 32-block chunks whose loads are issued together
+// 32-block chunks whose loads are issued together: 2 in FP64 (more would
+// spill under the 168-register cap), 3 with the FP32 planes (measured fastest)
+template <bool MIXED>
+__host__ __device__ constexpr int chunk_unroll() { return MIXED ? 3 : 2; }
 constexpr int kTileHeader = 256;                     // bytes of per-warp shared memory before the staging
 constexpr uint64_t kBarrierLimitNs = 2000000000ull;  // 2 s per bounded wait
 
@@ -190,8 +193,9 @@ struct SweepFlags {
 // Loads of one 32-block chunk: column indices and the nine coefficients of
 // each block (lane per block, coalesced plane loads).
 template <bool MIXED, typename real>
-__device__ __forceinline__ void load_chunk(const SolveArgs& a, int base, int ke, int lane, int (&jj)[kChunkUnroll],
-                                           real (&w)[kChunkUnroll][9]) {
+__device__ __forceinline__ void load_chunk(const SolveArgs& a, int base, int ke, int lane,
+                                           int (&jj)[chunk_unroll<MIXED>()], real (&w)[chunk_unroll<MIXED>()][9]) {
+  constexpr int kChunkUnroll = chunk_unroll<MIXED>();
 #pragma unroll
   for (int u = 0; u < kChunkUnroll; u++) {
     const int k = base + u * kWarp + lane;
@@ -227,7 +231,8 @@ __device__ __forceinline__ void load_r(const SolveArgs& a, int buf, int j, real&
 // one chunk, and the Gauss-Seidel products of up to gcap blocks of the tile
 template <bool MIXED>
 __host__ __device__ constexpr size_t solve_warp_smem(int gcap) {
-  return (size_t)kTileHeader + (size_t)(3 * kWarp * kChunkUnroll + 3 * gcap) * (MIXED ? sizeof(float) : sizeof(double));
+  return (size_t)kTileHeader +
+         (size_t)(3 * kWarp * chunk_unroll<MIXED>() + 3 * gcap) * (MIXED ? sizeof(float) : sizeof(double));
 }
 // shared memory of a warp: fixed part and bytes per staged block
 template <bool MIXED>
@@ -258,6 +263,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
                                            int s, int rin, int rout, int prob, unsigned char* wsm,
                                            double& errup, double& errlo, double& mnum) {
   typedef typename std::conditional<MIXED, float, double>::type real;
+  constexpr int kChunkUnroll = chunk_unroll<MIXED>();
   constexpr int kSlots = kWarp * kChunkUnroll;
   int* tp = reinterpret_cast<int*>(wsm);                                              // [kWarp + 1]
   real(*mst)[kSlots] = reinterpret_cast<real(*)[kSlots]>(wsm + kTileHeader);          // [3][kSlots]
