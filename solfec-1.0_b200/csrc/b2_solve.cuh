@@ -20,20 +20,25 @@
 // iteration s+1 from the U its merit pass wrote) and the stopping decision for
 // iterate s are the reference's, while W is streamed once per iteration.
 //
-// Scheduling. Instead of a grid-wide barrier per colour, warps claim tiles of
-// 32 rows from one counter in (sweep, colour, tile) order and wait only for
-// the rows a tile reads: for sweep s, a neighbour earlier in the sweep must
-// have completed sweep s, a later one sweep s-1 (per-row completion counters).
-// Reactions are triple-buffered, so a tile of sweep s+1 may run while sweep s
-// is being decided; sweep s+2 waits for that decision. Every wait is bounded.
+// Scheduling. Instead of a grid-wide barrier per colour, warps claim tiles
+// (runs of at most 32 rows of one colour and one problem) from one counter in
+// (sweep, colour, tile) order and wait only for the rows a tile reads: for
+// sweep s, a neighbour earlier in the sweep must have completed sweep s, a
+// later one sweep s-1 (per-row completion counters). Reactions are
+// triple-buffered, so a tile of sweep s+1 may run while sweep s is being
+// decided; sweep s+2 waits for that decision. Every wait is bounded.
 // Progress: a tile only waits for rows of tiles claimed before it, so the
 // earliest unfinished tile can always proceed (all blocks are co-resident,
 // cooperative launch).
 //
+// Problems. One launch may solve several independent problems (a batch of
+// scenes); each keeps its own decisions, and the tiles of a problem's sweeps
+// after its final decision are skipped.
+//
 // Reductions. Each tile writes its error and merit partial sums; the warp that
-// completes the last tile of a sweep adds them in tile order and takes the
-// stopping decision, decisions being taken in sweep order. Results therefore
-// do not depend on which warp ran which tile.
+// completes a problem's last tile of a sweep adds that problem's partials in
+// tile order and takes its stopping decision, decisions being taken in sweep
+// order. Results therefore do not depend on which warp ran which tile.
 #pragma once
 
 #include <cuda_runtime.h>
