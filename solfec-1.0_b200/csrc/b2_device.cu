@@ -1281,7 +1281,11 @@ int b2dev_autotune_batch(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_tune_res
   memset(res, 0, sizeof *res);
   if (n == 0) { res->tile_rows = c->tile_rows; return B2DEV_OK; }
   // initial state into a scratch copy
-  Buf save;
+  struct Scratch {  // freed on every return path
+    Buf b;
+    ~Scratch() { if (b.p) cudaFree(b.p); }
+  } scratch;
+  Buf& save = scratch.b;
   B2_TRY(ensure(save, sizeof(double4) * 2 * (size_t)n));
   double4* sv = ptr<double4>(save);
   B2_CK(cudaMemcpyAsync(sv, c->R64[c->state_r].p, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st));
@@ -1335,7 +1339,6 @@ int b2dev_autotune_batch(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_tune_res
   cudaMemcpyAsync(c->R64[0].p, sv, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(c->Us[0].p, sv + n, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st);
   cudaStreamSynchronize(st);
-  cudaFree(save.p);
   c->state_r = 0;
   c->state_u = &c->Us[0];
   c->state_cm = nullptr;

@@ -180,18 +180,15 @@ int mlp_check(b2dev_mlp* net) {
   return B2DEV_OK;
 }
 
+// dynamic shared memory limit of the network kernels on the current device
+// (set on every call: cheap, and free of shared state between host threads)
 int mlp_smem_attr() {
-  static bool done[64] = {false};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && done[dev]) return B2DEV_OK;
   const int bytes = b2::mlp::kSmemGrad + b2::mlp::kSmemAlign;
   B2_CK(cudaFuncSetAttribute((const void*)b2::mlp::k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   B2_CK(cudaFuncSetAttribute((const void*)b2::mlp::k_mlp_forward<b2::mlp::ArraySrc, b2::mlp::ArrayDst>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   B2_CK(cudaFuncSetAttribute((const void*)b2::mlp::k_mlp_forward<NnSrc, NnDst>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  if (dev >= 0 && dev < 64) done[dev] = true;
   return B2DEV_OK;
 }
 
