@@ -187,6 +187,73 @@ __device__ __forceinline__ double4 ldcg4(const double4* p) {
   return make_double4(lo.x, lo.y, hi.x, hi.y);
 }
 
+// ---- staging of a tile's column indices and FP32 coefficient planes (TMA) --
+
+// The FP32 sweeps copy each window of a tile's blocks into the warp's shared
+// memory with one-dimensional bulk copies (no cluster, no multicast), so
+// passes 1 and 2 read W and the column indices there instead of re-reading
+// them through L1.
+template <bool MIXED>
+__host__ __device__ constexpr bool stage_w() { return MIXED; }
+constexpr int kStageBar = 192;  // byte offset of the warp's staging barrier in its header
+constexpr int kStageSlack = 8;  // window planes hold gcap + slack blocks (16-byte aligned copy ranges)
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void stage_bar_init(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool stage_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the staging copies of the given phase.
+__device__ __noinline__ bool stage_wait(uint32_t bar, uint32_t parity, SolveControl* ctrl) {
+  if (stage_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  while (!stage_try_wait(bar, parity)) {
+    if (globaltimer_ns() - t0 > kBarrierLimitNs) { *(volatile int*)&ctrl->timeout = 1; return false; }
+  }
+  return true;
+}
+
+// Blocks [a0, a1) (multiples of 4: every copy starts on a 16-byte boundary and
+// is a multiple of 16 bytes) of the column indices and the nine FP32 planes
+// into the warp's window, completion counted on its barrier. One lane issues.
+template <typename real>
+__device__ __forceinline__ void stage_issue(uint32_t bar, uint32_t col_s, uint32_t w_s, int wstride, const int* col,
+                                            const real* W, long long kstride, int a0, int a1) {
+  const uint32_t bytes = (uint32_t)(a1 - a0) * 4u;
+  const uint32_t wbytes = (uint32_t)(a1 - a0) * (uint32_t)sizeof(real);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the window's previous reads are done
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes + 9u * wbytes)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(col_s),
+               "l"(col + a0), "r"(bytes), "r"(bar)
+               : "memory");
+#pragma unroll
+  for (int q = 0; q < 9; q++)
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     w_s + (uint32_t)q * (uint32_t)wstride * (uint32_t)sizeof(real)),
+                 "l"(W + q * kstride + a0), "r"(wbytes), "r"(bar)
+                 : "memory");
+}
+
+template <bool MIXED>
+__device__ __forceinline__ auto stage_src(const SolveArgs& a) {
+  if constexpr (MIXED) return a.W32;
+  else return a.W64;
+}
+
 // Per-sweep flags shared by the tile routine.
 struct SweepFlags {
   bool gs;        // Gauss-Seidel update of this sweep (false: merit-only pass)
@@ -199,12 +266,14 @@ struct SweepFlags {
 // each block (lane per block, coalesced plane loads).
 template <bool MIXED, typename real>
 __device__ __forceinline__ void load_chunk(const SolveArgs& a, int base, int ke, int lane,
-                                           int (&jj)[chunk_unroll<MIXED>()], real (&w)[chunk_unroll<MIXED>()][9]) {
+                                           int (&jj)[chunk_unroll<MIXED>()], real (&w)[chunk_unroll<MIXED>()][9],
+                                           const int* col_s, const real* w_s, int a0, int wstride) {
   constexpr int kChunkUnroll = chunk_unroll<MIXED>();
 #pragma unroll
   for (int u = 0; u < kChunkUnroll; u++) {
     const int k = base + u * kWarp + lane;
-    jj[u] = k < ke ? __ldg(a.col + k) : -1;
+    if constexpr (stage_w<MIXED>()) jj[u] = k < ke ? col_s[k - a0] : -1;
+    else jj[u] = k < ke ? __ldg(a.col + k) : -1;
   }
 #pragma unroll
   for (int u = 0; u < kChunkUnroll; u++) {
@@ -212,7 +281,8 @@ __device__ __forceinline__ void load_chunk(const SolveArgs& a, int base, int ke,
 #pragma unroll
     for (int q = 0; q < 9; q++) {
       if (k < ke) {
-        if constexpr (MIXED) w[u][q] = __ldg(a.W32 + q * a.kstride + k);
+        if constexpr (stage_w<MIXED>()) w[u][q] = w_s[q * wstride + k - a0];
+        else if constexpr (MIXED) w[u][q] = __ldg(a.W32 + q * a.kstride + k);
         else w[u][q] = __ldg(a.W64 + q * a.kstride + k);
       } else {
         w[u][q] = real(0);
@@ -237,13 +307,17 @@ __device__ __forceinline__ void load_r(const SolveArgs& a, int buf, int j, real&
 template <bool MIXED>
 __host__ __device__ constexpr size_t solve_warp_smem(int gcap) {
   return (size_t)kTileHeader +
-         (size_t)(3 * kWarp * chunk_unroll<MIXED>() + 3 * gcap) * (MIXED ? sizeof(float) : sizeof(double));
+         (size_t)(3 * kWarp * chunk_unroll<MIXED>() + 3 * gcap) * (MIXED ? sizeof(float) : sizeof(double)) +
+         (stage_w<MIXED>() ? (size_t)(gcap + kStageSlack) * (4 + 9 * (MIXED ? sizeof(float) : sizeof(double))) : 0);
 }
 // shared memory of a warp: fixed part and bytes per staged block
 template <bool MIXED>
 __host__ __device__ constexpr size_t solve_smem_fixed() { return solve_warp_smem<MIXED>(0); }
 template <bool MIXED>
-__host__ __device__ constexpr size_t solve_smem_per_block() { return 3 * (MIXED ? sizeof(float) : sizeof(double)); }
+__host__ __device__ constexpr size_t solve_smem_per_block() {
+  return 3 * (MIXED ? sizeof(float) : sizeof(double)) +
+         (stage_w<MIXED>() ? 4 + 9 * (MIXED ? sizeof(float) : sizeof(double)) : 0);
+}
 
 // One tile of up to 32 consecutive rows of one colour, owned by one warp.
 //
@@ -265,7 +339,7 @@ __host__ __device__ constexpr size_t solve_smem_per_block() { return 3 * (MIXED 
 // the solve has stopped.
 template <bool MIXED>
 __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags& f, int r0, int nr, int cs, int ce,
-                                           int s, int rin, int rout, int prob, unsigned char* wsm,
+                                           int s, int rin, int rout, int prob, unsigned char* wsm, uint32_t& phase,
                                            double& errup, double& errlo, double& mnum) {
   typedef typename std::conditional<MIXED, float, double>::type real;
   constexpr int kChunkUnroll = chunk_unroll<MIXED>();
@@ -274,12 +348,23 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   real(*mst)[kSlots] = reinterpret_cast<real(*)[kSlots]>(wsm + kTileHeader);          // [3][kSlots]
   real* gst = reinterpret_cast<real*>(wsm + kTileHeader + 3 * kSlots * sizeof(real));  // [3][gcap]
   const int gcap = a.gcap;
+  const int wstride = gcap + kStageSlack;
+  int* col_s = reinterpret_cast<int*>(gst + 3 * gcap);                                   // [wstride] (staged)
+  real* w_s = reinterpret_cast<real*>(col_s + wstride);                                  // [9][wstride] (staged)
+  const uint32_t bar = smem_addr(wsm + kStageBar);
   const int lane = threadIdx.x & (kWarp - 1);
   const int n = a.n;
   const bool own = lane < nr;
   const int p = r0 + lane;
   if (lane <= nr) tp[lane] = __ldg(a.rowptr + r0 + lane);
   if (lane == 0 && nr == kWarp) tp[kWarp] = __ldg(a.rowptr + r0 + kWarp);
+  if constexpr (stage_w<MIXED>()) {  // window 0 on its way while the row data is read
+    __syncwarp();
+    const int kb0 = tp[0], ke0 = tp[nr];
+    if (lane == 0 && ke0 > kb0)
+      stage_issue(bar, smem_addr(col_s), smem_addr(w_s), wstride, a.col, stage_src<MIXED>(a), a.kstride, kb0 & ~3,
+                  (min(ke0, kb0 + gcap) + 3) & ~3);
+  }
   bool ok = true;
   if (own) ok = wait_at_least(a.done + p, s, a.ctrl);  // this row's previous sweep is complete
 
@@ -312,11 +397,20 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
 
   for (int win = 0; win < nwin; win++) {
     const int wb = kb + win * gcap, we = min(ke, wb + gcap);
+    const int a0 = wb & ~3;
+    if constexpr (stage_w<MIXED>()) {
+      if (we > wb) {
+        if (win > 0 && lane == 0)
+          stage_issue(bar, smem_addr(col_s), smem_addr(w_s), wstride, a.col, stage_src<MIXED>(a), a.kstride, a0, (we + 3) & ~3);
+        ok = stage_wait(bar, phase, a.ctrl) && ok;
+        phase ^= 1u;
+      }
+    }
     // ---- pass 1: previous-sweep values (merit products, later neighbours)
     for (int base = wb; base < we; base += kSlots) {
       int jj[kChunkUnroll];
       real w[kChunkUnroll][9];
-      load_chunk<MIXED, real>(a, base, we, lane, jj, w);
+      load_chunk<MIXED, real>(a, base, we, lane, jj, w, col_s, w_s, a0, wstride);
 #pragma unroll
       for (int u = 0; u < kChunkUnroll; u++) {
         const int j = jj[u];
@@ -371,14 +465,17 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
       for (int u = 0; u < kChunkUnroll; u++) {
         const int k = base + u * kWarp + lane;
         if (k < we) {
-          const int j = __ldg(a.col + k);
+          int j;
+          if constexpr (stage_w<MIXED>()) j = col_s[k - a0];
+          else j = __ldg(a.col + k);
           const bool earlier = f.backward ? (j >= ce) : (j < cs);
           if (earlier) {
             ok = wait_at_least(a.done + j, s + 1, a.ctrl) && ok;
             real Wk[9];
 #pragma unroll
             for (int q = 0; q < 9; q++) {
-              if constexpr (MIXED) Wk[q] = __ldg(a.W32 + q * a.kstride + k);
+              if constexpr (stage_w<MIXED>()) Wk[q] = w_s[q * wstride + k - a0];
+              else if constexpr (MIXED) Wk[q] = __ldg(a.W32 + q * a.kstride + k);
               else Wk[q] = __ldg(a.W64 + q * a.kstride + k);
             }
             real rn0, rn1, rn2;
@@ -554,6 +651,11 @@ __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(SolveArgs a) {
   volatile int* stop = &a.ctrl->stop;
   const int T = a.ntiles;
   if (blockIdx.x == 0 && threadIdx.x == 0) a.ctrl->t_start = globaltimer_ns();
+  uint32_t phase = 0;  // parity of the warp's staging barrier
+  if constexpr (stage_w<MIXED>()) {
+    if (lane == 0) stage_bar_init(smem_addr(wsm + kStageBar));
+    __syncwarp();
+  }
 
   while (true) {
     unsigned t = 0;
@@ -582,7 +684,7 @@ __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(SolveArgs a) {
     const int rin = (a.in + s) % 3;       // iterate s-1
     const int rout = (a.in + s + 1) % 3;  // iterate s
     double errup = 0.0, errlo = 0.0, mnum = 0.0;
-    if (!solve_tile<MIXED>(a, f, ti.x, nr, ti.z, ti.w, s, rin, rout, prob, wsm, errup, errlo, mnum)) break;
+    if (!solve_tile<MIXED>(a, f, ti.x, nr, ti.z, ti.w, s, rin, rout, prob, wsm, phase, errup, errlo, mnum)) break;
 #pragma unroll
     for (int d = 16; d >= 1; d >>= 1) {
       errup += __shfl_down_sync(0xffffffffu, errup, d);
