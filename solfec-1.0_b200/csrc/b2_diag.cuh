@@ -27,14 +27,15 @@ __device__ __forceinline__ int lu3_solve(double* a, double* b) {
 #pragma unroll
   for (int j = 0; j < 3; j++) {
     int p = j;
-    double amax = fabs(a[j + 3 * j]);
+    double apiv = a[j + 3 * j];  // a[p + 3 j], tracked so that no index is a runtime value
+    double amax = fabs(apiv);
 #pragma unroll
     for (int i = j + 1; i < 3; i++) {
       double v = fabs(a[i + 3 * j]);
-      if (v > amax) { amax = v; p = i; }
+      if (v > amax) { amax = v; p = i; apiv = a[i + 3 * j]; }
     }
     ipiv[j] = p;
-    if (a[p + 3 * j] != 0.0) {
+    if (apiv != 0.0) {
       if (p != j) {
 #pragma unroll
         for (int c = 0; c < 3; c++) {
@@ -376,32 +377,40 @@ __device__ __forceinline__ int diagonal_solve(int solver, const ContactParams& c
   return 0;
 }
 
-// State of one row handed to the out-of-line solvers (rare path only, so the
-// arrays of the common path stay in registers).
+// State of one row handed to the out-of-line path (rare: a failed first
+// attempt or a solver other than SSN). Only this copy has its address taken,
+// so the common path keeps the row's parameters and arrays in registers.
 struct RowState {
-  double W[9], B[3], V[3], U[3], R[3];
+  ContactParams cp;
+  double W[9], B[3], V[3], U[3], R[3], R0[3];
 };
 
-__device__ __noinline__ int diagonal_solve_slow(int solver, const ContactParams& cp, double epsilon, int maxiter,
-                                                double rho, RowState& st) {
-  return diagonal_solve(solver, cp, epsilon, maxiter, rho, st.W, st.B, st.V, st.U, st.R);
-}
-
-// FAILURE_CONTINUE fallback chain (bgs.c:976-1003): the other solvers in the
-// order SSN, PG, DSF, PN, each from the previous reaction R0; if all fail the
-// previous reaction is kept (U keeps the last attempt's value).
-__device__ __noinline__ void fallback_chain(int solver, const ContactParams& cp, double epsilon, int maxiter,
-                                            double rho, RowState& st, const double* R0) {
-  const int chain[4] = {DS_SEMISMOOTH_NEWTON, DS_PROJECTED_GRADIENT, DS_DE_SAXCE_FENG, DS_PROJECTED_NEWTON};
-  int it = maxiter;
-  for (int t = 0; t < 4; t++) {
-    if (chain[t] != solver) {
-      st.R[0] = R0[0]; st.R[1] = R0[1]; st.R[2] = R0[2];
-      it = diagonal_solve(chain[t], cp, epsilon, maxiter, rho, st.W, st.B, st.V, st.U, st.R);
-      if (it < maxiter && it >= 0) break;
-    }
+// Everything after a failed SSN attempt (it = its return value), or the whole
+// solve for the other solvers (bgs.c:969-1013). FAILURE_CONTINUE runs the
+// fallback chain (bgs.c:976-1003): the other solvers in the order SSN, PG, DSF,
+// PN, each from the previous reaction R0; if all fail the previous reaction is
+// kept (U keeps the last attempt's value). Returns the failure kind of the
+// first attempt: 0 none, 1 diverged (iterations >= maxiter), 2 failed (< 0).
+__device__ __noinline__ int diagonal_solve_row_slow(int solver, int failure, double epsilon, int maxiter, double rho,
+                                                    int it, RowState& st) {
+  if (solver != DS_SEMISMOOTH_NEWTON) {
+    it = diagonal_solve(solver, st.cp, epsilon, maxiter, rho, st.W, st.B, st.V, st.U, st.R);
+    if (it < maxiter && it >= 0) return 0;
   }
-  if (it >= maxiter || it < 0) { st.R[0] = R0[0]; st.R[1] = R0[1]; st.R[2] = R0[2]; }
+  const int kind = it < 0 ? 2 : 1;
+  if (failure == FAIL_CONTINUE) {
+    const int chain[4] = {DS_SEMISMOOTH_NEWTON, DS_PROJECTED_GRADIENT, DS_DE_SAXCE_FENG, DS_PROJECTED_NEWTON};
+    it = maxiter;
+    for (int t = 0; t < 4; t++) {
+      if (chain[t] != solver) {
+        st.R[0] = st.R0[0]; st.R[1] = st.R0[1]; st.R[2] = st.R0[2];
+        it = diagonal_solve(chain[t], st.cp, epsilon, maxiter, rho, st.W, st.B, st.V, st.U, st.R);
+        if (it < maxiter && it >= 0) break;
+      }
+    }
+    if (it >= maxiter || it < 0) { st.R[0] = st.R0[0]; st.R[1] = st.R0[1]; st.R[2] = st.R0[2]; }
+  }
+  return kind;
 }
 
 // Diagonal solve of one row with the reference's failure handling
@@ -410,27 +419,20 @@ __device__ __noinline__ void fallback_chain(int solver, const ContactParams& cp,
 __device__ __forceinline__ int diagonal_solve_row(int solver, int failure, const ContactParams& cp, double epsilon,
                                                   int maxiter, double rho, const double* W, const double* B,
                                                   const double* V, double* U, double* R) {
-  const double R0[3] = {R[0], R[1], R[2]};
-  int it;
+  const double r0 = R[0], r1 = R[1], r2 = R[2];
+  int it = -1;
   if (solver == DS_SEMISMOOTH_NEWTON) {
     it = semismooth_newton(cp, epsilon, maxiter, rho, W, B, V, U, R);
     if (it < maxiter && it >= 0) return 0;
   }
   RowState st;
+  st.cp = cp;
 #pragma unroll
   for (int q = 0; q < 9; q++) st.W[q] = W[q];
 #pragma unroll
   for (int q = 0; q < 3; q++) { st.B[q] = B[q]; st.V[q] = V[q]; st.U[q] = U[q]; st.R[q] = R[q]; }
-  if (solver != DS_SEMISMOOTH_NEWTON) {
-    it = diagonal_solve_slow(solver, cp, epsilon, maxiter, rho, st);
-    if (it < maxiter && it >= 0) {
-#pragma unroll
-      for (int q = 0; q < 3; q++) { U[q] = st.U[q]; R[q] = st.R[q]; }
-      return 0;
-    }
-  }
-  const int kind = it < 0 ? 2 : 1;
-  if (failure == FAIL_CONTINUE) fallback_chain(solver, cp, epsilon, maxiter, rho, st, R0);
+  st.R0[0] = r0; st.R0[1] = r1; st.R0[2] = r2;
+  const int kind = diagonal_solve_row_slow(solver, failure, epsilon, maxiter, rho, it, st);
 #pragma unroll
   for (int q = 0; q < 3; q++) { U[q] = st.U[q]; R[q] = st.R[q]; }
   return kind;

@@ -146,9 +146,10 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 }
 
 // Bounded wait until *p >= need. Returns false when the solve has stopped or
-// the wait ran out (the timeout is recorded in ctrl).
-__device__ __noinline__ bool wait_at_least(const int* p, int need, SolveControl* ctrl) {
-  if (ld_acquire(p) >= need) return true;
+// the wait ran out (the timeout is recorded in ctrl). The first check is
+// inlined; only the spin is out of line (a call site saves live registers, so
+// the common case must not be a call).
+__device__ __noinline__ bool wait_at_least_spin(const int* p, int need, SolveControl* ctrl) {
   const uint64_t t0 = globaltimer_ns();
   volatile int* stop = &ctrl->stop;
   volatile int* to = &ctrl->timeout;
@@ -159,12 +160,16 @@ __device__ __noinline__ bool wait_at_least(const int* p, int need, SolveControl*
   }
   return true;
 }
+__device__ __forceinline__ bool wait_at_least(const int* p, int need, SolveControl* ctrl) {
+  if (ld_acquire(p) >= need) return true;
+  return wait_at_least_spin(p, need, ctrl);
+}
 
 // Gate of a tile of sweep s >= 2 of one problem: 1 = run (the decision after
 // sweep s-2 is to continue), 2 = skip (the problem has taken its final
 // decision, so later sweeps are discarded), 0 = the solve is ending or the
 // bounded wait gave up.
-__device__ __noinline__ int gate_wait(const int* decided_s2, const int* pstop, SolveControl* ctrl) {
+__device__ __noinline__ int gate_wait_spin(const int* decided_s2, const int* pstop, SolveControl* ctrl) {
   const uint64_t t0 = globaltimer_ns();
   volatile int* stop = &ctrl->stop;
   volatile int* to = &ctrl->timeout;
@@ -177,6 +182,10 @@ __device__ __noinline__ int gate_wait(const int* decided_s2, const int* pstop, S
     if (globaltimer_ns() - t0 > kBarrierLimitNs) { *to = 1; return 0; }
     __nanosleep(64);
   }
+}
+__device__ __forceinline__ int gate_wait(const int* decided_s2, const int* pstop, SolveControl* ctrl) {
+  if (ld_acquire(decided_s2) == DECIDE_CONTINUE) return 1;
+  return gate_wait_spin(decided_s2, pstop, ctrl);
 }
 
 // 32-byte load that bypasses L1 (reaction buffers are rewritten by other SMs
@@ -217,13 +226,16 @@ __device__ __forceinline__ bool stage_try_wait(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait for the staging copies of the given phase.
-__device__ __noinline__ bool stage_wait(uint32_t bar, uint32_t parity, SolveControl* ctrl) {
-  if (stage_try_wait(bar, parity)) return true;
+__device__ __noinline__ bool stage_wait_spin(uint32_t bar, uint32_t parity, SolveControl* ctrl) {
   const uint64_t t0 = globaltimer_ns();
   while (!stage_try_wait(bar, parity)) {
     if (globaltimer_ns() - t0 > kBarrierLimitNs) { *(volatile int*)&ctrl->timeout = 1; return false; }
   }
   return true;
+}
+__device__ __forceinline__ bool stage_wait(uint32_t bar, uint32_t parity, SolveControl* ctrl) {
+  if (stage_try_wait(bar, parity)) return true;
+  return stage_wait_spin(bar, parity, ctrl);
 }
 
 // Blocks [a0, a1) (multiples of 4: every copy starts on a 16-byte boundary and
@@ -641,7 +653,7 @@ __device__ __noinline__ void finalize_sweep(const SolveArgs& a, int prob, int s)
 // list-order colouring a sweep has about six levels of ~1.5k tiles each, so
 // 1,776 resident warps hold a whole level in one wave.
 template <bool MIXED>
-__global__ void __launch_bounds__(kSolveThreads, 6) k_solve(SolveArgs a) {
+__global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constant__ SolveArgs a) {
   extern __shared__ __align__(16) unsigned char solve_smem[];
   const int warp = threadIdx.x / kWarp;
   const int lane = threadIdx.x & (kWarp - 1);
