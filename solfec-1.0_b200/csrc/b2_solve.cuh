@@ -272,6 +272,7 @@ struct SweepFlags {
   bool merit;     // evaluate the merit of the input iterate
   bool u_merit;   // hand the merit U to the diagonal solver
   bool backward;  // colours in reverse order
+  bool prev_done; // every row of the problem has completed the previous sweep (its decision is taken)
 };
 
 // Loads of one 32-block chunk: column indices and the nine coefficients of
@@ -378,7 +379,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
                   (min(ke0, kb0 + gcap) + 3) & ~3);
   }
   bool ok = true;
-  if (own) ok = wait_at_least(a.done + p, s, a.ctrl);  // this row's previous sweep is complete
+  if (own && !f.prev_done) ok = wait_at_least(a.done + p, s, a.ctrl);  // this row's previous sweep is complete
 
   double B[3] = {0.0, 0.0, 0.0}, W[9], Rold[3] = {0.0, 0.0, 0.0}, ag[3], am[3] = {0.0, 0.0, 0.0};
   double V[3] = {0.0, 0.0, 0.0};
@@ -429,7 +430,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
         const int slot = u * kWarp + lane;
         if (j >= 0) {
           const bool earlier = f.backward ? (j >= ce) : (j < cs);
-          ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
+          if (!f.prev_done) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
           real ro0, ro1, ro2;
           load_r<MIXED, real>(a, rin, j, ro0, ro1, ro2);
           const real* Wk = w[u];
@@ -681,6 +682,7 @@ __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constan
     f.merit = merit_mode;
     f.u_merit = merit_mode && (s >= 1 || a.u0_from_merit);
     f.backward = a.reverse && ((a.iter0 + s) & 1);
+    f.prev_done = s == 0;
     const int tile = f.backward ? T - 1 - w : w;
     const int4 ti = __ldg(a.tiles + tile);  // first row, rows | problem << 6, colour bounds
     const int prob = ti.y >> 6, nr = ti.y & 63;
@@ -692,6 +694,12 @@ __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constan
       gate = __shfl_sync(0xffffffffu, gate, 0);
       if (gate == 0) break;
       if (gate == 2) continue;  // this problem has finished: its later sweeps are not run
+    }
+    if (s >= 1) {  // the decision after sweep s-1 is taken only once all its tiles have completed (and
+                   // released their rows): then no neighbour needs its own wait in pass 1
+      int pd = 0;
+      if (lane == 0) pd = ld_acquire((const int*)decided + s - 1) != DECIDE_NONE;
+      f.prev_done = __shfl_sync(0xffffffffu, pd, 0) != 0;
     }
     const int rin = (a.in + s) % 3;       // iterate s-1
     const int rout = (a.in + s + 1) % 3;  // iterate s
