@@ -198,10 +198,11 @@ __device__ __forceinline__ double4 ldcg4(const double4* p) {
 
 // ---- staging of a tile's column indices and FP32 coefficient planes (TMA) --
 
-// The FP32 sweeps copy each window of a tile's blocks into the warp's shared
-// memory with one-dimensional bulk copies (no cluster, no multicast), so
-// passes 1 and 2 read W and the column indices there instead of re-reading
-// them through L1.
+// Each window of a tile's blocks is copied into the warp's shared memory with
+// one-dimensional bulk copies (no cluster, no multicast): the column indices
+// always, the nine W planes in the FP32 sweeps (at 72 bytes a block the FP64
+// planes would leave windows too small to hold a tile). Passes 1 and 2 read
+// them there instead of through L1.
 template <bool MIXED>
 __host__ __device__ constexpr bool stage_w() { return MIXED; }
 constexpr int kStageBar = 192;  // byte offset of the warp's staging barrier in its header
@@ -239,19 +240,21 @@ __device__ __forceinline__ bool stage_wait(uint32_t bar, uint32_t parity, SolveC
 }
 
 // Blocks [a0, a1) (multiples of 4: every copy starts on a 16-byte boundary and
-// is a multiple of 16 bytes) of the column indices and the nine FP32 planes
-// into the warp's window, completion counted on its barrier. One lane issues.
-template <typename real>
+// is a multiple of 16 bytes) of the column indices and, with WITHW, the nine W
+// planes into the warp's window, completion counted on its barrier. One lane
+// issues.
+template <bool WITHW, typename real>
 __device__ __forceinline__ void stage_issue(uint32_t bar, uint32_t col_s, uint32_t w_s, int wstride, const int* col,
                                             const real* W, long long kstride, int a0, int a1) {
   const uint32_t bytes = (uint32_t)(a1 - a0) * 4u;
-  const uint32_t wbytes = (uint32_t)(a1 - a0) * (uint32_t)sizeof(real);
+  const uint32_t wbytes = WITHW ? (uint32_t)(a1 - a0) * (uint32_t)sizeof(real) : 0u;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the window's previous reads are done
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes + 9u * wbytes)
                : "memory");
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(col_s),
                "l"(col + a0), "r"(bytes), "r"(bar)
                : "memory");
+  if constexpr (WITHW)
 #pragma unroll
   for (int q = 0; q < 9; q++)
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -285,8 +288,7 @@ __device__ __forceinline__ void load_chunk(const SolveArgs& a, int base, int ke,
 #pragma unroll
   for (int u = 0; u < kChunkUnroll; u++) {
     const int k = base + u * kWarp + lane;
-    if constexpr (stage_w<MIXED>()) jj[u] = k < ke ? col_s[k - a0] : -1;
-    else jj[u] = k < ke ? __ldg(a.col + k) : -1;
+    jj[u] = k < ke ? col_s[k - a0] : -1;
   }
 #pragma unroll
   for (int u = 0; u < kChunkUnroll; u++) {
@@ -321,7 +323,7 @@ template <bool MIXED>
 __host__ __device__ constexpr size_t solve_warp_smem(int gcap) {
   return (size_t)kTileHeader +
          (size_t)(3 * kWarp * chunk_unroll<MIXED>() + 3 * gcap) * (MIXED ? sizeof(float) : sizeof(double)) +
-         (stage_w<MIXED>() ? (size_t)(gcap + kStageSlack) * (4 + 9 * (MIXED ? sizeof(float) : sizeof(double))) : 0);
+         (size_t)(gcap + kStageSlack) * (4 + (stage_w<MIXED>() ? 9 * (MIXED ? sizeof(float) : sizeof(double)) : 0));
 }
 // shared memory of a warp: fixed part and bytes per staged block
 template <bool MIXED>
@@ -329,7 +331,7 @@ __host__ __device__ constexpr size_t solve_smem_fixed() { return solve_warp_smem
 template <bool MIXED>
 __host__ __device__ constexpr size_t solve_smem_per_block() {
   return 3 * (MIXED ? sizeof(float) : sizeof(double)) +
-         (stage_w<MIXED>() ? 4 + 9 * (MIXED ? sizeof(float) : sizeof(double)) : 0);
+         4 + (stage_w<MIXED>() ? 9 * (MIXED ? sizeof(float) : sizeof(double)) : 0);
 }
 
 // One tile of up to 32 consecutive rows of one colour, owned by one warp.
@@ -371,11 +373,11 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   const int p = r0 + lane;
   if (lane <= nr) tp[lane] = __ldg(a.rowptr + r0 + lane);
   if (lane == 0 && nr == kWarp) tp[kWarp] = __ldg(a.rowptr + r0 + kWarp);
-  if constexpr (stage_w<MIXED>()) {  // window 0 on its way while the row data is read
+  {  // window 0 on its way while the row data is read
     __syncwarp();
     const int kb0 = tp[0], ke0 = tp[nr];
     if (lane == 0 && ke0 > kb0)
-      stage_issue(bar, smem_addr(col_s), smem_addr(w_s), wstride, a.col, stage_src<MIXED>(a), a.kstride, kb0 & ~3,
+      stage_issue<stage_w<MIXED>()>(bar, smem_addr(col_s), smem_addr(w_s), wstride, a.col, stage_src<MIXED>(a), a.kstride, kb0 & ~3,
                   (min(ke0, kb0 + gcap) + 3) & ~3);
   }
   bool ok = true;
@@ -411,10 +413,10 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   for (int win = 0; win < nwin; win++) {
     const int wb = kb + win * gcap, we = min(ke, wb + gcap);
     const int a0 = wb & ~3;
-    if constexpr (stage_w<MIXED>()) {
+    {
       if (we > wb) {
         if (win > 0 && lane == 0)
-          stage_issue(bar, smem_addr(col_s), smem_addr(w_s), wstride, a.col, stage_src<MIXED>(a), a.kstride, a0, (we + 3) & ~3);
+          stage_issue<stage_w<MIXED>()>(bar, smem_addr(col_s), smem_addr(w_s), wstride, a.col, stage_src<MIXED>(a), a.kstride, a0, (we + 3) & ~3);
         ok = stage_wait(bar, phase, a.ctrl) && ok;
         phase ^= 1u;
       }
@@ -478,9 +480,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
       for (int u = 0; u < kChunkUnroll; u++) {
         const int k = base + u * kWarp + lane;
         if (k < we) {
-          int j;
-          if constexpr (stage_w<MIXED>()) j = col_s[k - a0];
-          else j = __ldg(a.col + k);
+          const int j = col_s[k - a0];
           const bool earlier = f.backward ? (j >= ce) : (j < cs);
           if (earlier) {
             ok = wait_at_least(a.done + j, s + 1, a.ctrl) && ok;
@@ -665,10 +665,8 @@ __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constan
   const int T = a.ntiles;
   if (blockIdx.x == 0 && threadIdx.x == 0) a.ctrl->t_start = globaltimer_ns();
   uint32_t phase = 0;  // parity of the warp's staging barrier
-  if constexpr (stage_w<MIXED>()) {
-    if (lane == 0) stage_bar_init(smem_addr(wsm + kStageBar));
-    __syncwarp();
-  }
+  if (lane == 0) stage_bar_init(smem_addr(wsm + kStageBar));
+  __syncwarp();
 
   while (true) {
     unsigned t = 0;
