@@ -317,12 +317,11 @@ __device__ __forceinline__ void load_r(const SolveArgs& a, int buf, int j, real&
   }
 }
 
-// shared memory of one warp of k_solve: tile row offsets, merit products of
-// one chunk, and the Gauss-Seidel products of up to gcap blocks of the tile
+// shared memory of one warp of k_solve: tile row offsets, the products of up
+// to gcap blocks of the tile, and the staged column indices (and FP32 W)
 template <bool MIXED>
 __host__ __device__ constexpr size_t solve_warp_smem(int gcap) {
-  return (size_t)kTileHeader +
-         (size_t)(3 * kWarp * chunk_unroll<MIXED>() + 3 * gcap) * (MIXED ? sizeof(float) : sizeof(double)) +
+  return (size_t)kTileHeader + (size_t)(3 * gcap) * (MIXED ? sizeof(float) : sizeof(double)) +
          (size_t)(gcap + kStageSlack) * (4 + (stage_w<MIXED>() ? 9 * (MIXED ? sizeof(float) : sizeof(double)) : 0));
 }
 // shared memory of a warp: fixed part and bytes per staged block
@@ -359,9 +358,8 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   typedef typename std::conditional<MIXED, float, double>::type real;
   constexpr int kChunkUnroll = chunk_unroll<MIXED>();
   constexpr int kSlots = kWarp * kChunkUnroll;
-  int* tp = reinterpret_cast<int*>(wsm);                                              // [kWarp + 1]
-  real(*mst)[kSlots] = reinterpret_cast<real(*)[kSlots]>(wsm + kTileHeader);          // [3][kSlots]
-  real* gst = reinterpret_cast<real*>(wsm + kTileHeader + 3 * kSlots * sizeof(real));  // [3][gcap]
+  int* tp = reinterpret_cast<int*>(wsm);                     // [kWarp + 1]
+  real* gst = reinterpret_cast<real*>(wsm + kTileHeader);     // [3][gcap] products W_ij R_j of the window
   const int gcap = a.gcap;
   const int wstride = gcap + kStageSlack;
   int* col_s = reinterpret_cast<int*>(gst + 3 * gcap);                                   // [wstride] (staged)
@@ -421,7 +419,8 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
         phase ^= 1u;
       }
     }
-    // ---- pass 1: previous-sweep values (merit products, later neighbours)
+    // ---- pass 1: previous-sweep values. W_ij R_j^(s-1) of every block (the
+    // merit's products, and the Gauss-Seidel products of later neighbours)
     for (int base = wb; base < we; base += kSlots) {
       int jj[kChunkUnroll];
       real w[kChunkUnroll][9];
@@ -429,39 +428,32 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
 #pragma unroll
       for (int u = 0; u < kChunkUnroll; u++) {
         const int j = jj[u];
-        const int slot = u * kWarp + lane;
         if (j >= 0) {
           const bool earlier = f.backward ? (j >= ce) : (j < cs);
-          if (!f.prev_done) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
-          real ro0, ro1, ro2;
-          load_r<MIXED, real>(a, rin, j, ro0, ro1, ro2);
-          const real* Wk = w[u];
-          real m0 = 0, m1 = 0, m2 = 0;
           if (f.merit || (f.gs && !earlier)) {
-            m0 = Wk[0] * ro0 + Wk[3] * ro1 + Wk[6] * ro2;
-            m1 = Wk[1] * ro0 + Wk[4] * ro1 + Wk[7] * ro2;
-            m2 = Wk[2] * ro0 + Wk[5] * ro1 + Wk[8] * ro2;
-          }
-          if (f.merit) { mst[0][slot] = m0; mst[1][slot] = m1; mst[2][slot] = m2; }
-          if (f.gs && !earlier) {
-            const int g = base + slot - wb;
-            gst[g] = m0; gst[gcap + g] = m1; gst[2 * gcap + g] = m2;
+            if (!f.prev_done) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
+            real ro0, ro1, ro2;
+            load_r<MIXED, real>(a, rin, j, ro0, ro1, ro2);
+            const real* Wk = w[u];
+            const int g = base + u * kWarp + lane - wb;
+            gst[g] = Wk[0] * ro0 + Wk[3] * ro1 + Wk[6] * ro2;
+            gst[gcap + g] = Wk[1] * ro0 + Wk[4] * ro1 + Wk[7] * ro2;
+            gst[2 * gcap + g] = Wk[2] * ro0 + Wk[5] * ro1 + Wk[8] * ro2;
           }
         }
       }
-      __syncwarp();
-      if (f.merit) {  // each row adds its own merit products, in list order
-        const int lo = mb > base ? mb : base;
-        const int cend = base + kSlots < we ? base + kSlots : we;  // this chunk, inside this window
-        const int hi = me < cend ? me : cend;
-        for (int k = lo; k < hi; k++) {
-          const int slot = k - base;
-          am[0] = am[0] + (double)mst[0][slot];
-          am[1] = am[1] + (double)mst[1][slot];
-          am[2] = am[2] + (double)mst[2][slot];
-        }
+    }
+    __syncwarp();
+    if (f.merit) {  // each row adds its own merit products, in list order
+      const int lo = mb > wb ? mb : wb;
+      const int hi = me < we ? me : we;
+      for (int k = lo; k < hi; k++) {
+        const int g = k - wb;
+        am[0] = am[0] + (double)gst[g];
+        am[1] = am[1] + (double)gst[gcap + g];
+        am[2] = am[2] + (double)gst[2 * gcap + g];
       }
-      __syncwarp();
+      __syncwarp();  // pass 2 overwrites the slots of earlier neighbours
     }
     // ---- merit term of each row (mrf.c:81-87), once its U is complete
     if (win == nwin - 1 && f.merit && own) {
