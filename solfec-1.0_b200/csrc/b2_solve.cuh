@@ -49,10 +49,11 @@ namespace b2 {
 
 constexpr int kSolveThreads = 64;
 constexpr int kSolveWarps = kSolveThreads / kWarp;
-// 32-block chunks whose loads are issued together: 2 in FP64 (more would
-// spill under the 168-register cap), 3 with the FP32 planes (measured fastest)
+// 32-block chunks whose loads are issued together: 2 in FP64 (more would spill
+// under the 168-register cap); 1 in the FP32 sweeps, whose pass 1 reads only
+// shared memory (staged W, gathered reactions) -- measured fastest
 template <bool MIXED>
-__host__ __device__ constexpr int chunk_unroll() { return MIXED ? 3 : 2; }
+__host__ __device__ constexpr int chunk_unroll() { return MIXED ? 1 : 2; }
 constexpr int kTileHeader = 256;                     // bytes of per-warp shared memory before the staging
 constexpr uint64_t kBarrierLimitNs = 2000000000ull;  // 2 s per bounded wait
 
@@ -317,11 +318,36 @@ __device__ __forceinline__ void load_r(const SolveArgs& a, int buf, int j, real&
   }
 }
 
-// shared memory of one warp of k_solve: tile row offsets, the products of up
-// to gcap blocks of the tile, and the staged column indices (and FP32 W)
+// 16-byte asynchronous copy global -> shared memory, cached in L2 only (the
+// reaction buffers are rewritten by other SMs while the kernel runs, so a line
+// cached in L1 could be stale).
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+// Completion of this thread's asynchronous copies (visible to the thread).
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// The FP32 sweeps gather the previous-sweep reactions of a whole window with
+// asynchronous copies before pass 1 (one round trip instead of one per
+// chunk). The FP64 sweeps load them in pass 1, next to their uncoalesced W
+// loads, which set the chain there (measured: gathering first is slower).
+template <bool MIXED>
+__host__ __device__ constexpr bool gather_r() { return MIXED; }
+
+// Bytes per block of the window's products: FP32 sweeps, one float4 slot that
+// first receives the gathered reaction and is then overwritten by the product
+// (in place, by the lane that gathered it); FP64 sweeps, three planes of
+// doubles (conflict-free row sums; measured faster than 32-byte slots).
+template <bool MIXED>
+__host__ __device__ constexpr size_t slot_bytes() { return MIXED ? 16 : 24; }
+
+// shared memory of one warp of k_solve: tile row offsets, one slot per block of
+// the window, and the staged column indices (and FP32 W)
 template <bool MIXED>
 __host__ __device__ constexpr size_t solve_warp_smem(int gcap) {
-  return (size_t)kTileHeader + (size_t)(3 * gcap) * (MIXED ? sizeof(float) : sizeof(double)) +
+  return (size_t)kTileHeader + (size_t)gcap * slot_bytes<MIXED>() +
          (size_t)(gcap + kStageSlack) * (4 + (stage_w<MIXED>() ? 9 * (MIXED ? sizeof(float) : sizeof(double)) : 0));
 }
 // shared memory of a warp: fixed part and bytes per staged block
@@ -329,8 +355,7 @@ template <bool MIXED>
 __host__ __device__ constexpr size_t solve_smem_fixed() { return solve_warp_smem<MIXED>(0); }
 template <bool MIXED>
 __host__ __device__ constexpr size_t solve_smem_per_block() {
-  return 3 * (MIXED ? sizeof(float) : sizeof(double)) +
-         4 + (stage_w<MIXED>() ? 9 * (MIXED ? sizeof(float) : sizeof(double)) : 0);
+  return slot_bytes<MIXED>() + 4 + (stage_w<MIXED>() ? 9 * (MIXED ? sizeof(float) : sizeof(double)) : 0);
 }
 
 // One tile of up to 32 consecutive rows of one colour, owned by one warp.
@@ -358,11 +383,25 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   typedef typename std::conditional<MIXED, float, double>::type real;
   constexpr int kChunkUnroll = chunk_unroll<MIXED>();
   constexpr int kSlots = kWarp * kChunkUnroll;
-  int* tp = reinterpret_cast<int*>(wsm);                     // [kWarp + 1]
-  real* gst = reinterpret_cast<real*>(wsm + kTileHeader);     // [3][gcap] products W_ij R_j of the window
   const int gcap = a.gcap;
   const int wstride = gcap + kStageSlack;
-  int* col_s = reinterpret_cast<int*>(gst + 3 * gcap);                                   // [wstride] (staged)
+  int* tp = reinterpret_cast<int*>(wsm);                        // [kWarp + 1]
+  float4* slot = reinterpret_cast<float4*>(wsm + kTileHeader);   // FP32: [gcap] R_j, then W_ij R_j
+  real* gst = reinterpret_cast<real*>(wsm + kTileHeader);        // FP64: [3][gcap] W_ij R_j
+  int* col_s = reinterpret_cast<int*>(wsm + kTileHeader + (size_t)gcap * slot_bytes<MIXED>());  // [wstride] (staged)
+  // product of the window's block g, and its read-back for the row sums
+  auto put = [&](int g, real m0, real m1, real m2) {
+    if constexpr (MIXED) slot[g] = make_float4(m0, m1, m2, 0.f);
+    else { gst[g] = m0; gst[gcap + g] = m1; gst[2 * gcap + g] = m2; }
+  };
+  auto add = [&](int g, double (&acc)[3]) {
+    if constexpr (MIXED) {
+      const float4 v = slot[g];
+      acc[0] = acc[0] + (double)v.x; acc[1] = acc[1] + (double)v.y; acc[2] = acc[2] + (double)v.z;
+    } else {
+      acc[0] = acc[0] + (double)gst[g]; acc[1] = acc[1] + (double)gst[gcap + g]; acc[2] = acc[2] + (double)gst[2 * gcap + g];
+    }
+  };
   real* w_s = reinterpret_cast<real*>(col_s + wstride);                                  // [9][wstride] (staged)
   const uint32_t bar = smem_addr(wsm + kStageBar);
   const int lane = threadIdx.x & (kWarp - 1);
@@ -419,8 +458,23 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
         phase ^= 1u;
       }
     }
+    // ---- gather of the previous-sweep reactions the window needs: 16-byte
+    // asynchronous copies into the blocks' slots, all in flight together. Lane
+    // l copies the blocks k = wb + l (mod 32), the blocks it computes below.
+    if constexpr (gather_r<MIXED>()) {
+    for (int k = wb + lane; k < we; k += kWarp) {
+      const int j = col_s[k - a0];
+      const bool earlier = f.backward ? (j >= ce) : (j < cs);
+      if (f.merit || (f.gs && !earlier)) {
+        if (!f.prev_done) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
+        cp_async16(smem_addr(slot + (k - wb)), a.R32[rin] + j);
+      }
+    }
+    cp_async_wait_all();
+    }
     // ---- pass 1: previous-sweep values. W_ij R_j^(s-1) of every block (the
-    // merit's products, and the Gauss-Seidel products of later neighbours)
+    // merit's products, and the Gauss-Seidel products of later neighbours),
+    // written over the block's gathered reaction
     for (int base = wb; base < we; base += kSlots) {
       int jj[kChunkUnroll];
       real w[kChunkUnroll][9];
@@ -431,14 +485,18 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
         if (j >= 0) {
           const bool earlier = f.backward ? (j >= ce) : (j < cs);
           if (f.merit || (f.gs && !earlier)) {
-            if (!f.prev_done) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
-            real ro0, ro1, ro2;
-            load_r<MIXED, real>(a, rin, j, ro0, ro1, ro2);
-            const real* Wk = w[u];
             const int g = base + u * kWarp + lane - wb;
-            gst[g] = Wk[0] * ro0 + Wk[3] * ro1 + Wk[6] * ro2;
-            gst[gcap + g] = Wk[1] * ro0 + Wk[4] * ro1 + Wk[7] * ro2;
-            gst[2 * gcap + g] = Wk[2] * ro0 + Wk[5] * ro1 + Wk[8] * ro2;
+            real ro0, ro1, ro2;
+            if constexpr (gather_r<MIXED>()) {
+              const float4 v = slot[g];
+              ro0 = v.x; ro1 = v.y; ro2 = v.z;
+            } else {
+              if (!f.prev_done) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
+              load_r<MIXED, real>(a, rin, j, ro0, ro1, ro2);
+            }
+            const real* Wk = w[u];
+            put(g, Wk[0] * ro0 + Wk[3] * ro1 + Wk[6] * ro2, Wk[1] * ro0 + Wk[4] * ro1 + Wk[7] * ro2,
+                Wk[2] * ro0 + Wk[5] * ro1 + Wk[8] * ro2);
           }
         }
       }
@@ -447,12 +505,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
     if (f.merit) {  // each row adds its own merit products, in list order
       const int lo = mb > wb ? mb : wb;
       const int hi = me < we ? me : we;
-      for (int k = lo; k < hi; k++) {
-        const int g = k - wb;
-        am[0] = am[0] + (double)gst[g];
-        am[1] = am[1] + (double)gst[gcap + g];
-        am[2] = am[2] + (double)gst[2 * gcap + g];
-      }
+      for (int k = lo; k < hi; k++) add(k - wb, am);
       __syncwarp();  // pass 2 overwrites the slots of earlier neighbours
     }
     // ---- merit term of each row (mrf.c:81-87), once its U is complete
@@ -485,10 +538,8 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
             }
             real rn0, rn1, rn2;
             load_r<MIXED, real>(a, rout, j, rn0, rn1, rn2);
-            const int g = k - wb;
-            gst[g] = Wk[0] * rn0 + Wk[3] * rn1 + Wk[6] * rn2;
-            gst[gcap + g] = Wk[1] * rn0 + Wk[4] * rn1 + Wk[7] * rn2;
-            gst[2 * gcap + g] = Wk[2] * rn0 + Wk[5] * rn1 + Wk[8] * rn2;
+            put(k - wb, Wk[0] * rn0 + Wk[3] * rn1 + Wk[6] * rn2, Wk[1] * rn0 + Wk[4] * rn1 + Wk[7] * rn2,
+                Wk[2] * rn0 + Wk[5] * rn1 + Wk[8] * rn2);
           }
         }
       }
@@ -497,12 +548,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
     {  // each row adds its own Gauss-Seidel products, in list order
       const int lo = mb > wb ? mb : wb;
       const int hi = me < we ? me : we;
-      for (int k = lo; k < hi; k++) {
-        const int g = k - wb;
-        ag[0] = ag[0] + (double)gst[g];
-        ag[1] = ag[1] + (double)gst[gcap + g];
-        ag[2] = ag[2] + (double)gst[2 * gcap + g];
-      }
+      for (int k = lo; k < hi; k++) add(k - wb, ag);
     }
     __syncwarp();
   }
