@@ -181,7 +181,7 @@ struct b2dev_ctx {
   // of problem k are caller rows prob_off[k] .. prob_off[k+1]-1
   int nprob = 1;
   std::vector<int> prob_off;
-  Buf tiles, tile_prob, ptile_ptr, ptile, row_prob, pctl, pfe, pvec;
+  Buf tiles, tilek, tile_prob, ptile_ptr, ptile, row_prob, pctl, pfe, pvec;
   std::vector<int> ptile_count;  // tiles per problem
   int trace_sweep = -1;  // sweep of the next solve whose diagonal solves are recorded
 
@@ -236,6 +236,7 @@ int build_tiles(b2dev_ctx* c, int rows) {
   rows = std::max(1, std::min(kWarp, rows));
   c->tile_rows = rows;
   std::vector<int4> tl;
+  std::vector<int2> tk;  // off-diagonal block range of each tile
   std::vector<int> tp;
   int mx = 0;
   for (int k = 0; k < c->ncolours; k++) {
@@ -245,6 +246,7 @@ int build_tiles(b2dev_ctx* c, int rows) {
       int e = r + 1;
       while (e < ce && e - r < rows && c->rprob_h[e] == pr) e++;
       tl.push_back(make_int4(r, (e - r) | (pr << 6), cb, ce));  // rows | problem << 6
+      tk.push_back(make_int2(c->rowptr_h[r], c->rowptr_h[e]));
       tp.push_back(pr);
       mx = std::max(mx, c->rowptr_h[e] - c->rowptr_h[r]);
       r = e;
@@ -263,11 +265,13 @@ int build_tiles(b2dev_ctx* c, int rows) {
     for (int t = 0; t < T; t++) plist[cur[tp[t]]++] = t;
   }
   B2_TRY(ensure(c->tiles, sizeof(int4) * (T + 1)));
+  B2_TRY(ensure(c->tilek, sizeof(int2) * (T + 1)));
   B2_TRY(ensure(c->tile_prob, sizeof(int) * (T + 1)));
   B2_TRY(ensure(c->ptile_ptr, sizeof(int) * (c->nprob + 1)));
   B2_TRY(ensure(c->ptile, sizeof(int) * (T + 1)));
   if (T > 0) {
     B2_CK(cudaMemcpyAsync(c->tiles.p, tl.data(), sizeof(int4) * T, cudaMemcpyHostToDevice, st));
+    B2_CK(cudaMemcpyAsync(c->tilek.p, tk.data(), sizeof(int2) * T, cudaMemcpyHostToDevice, st));
     B2_CK(cudaMemcpyAsync(c->tile_prob.p, tp.data(), sizeof(int) * T, cudaMemcpyHostToDevice, st));
     B2_CK(cudaMemcpyAsync(c->ptile.p, plist.data(), sizeof(int) * T, cudaMemcpyHostToDevice, st));
   }
@@ -531,6 +535,7 @@ int solve_setup(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter
   A.nactive = 0;
   for (int k = 0; k < P; k++) A.nactive += c->ptile_count[k] > 0 ? 1 : 0;
   A.tiles = ptr<int4>(c->tiles);
+  A.tilek = ptr<int2>(c->tilek);
   A.ptile_ptr = ptr<int>(c->ptile_ptr);
   A.ptile = ptr<int>(c->ptile);
   A.done = ptr<int>(c->done);
@@ -726,7 +731,7 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->cctrl, &c->keys_out, &c->iota, &c->perm, &c->iperm, &c->colptr, &c->sdeg, &c->rowptr, &c->col,
                 &c->W64, &c->W32, &c->Wd, &c->Ad, &c->Bv, &c->Vv, &c->rho, &c->gap, &c->fric, &c->rest, &c->coh,
                 &c->R64[0], &c->R64[1], &c->R64[2], &c->R32[0], &c->R32[1], &c->R32[2], &c->Us[0], &c->Us[1],
-                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec, &c->gptr_prev, &c->gcol_prev,
+                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tilek, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec, &c->gptr_prev, &c->gcol_prev,
                 &c->part, &c->rer,
                 &c->mer, &c->failkey, &c->failcount, &c->sctrl, &c->io, &c->cub_tmp, &c->trace};
   for (Buf* b : all)

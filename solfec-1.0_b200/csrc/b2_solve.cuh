@@ -90,6 +90,7 @@ struct SolveArgs {
   int n, ntiles, nprob;
   int nactive;              // problems with at least one row (the launch ends when all have decided)
   const int4* tiles;        // [ntiles] first row, rows | problem << 6, first and end row of its colour (forward order)
+  const int2* tilek;        // [ntiles] the tile's off-diagonal blocks [kb, ke)
   const int* ptile_ptr;     // [nprob+1] the tiles of each problem ...
   const int* ptile;         // [ntiles]  ... in ascending order (fixed summation order)
   const int* rowptr;        // [n+1]
@@ -378,8 +379,8 @@ __host__ __device__ constexpr size_t solve_smem_per_block() {
 // the solve has stopped.
 template <bool MIXED>
 __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags& f, int r0, int nr, int cs, int ce,
-                                           int s, int rin, int rout, int prob, unsigned char* wsm, uint32_t& phase,
-                                           double& errup, double& errlo, double& mnum) {
+                                           int s, int rin, int rout, int prob, int kb0, int ke0, unsigned char* wsm,
+                                           uint32_t& phase, double& errup, double& errlo, double& mnum) {
   typedef typename std::conditional<MIXED, float, double>::type real;
   constexpr int kChunkUnroll = chunk_unroll<MIXED>();
   constexpr int kSlots = kWarp * kChunkUnroll;
@@ -408,15 +409,21 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   const int n = a.n;
   const bool own = lane < nr;
   const int p = r0 + lane;
-  if (lane <= nr) tp[lane] = __ldg(a.rowptr + r0 + lane);
-  if (lane == 0 && nr == kWarp) tp[kWarp] = __ldg(a.rowptr + r0 + kWarp);
-  {  // window 0 on its way while the row data is read
-    __syncwarp();
-    const int kb0 = tp[0], ke0 = tp[nr];
-    if (lane == 0 && ke0 > kb0)
+  // window 0 on its way while the row data is read (the tile's block range is
+  // in its record, so the copy does not wait for the row offsets)
+  if (lane == 0 && ke0 > kb0)
       stage_issue<stage_w<MIXED>()>(bar, smem_addr(col_s), smem_addr(w_s), wstride, a.col, stage_src<MIXED>(a), a.kstride, kb0 & ~3,
                   (min(ke0, kb0 + gcap) + 3) & ~3);
+  if constexpr (!stage_w<MIXED>()) {  // FP64 W planes of the tile into L2 ahead of pass 1 (a hint)
+    if (lane < 9 && ke0 > kb0) {
+      const int p0 = kb0 & ~1, p1 = (ke0 + 1) & ~1;  // 16-byte aligned range of doubles
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a.W64 + lane * a.kstride + p0),
+                   "r"((uint32_t)(p1 - p0) * 8u)
+                   : "memory");
+    }
   }
+  if (lane <= nr) tp[lane] = __ldg(a.rowptr + r0 + lane);
+  if (lane == 0 && nr == kWarp) tp[kWarp] = __ldg(a.rowptr + r0 + kWarp);
   bool ok = true;
   if (own && !f.prev_done) ok = wait_at_least(a.done + p, s, a.ctrl);  // this row's previous sweep is complete
 
@@ -721,6 +728,7 @@ __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constan
     f.prev_done = s == 0;
     const int tile = f.backward ? T - 1 - w : w;
     const int4 ti = __ldg(a.tiles + tile);  // first row, rows | problem << 6, colour bounds
+    const int2 tk = __ldg(a.tilek + tile);  // its blocks
     const int prob = ti.y >> 6, nr = ti.y & 63;
     const unsigned ntp = a.nprob == 1 ? (unsigned)T : (unsigned)(__ldg(a.ptile_ptr + prob + 1) - __ldg(a.ptile_ptr + prob));
     volatile int* decided = a.decided + (size_t)prob * a.pstride;
@@ -740,7 +748,7 @@ __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constan
     const int rin = (a.in + s) % 3;       // iterate s-1
     const int rout = (a.in + s + 1) % 3;  // iterate s
     double errup = 0.0, errlo = 0.0, mnum = 0.0;
-    if (!solve_tile<MIXED>(a, f, ti.x, nr, ti.z, ti.w, s, rin, rout, prob, wsm, phase, errup, errlo, mnum)) break;
+    if (!solve_tile<MIXED>(a, f, ti.x, nr, ti.z, ti.w, s, rin, rout, prob, tk.x, tk.y, wsm, phase, errup, errlo, mnum)) break;
 #pragma unroll
     for (int d = 16; d >= 1; d >>= 1) {
       errup += __shfl_down_sync(0xffffffffu, errup, d);
