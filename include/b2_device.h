@@ -86,6 +86,26 @@ int b2dev_upload_scene(b2dev_ctx* ctx, int nbod, const double* rot, const double
  * the rows out colour by colour. */
 int b2dev_assemble(b2dev_ctx* ctx, double step, int dynamic, uint64_t colour_seed);
 
+/* Rigid time integration on either side of the solve (bod.c:1313-1493,
+ * BODY_Dynamic_Step_Begin / BODY_Dynamic_Step_End for RIG and OBS bodies): the
+ * uploaded body arrays (rotation, velocities) are updated in place, so the
+ * next b2dev_assemble reads them without a host round trip.
+ *   b2dev_rigid_setup: referential inertia J[9] (column-major), mass, current
+ *     mass centre x[3] and scheme per body (0 = RIG_POS, 1 = RIG_NEG, the
+ *     reference's default; NULL = all RIG_NEG; RIG_IMP is not supported).
+ *   b2dev_rigid_step_begin: velo0 <- velo, half step of position and rotation,
+ *     free velocity with gravity (m g) and the bodies' point loads at
+ *     t + step/2 (loads: [nbod][9] linear force, spatial torque, referential
+ *     torque, as rig_point_forces_accumulate sums them; NULL = none).
+ *   b2dev_rigid_step_end: the reactions of the last solve (rig_constraints_force),
+ *     velocity, second half step, rotation update of the scheme.
+ *   b2dev_rigid_get: rot[9], x[3], velo[6], velo0[6] per body (any may be NULL). */
+int b2dev_rigid_setup(b2dev_ctx* ctx, const double* J, const double* mass, const double* x, const int* scheme,
+                      int on_device);
+int b2dev_rigid_step_begin(b2dev_ctx* ctx, double step, const double* gravity, const double* loads, int on_device);
+int b2dev_rigid_step_end(b2dev_ctx* ctx, double step);
+int b2dev_rigid_get(b2dev_ctx* ctx, double* rot, double* x, double* velo, double* velo0, int on_device);
+
 /* Load an already assembled local dynamics (rows in caller order, blocks of
  * row i at adjptr[i]..adjptr[i+1]-1, Woff 9 doubles per block), colour it and
  * lay it out; the same data the reference solver reads from LOCDYN. */

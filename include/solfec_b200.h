@@ -136,6 +136,11 @@ void b2gs_locdyn_destroy (b2gs_locdyn *ldy);
 int b2gs_locdyn_update_begin (b2gs_locdyn *ldy, const b2gs_bodies *bod, const b2gs_contacts *con,
                               double step, int dynamic);
 
+/* LOCDYN_Update_Begin again on the device-resident bodies of the last
+ * b2gs_locdyn_update_begin, as moved by b2dev_rigid_step_begin (same contacts:
+ * referential points, frames, gaps and materials are kept). */
+int b2gs_locdyn_update_begin_resident (b2gs_locdyn *ldy, double step, int dynamic);
+
 /* An assembled local dynamics as the reference solver reads it: rows in list
  * order with W[9], A[9], rho, B[3], V[3], gap, friction, restitution,
  * cohesion; blocks of row i at adjptr[i]..adjptr[i+1]-1 (adjcol = neighbour

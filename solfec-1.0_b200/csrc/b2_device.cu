@@ -23,6 +23,7 @@
 #include "b2_solve.cuh"
 #include "b2_assemble.cuh"
 #include "b2_colour.cuh"
+#include "b2_rigid.cuh"
 
 using namespace b2;
 
@@ -182,6 +183,10 @@ struct b2dev_ctx {
   int nprob = 1;
   std::vector<int> prob_off;
   Buf tiles, tilek, tile_prob, ptile_ptr, ptile, row_prob, pctl, pfe, pvec;
+  // rigid time integration (b2dev_rigid_*): mass centre, inertia, mass, scheme,
+  // external force of the step, NEW2 auxiliary vector, per-step loads
+  Buf rb_x, rb_J, rb_mass, rb_scheme, rb_fext, rb_aux, rb_loads;
+  bool have_rigid = false;
   std::vector<int> ptile_count;  // tiles per problem
   int trace_sweep = -1;  // sweep of the next solve whose diagonal solves are recorded
 
@@ -731,7 +736,7 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->cctrl, &c->keys_out, &c->iota, &c->perm, &c->iperm, &c->colptr, &c->sdeg, &c->rowptr, &c->col,
                 &c->W64, &c->W32, &c->Wd, &c->Ad, &c->Bv, &c->Vv, &c->rho, &c->gap, &c->fric, &c->rest, &c->coh,
                 &c->R64[0], &c->R64[1], &c->R64[2], &c->R32[0], &c->R32[1], &c->R32[2], &c->Us[0], &c->Us[1],
-                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tilek, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec, &c->gptr_prev, &c->gcol_prev,
+                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tilek, &c->rb_x, &c->rb_J, &c->rb_mass, &c->rb_scheme, &c->rb_fext, &c->rb_aux, &c->rb_loads, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec, &c->gptr_prev, &c->gcol_prev,
                 &c->part, &c->rer,
                 &c->mer, &c->failkey, &c->failcount, &c->sctrl, &c->io, &c->cub_tmp, &c->trace};
   for (Buf* b : all)
@@ -772,6 +777,7 @@ int b2dev_upload_scene(b2dev_ctx* c, int nbod, const double* rot, const double* 
   B2_TRY(upload(c, c->rest_c, restitution, (size_t)ncon, on_device));
   B2_TRY(upload(c, c->coh_c, cohesion, (size_t)ncon, on_device));
   c->have_scene = true;
+  c->have_rigid = false;  // b2dev_rigid_setup again for the new bodies
   c->ready = false;
   return B2DEV_OK;
 }
@@ -948,6 +954,100 @@ int b2dev_set_state(b2dev_ctx* c, const double* R, const double* U, int on_devic
   c->state_u = &c->Us[0];
   c->state_cm = nullptr;
   B2_CK(cudaGetLastError());
+  return B2DEV_OK;
+}
+
+// ---- rigid time integration (bod.c:1313-1493) ----
+
+static RigidDev rigid_view(b2dev_ctx* c) {
+  RigidDev d;
+  d.nbod = c->nbod;
+  d.rot = ptr<double>(c->rot); d.x = ptr<double>(c->rb_x); d.velo = ptr<double>(c->velo);
+  d.velo0 = ptr<double>(c->velo0); d.fext = ptr<double>(c->rb_fext); d.aux = ptr<double>(c->rb_aux);
+  d.J = ptr<double>(c->rb_J); d.jinv = ptr<double>(c->jinv); d.mass = ptr<double>(c->rb_mass);
+  d.minv = ptr<double>(c->minv); d.scheme = ptr<int>(c->rb_scheme); d.obstacle = ptr<int>(c->obst);
+  return d;
+}
+
+int b2dev_rigid_setup(b2dev_ctx* c, const double* J, const double* mass, const double* x, const int* scheme,
+                      int on_device) {
+  if (!c || !c->have_scene) { set_err("rigid_setup: no scene uploaded"); return B2DEV_ESTATE; }
+  if (!J || !mass || !x) { set_err("rigid_setup: inertia, mass and mass centre are required"); return B2DEV_EINVAL; }
+  DeviceGuard g(c->device);
+  const int nb = c->nbod;
+  std::vector<int> sch(nb, SCH_RIG_NEG);  // the reference's default (bod.c:1008)
+  if (scheme) {
+    if (on_device) {
+      B2_CK(cudaMemcpy(sch.data(), scheme, sizeof(int) * nb, cudaMemcpyDeviceToHost));
+    } else {
+      std::copy(scheme, scheme + nb, sch.begin());
+    }
+    for (int b = 0; b < nb; b++)
+      if (sch[b] != SCH_RIG_POS && sch[b] != SCH_RIG_NEG) {
+        set_err("rigid_setup: body %d: scheme %d is not RIG_POS (0) or RIG_NEG (1)", b, sch[b]);
+        return B2DEV_EUNSUPPORTED;
+      }
+  }
+  B2_TRY(upload(c, c->rb_J, J, (size_t)9 * nb, on_device));
+  B2_TRY(upload(c, c->rb_mass, mass, (size_t)nb, on_device));
+  B2_TRY(upload(c, c->rb_x, x, (size_t)3 * nb, on_device));
+  B2_TRY(upload(c, c->rb_scheme, sch.data(), (size_t)nb, 0));
+  B2_TRY(ensure(c->rb_fext, sizeof(double) * 6 * (nb + 1)));
+  B2_TRY(ensure(c->rb_aux, sizeof(double) * 3 * (nb + 1)));
+  B2_CK(cudaMemsetAsync(c->rb_aux.p, 0, sizeof(double) * 3 * (nb + 1), c->stream));
+  B2_CK(cudaStreamSynchronize(c->stream));
+  c->have_rigid = true;
+  return B2DEV_OK;
+}
+
+int b2dev_rigid_step_begin(b2dev_ctx* c, double step, const double* gravity, const double* loads, int on_device) {
+  if (!c || !c->have_rigid) { set_err("rigid_step_begin: no rigid bodies set up"); return B2DEV_ESTATE; }
+  if (!(step > 0.0)) { set_err("rigid_step_begin: step must be positive"); return B2DEV_EINVAL; }
+  DeviceGuard g(c->device);
+  const int nb = c->nbod;
+  if (nb == 0) return B2DEV_OK;
+  const double* dl = nullptr;
+  if (loads) {
+    B2_TRY(upload(c, c->rb_loads, loads, (size_t)9 * nb, on_device));
+    dl = ptr<double>(c->rb_loads);
+  }
+  const double g0 = gravity ? gravity[0] : 0.0, g1 = gravity ? gravity[1] : 0.0, g2 = gravity ? gravity[2] : 0.0;
+  c->launches++;
+  k_rigid_begin<<<blocks_for(nb, 128), 128, 0, c->stream>>>(rigid_view(c), step, g0, g1, g2, dl);
+  B2_CK(cudaGetLastError());
+  c->ready = false;  // the bodies moved: the local dynamics must be assembled again
+  return B2DEV_OK;
+}
+
+int b2dev_rigid_step_end(b2dev_ctx* c, double step) {
+  if (!c || !c->have_rigid) { set_err("rigid_step_end: no rigid bodies set up"); return B2DEV_ESTATE; }
+  if (!c->ready || !c->assembled_mode) { set_err("rigid_step_end: no solved local dynamics of these bodies"); return B2DEV_ESTATE; }
+  if (!(step > 0.0)) { set_err("rigid_step_end: step must be positive"); return B2DEV_EINVAL; }
+  DeviceGuard g(c->device);
+  const int nb = c->nbod;
+  if (nb == 0) return B2DEV_OK;
+  c->launches++;
+  k_rigid_end<<<blocks_for(nb, 128), 128, 0, c->stream>>>(
+      rigid_view(c), step, ptr<double>(c->x0), ptr<int>(c->master), ptr<double>(c->mpnt), ptr<double>(c->spnt),
+      ptr<double>(c->base), ptr<int>(c->bptr), ptr<int>(c->brow), ptr<double4>(c->R64[c->state_r]),
+      ptr<int>(c->iperm));
+  B2_CK(cudaGetLastError());
+  return B2DEV_OK;
+}
+
+int b2dev_rigid_get(b2dev_ctx* c, double* rot, double* x, double* velo, double* velo0, int on_device) {
+  if (!c || !c->have_rigid) { set_err("rigid_get: no rigid bodies set up"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  const int nb = c->nbod;
+  cudaStream_t st = c->stream;
+  const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (nb > 0) {
+    if (rot) B2_CK(cudaMemcpyAsync(rot, c->rot.p, sizeof(double) * 9 * nb, kd, st));
+    if (x) B2_CK(cudaMemcpyAsync(x, c->rb_x.p, sizeof(double) * 3 * nb, kd, st));
+    if (velo) B2_CK(cudaMemcpyAsync(velo, c->velo.p, sizeof(double) * 6 * nb, kd, st));
+    if (velo0) B2_CK(cudaMemcpyAsync(velo0, c->velo0.p, sizeof(double) * 6 * nb, kd, st));
+  }
+  B2_CK(cudaStreamSynchronize(st));
   return B2DEV_OK;
 }
 

@@ -324,6 +324,13 @@ int b2gs_locdyn_update_begin (b2gs_locdyn *ldy, const b2gs_bodies *bod, const b2
   return b2dev_assemble (ldy->dev, step, dynamic, ldy->colour_seed);
 }
 
+int b2gs_locdyn_update_begin_resident (b2gs_locdyn *ldy, double step, int dynamic)
+{
+  host_err[0] = '\0';
+  if (!ldy) return B2DEV_EINVAL;
+  return b2dev_assemble (ldy->dev, step, dynamic, ldy->colour_seed);
+}
+
 int b2gs_locdyn_set (b2gs_locdyn *ldy, int n, const double *W, const double *A, const double *rho,
                      const double *B, const double *V, const double *gap, const double *friction,
                      const double *restitution, const double *cohesion, const int *adjptr, const int *adjcol,

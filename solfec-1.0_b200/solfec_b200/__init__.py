@@ -6,3 +6,4 @@ The compute path is libsolfec_b200.so (sm_100a CUDA kernels, host code in C);
 this package binds it and provides the seeded synthetic scenes."""
 from .solver import GAUSS_SEIDEL_SOLVER, LOCDYN, SolfecError, DeviceError  # noqa: F401
 from . import scenes  # noqa: F401
+from . import dynamics  # noqa: F401

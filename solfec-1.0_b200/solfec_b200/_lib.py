@@ -74,6 +74,10 @@ _SIGNATURES = {
     'b2dev_stream': (C.c_void_p, [C.c_void_p]),
     'b2dev_upload_scene': (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 7 + [C.c_int] + [C.c_void_p] * 9 + [C.c_int]),
     'b2dev_assemble': (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_uint64]),
+    'b2dev_rigid_setup': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    'b2dev_rigid_step_begin': (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int]),
+    'b2dev_rigid_step_end': (C.c_int, [C.c_void_p, C.c_double]),
+    'b2dev_rigid_get': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     'b2dev_upload_locdyn': (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 12 + [C.c_double, C.c_double, C.c_int,
                                                                                   C.c_uint64, C.c_int]),
     'b2dev_set_state': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
@@ -144,6 +148,7 @@ _SIGNATURES = {
     'b2gs_get_report': (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     'b2gs_locdyn_create': (C.c_void_p, [C.c_int, C.c_void_p]),
     'b2gs_locdyn_destroy': (None, [C.c_void_p]),
+    'b2gs_locdyn_update_begin_resident': (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
     'b2gs_locdyn_update_begin': (C.c_int, [C.c_void_p, C.POINTER(b2gs_bodies), C.POINTER(b2gs_contacts),
                                            C.c_double, C.c_int]),
     'b2gs_locdyn_set': (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 12 + [C.c_double, C.c_double, C.c_int,

@@ -439,6 +439,49 @@ def batched_scenes(seed: int = 4, count: int = 256, nmin: int = 50, nmax: int = 
     return [batched_scene(sp) for sp in specs]
 
 
+def box_inertia(mass: float, a: float, b: float, c: float) -> np.ndarray:
+    """Referential inertia (column-major 9) of a solid a x b x c box about its
+    mass centre."""
+    return np.diag([mass * (b * b + c * c) / 12.0, mass * (a * a + c * c) / 12.0,
+                    mass * (a * a + b * b) / 12.0]).reshape(9)
+
+
+def block_sliding(step: float = 1e-3, friction: float = 0.8, density: float = 111.11111111111111111):
+    """The scene of the reference's tests/block-sliding.py as a fixed contact
+    set: a 0.3 x 0.3 x 0.1 block (mass 1) resting on a 1 x 0.3 x 0.1 table
+    (an obstacle), both translated by (3, 0, 0). The block touches the table
+    with its bottom face, split 2 x 2 as the test's HEX (cube, 2, 2, 1) mesh
+    splits it: one contact at the centre of each quarter, normal +z (from the
+    table to the block), gap 0, friction 0.8, no restitution or cohesion.
+    Returns (scene, J, mass): the inertia and masses for RIGID_DYNAMICS."""
+    xt = np.array([3.0, 0.0, -0.05])   # table centre
+    xb = np.array([3.0, 0.0, 0.05])    # block centre
+    mt = density * (1.0 * 0.3 * 0.1)
+    mb = density * (0.3 * 0.3 * 0.1)
+    J = np.stack([box_inertia(mt, 1.0, 0.3, 0.1), box_inertia(mb, 0.3, 0.3, 0.1)])
+    jinv = np.stack([np.linalg.inv(Ji.reshape(3, 3)).T.reshape(9) for Ji in J])
+    mass = np.array([mt, mb])
+    pts = np.array([[3.0 + dx, dy, 0.0] for dx in (-0.075, 0.075) for dy in (-0.075, 0.075)])
+    nc = pts.shape[0]
+    base = np.tile(np.eye(3).T.reshape(9), (nc, 1))  # columns t1 = x, t2 = y, n = z
+    scene = Scene(name='block-sliding', step=step, dynamic=1,
+                  rot=np.tile(np.eye(3).reshape(9), (2, 1)), x=np.stack([xt, xb]), x0=np.stack([xt, xb]),
+                  jinv=jinv, minv=1.0 / mass, velo=np.zeros((2, 6)), velo0=np.zeros((2, 6)),
+                  obstacle=np.array([1, 0], dtype=np.int32),
+                  master=np.full(nc, 1, dtype=np.int32), slave=np.zeros(nc, dtype=np.int32),
+                  mpnt=pts.copy(), spnt=pts.copy(), base=base, gap=np.zeros(nc), friction=np.full(nc, friction),
+                  restitution=np.zeros(nc), cohesion=np.zeros(nc), mass=mass)
+    return scene, J, mass
+
+
+def block_sliding_loads(t: float) -> np.ndarray:
+    """The test's block_force callback, 8 cos(t) along x on the block, as the
+    (nbod, 9) load triples RIGID_DYNAMICS.step_begin takes."""
+    L = np.zeros((2, 9))
+    L[1, 0] = 8.0 * np.cos(t)
+    return L
+
+
 def advance_velocities(scene: Scene, R: np.ndarray) -> Scene:
     """One velocity step of the rigid bodies with the solved reactions: the new
     velocity at t is u = u_free + h M^-1 sum H^T R (bod.c:418-439 force

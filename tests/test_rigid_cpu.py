@@ -1,0 +1,143 @@
+"""CPU tests of the rigid time-integration oracle (oracle/rigid_oracle.py):
+the reference's own end-to-end pins (tests/block-sliding.py:64-80) through
+the restated integrator and the restated (and, when built, the compiled
+reference) Gauss-Seidel solver, and properties of the schemes."""
+import dataclasses
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import rigid_oracle as ro
+from solfec_b200 import scenes
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def run_block_sliding_cpu(nsteps, impl='oracle'):
+    sc, J, mass = scenes.block_sliding()
+    bd = ro.Bodies(sc.rot, sc.x, sc.velo, J, sc.jinv, mass, sc.minv, sc.x0, sc.obstacle)
+    h = sc.step
+    R = np.zeros(3 * sc.ncon)
+    U = np.zeros(3 * sc.ncon)
+    X, V = [], []
+    t = 0.0
+    for _ in range(nsteps):
+        ro.step_begin(bd, h, (0.0, 0.0, -9.81), scenes.block_sliding_loads(t + 0.5 * h))
+        cur = dataclasses.replace(sc, rot=np.array(bd.rot), velo=np.array(bd.velo), velo0=np.array(bd.velo0))
+        out = oracle.solve(oracle.assemble(cur), R, U, epsilon=1e-3, maxiter=1000, impl=impl)
+        R, U = out['R'], out['U']
+        ro.step_end(bd, h, sc.master, sc.slave, sc.mpnt, sc.spnt, sc.base, R.reshape(-1, 3))
+        t += h
+        X.append(bd.x[1][0])
+        V.append(bd.velo[1][3])
+    return np.array(X), np.array(V)
+
+
+def check_pins(X, V):
+    ref = json.load(open(os.path.join(HERE, 'golden', 'block_sliding_ref.json')))
+    for p in ref['pins']:
+        val = X[p['index']] if p['quantity'] == 'x' else V[p['index']]
+        err = abs(val - p['value']) / max(1.0, p['value'])
+        assert err <= ref['tolerance'], (p, val, err)
+
+
+@pytest.mark.parametrize('impl', ['oracle', 'ref'])
+def test_block_sliding_pins_cpu(impl):
+    if impl == 'ref' and not oracle.ref_available():
+        pytest.skip('compiled reference solver not built')
+    X, V = run_block_sliding_cpu(8001, impl)
+    check_pins(X, V)
+
+
+def test_expmap_rotation():
+    rng = np.random.default_rng(5)
+    for scale in (1e-6, 1e-2, 0.17, 0.18, 1.0, 3.0):
+        for _ in range(20):
+            w = rng.normal(size=3)
+            w *= scale / np.linalg.norm(w)
+            R = np.array(ro.expmap(list(w))).reshape(3, 3).T  # row-major
+            assert np.abs(R @ R.T - np.eye(3)).max() < 1e-14
+            assert abs(np.linalg.det(R) - 1.0) < 1e-14
+            a = np.linalg.norm(w)
+            K = np.array([[0, -w[2], w[1]], [w[2], 0, -w[0]], [-w[1], w[0], 0]])
+            Rr = np.eye(3) + math.sin(a) / a * K + (1 - math.cos(a)) / a ** 2 * K @ K
+            assert np.abs(R - Rr).max() < 1e-14
+            assert np.allclose(R @ w, w, atol=1e-15 * max(1.0, a))  # the axis is fixed
+
+
+def _spinning_body(scheme):
+    J = np.diag([0.4, 0.7, 1.1]).reshape(9)
+    jinv = np.linalg.inv(J.reshape(3, 3)).reshape(9)
+    return ro.Bodies(rot=np.eye(3).reshape(1, 9), x=[[0.0, 0.0, 0.0]], velo=[[0.3, 2.0, -0.5, 0.0, 0.0, 0.0]],
+                     J=J[None], jinv=jinv[None], mass=[2.0], minv=[0.5], x0=[[0.0, 0.0, 0.0]], obstacle=[0],
+                     scheme=[scheme])
+
+
+def test_neg_scheme_conserves_angular_momentum():
+    """NEW2 (RIG_NEG) conserves the spatial angular momentum of a free body
+    exactly up to rounding (bod.h:83)."""
+    bd = _spinning_body(ro.SCH_RIG_NEG)
+    L0 = np.array(ro.spatial_angular_momentum(bd, 0))
+    for _ in range(2000):
+        ro.step_begin(bd, 1e-3)
+        ro.step_end(bd, 1e-3, [], [], np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 9)), np.zeros((0, 3)))
+    L = np.array(ro.spatial_angular_momentum(bd, 0))
+    assert np.linalg.norm(L - L0) / np.linalg.norm(L0) < 1e-12
+    Rm = np.array(bd.rot[0]).reshape(3, 3)
+    assert np.abs(Rm @ Rm.T - np.eye(3)).max() < 1e-12
+
+
+def test_pos_scheme_energy_bounded():
+    """NEW1 (RIG_POS): a free body's kinetic energy stays within a small
+    drift over many steps."""
+    bd = _spinning_body(ro.SCH_RIG_POS)
+    e0 = ro.kinetic_energy(bd, 0)
+    for _ in range(2000):
+        ro.step_begin(bd, 1e-3)
+        ro.step_end(bd, 1e-3, [], [], np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 9)), np.zeros((0, 3)))
+    assert abs(ro.kinetic_energy(bd, 0) - e0) / e0 < 1e-3
+
+
+def test_free_fall_is_exact():
+    """Constant gravity: the half-step position updates integrate a constant
+    acceleration exactly (x = x0 + v0 t + g t^2 / 2 up to rounding)."""
+    bd = ro.Bodies(rot=np.eye(3).reshape(1, 9), x=[[0.0, 0.0, 1.0]], velo=[[0.0, 0.0, 0.0, 0.5, 0.0, 0.0]],
+                   J=np.eye(3).reshape(1, 9), jinv=np.eye(3).reshape(1, 9), mass=[3.0], minv=[1.0 / 3.0],
+                   x0=[[0.0, 0.0, 1.0]], obstacle=[0])
+    h, n = 1e-3, 500
+    for _ in range(n):
+        ro.step_begin(bd, h, (0.0, 0.0, -9.81))
+        ro.step_end(bd, h, [], [], np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 9)), np.zeros((0, 3)))
+    t = n * h
+    assert abs(bd.x[0][2] - (1.0 - 0.5 * 9.81 * t * t)) < 1e-12
+    assert abs(bd.x[0][0] - 0.5 * t) < 1e-12
+    assert abs(bd.velo[0][5] + 9.81 * t) < 1e-12
+
+
+def test_constraint_force_is_HtR():
+    """rig_constraints_force of one contact equals H^T R of the operator
+    written out with numpy (spatial force on the master, opposite on the
+    slave), H = [base^T R skew(X - X0)^T | base^T] (bod.c:216-228)."""
+    rng = np.random.default_rng(7)
+    Rm = np.linalg.qr(rng.normal(size=(3, 3)))[0]
+    Rm *= np.sign(np.linalg.det(Rm))
+    base = np.linalg.qr(rng.normal(size=(3, 3)))[0]
+    X0 = rng.normal(size=3)
+    X = rng.normal(size=3)
+    r = rng.normal(size=3)
+    H = np.array(ro.operator_H(list(Rm.T.reshape(9)), list(X0), list(base.T.reshape(9)), list(X)))
+    H = H.reshape(6, 3).T  # 3 x 6
+    A = X - X0
+    S = np.array([[0, -A[2], A[1]], [A[2], 0, -A[0]], [-A[1], A[0], 0]])
+    Href = np.hstack([base.T @ Rm @ S.T, base.T])
+    assert np.allclose(H, Href, atol=1e-14)
+    # one body on one contact: the end-of-step velocity change is h M^-1 H^T r
+    bd = ro.Bodies(rot=Rm.T.reshape(1, 9), x=[X0], velo=[[0.0] * 6], J=np.eye(3).reshape(1, 9),
+                   jinv=np.eye(3).reshape(1, 9), mass=[1.0], minv=[1.0], x0=[X0], obstacle=[0],
+                   scheme=[ro.SCH_RIG_POS])
+    ro.step_end(bd, 1.0, [0], [-1], X[None], X[None], base.T.reshape(1, 9), r[None])
+    assert np.allclose(np.array(bd.velo[0]), Href.T @ r, atol=1e-13)
