@@ -263,12 +263,98 @@ def bench_product(args, ws, rank, local):
         gs.precision = 'MIXED'
         e2e_ms, _, _ = timed(step_e2e, gs, args.steps, args.warmup)
     nrows, K, ncol, fe = ldy.sizes()
+    rigid = rigid_step_timing(ldy, sc, bd, cd, stream, barrier, dev)
     results['mixed_nn']['nn'] = nn_reps[-1] if nn_reps else None
     results['mixed_nn']['nn_used_steps'] = sum(1 for r in nn_reps if r['used_nn'])
     results['mixed_nn']['nn_steps'] = len(nn_reps)
     net.close()
     return dict(results=results, e2e_ms=e2e_ms, h2d=h2d_bytes, d2h=d2h_bytes, n=nrows, K=K, ncolours=ncol,
-                clocks=clk.summary(), iters_prev=iters_prev, nbod=sc.nbod, scene=sc, R0=R0, U0=U0)
+                clocks=clk.summary(), iters_prev=iters_prev, nbod=sc.nbod, scene=sc, R0=R0, U0=U0, rigid=rigid)
+
+
+# Algorithmic bytes of the rigid time integration kernels (csrc/b2_rigid.cuh),
+# each datum counted once. Per body: begin reads velo, rot, x, J, jinv, mass,
+# minv, scheme, obstacle (312 B) and writes velo0, rot, x, aux, fext, velo
+# (264 B); end reads rot, x0, x, velo, jinv, minv, scheme, obstacle, aux, bptr
+# (280 B) and writes velo, x, rot, aux (168 B). End also reads per contact its
+# frame, reaction (double4), master index and sorted position (112 B) and per
+# contact side of a moving body the row index and referential point (28 B).
+RIGID_BYTES_BEGIN = 576
+RIGID_BYTES_END_BODY = 448
+RIGID_BYTES_END_CONTACT = 112
+RIGID_BYTES_END_SIDE = 28
+RIGID_REPS = 20
+GRAVITY_VEC = (0.0, 0.0, -9.81)
+RIGID_CPU_SAMPLE = 2000
+
+
+def _rigid_inertia(sc, k=None):
+    k = sc.nbod if k is None else k
+    ob = sc.obstacle[:k] != 0  # walls: zero inverse inertia and mass (never accelerated)
+    J = np.stack([np.eye(3).reshape(9) if o else np.linalg.inv(j.reshape(3, 3).T).T.reshape(9)
+                  for j, o in zip(sc.jinv[:k], ob)])
+    mass = np.where(ob, 1.0, 1.0 / np.where(ob, 1.0, sc.minv[:k]))
+    return J, mass
+
+
+def rigid_step_timing(ldy, sc, bd, cd, stream, barrier, dev):
+    """Device time of BODY_Dynamic_Step_Begin / End (k_rigid_begin,
+    k_rigid_end) for every body of the bench scene, measured inside the step
+    they belong to: each repetition is begin, assembly on the device bodies,
+    a 5-sweep FP64 solve, end, with CUDA events on the library's stream around
+    begin and around end. The solve streams the W planes (far beyond L2)
+    between the two, so the body arrays come from DRAM as in a time loop (a
+    plain buffer write between back-to-back launches left them in L2).
+    Averaged over RIGID_REPS repetitions, outside the timed solve region."""
+    import ctypes as C
+    import torch
+    from solfec_b200 import GAUSS_SEIDEL_SOLVER
+    from solfec_b200.dynamics import RIGID_DYNAMICS
+    from solfec_b200._lib import lib
+    J, mass = _rigid_inertia(sc)
+    ldy.update_begin_arrays(bd, cd, sc.step, sc.dynamic)
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    gs = GAUSS_SEIDEL_SOLVER(epsilon=1e-12, maxiter=5, meritval=1e-12, diagepsilon=1e-6, diagmaxiter=100)
+    n = sc.ncon
+    Rz = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    Uz = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    pairs = []
+    for rep in range(3 + RIGID_REPS):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(stream)
+        dyn.step_begin(sc.step, GRAVITY_VEC)
+        ev[1].record(stream)
+        if lib().b2gs_locdyn_update_begin_resident(ldy.handle, sc.step, sc.dynamic) != 0:
+            raise RuntimeError('LOCDYN update on the device bodies failed')
+        ldy.set_state_ptr(C.c_void_p(Rz.data_ptr()), C.c_void_p(Uz.data_ptr()), 1)
+        gs.solve(ldy)
+        ev[2].record(stream)
+        dyn.step_end(sc.step)
+        ev[3].record(stream)
+        if rep >= 3:
+            pairs.append(ev)
+    barrier()
+    tb = max_over_ranks(sum(e[0].elapsed_time(e[1]) for e in pairs) / RIGID_REPS, dev)
+    te = max_over_ranks(sum(e[2].elapsed_time(e[3]) for e in pairs) / RIGID_REPS, dev)
+    ob = sc.obstacle != 0
+    inc = int(np.sum(~ob[sc.master]) + np.sum((sc.slave >= 0) & ~ob[np.maximum(sc.slave, 0)]))
+    nb = sc.nbod
+    return dict(bodies=nb, contact_sides=inc, begin_ms=tb, end_ms=te, begin_bytes=nb * RIGID_BYTES_BEGIN,
+                end_bytes=nb * RIGID_BYTES_END_BODY + sc.ncon * RIGID_BYTES_END_CONTACT + inc * RIGID_BYTES_END_SIDE)
+
+
+def rigid_cpu_sample(sc, nsample=RIGID_CPU_SAMPLE):
+    """Host time of the restated BODY_Dynamic_Step_Begin (oracle/rigid_oracle.py,
+    one core, scalar Python) on the first `nsample` bodies of the scene, per
+    1000 bodies."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import rigid_oracle as ro
+    k = min(nsample, sc.nbod)
+    J, mass = _rigid_inertia(sc, k)
+    bd = ro.Bodies(sc.rot[:k], sc.x[:k], sc.velo[:k], J, sc.jinv[:k], mass, sc.minv[:k], sc.x0[:k], sc.obstacle[:k])
+    t0 = time.perf_counter()
+    ro.step_begin(bd, sc.step, GRAVITY_VEC)
+    return 1e3 * (time.perf_counter() - t0) * 1000.0 / k
 
 
 BATCH = dict(seed=4, count=256, nmin=50, nmax=2000, settle_iters=300)
@@ -510,6 +596,19 @@ def main():
                              'iterations the step takes (the FP64 GPU path takes the same iterates)'
                              % (out['n'], t['sample_iters'], fp64['iters']),
                    'assemble_ms': round(t['assemble_ms'], 3), 'per_iteration_ms': round(t['per_iter_ms'], 3)}
+        rg = out['rigid']
+        gb = rg['begin_bytes'] / (rg['begin_ms'] * 1e-3) / 1e9
+        ge = rg['end_bytes'] / (rg['end_ms'] * 1e-3) / 1e9
+        rigid = {'bodies': rg['bodies'], 'contact_sides': rg['contact_sides'],
+                 'kernels': 'k_rigid_begin / k_rigid_end (BODY_Dynamic_Step_Begin / End of every body)',
+                 'begin_ms': round(rg['begin_ms'], 5), 'end_ms': round(rg['end_ms'], 5),
+                 'begin_bytes': rg['begin_bytes'], 'end_bytes': rg['end_bytes'],
+                 'begin_gbs': round(gb, 1), 'end_gbs': round(ge, 1), 'peak_gbs': peak,
+                 'begin_frac': round(gb / peak, 3), 'end_frac': round(ge / peak, 3),
+                 'timing': 'inside the step: begin after the previous step\'s solve, end right after a 5-sweep '
+                           'solve whose reactions and layout it reads back from L2 (end_frac > 1 reflects that)',
+                 'cpu_port_ms_per_1k_bodies': None if args.no_cpu_baseline
+                 else round(rigid_cpu_sample(out['scene']), 3)}
         line = {
             'metric': METRIC, 'value': round(mnn['ms'], 4), 'unit': 'ms', 'n_gpus': ws, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': round(mnn['ms'], 4), 'higher_is_better': False,
@@ -542,6 +641,7 @@ def main():
                     'd2h_bytes_per_step': out['d2h']},
             'gpu_launches': int(mnn['launches']),
             'clocks': out['clocks'],
+            'rigid_step': rigid,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
