@@ -141,6 +141,28 @@ int b2gs_locdyn_update_begin (b2gs_locdyn *ldy, const b2gs_bodies *bod, const b2
  * referential points, frames, gaps and materials are kept). */
 int b2gs_locdyn_update_begin_resident (b2gs_locdyn *ldy, double step, int dynamic);
 
+/* ---- interchange formats of the local dynamics (host/b2io.c) ---- */
+
+/* LOCDYN_W_MatrixMarket (ldy.c:1005-1052): W as a 3n x 3n coordinate matrix,
+ * rows in list order, the diagonal block then the row's off-diagonal blocks
+ * in their list order, "%.15g". From host arrays in caller order (W[9n],
+ * adjptr[n+1], adjcol[K], Woff[9K]), or from the device after assembly. */
+int b2gs_write_w_matrix_market (const char *path, int n, const double *W, const int *adjptr, const int *adjcol,
+                                const double *Woff);
+int b2gs_locdyn_w_matrix_market (b2gs_locdyn *ldy, const char *path);
+
+/* LOCDYN_Dump (ldy.c:892-1002): one line per row with its spatial point,
+ * body ids, frame, W, B, V, U, R ("%.6g"), then " => " each neighbour with
+ * the neighbour's blocks summed, neighbours in the reference's dump order.
+ * point[3n] (spatial contact points), master_id/slave_id[n] (body ids; -1
+ * for none) and base[9n] come from the caller; the device version reads W, B,
+ * V, the blocks and the current R, U from the device. */
+int b2gs_write_locdyn_dump (const char *path, int n, const double *point, const int *master_id, const int *slave_id,
+                            const double *base, const double *W, const double *B, const double *V, const double *U,
+                            const double *R, const int *adjptr, const int *adjcol, const double *Woff);
+int b2gs_locdyn_dump (b2gs_locdyn *ldy, const char *path, const double *point, const int *master_id,
+                      const int *slave_id, const double *base);
+
 /* An assembled local dynamics as the reference solver reads it: rows in list
  * order with W[9], A[9], rho, B[3], V[3], gap, friction, restitution,
  * cohesion; blocks of row i at adjptr[i]..adjptr[i+1]-1 (adjcol = neighbour

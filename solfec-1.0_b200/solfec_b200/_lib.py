@@ -149,6 +149,10 @@ _SIGNATURES = {
     'b2gs_locdyn_create': (C.c_void_p, [C.c_int, C.c_void_p]),
     'b2gs_locdyn_destroy': (None, [C.c_void_p]),
     'b2gs_locdyn_update_begin_resident': (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
+    'b2gs_write_w_matrix_market': (C.c_int, [C.c_char_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    'b2gs_locdyn_w_matrix_market': (C.c_int, [C.c_void_p, C.c_char_p]),
+    'b2gs_write_locdyn_dump': (C.c_int, [C.c_char_p, C.c_int] + [C.c_void_p] * 12),
+    'b2gs_locdyn_dump': (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     'b2gs_locdyn_update_begin': (C.c_int, [C.c_void_p, C.POINTER(b2gs_bodies), C.POINTER(b2gs_contacts),
                                            C.c_double, C.c_int]),
     'b2gs_locdyn_set': (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 12 + [C.c_double, C.c_double, C.c_int,

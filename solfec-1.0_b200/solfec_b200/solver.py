@@ -17,6 +17,7 @@ CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -179,6 +180,21 @@ class LOCDYN:
                                       ptr(adjcol), ptr(Woff), C.byref(fe)), 'get_locdyn')
         return dict(W=W[:9 * n], A=A[:9 * n], rho=rho[:n], B=B[:3 * n], V=V[:3 * n], adjptr=adjptr,
                     adjcol=adjcol[:K], Woff=Woff[:9 * K], free_energy=fe.value)
+
+    def w_matrix_market(self, path: str):
+        """LOCDYN_W_MatrixMarket (ldy.c:1005-1052) of the assembled local dynamics."""
+        _check(lib().b2gs_locdyn_w_matrix_market(self._h, os.fsencode(path)), 'LOCDYN_W_MatrixMarket')
+
+    def dump(self, path: str, point, master_id, slave_id, base):
+        """LOCDYN_Dump (ldy.c:892-1002) of the assembled local dynamics and its
+        current R, U: point (n, 3) spatial contact points, master_id /
+        slave_id (n,) body ids (-1: none), base (n, 9) local frames."""
+        n = self.sizes()[0]
+        p, b = _f64(point).reshape(-1), _f64(base).reshape(-1)
+        mi, si = _i32(master_id).reshape(-1), _i32(slave_id).reshape(-1)
+        if p.shape[0] != 3 * n or b.shape[0] != 9 * n or mi.shape[0] != n or si.shape[0] != n:
+            raise ValueError('dump: point (n, 3), master_id (n,), slave_id (n,) and base (n, 9) are required')
+        _check(lib().b2gs_locdyn_dump(self._h, os.fsencode(path), ptr(p), ptr(mi), ptr(si), ptr(b)), 'LOCDYN_Dump')
 
     @property
     def assemble_ms(self) -> float:
