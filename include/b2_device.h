@@ -97,7 +97,8 @@ int b2dev_assemble(b2dev_ctx* ctx, double step, int dynamic, uint64_t colour_see
  *     free velocity with gravity (m g) and the bodies' point loads at
  *     t + step/2 (loads: [nbod][9] linear force, spatial torque, referential
  *     torque, as rig_point_forces_accumulate sums them; NULL = none).
- *   b2dev_rigid_step_end: the reactions of the last solve (rig_constraints_force),
+ *   b2dev_rigid_step_end: the reactions of the last solve (rig_constraints_force; a scene
+ *     without contacts needs no solve),
  *     velocity, second half step, rotation update of the scheme.
  *   b2dev_rigid_get: rot[9], x[3], velo[6], velo0[6] per body (any may be NULL). */
 int b2dev_rigid_setup(b2dev_ctx* ctx, const double* J, const double* mass, const double* x, const int* scheme,

@@ -1021,16 +1021,22 @@ int b2dev_rigid_step_begin(b2dev_ctx* c, double step, const double* gravity, con
 
 int b2dev_rigid_step_end(b2dev_ctx* c, double step) {
   if (!c || !c->have_rigid) { set_err("rigid_step_end: no rigid bodies set up"); return B2DEV_ESTATE; }
-  if (!c->ready || !c->assembled_mode) { set_err("rigid_step_end: no solved local dynamics of these bodies"); return B2DEV_ESTATE; }
+  const bool contacts = c->ncon > 0;  // without contacts there are no reactions to apply
+  if (contacts && (!c->ready || !c->assembled_mode)) {
+    set_err("rigid_step_end: no solved local dynamics of these bodies");
+    return B2DEV_ESTATE;
+  }
   if (!(step > 0.0)) { set_err("rigid_step_end: step must be positive"); return B2DEV_EINVAL; }
   DeviceGuard g(c->device);
   const int nb = c->nbod;
   if (nb == 0) return B2DEV_OK;
   c->launches++;
   k_rigid_end<<<blocks_for(nb, 128), 128, 0, c->stream>>>(
-      rigid_view(c), step, ptr<double>(c->x0), ptr<int>(c->master), ptr<double>(c->mpnt), ptr<double>(c->spnt),
-      ptr<double>(c->base), ptr<int>(c->bptr), ptr<int>(c->brow), ptr<double4>(c->R64[c->state_r]),
-      ptr<int>(c->iperm));
+      rigid_view(c), step, ptr<double>(c->x0), contacts ? ptr<int>(c->master) : nullptr,
+      contacts ? ptr<double>(c->mpnt) : nullptr, contacts ? ptr<double>(c->spnt) : nullptr,
+      contacts ? ptr<double>(c->base) : nullptr, contacts ? ptr<int>(c->bptr) : nullptr,
+      contacts ? ptr<int>(c->brow) : nullptr, contacts ? ptr<double4>(c->R64[c->state_r]) : nullptr,
+      contacts ? ptr<int>(c->iperm) : nullptr);
   B2_CK(cudaGetLastError());
   return B2DEV_OK;
 }

@@ -190,7 +190,8 @@ __global__ void k_rigid_begin(RigidDev d, double step, double g0, double g1, dou
 // body's contacts in ascending order, obstacles skipped), the velocity
 // update, the second half step of the position and the rotation update of the
 // body's scheme. R64/iperm: the solve's reactions in sorted row order and the
-// sorted position of each contact.
+// sorted position of each contact (all contact arrays may be null when the
+// scene has no contacts, with bptr null).
 __global__ void k_rigid_end(RigidDev d, double step, const double* x0, const int* master, const double* mpnt,
                             const double* spnt, const double* cbase, const int* bptr, const int* brow,
                             const double4* R64, const int* iperm) {
@@ -204,7 +205,7 @@ __global__ void k_rigid_end(RigidDev d, double step, const double* x0, const int
 #pragma unroll
   for (int q = 0; q < 9; q++) Rb[q] = R[q];
   X0[0] = x0[3 * (size_t)b]; X0[1] = x0[3 * (size_t)b + 1]; X0[2] = x0[3 * (size_t)b + 2];
-  if (!d.obstacle[b]) {  // obstacles do not react to contact forces
+  if (bptr && !d.obstacle[b]) {  // obstacles do not react to contact forces
     for (int k = bptr[b]; k < bptr[b + 1]; k++) {
       const int i = brow[k];
       const bool isma = master[i] == b;

@@ -482,6 +482,34 @@ def block_sliding_loads(t: float) -> np.ndarray:
     return L
 
 
+def projectile():
+    """The scene of the reference's tests/projectile.py: one rigid body of mass
+    0.45359237 kg and unit inertia at the origin, launched at (2.54, 0, 12.7)
+    m/s under gravity 9.81456 m/s^2, with a drag load -m v evaluated from the
+    velocity at the start of each step (projectile_loads); no contacts. Step
+    1.976 / 1024 s. Returns (scene, J, mass)."""
+    m = 0.45359237
+    z3, z9 = np.zeros((0, 3)), np.zeros((0, 9))
+    zi, zd = np.zeros(0, dtype=np.int32), np.zeros(0)
+    velo = np.array([[0.0, 0.0, 0.0, 2.54, 0.0, 12.7]])
+    scene = Scene(name='projectile', step=1.976 / 1024.0, dynamic=1, rot=np.eye(3).reshape(1, 9),
+                  x=np.zeros((1, 3)), x0=np.zeros((1, 3)), jinv=np.eye(3).reshape(1, 9), minv=np.array([1.0 / m]),
+                  velo=velo, velo0=velo.copy(), obstacle=np.zeros(1, dtype=np.int32), master=zi, slave=zi,
+                  mpnt=z3, spnt=z3, base=z9, gap=zd, friction=zd, restitution=zd, cohesion=zd, mass=np.array([m]))
+    return scene, np.eye(3).reshape(1, 9), np.array([m])
+
+
+def projectile_loads(mass: float, velo: np.ndarray) -> np.ndarray:
+    """The test's projectile_force callback, (-m v, 0, 0), from the body's
+    velocity [Omega; v] at the start of the step."""
+    L = np.zeros((1, 9))
+    L[0, 0:3] = [-mass * velo[3], -mass * velo[4], -mass * velo[5]]
+    return L
+
+
+PROJECTILE_GRAVITY = 9.81456
+
+
 def advance_velocities(scene: Scene, R: np.ndarray) -> Scene:
     """One velocity step of the rigid bodies with the solved reactions: the new
     velocity at t is u = u_free + h M^-1 sum H^T R (bod.c:418-439 force

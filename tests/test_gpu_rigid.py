@@ -135,3 +135,27 @@ def test_block_sliding_device():
         Vc.append(bd.velo[1][3])
     assert np.array_equal(X[:1000], np.array(Xc))
     assert np.array_equal(V[:1000], np.array(Vc))
+
+
+def test_projectile_device():
+    """The reference's tests/projectile.py on the device integrator (no
+    contacts): the pinned x distance within its 0.5%, and every step equal to
+    the CPU restatement bitwise."""
+    sc, J, mass = scenes.projectile()
+    ldy = LOCDYN()
+    ldy.update_begin(sc)
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    bd = ro.Bodies(sc.rot, sc.x, sc.velo, J, sc.jinv, mass, sc.minv, sc.x0, sc.obstacle)
+    g = (0.0, 0.0, -scenes.PROJECTILE_GRAVITY)
+    for _ in range(1024):
+        u = dyn.state()['velo'][0]
+        dyn.step_begin(sc.step, g, scenes.projectile_loads(mass[0], u))
+        dyn.step_end(sc.step)
+        ro.step_begin(bd, sc.step, g, scenes.projectile_loads(bd.mass[0], bd.velo[0]))
+        ro.step_end(bd, sc.step, [], [], np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 9)), np.zeros((0, 3)))
+        st = dyn.state()
+        assert np.array_equal(st['x'][0], np.array(bd.x[0])) and np.array_equal(st['velo'][0], np.array(bd.velo[0]))
+    ldy.close()
+    ref = json.load(open(os.path.join(HERE, 'golden', 'projectile_ref.json')))
+    x_in = st['x'][0, 0] / 0.0254
+    assert abs(x_in - ref['value']) / ref['value'] < ref['tolerance'], x_in

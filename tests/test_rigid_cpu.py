@@ -53,6 +53,21 @@ def test_block_sliding_pins_cpu(impl):
     check_pins(X, V)
 
 
+def test_projectile_pin_cpu():
+    """The reference's tests/projectile.py: drag load -m v and gravity, no
+    contacts; the x distance after the run in inches within 0.5% of 86.138
+    (the exact value, 2.54 (1 - exp(-1.976)) m)."""
+    sc, J, mass = scenes.projectile()
+    bd = ro.Bodies(sc.rot, sc.x, sc.velo, J, sc.jinv, mass, sc.minv, sc.x0, sc.obstacle)
+    for _ in range(1024):
+        L = scenes.projectile_loads(bd.mass[0], bd.velo[0])
+        ro.step_begin(bd, sc.step, (0.0, 0.0, -scenes.PROJECTILE_GRAVITY), L)
+        ro.step_end(bd, sc.step, [], [], np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 9)), np.zeros((0, 3)))
+    ref = json.load(open(os.path.join(HERE, 'golden', 'projectile_ref.json')))
+    x_in = bd.x[0][0] / 0.0254
+    assert abs(x_in - ref['value']) / ref['value'] < ref['tolerance'], x_in
+
+
 def test_expmap_rotation():
     rng = np.random.default_rng(5)
     for scale in (1e-6, 1e-2, 0.17, 0.18, 1.0, 3.0):
