@@ -162,6 +162,11 @@ struct b2dev_ctx {
   int colour_list = 1;            // 1: greedy order = list order, 0: seeded Jones-Plassmann priorities
   Buf gptr_prev, gcol_prev;       // graph of the last colouring (reused while the graph is unchanged)
   bool colour_valid = false;
+  // the colour-sorted layout (perm, rowptr, colptr, tile table) of the last
+  // prepare_layout, and what it was built for: reused with the colouring
+  bool layout_valid = false;
+  int layout_nprob = 0, layout_tile_rows = 0;
+  std::vector<int> layout_prob_off;
   int colour_n = -1, colour_mode = -1, ncolours_prev = 0;
   long long colour_K = -1;
   uint64_t colour_seed_prev = 0;
@@ -317,6 +322,11 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
     B2_CK(cudaStreamSynchronize(st));
     reuse = diff == 0;
   }
+  // same graph, same colours: the sorted layout and the tile table are those of
+  // the last layout, unless the problems or the rows per tile changed since
+  const bool same_layout = reuse && c->layout_valid && c->layout_nprob == c->nprob &&
+                           c->layout_prob_off == c->prob_off && c->layout_tile_rows == c->tile_rows;
+  c->layout_valid = false;
   if (reuse) {
     c->colour_reuse++;
     cc.ncolours = c->ncolours_prev;
@@ -359,6 +369,7 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   }
   c->ncolours = n > 0 ? cc.ncolours : 0;
 
+  if (!same_layout) {
   // rows sorted by colour, ascending row index inside a colour (stable radix sort)
   c->launches++;
   k_iota<<<blocks_for(n, T), T, 0, st>>>(n, ptr<int>(c->iota));
@@ -384,6 +395,7 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   if (c->ncolours > 0) {
     B2_CK(cudaMemcpyAsync(c->colptr_h.data(), c->colptr.p, sizeof(int) * (c->ncolours + 1), cudaMemcpyDeviceToHost, st));
     B2_CK(cudaStreamSynchronize(st));
+  }
   }
 
   const long long K = c->K;
@@ -432,7 +444,7 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
     B2_TRY(ensure(c->conmerit[b], sizeof(double) * (n + 1)));
   }
   B2_TRY(ensure(c->done, sizeof(int) * (n + 1)));
-  {  // sorted CSR offsets and the problem of every sorted row, kept on the host for the tile table
+  if (!same_layout) {  // sorted CSR offsets and the problem of every sorted row, kept on the host for the tile table
     c->rowptr_h.assign(n + 1, 0);
     B2_CK(cudaMemcpyAsync(c->rowptr_h.data(), c->rowptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, st));
     c->rprob_h.assign(n, 0);
@@ -447,7 +459,7 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
     B2_TRY(ensure(c->row_prob, sizeof(int) * (n + 1)));
     if (n > 0) B2_CK(cudaMemcpyAsync(c->row_prob.p, c->rprob_h.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
   }
-  B2_TRY(build_tiles(c, c->tile_rows));
+  if (!same_layout) B2_TRY(build_tiles(c, c->tile_rows));
   // new contacts start from R = U = 0 (MEM_Alloc zeroes, mem.c:64-86)
   B2_CK(cudaMemsetAsync(c->R64[0].p, 0, sizeof(double4) * (n + 1), st));
   B2_CK(cudaMemsetAsync(c->R32[0].p, 0, sizeof(float4) * (n + 1), st));
@@ -458,6 +470,10 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   c->state_cm = nullptr;
   B2_CK(cudaGetLastError());
   B2_CK(cudaStreamSynchronize(st));
+  c->layout_valid = c->colour_valid;
+  c->layout_nprob = c->nprob;
+  c->layout_prob_off = c->prob_off;
+  c->layout_tile_rows = c->tile_rows;
   c->ready = true;
   return B2DEV_OK;
 }

@@ -325,3 +325,35 @@ def test_polydisperse_pile_against_compiled_reference():
     assert same_bits(R, Rr) and same_bits(U, Ur)
     assert ldy.merit <= 1e-6 or gs.iters == 1000
     ldy.close()
+
+
+def test_layout_reuse_follows_tile_rows():
+    """An unchanged contact graph reuses the colouring and the colour-sorted
+    layout with its tile table; a change of rows per tile in between rebuilds
+    the tile table. Every solve equals a fresh context's bitwise (rows per tile
+    never change results)."""
+    from solfec_b200._lib import lib
+    sc = scene_cache('hexahedra_lattice', nx=20, ny=20, nz=6)
+    nxt = scenes.advance_velocities(sc, np.zeros((sc.ncon, 3)))
+
+    def solve(ldy):
+        gs = GAUSS_SEIDEL_SOLVER(1e-4, 1000, 1e-4)
+        gs.solve(ldy)
+        R, U, _ = ldy.get_state()
+        return gs.iters, R, U
+
+    fresh = LOCDYN()
+    fresh.update_begin(nxt)
+    ref = solve(fresh)
+    fresh.close()
+    ldy = LOCDYN()
+    ldy.update_begin(sc)
+    for rows in (8, 8, 32, 16):
+        assert lib().b2dev_set_tile_rows(ldy.device_context, rows) == 0
+        reuse0 = ldy.colour_reuse_count()
+        ldy.update_begin(nxt)
+        assert ldy.colour_reuse_count() == reuse0 + 1
+        assert lib().b2dev_tile_rows(ldy.device_context) == rows
+        it, R, U = solve(ldy)
+        assert it == ref[0] and same_bits(R, ref[1]) and same_bits(U, ref[2])
+    ldy.close()
