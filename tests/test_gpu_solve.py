@@ -327,7 +327,7 @@ def test_polydisperse_pile_against_compiled_reference():
     ldy.close()
 
 
-def test_layout_reuse_follows_tile_rows():
+def test_layout_reuse_follows_tile_rows(scene_cache):
     """An unchanged contact graph reuses the colouring and the colour-sorted
     layout with its tile table; a change of rows per tile in between rebuilds
     the tile table. Every solve equals a fresh context's bitwise (rows per tile
