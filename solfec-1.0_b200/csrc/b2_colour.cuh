@@ -148,16 +148,25 @@ __global__ void k_sorted_degree(int n, const int* perm, const int* adjptr, int* 
 // W_ij = h H_i^b M_b^-1 H_j^b^T for j > i (ldy.c:738-794, serial form
 // left = H_i, right = M^-1 H_j^T) and the transposed block of the pair for
 // j < i (ldy.c:829-844); the transposed block is recomputed with identical
-// operands and order, so it is bitwise the transpose. Warp per sorted row.
-__global__ void k_offdiag_assembled(int n, const int* perm, const int* iperm, const int* adjptr, const int* adjcol,
-                                    const int* adjbod, const int* master, const double* factors, double step,
-                                    const int* rowptr, int* col, double* W64, float* W32, long long kstride) {
-  const int p = blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
-  const int lane = threadIdx.x & (kWarp - 1);
-  if (p >= n) return;
+// operands and order, so it is bitwise the transpose. Thread per sorted
+// block (coalesced plane writes); the block's sorted row by binary search in
+// the sorted row offsets.
+__global__ void k_offdiag_assembled(int n, long long K, const int* perm, const int* iperm, const int* adjptr,
+                                    const int* adjcol, const int* adjbod, const int* master, const double* factors,
+                                    double step, const int* rowptr, int* col, double* W64, float* W32,
+                                    long long kstride) {
+  const long long qo = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (qo >= K) return;
+  int lo_r = 0, hi_r = n;  // rowptr[lo_r] <= qo < rowptr[hi_r]
+  while (hi_r - lo_r > 1) {
+    const int mid = (lo_r + hi_r) >> 1;
+    if (rowptr[mid] <= qo) lo_r = mid; else hi_r = mid;
+  }
+  const int p = lo_r;
   const int i = perm[p];
-  const int kb = adjptr[i], d = adjptr[i + 1] - kb, qb = rowptr[p];
-  for (int t = lane; t < d; t += kWarp) {
+  const int t = (int)(qo - rowptr[p]);
+  {
+    const int kb = adjptr[i];
     const int j = adjcol[kb + t], b = adjbod[kb + t];
     const int lo = j > i ? i : j, hi = j > i ? j : i;
     const double* left = factors + (size_t)lo * kFactorStride + (master[lo] == b ? 0 : 36);
@@ -170,7 +179,6 @@ __global__ void k_offdiag_assembled(int n, const int* perm, const int* iperm, co
     hp_add(Lr, Pr, W);
 #pragma unroll
     for (int q = 0; q < 9; q++) W[q] *= step;
-    const long long qo = qb + t;
     col[qo] = iperm[j];
 #pragma unroll
     for (int r = 0; r < 3; r++)

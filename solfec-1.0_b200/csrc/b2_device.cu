@@ -407,8 +407,8 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   if (n > 0 && K > 0) {
     if (assembled) {
       c->launches++;
-      k_offdiag_assembled<<<blocks_for(n, wpb), wpb * kWarp, 0, st>>>(
-          n, ptr<int>(c->perm), ptr<int>(c->iperm), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<int>(c->adjbod),
+      k_offdiag_assembled<<<blocks_for(K, 256), 256, 0, st>>>(
+          n, K, ptr<int>(c->perm), ptr<int>(c->iperm), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<int>(c->adjbod),
           ptr<int>(c->master), ptr<double>(c->factors), c->step, ptr<int>(c->rowptr), ptr<int>(c->col),
           ptr<double>(c->W64), ptr<float>(c->W32), c->kstride);
     } else {
