@@ -105,8 +105,9 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, 'gpurun_out', 'clocks_bench.csv') if os.path.isdir(
-            os.path.join(ROOT, 'gpurun_out')) else '/tmp/b2_clocks_%d.csv' % os.getpid()
+        # the raw samples go to B2_CLOCKS_CSV when set (the JSON line carries their summary)
+        self.path = os.environ.get('B2_CLOCKS_CSV') or os.path.join(
+            os.environ.get('TMPDIR', '/tmp'), 'b2_clocks_%d.csv' % os.getpid())
 
     def __enter__(self):
         try:
