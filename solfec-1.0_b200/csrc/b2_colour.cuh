@@ -191,6 +191,59 @@ __global__ void k_offdiag_assembled(int n, long long K, const int* perm, const i
   }
 }
 
+// Tile of every sorted row (forward tile numbering).
+__global__ void k_row_tile(int T, const int4* tiles, int* rtile) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  const int4 ti = tiles[t];
+  for (int r = 0; r < (ti.y & 63); r++) rtile[ti.x + r] = t;
+}
+
+// The tiles holding the neighbours of a tile's rows, earlier (side 0) and
+// later (side 1) in forward colour order, each tile once: a per-warp hash
+// table in shared memory (hcap slots per side, at least twice the tile's
+// blocks, so a probe always ends) deduplicates them. With depE null it counts
+// (cnt[side * (T + 1) + t]); otherwise it writes the lists at the scanned
+// offsets, in arbitrary order (they are sets). Warp per tile.
+__global__ void k_tile_deps(int T, const int4* tiles, const int2* tilek, const int* col, const int* rtile, int hcap,
+                            int* cnt, const int* ptrE, const int* ptrL, int* depE, int* depL) {
+  extern __shared__ int dep_smem[];
+  const int wpb = blockDim.x / kWarp, warp = threadIdx.x / kWarp, lane = threadIdx.x & (kWarp - 1);
+  const int t = blockIdx.x * wpb + warp;
+  if (t >= T) return;  // uniform per warp
+  int* tab = dep_smem + (size_t)warp * (2 * hcap + 2);
+  int* num = tab + 2 * hcap;
+  for (int i = lane; i < 2 * hcap; i += kWarp) tab[i] = -1;
+  if (lane < 2) num[lane] = 0;
+  __syncwarp();
+  const int4 ti = tiles[t];
+  const int2 tk = tilek[t];
+  const bool fill = depE != nullptr;
+  for (int k = tk.x + lane; k < tk.y; k += kWarp) {
+    const int j = col[k];
+    if (j >= ti.z && j < ti.w) continue;  // a row of the same colour (none: they share no body)
+    const int side = j < ti.z ? 0 : 1;
+    const int d = rtile[j];
+    int* tb = tab + side * hcap;
+    unsigned h = ((unsigned)d * 2654435761u) & (unsigned)(hcap - 1);
+    while (true) {
+      const int old = atomicCAS(tb + h, -1, d);
+      if (old == -1) {
+        const int pos = atomicAdd(num + side, 1);
+        if (fill) {
+          if (side == 0) depE[ptrE[t] + pos] = d;
+          else depL[ptrL[t] + pos] = d;
+        }
+        break;
+      }
+      if (old == d) break;
+      h = (h + 1) & (unsigned)(hcap - 1);
+    }
+  }
+  __syncwarp();
+  if (!fill && lane < 2) cnt[lane * (T + 1) + t] = num[lane];
+}
+
 // Off-diagonal blocks handed in by the caller (AoS, 9 doubles per block in
 // caller CSR order) gathered into the colour-sorted plane layout.
 __global__ void k_offdiag_copy(int n, const int* perm, const int* iperm, const int* adjptr, const int* adjcol,

@@ -188,6 +188,9 @@ struct b2dev_ctx {
   int nprob = 1;
   std::vector<int> prob_off;
   Buf tiles, tilek, tile_prob, ptile_ptr, ptile, row_prob, pctl, pfe, pvec;
+  // per tile: the tiles its rows depend on (earlier / later colours) and its completion flag
+  Buf rtile, dcnt, depE_ptr, depL_ptr, depE, depL, tile_done;
+  bool deps_valid = false;
   // rigid time integration (b2dev_rigid_*): mass centre, inertia, mass, scheme,
   // external force of the step, NEW2 auxiliary vector, per-step loads
   Buf rb_x, rb_J, rb_mass, rb_scheme, rb_fext, rb_aux, rb_loads;
@@ -235,6 +238,52 @@ int cooperative_grid(const void* func, int threads, int sms, int want, int* grid
   }
   int cap = per_sm * sms;
   *grid = std::max(1, std::min(cap, want > 0 ? want : cap));
+  return B2DEV_OK;
+}
+
+// Per tile, the tiles holding its rows' neighbours (in earlier and in later
+// colours, each once) and a completion flag per tile: a tile waits for these
+// few flags in one parallel round instead of one acquire per neighbour row.
+// Without them (tiles too large for the deduplication table) the solve waits
+// per row.
+int build_deps(b2dev_ctx* c) {
+  cudaStream_t st = c->stream;
+  c->deps_valid = false;
+  const int T = c->ntiles, n = c->n;
+  if (T == 0 || c->K == 0) return B2DEV_OK;
+  int hcap = 64;
+  while (hcap < 2 * c->max_tile_blocks + 2) hcap *= 2;
+  const size_t per_warp = sizeof(int) * (2 * (size_t)hcap + 2);
+  if (per_warp > 200 * 1024) return B2DEV_OK;
+  const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / per_warp));
+  const size_t smem = per_warp * wpb;
+  B2_TRY(ensure(c->rtile, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->dcnt, sizeof(int) * 2 * (T + 1)));
+  B2_TRY(ensure(c->depE_ptr, sizeof(int) * (T + 1)));
+  B2_TRY(ensure(c->depL_ptr, sizeof(int) * (T + 1)));
+  B2_TRY(ensure(c->tile_done, sizeof(int) * (T + 1)));
+  c->launches++;
+  k_row_tile<<<blocks_for(T, 256), 256, 0, st>>>(T, ptr<int4>(c->tiles), ptr<int>(c->rtile));
+  B2_CK(cudaMemsetAsync(c->dcnt.p, 0, sizeof(int) * 2 * (T + 1), st));
+  B2_CK(cudaFuncSetAttribute((const void*)k_tile_deps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  c->launches++;
+  k_tile_deps<<<blocks_for(T, wpb), wpb * kWarp, smem, st>>>(T, ptr<int4>(c->tiles), ptr<int2>(c->tilek),
+                                                             ptr<int>(c->col), ptr<int>(c->rtile), hcap,
+                                                             ptr<int>(c->dcnt), nullptr, nullptr, nullptr, nullptr);
+  B2_TRY(scan_exclusive(c, ptr<int>(c->dcnt), ptr<int>(c->depE_ptr), T + 1));
+  B2_TRY(scan_exclusive(c, ptr<int>(c->dcnt) + T + 1, ptr<int>(c->depL_ptr), T + 1));
+  int tot[2] = {0, 0};
+  B2_CK(cudaMemcpyAsync(&tot[0], ptr<int>(c->depE_ptr) + T, sizeof(int), cudaMemcpyDeviceToHost, st));
+  B2_CK(cudaMemcpyAsync(&tot[1], ptr<int>(c->depL_ptr) + T, sizeof(int), cudaMemcpyDeviceToHost, st));
+  B2_CK(cudaStreamSynchronize(st));
+  B2_TRY(ensure(c->depE, sizeof(int) * (tot[0] + 1)));
+  B2_TRY(ensure(c->depL, sizeof(int) * (tot[1] + 1)));
+  c->launches++;
+  k_tile_deps<<<blocks_for(T, wpb), wpb * kWarp, smem, st>>>(
+      T, ptr<int4>(c->tiles), ptr<int2>(c->tilek), ptr<int>(c->col), ptr<int>(c->rtile), hcap, ptr<int>(c->dcnt),
+      ptr<int>(c->depE_ptr), ptr<int>(c->depL_ptr), ptr<int>(c->depE), ptr<int>(c->depL));
+  B2_CK(cudaGetLastError());
+  c->deps_valid = true;
   return B2DEV_OK;
 }
 
@@ -287,7 +336,7 @@ int build_tiles(b2dev_ctx* c, int rows) {
   }
   B2_CK(cudaMemcpyAsync(c->ptile_ptr.p, pptr.data(), sizeof(int) * (c->nprob + 1), cudaMemcpyHostToDevice, st));
   B2_CK(cudaStreamSynchronize(st));  // the host vectors above go out of scope
-  return B2DEV_OK;
+  return build_deps(c);
 }
 
 // Colour the caller-order graph (adjptr/adjcol) and build the colour-sorted
@@ -560,6 +609,11 @@ int solve_setup(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter
   A.ptile_ptr = ptr<int>(c->ptile_ptr);
   A.ptile = ptr<int>(c->ptile);
   A.done = ptr<int>(c->done);
+  if (c->deps_valid) {
+    A.depE_ptr = ptr<int>(c->depE_ptr); A.depE = ptr<int>(c->depE);
+    A.depL_ptr = ptr<int>(c->depL_ptr); A.depL = ptr<int>(c->depL);
+    A.tile_done = ptr<int>(c->tile_done);
+  }
   A.decided = ptr<int>(c->decided);
   A.rowptr = ptr<int>(c->rowptr);
   A.col = ptr<int>(c->col);
@@ -624,6 +678,7 @@ int solve_enqueue(b2dev_ctx* c, bool mixed, const SolveArgs& a, int grid, size_t
   B2_CK(cudaMemsetAsync(c->sctrl.p, 0, sizeof(SolveControl), st));
   B2_CK(cudaMemsetAsync(c->pctl.p, 0, sizeof(ProblemControl) * P, st));
   B2_CK(cudaMemsetAsync(c->done.p, 0, sizeof(int) * (n + 1), st));
+  if (a.tile_done) B2_CK(cudaMemsetAsync(a.tile_done, 0, sizeof(int) * (a.ntiles + 1), st));
   B2_CK(cudaMemsetAsync(c->decided.p, 0, sizeof(int) * (size_t)P * a.pstride, st));
   if (a.iter0 == 0) {
     B2_CK(cudaMemsetAsync(c->failkey.p, 0, sizeof(unsigned long long) * (size_t)P * a.pstride, st));
@@ -752,7 +807,7 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->cctrl, &c->keys_out, &c->iota, &c->perm, &c->iperm, &c->colptr, &c->sdeg, &c->rowptr, &c->col,
                 &c->W64, &c->W32, &c->Wd, &c->Ad, &c->Bv, &c->Vv, &c->rho, &c->gap, &c->fric, &c->rest, &c->coh,
                 &c->R64[0], &c->R64[1], &c->R64[2], &c->R32[0], &c->R32[1], &c->R32[2], &c->Us[0], &c->Us[1],
-                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tilek, &c->rb_x, &c->rb_J, &c->rb_mass, &c->rb_scheme, &c->rb_fext, &c->rb_aux, &c->rb_loads, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec, &c->gptr_prev, &c->gcol_prev,
+                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tilek, &c->rtile, &c->dcnt, &c->depE_ptr, &c->depL_ptr, &c->depE, &c->depL, &c->tile_done, &c->rb_x, &c->rb_J, &c->rb_mass, &c->rb_scheme, &c->rb_fext, &c->rb_aux, &c->rb_loads, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec, &c->gptr_prev, &c->gcol_prev,
                 &c->part, &c->rer,
                 &c->mer, &c->failkey, &c->failcount, &c->sctrl, &c->io, &c->cub_tmp, &c->trace};
   for (Buf* b : all)

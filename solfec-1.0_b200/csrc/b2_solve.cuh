@@ -113,6 +113,14 @@ struct SolveArgs {
   double4* Um[2];           // merit U computed in sweep s: Um[s%2]
   double* conmerit[2];      // per-row merit numerator computed in sweep s: conmerit[s%2] (may be null)
   int* done;                // [n] sweeps completed per row (zeroed before launch)
+  // per tile (forward numbering), when available: the tiles holding its rows'
+  // neighbours in earlier / later colours, and sweeps completed per tile
+  // (zeroed before launch); null: the per-row flags above are used instead
+  const int* depE_ptr;
+  const int* depE;
+  const int* depL_ptr;
+  const int* depL;
+  int* tile_done;
   int* decided;             // [nprob][pstride] decision after each sweep (zeroed before launch)
   double* part;             // [3][ntiles][4] per-tile partial sums
   double* rerhist;          // [nprob][pstride] history arrays (indexed by iter0 + k)
@@ -188,6 +196,18 @@ __device__ __noinline__ int gate_wait_spin(const int* decided_s2, const int* pst
 __device__ __forceinline__ int gate_wait(const int* decided_s2, const int* pstop, SolveControl* ctrl) {
   if (ld_acquire(decided_s2) == DECIDE_CONTINUE) return 1;
   return gate_wait_spin(decided_s2, pstop, ctrl);
+}
+
+// Bounded wait until every tile of list[lo, hi) has completed `need` sweeps:
+// the lanes take the entries in turn (one parallel round for a typical tile),
+// and the warp barrier after the waits orders every lane's later loads after
+// all of them (each tile publishes its rows with one release after its own
+// warp barrier).
+__device__ __forceinline__ bool wait_tiles(const int* list, int lo, int hi, const int* tile_done, int need,
+                                           SolveControl* ctrl, int lane) {
+  bool ok = true;
+  for (int i = lo + lane; i < hi; i += kWarp) ok = wait_at_least(tile_done + __ldg(list + i), need, ctrl) && ok;
+  return ok;
 }
 
 // 32-byte load that bypasses L1 (reaction buffers are rewritten by other SMs
@@ -379,8 +399,9 @@ __host__ __device__ constexpr size_t solve_smem_per_block() {
 // the solve has stopped.
 template <bool MIXED>
 __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags& f, int r0, int nr, int cs, int ce,
-                                           int s, int rin, int rout, int prob, int kb0, int ke0, unsigned char* wsm,
-                                           uint32_t& phase, double& errup, double& errlo, double& mnum) {
+                                           int s, int rin, int rout, int prob, int kb0, int ke0, int tile,
+                                           unsigned char* wsm, uint32_t& phase, double& errup, double& errlo,
+                                           double& mnum) {
   typedef typename std::conditional<MIXED, float, double>::type real;
   constexpr int kChunkUnroll = chunk_unroll<MIXED>();
   constexpr int kSlots = kWarp * kChunkUnroll;
@@ -425,7 +446,17 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   if (lane <= nr) tp[lane] = __ldg(a.rowptr + r0 + lane);
   if (lane == 0 && nr == kWarp) tp[kWarp] = __ldg(a.rowptr + r0 + kWarp);
   bool ok = true;
-  if (own && !f.prev_done) ok = wait_at_least(a.done + p, s, a.ctrl);  // this row's previous sweep is complete
+  const bool by_tile = a.tile_done != nullptr;
+  if (!f.prev_done) {  // the rows and all neighbours of this tile have completed the previous sweep
+    if (by_tile) {
+      if (lane == 0) ok = wait_at_least(a.tile_done + tile, s, a.ctrl);
+      ok = wait_tiles(a.depE, __ldg(a.depE_ptr + tile), __ldg(a.depE_ptr + tile + 1), a.tile_done, s, a.ctrl, lane) && ok;
+      ok = wait_tiles(a.depL, __ldg(a.depL_ptr + tile), __ldg(a.depL_ptr + tile + 1), a.tile_done, s, a.ctrl, lane) && ok;
+      __syncwarp();
+    } else if (own) {
+      ok = wait_at_least(a.done + p, s, a.ctrl);
+    }
+  }
 
   double B[3] = {0.0, 0.0, 0.0}, W[9], Rold[3] = {0.0, 0.0, 0.0}, ag[3], am[3] = {0.0, 0.0, 0.0};
   double V[3] = {0.0, 0.0, 0.0};
@@ -473,7 +504,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
       const int j = col_s[k - a0];
       const bool earlier = f.backward ? (j >= ce) : (j < cs);
       if (f.merit || (f.gs && !earlier)) {
-        if (!f.prev_done) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
+        if (!f.prev_done && !by_tile) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
         cp_async16(smem_addr(slot + (k - wb)), a.R32[rin] + j);
       }
     }
@@ -498,7 +529,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
               const float4 v = slot[g];
               ro0 = v.x; ro1 = v.y; ro2 = v.z;
             } else {
-              if (!f.prev_done) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
+              if (!f.prev_done && !by_tile) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
               load_r<MIXED, real>(a, rin, j, ro0, ro1, ro2);
             }
             const real* Wk = w[u];
@@ -526,7 +557,37 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
       if (a.conmerit[0]) a.conmerit[s & 1][p] = up;
     }
     if (!f.gs) continue;
+    if (by_tile && win == 0) {  // every tile holding an earlier neighbour has completed this sweep
+      const int* ptr = f.backward ? a.depL_ptr : a.depE_ptr;
+      ok = wait_tiles(f.backward ? a.depL : a.depE, __ldg(ptr + tile), __ldg(ptr + tile + 1), a.tile_done, s + 1,
+                      a.ctrl, lane) && ok;
+      __syncwarp();
+    }
     // ---- pass 2: neighbours earlier in this sweep (their new reactions)
+    bool gathered = false;
+    if constexpr (gather_r<MIXED>()) {
+      if (by_tile) {  // no wait left per neighbour: all new reactions in one round of asynchronous copies
+        auto is_earlier = [&](int j) { return f.backward ? (j >= ce) : (j < cs); };
+        for (int k = wb + lane; k < we; k += kWarp) {
+          const int j = col_s[k - a0];
+          if (is_earlier(j)) cp_async16(smem_addr(slot + (k - wb)), a.R32[rout] + j);
+        }
+        cp_async_wait_all();
+        for (int k = wb + lane; k < we; k += kWarp) {
+          const int j = col_s[k - a0];
+          if (is_earlier(j)) {
+            const float4 v = slot[k - wb];
+            real Wk[9];
+#pragma unroll
+            for (int q = 0; q < 9; q++) Wk[q] = w_s[q * wstride + k - a0];
+            put(k - wb, Wk[0] * v.x + Wk[3] * v.y + Wk[6] * v.z, Wk[1] * v.x + Wk[4] * v.y + Wk[7] * v.z,
+                Wk[2] * v.x + Wk[5] * v.y + Wk[8] * v.z);
+          }
+        }
+        gathered = true;
+      }
+    }
+    if (!gathered)
     for (int base = wb; base < we; base += kSlots) {
 #pragma unroll
       for (int u = 0; u < kChunkUnroll; u++) {
@@ -535,7 +596,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
           const int j = col_s[k - a0];
           const bool earlier = f.backward ? (j >= ce) : (j < cs);
           if (earlier) {
-            ok = wait_at_least(a.done + j, s + 1, a.ctrl) && ok;
+            if (!by_tile) ok = wait_at_least(a.done + j, s + 1, a.ctrl) && ok;
             real Wk[9];
 #pragma unroll
             for (int q = 0; q < 9; q++) {
@@ -594,9 +655,10 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
       errup += d0 * d0 + d1 * d1 + d2 * d2;
       errlo += R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
     }
-    st_release(a.done + p, s + 1);  // publishes this row's writes of sweep s
+    if (!by_tile) st_release(a.done + p, s + 1);  // publishes this row's writes of sweep s
   }
   __syncwarp();
+  if (by_tile && lane == 0) st_release(a.tile_done + tile, s + 1);  // publishes the tile's writes of sweep s
   return true;
 }
 
@@ -748,7 +810,7 @@ __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constan
     const int rin = (a.in + s) % 3;       // iterate s-1
     const int rout = (a.in + s + 1) % 3;  // iterate s
     double errup = 0.0, errlo = 0.0, mnum = 0.0;
-    if (!solve_tile<MIXED>(a, f, ti.x, nr, ti.z, ti.w, s, rin, rout, prob, tk.x, tk.y, wsm, phase, errup, errlo, mnum)) break;
+    if (!solve_tile<MIXED>(a, f, ti.x, nr, ti.z, ti.w, s, rin, rout, prob, tk.x, tk.y, tile, wsm, phase, errup, errlo, mnum)) break;
 #pragma unroll
     for (int d = 16; d >= 1; d >>= 1) {
       errup += __shfl_down_sync(0xffffffffu, errup, d);
