@@ -125,38 +125,45 @@ struct NnDst {
   }
 };
 
-// Merit numerator of every row for the reactions R (mrf.c:61-87 arithmetic:
-// U = B + W_ii R_i + sum_j W_ij R_j in list order, up = <A C, C>).
+// Merit numerators of every row for two sets of reactions Ra and Rb in one
+// pass over W (mrf.c:61-87 arithmetic for each: U = B + W_ii R_i + sum_j
+// W_ij R_j in list order, up = <A C, C>).
 __global__ void k_merit_rows(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
                              const double* __restrict__ W64, long long kstride, const double* __restrict__ Wd,
                              const double* __restrict__ Ad, const double* __restrict__ Bv,
                              const double* __restrict__ Vv, const double* __restrict__ gap,
                              const double* __restrict__ fric, const double* __restrict__ rest,
-                             const double* __restrict__ coh, double step, int dynamic, const double4* __restrict__ R,
-                             double* __restrict__ up) {
+                             const double* __restrict__ coh, double step, int dynamic, const double4* __restrict__ Ra,
+                             const double4* __restrict__ Rb, double* __restrict__ upa, double* __restrict__ upb) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
-  double B[3], W[9], A[9], V[3], U[3];
-  const double4 rp = R[p];
-  const double Rp[3] = {rp.x, rp.y, rp.z};
+  double B[3], W[9], A[9], V[3], Ua[3], Ub[3];
+  const double4 ra = Ra[p], rb = Rb[p];
+  const double Rpa[3] = {ra.x, ra.y, ra.z}, Rpb[3] = {rb.x, rb.y, rb.z};
 #pragma unroll
   for (int q = 0; q < 3; q++) { B[q] = Bv[(size_t)q * n + p]; V[q] = Vv[(size_t)q * n + p]; }
 #pragma unroll
   for (int q = 0; q < 9; q++) { W[q] = Wd[(size_t)q * n + p]; A[q] = Ad[(size_t)q * n + p]; }
-  nvaddmul(B, W, Rp, U);
+  nvaddmul(B, W, Rpa, Ua);
+  nvaddmul(B, W, Rpb, Ub);
   for (int k = rowptr[p]; k < rowptr[p + 1]; k++) {
-    const double4 rj = R[col[k]];
+    const int j = col[k];
+    const double4 ja = Ra[j], jb = Rb[j];
     double w[9];
 #pragma unroll
     for (int q = 0; q < 9; q++) w[q] = W64[q * kstride + k];
-    U[0] = U[0] + (w[0] * rj.x + w[3] * rj.y + w[6] * rj.z);
-    U[1] = U[1] + (w[1] * rj.x + w[4] * rj.y + w[7] * rj.z);
-    U[2] = U[2] + (w[2] * rj.x + w[5] * rj.y + w[8] * rj.z);
+    Ua[0] = Ua[0] + (w[0] * ja.x + w[3] * ja.y + w[6] * ja.z);
+    Ua[1] = Ua[1] + (w[1] * ja.x + w[4] * ja.y + w[7] * ja.z);
+    Ua[2] = Ua[2] + (w[2] * ja.x + w[5] * ja.y + w[8] * ja.z);
+    Ub[0] = Ub[0] + (w[0] * jb.x + w[3] * jb.y + w[6] * jb.z);
+    Ub[1] = Ub[1] + (w[1] * jb.x + w[4] * jb.y + w[7] * jb.z);
+    Ub[2] = Ub[2] + (w[2] * jb.x + w[5] * jb.y + w[8] * jb.z);
   }
   ContactParams cp;
   cp.friction = fric[p]; cp.restitution = rest[p]; cp.cohesion = coh[p]; cp.gap = gap[p]; cp.step = step;
   cp.dynamic = dynamic;
-  up[p] = merit_row(cp, A, V, U, Rp);
+  upa[p] = merit_row(cp, A, V, Ua, Rpa);
+  upb[p] = merit_row(cp, A, V, Ub, Rpb);
 }
 
 }  // namespace
@@ -416,25 +423,30 @@ NnRows nn_rows(b2dev_ctx* c) {
 }
 
 // merit of reactions R (sorted order) into *out (host)
-int merit_of(b2dev_ctx* c, const double4* R, double* out) {
+// Merits (mrf.c:176-184) of two sets of reactions, one pass over W.
+int merit_of2(b2dev_ctx* c, const double4* Ra, const double4* Rb, double* outa, double* outb) {
   const int n = c->n;
   cudaStream_t st = c->stream;
-  B2_TRY(ensure(c->fe_part, sizeof(double) * (n + 1)));
+  B2_TRY(ensure(c->fe_part, sizeof(double) * 2 * (n + 1)));
+  double* pa = ptr<double>(c->fe_part);
+  double* pb = pa + (n + 1);
   c->launches++;
   k_merit_rows<<<blocks_for(n, 128), 128, 0, st>>>(n, ptr<int>(c->rowptr), ptr<int>(c->col), ptr<double>(c->W64),
                                                    c->kstride, ptr<double>(c->Wd), ptr<double>(c->Ad),
                                                    ptr<double>(c->Bv), ptr<double>(c->Vv), ptr<double>(c->gap),
                                                    ptr<double>(c->fric), ptr<double>(c->rest), ptr<double>(c->coh),
-                                                   c->step, c->dynamic, R, ptr<double>(c->fe_part));
+                                                   c->step, c->dynamic, Ra, Rb, pa, pb);
   B2_TRY(ensure(c->io, sizeof(double) * 2));
-  c->launches++;
-  k_sum_partials<<<1, 1024, 0, st>>>(ptr<double>(c->fe_part), n, ptr<double>(c->io));  // 0.5 sum up
-  double half = 0.0;
-  B2_CK(cudaMemcpyAsync(&half, c->io.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+  c->launches += 2;
+  k_sum_partials<<<1, 1024, 0, st>>>(pa, n, ptr<double>(c->io));  // 0.5 sum up
+  k_sum_partials<<<1, 1024, 0, st>>>(pb, n, ptr<double>(c->io) + 1);
+  double half[2] = {0.0, 0.0};
+  B2_CK(cudaMemcpyAsync(half, c->io.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
   B2_CK(cudaStreamSynchronize(st));
   double lo = c->free_energy < DBL_EPSILON ? 1.0 : c->free_energy;  // mrf.c:45
   lo = lo == 0.0 ? 1.0 : lo;
-  *out = half / lo;
+  *outa = half[0] / lo;
+  *outb = half[1] / lo;
   return B2DEV_OK;
 }
 
@@ -486,9 +498,9 @@ int b2dev_nn_warm_start(b2dev_ctx* c, b2dev_mlp* net, double accept_ratio, b2dev
   B2_CK(cudaGetLastError());
   int err = 0;
   B2_CK(cudaMemcpyAsync(&err, net->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-  B2_TRY(merit_of(c, ptr<double4>(c->R64[cand]), &rep->merit_nn));
+  B2_TRY(merit_of2(c, ptr<double4>(c->R64[cand]), ptr<double4>(c->R64[c->state_r]), &rep->merit_nn,
+                   &rep->merit_plain));
   if (err) { set_err("nn_warm_start: a bounded tensor-core wait timed out"); return B2DEV_ETIMEOUT; }
-  B2_TRY(merit_of(c, ptr<double4>(c->R64[c->state_r]), &rep->merit_plain));
   // the plain start stays unless the network's reactions have a merit below
   // accept_ratio times the plain start's (1: any improvement)
   rep->used_nn = rep->merit_nn < accept_ratio * rep->merit_plain ? 1 : 0;
