@@ -460,6 +460,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
 
   double B[3] = {0.0, 0.0, 0.0}, W[9], Rold[3] = {0.0, 0.0, 0.0}, ag[3], am[3] = {0.0, 0.0, 0.0};
   double V[3] = {0.0, 0.0, 0.0};
+  double rho_row = 0.0;  // the diagonal solver's rho, loaded with the row data
   ContactParams cp;
   cp.step = a.step;
   cp.dynamic = a.dynamic;
@@ -476,6 +477,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
     cp.restitution = __ldg(a.rest + p);
     cp.cohesion = __ldg(a.coh + p);
     cp.gap = __ldg(a.gap + p);
+    rho_row = __ldg(a.rho + p);
 #pragma unroll
     for (int q = 0; q < 3; q++) V[q] = __ldg(a.Vv + (size_t)q * n + p);
   }
@@ -635,7 +637,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
 #pragma unroll
         for (int q = 0; q < 3; q++) { tr[q] = ag[q]; tr[3 + q] = U[q]; tr[6 + q] = R[q]; }
       }
-      const int kind = diagonal_solve_row(a.diagsolver, a.failure, cp, a.diagepsilon, a.diagmaxiter, __ldg(a.rho + p),
+      const int kind = diagonal_solve_row(a.diagsolver, a.failure, cp, a.diagepsilon, a.diagmaxiter, rho_row,
                                           W, ag, V, U, R);
       if (tr) {
 #pragma unroll
