@@ -472,7 +472,6 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
     Rold[0] = ro.x; Rold[1] = ro.y; Rold[2] = ro.z;
 #pragma unroll
     for (int q = 0; q < 9; q++) W[q] = __ldg(a.Wd + (size_t)q * n + p);
-    if (f.merit) nvaddmul(B, W, Rold, am);
     cp.friction = __ldg(a.fric + p);
     cp.restitution = __ldg(a.rest + p);
     cp.cohesion = __ldg(a.coh + p);
@@ -543,6 +542,9 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
     }
     __syncwarp();
     if (f.merit) {  // each row adds its own merit products, in list order
+      // the row's own term first (ag still holds B here); set here, not at the
+      // row load, so that the load's latency hides behind the window's staging
+      if (win == 0 && own) nvaddmul(ag, W, Rold, am);
       const int lo = mb > wb ? mb : wb;
       const int hi = me < we ? me : we;
       for (int k = lo; k < hi; k++) add(k - wb, am);
