@@ -290,6 +290,65 @@ GRAVITY_VEC = (0.0, 0.0, -9.81)
 RIGID_CPU_SAMPLE = 2000
 
 
+# Sphere contact detection (csrc/b2_detect.cuh) on a grid of DETECT_GRID^3
+# overlapping spheres. Algorithmic bytes, each datum of a kernel counted once:
+# per sphere 520 B (current centre from the body: body index, referential
+# centre, radius, rotation, mass centres, written centre; grid cell and bucket;
+# one radix-sort pass over key and index; the sphere's own data in the count
+# and write passes; pair count and offset), per contact 1064 B (pair indices
+# written, ordered and read; the matched previous contact with its R and U; the
+# two spheres' centres, radii, bodies and surfaces; the 272-byte contact record
+# written, read back by the sparsification and the compaction and written
+# again; the body lists).
+DETECT_GRID = 100
+DETECT_BYTES_SPHERE = 520
+DETECT_BYTES_CONTACT = 1064
+DETECT_REPS = 10
+
+
+def detect_timing():
+    """Host call time of b2dev_detect_spheres (SPHERES.detect) on 1M spheres:
+    the first call detects every contact, the timed calls (after 3 warm-up
+    calls) update them all (same bodies); each call includes its three host
+    synchronisations (pair count, contact count, completion)."""
+    import time
+    import torch
+    from solfec_b200 import LOCDYN, scenes
+    from solfec_b200.detect import SPHERES, bodies_only
+    from solfec_b200.dynamics import RIGID_DYNAMICS
+    sc = scenes.spheres_grid(DETECT_GRID)
+    sp = scenes.sphere_shapes(sc, friction=0.3)
+    J, mass = scenes.sphere_inertia(sc)
+    ldy = LOCDYN()
+    try:
+        ldy.update_begin(bodies_only(sc))
+        RIGID_DYNAMICS(ldy, J, mass, sc.x)
+        s = SPHERES(ldy, **sp)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        nc, nn = s.detect()
+        first = time.perf_counter() - t0
+        for _ in range(3):
+            s.detect()
+        ts = []
+        for _ in range(DETECT_REPS):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.detect()
+            ts.append(time.perf_counter() - t0)
+        ms = float(np.median(ts)) * 1e3
+        nb = DETECT_BYTES_SPHERE * s.nsph + DETECT_BYTES_CONTACT * s.ncon
+        peak = _peaks()[0]
+        return {'workload': 'spheres-grid-%d: %d^3 spheres, pitch 0.0999, radius 0.05' % (s.nsph, DETECT_GRID),
+                'spheres': s.nsph, 'contacts': int(s.ncon), 'new_first_call': int(nn),
+                'first_call_ms': round(first * 1e3, 3), 'update_call_ms': round(ms, 3),
+                'contacts_per_s': round(s.ncon / (ms * 1e-3), 1), 'bytes_per_call': int(nb),
+                'achieved_gbs': round(nb / (ms * 1e-3) / 1e9, 1), 'peak_gbs': peak,
+                'frac': round(nb / (ms * 1e-3) / 1e9 / peak, 3), 'timing': 'host call time, median of %d' % DETECT_REPS}
+    finally:
+        ldy.close()
+
+
 def _rigid_inertia(sc, k=None):
     k = sc.nbod if k is None else k
     ob = sc.obstacle[:k] != 0  # walls: zero inverse inertia and mass (never accelerated)
@@ -649,6 +708,10 @@ def main():
             'clocks': out['clocks'],
             'rigid_step': rigid,
         }
+        try:
+            line['detect'] = detect_timing()
+        except Exception as e:  # the headline line is printed whatever happens here
+            line['detect'] = {'error': str(e)[:300]}
         print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.barrier()

@@ -107,6 +107,41 @@ int b2dev_rigid_step_begin(b2dev_ctx* ctx, double step, const double* gravity, c
 int b2dev_rigid_step_end(b2dev_ctx* ctx, double step);
 int b2dev_rigid_get(b2dev_ctx* ctx, double* rot, double* x, double* velo, double* velo0, int on_device);
 
+/* Contact update and detection between spheres held by the uploaded bodies:
+ * the contact part of DOM_Update_Begin (dom.c:3700-3790) for sphere pairs, on
+ * the device bodies (rotation of b2dev_upload_scene, mass centre of
+ * b2dev_rigid_setup, both as moved by the b2dev_rigid_* steps).
+ *   b2dev_spheres_setup: per sphere its body, referential centre[3], radius
+ *     and surface id (0 .. nsurf-1); material[2 * (s1 * nsurf + s2) + {0, 1}]
+ *     = friction, restitution of a surface pair (SPSET_Find resolved by the
+ *     caller; the table must be symmetric; host memory).
+ *   b2dev_detect_spheres: the contacts of the last detection are updated with
+ *     their master and slave kept (update_contact, dom.c:430-484) and dropped
+ *     where the spheres separated; every other pair of spheres of different
+ *     bodies, not both obstacles, whose gap (gjk.c:560-584) is below
+ *     GEOMETRIC_EPSILON becomes a new contact (detect_sphere_sphere,
+ *     goc.c:421-456; insert_contact, dom.c:315-330); new contacts with a
+ *     duplicate point are removed (sparsify_contacts, dom.c:2956-3054). The
+ *     result replaces the scene's contacts, listed by sphere pair (i < j)
+ *     ascending; *ncon and *nnew (either may be NULL) receive the number of
+ *     contacts and of new ones. Updated contacts carry their R and U from the
+ *     last solve, new ones start from zero.
+ *   b2dev_detect_carry_state: after b2dev_assemble of the detected contacts,
+ *     sets the solver state to the carried R and U (b2dev_set_state).
+ *   b2dev_get_contacts: the detected contacts (any pointer may be NULL):
+ *     bodies, spatial point[3], referential points[3], base[9], gap, friction,
+ *     restitution, sphere-pair key (i << 32 | j), slave_lo (1 when sphere i is
+ *     the slave), new flag, carried R[3] and U[3].
+ *   b2dev_sphere_centres: the current sphere centres[3] of the last detection. */
+int b2dev_spheres_setup(b2dev_ctx* ctx, int nsph, const int* body, const double* centre, const double* radius,
+                        const int* surface, int nsurf, const double* material, int on_device);
+int b2dev_detect_spheres(b2dev_ctx* ctx, int* ncon, int* nnew);
+int b2dev_detect_carry_state(b2dev_ctx* ctx);
+int b2dev_get_contacts(b2dev_ctx* ctx, int* master, int* slave, double* point, double* mpnt, double* spnt,
+                       double* base, double* gap, double* friction, double* restitution, long long* key,
+                       int* slave_lo, int* isnew, double* R0, double* U0, int on_device);
+int b2dev_sphere_centres(b2dev_ctx* ctx, double* cur, int on_device);
+
 /* Load an already assembled local dynamics (rows in caller order, blocks of
  * row i at adjptr[i]..adjptr[i+1]-1, Woff 9 doubles per block), colour it and
  * lay it out; the same data the reference solver reads from LOCDYN. */

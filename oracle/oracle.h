@@ -92,4 +92,32 @@ int orc_colour_ordered (int n, const int *adjptr, const int *adjcol, const int *
  * when more than maxcolours are needed. */
 int orc_colour (int n, const int *adjptr, const int *adjcol, uint64_t seed, int maxcolours, int *colour);
 
+/* ---------------- sphere contact update and detection (oracle_detect.c) ---------------- */
+
+/* gjk_sphere_sphere (gjk.c:560-584): gap of two spheres and their closest points. */
+double orc_gjk_sphere_sphere (const double *a, double ra, const double *b, double rb, double *p, double *q);
+
+/* localbase (dom.c:133-151): column-major frame with the normal as third column. */
+void orc_localbase (const double *n, double *loc);
+
+/* Current sphere centres: BODY_Cur_Point of the referential centres (bod.c:1702-1716). */
+void orc_sphere_centres (int nsph, const int *sbody, const double *sref, const double *rot, const double *x,
+                         const double *x0, double *cur);
+
+/* The contact part of DOM_Update_Begin for spheres (see oracle_detect.c): the
+ * previous contacts (key = i << 32 | j of the sphere pair, i < j; slave_lo = 1
+ * when sphere i is the slave; their R and U, may be NULL) are updated with
+ * their roles kept, new pairs are detected, new contacts with duplicate points
+ * are sparsified. mat[2 * (s1 * nsurf + s2) + {0, 1}] = friction, restitution.
+ * Returns the number of contacts (those beyond cap are counted, not written),
+ * or -1 for two coincident sphere centres. */
+int orc_detect_spheres (int nsph, const int *sbody, const double *sref, const double *rad, const int *surf,
+                        int nbod, const double *rot, const double *x, const double *x0, const int *obst,
+                        int nsurf, const double *mat,
+                        int nprev, const long long *prevkey, const int *prevslave_lo, const double *prevR,
+                        const double *prevU, int cap,
+                        long long *key, int *slave_lo, int *master, int *slave, double *point, double *mpnt,
+                        double *spnt, double *base, double *gap, double *friction, double *restitution,
+                        double *R0, double *U0, int *isnew);
+
 #endif

@@ -185,3 +185,104 @@ def merit(ld: LocalDynamics, R):
                       ld.restitution, ld.cohesion, np.ascontiguousarray(R, float).reshape(-1), U, cm,
                       ld.free_energy, ld.dynamic, ld.step)
     return m, U, cm[:ld.n]
+
+
+# ---------------------------------------------------------------- sphere contact detection
+
+_lp = np.ctypeslib.ndpointer(dtype=np.int64, flags='C_CONTIGUOUS')
+
+
+def _detect_sigs(lib):
+    if getattr(lib, '_detect_ready', False):
+        return
+    lib.orc_gjk_sphere_sphere.restype = C.c_double
+    lib.orc_gjk_sphere_sphere.argtypes = [_dp, C.c_double, _dp, C.c_double, _dp, _dp]
+    lib.orc_localbase.restype = None
+    lib.orc_localbase.argtypes = [_dp, _dp]
+    lib.orc_sphere_centres.restype = None
+    lib.orc_sphere_centres.argtypes = [C.c_int, _ip, _dp, _dp, _dp, _dp, _dp]
+    lib.orc_detect_spheres.restype = C.c_int
+    lib.orc_detect_spheres.argtypes = ([C.c_int, _ip, _dp, _dp, _ip, C.c_int, _dp, _dp, _dp, _ip, C.c_int, _dp,
+                                        C.c_int, _lp, _ip, _dp, _dp, C.c_int,
+                                        _lp, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip])
+    lib._detect_ready = True
+
+
+def gjk_sphere_sphere(a, ra, b, rb, which='oracle'):
+    """(gap, p, q) of gjk_sphere_sphere: the restatement, or the reference's
+    gjk.c compiled into _ref (which='ref')."""
+    lib = _load(which)
+    f = lib.orc_gjk_sphere_sphere if which == 'oracle' else lib.gjk_sphere_sphere
+    f.restype = C.c_double
+    f.argtypes = [_dp, C.c_double, _dp, C.c_double, _dp, _dp]
+    p, q = np.zeros(3), np.zeros(3)
+    g = f(np.ascontiguousarray(a, dtype=np.float64), float(ra), np.ascontiguousarray(b, dtype=np.float64),
+          float(rb), p, q)
+    return g, p, q
+
+
+def localbase(n):
+    lib = _load('oracle')
+    _detect_sigs(lib)
+    loc = np.zeros(9)
+    lib.orc_localbase(np.ascontiguousarray(n, dtype=np.float64), loc)
+    return loc
+
+
+def sphere_centres(sbody, sref, rot, x, x0):
+    lib = _load('oracle')
+    _detect_sigs(lib)
+    sbody = np.ascontiguousarray(sbody, dtype=np.int32)
+    cur = np.zeros((sbody.shape[0], 3))
+    lib.orc_sphere_centres(sbody.shape[0], sbody, np.ascontiguousarray(sref, dtype=np.float64).reshape(-1),
+                           np.ascontiguousarray(rot, dtype=np.float64).reshape(-1),
+                           np.ascontiguousarray(x, dtype=np.float64).reshape(-1),
+                           np.ascontiguousarray(x0, dtype=np.float64).reshape(-1), cur)
+    return cur
+
+
+def detect_spheres(sbody, sref, radius, surface, rot, x, x0, obstacle, material, prev=None):
+    """The contact part of DOM_Update_Begin for spheres (oracle_detect.c).
+    material: (nsurf, nsurf, 2) friction, restitution. prev: None or a dict
+    returned by an earlier call, with 'R' and 'U' set to the reactions and
+    velocities to carry over. Returns a dict of contact arrays in pair order."""
+    lib = _load('oracle')
+    _detect_sigs(lib)
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32).reshape(-1)
+    sbody, surface, obstacle = i32(sbody), i32(surface), i32(obstacle)
+    sref, radius, rot, x, x0 = f64(sref), f64(radius), f64(rot), f64(x), f64(x0)
+    mat = np.asarray(material, dtype=np.float64)
+    nsurf = mat.shape[0]
+    mat = f64(mat)
+    nsph, nbod = sbody.shape[0], obstacle.shape[0]
+    if prev is None:
+        pk, ps, pR, pU, npv = np.zeros(1, np.int64), np.zeros(1, np.int32), np.zeros(3), np.zeros(3), 0
+    else:
+        npv = prev['key'].shape[0]
+        pk = np.ascontiguousarray(prev['key'], dtype=np.int64)
+        ps = i32(prev['slave_lo'])
+        pR = f64(prev.get('R', np.zeros((npv, 3))))
+        pU = f64(prev.get('U', np.zeros((npv, 3))))
+        if npv == 0:
+            pk, ps, pR, pU = np.zeros(1, np.int64), np.zeros(1, np.int32), np.zeros(3), np.zeros(3)
+
+    def run(cap):
+        c1 = max(cap, 1)
+        out = dict(key=np.zeros(c1, np.int64), slave_lo=np.zeros(c1, np.int32), master=np.zeros(c1, np.int32),
+                   slave=np.zeros(c1, np.int32), point=np.zeros((c1, 3)), mpnt=np.zeros((c1, 3)),
+                   spnt=np.zeros((c1, 3)), base=np.zeros((c1, 9)), gap=np.zeros(c1), friction=np.zeros(c1),
+                   restitution=np.zeros(c1), R=np.zeros((c1, 3)), U=np.zeros((c1, 3)), isnew=np.zeros(c1, np.int32))
+        n = lib.orc_detect_spheres(nsph, sbody, sref, radius, surface, nbod, rot, x, x0, obstacle, nsurf, mat,
+                                   npv, pk, ps, pR, pU, cap,
+                                   out['key'], out['slave_lo'], out['master'], out['slave'], out['point'],
+                                   out['mpnt'], out['spnt'], out['base'], out['gap'], out['friction'],
+                                   out['restitution'], out['R'], out['U'], out['isnew'])
+        return n, out
+
+    n, out = run(8 * nsph + 16)
+    if n < 0:
+        raise ValueError('coincident sphere centres')
+    if n > 8 * nsph + 16:
+        n, out = run(n)
+    return {k: v[:n] for k, v in out.items()}

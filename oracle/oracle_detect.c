@@ -1,0 +1,315 @@
+/*
+ * oracle_detect.c -- TEST INFRASTRUCTURE. Not part of the product.
+ *
+ * CPU restatement of the reference's contact update and detection for pairs of
+ * spheres held by rigid bodies, the checker of the device detection
+ * (solfec-1.0_b200/csrc/b2_detect.cuh). One call is the contact part of
+ * DOM_Update_Begin (dom.c:3700-3790) for a scene of spheres:
+ *
+ *  - sphere centres moved with their bodies: SPHERE_Update (sph.c:322-344)
+ *    with BODY_Cur_Point (bod.c:1702-1716);
+ *  - contacts of the previous step updated with their master and slave kept
+ *    (update_contact, dom.c:430-484, update_sphere_sphere, goc.c:658-677) and
+ *    removed when the spheres separated;
+ *  - new contacts for every other pair of spheres of different bodies, not
+ *    both obstacles (box.c:104-108), whose gap gjk_sphere_sphere (gjk.c:560-584)
+ *    finds below GEOMETRIC_EPSILON (detect_sphere_sphere, goc.c:421-456), with
+ *    the master chosen by the point order of the centres (goc.c:409-419,
+ *    dom.c:386-404);
+ *  - insert_contact (dom.c:315-330): spatial point, referential points
+ *    (BODY_Ref_Point, bod.c:1736-1750), local base (localbase, dom.c:133-151),
+ *    gap, surface material (SPSET_Find, sps.c:152-184, resolved by the caller
+ *    into a symmetric table of friction and restitution);
+ *  - sparsify_contacts (dom.c:2956-3054): a new contact whose spatial point
+ *    lies within 2 mindist (max-norm) of another contact of one of its bodies is
+ *    removed when that contact is old or comes later in the list. Sphere
+ *    contacts all have area 1, so the area branches never apply.
+ *
+ * The reference finds candidate pairs with an AABB sweep (hyb.c) over extents
+ * inflated by GEOMETRIC_EPSILON (sph.c:240-252); every pair whose gap is below
+ * GEOMETRIC_EPSILON overlaps there, so the candidates only prune and this
+ * restatement uses a sweep along x with a wider margin.
+ *
+ * Order: contacts are listed by sphere pair (i, j), i < j, ascending. The
+ * reference lists them in insertion order (broad-phase callback order), which
+ * depends on its AABB algorithm; the same order also stands in for the
+ * reference's contact ids in the sparsification tie-break.
+ *
+ * gjk_sphere_sphere here is checked bit for bit against the reference's own
+ * gjk.c, compiled into oracle/_ref.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "oracle.h"
+
+#define GEPS 1E-6 /* GEOMETRIC_EPSILON, alg.c:24 */
+
+/* gjk.c:560-584 */
+double orc_gjk_sphere_sphere (const double *a, double ra, const double *b, double rb, double *p, double *q)
+{
+  double d[3], dlen, deno;
+  d[0] = a[0] - b[0]; d[1] = a[1] - b[1]; d[2] = a[2] - b[2];
+  dlen = sqrt (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  if (dlen == 0.0)
+  {
+    memcpy (p, a, sizeof (double) * 3);
+    memcpy (q, b, sizeof (double) * 3);
+    return 0.0;
+  }
+  deno = ra / dlen;
+  for (int k = 0; k < 3; k++) p[k] = a[k] - deno * d[k];
+  deno = rb / dlen;
+  for (int k = 0; k < 3; k++) q[k] = b[k] + deno * d[k];
+  deno = ra + rb;
+  if (dlen > deno) return dlen - deno;
+  for (int k = 0; k < 3; k++) p[k] = .5 * (p[k] + q[k]);
+  memcpy (q, p, sizeof (double) * 3);
+  return 0.0;
+}
+
+/* localbase, dom.c:133-151: the normal as the third column, the first column
+ * e_x x n normalised (e_y x n when that is shorter than GEOMETRIC_EPSILON) and
+ * the second their cross product */
+void orc_localbase (const double *n, double *loc)
+{
+  const double e[2][3] = {{1., 0., 0.}, {0., 1., 0.}};
+  double len;
+  loc[6] = n[0]; loc[7] = n[1]; loc[8] = n[2];
+  loc[0] = e[0][1] * n[2] - e[0][2] * n[1];
+  loc[1] = e[0][2] * n[0] - e[0][0] * n[2];
+  loc[2] = e[0][0] * n[1] - e[0][1] * n[0];
+  len = sqrt (loc[0] * loc[0] + loc[1] * loc[1] + loc[2] * loc[2]);
+  if (len < GEPS)
+  {
+    loc[0] = e[1][1] * n[2] - e[1][2] * n[1];
+    loc[1] = e[1][2] * n[0] - e[1][0] * n[2];
+    loc[2] = e[1][0] * n[1] - e[1][1] * n[0];
+    len = sqrt (loc[0] * loc[0] + loc[1] * loc[1] + loc[2] * loc[2]);
+  }
+  loc[0] /= len; loc[1] /= len; loc[2] /= len;
+  loc[3] = loc[1] * n[2] - loc[2] * n[1];
+  loc[4] = loc[2] * n[0] - loc[0] * n[2];
+  loc[5] = loc[0] * n[1] - loc[1] * n[0];
+}
+
+/* BODY_Cur_Point (bod.c:1702-1716): x = c + R (X - X0), R column-major */
+static void cur_point (const double *R, const double *c, const double *X0, const double *X, double *x)
+{
+  double A[3] = {X[0] - X0[0], X[1] - X0[1], X[2] - X0[2]};
+  x[0] = c[0] + (R[0] * A[0] + R[3] * A[1] + R[6] * A[2]);
+  x[1] = c[1] + (R[1] * A[0] + R[4] * A[1] + R[7] * A[2]);
+  x[2] = c[2] + (R[2] * A[0] + R[5] * A[1] + R[8] * A[2]);
+}
+
+/* BODY_Ref_Point (bod.c:1736-1750): X = X0 + R^T (x - c) */
+static void ref_point (const double *R, const double *c, const double *X0, const double *x, double *X)
+{
+  double a[3] = {x[0] - c[0], x[1] - c[1], x[2] - c[2]};
+  X[0] = X0[0] + (R[0] * a[0] + R[1] * a[1] + R[2] * a[2]);
+  X[1] = X0[1] + (R[3] * a[0] + R[4] * a[1] + R[5] * a[2]);
+  X[2] = X0[2] + (R[6] * a[0] + R[7] * a[1] + R[8] * a[2]);
+}
+
+/* pntcmp, goc.c:409-419 */
+static int pntcmp (const double *a, const double *b)
+{
+  for (int i = 0; i < 3; i++)
+  {
+    if (a[i] < b[i]) return -1;
+    else if (a[i] > b[i]) return 1;
+  }
+  return 0;
+}
+
+void orc_sphere_centres (int nsph, const int *sbody, const double *sref, const double *rot, const double *x,
+                         const double *x0, double *cur)
+{
+  for (int s = 0; s < nsph; s++)
+  {
+    const int b = sbody[s];
+    cur_point (rot + 9 * (size_t) b, x + 3 * (size_t) b, x0 + 3 * (size_t) b, sref + 3 * (size_t) s, cur + 3 * (size_t) s);
+  }
+}
+
+typedef struct { long long key; int slave_lo; double R[3], U[3]; } prevrec;
+
+static int prevcmp (const void *a, const void *b)
+{
+  long long x = ((const prevrec *) a)->key, y = ((const prevrec *) b)->key;
+  return x < y ? -1 : x > y;
+}
+
+typedef struct { double lo; int s; } sweeprec;
+
+static int sweepcmp (const void *a, const void *b)
+{
+  const sweeprec *x = a, *y = b;
+  if (x->lo < y->lo) return -1;
+  if (x->lo > y->lo) return 1;
+  return x->s - y->s;
+}
+
+typedef struct { int i, j; } pairrec;
+
+static int paircmp (const void *a, const void *b)
+{
+  const pairrec *x = a, *y = b;
+  if (x->i != y->i) return x->i - y->i;
+  return x->j - y->j;
+}
+
+int orc_detect_spheres (int nsph, const int *sbody, const double *sref, const double *rad, const int *surf,
+                        int nbod, const double *rot, const double *x, const double *x0, const int *obst,
+                        int nsurf, const double *mat,
+                        int nprev, const long long *prevkey, const int *prevslave_lo, const double *prevR,
+                        const double *prevU, int cap,
+                        long long *key, int *slave_lo, int *master, int *slave, double *point, double *mpnt,
+                        double *spnt, double *base, double *gap, double *friction, double *restitution,
+                        double *R0, double *U0, int *isnew)
+{
+  double *cur = malloc (sizeof (double) * 3 * (size_t) (nsph + 1));
+  sweeprec *sw = malloc (sizeof (sweeprec) * (size_t) (nsph + 1));
+  prevrec *pv = malloc (sizeof (prevrec) * (size_t) (nprev + 1));
+  size_t pcap = 1024, np = 0;
+  pairrec *pairs = malloc (sizeof (pairrec) * pcap);
+  int ret = 0;
+  (void) nbod;
+  orc_sphere_centres (nsph, sbody, sref, rot, x, x0, cur);
+  for (int k = 0; k < nprev; k++)
+  {
+    pv[k].key = prevkey[k]; pv[k].slave_lo = prevslave_lo[k];
+    for (int q = 0; q < 3; q++) { pv[k].R[q] = prevR ? prevR[3 * k + q] : 0.0; pv[k].U[q] = prevU ? prevU[3 * k + q] : 0.0; }
+  }
+  qsort (pv, nprev, sizeof (prevrec), prevcmp);
+
+  /* candidate pairs: sweep along x with a margin above GEOMETRIC_EPSILON */
+  for (int s = 0; s < nsph; s++) { sw[s].lo = cur[3 * s] - rad[s]; sw[s].s = s; }
+  qsort (sw, nsph, sizeof (sweeprec), sweepcmp);
+  for (int a = 0; a < nsph; a++)
+  {
+    const int i = sw[a].s;
+    const double hi = cur[3 * i] + rad[i] + 4 * GEPS;
+    for (int b = a + 1; b < nsph && sw[b].lo <= hi; b++)
+    {
+      int s1 = i, s2 = sw[b].s;
+      double p[3], q[3];
+      if (s1 > s2) { int t = s1; s1 = s2; s2 = t; }
+      if (sbody[s1] == sbody[s2]) continue;
+      if (obst[sbody[s1]] && obst[sbody[s2]]) continue;
+      if (orc_gjk_sphere_sphere (cur + 3 * s1, rad[s1], cur + 3 * s2, rad[s2], p, q) < GEPS)
+      {
+        if (np == pcap) { pcap *= 2; pairs = realloc (pairs, sizeof (pairrec) * pcap); }
+        pairs[np].i = s1; pairs[np].j = s2; np++;
+      }
+    }
+  }
+  qsort (pairs, np, sizeof (pairrec), paircmp);
+
+  /* contacts in pair order */
+  {
+    const size_t n = np;
+    int *keep = malloc (sizeof (int) * (n + 1));
+    int *bcnt = calloc ((size_t) nbod + 1, sizeof (int)), *bptr = malloc (sizeof (int) * ((size_t) nbod + 2));
+    int *blist = malloc (sizeof (int) * (2 * n + 1));
+    long long *k_ = malloc (sizeof (long long) * (n + 1));
+    int *sl_ = malloc (sizeof (int) * (n + 1)), *ms_ = malloc (sizeof (int) * (n + 1)), *sv_ = malloc (sizeof (int) * (n + 1));
+    int *nw_ = malloc (sizeof (int) * (n + 1));
+    double *pt_ = malloc (sizeof (double) * 3 * (n + 1)), *mp_ = malloc (sizeof (double) * 3 * (n + 1));
+    double *sp_ = malloc (sizeof (double) * 3 * (n + 1)), *bs_ = malloc (sizeof (double) * 9 * (n + 1));
+    double *gp_ = malloc (sizeof (double) * (n + 1)), *fr_ = malloc (sizeof (double) * (n + 1));
+    double *rs_ = malloc (sizeof (double) * (n + 1));
+    double *r0_ = malloc (sizeof (double) * 3 * (n + 1)), *u0_ = malloc (sizeof (double) * 3 * (n + 1));
+    size_t out = 0;
+    for (size_t c = 0; c < n && ret == 0; c++)
+    {
+      const int i = pairs[c].i, j = pairs[c].j;
+      prevrec probe, *hit;
+      int lo_is_slave, s, m;
+      double p[3], q[3], nrm[3], len;
+      probe.key = ((long long) i << 32) | (long long) j;
+      hit = nprev ? bsearch (&probe, pv, nprev, sizeof (prevrec), prevcmp) : NULL;
+      if (hit) lo_is_slave = hit->slave_lo;                        /* update: roles kept */
+      else lo_is_slave = pntcmp (cur + 3 * i, cur + 3 * j) <= 0;   /* detection: lower centre is the slave */
+      s = lo_is_slave ? i : j;
+      m = lo_is_slave ? j : i;
+      orc_gjk_sphere_sphere (cur + 3 * s, rad[s], cur + 3 * m, rad[m], p, q);
+      nrm[0] = p[0] - cur[3 * s]; nrm[1] = p[1] - cur[3 * s + 1]; nrm[2] = p[2] - cur[3 * s + 2];
+      len = sqrt (nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+      if (!(len > 0.0)) { ret = -1; break; } /* coincident centres: no normal */
+      nrm[0] /= len; nrm[1] /= len; nrm[2] /= len;
+      k_[c] = probe.key;
+      sl_[c] = lo_is_slave;
+      ms_[c] = sbody[m];
+      sv_[c] = sbody[s];
+      nw_[c] = hit == NULL;
+      {
+        /* sphere_sphere_gap, goc.c:52-61 */
+        double xx[3] = {cur[3 * m] - cur[3 * s], cur[3 * m + 1] - cur[3 * s + 1], cur[3 * m + 2] - cur[3 * s + 2]};
+        double d = xx[0] * nrm[0] + xx[1] * nrm[1] + xx[2] * nrm[2], e = rad[s] + rad[m];
+        gp_[c] = e > d ? d - e : 0;
+      }
+      memcpy (pt_ + 3 * c, q, sizeof (double) * 3);
+      ref_point (rot + 9 * (size_t) sbody[m], x + 3 * (size_t) sbody[m], x0 + 3 * (size_t) sbody[m], q, mp_ + 3 * c);
+      ref_point (rot + 9 * (size_t) sbody[s], x + 3 * (size_t) sbody[s], x0 + 3 * (size_t) sbody[s], p, sp_ + 3 * c);
+      orc_localbase (nrm, bs_ + 9 * c);
+      {
+        const size_t t = (size_t) surf[s] * (size_t) nsurf + (size_t) surf[m];
+        fr_[c] = mat[2 * t];
+        rs_[c] = mat[2 * t + 1];
+      }
+      for (int v = 0; v < 3; v++)
+      {
+        r0_[3 * c + v] = hit ? hit->R[v] : 0.0;
+        u0_[3 * c + v] = hit ? hit->U[v] : 0.0;
+      }
+    }
+    if (ret == 0)
+    {
+      /* sparsify_contacts: per body, its contacts */
+      for (size_t c = 0; c < n; c++) { bcnt[ms_[c]]++; bcnt[sv_[c]]++; }
+      bptr[0] = 0;
+      for (int b = 0; b < nbod; b++) bptr[b + 1] = bptr[b] + bcnt[b];
+      for (int b = 0; b < nbod; b++) bcnt[b] = bptr[b];
+      for (size_t c = 0; c < n; c++) { blist[bcnt[ms_[c]]++] = (int) c; blist[bcnt[sv_[c]]++] = (int) c; }
+      for (size_t c = 0; c < n; c++)
+      {
+        keep[c] = 1;
+        if (!nw_[c]) continue;
+        const int bb[2] = {ms_[c], sv_[c]};
+        for (int t = 0; t < 2 && keep[c]; t++)
+          for (int u = bptr[bb[t]]; u < bptr[bb[t] + 1]; u++)
+          {
+            const int a = blist[u];
+            double dd, mx = 0.0;
+            if (a == (int) c) continue;
+            for (int v = 0; v < 3; v++) { dd = fabs (pt_[3 * c + v] - pt_[3 * (size_t) a + v]); if (dd > mx) mx = dd; }
+            if (mx < 2.0 * GEPS && ((int) c < a || !nw_[a])) { keep[c] = 0; break; }
+          }
+      }
+      for (size_t c = 0; c < n; c++)
+      {
+        if (!keep[c]) continue;
+        if ((int) out < cap)
+        {
+          key[out] = k_[c]; slave_lo[out] = sl_[c]; master[out] = ms_[c]; slave[out] = sv_[c];
+          memcpy (point + 3 * out, pt_ + 3 * c, sizeof (double) * 3);
+          memcpy (mpnt + 3 * out, mp_ + 3 * c, sizeof (double) * 3);
+          memcpy (spnt + 3 * out, sp_ + 3 * c, sizeof (double) * 3);
+          memcpy (base + 9 * out, bs_ + 9 * c, sizeof (double) * 9);
+          gap[out] = gp_[c]; friction[out] = fr_[c]; restitution[out] = rs_[c];
+          memcpy (R0 + 3 * out, r0_ + 3 * c, sizeof (double) * 3);
+          memcpy (U0 + 3 * out, u0_ + 3 * c, sizeof (double) * 3);
+          isnew[out] = nw_[c];
+        }
+        out++;
+      }
+      ret = (int) out;
+    }
+    free (keep); free (bcnt); free (bptr); free (blist); free (k_); free (sl_); free (ms_); free (sv_); free (nw_);
+    free (pt_); free (mp_); free (sp_); free (bs_); free (gp_); free (fr_); free (rs_); free (r0_); free (u0_);
+  }
+  free (cur); free (sw); free (pv); free (pairs);
+  return ret;
+}

@@ -1,0 +1,372 @@
+// b2_detect.cuh -- contact update and detection between spheres of rigid bodies
+// (the contact part of DOM_Update_Begin, dom.c:3700-3790, for sphere pairs).
+//
+//   k_sph_centres   SPHERE_Update with BODY_Cur_Point (sph.c:322-344,
+//                   bod.c:1702-1716); largest radius for the cell size
+//   k_sph_cells     uniform grid cell of each centre (edge 2 r_max + 2 eps) and
+//                   its hash bucket
+//   k_sph_buckets   first and last sorted sphere of each bucket
+//   k_sph_pairs     per sphere i, the spheres j > i of the 27 surrounding cells
+//                   whose gjk_sphere_sphere gap (gjk.c:560-584) is below
+//                   GEOMETRIC_EPSILON (goc.c:431), bodies different and not
+//                   both obstacles (box.c:104-108): counted, then written
+//   k_sph_sort_seg  the pairs of each sphere in ascending j (list order)
+//   k_sph_contacts  one contact per pair: roles kept from the previous step
+//                   (update_contact, dom.c:430-484; update_sphere_sphere,
+//                   goc.c:658-677) or set by the centres' point order
+//                   (detect_sphere_sphere, goc.c:421-456); spatial point,
+//                   normal, gap (goc.c:52-61), referential points
+//                   (BODY_Ref_Point, bod.c:1736-1750), local base (localbase,
+//                   dom.c:133-151), surface material, carried R and U
+//   k_sph_body_*    per body, its contacts (sparsification neighbourhoods)
+//   k_sph_sparsify  sparsify_contacts (dom.c:2956-3054) for sphere contacts
+//                   (area 1): a new contact within 2 mindist (max-norm) of an
+//                   old contact, or of a later new one, of one of its bodies
+//   k_sph_compact   the kept contacts into the scene arrays
+//
+// Every pair with gap below GEOMETRIC_EPSILON has its centres within
+// r_i + r_j + eps < cell edge along each axis, so the 27 cells around a sphere
+// hold all its candidates; the reference's inflated AABBs (sph.c:240-252) also
+// overlap for every such pair, so the grid replaces its broad phase exactly.
+// Arithmetic follows the reference's macros (alg.h) operation by operation;
+// the library is built without fused multiply-adds, so results match the
+// oracle bit for bit.
+#pragma once
+
+#include <cstdint>
+
+namespace b2 {
+
+constexpr double kGeomEps = 1e-6;  // GEOMETRIC_EPSILON, alg.c:24
+
+struct SphereDev {
+  int nsph, nbod;
+  const int* body;      // body of each sphere
+  const double* ref;    // referential centre [3]
+  const double* rad;    // radius
+  const int* surf;      // surface id
+  double* cur;          // current centre [3]
+  int4* cell;           // grid cell (x, y, z, unused)
+  unsigned int* hkey;   // hash bucket of the cell
+};
+
+__device__ __forceinline__ void cur_point(const double* R, const double* c, const double* X0, const double* X,
+                                          double* x) {
+  const double A0 = X[0] - X0[0], A1 = X[1] - X0[1], A2 = X[2] - X0[2];
+  x[0] = c[0] + (R[0] * A0 + R[3] * A1 + R[6] * A2);
+  x[1] = c[1] + (R[1] * A0 + R[4] * A1 + R[7] * A2);
+  x[2] = c[2] + (R[2] * A0 + R[5] * A1 + R[8] * A2);
+}
+
+__device__ __forceinline__ void ref_point(const double* R, const double* c, const double* X0, const double* x,
+                                          double* X) {
+  const double a0 = x[0] - c[0], a1 = x[1] - c[1], a2 = x[2] - c[2];
+  X[0] = X0[0] + (R[0] * a0 + R[1] * a1 + R[2] * a2);
+  X[1] = X0[1] + (R[3] * a0 + R[4] * a1 + R[5] * a2);
+  X[2] = X0[2] + (R[6] * a0 + R[7] * a1 + R[8] * a2);
+}
+
+// gjk_sphere_sphere, gjk.c:560-584: gap and the closest points p (on a), q (on b)
+__device__ __forceinline__ double gjk_spheres(const double* a, double ra, const double* b, double rb, double* p,
+                                              double* q) {
+  const double d0 = a[0] - b[0], d1 = a[1] - b[1], d2 = a[2] - b[2];
+  const double dlen = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  if (dlen == 0.0) {
+    p[0] = a[0]; p[1] = a[1]; p[2] = a[2];
+    q[0] = b[0]; q[1] = b[1]; q[2] = b[2];
+    return 0.0;
+  }
+  double deno = ra / dlen;
+  p[0] = a[0] - deno * d0; p[1] = a[1] - deno * d1; p[2] = a[2] - deno * d2;
+  deno = rb / dlen;
+  q[0] = b[0] + deno * d0; q[1] = b[1] + deno * d1; q[2] = b[2] + deno * d2;
+  deno = ra + rb;
+  if (dlen > deno) return dlen - deno;
+  p[0] = .5 * (p[0] + q[0]); p[1] = .5 * (p[1] + q[1]); p[2] = .5 * (p[2] + q[2]);
+  q[0] = p[0]; q[1] = p[1]; q[2] = p[2];
+  return 0.0;
+}
+
+// the gap alone (the same operations as gjk_spheres up to its return value)
+__device__ __forceinline__ double gjk_spheres_gap(const double* a, double ra, const double* b, double rb) {
+  const double d0 = a[0] - b[0], d1 = a[1] - b[1], d2 = a[2] - b[2];
+  const double dlen = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  const double deno = ra + rb;
+  return dlen > deno ? dlen - deno : 0.0;
+}
+
+// localbase, dom.c:133-151
+__device__ __forceinline__ void local_base(const double* n, double* loc) {
+  const double e0[3] = {1., 0., 0.}, e1[3] = {0., 1., 0.};
+  loc[6] = n[0]; loc[7] = n[1]; loc[8] = n[2];
+  loc[0] = e0[1] * n[2] - e0[2] * n[1];
+  loc[1] = e0[2] * n[0] - e0[0] * n[2];
+  loc[2] = e0[0] * n[1] - e0[1] * n[0];
+  double len = sqrt(loc[0] * loc[0] + loc[1] * loc[1] + loc[2] * loc[2]);
+  if (len < kGeomEps) {
+    loc[0] = e1[1] * n[2] - e1[2] * n[1];
+    loc[1] = e1[2] * n[0] - e1[0] * n[2];
+    loc[2] = e1[0] * n[1] - e1[1] * n[0];
+    len = sqrt(loc[0] * loc[0] + loc[1] * loc[1] + loc[2] * loc[2]);
+  }
+  loc[0] /= len; loc[1] /= len; loc[2] /= len;
+  loc[3] = loc[1] * n[2] - loc[2] * n[1];
+  loc[4] = loc[2] * n[0] - loc[0] * n[2];
+  loc[5] = loc[0] * n[1] - loc[1] * n[0];
+}
+
+// pntcmp, goc.c:409-419
+__device__ __forceinline__ int point_cmp(const double* a, const double* b) {
+  for (int i = 0; i < 3; i++) {
+    if (a[i] < b[i]) return -1;
+    if (a[i] > b[i]) return 1;
+  }
+  return 0;
+}
+
+__device__ __forceinline__ unsigned int cell_hash(int x, int y, int z, unsigned int mask) {
+  return (((unsigned int)x * 73856093u) ^ ((unsigned int)y * 19349663u) ^ ((unsigned int)z * 83492791u)) & mask;
+}
+
+// bad flags (bit or): 1 a radius not positive and finite or a centre not finite,
+// 2 a centre too far from the origin for the grid, 4 two coincident centres,
+// 8 a surface id out of range, 16 a body index out of range
+__global__ void k_sph_centres(SphereDev s, const double* rot, const double* xb, const double* x0,
+                              unsigned long long* rmax_bits, int* bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.nsph) return;
+  const int b = s.body[i];
+  if (b < 0 || b >= s.nbod) { atomicOr(bad, 16); return; }
+  double c[3];
+  cur_point(rot + 9 * (size_t)b, xb + 3 * (size_t)b, x0 + 3 * (size_t)b, s.ref + 3 * (size_t)i, c);
+  s.cur[3 * (size_t)i] = c[0]; s.cur[3 * (size_t)i + 1] = c[1]; s.cur[3 * (size_t)i + 2] = c[2];
+  const double r = s.rad[i];
+  if (!(r > 0.0) || !isfinite(r) || !isfinite(c[0]) || !isfinite(c[1]) || !isfinite(c[2])) { atomicOr(bad, 1); return; }
+  atomicMax(rmax_bits, (unsigned long long)__double_as_longlong(r));  // positive doubles order as integers
+}
+
+__global__ void k_sph_cells(SphereDev s, const unsigned long long* rmax_bits, unsigned int mask, int* sidx,
+                            int* bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.nsph) return;
+  const double h = 2.0 * __longlong_as_double((long long)*rmax_bits) + 2.0 * kGeomEps;
+  int q[3];
+  for (int k = 0; k < 3; k++) {
+    const double f = floor(s.cur[3 * (size_t)i + k] / h);
+    if (!(fabs(f) < 1.0e9)) { atomicOr(bad, 2); q[k] = 0; }
+    else q[k] = (int)f;
+  }
+  s.cell[i] = make_int4(q[0], q[1], q[2], 0);
+  s.hkey[i] = cell_hash(q[0], q[1], q[2], mask);
+  sidx[i] = i;
+}
+
+__global__ void k_sph_buckets(int n, const unsigned int* key, int* bstart, int* bend) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const unsigned int k = key[t];
+  if (t == 0 || key[t - 1] != k) bstart[k] = t;
+  if (t == n - 1 || key[t + 1] != k) bend[k] = t + 1;
+}
+
+// WRITE = false: count[i] = pairs (i, j > i); WRITE = true: their j at off[i]..
+template <bool WRITE>
+__global__ void k_sph_pairs(SphereDev s, const int* obst, const int* sorted, const int* bstart, const int* bend,
+                            unsigned int mask, int* count, const int* off, int* pj) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= s.nsph) return;
+  const int i = sorted[t];
+  const int4 ci = s.cell[i];
+  const int bi = s.body[i];
+  if (bi < 0 || bi >= s.nbod) return;  // reported by k_sph_centres
+  const bool oi = obst[bi] != 0;
+  const double a[3] = {s.cur[3 * (size_t)i], s.cur[3 * (size_t)i + 1], s.cur[3 * (size_t)i + 2]};
+  const double ra = s.rad[i];
+  int cnt = 0;
+  int w = WRITE ? off[i] : 0;
+  for (int dz = -1; dz <= 1; dz++)
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) {
+        const int nx = ci.x + dx, ny = ci.y + dy, nz = ci.z + dz;
+        const unsigned int hb = cell_hash(nx, ny, nz, mask);
+        const int u0 = bstart[hb], u1 = bend[hb];
+        for (int u = u0; u < u1; u++) {
+          const int j = sorted[u];
+          if (j <= i) continue;
+          const int4 cj = s.cell[j];
+          if (cj.x != nx || cj.y != ny || cj.z != nz) continue;  // another cell in the same bucket
+          const int bj = s.body[j];
+          if (bj < 0 || bj >= s.nbod || bj == bi || (oi && obst[bj])) continue;
+          const double b[3] = {s.cur[3 * (size_t)j], s.cur[3 * (size_t)j + 1], s.cur[3 * (size_t)j + 2]};
+          if (gjk_spheres_gap(a, ra, b, s.rad[j]) < kGeomEps) {
+            if (WRITE) pj[w++] = j;
+            cnt++;
+          }
+        }
+      }
+  if (!WRITE) count[i] = cnt;
+}
+
+__global__ void k_sph_sort_seg(int nsph, const int* off, int* pj, int* pi) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsph) return;
+  const int b = off[i], e = off[i + 1];
+  for (int k = b + 1; k < e; k++) {  // a sphere has a few tens of pairs at most
+    const int v = pj[k];
+    int m = k - 1;
+    while (m >= b && pj[m] > v) { pj[m + 1] = pj[m]; m--; }
+    pj[m + 1] = v;
+  }
+  for (int k = b; k < e; k++) pi[k] = i;
+}
+
+struct ContactOut {
+  int* master; int* slave; double* point; double* mpnt; double* spnt; double* base; double* gap;
+  double* fric; double* rest; double* coh; double* R0; double* U0; long long* key; int* slave_lo; int* isnew;
+};
+
+__global__ void k_sph_contacts(int npair, SphereDev s, const int* pi, const int* pj, const double* rot,
+                               const double* xb, const double* x0, int nsurf, const double* mat, int nprev,
+                               const long long* prevkey, const int* prevslave_lo, const double* prevR,
+                               const double* prevU, ContactOut o, int* bad) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npair) return;
+  const int i = pi[k], j = pj[k];
+  const long long key = ((long long)i << 32) | (long long)j;
+  int hit = -1;
+  {  // the previous step's contacts are in ascending key order
+    int lo = 0, hi = nprev - 1;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      const long long v = prevkey[mid];
+      if (v == key) { hit = mid; break; }
+      if (v < key) lo = mid + 1; else hi = mid - 1;
+    }
+  }
+  const double* ci = s.cur + 3 * (size_t)i;
+  const double* cj = s.cur + 3 * (size_t)j;
+  const int lo_slave = hit >= 0 ? prevslave_lo[hit] : (point_cmp(ci, cj) <= 0 ? 1 : 0);
+  const int sv = lo_slave ? i : j, ms = lo_slave ? j : i;
+  const double* cs = s.cur + 3 * (size_t)sv;
+  const double* cm = s.cur + 3 * (size_t)ms;
+  const double rs = s.rad[sv], rm = s.rad[ms];
+  const int bm = s.body[ms], bs = s.body[sv];
+  // every index array of the contact is written before anything is checked:
+  // the body lists of the sparsification read them
+  o.master[k] = bm;
+  o.slave[k] = bs;
+  o.key[k] = key;
+  o.slave_lo[k] = lo_slave;
+  o.isnew[k] = hit < 0;
+  double p[3], q[3], n[3];
+  gjk_spheres(cs, rs, cm, rm, p, q);
+  n[0] = p[0] - cs[0]; n[1] = p[1] - cs[1]; n[2] = p[2] - cs[2];
+  const double len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  if (!(len > 0.0)) atomicOr(bad, 4);  // coincident centres: the normal is not finite, the call fails
+  n[0] /= len; n[1] /= len; n[2] /= len;
+  double g;
+  {  // sphere_sphere_gap, goc.c:52-61
+    const double x0_ = cm[0] - cs[0], x1_ = cm[1] - cs[1], x2_ = cm[2] - cs[2];
+    const double d = x0_ * n[0] + x1_ * n[1] + x2_ * n[2];
+    const double e = rs + rm;
+    g = e > d ? d - e : 0;
+  }
+  for (int v = 0; v < 3; v++) o.point[3 * (size_t)k + v] = q[v];
+  double X[3];
+  ref_point(rot + 9 * (size_t)bm, xb + 3 * (size_t)bm, x0 + 3 * (size_t)bm, q, X);
+  for (int v = 0; v < 3; v++) o.mpnt[3 * (size_t)k + v] = X[v];
+  ref_point(rot + 9 * (size_t)bs, xb + 3 * (size_t)bs, x0 + 3 * (size_t)bs, p, X);
+  for (int v = 0; v < 3; v++) o.spnt[3 * (size_t)k + v] = X[v];
+  double loc[9];
+  local_base(n, loc);
+  for (int v = 0; v < 9; v++) o.base[9 * (size_t)k + v] = loc[v];
+  o.gap[k] = g;
+  const int s1 = s.surf[sv], s2 = s.surf[ms];
+  if (s1 < 0 || s1 >= nsurf || s2 < 0 || s2 >= nsurf) {
+    atomicOr(bad, 8);
+    o.fric[k] = o.rest[k] = 0.0;
+  } else {
+    const size_t t = (size_t)s1 * nsurf + s2;
+    o.fric[k] = mat[2 * t];
+    o.rest[k] = mat[2 * t + 1];
+  }
+  o.coh[k] = 0.0;
+  for (int v = 0; v < 3; v++) {
+    o.R0[3 * (size_t)k + v] = hit >= 0 ? prevR[3 * (size_t)hit + v] : 0.0;
+    o.U0[3 * (size_t)k + v] = hit >= 0 ? prevU[3 * (size_t)hit + v] : 0.0;
+  }
+}
+
+// body indices come from k_sph_contacts, which takes them from the checked
+// sphere bodies; the range tests below keep a corrupted entry from addressing
+// outside the per-body arrays
+__global__ void k_sph_body_count(int n, int nb, const int* master, const int* slave, int* bcnt, int* bad) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int m = master[k], s = slave[k];
+  if (m < 0 || m >= nb || s < 0 || s >= nb) { atomicOr(bad, 16); return; }
+  atomicAdd(bcnt + m, 1);
+  atomicAdd(bcnt + s, 1);
+}
+
+__global__ void k_sph_body_fill(int n, int nb, const int* master, const int* slave, int* cursor, int* blist) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int m = master[k], s = slave[k];
+  if (m < 0 || m >= nb || s < 0 || s >= nb) return;
+  blist[atomicAdd(cursor + m, 1)] = k;
+  blist[atomicAdd(cursor + s, 1)] = k;
+}
+
+// keep[k] = 0 for a new contact with a duplicate point (the decision does not
+// depend on the order of the body lists)
+__global__ void k_sph_sparsify(int n, int nb, const int* master, const int* slave, const int* isnew,
+                               const double* point, const int* bptr, const int* blist, double margin, int* keep) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int kp = 1;
+  const int m = master[k], s = slave[k];
+  if (isnew[k] && m >= 0 && m < nb && s >= 0 && s < nb) {
+    const double p0 = point[3 * (size_t)k], p1 = point[3 * (size_t)k + 1], p2 = point[3 * (size_t)k + 2];
+    const int bb[2] = {m, s};
+    for (int t = 0; t < 2 && kp; t++)
+      for (int u = bptr[bb[t]]; u < bptr[bb[t] + 1]; u++) {
+        const int a = blist[u];
+        if (a == k || a < 0 || a >= n) continue;
+        const double e0 = fabs(p0 - point[3 * (size_t)a]), e1 = fabs(p1 - point[3 * (size_t)a + 1]),
+                     e2 = fabs(p2 - point[3 * (size_t)a + 2]);
+        double mx = 0.0;
+        if (e0 > mx) mx = e0;
+        if (e1 > mx) mx = e1;
+        if (e2 > mx) mx = e2;
+        if (mx < margin && (k < a || !isnew[a])) { kp = 0; break; }
+      }
+  }
+  keep[k] = kp;
+}
+
+// scatter kept contact k to slot pos[k] of the output arrays
+__global__ void k_sph_compact(int n, const int* keep, const int* pos, ContactOut in, ContactOut out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n || !keep[k]) return;
+  const int d = pos[k];
+  out.master[d] = in.master[k];
+  out.slave[d] = in.slave[k];
+  out.key[d] = in.key[k];
+  out.slave_lo[d] = in.slave_lo[k];
+  out.isnew[d] = in.isnew[k];
+  out.gap[d] = in.gap[k];
+  out.fric[d] = in.fric[k];
+  out.rest[d] = in.rest[k];
+  out.coh[d] = in.coh[k];
+  for (int v = 0; v < 3; v++) {
+    out.point[3 * (size_t)d + v] = in.point[3 * (size_t)k + v];
+    out.mpnt[3 * (size_t)d + v] = in.mpnt[3 * (size_t)k + v];
+    out.spnt[3 * (size_t)d + v] = in.spnt[3 * (size_t)k + v];
+    out.R0[3 * (size_t)d + v] = in.R0[3 * (size_t)k + v];
+    out.U0[3 * (size_t)d + v] = in.U0[3 * (size_t)k + v];
+  }
+  for (int v = 0; v < 9; v++) out.base[9 * (size_t)d + v] = in.base[9 * (size_t)k + v];
+}
+
+}  // namespace b2

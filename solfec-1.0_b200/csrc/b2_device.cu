@@ -24,6 +24,7 @@
 #include "b2_assemble.cuh"
 #include "b2_colour.cuh"
 #include "b2_rigid.cuh"
+#include "b2_detect.cuh"
 
 using namespace b2;
 
@@ -195,6 +196,20 @@ struct b2dev_ctx {
   // external force of the step, NEW2 auxiliary vector, per-step loads
   Buf rb_x, rb_J, rb_mass, rb_scheme, rb_fext, rb_aux, rb_loads;
   bool have_rigid = false;
+  // sphere contact detection (b2dev_spheres_setup, b2dev_detect_spheres): the
+  // spheres, the grid, the pair lists, the contacts before sparsification
+  // (st_*), and per contact of the last detection its sphere pair key, role
+  // flag, spatial point, new flag and carried R, U
+  int nsph = 0, nsurf = 0;
+  std::vector<double> sph_mat_h;
+  Buf sph_body, sph_ref, sph_rad, sph_surf, sph_mat, sph_cur, sph_cell, sph_hkey, sph_hkey_s, sph_idx, sph_sorted,
+      sph_bstart, sph_bend, sph_cnt, sph_off, sph_pi, sph_pj, sph_rmax, sph_keep, sph_pos, sph_bcnt, sph_bptr,
+      sph_blist, sph_pkey, sph_pslo, sph_pR, sph_pU;
+  Buf st_master, st_slave, st_point, st_mpnt, st_spnt, st_base, st_gap, st_fric, st_rest, st_coh, st_R0, st_U0,
+      st_key, st_slo, st_new;
+  Buf det_point, det_R0, det_U0, det_key, det_slo, det_new;
+  bool det_valid = false;       // the scene's contacts are those of the last detection
+  bool det_assembled = false;   // ... and the local dynamics was assembled from them
   std::vector<int> ptile_count;  // tiles per problem
   int trace_sweep = -1;  // sweep of the next solve whose diagonal solves are recorded
 
@@ -849,6 +864,7 @@ int b2dev_upload_scene(b2dev_ctx* c, int nbod, const double* rot, const double* 
   B2_TRY(upload(c, c->coh_c, cohesion, (size_t)ncon, on_device));
   c->have_scene = true;
   c->have_rigid = false;  // b2dev_rigid_setup again for the new bodies
+  c->det_valid = c->det_assembled = false;
   c->ready = false;
   return B2DEV_OK;
 }
@@ -868,6 +884,7 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
   c->step = step;
   c->dynamic = dynamic ? 1 : 0;
   c->assembled_mode = true;
+  c->det_assembled = c->det_valid;
   B2_CK(cudaEventRecord(c->ev[0], st));
 
   B2_TRY(ensure(c->factors, sizeof(double) * kFactorStride * (n + 1)));
@@ -1125,6 +1142,295 @@ int b2dev_rigid_get(b2dev_ctx* c, double* rot, double* x, double* velo, double* 
     if (velo0) B2_CK(cudaMemcpyAsync(velo0, c->velo0.p, sizeof(double) * 6 * nb, kd, st));
   }
   B2_CK(cudaStreamSynchronize(st));
+  return B2DEV_OK;
+}
+
+// ---- contact update and detection between spheres (dom.c:3700-3790) ----
+
+int b2dev_spheres_setup(b2dev_ctx* c, int nsph, const int* body, const double* centre, const double* radius,
+                        const int* surface, int nsurf, const double* material, int on_device) {
+  if (!c || !c->have_scene) { set_err("spheres_setup: no scene uploaded"); return B2DEV_ESTATE; }
+  if (nsph < 0 || !body || !centre || !radius || !surface || nsurf <= 0 || !material) {
+    set_err("spheres_setup: invalid arguments");
+    return B2DEV_EINVAL;
+  }
+  if (nsph > (1 << 30)) { set_err("spheres_setup: %d spheres exceed the pair key range", nsph); return B2DEV_EINVAL; }
+  for (int a = 0; a < nsurf; a++)
+    for (int b = 0; b < nsurf; b++)
+      for (int v = 0; v < 2; v++)
+        if (material[2 * ((size_t)a * nsurf + b) + v] != material[2 * ((size_t)b * nsurf + a) + v]) {
+          set_err("spheres_setup: the material table is not symmetric at surfaces (%d, %d)", a, b);
+          return B2DEV_EINVAL;
+        }
+  DeviceGuard g(c->device);
+  c->nsph = nsph;
+  c->nsurf = nsurf;
+  c->sph_mat_h.assign(material, material + 2 * (size_t)nsurf * nsurf);
+  B2_TRY(upload(c, c->sph_body, body, (size_t)nsph, on_device));
+  B2_TRY(upload(c, c->sph_ref, centre, (size_t)3 * nsph, on_device));
+  B2_TRY(upload(c, c->sph_rad, radius, (size_t)nsph, on_device));
+  B2_TRY(upload(c, c->sph_surf, surface, (size_t)nsph, on_device));
+  B2_TRY(upload(c, c->sph_mat, c->sph_mat_h.data(), c->sph_mat_h.size(), 0));
+  B2_CK(cudaStreamSynchronize(c->stream));
+  c->det_valid = c->det_assembled = false;
+  return B2DEV_OK;
+}
+
+static const char* detect_bad_text(int bad) {
+  if (bad & 16) return "a sphere's body index is out of range";
+  if (bad & 1) return "a sphere radius is not positive and finite, or a centre is not finite";
+  if (bad & 2) return "a sphere centre is too far from the origin for the detection grid";
+  if (bad & 4) return "two sphere centres coincide (no contact normal)";
+  return "a sphere's surface id is out of the material table";
+}
+
+static ContactOut staged(b2dev_ctx* c) {
+  ContactOut o;
+  o.master = ptr<int>(c->st_master); o.slave = ptr<int>(c->st_slave); o.point = ptr<double>(c->st_point);
+  o.mpnt = ptr<double>(c->st_mpnt); o.spnt = ptr<double>(c->st_spnt); o.base = ptr<double>(c->st_base);
+  o.gap = ptr<double>(c->st_gap); o.fric = ptr<double>(c->st_fric); o.rest = ptr<double>(c->st_rest);
+  o.coh = ptr<double>(c->st_coh); o.R0 = ptr<double>(c->st_R0); o.U0 = ptr<double>(c->st_U0);
+  o.key = ptr<long long>(c->st_key); o.slave_lo = ptr<int>(c->st_slo); o.isnew = ptr<int>(c->st_new);
+  return o;
+}
+
+int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
+  if (!c) { set_err("detect: null context"); return B2DEV_EINVAL; }
+  if (!c->have_scene || !c->have_rigid) {
+    set_err("detect: upload a scene and set up its rigid bodies (mass centres) first");
+    return B2DEV_ESTATE;
+  }
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  const int T = 256, ns = c->nsph, nb = c->nbod;
+
+  // the previous step's contacts: keys, roles and their R, U (the last solve's
+  // state when it was assembled from them, else the values they were given)
+  int nprev = c->det_valid ? c->ncon : 0;
+  B2_TRY(ensure(c->sph_pkey, sizeof(long long) * (nprev + 1)));
+  B2_TRY(ensure(c->sph_pslo, sizeof(int) * (nprev + 1)));
+  B2_TRY(ensure(c->sph_pR, sizeof(double) * 3 * (nprev + 1)));
+  B2_TRY(ensure(c->sph_pU, sizeof(double) * 3 * (nprev + 1)));
+  if (nprev > 0) {
+    B2_CK(cudaMemcpyAsync(c->sph_pkey.p, c->det_key.p, sizeof(long long) * nprev, cudaMemcpyDeviceToDevice, st));
+    B2_CK(cudaMemcpyAsync(c->sph_pslo.p, c->det_slo.p, sizeof(int) * nprev, cudaMemcpyDeviceToDevice, st));
+    if (c->det_assembled && c->n == nprev && c->state_u) {
+      c->launches++;
+      k_state_out<<<blocks_for(nprev, T), T, 0, st>>>(nprev, ptr<int>(c->perm), ptr<double4>(c->R64[c->state_r]),
+                                                       ptr<double4>(*c->state_u), nullptr, 1.0,
+                                                       ptr<double>(c->sph_pR), ptr<double>(c->sph_pU), nullptr);
+    } else {
+      B2_CK(cudaMemcpyAsync(c->sph_pR.p, c->det_R0.p, sizeof(double) * 3 * nprev, cudaMemcpyDeviceToDevice, st));
+      B2_CK(cudaMemcpyAsync(c->sph_pU.p, c->det_U0.p, sizeof(double) * 3 * nprev, cudaMemcpyDeviceToDevice, st));
+    }
+  }
+
+  // grid: cell edge from the largest radius, 2^k >= 2 n buckets
+  unsigned int M = 1024;
+  while (M < 2u * (unsigned int)ns) M *= 2;
+  int mbits = 0;
+  while ((1u << mbits) < M) mbits++;
+  B2_TRY(ensure(c->sph_cur, sizeof(double) * 3 * (ns + 1)));
+  B2_TRY(ensure(c->sph_cell, sizeof(int4) * (ns + 1)));
+  B2_TRY(ensure(c->sph_hkey, sizeof(unsigned int) * (ns + 1)));
+  B2_TRY(ensure(c->sph_hkey_s, sizeof(unsigned int) * (ns + 1)));
+  B2_TRY(ensure(c->sph_idx, sizeof(int) * (ns + 1)));
+  B2_TRY(ensure(c->sph_sorted, sizeof(int) * (ns + 1)));
+  B2_TRY(ensure(c->sph_bstart, sizeof(int) * M));
+  B2_TRY(ensure(c->sph_bend, sizeof(int) * M));
+  B2_TRY(ensure(c->sph_cnt, sizeof(int) * (ns + 1)));
+  B2_TRY(ensure(c->sph_off, sizeof(int) * (ns + 1)));
+  B2_TRY(ensure(c->sph_rmax, sizeof(unsigned long long)));
+  B2_TRY(ensure(c->bad, sizeof(int)));
+  B2_CK(cudaMemsetAsync(c->bad.p, 0, sizeof(int), st));
+  B2_CK(cudaMemsetAsync(c->sph_rmax.p, 0, sizeof(unsigned long long), st));
+  B2_CK(cudaMemsetAsync(c->sph_bstart.p, 0, sizeof(int) * M, st));
+  B2_CK(cudaMemsetAsync(c->sph_bend.p, 0, sizeof(int) * M, st));
+  B2_CK(cudaMemsetAsync(c->sph_cnt.p, 0, sizeof(int) * (ns + 1), st));
+  SphereDev sd;
+  sd.nsph = ns;
+  sd.nbod = nb;
+  sd.body = ptr<int>(c->sph_body); sd.ref = ptr<double>(c->sph_ref); sd.rad = ptr<double>(c->sph_rad);
+  sd.surf = ptr<int>(c->sph_surf); sd.cur = ptr<double>(c->sph_cur); sd.cell = ptr<int4>(c->sph_cell);
+  sd.hkey = ptr<unsigned int>(c->sph_hkey);
+  int npair = 0, bad = 0;
+  if (ns > 0) {
+    c->launches += 2;
+    k_sph_centres<<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<double>(c->rot), ptr<double>(c->rb_x),
+                                                   ptr<double>(c->x0), ptr<unsigned long long>(c->sph_rmax),
+                                                   ptr<int>(c->bad));
+    k_sph_cells<<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<unsigned long long>(c->sph_rmax), M - 1,
+                                                 ptr<int>(c->sph_idx), ptr<int>(c->bad));
+    size_t bytes = 0;
+    B2_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, ptr<unsigned int>(c->sph_hkey),
+                                          ptr<unsigned int>(c->sph_hkey_s), ptr<int>(c->sph_idx),
+                                          ptr<int>(c->sph_sorted), ns, 0, mbits, st));
+    B2_TRY(ensure(c->cub_tmp, bytes));
+    B2_CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, bytes, ptr<unsigned int>(c->sph_hkey),
+                                          ptr<unsigned int>(c->sph_hkey_s), ptr<int>(c->sph_idx),
+                                          ptr<int>(c->sph_sorted), ns, 0, mbits, st));
+    c->launches += 2;
+    k_sph_buckets<<<blocks_for(ns, T), T, 0, st>>>(ns, ptr<unsigned int>(c->sph_hkey_s), ptr<int>(c->sph_bstart),
+                                                   ptr<int>(c->sph_bend));
+    k_sph_pairs<false><<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<int>(c->obst), ptr<int>(c->sph_sorted),
+                                                        ptr<int>(c->sph_bstart), ptr<int>(c->sph_bend), M - 1,
+                                                        ptr<int>(c->sph_cnt), nullptr, nullptr);
+    B2_TRY(scan_exclusive(c, ptr<int>(c->sph_cnt), ptr<int>(c->sph_off), ns + 1));
+    B2_CK(cudaMemcpyAsync(&npair, ptr<int>(c->sph_off) + ns, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaMemcpyAsync(&bad, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaStreamSynchronize(st));
+    if (bad) { set_err("detect: %s", detect_bad_text(bad)); return B2DEV_EINVAL; }
+  }
+
+  // contacts of the pairs, in pair order
+  const size_t np1 = (size_t)npair + 1;
+  B2_TRY(ensure(c->sph_pi, sizeof(int) * np1));
+  B2_TRY(ensure(c->sph_pj, sizeof(int) * np1));
+  B2_TRY(ensure(c->st_master, sizeof(int) * np1));
+  B2_TRY(ensure(c->st_slave, sizeof(int) * np1));
+  B2_TRY(ensure(c->st_point, sizeof(double) * 3 * np1));
+  B2_TRY(ensure(c->st_mpnt, sizeof(double) * 3 * np1));
+  B2_TRY(ensure(c->st_spnt, sizeof(double) * 3 * np1));
+  B2_TRY(ensure(c->st_base, sizeof(double) * 9 * np1));
+  B2_TRY(ensure(c->st_gap, sizeof(double) * np1));
+  B2_TRY(ensure(c->st_fric, sizeof(double) * np1));
+  B2_TRY(ensure(c->st_rest, sizeof(double) * np1));
+  B2_TRY(ensure(c->st_coh, sizeof(double) * np1));
+  B2_TRY(ensure(c->st_R0, sizeof(double) * 3 * np1));
+  B2_TRY(ensure(c->st_U0, sizeof(double) * 3 * np1));
+  B2_TRY(ensure(c->st_key, sizeof(long long) * np1));
+  B2_TRY(ensure(c->st_slo, sizeof(int) * np1));
+  B2_TRY(ensure(c->st_new, sizeof(int) * np1));
+  B2_TRY(ensure(c->sph_keep, sizeof(int) * np1));
+  B2_TRY(ensure(c->sph_pos, sizeof(int) * np1));
+  B2_TRY(ensure(c->sph_bcnt, sizeof(int) * (nb + 1)));
+  B2_TRY(ensure(c->sph_bptr, sizeof(int) * (nb + 1)));
+  B2_TRY(ensure(c->sph_blist, sizeof(int) * 2 * np1));
+  const ContactOut so = staged(c);
+  int nkeep = 0, nfresh = 0;
+  if (npair > 0) {
+    c->launches += 3;
+    k_sph_pairs<true><<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<int>(c->obst), ptr<int>(c->sph_sorted),
+                                                       ptr<int>(c->sph_bstart), ptr<int>(c->sph_bend), M - 1,
+                                                       nullptr, ptr<int>(c->sph_off), ptr<int>(c->sph_pj));
+    k_sph_sort_seg<<<blocks_for(ns, T), T, 0, st>>>(ns, ptr<int>(c->sph_off), ptr<int>(c->sph_pj),
+                                                    ptr<int>(c->sph_pi));
+    k_sph_contacts<<<blocks_for(npair, T), T, 0, st>>>(
+        npair, sd, ptr<int>(c->sph_pi), ptr<int>(c->sph_pj), ptr<double>(c->rot), ptr<double>(c->rb_x),
+        ptr<double>(c->x0), c->nsurf, ptr<double>(c->sph_mat), nprev, ptr<long long>(c->sph_pkey),
+        ptr<int>(c->sph_pslo), ptr<double>(c->sph_pR), ptr<double>(c->sph_pU), so, ptr<int>(c->bad));
+    // sparsification neighbourhoods: the contacts of each body
+    B2_CK(cudaMemsetAsync(c->sph_bcnt.p, 0, sizeof(int) * (nb + 1), st));
+    c->launches++;
+    k_sph_body_count<<<blocks_for(npair, T), T, 0, st>>>(npair, nb, so.master, so.slave, ptr<int>(c->sph_bcnt),
+                                                         ptr<int>(c->bad));
+    B2_TRY(scan_exclusive(c, ptr<int>(c->sph_bcnt), ptr<int>(c->sph_bptr), nb + 1));
+    B2_CK(cudaMemcpyAsync(c->sph_bcnt.p, c->sph_bptr.p, sizeof(int) * (nb + 1), cudaMemcpyDeviceToDevice, st));
+    c->launches += 2;
+    k_sph_body_fill<<<blocks_for(npair, T), T, 0, st>>>(npair, nb, so.master, so.slave, ptr<int>(c->sph_bcnt),
+                                                        ptr<int>(c->sph_blist));
+    k_sph_sparsify<<<blocks_for(npair, T), T, 0, st>>>(npair, nb, so.master, so.slave, so.isnew, so.point,
+                                                       ptr<int>(c->sph_bptr), ptr<int>(c->sph_blist),
+                                                       2.0 * kGeomEps, ptr<int>(c->sph_keep));
+    B2_TRY(scan_exclusive(c, ptr<int>(c->sph_keep), ptr<int>(c->sph_pos), npair));
+    int lastpos = 0, lastkeep = 0;
+    B2_CK(cudaMemcpyAsync(&lastpos, ptr<int>(c->sph_pos) + npair - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaMemcpyAsync(&lastkeep, ptr<int>(c->sph_keep) + npair - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaMemcpyAsync(&bad, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaStreamSynchronize(st));
+    if (bad) { set_err("detect: %s", detect_bad_text(bad)); return B2DEV_EINVAL; }
+    nkeep = lastpos + lastkeep;
+  }
+
+  // the kept contacts become the scene's contacts
+  const size_t nk1 = (size_t)nkeep + 1;
+  B2_TRY(ensure(c->master, sizeof(int) * nk1));
+  B2_TRY(ensure(c->slave, sizeof(int) * nk1));
+  B2_TRY(ensure(c->mpnt, sizeof(double) * 3 * nk1));
+  B2_TRY(ensure(c->spnt, sizeof(double) * 3 * nk1));
+  B2_TRY(ensure(c->base, sizeof(double) * 9 * nk1));
+  B2_TRY(ensure(c->gap_c, sizeof(double) * nk1));
+  B2_TRY(ensure(c->fric_c, sizeof(double) * nk1));
+  B2_TRY(ensure(c->rest_c, sizeof(double) * nk1));
+  B2_TRY(ensure(c->coh_c, sizeof(double) * nk1));
+  B2_TRY(ensure(c->det_point, sizeof(double) * 3 * nk1));
+  B2_TRY(ensure(c->det_R0, sizeof(double) * 3 * nk1));
+  B2_TRY(ensure(c->det_U0, sizeof(double) * 3 * nk1));
+  B2_TRY(ensure(c->det_key, sizeof(long long) * nk1));
+  B2_TRY(ensure(c->det_slo, sizeof(int) * nk1));
+  B2_TRY(ensure(c->det_new, sizeof(int) * nk1));
+  if (npair > 0) {
+    ContactOut d;
+    d.master = ptr<int>(c->master); d.slave = ptr<int>(c->slave); d.point = ptr<double>(c->det_point);
+    d.mpnt = ptr<double>(c->mpnt); d.spnt = ptr<double>(c->spnt); d.base = ptr<double>(c->base);
+    d.gap = ptr<double>(c->gap_c); d.fric = ptr<double>(c->fric_c); d.rest = ptr<double>(c->rest_c);
+    d.coh = ptr<double>(c->coh_c); d.R0 = ptr<double>(c->det_R0); d.U0 = ptr<double>(c->det_U0);
+    d.key = ptr<long long>(c->det_key); d.slave_lo = ptr<int>(c->det_slo); d.isnew = ptr<int>(c->det_new);
+    c->launches++;
+    k_sph_compact<<<blocks_for(npair, T), T, 0, st>>>(npair, ptr<int>(c->sph_keep), ptr<int>(c->sph_pos), so, d);
+    // new contacts kept
+    B2_TRY(ensure(c->sph_cnt, sizeof(int) * nk1));
+    size_t bytes = 0;
+    B2_CK(cub::DeviceReduce::Sum(nullptr, bytes, ptr<int>(c->det_new), ptr<int>(c->sph_cnt), nkeep, st));
+    B2_TRY(ensure(c->cub_tmp, bytes));
+    B2_CK(cub::DeviceReduce::Sum(c->cub_tmp.p, bytes, ptr<int>(c->det_new), ptr<int>(c->sph_cnt), nkeep, st));
+    B2_CK(cudaMemcpyAsync(&nfresh, c->sph_cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  }
+  B2_CK(cudaGetLastError());
+  B2_CK(cudaStreamSynchronize(st));
+  c->ncon = nkeep;
+  c->det_valid = true;
+  c->det_assembled = false;
+  c->ready = false;  // the local dynamics must be assembled for the new contacts
+  if (ncon) *ncon = nkeep;
+  if (nnew) *nnew = nfresh;
+  return B2DEV_OK;
+}
+
+int b2dev_detect_carry_state(b2dev_ctx* c) {
+  if (!c || !c->det_valid || !c->det_assembled || !c->ready || c->n != c->ncon) {
+    set_err("detect_carry_state: assemble the contacts of the last detection first");
+    return B2DEV_ESTATE;
+  }
+  return b2dev_set_state(c, ptr<double>(c->det_R0), ptr<double>(c->det_U0), 1);
+}
+
+int b2dev_get_contacts(b2dev_ctx* c, int* master, int* slave, double* point, double* mpnt, double* spnt,
+                       double* base, double* gap, double* friction, double* restitution, long long* key,
+                       int* slave_lo, int* isnew, double* R0, double* U0, int on_device) {
+  if (!c || !c->det_valid) { set_err("get_contacts: no detection"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  const size_t n = (size_t)c->ncon;
+  const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (n > 0) {
+    if (master) B2_CK(cudaMemcpyAsync(master, c->master.p, sizeof(int) * n, kd, st));
+    if (slave) B2_CK(cudaMemcpyAsync(slave, c->slave.p, sizeof(int) * n, kd, st));
+    if (point) B2_CK(cudaMemcpyAsync(point, c->det_point.p, sizeof(double) * 3 * n, kd, st));
+    if (mpnt) B2_CK(cudaMemcpyAsync(mpnt, c->mpnt.p, sizeof(double) * 3 * n, kd, st));
+    if (spnt) B2_CK(cudaMemcpyAsync(spnt, c->spnt.p, sizeof(double) * 3 * n, kd, st));
+    if (base) B2_CK(cudaMemcpyAsync(base, c->base.p, sizeof(double) * 9 * n, kd, st));
+    if (gap) B2_CK(cudaMemcpyAsync(gap, c->gap_c.p, sizeof(double) * n, kd, st));
+    if (friction) B2_CK(cudaMemcpyAsync(friction, c->fric_c.p, sizeof(double) * n, kd, st));
+    if (restitution) B2_CK(cudaMemcpyAsync(restitution, c->rest_c.p, sizeof(double) * n, kd, st));
+    if (key) B2_CK(cudaMemcpyAsync(key, c->det_key.p, sizeof(long long) * n, kd, st));
+    if (slave_lo) B2_CK(cudaMemcpyAsync(slave_lo, c->det_slo.p, sizeof(int) * n, kd, st));
+    if (isnew) B2_CK(cudaMemcpyAsync(isnew, c->det_new.p, sizeof(int) * n, kd, st));
+    if (R0) B2_CK(cudaMemcpyAsync(R0, c->det_R0.p, sizeof(double) * 3 * n, kd, st));
+    if (U0) B2_CK(cudaMemcpyAsync(U0, c->det_U0.p, sizeof(double) * 3 * n, kd, st));
+  }
+  B2_CK(cudaStreamSynchronize(st));
+  return B2DEV_OK;
+}
+
+int b2dev_sphere_centres(b2dev_ctx* c, double* cur, int on_device) {
+  if (!c || !cur) { set_err("sphere_centres: null argument"); return B2DEV_EINVAL; }
+  if (!c->det_valid) { set_err("sphere_centres: no detection"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  if (c->nsph > 0)
+    B2_CK(cudaMemcpyAsync(cur, c->sph_cur.p, sizeof(double) * 3 * c->nsph,
+                          on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
+  B2_CK(cudaStreamSynchronize(c->stream));
   return B2DEV_OK;
 }
 

@@ -7,3 +7,4 @@ this package binds it and provides the seeded synthetic scenes."""
 from .solver import GAUSS_SEIDEL_SOLVER, LOCDYN, SolfecError, DeviceError  # noqa: F401
 from . import scenes  # noqa: F401
 from . import dynamics  # noqa: F401
+from . import detect  # noqa: F401

@@ -78,6 +78,12 @@ _SIGNATURES = {
     'b2dev_rigid_step_begin': (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int]),
     'b2dev_rigid_step_end': (C.c_int, [C.c_void_p, C.c_double]),
     'b2dev_rigid_get': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    'b2dev_spheres_setup': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                      C.c_void_p, C.c_int]),
+    'b2dev_detect_spheres': (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    'b2dev_detect_carry_state': (C.c_int, [C.c_void_p]),
+    'b2dev_get_contacts': (C.c_int, [C.c_void_p] + [C.c_void_p] * 14 + [C.c_int]),
+    'b2dev_sphere_centres': (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     'b2dev_upload_locdyn': (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 12 + [C.c_double, C.c_double, C.c_int,
                                                                                   C.c_uint64, C.c_int]),
     'b2dev_set_state': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),

@@ -53,6 +53,7 @@ class Scene:
     restitution: np.ndarray
     cohesion: np.ndarray   # (nc,) cohesion * area, as dbs.c:500 forms it
     mass: np.ndarray = None  # (nb,) for diagnostics
+    radius: np.ndarray = None  # (nb,) sphere radius of sphere bodies, 0 for the others
 
     @property
     def nbod(self) -> int:
@@ -231,8 +232,10 @@ def _sphere_scene(name, rng, x, r, density, lo, hi, step, friction, restitution,
         velo0[:n, 0:3] = rng.normal(0.0, vel_sigma, (n, 3)) / r[:, None]
     obstacle = np.zeros(nb, np.int32); obstacle[n:] = 1
     fr = friction(master.shape[0]) if callable(friction) else friction
-    return _assemble_scene(name, step, xb, rot, x0, jinv, minv, mass, velo0, obstacle, master, slave, points,
-                           normals, gaps, fr, restitution, 0.0)
+    sc = _assemble_scene(name, step, xb, rot, x0, jinv, minv, mass, velo0, obstacle, master, slave, points,
+                         normals, gaps, fr, restitution, 0.0)
+    rad = np.zeros(nb); rad[:n] = r
+    return dataclasses.replace(sc, radius=rad)
 
 
 # ----------------------------------------------------------------------------- configurations
@@ -548,3 +551,93 @@ CONFIGS = {
     'spheres20k': spheres_polydisperse,
     'hexahedra100k': hexahedra_lattice,
 }
+
+
+# ----------------------------------------------------------------------------- sphere shapes for detection
+
+def sphere_shapes(scene: Scene, friction: float = None, restitution: float = 0.0) -> dict:
+    """SPHERES arguments for the sphere bodies of a scene (radius > 0): one
+    sphere per body, centred on its referential mass centre, one surface, and
+    the scene's friction (its first contact's) unless given."""
+    if scene.radius is None:
+        raise ValueError('scene %s has no sphere bodies' % scene.name)
+    body = np.nonzero(scene.radius > 0)[0].astype(np.int32)
+    if friction is None:
+        friction = float(scene.friction[0]) if scene.ncon else 0.0
+    return dict(body=body, centre=scene.x0[body].copy(), radius=scene.radius[body].copy(),
+                surface=np.zeros(body.shape[0], np.int32), material=(float(friction), float(restitution)))
+
+
+def sphere_inertia(scene: Scene):
+    """(J, mass) of a sphere scene for RIGID_DYNAMICS: J = 0.4 m r^2 I for the
+    spheres, the identity and mass 1 for the other (obstacle) bodies."""
+    nb = scene.nbod
+    mass = np.ones(nb) if scene.mass is None else np.asarray(scene.mass, float).copy()
+    J = np.zeros((nb, 9))
+    r = np.zeros(nb) if scene.radius is None else scene.radius
+    for k in (0, 4, 8):
+        J[:, k] = np.where(r > 0, 0.4 * mass * r ** 2, 1.0)
+    return J, mass
+
+
+def spheres_on_bed(seed: int = 5, n_side: int = 6, layers: int = 3, radius: float = 0.05, pitch: float = 0.11,
+                   bed_radius: float = 0.1, bed_pitch: float = 0.2, density: float = 2000.0, friction: float = 0.3,
+                   step: float = 1e-3, drop: float = 0.002):
+    """Spheres falling onto a bed of fixed spheres: an n_side x n_side x layers
+    jittered lattice of spheres (radius, pitch) above a square grid of obstacle
+    spheres (bed_radius, bed_pitch) covering the lattice's footprint. The lowest
+    layer starts ``drop`` above the bed. Every body is one sphere, so the
+    contacts come from sphere detection alone.
+
+    Returns (scene without contacts, SPHERES arguments, J, mass)."""
+    rng = np.random.default_rng(seed)
+    half = (n_side - 1) / 2.0 * pitch + radius
+    nbed = int(np.ceil(2 * half / bed_pitch)) + 1
+    gb = (np.arange(nbed) - (nbed - 1) / 2.0) * bed_pitch
+    BX, BY = np.meshgrid(gb, gb, indexing='ij')
+    bed = np.stack([BX.ravel(), BY.ravel(), np.zeros(BX.size)], axis=1)
+    g = (np.arange(n_side) - (n_side - 1) / 2.0) * pitch
+    z0 = bed_radius + radius + drop
+    X, Y, Z = np.meshgrid(g, g, z0 + np.arange(layers) * pitch, indexing='ij')
+    xs = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    xs[:, :2] += rng.uniform(-0.1 * (pitch - 2 * radius), 0.1 * (pitch - 2 * radius), (xs.shape[0], 2))
+    n = xs.shape[0]
+    nb = n + bed.shape[0]
+    x = np.concatenate([xs, bed], axis=0)
+    r = np.concatenate([np.full(n, radius), np.full(bed.shape[0], bed_radius)])
+    mass = np.ones(nb); mass[:n] = density * 4.0 / 3.0 * math.pi * radius ** 3
+    jinv = np.zeros((nb, 9)); jinv[:n, 0] = jinv[:n, 4] = jinv[:n, 8] = 1.0 / (0.4 * mass[:n] * radius ** 2)
+    minv = np.zeros(nb); minv[:n] = 1.0 / mass[:n]
+    rot = np.zeros((nb, 9)); rot[:, 0] = rot[:, 4] = rot[:, 8] = 1.0
+    rot[:n] = _random_rotations(rng, n)
+    obstacle = np.zeros(nb, np.int32); obstacle[n:] = 1
+    z = np.zeros((nb, 6))
+    e = np.zeros(0)
+    sc = Scene(name='spheres-on-bed-%d' % n, step=step, dynamic=1, rot=rot, x=x.copy(), x0=x.copy(), jinv=jinv,
+               minv=minv, velo=z.copy(), velo0=z.copy(), obstacle=obstacle, master=np.zeros(0, np.int32),
+               slave=np.zeros(0, np.int32), mpnt=np.zeros((0, 3)), spnt=np.zeros((0, 3)), base=np.zeros((0, 9)),
+               gap=e, friction=e, restitution=e, cohesion=e, mass=mass, radius=r)
+    J, mass = sphere_inertia(sc)
+    sph = dict(body=np.arange(nb, dtype=np.int32), centre=x.copy(), radius=r.copy(),
+               surface=np.zeros(nb, np.int32), material=(friction, 0.0))
+    return sc, sph, J, mass
+
+
+def spheres_grid(n_side: int = 100, radius: float = 0.05, pitch: float = 0.0999, jitter: float = 1e-5,
+                 density: float = 2000.0, seed: int = 8, step: float = 1e-3) -> Scene:
+    """n_side^3 spheres on a cubic grid whose face neighbours overlap by
+    2 radius - pitch (jittered by +-jitter per coordinate), no obstacles and no
+    contacts: a detection workload with six contacts per interior sphere."""
+    rng = np.random.default_rng(seed)
+    g = np.arange(n_side) * pitch
+    X, Y, Z = np.meshgrid(g, g, g, indexing='ij')
+    x = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1) + rng.uniform(-jitter, jitter, (n_side ** 3, 3))
+    n = x.shape[0]
+    m = density * 4.0 / 3.0 * math.pi * radius ** 3
+    eye = np.tile(np.eye(3).reshape(9), (n, 1))
+    e = np.zeros(0)
+    return Scene(name='spheres-grid-%d' % n, step=step, dynamic=1, rot=eye.copy(), x=x, x0=x.copy(),
+                 jinv=eye / (0.4 * m * radius ** 2), minv=np.full(n, 1.0 / m), velo=np.zeros((n, 6)),
+                 velo0=np.zeros((n, 6)), obstacle=np.zeros(n, np.int32), master=np.zeros(0, np.int32),
+                 slave=np.zeros(0, np.int32), mpnt=np.zeros((0, 3)), spnt=np.zeros((0, 3)), base=np.zeros((0, 9)),
+                 gap=e, friction=e, restitution=e, cohesion=e, mass=np.full(n, m), radius=np.full(n, radius))

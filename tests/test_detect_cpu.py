@@ -1,0 +1,174 @@
+"""CPU tests of the sphere contact detection oracle (oracle/oracle_detect.c):
+gjk_sphere_sphere pinned bit for bit to the reference's own gjk.c (compiled
+into oracle/_ref), the restated contact formulas against an independent
+vectorised restatement, and the update, filter and sparsification rules of
+dom.c and box.c on hand-built cases."""
+import numpy as np
+import pytest
+
+import oracle
+from solfec_b200 import scenes
+
+MAT = np.array([[[0.3, 0.0]]])
+EPS = 1e-6
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, dtype=np.float64).view(np.uint64)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason='reference build unavailable')
+def test_gjk_sphere_sphere_pinned_to_reference():
+    rng = np.random.default_rng(11)
+    for t in range(3000):
+        a = rng.normal(size=3)
+        scale = [1e-7, 1e-3, 0.1, 1.0][t % 4]
+        b = a + rng.normal(size=3) * scale
+        ra, rb = rng.uniform(0.01, 1.0, 2)
+        if t % 5 == 0:   # touching within GEOMETRIC_EPSILON
+            d = rng.normal(size=3)
+            d /= np.linalg.norm(d)
+            b = a + d * (ra + rb + rng.uniform(-2e-6, 2e-6))
+        if t % 97 == 0:
+            b = a.copy()
+        g1, p1, q1 = oracle.gjk_sphere_sphere(a, ra, b, rb, 'oracle')
+        g2, p2, q2 = oracle.gjk_sphere_sphere(a, ra, b, rb, 'ref')
+        assert _bits([g1]) == _bits([g2]) and np.array_equal(_bits(p1), _bits(p2)) and np.array_equal(_bits(q1), _bits(q2))
+
+
+def test_localbase_frame():
+    rng = np.random.default_rng(3)
+    ns = [np.array([1.0, 0, 0]), np.array([-1.0, 0, 0]), np.array([0, 0, 1.0])]
+    ns += [v / np.linalg.norm(v) for v in rng.normal(size=(50, 3))]
+    for n in ns:
+        L = oracle.localbase(n).reshape(3, 3).T   # column-major storage
+        assert np.array_equal(L[:, 2], n)
+        assert np.allclose(L.T @ L, np.eye(3), atol=1e-14)
+    # e_x x n vanishes for n = e_x: the reference falls back to e_y x n
+    L = oracle.localbase([1.0, 0, 0]).reshape(3, 3).T
+    assert np.array_equal(L[:, 0], [0.0, 0.0, -1.0])
+
+
+def _numpy_contacts(cur, rad, sbody, obst):
+    """Independent restatement: all pairs by brute force, the reference's
+    formulas in numpy, the lower centre (point order) as the slave."""
+    n = cur.shape[0]
+    I, J = np.triu_indices(n, 1)
+    keep = (sbody[I] != sbody[J]) & ~((obst[sbody[I]] != 0) & (obst[sbody[J]] != 0))
+    I, J = I[keep], J[keep]
+    d = cur[I] - cur[J]
+    dlen = np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+    deno = rad[I] + rad[J]
+    g = np.where(dlen > deno, dlen - deno, 0.0)
+    m = g < EPS
+    I, J = I[m], J[m]
+    lo_slave = np.array([tuple(cur[i]) <= tuple(cur[j]) for i, j in zip(I, J)], dtype=bool)
+    s = np.where(lo_slave, I, J)
+    mm = np.where(lo_slave, J, I)
+    d = cur[s] - cur[mm]
+    dlen = np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+    p = cur[s] - (rad[s] / dlen)[:, None] * d
+    q = cur[mm] + (rad[mm] / dlen)[:, None] * d
+    over = ~(dlen > rad[s] + rad[mm])
+    mid = .5 * (p + q)
+    p = np.where(over[:, None], mid, p)
+    q = np.where(over[:, None], mid, q)
+    nrm = p - cur[s]
+    ln = np.sqrt(nrm[:, 0] * nrm[:, 0] + nrm[:, 1] * nrm[:, 1] + nrm[:, 2] * nrm[:, 2])
+    nrm = nrm / ln[:, None]
+    x = cur[mm] - cur[s]
+    dd = x[:, 0] * nrm[:, 0] + x[:, 1] * nrm[:, 1] + x[:, 2] * nrm[:, 2]
+    e = rad[s] + rad[mm]
+    gap = np.where(e > dd, dd - e, 0.0)
+    return dict(key=(I.astype(np.int64) << 32) | J, slave_lo=lo_slave.astype(np.int32), point=q, gap=gap,
+                normal=nrm, master=sbody[mm], slave=sbody[s])
+
+
+def test_oracle_matches_vectorised_restatement(scene_cache):
+    sc = scene_cache('spheres_lattice')
+    sp = scenes.sphere_shapes(sc)
+    got = oracle.detect_spheres(sp['body'], sp['centre'], sp['radius'], sp['surface'], sc.rot, sc.x, sc.x0,
+                                sc.obstacle, MAT)
+    cur = oracle.sphere_centres(sp['body'], sp['centre'], sc.rot, sc.x, sc.x0)
+    ref = _numpy_contacts(cur, sp['radius'], sp['body'], sc.obstacle)
+    assert got['key'].shape[0] > 1000
+    assert np.array_equal(got['key'], ref['key'])
+    assert np.array_equal(got['slave_lo'], ref['slave_lo'])
+    assert np.array_equal(got['master'], ref['master']) and np.array_equal(got['slave'], ref['slave'])
+    for k in ('point', 'gap'):
+        assert np.array_equal(_bits(got[k]), _bits(ref[k])), k
+    assert np.array_equal(_bits(got['base'][:, 6:9]), _bits(ref['normal']))
+    assert np.all(got['friction'] == 0.3) and np.all(got['isnew'] == 1)
+    # referential points map back onto the spatial ones
+    R = sc.rot.reshape(-1, 3, 3).transpose(0, 2, 1)
+    xm = sc.x[got['master']] + np.einsum('nij,nj->ni', R[got['master']], got['mpnt'] - sc.x0[got['master']])
+    assert np.allclose(xm, got['point'], atol=1e-12)
+
+
+def _two_spheres(c0, c1, r=(0.5, 0.5), obst=(0, 0), body=(0, 1)):
+    nb = max(body) + 1
+    rot = np.tile(np.eye(3).reshape(9), (nb, 1))
+    x = np.zeros((nb, 3))
+    x0 = np.zeros((nb, 3))
+    sref = np.array([c0, c1], float)
+    return dict(sbody=np.array(body), sref=sref, rad=np.array(r, float), surf=np.zeros(2, np.int32), rot=rot, x=x,
+                x0=x0, obst=np.array(obst[:nb]))
+
+
+def _detect(c, prev=None):
+    return oracle.detect_spheres(c['sbody'], c['sref'], c['rad'], c['surf'], c['rot'], c['x'], c['x0'], c['obst'],
+                                 MAT, prev)
+
+
+def test_update_keeps_roles_and_drops_separated():
+    # sphere 0 below sphere 1 (equal x and y): sphere 0 is the slave
+    c = _two_spheres([0, 0, 0], [0, 0, 0.999])
+    a = _detect(c)
+    assert a['key'].tolist() == [1] and a['slave_lo'].tolist() == [1] and a['isnew'].tolist() == [1]
+    # the centres swap heights: a fresh detection would make sphere 1 the slave,
+    # the update keeps sphere 0 as the slave (update_contact keeps the roles)
+    c2 = _two_spheres([0, 0, 0.999], [0, 0, 0])
+    assert _detect(c2)['slave_lo'].tolist() == [0]
+    prev = dict(a, R=np.array([[1.0, 2.0, 3.0]]), U=np.array([[4.0, 5.0, 6.0]]))
+    b = _detect(c2, prev)
+    assert b['slave_lo'].tolist() == [1] and b['isnew'].tolist() == [0]
+    assert b['R'].tolist() == [[1.0, 2.0, 3.0]] and b['U'].tolist() == [[4.0, 5.0, 6.0]]
+    assert b['slave'].tolist() == [0] and b['master'].tolist() == [1]
+    # separated by more than GEOMETRIC_EPSILON: removed; within it: kept with gap 0
+    assert _detect(_two_spheres([0, 0, 0], [0, 0, 1.0 + 2e-6]), prev)['key'].shape[0] == 0
+    k = _detect(_two_spheres([0, 0, 0], [0, 0, 1.0 + 5e-7]), prev)
+    assert k['key'].shape[0] == 1 and k['gap'][0] == 0.0
+
+
+def test_filters_same_body_and_obstacle_pairs():
+    assert _detect(_two_spheres([0, 0, 0], [0, 0, 0.9], body=(0, 0)))['key'].shape[0] == 0
+    assert _detect(_two_spheres([0, 0, 0], [0, 0, 0.9], obst=(1, 1)))['key'].shape[0] == 0
+    assert _detect(_two_spheres([0, 0, 0], [0, 0, 0.9], obst=(1, 0)))['key'].shape[0] == 1
+
+
+def test_coincident_centres_rejected():
+    with pytest.raises(ValueError):
+        _detect(_two_spheres([0, 0, 0], [0, 0, 0]))
+
+
+def _three():
+    # sphere 0 touches spheres 1 and 2, whose contact points with it lie within
+    # 2 mindist of each other; 1 and 2 (other bodies) overlap too
+    nb = 3
+    rot = np.tile(np.eye(3).reshape(9), (nb, 1))
+    sref = np.array([[0, 0, 0], [0.999, 0, 0], [0.999 + 1e-7, 0, 0]], float)
+    return dict(sbody=np.arange(3), sref=sref, rad=np.full(3, 0.5), surf=np.zeros(3, np.int32), rot=rot,
+                x=np.zeros((3, 3)), x0=np.zeros((3, 3)), obst=np.zeros(3, np.int32))
+
+
+def test_sparsify_duplicate_points():
+    c = _three()
+    out = _detect(c)
+    # pairs (0,1), (0,2), (1,2): the earlier of the two new contacts of sphere 0
+    # with duplicate points, (0,1), is removed (sparsify_contacts keeps the later id)
+    assert out['key'].tolist() == [(0 << 32) | 2, (1 << 32) | 2]
+    # with (0,1) an old contact, the new (0,2) goes instead
+    first = _detect(_two_spheres([0, 0, 0], [0.999, 0, 0]))
+    prev = dict(key=first['key'], slave_lo=first['slave_lo'])
+    out = _detect(c, prev)
+    assert out['key'].tolist() == [1, (1 << 32) | 2] and out['isnew'].tolist() == [0, 1]

@@ -1,0 +1,150 @@
+"""GPU tests of the sphere contact update and detection (csrc/b2_detect.cuh
+through the C ABI b2dev_spheres_setup / b2dev_detect_spheres): bit-for-bit
+parity of every contact array with the CPU restatement
+oracle/oracle_detect.c on settled packings (1000 equal spheres, 20000
+polydisperse spheres), and inside a device time loop where bodies move,
+contacts appear, persist with their roles and carried R and U, and separate."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import oracle
+from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN, DeviceError, scenes
+from solfec_b200._lib import lib
+from solfec_b200.detect import SPHERES, bodies_only, run_spheres
+from solfec_b200.dynamics import RIGID_DYNAMICS
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ['key', 'slave_lo', 'master', 'slave', 'point', 'mpnt', 'spnt', 'base', 'gap', 'friction', 'restitution',
+        'R', 'U', 'isnew']
+
+
+def _same(dev, orc):
+    assert dev['key'].shape[0] == orc['key'].shape[0]
+    for k in KEYS:
+        a, b = np.asarray(dev[k]), np.asarray(orc[k])
+        if a.dtype.kind == 'f':
+            assert np.array_equal(a.view(np.uint64), np.ascontiguousarray(b, dtype=np.float64).view(np.uint64)), k
+        else:
+            assert np.array_equal(a.astype(np.int64), b.astype(np.int64)), k
+
+
+def _oracle(sp, rot, x, x0, obst, prev=None):
+    mat = np.asarray(sp['material'], float).reshape(1, 1, 2)
+    return oracle.detect_spheres(sp['body'], sp['centre'], sp['radius'], sp['surface'], rot, x, x0, obst, mat, prev)
+
+
+def _detect_scene(sc):
+    sp = scenes.sphere_shapes(sc)
+    J, mass = scenes.sphere_inertia(sc)
+    ldy = LOCDYN()
+    ldy.update_begin(bodies_only(sc))
+    RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    sph = SPHERES(ldy, **sp)
+    nc, nn = sph.detect()
+    dev = sph.contacts()
+    cur = sph.centres()
+    orc = _oracle(sp, sc.rot, sc.x, sc.x0, sc.obstacle)
+    assert nc == nn == orc['key'].shape[0]
+    assert np.array_equal(cur, oracle.sphere_centres(sp['body'], sp['centre'], sc.rot, sc.x, sc.x0))
+    _same(dev, orc)
+    ldy.close()
+    return nc
+
+
+def test_detect_lattice_matches_oracle(scene_cache):
+    assert _detect_scene(scene_cache('spheres_lattice')) > 1000
+
+
+def test_detect_polydisperse_matches_oracle(scene_cache):
+    assert _detect_scene(scene_cache('spheres_polydisperse')) > 10000
+
+
+def test_time_loop_matches_oracle_every_step():
+    """Spheres falling onto a bed of fixed spheres: every step's detection on
+    the device bodies equals the oracle's, given the previous step's contacts
+    and the R and U of the device solve."""
+    sc, sp, J, mass = scenes.spheres_on_bed()
+    ldy = LOCDYN()
+    ldy.update_begin(bodies_only(sc))
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    sph = SPHERES(ldy, **sp)
+    gs = GAUSS_SEIDEL_SOLVER(1e-6, 200, diagsolver='SEMISMOOTH_NEWTON')
+    prev = None
+    seen_new = seen_kept = seen_dropped = 0
+    h = sc.step
+    for k in range(120):
+        dyn.step_begin(h, (0.0, 0.0, -9.81))
+        st = dyn.state()
+        nc, nn = sph.detect()
+        dev = sph.contacts()
+        orc = _oracle(sp, st['rot'], st['x'], sc.x0, sc.obstacle, prev)
+        _same(dev, orc)
+        if prev is not None:
+            seen_dropped += int(np.setdiff1d(prev['key'], dev['key']).shape[0])
+        seen_new += nn
+        seen_kept += nc - nn
+        if nc > 0:
+            assert lib().b2gs_locdyn_update_begin_resident(ldy.handle, h, 1) == 0
+            sph.carry_state()
+            R0, U0, _ = ldy.get_state()
+            assert np.array_equal(R0, dev['R']) and np.array_equal(U0, dev['U'])
+            gs.solve(ldy)
+            R, U, _ = ldy.get_state()
+            prev = dict(key=dev['key'], slave_lo=dev['slave_lo'], R=R, U=U)
+        else:
+            prev = dict(key=dev['key'], slave_lo=dev['slave_lo'])
+        dyn.step_end(h)
+    assert seen_new > 0 and seen_kept > 0
+    # the spheres rest on the bed: no deep interpenetration, none fell through
+    assert dev['gap'].min() > -2e-3, dev['gap'].min()
+    assert np.all(dyn.state()['x'][sc.obstacle == 0, 2] > 0.04)
+    ldy.close()
+
+
+def test_run_spheres_loop():
+    sc, sp, J, mass = scenes.spheres_on_bed(seed=6, n_side=4, layers=2)
+    gs = GAUSS_SEIDEL_SOLVER(1e-6, 200)
+    counts = []
+    dyn, sph, ldy = run_spheres(sc, sp, gs, 80, J, mass, gravity=(0.0, 0.0, -9.81),
+                                callback=lambda k, d, s, l: counts.append(s.ncon))
+    assert max(counts) > 0 and counts[0] == 0
+    assert np.all(dyn.state()['x'][sc.obstacle == 0, 2] > 0.04)
+    ldy.close()
+
+
+def _pair_scene(dz):
+    """spheres_on_bed with body 1 moved onto body 0 (dz above it); every
+    sphere centred on its body, so the current centres are exact."""
+    sc, sp, J, mass = scenes.spheres_on_bed(seed=7, n_side=2, layers=1)
+    x = sc.x.copy()
+    x[1] = x[0] + np.array([0.0, 0.0, dz])
+    sc = dataclasses.replace(sc, x=x, x0=x.copy())
+    sp = dict(sp, centre=x.copy())
+    return sc, sp, J, mass
+
+
+def _setup(sc, J, mass):
+    ldy = LOCDYN()
+    ldy.update_begin(bodies_only(sc))
+    RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    return ldy
+
+
+def test_detect_errors_reported():
+    sc, sp, J, mass = _pair_scene(0.0)   # coincident centres of two bodies
+    ldy = _setup(sc, J, mass)
+    with pytest.raises(DeviceError, match='coincide'):
+        SPHERES(ldy, **sp).detect()
+    ldy.close()
+    sc, sp, J, mass = _pair_scene(0.09)  # one contact, surface 3 of a one-surface table
+    ldy = _setup(sc, J, mass)
+    with pytest.raises(DeviceError, match='surface'):
+        SPHERES(ldy, **dict(sp, surface=np.full(sp['body'].shape[0], 3, np.int32))).detect()
+    with pytest.raises(DeviceError, match='symmetric'):
+        SPHERES(ldy, **dict(sp, material=np.array([[[0.1, 0.0], [0.2, 0.0]], [[0.3, 0.0], [0.1, 0.0]]])))
+    s = SPHERES(ldy, **sp)
+    assert s.detect() == (1, 1)
+    ldy.close()
