@@ -24,6 +24,10 @@ persistent launch replayed from a CUDA graph, launch shape autotuned; it
 reports contacts solved per second and the per-scene time to the final
 decision (p50, p99).
 
+--workload detect times the sphere contact update and detection alone on a
+grid of --detect-grid^3 overlapping spheres (the `detect` key of the default
+line, on 100^3 spheres).
+
 With --gpus N > 1 (torchrun), every rank solves its own replica scene (the
 path has no exchange step for independent scenes): per-step time is the max
 over ranks.
@@ -306,8 +310,8 @@ DETECT_BYTES_CONTACT = 1064
 DETECT_REPS = 10
 
 
-def detect_timing():
-    """Host call time of b2dev_detect_spheres (SPHERES.detect) on 1M spheres:
+def detect_timing(grid=DETECT_GRID):
+    """Host call time of b2dev_detect_spheres (SPHERES.detect) on grid^3 spheres:
     the first call detects every contact, the timed calls (after 3 warm-up
     calls) update them all (same bodies); each call includes its three host
     synchronisations (pair count, contact count, completion)."""
@@ -316,7 +320,7 @@ def detect_timing():
     from solfec_b200 import LOCDYN, scenes
     from solfec_b200.detect import SPHERES, bodies_only
     from solfec_b200.dynamics import RIGID_DYNAMICS
-    sc = scenes.spheres_grid(DETECT_GRID)
+    sc = scenes.spheres_grid(grid)
     sp = scenes.sphere_shapes(sc, friction=0.3)
     J, mass = scenes.sphere_inertia(sc)
     ldy = LOCDYN()
@@ -339,7 +343,7 @@ def detect_timing():
         ms = float(np.median(ts)) * 1e3
         nb = DETECT_BYTES_SPHERE * s.nsph + DETECT_BYTES_CONTACT * s.ncon
         peak = _peaks()[0]
-        return {'workload': 'spheres-grid-%d: %d^3 spheres, pitch 0.0999, radius 0.05' % (s.nsph, DETECT_GRID),
+        return {'workload': 'spheres-grid-%d: %d^3 spheres, pitch 0.0999, radius 0.05' % (s.nsph, grid),
                 'spheres': s.nsph, 'contacts': int(s.ncon), 'new_first_call': int(nn),
                 'first_call_ms': round(first * 1e3, 3), 'update_call_ms': round(ms, 3),
                 'contacts_per_s': round(s.ncon / (ms * 1e-3), 1), 'bytes_per_call': int(nb),
@@ -612,7 +616,8 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--scene', default=None, help='NXxNYxNZ lattice of a smaller case (profiling)')
     ap.add_argument('--maxiter', type=int, default=None, help='iteration cap of a smaller case (profiling)')
-    ap.add_argument('--workload', default='hexahedra', choices=['hexahedra', 'batched'])
+    ap.add_argument('--workload', default='hexahedra', choices=['hexahedra', 'batched', 'detect'])
+    ap.add_argument('--detect-grid', type=int, default=DETECT_GRID, help='spheres per grid side (--workload detect)')
     args = ap.parse_args()
     global WORKLOAD
     if args.scene:
@@ -631,6 +636,15 @@ def main():
         import datetime
         torch.cuda.set_device(local)
         torch.distributed.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    if args.workload == 'detect':  # sphere contact detection alone (profiling)
+        torch.cuda.set_device(local)
+        d = detect_timing(args.detect_grid)
+        if rank == 0:
+            print(json.dumps(dict(d, metric='sphere contact update call time', impl='product')), flush=True)
+        if ws > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return
     if args.workload == 'batched':
         out = bench_batched(args, ws, rank, local)
         if rank == 0:

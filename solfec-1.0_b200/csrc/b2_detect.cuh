@@ -134,15 +134,27 @@ __device__ __forceinline__ unsigned int cell_hash(int x, int y, int z, unsigned 
 __global__ void k_sph_centres(SphereDev s, const double* rot, const double* xb, const double* x0,
                               unsigned long long* rmax_bits, int* bad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.nsph) return;
-  const int b = s.body[i];
-  if (b < 0 || b >= s.nbod) { atomicOr(bad, 16); return; }
-  double c[3];
-  cur_point(rot + 9 * (size_t)b, xb + 3 * (size_t)b, x0 + 3 * (size_t)b, s.ref + 3 * (size_t)i, c);
-  s.cur[3 * (size_t)i] = c[0]; s.cur[3 * (size_t)i + 1] = c[1]; s.cur[3 * (size_t)i + 2] = c[2];
-  const double r = s.rad[i];
-  if (!(r > 0.0) || !isfinite(r) || !isfinite(c[0]) || !isfinite(c[1]) || !isfinite(c[2])) { atomicOr(bad, 1); return; }
-  atomicMax(rmax_bits, (unsigned long long)__double_as_longlong(r));  // positive doubles order as integers
+  unsigned long long rb = 0;  // this thread's radius bits (positive doubles order as integers)
+  if (i < s.nsph) {
+    const int b = s.body[i];
+    if (b < 0 || b >= s.nbod) {
+      atomicOr(bad, 16);
+    } else {
+      double c[3];
+      cur_point(rot + 9 * (size_t)b, xb + 3 * (size_t)b, x0 + 3 * (size_t)b, s.ref + 3 * (size_t)i, c);
+      s.cur[3 * (size_t)i] = c[0]; s.cur[3 * (size_t)i + 1] = c[1]; s.cur[3 * (size_t)i + 2] = c[2];
+      const double r = s.rad[i];
+      if (!(r > 0.0) || !isfinite(r) || !isfinite(c[0]) || !isfinite(c[1]) || !isfinite(c[2])) atomicOr(bad, 1);
+      else rb = (unsigned long long)__double_as_longlong(r);
+    }
+  }
+  // the largest radius: a warp maximum, then one atomic per warp (every lane
+  // of the warp reaches the shuffles: the block size is a multiple of 32)
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long v = __shfl_xor_sync(0xffffffffu, rb, o);
+    rb = v > rb ? v : rb;
+  }
+  if ((threadIdx.x & 31) == 0 && rb) atomicMax(rmax_bits, rb);
 }
 
 __global__ void k_sph_cells(SphereDev s, const unsigned long long* rmax_bits, unsigned int mask, int* sidx,
