@@ -299,14 +299,15 @@ RIGID_CPU_SAMPLE = 2000
 # per sphere 520 B (current centre from the body: body index, referential
 # centre, radius, rotation, mass centres, written centre; grid cell and bucket;
 # one radix-sort pass over key and index; the sphere's own data in the count
-# and write passes; pair count and offset), per contact 1064 B (pair indices
+# and write passes; pair count and offset), per contact 512 B (pair indices
 # written, ordered and read; the matched previous contact with its R and U; the
 # two spheres' centres, radii, bodies and surfaces; the 272-byte contact record
-# written, read back by the sparsification and the compaction and written
-# again; the body lists).
+# written once; the sparsification's reads of bodies, flag and point; the body
+# lists). A compaction copy, needed only when the sparsification removes
+# contacts, is not counted.
 DETECT_GRID = 100
 DETECT_BYTES_SPHERE = 520
-DETECT_BYTES_CONTACT = 1064
+DETECT_BYTES_CONTACT = 512
 DETECT_REPS = 10
 
 

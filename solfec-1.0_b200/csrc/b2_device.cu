@@ -1342,33 +1342,45 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     nkeep = lastpos + lastkeep;
   }
 
-  // the kept contacts become the scene's contacts
+  // the kept contacts become the scene's contacts: when nothing was removed
+  // (the common case) the staged arrays are taken over as they are, else the
+  // kept ones are compacted into the scene's arrays
   const size_t nk1 = (size_t)nkeep + 1;
-  B2_TRY(ensure(c->master, sizeof(int) * nk1));
-  B2_TRY(ensure(c->slave, sizeof(int) * nk1));
-  B2_TRY(ensure(c->mpnt, sizeof(double) * 3 * nk1));
-  B2_TRY(ensure(c->spnt, sizeof(double) * 3 * nk1));
-  B2_TRY(ensure(c->base, sizeof(double) * 9 * nk1));
-  B2_TRY(ensure(c->gap_c, sizeof(double) * nk1));
-  B2_TRY(ensure(c->fric_c, sizeof(double) * nk1));
-  B2_TRY(ensure(c->rest_c, sizeof(double) * nk1));
-  B2_TRY(ensure(c->coh_c, sizeof(double) * nk1));
-  B2_TRY(ensure(c->det_point, sizeof(double) * 3 * nk1));
-  B2_TRY(ensure(c->det_R0, sizeof(double) * 3 * nk1));
-  B2_TRY(ensure(c->det_U0, sizeof(double) * 3 * nk1));
-  B2_TRY(ensure(c->det_key, sizeof(long long) * nk1));
-  B2_TRY(ensure(c->det_slo, sizeof(int) * nk1));
-  B2_TRY(ensure(c->det_new, sizeof(int) * nk1));
-  if (npair > 0) {
-    ContactOut d;
-    d.master = ptr<int>(c->master); d.slave = ptr<int>(c->slave); d.point = ptr<double>(c->det_point);
-    d.mpnt = ptr<double>(c->mpnt); d.spnt = ptr<double>(c->spnt); d.base = ptr<double>(c->base);
-    d.gap = ptr<double>(c->gap_c); d.fric = ptr<double>(c->fric_c); d.rest = ptr<double>(c->rest_c);
-    d.coh = ptr<double>(c->coh_c); d.R0 = ptr<double>(c->det_R0); d.U0 = ptr<double>(c->det_U0);
-    d.key = ptr<long long>(c->det_key); d.slave_lo = ptr<int>(c->det_slo); d.isnew = ptr<int>(c->det_new);
-    c->launches++;
-    k_sph_compact<<<blocks_for(npair, T), T, 0, st>>>(npair, ptr<int>(c->sph_keep), ptr<int>(c->sph_pos), so, d);
-    // new contacts kept
+  if (npair > 0 && nkeep == npair) {
+    std::swap(c->master, c->st_master); std::swap(c->slave, c->st_slave); std::swap(c->det_point, c->st_point);
+    std::swap(c->mpnt, c->st_mpnt); std::swap(c->spnt, c->st_spnt); std::swap(c->base, c->st_base);
+    std::swap(c->gap_c, c->st_gap); std::swap(c->fric_c, c->st_fric); std::swap(c->rest_c, c->st_rest);
+    std::swap(c->coh_c, c->st_coh); std::swap(c->det_R0, c->st_R0); std::swap(c->det_U0, c->st_U0);
+    std::swap(c->det_key, c->st_key); std::swap(c->det_slo, c->st_slo); std::swap(c->det_new, c->st_new);
+  } else {
+    B2_TRY(ensure(c->master, sizeof(int) * nk1));
+    B2_TRY(ensure(c->slave, sizeof(int) * nk1));
+    B2_TRY(ensure(c->mpnt, sizeof(double) * 3 * nk1));
+    B2_TRY(ensure(c->spnt, sizeof(double) * 3 * nk1));
+    B2_TRY(ensure(c->base, sizeof(double) * 9 * nk1));
+    B2_TRY(ensure(c->gap_c, sizeof(double) * nk1));
+    B2_TRY(ensure(c->fric_c, sizeof(double) * nk1));
+    B2_TRY(ensure(c->rest_c, sizeof(double) * nk1));
+    B2_TRY(ensure(c->coh_c, sizeof(double) * nk1));
+    B2_TRY(ensure(c->det_point, sizeof(double) * 3 * nk1));
+    B2_TRY(ensure(c->det_R0, sizeof(double) * 3 * nk1));
+    B2_TRY(ensure(c->det_U0, sizeof(double) * 3 * nk1));
+    B2_TRY(ensure(c->det_key, sizeof(long long) * nk1));
+    B2_TRY(ensure(c->det_slo, sizeof(int) * nk1));
+    B2_TRY(ensure(c->det_new, sizeof(int) * nk1));
+    if (npair > 0) {
+      ContactOut d;
+      d.master = ptr<int>(c->master); d.slave = ptr<int>(c->slave); d.point = ptr<double>(c->det_point);
+      d.mpnt = ptr<double>(c->mpnt); d.spnt = ptr<double>(c->spnt); d.base = ptr<double>(c->base);
+      d.gap = ptr<double>(c->gap_c); d.fric = ptr<double>(c->fric_c); d.rest = ptr<double>(c->rest_c);
+      d.coh = ptr<double>(c->coh_c); d.R0 = ptr<double>(c->det_R0); d.U0 = ptr<double>(c->det_U0);
+      d.key = ptr<long long>(c->det_key); d.slave_lo = ptr<int>(c->det_slo); d.isnew = ptr<int>(c->det_new);
+      c->launches++;
+      k_sph_compact<<<blocks_for(npair, T), T, 0, st>>>(npair, ptr<int>(c->sph_keep), ptr<int>(c->sph_pos), so,
+                                                         d);
+    }
+  }
+  if (npair > 0) {  // new contacts kept
     B2_TRY(ensure(c->sph_cnt, sizeof(int) * nk1));
     size_t bytes = 0;
     B2_CK(cub::DeviceReduce::Sum(nullptr, bytes, ptr<int>(c->det_new), ptr<int>(c->sph_cnt), nkeep, st));

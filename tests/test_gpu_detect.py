@@ -148,3 +148,22 @@ def test_detect_errors_reported():
     s = SPHERES(ldy, **sp)
     assert s.detect() == (1, 1)
     ldy.close()
+
+
+def test_sparsified_contacts_match_oracle():
+    """Sphere 0 touches spheres 1 and 2, whose centres lie 1e-7 apart: the two
+    contact points are duplicates and the earlier new contact is removed
+    (the compaction path; without removals the staged arrays are taken over)."""
+    sc, sp, J, mass = scenes.spheres_on_bed(seed=7, n_side=2, layers=1)
+    x = sc.x.copy()
+    x[1] = x[0] + np.array([0.099, 0.0, 0.0])
+    x[2] = x[1] + np.array([1e-7, 0.0, 0.0])
+    sc = dataclasses.replace(sc, x=x, x0=x.copy())
+    sp = dict(sp, centre=x.copy())
+    ldy = _setup(sc, J, mass)
+    s = SPHERES(ldy, **sp)
+    assert s.detect() == (2, 2)
+    dev = s.contacts()
+    assert dev['key'].tolist() == [(0 << 32) | 2, (1 << 32) | 2]
+    _same(dev, _oracle(sp, sc.rot, sc.x, sc.x0, sc.obstacle))
+    ldy.close()
