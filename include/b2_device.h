@@ -136,6 +136,16 @@ int b2dev_rigid_get(b2dev_ctx* ctx, double* rot, double* x, double* velo, double
 int b2dev_spheres_setup(b2dev_ctx* ctx, int nsph, const int* body, const double* centre, const double* radius,
                         const int* surface, int nsurf, const double* material, int on_device);
 int b2dev_detect_spheres(b2dev_ctx* ctx, int* ncon, int* nnew);
+/* Convex obstacles (and other convex shapes) the spheres collide with
+ * (detect_convex_sphere, goc.c:308-349; the convex is the slave): per convex c
+ * its body, referential vertices vert[3 (vptr[c] .. vptr[c+1]-1)], faces
+ * fac[fptr[c] ..] (per face its vertex count, then indices into the convex's
+ * vertices, counter-clockwise seen from outside) and a surface id per face
+ * surf[sptr[c] .. sptr[c+1]-1] (-INT_MAX marks internal faces, as MESH_Convex
+ * does). A sphere i and a convex c form the pair key i << 32 | (nsph + c).
+ * Host memory; validated here. nconv = 0 removes them. */
+int b2dev_convexes_setup(b2dev_ctx* ctx, int nconv, const int* body, const int* vptr, const double* vert,
+                         const int* fptr, const int* fac, const int* sptr, const int* surf);
 int b2dev_detect_carry_state(b2dev_ctx* ctx);
 int b2dev_get_contacts(b2dev_ctx* ctx, int* master, int* slave, double* point, double* mpnt, double* spnt,
                        double* base, double* gap, double* friction, double* restitution, long long* key,

@@ -120,4 +120,29 @@ int orc_detect_spheres (int nsph, const int *sbody, const double *sref, const do
                         double *spnt, double *base, double *gap, double *friction, double *restitution,
                         double *R0, double *U0, int *isnew);
 
+/* gjk_convex_point (gjk.c:510-556): distance from p to the hull of the na
+ * vertices a[3 na], nearest hull point q. */
+double orc_gjk_convex_point (const double *a, int na, const double *p, double *q);
+
+/* computeplanes (cvx.c:72-89) with CONVEX_Planes' layout (cvx.c:1412-1427):
+ * per face its unit normal and its first vertex, pla[6 nfac]. */
+void orc_convex_planes (int nfac, const int *fac, const double *cur, double *pla);
+
+/* orc_detect_spheres with convex obstacles as well: per convex c its body,
+ * referential vertices cvert[3 (cvptr[c] .. cvptr[c+1]-1)], faces fac[cfptr[c] ..]
+ * (per face its vertex count, then the convex's vertex indices) and a surface
+ * id per face csurf[csptr[c] .. csptr[c+1]-1]. A sphere i and convex c form the
+ * pair key i << 32 | (nsph + c) (detect_convex_sphere, goc.c:308-349; the
+ * convex is the slave). Returns -2 for a convex without surface faces. */
+int orc_detect (int nsph, const int *sbody, const double *sref, const double *rad, const int *surf,
+                int nconv, const int *cbody, const int *cvptr, const double *cvert, const int *cfptr, const int *fac,
+                const int *csptr, const int *csurf,
+                int nbod, const double *rot, const double *x, const double *x0, const int *obst,
+                int nsurf, const double *mat,
+                int nprev, const long long *prevkey, const int *prevslave_lo, const double *prevR,
+                const double *prevU, int cap,
+                long long *key, int *slave_lo, int *master, int *slave, double *point, double *mpnt,
+                double *spnt, double *base, double *gap, double *friction, double *restitution,
+                double *R0, double *U0, int *isnew);
+
 #endif

@@ -205,6 +205,15 @@ def _detect_sigs(lib):
     lib.orc_detect_spheres.argtypes = ([C.c_int, _ip, _dp, _dp, _ip, C.c_int, _dp, _dp, _dp, _ip, C.c_int, _dp,
                                         C.c_int, _lp, _ip, _dp, _dp, C.c_int,
                                         _lp, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip])
+    lib.orc_gjk_convex_point.restype = C.c_double
+    lib.orc_gjk_convex_point.argtypes = [_dp, C.c_int, _dp, _dp]
+    lib.orc_convex_planes.restype = None
+    lib.orc_convex_planes.argtypes = [C.c_int, _ip, _dp, _dp]
+    lib.orc_detect.restype = C.c_int
+    lib.orc_detect.argtypes = ([C.c_int, _ip, _dp, _dp, _ip, C.c_int, _ip, _ip, _dp, _ip, _ip, _ip, _ip,
+                                C.c_int, _dp, _dp, _dp, _ip, C.c_int, _dp,
+                                C.c_int, _lp, _ip, _dp, _dp, C.c_int,
+                                _lp, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip])
     lib._detect_ready = True
 
 
@@ -219,6 +228,37 @@ def gjk_sphere_sphere(a, ra, b, rb, which='oracle'):
     g = f(np.ascontiguousarray(a, dtype=np.float64), float(ra), np.ascontiguousarray(b, dtype=np.float64),
           float(rb), p, q)
     return g, p, q
+
+
+def gjk_convex_point(a, p, which='oracle'):
+    """(distance, nearest hull point) of gjk_convex_point: the restatement, or
+    the reference's gjk.c compiled into _ref (which='ref')."""
+    lib = _load(which)
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    if which == 'oracle':
+        _detect_sigs(lib)
+        f = lib.orc_gjk_convex_point
+    else:
+        f = lib.gjk_convex_point
+        f.restype = C.c_double
+        f.argtypes = [_dp, C.c_int, _dp, _dp]
+    q = np.zeros(3)
+    d = f(a, a.shape[0] // 3, np.ascontiguousarray(p, dtype=np.float64), q)
+    return d, q
+
+
+def convex_planes(fac, cur):
+    """computeplanes: (nfac, 6) unit normal and first vertex per face."""
+    lib = _load('oracle')
+    _detect_sigs(lib)
+    fac = np.ascontiguousarray(fac, dtype=np.int32)
+    nf, m = 0, 0
+    while m < fac.shape[0]:
+        nf += 1
+        m += fac[m] + 1
+    pla = np.zeros((max(nf, 1), 6))
+    lib.orc_convex_planes(nf, fac, np.ascontiguousarray(cur, dtype=np.float64).reshape(-1), pla)
+    return pla[:nf]
 
 
 def localbase(n):
@@ -241,7 +281,7 @@ def sphere_centres(sbody, sref, rot, x, x0):
     return cur
 
 
-def detect_spheres(sbody, sref, radius, surface, rot, x, x0, obstacle, material, prev=None):
+def detect_spheres(sbody, sref, radius, surface, rot, x, x0, obstacle, material, prev=None, convex=None):
     """The contact part of DOM_Update_Begin for spheres (oracle_detect.c).
     material: (nsurf, nsurf, 2) friction, restitution. prev: None or a dict
     returned by an earlier call, with 'R' and 'U' set to the reactions and
@@ -267,22 +307,35 @@ def detect_spheres(sbody, sref, radius, surface, rot, x, x0, obstacle, material,
         if npv == 0:
             pk, ps, pR, pU = np.zeros(1, np.int64), np.zeros(1, np.int32), np.zeros(3), np.zeros(3)
 
+    if convex is not None:
+        cb = i32(convex['body'])
+        cvptr, cvert = i32(convex['vptr']), f64(convex['vert'])
+        cfptr, fac = i32(convex['fptr']), i32(convex['fac'])
+        csptr, csurf = i32(convex['sptr']), i32(convex['surf'])
+        nconv = cb.shape[0]
+    else:
+        nconv = 0
+        cb, cvptr, cfptr, csptr = (np.zeros(1, np.int32) for _ in range(4))
+        cvert, fac, csurf = np.zeros(3), np.zeros(1, np.int32), np.zeros(1, np.int32)
+
     def run(cap):
         c1 = max(cap, 1)
         out = dict(key=np.zeros(c1, np.int64), slave_lo=np.zeros(c1, np.int32), master=np.zeros(c1, np.int32),
                    slave=np.zeros(c1, np.int32), point=np.zeros((c1, 3)), mpnt=np.zeros((c1, 3)),
                    spnt=np.zeros((c1, 3)), base=np.zeros((c1, 9)), gap=np.zeros(c1), friction=np.zeros(c1),
                    restitution=np.zeros(c1), R=np.zeros((c1, 3)), U=np.zeros((c1, 3)), isnew=np.zeros(c1, np.int32))
-        n = lib.orc_detect_spheres(nsph, sbody, sref, radius, surface, nbod, rot, x, x0, obstacle, nsurf, mat,
-                                   npv, pk, ps, pR, pU, cap,
+        n = lib.orc_detect(nsph, sbody, sref, radius, surface, nconv, cb, cvptr, cvert, cfptr, fac, csptr, csurf,
+                           nbod, rot, x, x0, obstacle, nsurf, mat, npv, pk, ps, pR, pU, cap,
                                    out['key'], out['slave_lo'], out['master'], out['slave'], out['point'],
                                    out['mpnt'], out['spnt'], out['base'], out['gap'], out['friction'],
                                    out['restitution'], out['R'], out['U'], out['isnew'])
         return n, out
 
     n, out = run(8 * nsph + 16)
-    if n < 0:
+    if n == -1:
         raise ValueError('coincident sphere centres')
+    if n < 0:
+        raise ValueError('a convex without surface faces')
     if n > 8 * nsph + 16:
         n, out = run(n)
     return {k: v[:n] for k, v in out.items()}

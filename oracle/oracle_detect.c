@@ -38,6 +38,8 @@
  * gjk_sphere_sphere here is checked bit for bit against the reference's own
  * gjk.c, compiled into oracle/_ref.
  */
+#include <float.h>
+#include <limits.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -67,6 +69,180 @@ double orc_gjk_sphere_sphere (const double *a, double ra, const double *b, doubl
   for (int k = 0; k < 3; k++) p[k] = .5 * (p[k] + q[k]);
   memcpy (q, p, sizeof (double) * 3);
   return 0.0;
+}
+
+/* ---- convex polyhedra: GJK distance to a point (gjk.c:510-556) with Johnson's
+ * sub-algorithm as gjk.c:213-330 evaluates it: the sub-simplices of the current
+ * simplex are tried in a fixed order (singletons, pairs, triples, the whole) and
+ * the first whose barycentric weights (delta) are positive on its members and
+ * non-positive off them gives the projection of the origin. */
+
+typedef struct { double w[3]; const double *a; } simplex_pt;
+
+/* sub-simplex masks in the order they are tried (bit i = simplex vertex i) and
+ * how many of them a simplex of n vertices tries */
+static const int sub_mask[15] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 11, 13, 14, 15};
+static const int sub_count[5] = {0, 0, 3, 7, 15};
+
+static int popcount4 (int s) { return (s & 1) + ((s >> 1) & 1) + ((s >> 2) & 1) + ((s >> 3) & 1); }
+
+static int johnson (simplex_pt *w, int n, double *l, double *v)
+{
+  double dot[4][4], delta[16][4], sum;
+  if (n == 1)
+  {
+    l[0] = 1.0;
+    v[0] = w[0].w[0]; v[1] = w[0].w[1]; v[2] = w[0].w[2];
+    return 1;
+  }
+  for (int i = 0; i < n; i++)
+    for (int j = i; j < n; j++)
+    {
+      dot[i][j] = w[i].w[0] * w[j].w[0] + w[i].w[1] * w[j].w[1] + w[i].w[2] * w[j].w[2];
+      dot[j][i] = dot[i][j];
+    }
+  for (int m = 0; m < sub_count[n]; m++)
+  {
+    const int s = sub_mask[m];
+    int ok = 1, k = -1;
+    if (popcount4 (s) == 1)
+    {
+      for (int i = 0; i < n; i++) if (s & (1 << i)) { delta[s][i] = 1.0; k = i; break; }
+      for (int j = 0; j < n; j++)
+        if (!(s & (1 << j)))
+        {
+          delta[s][j] = dot[k][k] - dot[k][j];
+          if (delta[s][j] > 0.0) ok = 0;
+        }
+    }
+    else
+    {
+      for (int i = 0; i < n; i++)
+        if (s & (1 << i))
+        {
+          if (k < 0) k = i;
+          delta[s][i] = delta[s & ~(1 << i)][i];
+          if (delta[s][i] <= 0.0) ok = 0;
+        }
+      for (int j = 0; j < n; j++)
+        if (!(s & (1 << j)))
+        {
+          delta[s][j] = 0.0;
+          for (int i = 0; i < n; i++)
+            if (s & (1 << i)) delta[s][j] += delta[s][i] * (dot[i][k] - dot[i][j]);
+          if (delta[s][j] > 0.0) ok = 0;
+        }
+    }
+    if (ok)
+    {
+      int o = 0;
+      sum = 0.0;
+      for (int i = 0; i < n; i++)
+        if (s & (1 << i))
+        {
+          w[o] = w[i];
+          l[o] = delta[s][i];
+          sum += l[o];
+          o++;
+        }
+      v[0] = v[1] = v[2] = 0.0;
+      for (int i = 0; i < o; i++)
+      {
+        l[i] /= sum;
+        for (int c = 0; c < 3; c++) v[c] = v[c] + l[i] * w[i].w[c];
+      }
+      return o;
+    }
+  }
+  return 0;
+}
+
+/* gjk_convex_point (gjk.c:510-556): distance from point p to the hull of the
+ * na vertices a, and the nearest hull point q */
+double orc_gjk_convex_point (const double *a, int na, const double *p, double *q)
+{
+  simplex_pt w[4];
+  double v[3], vlen, delta, mi = 0.0, l[4];
+  int toofar = 1, n = 0, j = 0;
+  const int k = 4 * na * na;
+  v[0] = a[0] - p[0]; v[1] = a[1] - p[1]; v[2] = a[2] - p[2];
+  vlen = sqrt (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  while (toofar && vlen > GEPS && n < 4 && j++ < k)
+  {
+    double dmin = DBL_MAX;
+    const double *best = NULL;
+    for (int t = 0; t < na; t++)
+    {
+      const double *c = a + 3 * t;
+      const double d = c[0] * v[0] + c[1] * v[1] + c[2] * v[2];
+      if (d < dmin) { dmin = d; best = c; }
+    }
+    w[n].a = best;
+    w[n].w[0] = best[0] - p[0]; w[n].w[1] = best[1] - p[1]; w[n].w[2] = best[2] - p[2];
+    delta = (v[0] * w[n].w[0] + v[1] * w[n].w[1] + v[2] * w[n].w[2]) / vlen;
+    mi = mi > delta ? mi : delta;
+    toofar = (vlen - mi) > GEPS;
+    if (toofar)
+    {
+      n = johnson (w, n + 1, l, v);
+      vlen = sqrt (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    }
+  }
+  if (n)
+  {
+    q[0] = q[1] = q[2] = 0.0;
+    for (n--; n >= 0; n--)
+      for (int c = 0; c < 3; c++) q[c] = q[c] + l[n] * w[n].a[c];
+  }
+  else { q[0] = a[0]; q[1] = a[1]; q[2] = a[2]; }
+  return vlen;
+}
+
+/* computeplanes (cvx.c:72-89): per face the unit normal of (b - a) x (c - b)
+ * over its first three vertices, and a point of the face (its first vertex,
+ * as CONVEX_Planes, cvx.c:1412-1427, lists it); fac = per face its vertex
+ * count then its vertex indices */
+void orc_convex_planes (int nfac, const int *fac, const double *cur, double *pla)
+{
+  for (int f = 0, m = 0; f < nfac; f++, m += fac[m] + 1)
+  {
+    const double *a = cur + 3 * fac[m + 1], *b = cur + 3 * fac[m + 2], *c = cur + 3 * fac[m + 3];
+    double ba[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, cb[3] = {c[0] - b[0], c[1] - b[1], c[2] - b[2]};
+    double *nl = pla + 6 * f, len;
+    nl[0] = ba[1] * cb[2] - ba[2] * cb[1];
+    nl[1] = ba[2] * cb[0] - ba[0] * cb[2];
+    nl[2] = ba[0] * cb[1] - ba[1] * cb[0];
+    len = sqrt (nl[0] * nl[0] + nl[1] * nl[1] + nl[2] * nl[2]);
+    nl[0] /= len; nl[1] /= len; nl[2] /= len;
+    nl[3] = a[0]; nl[4] = a[1]; nl[5] = a[2];
+  }
+}
+
+/* nearest_normal and nearest_surface, goc.c:87-122 */
+static const double *nearest_normal (const double *pnt, const double *pla, int n)
+{
+  double max = -DBL_MAX;
+  const double *ret = NULL;
+  for (; n > 0; n--, pla += 6)
+  {
+    const double v[3] = {pnt[0] - pla[3], pnt[1] - pla[4], pnt[2] - pla[5]};
+    const double d = pla[0] * v[0] + pla[1] * v[1] + pla[2] * v[2];
+    if (d > max) { ret = pla; max = d; }
+  }
+  return ret;
+}
+
+static int nearest_surface (const double *pnt, const double *pla, const int *sur, int n)
+{
+  double min = DBL_MAX;
+  int ret = sur[0];
+  for (; n > 0; n--, pla += 6, sur++)
+  {
+    const double v[3] = {pnt[0] - pla[3], pnt[1] - pla[4], pnt[2] - pla[5]};
+    const double d = pla[0] * v[0] + pla[1] * v[1] + pla[2] * v[2];
+    if (fabs (d) < min) { min = fabs (d); ret = *sur; }
+  }
+  return ret;
 }
 
 /* localbase, dom.c:133-151: the normal as the third column, the first column
@@ -160,14 +336,27 @@ static int paircmp (const void *a, const void *b)
   return x->j - y->j;
 }
 
-int orc_detect_spheres (int nsph, const int *sbody, const double *sref, const double *rad, const int *surf,
-                        int nbod, const double *rot, const double *x, const double *x0, const int *obst,
-                        int nsurf, const double *mat,
-                        int nprev, const long long *prevkey, const int *prevslave_lo, const double *prevR,
-                        const double *prevU, int cap,
-                        long long *key, int *slave_lo, int *master, int *slave, double *point, double *mpnt,
-                        double *spnt, double *base, double *gap, double *friction, double *restitution,
-                        double *R0, double *U0, int *isnew)
+/* convex obstacles of orc_detect: per convex its body, vertices cvert[3 *
+ * (cvptr[c] .. cvptr[c+1]-1)] in the body's referential frame, faces
+ * fac[cfptr[c] ..] (per face its vertex count, then indices into the convex's
+ * vertices) and a surface id per face csurf[csptr[c] .. csptr[c+1]-1] */
+typedef struct
+{
+  int n;
+  const int *body, *vptr, *fptr, *fac, *sptr, *surf;
+  const double *vert;
+  double *cur, *pla;   /* current vertices and planes (6 per face) */
+} convexes;
+
+static int detect_all (int nsph, const int *sbody, const double *sref, const double *rad, const int *surf,
+                       convexes *cv,
+                       int nbod, const double *rot, const double *x, const double *x0, const int *obst,
+                       int nsurf, const double *mat,
+                       int nprev, const long long *prevkey, const int *prevslave_lo, const double *prevR,
+                       const double *prevU, int cap,
+                       long long *key, int *slave_lo, int *master, int *slave, double *point, double *mpnt,
+                       double *spnt, double *base, double *gap, double *friction, double *restitution,
+                       double *R0, double *U0, int *isnew)
 {
   double *cur = malloc (sizeof (double) * 3 * (size_t) (nsph + 1));
   sweeprec *sw = malloc (sizeof (sweeprec) * (size_t) (nsph + 1));
@@ -205,6 +394,24 @@ int orc_detect_spheres (int nsph, const int *sbody, const double *sref, const do
       }
     }
   }
+  /* sphere-convex pairs: every pair tested (the candidate boxes of the
+   * reference overlap for every pair the distance test accepts) */
+  for (int c = 0; c < cv->n; c++)
+  {
+    const int nv = cv->vptr[c + 1] - cv->vptr[c], bc = cv->body[c];
+    const double *vc = cv->cur + 3 * (size_t) cv->vptr[c];
+    for (int i = 0; i < nsph; i++)
+    {
+      double q[3];
+      if (sbody[i] == bc) continue;
+      if (obst[sbody[i]] && obst[bc]) continue;
+      if (orc_gjk_convex_point (vc, nv, cur + 3 * i, q) < rad[i] + GEPS)
+      {
+        if (np == pcap) { pcap *= 2; pairs = realloc (pairs, sizeof (pairrec) * pcap); }
+        pairs[np].i = i; pairs[np].j = nsph + c; np++;
+      }
+    }
+  }
   qsort (pairs, np, sizeof (pairrec), paircmp);
 
   /* contacts in pair order */
@@ -230,6 +437,58 @@ int orc_detect_spheres (int nsph, const int *sbody, const double *sref, const do
       double p[3], q[3], nrm[3], len;
       probe.key = ((long long) i << 32) | (long long) j;
       hit = nprev ? bsearch (&probe, pv, nprev, sizeof (prevrec), prevcmp) : NULL;
+      if (j >= nsph)
+      {
+        /* detect_convex_sphere / update_convex_sphere (goc.c:308-349, 555-597):
+         * the convex is the slave (its outward normal), the sphere the master */
+        const int cx = j - nsph, bc = cv->body[cx], bi = sbody[i];
+        const int nv = cv->vptr[cx + 1] - cv->vptr[cx], nf = cv->sptr[cx + 1] - cv->sptr[cx];
+        const double *vc = cv->cur + 3 * (size_t) cv->vptr[cx], *pla = cv->pla + 6 * (size_t) cv->sptr[cx];
+        const int *fs = cv->surf + cv->sptr[cx];
+        const double *cc = cur + 3 * i;
+        double one[3], two[3], dot, ln;
+        int ns = 0;
+        while (ns < nf && fs[ns] != -INT_MAX) ns++;
+        orc_gjk_convex_point (vc, nv, cc, one);
+        nrm[0] = cc[0] - one[0]; nrm[1] = cc[1] - one[1]; nrm[2] = cc[2] - one[2];
+        dot = nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2];
+        if (dot == 0.0)
+        {
+          const double *nn = nearest_normal (one, pla, ns);
+          ln = rad[i];
+          if (!nn) { ret = -2; break; }
+          nrm[0] = nn[0]; nrm[1] = nn[1]; nrm[2] = nn[2];
+        }
+        else
+        {
+          const double il = 1.0 / (ln = sqrt (dot));
+          nrm[0] *= il; nrm[1] *= il; nrm[2] *= il;
+        }
+        for (int v = 0; v < 3; v++) two[v] = cc[v] + (-rad[i]) * nrm[v];
+        k_[c] = probe.key;
+        sl_[c] = 0;
+        ms_[c] = bi;
+        sv_[c] = bc;
+        nw_[c] = hit == NULL;
+        dot = ln - rad[i];
+        gp_[c] = dot < 0.0 ? dot : 0.0;
+        memcpy (pt_ + 3 * c, two, sizeof (double) * 3);
+        ref_point (rot + 9 * (size_t) bi, x + 3 * (size_t) bi, x0 + 3 * (size_t) bi, two, mp_ + 3 * c);
+        ref_point (rot + 9 * (size_t) bc, x + 3 * (size_t) bc, x0 + 3 * (size_t) bc, one, sp_ + 3 * c);
+        orc_localbase (nrm, bs_ + 9 * c);
+        {
+          const int s0 = nearest_surface (one, pla, fs, ns);
+          const size_t t = (size_t) s0 * (size_t) nsurf + (size_t) surf[i];
+          fr_[c] = mat[2 * t];
+          rs_[c] = mat[2 * t + 1];
+        }
+        for (int v = 0; v < 3; v++)
+        {
+          r0_[3 * c + v] = hit ? hit->R[v] : 0.0;
+          u0_[3 * c + v] = hit ? hit->U[v] : 0.0;
+        }
+        continue;
+      }
       if (hit) lo_is_slave = hit->slave_lo;                        /* update: roles kept */
       else lo_is_slave = pntcmp (cur + 3 * i, cur + 3 * j) <= 0;   /* detection: lower centre is the slave */
       s = lo_is_slave ? i : j;
@@ -311,5 +570,55 @@ int orc_detect_spheres (int nsph, const int *sbody, const double *sref, const do
     free (pt_); free (mp_); free (sp_); free (bs_); free (gp_); free (fr_); free (rs_); free (r0_); free (u0_);
   }
   free (cur); free (sw); free (pv); free (pairs);
+  return ret;
+}
+
+int orc_detect_spheres (int nsph, const int *sbody, const double *sref, const double *rad, const int *surf,
+                        int nbod, const double *rot, const double *x, const double *x0, const int *obst,
+                        int nsurf, const double *mat,
+                        int nprev, const long long *prevkey, const int *prevslave_lo, const double *prevR,
+                        const double *prevU, int cap,
+                        long long *key, int *slave_lo, int *master, int *slave, double *point, double *mpnt,
+                        double *spnt, double *base, double *gap, double *friction, double *restitution,
+                        double *R0, double *U0, int *isnew)
+{
+  convexes none;
+  memset (&none, 0, sizeof none);
+  return detect_all (nsph, sbody, sref, rad, surf, &none, nbod, rot, x, x0, obst, nsurf, mat, nprev, prevkey,
+                     prevslave_lo, prevR, prevU, cap, key, slave_lo, master, slave, point, mpnt, spnt, base, gap,
+                     friction, restitution, R0, U0, isnew);
+}
+
+int orc_detect (int nsph, const int *sbody, const double *sref, const double *rad, const int *surf,
+                int nconv, const int *cbody, const int *cvptr, const double *cvert, const int *cfptr, const int *fac,
+                const int *csptr, const int *csurf,
+                int nbod, const double *rot, const double *x, const double *x0, const int *obst,
+                int nsurf, const double *mat,
+                int nprev, const long long *prevkey, const int *prevslave_lo, const double *prevR,
+                const double *prevU, int cap,
+                long long *key, int *slave_lo, int *master, int *slave, double *point, double *mpnt,
+                double *spnt, double *base, double *gap, double *friction, double *restitution,
+                double *R0, double *U0, int *isnew)
+{
+  convexes cv;
+  int ret;
+  cv.n = nconv; cv.body = cbody; cv.vptr = cvptr; cv.vert = cvert; cv.fptr = cfptr; cv.fac = fac;
+  cv.sptr = csptr; cv.surf = csurf;
+  cv.cur = malloc (sizeof (double) * 3 * (size_t) (nconv ? cvptr[nconv] + 1 : 1));
+  cv.pla = malloc (sizeof (double) * 6 * (size_t) (nconv ? csptr[nconv] + 1 : 1));
+  for (int c = 0; c < nconv; c++)
+  {
+    const int b = cbody[c];
+    for (int v = cvptr[c]; v < cvptr[c + 1]; v++)
+      cur_point (rot + 9 * (size_t) b, x + 3 * (size_t) b, x0 + 3 * (size_t) b, cvert + 3 * (size_t) v,
+                 cv.cur + 3 * (size_t) v);
+    orc_convex_planes (csptr[c + 1] - csptr[c], fac + cfptr[c], cv.cur + 3 * (size_t) cvptr[c],
+                       cv.pla + 6 * (size_t) csptr[c]);
+  }
+  ret = detect_all (nsph, sbody, sref, rad, surf, &cv, nbod, rot, x, x0, obst, nsurf, mat, nprev, prevkey,
+                    prevslave_lo, prevR, prevU, cap, key, slave_lo, master, slave, point, mpnt, spnt, base, gap,
+                    friction, restitution, R0, U0, isnew);
+  free (cv.cur);
+  free (cv.pla);
   return ret;
 }

@@ -6,10 +6,14 @@
 //   k_sph_cells     uniform grid cell of each centre (edge 2 r_max + 2 eps) and
 //                   its hash bucket
 //   k_sph_buckets   first and last sorted sphere of each bucket
+//   k_cvx_update    convex obstacles moved with their bodies (CONVEX_Update,
+//                   cvx.c:1362-1396): vertices, face planes, bounding box
 //   k_sph_pairs     per sphere i, the spheres j > i of the 27 surrounding cells
 //                   whose gjk_sphere_sphere gap (gjk.c:560-584) is below
-//                   GEOMETRIC_EPSILON (goc.c:431), bodies different and not
-//                   both obstacles (box.c:104-108): counted, then written
+//                   GEOMETRIC_EPSILON (goc.c:431), and the convexes whose
+//                   gjk_convex_point distance (gjk.c:510-556) is below
+//                   r + GEOMETRIC_EPSILON (goc.c:319), bodies different and
+//                   not both obstacles (box.c:104-108): counted, then written
 //   k_sph_sort_seg  the pairs of each sphere in ascending j (list order)
 //   k_sph_contacts  one contact per pair: roles kept from the previous step
 //                   (update_contact, dom.c:430-484; update_sphere_sphere,
@@ -33,6 +37,7 @@
 // oracle bit for bit.
 #pragma once
 
+#include <cfloat>
 #include <cstdint>
 
 namespace b2 {
@@ -124,13 +129,195 @@ __device__ __forceinline__ int point_cmp(const double* a, const double* b) {
   return 0;
 }
 
+// ---- convex obstacles (detect_convex_sphere, goc.c:308-349) ----
+
+struct ConvexDev {
+  int n;
+  const int* body;     // body of each convex
+  const int* vptr;     // vertices of convex c: vptr[c] .. vptr[c+1]-1
+  const double* vert;  // referential vertices [3]
+  const int* fptr;     // faces of convex c in fac[fptr[c] ..]: count, then vertex indices
+  const int* fac;
+  const int* sptr;     // faces of convex c: sptr[c] .. sptr[c+1]-1 (surface ids, planes)
+  const int* surf;
+  const int* nsurf_face;  // faces before the first internal one (surface -INT_MAX)
+  double* cur;         // current vertices [3]
+  double* pla;         // per face unit normal and first vertex [6]
+  double* box;         // per convex min[3], max[3] of the current vertices
+};
+
+// Johnson's sub-algorithm as gjk.c:213-330 evaluates it: sub-simplices tried
+// in a fixed order (singletons, pairs, triples, the whole simplex), the first
+// whose barycentric weights are positive on its members and non-positive off
+// them gives the projection of the origin. w[i] holds a Minkowski point and
+// wa[i] the index of its hull vertex.
+__device__ int johnson_project(double (*w)[3], int* wa, int n, double* l, double* v) {
+  const int sub_mask[15] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 11, 13, 14, 15};
+  const int sub_count[5] = {0, 0, 3, 7, 15};
+  double dot[4][4], delta[16][4];
+  if (n == 1) {
+    l[0] = 1.0;
+    v[0] = w[0][0]; v[1] = w[0][1]; v[2] = w[0][2];
+    return 1;
+  }
+  for (int i = 0; i < n; i++)
+    for (int j = i; j < n; j++) {
+      dot[i][j] = w[i][0] * w[j][0] + w[i][1] * w[j][1] + w[i][2] * w[j][2];
+      dot[j][i] = dot[i][j];
+    }
+  for (int m = 0; m < sub_count[n]; m++) {
+    const int s = sub_mask[m];
+    bool ok = true;
+    int k = -1;
+    if (__popc(s) == 1) {
+      for (int i = 0; i < n; i++)
+        if (s & (1 << i)) { delta[s][i] = 1.0; k = i; break; }
+      for (int j = 0; j < n; j++)
+        if (!(s & (1 << j))) {
+          delta[s][j] = dot[k][k] - dot[k][j];
+          if (delta[s][j] > 0.0) ok = false;
+        }
+    } else {
+      for (int i = 0; i < n; i++)
+        if (s & (1 << i)) {
+          if (k < 0) k = i;
+          delta[s][i] = delta[s & ~(1 << i)][i];
+          if (delta[s][i] <= 0.0) ok = false;
+        }
+      for (int j = 0; j < n; j++)
+        if (!(s & (1 << j))) {
+          delta[s][j] = 0.0;
+          for (int i = 0; i < n; i++)
+            if (s & (1 << i)) delta[s][j] += delta[s][i] * (dot[i][k] - dot[i][j]);
+          if (delta[s][j] > 0.0) ok = false;
+        }
+    }
+    if (ok) {
+      int o = 0;
+      double sum = 0.0;
+      for (int i = 0; i < n; i++)
+        if (s & (1 << i)) {
+          w[o][0] = w[i][0]; w[o][1] = w[i][1]; w[o][2] = w[i][2];
+          wa[o] = wa[i];
+          l[o] = delta[s][i];
+          sum += l[o];
+          o++;
+        }
+      v[0] = v[1] = v[2] = 0.0;
+      for (int i = 0; i < o; i++) {
+        l[i] /= sum;
+        for (int c = 0; c < 3; c++) v[c] = v[c] + l[i] * w[i][c];
+      }
+      return o;
+    }
+  }
+  return 0;
+}
+
+// gjk_convex_point, gjk.c:510-556: distance from p to the hull of the na
+// vertices a[3 na] and the nearest hull point q (an upper bound of the exact
+// distance within GEOMETRIC_EPSILON)
+__device__ double gjk_convex_point(const double* a, int na, const double* p, double* q) {
+  double w[4][3], v[3], l[4], mi = 0.0;
+  int wa[4];
+  int n = 0, j = 0;
+  bool toofar = true;
+  const int k = 4 * na * na;
+  v[0] = a[0] - p[0]; v[1] = a[1] - p[1]; v[2] = a[2] - p[2];
+  double vlen = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  while (toofar && vlen > kGeomEps && n < 4 && j++ < k) {
+    double dmin = DBL_MAX;
+    int best = 0;
+    for (int t = 0; t < na; t++) {
+      const double d = a[3 * t] * v[0] + a[3 * t + 1] * v[1] + a[3 * t + 2] * v[2];
+      if (d < dmin) { dmin = d; best = t; }
+    }
+    wa[n] = best;
+    w[n][0] = a[3 * best] - p[0]; w[n][1] = a[3 * best + 1] - p[1]; w[n][2] = a[3 * best + 2] - p[2];
+    const double delta = (v[0] * w[n][0] + v[1] * w[n][1] + v[2] * w[n][2]) / vlen;
+    mi = mi > delta ? mi : delta;
+    toofar = (vlen - mi) > kGeomEps;
+    if (toofar) {
+      n = johnson_project(w, wa, n + 1, l, v);
+      vlen = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    }
+  }
+  if (n) {
+    q[0] = q[1] = q[2] = 0.0;
+    for (n--; n >= 0; n--)
+      for (int c = 0; c < 3; c++) q[c] = q[c] + l[n] * a[3 * wa[n] + c];
+  } else {
+    q[0] = a[0]; q[1] = a[1]; q[2] = a[2];
+  }
+  return vlen;
+}
+
+// computeplanes (cvx.c:72-89) in CONVEX_Planes' layout, current vertices from
+// the body (CONVEX_Update, cvx.c:1362-1396) and the bounding box: one thread
+// per convex (obstacles and other large shapes are few)
+__global__ void k_cvx_update(ConvexDev cv, const double* rot, const double* xb, const double* x0) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cv.n) return;
+  const int b = cv.body[c];
+  double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+  for (int v = cv.vptr[c]; v < cv.vptr[c + 1]; v++) {
+    double x[3];
+    cur_point(rot + 9 * (size_t)b, xb + 3 * (size_t)b, x0 + 3 * (size_t)b, cv.vert + 3 * (size_t)v, x);
+    for (int k = 0; k < 3; k++) {
+      cv.cur[3 * (size_t)v + k] = x[k];
+      lo[k] = x[k] < lo[k] ? x[k] : lo[k];
+      hi[k] = x[k] > hi[k] ? x[k] : hi[k];
+    }
+  }
+  for (int k = 0; k < 3; k++) { cv.box[6 * c + k] = lo[k]; cv.box[6 * c + 3 + k] = hi[k]; }
+  const double* cur = cv.cur + 3 * (size_t)cv.vptr[c];
+  for (int f = cv.sptr[c], m = cv.fptr[c]; f < cv.sptr[c + 1]; f++, m += cv.fac[m] + 1) {
+    const double* a = cur + 3 * cv.fac[m + 1];
+    const double* bb = cur + 3 * cv.fac[m + 2];
+    const double* cc = cur + 3 * cv.fac[m + 3];
+    const double ba0 = bb[0] - a[0], ba1 = bb[1] - a[1], ba2 = bb[2] - a[2];
+    const double cb0 = cc[0] - bb[0], cb1 = cc[1] - bb[1], cb2 = cc[2] - bb[2];
+    double* nl = cv.pla + 6 * (size_t)f;
+    nl[0] = ba1 * cb2 - ba2 * cb1;
+    nl[1] = ba2 * cb0 - ba0 * cb2;
+    nl[2] = ba0 * cb1 - ba1 * cb0;
+    const double len = sqrt(nl[0] * nl[0] + nl[1] * nl[1] + nl[2] * nl[2]);
+    nl[0] /= len; nl[1] /= len; nl[2] /= len;
+    nl[3] = a[0]; nl[4] = a[1]; nl[5] = a[2];
+  }
+}
+
+// nearest_normal and nearest_surface, goc.c:87-122
+__device__ __forceinline__ int nearest_plane_max(const double* pnt, const double* pla, int n) {
+  double max = -DBL_MAX;
+  int ret = -1;
+  for (int f = 0; f < n; f++, pla += 6) {
+    const double v0 = pnt[0] - pla[3], v1 = pnt[1] - pla[4], v2 = pnt[2] - pla[5];
+    const double d = pla[0] * v0 + pla[1] * v1 + pla[2] * v2;
+    if (d > max) { ret = f; max = d; }
+  }
+  return ret;
+}
+
+__device__ __forceinline__ int nearest_surface_id(const double* pnt, const double* pla, const int* sur, int n) {
+  double min = DBL_MAX;
+  int ret = sur[0];
+  for (int f = 0; f < n; f++, pla += 6) {
+    const double v0 = pnt[0] - pla[3], v1 = pnt[1] - pla[4], v2 = pnt[2] - pla[5];
+    const double d = pla[0] * v0 + pla[1] * v1 + pla[2] * v2;
+    if (fabs(d) < min) { min = fabs(d); ret = sur[f]; }
+  }
+  return ret;
+}
+
 __device__ __forceinline__ unsigned int cell_hash(int x, int y, int z, unsigned int mask) {
   return (((unsigned int)x * 73856093u) ^ ((unsigned int)y * 19349663u) ^ ((unsigned int)z * 83492791u)) & mask;
 }
 
 // bad flags (bit or): 1 a radius not positive and finite or a centre not finite,
 // 2 a centre too far from the origin for the grid, 4 two coincident centres,
-// 8 a surface id out of range, 16 a body index out of range
+// 8 a surface id out of range, 16 a body index out of range, 32 a convex
+// without a finite face plane
 __global__ void k_sph_centres(SphereDev s, const double* rot, const double* xb, const double* x0,
                               unsigned long long* rmax_bits, int* bad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -219,6 +406,44 @@ __global__ void k_sph_pairs(SphereDev s, const int* obst, const int* sorted, con
   if (!WRITE) count[i] = cnt;
 }
 
+// convex partners of sphere i (pair index nsph + c): a box test first (the
+// distance test accepts only spheres within r + eps of the hull), then the
+// gjk_convex_point distance. WRITE = false: ccount[i]; WRITE = true: written
+// after the sphere's sphere partners, at off[i] + scount[i]
+template <bool WRITE>
+__global__ void k_cvx_pairs(SphereDev s, ConvexDev cv, const int* obst, int* ccount, const int* off,
+                            const int* scount, int* pj) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.nsph) return;
+  const int bi = s.body[i];
+  if (bi < 0 || bi >= s.nbod) return;  // reported by k_sph_centres
+  const bool oi = obst[bi] != 0;
+  const double a[3] = {s.cur[3 * (size_t)i], s.cur[3 * (size_t)i + 1], s.cur[3 * (size_t)i + 2]};
+  const double ra = s.rad[i];
+  int cnt = 0;
+  int w = WRITE ? off[i] + scount[i] : 0;
+  for (int c = 0; c < cv.n; c++) {
+    const int bc = cv.body[c];
+    if (bc == bi || (oi && obst[bc])) continue;
+    const double* bx = cv.box + 6 * (size_t)c;
+    bool near = true;
+    for (int k = 0; k < 3; k++)
+      if (a[k] < bx[k] - ra - 2.0 * kGeomEps || a[k] > bx[3 + k] + ra + 2.0 * kGeomEps) near = false;
+    if (!near) continue;
+    double q[3];
+    if (gjk_convex_point(cv.cur + 3 * (size_t)cv.vptr[c], cv.vptr[c + 1] - cv.vptr[c], a, q) < ra + kGeomEps) {
+      if (WRITE) pj[w++] = s.nsph + c;
+      cnt++;
+    }
+  }
+  if (!WRITE) ccount[i] = cnt;
+}
+
+__global__ void k_add_counts(int n, const int* a, int* b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] += a[i];
+}
+
 __global__ void k_sph_sort_seg(int nsph, const int* off, int* pj, int* pi) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsph) return;
@@ -237,7 +462,7 @@ struct ContactOut {
   double* fric; double* rest; double* coh; double* R0; double* U0; long long* key; int* slave_lo; int* isnew;
 };
 
-__global__ void k_sph_contacts(int npair, SphereDev s, const int* pi, const int* pj, const double* rot,
+__global__ void k_sph_contacts(int npair, SphereDev s, ConvexDev cv, const int* pi, const int* pj, const double* rot,
                                const double* xb, const double* x0, int nsurf, const double* mat, int nprev,
                                const long long* prevkey, const int* prevslave_lo, const double* prevR,
                                const double* prevU, ContactOut o, int* bad) {
@@ -254,6 +479,63 @@ __global__ void k_sph_contacts(int npair, SphereDev s, const int* pi, const int*
       if (v == key) { hit = mid; break; }
       if (v < key) lo = mid + 1; else hi = mid - 1;
     }
+  }
+  if (j >= s.nsph) {
+    // detect_convex_sphere / update_convex_sphere (goc.c:308-349, 555-597):
+    // the convex is the slave (its outward normal), the sphere the master
+    const int c = j - s.nsph, bc = cv.body[c], bi = s.body[i];
+    o.master[k] = bi;
+    o.slave[k] = bc;
+    o.key[k] = key;
+    o.slave_lo[k] = 0;
+    o.isnew[k] = hit < 0;
+    const double* cc = s.cur + 3 * (size_t)i;
+    const double r = s.rad[i];
+    const double* pla = cv.pla + 6 * (size_t)cv.sptr[c];
+    const int* fs = cv.surf + cv.sptr[c];
+    const int ns = cv.nsurf_face[c];
+    double one[3], n[3], len;
+    gjk_convex_point(cv.cur + 3 * (size_t)cv.vptr[c], cv.vptr[c + 1] - cv.vptr[c], cc, one);
+    n[0] = cc[0] - one[0]; n[1] = cc[1] - one[1]; n[2] = cc[2] - one[2];
+    const double dot = n[0] * n[0] + n[1] * n[1] + n[2] * n[2];
+    if (dot == 0.0) {  // centre on the hull: the normal of the plane it is furthest out of
+      const int f = nearest_plane_max(one, pla, ns);
+      len = r;
+      if (f < 0) { atomicOr(bad, 32); n[0] = n[1] = 0.0; n[2] = 1.0; }
+      else { n[0] = pla[6 * f]; n[1] = pla[6 * f + 1]; n[2] = pla[6 * f + 2]; }
+    } else {
+      len = sqrt(dot);
+      const double il = 1.0 / len;
+      n[0] *= il; n[1] *= il; n[2] *= il;
+    }
+    double two[3];
+    for (int v = 0; v < 3; v++) two[v] = cc[v] + (-r) * n[v];
+    const double g = len - r;
+    o.gap[k] = g < 0.0 ? g : 0.0;
+    for (int v = 0; v < 3; v++) o.point[3 * (size_t)k + v] = two[v];
+    double X[3];
+    ref_point(rot + 9 * (size_t)bi, xb + 3 * (size_t)bi, x0 + 3 * (size_t)bi, two, X);
+    for (int v = 0; v < 3; v++) o.mpnt[3 * (size_t)k + v] = X[v];
+    ref_point(rot + 9 * (size_t)bc, xb + 3 * (size_t)bc, x0 + 3 * (size_t)bc, one, X);
+    for (int v = 0; v < 3; v++) o.spnt[3 * (size_t)k + v] = X[v];
+    double loc[9];
+    local_base(n, loc);
+    for (int v = 0; v < 9; v++) o.base[9 * (size_t)k + v] = loc[v];
+    const int s1 = nearest_surface_id(one, pla, fs, ns), s2 = s.surf[i];
+    if (s1 < 0 || s1 >= nsurf || s2 < 0 || s2 >= nsurf) {
+      atomicOr(bad, 8);
+      o.fric[k] = o.rest[k] = 0.0;
+    } else {
+      const size_t t = (size_t)s1 * nsurf + s2;
+      o.fric[k] = mat[2 * t];
+      o.rest[k] = mat[2 * t + 1];
+    }
+    o.coh[k] = 0.0;
+    for (int v = 0; v < 3; v++) {
+      o.R0[3 * (size_t)k + v] = hit >= 0 ? prevR[3 * (size_t)hit + v] : 0.0;
+      o.U0[3 * (size_t)k + v] = hit >= 0 ? prevU[3 * (size_t)hit + v] : 0.0;
+    }
+    return;
   }
   const double* ci = s.cur + 3 * (size_t)i;
   const double* cj = s.cur + 3 * (size_t)j;

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <cfloat>
+#include <climits>
 #include <vector>
 #include <algorithm>
 #include <mutex>
@@ -204,10 +205,13 @@ struct b2dev_ctx {
   std::vector<double> sph_mat_h;
   Buf sph_body, sph_ref, sph_rad, sph_surf, sph_mat, sph_cur, sph_cell, sph_hkey, sph_hkey_s, sph_idx, sph_sorted,
       sph_bstart, sph_bend, sph_cnt, sph_off, sph_pi, sph_pj, sph_rmax, sph_keep, sph_pos, sph_bcnt, sph_bptr,
-      sph_blist, sph_pkey, sph_pslo, sph_pR, sph_pU;
+      sph_blist, sph_pkey, sph_pslo, sph_pR, sph_pU, sph_ccnt;
   Buf st_master, st_slave, st_point, st_mpnt, st_spnt, st_base, st_gap, st_fric, st_rest, st_coh, st_R0, st_U0,
       st_key, st_slo, st_new;
   Buf det_point, det_R0, det_U0, det_key, det_slo, det_new;
+  // convex obstacles of the detection (b2dev_convexes_setup)
+  int nconv = 0;
+  Buf cvx_body, cvx_vptr, cvx_vert, cvx_fptr, cvx_fac, cvx_sptr, cvx_surf, cvx_ns, cvx_cur, cvx_pla, cvx_box;
   bool det_valid = false;       // the scene's contacts are those of the last detection
   bool det_assembled = false;   // ... and the local dynamics was assembled from them
   std::vector<int> ptile_count;  // tiles per problem
@@ -1176,12 +1180,77 @@ int b2dev_spheres_setup(b2dev_ctx* c, int nsph, const int* body, const double* c
   return B2DEV_OK;
 }
 
+int b2dev_convexes_setup(b2dev_ctx* c, int nconv, const int* body, const int* vptr, const double* vert,
+                         const int* fptr, const int* fac, const int* sptr, const int* surf) {
+  if (!c || !c->have_scene) { set_err("convexes_setup: no scene uploaded"); return B2DEV_ESTATE; }
+  if (nconv < 0 || (nconv > 0 && (!body || !vptr || !vert || !fptr || !fac || !sptr || !surf))) {
+    set_err("convexes_setup: invalid arguments");
+    return B2DEV_EINVAL;
+  }
+  std::vector<int> ns(std::max(nconv, 1), 0);
+  if (nconv > 0 && (vptr[0] != 0 || fptr[0] != 0 || sptr[0] != 0)) {
+    set_err("convexes_setup: offsets must start at 0");
+    return B2DEV_EINVAL;
+  }
+  for (int k = 0; k < nconv; k++) {
+    const int nv = vptr[k + 1] - vptr[k], nf = sptr[k + 1] - sptr[k];
+    if (body[k] < 0 || body[k] >= c->nbod) { set_err("convexes_setup: convex %d: body out of range", k); return B2DEV_EINVAL; }
+    if (nv < 1 || nv > 256 || nf < 1 || fptr[k + 1] < fptr[k]) {  // GJK runs at most 4 nv^2 steps
+      set_err("convexes_setup: convex %d: %d vertices and %d faces", k, nv, nf);
+      return B2DEV_EINVAL;
+    }
+    int m = fptr[k];
+    for (int f = 0; f < nf; f++) {
+      if (m >= fptr[k + 1] || fac[m] < 3 || m + fac[m] >= fptr[k + 1]) {
+        set_err("convexes_setup: convex %d: face %d overruns its face list", k, f);
+        return B2DEV_EINVAL;
+      }
+      for (int t = 1; t <= fac[m]; t++)
+        if (fac[m + t] < 0 || fac[m + t] >= nv) {
+          set_err("convexes_setup: convex %d: face %d: vertex index out of range", k, f);
+          return B2DEV_EINVAL;
+        }
+      m += fac[m] + 1;
+    }
+    while (ns[k] < nf && surf[sptr[k] + ns[k]] != -INT_MAX) ns[k]++;
+    if (ns[k] == 0) { set_err("convexes_setup: convex %d has no surface face", k); return B2DEV_EINVAL; }
+  }
+  DeviceGuard g(c->device);
+  c->nconv = nconv;
+  const int nvt = nconv > 0 ? vptr[nconv] : 0, nft = nconv > 0 ? sptr[nconv] : 0, nfac = nconv > 0 ? fptr[nconv] : 0;
+  B2_TRY(upload(c, c->cvx_body, body, (size_t)nconv, 0));
+  B2_TRY(upload(c, c->cvx_vptr, vptr, (size_t)nconv + (nconv > 0), 0));
+  B2_TRY(upload(c, c->cvx_vert, vert, (size_t)3 * nvt, 0));
+  B2_TRY(upload(c, c->cvx_fptr, fptr, (size_t)nconv + (nconv > 0), 0));
+  B2_TRY(upload(c, c->cvx_fac, fac, (size_t)nfac, 0));
+  B2_TRY(upload(c, c->cvx_sptr, sptr, (size_t)nconv + (nconv > 0), 0));
+  B2_TRY(upload(c, c->cvx_surf, surf, (size_t)nft, 0));
+  B2_TRY(upload(c, c->cvx_ns, ns.data(), (size_t)nconv, 0));
+  B2_TRY(ensure(c->cvx_cur, sizeof(double) * 3 * (nvt + 1)));
+  B2_TRY(ensure(c->cvx_pla, sizeof(double) * 6 * (nft + 1)));
+  B2_TRY(ensure(c->cvx_box, sizeof(double) * 6 * (nconv + 1)));
+  B2_CK(cudaStreamSynchronize(c->stream));
+  c->det_valid = c->det_assembled = false;
+  return B2DEV_OK;
+}
+
+static ConvexDev convex_view(b2dev_ctx* c) {
+  ConvexDev v;
+  v.n = c->nconv;
+  v.body = ptr<int>(c->cvx_body); v.vptr = ptr<int>(c->cvx_vptr); v.vert = ptr<double>(c->cvx_vert);
+  v.fptr = ptr<int>(c->cvx_fptr); v.fac = ptr<int>(c->cvx_fac); v.sptr = ptr<int>(c->cvx_sptr);
+  v.surf = ptr<int>(c->cvx_surf); v.nsurf_face = ptr<int>(c->cvx_ns); v.cur = ptr<double>(c->cvx_cur);
+  v.pla = ptr<double>(c->cvx_pla); v.box = ptr<double>(c->cvx_box);
+  return v;
+}
+
 static const char* detect_bad_text(int bad) {
   if (bad & 16) return "a sphere's body index is out of range";
   if (bad & 1) return "a sphere radius is not positive and finite, or a centre is not finite";
   if (bad & 2) return "a sphere centre is too far from the origin for the detection grid";
   if (bad & 4) return "two sphere centres coincide (no contact normal)";
-  return "a sphere's surface id is out of the material table";
+  if (bad & 32) return "a convex has no finite face plane";
+  return "a surface id is out of the material table";
 }
 
 static ContactOut staged(b2dev_ctx* c) {
@@ -1253,12 +1322,18 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
   sd.body = ptr<int>(c->sph_body); sd.ref = ptr<double>(c->sph_ref); sd.rad = ptr<double>(c->sph_rad);
   sd.surf = ptr<int>(c->sph_surf); sd.cur = ptr<double>(c->sph_cur); sd.cell = ptr<int4>(c->sph_cell);
   sd.hkey = ptr<unsigned int>(c->sph_hkey);
+  const ConvexDev cvd = convex_view(c);
   int npair = 0, bad = 0;
   if (ns > 0) {
     c->launches += 2;
     k_sph_centres<<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<double>(c->rot), ptr<double>(c->rb_x),
                                                    ptr<double>(c->x0), ptr<unsigned long long>(c->sph_rmax),
                                                    ptr<int>(c->bad));
+    if (c->nconv > 0) {
+      c->launches++;
+      k_cvx_update<<<blocks_for(c->nconv, 64), 64, 0, st>>>(cvd, ptr<double>(c->rot), ptr<double>(c->rb_x),
+                                                          ptr<double>(c->x0));
+    }
     k_sph_cells<<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<unsigned long long>(c->sph_rmax), M - 1,
                                                  ptr<int>(c->sph_idx), ptr<int>(c->bad));
     size_t bytes = 0;
@@ -1275,7 +1350,17 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     k_sph_pairs<false><<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<int>(c->obst), ptr<int>(c->sph_sorted),
                                                         ptr<int>(c->sph_bstart), ptr<int>(c->sph_bend), M - 1,
                                                         ptr<int>(c->sph_cnt), nullptr, nullptr);
-    B2_TRY(scan_exclusive(c, ptr<int>(c->sph_cnt), ptr<int>(c->sph_off), ns + 1));
+    const int* pair_count = ptr<int>(c->sph_cnt);
+    if (c->nconv > 0) {  // convex partners: counted apart, the totals scanned
+      B2_TRY(ensure(c->sph_ccnt, sizeof(int) * (ns + 1)));
+      B2_CK(cudaMemsetAsync(c->sph_ccnt.p, 0, sizeof(int) * (ns + 1), st));
+      c->launches += 2;
+      k_cvx_pairs<false><<<blocks_for(ns, 128), 128, 0, st>>>(sd, cvd, ptr<int>(c->obst), ptr<int>(c->sph_ccnt),
+                                                               nullptr, nullptr, nullptr);
+      k_add_counts<<<blocks_for(ns, T), T, 0, st>>>(ns, ptr<int>(c->sph_cnt), ptr<int>(c->sph_ccnt));
+      pair_count = ptr<int>(c->sph_ccnt);
+    }
+    B2_TRY(scan_exclusive(c, pair_count, ptr<int>(c->sph_off), ns + 1));
     B2_CK(cudaMemcpyAsync(&npair, ptr<int>(c->sph_off) + ns, sizeof(int), cudaMemcpyDeviceToHost, st));
     B2_CK(cudaMemcpyAsync(&bad, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     B2_CK(cudaStreamSynchronize(st));
@@ -1313,10 +1398,16 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     k_sph_pairs<true><<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<int>(c->obst), ptr<int>(c->sph_sorted),
                                                        ptr<int>(c->sph_bstart), ptr<int>(c->sph_bend), M - 1,
                                                        nullptr, ptr<int>(c->sph_off), ptr<int>(c->sph_pj));
+    if (c->nconv > 0) {  // after the sphere partners (sph_cnt still holds their count)
+      c->launches++;
+      k_cvx_pairs<true><<<blocks_for(ns, 128), 128, 0, st>>>(sd, cvd, ptr<int>(c->obst), nullptr,
+                                                              ptr<int>(c->sph_off), ptr<int>(c->sph_cnt),
+                                                              ptr<int>(c->sph_pj));
+    }
     k_sph_sort_seg<<<blocks_for(ns, T), T, 0, st>>>(ns, ptr<int>(c->sph_off), ptr<int>(c->sph_pj),
                                                     ptr<int>(c->sph_pi));
     k_sph_contacts<<<blocks_for(npair, T), T, 0, st>>>(
-        npair, sd, ptr<int>(c->sph_pi), ptr<int>(c->sph_pj), ptr<double>(c->rot), ptr<double>(c->rb_x),
+        npair, sd, cvd, ptr<int>(c->sph_pi), ptr<int>(c->sph_pj), ptr<double>(c->rot), ptr<double>(c->rb_x),
         ptr<double>(c->x0), c->nsurf, ptr<double>(c->sph_mat), nprev, ptr<long long>(c->sph_pkey),
         ptr<int>(c->sph_pslo), ptr<double>(c->sph_pR), ptr<double>(c->sph_pU), so, ptr<int>(c->bad));
     // sparsification neighbourhoods: the contacts of each body

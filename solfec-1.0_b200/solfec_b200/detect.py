@@ -15,6 +15,11 @@ with only the contact count crossing to the host. Contacts are listed by sphere
 pair (i, j), i < j. Kept contacts carry their R and U from the last solve (the
 reference keeps con->R and con->U), new ones start from zero.
 
+Convex obstacles (box walls, say) collide with the spheres as the
+reference's detect_convex_sphere does: the closest hull point by GJK
+(gjk_convex_point), the convex as the slave, the material of the nearest face's
+surface.
+
 Materials: a symmetric table (nsurf, nsurf, 2) of friction and restitution per
 surface pair (SPSET_Find resolved by the caller). Cohesion is not supported:
 the reference gives it only to contacts created at time zero and updates
@@ -62,11 +67,12 @@ class SPHERES:
 
     body: (nsph,) body of each sphere; centre: (nsph, 3) referential centres;
     radius: (nsph,); surface: (nsph,) surface ids (default 0); material: see
-    material_table. The LOCDYN's bodies need RIGID_DYNAMICS set up (mass
-    centres) before the first detect().
+    material_table; convex: None or the keyword arguments of set_convexes
+    (convex obstacles, detect_convex_sphere of goc.c:308-349). The LOCDYN's
+    bodies need RIGID_DYNAMICS set up (mass centres) before the first detect().
     """
 
-    def __init__(self, ldy: LOCDYN, body, centre, radius, surface=None, material=(0.0, 0.0)):
+    def __init__(self, ldy: LOCDYN, body, centre, radius, surface=None, material=(0.0, 0.0), convex=None):
         self.ldy = ldy
         self.nsph = int(np.asarray(body).reshape(-1).shape[0])
         n = self.nsph
@@ -80,6 +86,24 @@ class SPHERES:
         _check(lib().b2dev_spheres_setup(ldy.device_context, n, ptr(self._body), ptr(self._centre),
                                          ptr(self._radius), ptr(self._surface), int(self._mat.shape[0]),
                                          ptr(self._mat), 0), 'b2dev_spheres_setup')
+        self.nconv = 0
+        if convex is not None:
+            self.set_convexes(**convex)
+
+    def set_convexes(self, body, vptr, vert, fptr, fac, sptr, surf):
+        """Convex obstacles the spheres collide with (b2dev_convexes_setup):
+        per convex its body, referential vertices vert[vptr[c]:vptr[c+1]], faces
+        fac[fptr[c]:fptr[c+1]] (per face its vertex count then vertex indices,
+        counter-clockwise seen from outside) and surface ids surf[sptr[c]:sptr[c+1]]."""
+        nc = int(np.asarray(body).reshape(-1).shape[0])
+        vptr = _i32(vptr, nc + 1)
+        sptr = _i32(sptr, nc + 1)
+        fptr = _i32(fptr, nc + 1)
+        self._cvx = [_i32(body, nc), vptr, _f64(vert, 3 * int(vptr[-1])), fptr, _i32(fac, int(fptr[-1])), sptr,
+                     _i32(surf, int(sptr[-1]))]
+        _check(lib().b2dev_convexes_setup(self.ldy.device_context, nc, *[ptr(a) for a in self._cvx]),
+               'b2dev_convexes_setup')
+        self.nconv = nc
 
     def detect(self):
         """Update and detection of the contacts; returns (contacts, new contacts)."""
@@ -125,7 +149,7 @@ def run_spheres(scene, spheres: dict, gs, nsteps: int, J, mass, gravity=(0.0, 0.
     """Time loop of a sphere scene with contact detection on the device.
 
     scene: bodies (its contacts are ignored); spheres: keyword arguments of
-    SPHERES (body, centre, radius, surface, material). Every step: bodies to
+    SPHERES (body, centre, radius, surface, material, convex). Every step: bodies to
     t + h/2 and free velocities, contact update and detection, local dynamics,
     R and U carried over, GAUSS_SEIDEL solve, reactions and second half step.
     callback(k, dyn, sph, ldy) after step k (from 1); False stops the loop.

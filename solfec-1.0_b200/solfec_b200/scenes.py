@@ -641,3 +641,70 @@ def spheres_grid(n_side: int = 100, radius: float = 0.05, pitch: float = 0.0999,
                  velo0=np.zeros((n, 6)), obstacle=np.zeros(n, np.int32), master=np.zeros(0, np.int32),
                  slave=np.zeros(0, np.int32), mpnt=np.zeros((0, 3)), spnt=np.zeros((0, 3)), base=np.zeros((0, 9)),
                  gap=e, friction=e, restitution=e, cohesion=e, mass=np.full(n, m), radius=np.full(n, radius))
+
+
+# faces of a hexahedron whose vertex v = i + 2 j + 4 k sits at corner (x_i, y_j, z_k):
+# counter-clockwise seen from outside, so (b - a) x (c - b) points out
+HEX_FACES = ((0, 4, 6, 2), (1, 3, 7, 5), (0, 1, 5, 4), (2, 6, 7, 3), (0, 2, 3, 1), (4, 5, 7, 6))
+
+
+def box_convex(lo, hi):
+    """Vertices (8, 3) and faces (reference fac layout: count, then indices) of
+    the axis-aligned box [lo, hi]."""
+    lo = np.asarray(lo, float); hi = np.asarray(hi, float)
+    v = np.array([[(lo, hi)[i][0], (lo, hi)[j][1], (lo, hi)[k][2]] for k in (0, 1) for j in (0, 1) for i in (0, 1)])
+    fac = []
+    for f in HEX_FACES:
+        fac += [4] + list(f)
+    return v, np.array(fac, np.int32)
+
+
+def spheres_in_box(seed: int = 9, n_side: int = 5, layers: int = 3, radius: float = 0.05, pitch: float = 0.11,
+                   wall: float = 0.05, clearance: float = 0.002, density: float = 2000.0, friction: float = 0.3,
+                   step: float = 1e-3):
+    """A jittered lattice of spheres in an open-topped box of five fixed
+    hexahedral walls (floor and four sides, each `wall` thick), the lowest
+    layer `clearance` above the floor and the outer columns `clearance` from
+    the sides. Walls are convex obstacles; every sphere is its own body.
+
+    Returns (scene without contacts, SPHERES arguments with `convex`, J, mass)."""
+    rng = np.random.default_rng(seed)
+    half = (n_side - 1) / 2.0 * pitch + radius + clearance
+    top = clearance + radius + (layers - 1) * pitch + radius + pitch
+    g = (np.arange(n_side) - (n_side - 1) / 2.0) * pitch
+    X, Y, Z = np.meshgrid(g, g, clearance + radius + np.arange(layers) * pitch, indexing='ij')
+    xs = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    xs[:, :2] += rng.uniform(-0.1 * (pitch - 2 * radius), 0.1 * (pitch - 2 * radius), (xs.shape[0], 2))
+    n = xs.shape[0]
+    walls = [([-half - wall, -half - wall, -wall], [half + wall, half + wall, 0.0]),       # floor
+             ([-half - wall, -half - wall, 0.0], [-half, half + wall, top]),               # -x
+             ([half, -half - wall, 0.0], [half + wall, half + wall, top]),                 # +x
+             ([-half, -half - wall, 0.0], [half, -half, top]),                             # -y
+             ([-half, half, 0.0], [half, half + wall, top])]                               # +y
+    nw = len(walls)
+    nb = n + nw
+    centres = np.array([0.5 * (np.asarray(a) + np.asarray(b)) for a, b in walls])
+    x = np.concatenate([xs, centres], axis=0)
+    mass = np.ones(nb); mass[:n] = density * 4.0 / 3.0 * math.pi * radius ** 3
+    jinv = np.zeros((nb, 9)); jinv[:n, 0] = jinv[:n, 4] = jinv[:n, 8] = 1.0 / (0.4 * mass[:n] * radius ** 2)
+    minv = np.zeros(nb); minv[:n] = 1.0 / mass[:n]
+    rot = np.zeros((nb, 9)); rot[:, 0] = rot[:, 4] = rot[:, 8] = 1.0
+    rot[:n] = _random_rotations(rng, n)
+    obstacle = np.zeros(nb, np.int32); obstacle[n:] = 1
+    r = np.zeros(nb); r[:n] = radius
+    z = np.zeros((nb, 6)); e = np.zeros(0)
+    sc = Scene(name='spheres-in-box-%d' % n, step=step, dynamic=1, rot=rot, x=x.copy(), x0=x.copy(), jinv=jinv,
+               minv=minv, velo=z.copy(), velo0=z.copy(), obstacle=obstacle, master=np.zeros(0, np.int32),
+               slave=np.zeros(0, np.int32), mpnt=np.zeros((0, 3)), spnt=np.zeros((0, 3)), base=np.zeros((0, 9)),
+               gap=e, friction=e, restitution=e, cohesion=e, mass=mass, radius=r)
+    J, mass = sphere_inertia(sc)
+    verts, facs = [], []
+    for lo, hi in walls:
+        v, f = box_convex(lo, hi)
+        verts.append(v); facs.append(f)
+    convex = dict(body=np.arange(n, nb, dtype=np.int32), vptr=np.arange(nw + 1, dtype=np.int32) * 8,
+                  vert=np.concatenate(verts), fptr=np.arange(nw + 1, dtype=np.int32) * 30, fac=np.concatenate(facs),
+                  sptr=np.arange(nw + 1, dtype=np.int32) * 6, surf=np.zeros(6 * nw, np.int32))
+    sph = dict(body=np.arange(n, dtype=np.int32), centre=xs.copy(), radius=np.full(n, radius),
+               surface=np.zeros(n, np.int32), material=(friction, 0.0), convex=convex)
+    return sc, sph, J, mass

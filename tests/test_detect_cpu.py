@@ -172,3 +172,71 @@ def test_sparsify_duplicate_points():
     prev = dict(key=first['key'], slave_lo=first['slave_lo'])
     out = _detect(c, prev)
     assert out['key'].tolist() == [1, (1 << 32) | 2] and out['isnew'].tolist() == [0, 1]
+
+
+# ---------------------------------------------------------------- convex obstacles
+
+@pytest.mark.skipif(not oracle.ref_available(), reason='reference build unavailable')
+def test_gjk_convex_point_pinned_to_reference():
+    rng = np.random.default_rng(12)
+    for t in range(3000):
+        box = np.array([[x, y, z] for x in (0, 1) for y in (0, 1) for z in (0, 1)], float) * rng.uniform(0.2, 2, 3)
+        box += rng.normal(size=box.shape) * 0.05
+        R = np.linalg.qr(rng.normal(size=(3, 3)))[0]
+        a = box @ R.T + rng.normal(size=3)
+        p = a.mean(0) + rng.normal(size=3) * [0.05, 0.5, 1.0, 3.0][t % 4]   # inside, near and far
+        d1, q1 = oracle.gjk_convex_point(a, p, 'oracle')
+        d2, q2 = oracle.gjk_convex_point(a, p, 'ref')
+        assert _bits([d1]) == _bits([d2]) and np.array_equal(_bits(q1), _bits(q2))
+
+
+def test_box_planes_point_outward():
+    v, f = scenes.box_convex([0, 0, 0], [1, 2, 3])
+    pla = oracle.convex_planes(f, v)
+    assert np.array_equal(pla[:, :3], np.array([[-1, 0, 0], [1, 0, 0], [0, -1, 0], [0, 1, 0], [0, 0, -1], [0, 0, 1.0]]))
+    for k in range(6):   # each plane's point lies on its face
+        axis = k // 2
+        assert pla[k, 3 + axis] == (v[:, axis].max() if k % 2 else v[:, axis].min())
+
+
+def _box_contacts(shift, prev=None):
+    sc, sp, J, mass = scenes.spheres_in_box()
+    n = sp['body'].shape[0]
+    x = sc.x.copy()
+    x[:n] += shift
+    out = oracle.detect_spheres(sp['body'], sp['centre'], sp['radius'], sp['surface'], sc.rot, x, sc.x0, sc.obstacle,
+                                MAT, prev, convex=sp['convex'])
+    return sc, sp, x, out
+
+
+def test_spheres_on_box_floor():
+    sc, sp, x, out = _box_contacts([0.0, 0.0, -0.00201])   # the lowest layer 10 um into the floor
+    n = sp['body'].shape[0]
+    j = out['key'] & 0xFFFFFFFF
+    wall = j >= n
+    floor_body = n   # the first convex, the floor
+    assert wall.sum() == 25 and np.all(out['slave'][wall] == floor_body)
+    assert np.all(out['master'][wall] == (out['key'][wall] >> 32))
+    assert np.all(out['slave_lo'][wall] == 0)
+    assert np.allclose(out['gap'][wall], -1e-5, atol=1e-12)
+    nrm = out['base'][wall][:, 6:9]
+    assert np.allclose(nrm, [0, 0, 1], atol=1e-12)
+    ctr = x[out['master'][wall]]
+    assert np.allclose(out['point'][wall], ctr - 0.05 * nrm, atol=1e-15)
+    assert np.allclose(out['spnt'][wall][:, 2], 0.0, atol=1e-12)   # on the floor's top face (referential = spatial)
+
+
+def test_box_side_wall_and_update():
+    # shifted 3.5 mm towards the +x wall (clearance 2 mm, jitter up to 1 mm):
+    # the whole last column touches it; the update carries R
+    sc, sp, x, out = _box_contacts([0.0035, 0.0, 0.0])
+    n = sp['body'].shape[0]
+    j = out['key'] & 0xFFFFFFFF
+    side = j == n + 2   # the +x wall
+    assert side.sum() == 15 and np.all(out['isnew'] == 1)
+    assert np.allclose(out['base'][side][:, 6:9], [-1, 0, 0], atol=1e-12)
+    prev = dict(key=out['key'], slave_lo=out['slave_lo'], R=np.arange(3 * len(j), dtype=float).reshape(-1, 3),
+                U=np.zeros((len(j), 3)))
+    sc, sp, x2, out2 = _box_contacts([0.0036, 0.0, 0.0], prev)
+    assert np.array_equal(out2['key'], out['key']) and np.all(out2['isnew'] == 0)
+    assert np.array_equal(out2['R'], prev['R'])

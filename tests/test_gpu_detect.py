@@ -167,3 +167,61 @@ def test_sparsified_contacts_match_oracle():
     assert dev['key'].tolist() == [(0 << 32) | 2, (1 << 32) | 2]
     _same(dev, _oracle(sp, sc.rot, sc.x, sc.x0, sc.obstacle))
     ldy.close()
+
+
+def _oracle_box(sp, rot, x, x0, obst, prev=None):
+    mat = np.asarray(sp['material'], float).reshape(1, 1, 2)
+    return oracle.detect_spheres(sp['body'], sp['centre'], sp['radius'], sp['surface'], rot, x, x0, obst, mat, prev,
+                                 convex=sp['convex'])
+
+
+def test_box_walls_match_oracle():
+    """Spheres pressed into the floor and a side wall of a box of convex walls:
+    sphere-convex contacts (GJK closest points, planes, nearest surface) equal
+    the oracle bit for bit."""
+    sc, sp, J, mass = scenes.spheres_in_box()
+    n = sp['body'].shape[0]
+    x = sc.x.copy()
+    x[:n] += np.array([0.0035, 0.0, -0.0021])
+    sc = dataclasses.replace(sc, x=x)
+    ldy = _setup(sc, J, mass)
+    s = SPHERES(ldy, **sp)
+    nc, nn = s.detect()
+    dev = s.contacts()
+    orc = _oracle_box(sp, sc.rot, sc.x, sc.x0, sc.obstacle)
+    assert nc == nn == orc['key'].shape[0] and int(((dev['key'] & 0xFFFFFFFF) >= n).sum()) >= 25 + 15
+    _same(dev, orc)
+    ldy.close()
+
+
+def test_box_time_loop_matches_oracle_every_step():
+    """Spheres dropped into the box: every step's contacts (sphere-sphere and
+    sphere-wall) equal the oracle's on the device bodies, with the carried R, U."""
+    sc, sp, J, mass = scenes.spheres_in_box(n_side=4, layers=3)
+    ldy = LOCDYN()
+    ldy.update_begin(bodies_only(sc))
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    sph = SPHERES(ldy, **sp)
+    gs = GAUSS_SEIDEL_SOLVER(1e-6, 200)
+    prev = None
+    walls = 0
+    h = sc.step
+    for k in range(80):
+        dyn.step_begin(h, (0.0, 0.0, -9.81))
+        st = dyn.state()
+        nc, nn = sph.detect()
+        dev = sph.contacts()
+        _same(dev, _oracle_box(sp, st['rot'], st['x'], sc.x0, sc.obstacle, prev))
+        walls = max(walls, int(((dev['key'] & 0xFFFFFFFF) >= sp['body'].shape[0]).sum()))
+        if nc > 0:
+            assert lib().b2gs_locdyn_update_begin_resident(ldy.handle, h, 1) == 0
+            sph.carry_state()
+            gs.solve(ldy)
+            R, U, _ = ldy.get_state()
+            prev = dict(key=dev['key'], slave_lo=dev['slave_lo'], R=R, U=U)
+        else:
+            prev = dict(key=dev['key'], slave_lo=dev['slave_lo'])
+        dyn.step_end(h)
+    assert walls >= 16   # the lowest layer rests on the floor
+    assert np.all(dyn.state()['x'][:sp['body'].shape[0], 2] > 0.04)
+    ldy.close()
