@@ -20,6 +20,12 @@
  *    (BODY_Ref_Point, bod.c:1736-1750), local base (localbase, dom.c:133-151),
  *    gap, surface material (SPSET_Find, sps.c:152-184, resolved by the caller
  *    into a symmetric table of friction and restitution);
+ *  - convex obstacles (orc_detect): vertices moved with their bodies and face
+ *    planes recomputed (CONVEX_Update, cvx.c:1362-1396; computeplanes,
+ *    cvx.c:72-89); a sphere within r + GEOMETRIC_EPSILON of a hull by
+ *    gjk_convex_point (gjk.c:510-556) makes a contact with the convex as the
+ *    slave (detect_convex_sphere / update_convex_sphere, goc.c:308-349,
+ *    555-597; nearest_normal and nearest_surface, goc.c:87-122);
  *  - sparsify_contacts (dom.c:2956-3054): a new contact whose spatial point
  *    lies within 2 mindist (max-norm) of another contact of one of its bodies is
  *    removed when that contact is old or comes later in the list. Sphere
@@ -30,13 +36,14 @@
  * GEOMETRIC_EPSILON overlaps there, so the candidates only prune and this
  * restatement uses a sweep along x with a wider margin.
  *
- * Order: contacts are listed by sphere pair (i, j), i < j, ascending. The
+ * Order: contacts are listed by pair (i, j), i < j, ascending, where a convex c
+ * counts as object nsph + c. The
  * reference lists them in insertion order (broad-phase callback order), which
  * depends on its AABB algorithm; the same order also stands in for the
  * reference's contact ids in the sparsification tie-break.
  *
- * gjk_sphere_sphere here is checked bit for bit against the reference's own
- * gjk.c, compiled into oracle/_ref.
+ * gjk_sphere_sphere and gjk_convex_point here are checked bit for bit against
+ * the reference's own gjk.c, compiled into oracle/_ref.
  */
 #include <float.h>
 #include <limits.h>

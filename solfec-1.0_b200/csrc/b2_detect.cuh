@@ -1,5 +1,6 @@
-// b2_detect.cuh -- contact update and detection between spheres of rigid bodies
-// (the contact part of DOM_Update_Begin, dom.c:3700-3790, for sphere pairs).
+// b2_detect.cuh -- contact update and detection between spheres of rigid bodies,
+// and between spheres and convex obstacles (the contact part of
+// DOM_Update_Begin, dom.c:3700-3790, for those pairs).
 //
 //   k_sph_centres   SPHERE_Update with BODY_Cur_Point (sph.c:322-344,
 //                   bod.c:1702-1716); largest radius for the cell size
@@ -10,18 +11,21 @@
 //                   cvx.c:1362-1396): vertices, face planes, bounding box
 //   k_sph_pairs     per sphere i, the spheres j > i of the 27 surrounding cells
 //                   whose gjk_sphere_sphere gap (gjk.c:560-584) is below
-//                   GEOMETRIC_EPSILON (goc.c:431), and the convexes whose
-//                   gjk_convex_point distance (gjk.c:510-556) is below
-//                   r + GEOMETRIC_EPSILON (goc.c:319), bodies different and
-//                   not both obstacles (box.c:104-108): counted, then written
+//                   GEOMETRIC_EPSILON (goc.c:431), bodies different and not
+//                   both obstacles (box.c:104-108): counted, then written
 //   k_sph_sort_seg  the pairs of each sphere in ascending j (list order)
+//   k_cvx_pairs     per sphere, the convexes whose gjk_convex_point distance
+//                   (gjk.c:510-556) is below r + GEOMETRIC_EPSILON (goc.c:319),
+//                   after a box test, with the same body filters: counted,
+//                   then written after the sphere's sphere partners
 //   k_sph_contacts  one contact per pair: roles kept from the previous step
 //                   (update_contact, dom.c:430-484; update_sphere_sphere,
 //                   goc.c:658-677) or set by the centres' point order
 //                   (detect_sphere_sphere, goc.c:421-456); spatial point,
 //                   normal, gap (goc.c:52-61), referential points
 //                   (BODY_Ref_Point, bod.c:1736-1750), local base (localbase,
-//                   dom.c:133-151), surface material, carried R and U
+//                   dom.c:133-151), surface material, carried R and U; for a
+//                   convex partner detect_convex_sphere (goc.c:308-349)
 //   k_sph_body_*    per body, its contacts (sparsification neighbourhoods)
 //   k_sph_sparsify  sparsify_contacts (dom.c:2956-3054) for sphere contacts
 //                   (area 1): a new contact within 2 mindist (max-norm) of an
