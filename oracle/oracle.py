@@ -32,10 +32,20 @@ def build():
 def _load(name):
     if name in _LIBS:
         return _LIBS[name]
-    path = os.path.join(HERE, {'oracle': 'lib/liboracle.so', 'ref': '_ref/libref_bgs.so'}[name])
+    path = os.path.join(HERE, {'oracle': 'lib/liboracle.so', 'ref': '_ref/libref_bgs.so',
+                               'geo': '_ref/libref_geo.so'}[name])
     if not os.path.exists(path):
         build()
     lib = C.CDLL(path)
+    if name == 'geo':
+        lib.ref_gobj_sphere_sphere.restype = C.c_int
+        lib.ref_gobj_sphere_sphere.argtypes = [C.c_int, _dp, C.c_double, C.c_int, _dp, C.c_double, C.c_int,
+                                               _dp, _dp, _dp, _dp, _ip]
+        lib.ref_gobj_convex_sphere.restype = C.c_int
+        lib.ref_gobj_convex_sphere.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_int, _ip, _ip, _dp, C.c_double,
+                                               C.c_int, _dp, _dp, _dp, _dp, _ip]
+        _LIBS[name] = lib
+        return lib
     solve = lib.orc_gs_solve if name == 'oracle' else lib.ref_gs_solve
     solve.restype = C.c_int
     solve.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
@@ -339,3 +349,35 @@ def detect_spheres(sbody, sref, radius, surface, rot, x, x0, obstacle, material,
     if n > 8 * nsph + 16:
         n, out = run(n)
     return {k: v[:n] for k, v in out.items()}
+
+
+# ---------------------------------------------------------------- the reference's own contact geometry
+
+def geo_available() -> bool:
+    return os.path.exists(os.path.join(HERE, '_ref/libref_geo.so')) or os.path.isdir('/root/reference')
+
+
+def ref_gobj_sphere_sphere(ca, ra, sa, cb, rb, sb, update=False):
+    """gobjcontact (goc.c:1362) of the reference for spheres a (first) and b:
+    (state, onepnt, twopnt, normal, gap, spair)."""
+    lib = _load('geo')
+    one, two, nrm, gap, sp = np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(1), np.zeros(2, np.int32)
+    st = lib.ref_gobj_sphere_sphere(int(update), np.ascontiguousarray(ca, dtype=np.float64), float(ra), int(sa),
+                                    np.ascontiguousarray(cb, dtype=np.float64), float(rb), int(sb),
+                                    one, two, nrm, gap, sp)
+    return st, one, two, nrm, gap[0], sp
+
+
+def ref_gobj_convex_sphere(ver, fac, surf, c, r, s, sphere_first=False, update=False):
+    """gobjcontact of the reference for a convex (vertices, reference face
+    layout, surface per face) and a sphere: (state, onepnt, twopnt, normal,
+    gap, spair), onepnt on the first object."""
+    lib = _load('geo')
+    ver = np.ascontiguousarray(ver, dtype=np.float64).reshape(-1)
+    fac = np.ascontiguousarray(fac, dtype=np.int32)
+    surf = np.ascontiguousarray(surf, dtype=np.int32)
+    one, two, nrm, gap, sp = np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(1), np.zeros(2, np.int32)
+    st = lib.ref_gobj_convex_sphere(int(update), int(sphere_first), ver.shape[0] // 3, ver, surf.shape[0], fac, surf,
+                                    np.ascontiguousarray(c, dtype=np.float64), float(r), int(s), one, two, nrm,
+                                    gap, sp)
+    return st, one, two, nrm, gap[0], sp

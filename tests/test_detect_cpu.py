@@ -240,3 +240,109 @@ def test_box_side_wall_and_update():
     sc, sp, x2, out2 = _box_contacts([0.0036, 0.0, 0.0], prev)
     assert np.array_equal(out2['key'], out['key']) and np.all(out2['isnew'] == 0)
     assert np.array_equal(out2['R'], prev['R'])
+
+
+# ---------------------------------------------------------------- pinned to the reference's gobjcontact
+
+def _same_bits(a, b):
+    return np.array_equal(_bits(np.atleast_1d(a)), _bits(np.atleast_1d(b)))
+
+
+@pytest.mark.skipif(not oracle.geo_available(), reason='reference build unavailable')
+def test_sphere_contacts_pinned_to_reference_gobjcontact(scene_cache):
+    """Every contact the oracle forms on the settled lattice equals the
+    reference's own detect_sphere_sphere (gobjcontact, CONTACT_DETECT) bit for
+    bit, whichever sphere the broad phase hands over first: roles, normal,
+    gap and both points; and a pair the oracle leaves out is no contact there."""
+    from scipy.spatial import cKDTree
+    sc = scene_cache('spheres_lattice')
+    sp = scenes.sphere_shapes(sc)
+    out = oracle.detect_spheres(sp['body'], sp['centre'], sp['radius'], sp['surface'], sc.rot, sc.x, sc.x0,
+                                sc.obstacle, MAT)
+    cur = oracle.sphere_centres(sp['body'], sp['centre'], sc.rot, sc.x, sc.x0)
+    rad = sp['radius']
+    found = set()
+    for k in range(out['key'].shape[0]):
+        i, j = int(out['key'][k] >> 32), int(out['key'][k] & 0xFFFFFFFF)
+        found.add((i, j))
+        for first, second in ((i, j), (j, i)):
+            st, one, two, nrm, gap, _ = oracle.ref_gobj_sphere_sphere(cur[first], rad[first], 0, cur[second],
+                                                                       rad[second], 0)
+            assert st in (1, 2)
+            master = second if st == 1 else first   # dom.c:386-404
+            mpt, spt = (two, one) if st == 1 else (one, two)
+            assert sp['body'][master] == out['master'][k]
+            assert _same_bits(nrm, out['base'][k, 6:9]) and _same_bits(gap, out['gap'][k])
+            assert _same_bits(mpt, out['point'][k])
+    near = cKDTree(cur).query_pairs(2 * rad.max() + 1e-5, output_type='ndarray')
+    left = [(int(a), int(b)) for a, b in near if (int(a), int(b)) not in found][:300]
+    assert left
+    for a, b in left:
+        assert oracle.ref_gobj_sphere_sphere(cur[a], rad[a], 0, cur[b], rad[b], 0)[0] == 0
+
+
+@pytest.mark.skipif(not oracle.geo_available(), reason='reference build unavailable')
+def test_sphere_update_pinned_to_reference_gobjcontact():
+    """Kept contacts after the centres moved (roles kept): the reference's
+    update_sphere_sphere (CONTACT_UPDATE, slave first) gives the oracle's
+    normal, gap and points bit for bit, also where the centres' point order
+    has flipped."""
+    rng = np.random.default_rng(21)
+    for t in range(200):
+        a = rng.normal(size=3)
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        c = _two_spheres(a, a + d * rng.uniform(0.95, 1.0), r=(0.5, 0.5))
+        first = _detect(c)
+        assert first['key'].shape[0] == 1
+        b = a + d * rng.uniform(0.9, 1.0) * np.where(rng.uniform() < 0.5, 1, -1)   # may swap the point order
+        c2 = _two_spheres(a, b, r=(0.5, 0.5))
+        out = _detect(c2, dict(key=first['key'], slave_lo=first['slave_lo']))
+        assert out['key'].shape[0] == 1 and out['isnew'][0] == 0
+        s, m = (0, 1) if first['slave_lo'][0] else (1, 0)
+        cs = [a, b]
+        st, one, two, nrm, gap, _ = oracle.ref_gobj_sphere_sphere(cs[s], 0.5, 0, cs[m], 0.5, 0, update=True)
+        assert st == 1
+        assert _same_bits(nrm, out['base'][0, 6:9]) and _same_bits(gap, out['gap'][0])
+        assert _same_bits(two, out['point'][0])
+
+
+@pytest.mark.skipif(not oracle.geo_available(), reason='reference build unavailable')
+def test_convex_contacts_pinned_to_reference_gobjcontact():
+    """Spheres pressed into the floor and a side wall of the box: every
+    sphere-wall contact equals the reference's detect_convex_sphere
+    (gobjcontact with the convex first and with the sphere first) and
+    update_convex_sphere bit for bit; spheres the oracle leaves out touch no
+    wall there."""
+    sc, sp, x, out = _box_contacts([0.0035, 0.0, -0.0021])
+    cv = sp['convex']
+    n = sp['body'].shape[0]
+    cur = oracle.sphere_centres(sp['body'], sp['centre'], sc.rot, x, sc.x0)
+    walls = {}
+    for c in range(cv['body'].shape[0]):
+        b = cv['body'][c]
+        X = cv['vert'][cv['vptr'][c]:cv['vptr'][c + 1]]
+        A = X - sc.x0[b]   # the walls do not rotate: R (X - X0) is X - X0 exactly
+        walls[c] = (x[b] + A, cv['fac'][cv['fptr'][c]:cv['fptr'][c + 1]], cv['surf'][cv['sptr'][c]:cv['sptr'][c + 1]])
+    seen = set()
+    for k in range(out['key'].shape[0]):
+        i, j = int(out['key'][k] >> 32), int(out['key'][k] & 0xFFFFFFFF)
+        if j < n:
+            continue
+        c = j - n
+        seen.add((i, c))
+        ver, fac, surf = walls[c]
+        for sphere_first in (False, True):
+            for update in (False, True):
+                st, one, two, nrm, gap, spair = oracle.ref_gobj_convex_sphere(ver, fac, surf, cur[i], 0.05, 0,
+                                                                              sphere_first, update)
+                assert st == (2 if sphere_first and not update else 1)
+                mpt = one if sphere_first else two
+                assert _same_bits(nrm, out['base'][k, 6:9]) and _same_bits(gap, out['gap'][k])
+                assert _same_bits(mpt, out['point'][k])
+    assert len(seen) >= 40
+    for i in range(n):
+        for c in walls:
+            if (i, c) not in seen:
+                ver, fac, surf = walls[c]
+                assert oracle.ref_gobj_convex_sphere(ver, fac, surf, cur[i], 0.05, 0)[0] == 0
