@@ -311,6 +311,29 @@ DETECT_BYTES_CONTACT = 512
 DETECT_REPS = 10
 
 
+DETECT_CPU_GRID = 60
+
+
+def detect_cpu_baseline():
+    """The reference's own CPU detection (oracle/_ref/libref_geo.so: the hyb.c
+    hybrid broad phase over the eps-inflated sphere boxes and goc.c's
+    detect_sphere_sphere per overlap, one host core) on a DETECT_CPU_GRID^3
+    sample of the same grid, as contacts per second. Insertion into the domain
+    and the sparsification are not timed, so the figure favours the reference."""
+    import time
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import oracle as O
+    from solfec_b200 import scenes
+    sc = scenes.spheres_grid(DETECT_CPU_GRID)
+    sp = scenes.sphere_shapes(sc, friction=0.3)
+    t0 = time.perf_counter()
+    n = O.ref_detect_spheres_hybrid(sc.x, sp['radius'], sp['body'])
+    dt = time.perf_counter() - t0
+    return {'value': round(n / dt, 1), 'unit': 'contacts/s', 'cores': 1, 'kind': 'reference',
+            'sample': 'spheres-grid %d^3 (%d spheres, %d contacts): hyb.c hybrid + detect_sphere_sphere, %.2f s'
+                      % (DETECT_CPU_GRID, sc.nbod, n, dt)}
+
+
 def detect_timing(grid=DETECT_GRID):
     """Host call time of b2dev_detect_spheres (SPHERES.detect) on grid^3 spheres:
     the first call detects every contact, the timed calls (after 3 warm-up
@@ -344,12 +367,14 @@ def detect_timing(grid=DETECT_GRID):
         ms = float(np.median(ts)) * 1e3
         nb = DETECT_BYTES_SPHERE * s.nsph + DETECT_BYTES_CONTACT * s.ncon
         peak = _peaks()[0]
+        cpu = detect_cpu_baseline()
         return {'workload': 'spheres-grid-%d: %d^3 spheres, pitch 0.0999, radius 0.05' % (s.nsph, grid),
                 'spheres': s.nsph, 'contacts': int(s.ncon), 'new_first_call': int(nn),
                 'first_call_ms': round(first * 1e3, 3), 'update_call_ms': round(ms, 3),
                 'contacts_per_s': round(s.ncon / (ms * 1e-3), 1), 'bytes_per_call': int(nb),
                 'achieved_gbs': round(nb / (ms * 1e-3) / 1e9, 1), 'peak_gbs': peak,
-                'frac': round(nb / (ms * 1e-3) / 1e9 / peak, 3), 'timing': 'host call time, median of %d' % DETECT_REPS}
+                'frac': round(nb / (ms * 1e-3) / 1e9 / peak, 3), 'timing': 'host call time, median of %d' % DETECT_REPS,
+                'cpu_baseline': cpu}
     finally:
         ldy.close()
 

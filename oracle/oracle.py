@@ -41,6 +41,8 @@ def _load(name):
         lib.ref_gobj_sphere_sphere.restype = C.c_int
         lib.ref_gobj_sphere_sphere.argtypes = [C.c_int, _dp, C.c_double, C.c_int, _dp, C.c_double, C.c_int,
                                                _dp, _dp, _dp, _dp, _ip]
+        lib.ref_detect_spheres_hybrid.restype = C.c_longlong
+        lib.ref_detect_spheres_hybrid.argtypes = [C.c_int, _dp, _dp, _ip, C.c_void_p, C.c_longlong]
         lib.ref_gobj_convex_sphere.restype = C.c_int
         lib.ref_gobj_convex_sphere.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_int, _ip, _ip, _dp, C.c_double,
                                                C.c_int, _dp, _dp, _dp, _dp, _ip]
@@ -381,3 +383,22 @@ def ref_gobj_convex_sphere(ver, fac, surf, c, r, s, sphere_first=False, update=F
                                     np.ascontiguousarray(c, dtype=np.float64), float(r), int(s), one, two, nrm,
                                     gap, sp)
     return st, one, two, nrm, gap[0], sp
+
+
+def ref_detect_spheres_hybrid(centre, radius, body, pairs=False):
+    """The reference's CPU detection of a sphere set (hyb.c hybrid broad phase
+    and detect_sphere_sphere per overlap): the number of contacts, or with
+    pairs=True their sphere-pair keys (i << 32 | j, ascending)."""
+    lib = _load('geo')
+    n = int(np.asarray(radius).shape[0])
+    args = (n, np.ascontiguousarray(centre, dtype=np.float64).reshape(-1),
+            np.ascontiguousarray(radius, dtype=np.float64), np.ascontiguousarray(body, dtype=np.int32))
+    if not pairs:
+        return int(lib.ref_detect_spheres_hybrid(*args, None, 0))
+    cap = 16 * n + 16
+    out = np.zeros(cap, np.int64)
+    m = int(lib.ref_detect_spheres_hybrid(*args, out.ctypes.data_as(C.c_void_p), cap))
+    if m > cap:
+        out = np.zeros(m, np.int64)
+        m = int(lib.ref_detect_spheres_hybrid(*args, out.ctypes.data_as(C.c_void_p), m))
+    return out[:m]

@@ -22,6 +22,7 @@
 #include "msh.h"
 #include "fem.h"
 #include "mat.h"
+#include "hyb.h"
 
 /* action: 0 CONTACT_DETECT, 1 CONTACT_UPDATE; sphere a is the first object */
 int ref_gobj_sphere_sphere (int action, const double *ca, double ra, int sa, const double *cb, double rb, int sb,
@@ -65,6 +66,76 @@ int ref_gobj_convex_sphere (int action, int sphere_first, int nver, const double
   free (tri);
   CONVEX_Destroy (cvx);
   return state;
+}
+
+/* ---- the reference's CPU detection of a sphere set: its hybrid broad phase
+ * (hyb.c:317) over the spheres' boxes (SPHERE_Extents, sph.c:240-252) and
+ * detect_sphere_sphere (gobjcontact) for every overlap of spheres of different
+ * bodies (the body filter of box.c:107-108). Insertion into the domain and the
+ * sparsification are not included. Returns the number of contacts; the first
+ * cap sphere pairs (i << 32 | j, i < j, ascending) go to pairs (may be NULL). */
+
+typedef struct { SPHERE *sph; const int *body; long long *pair; size_t n, cap; } hyb_state;
+
+/* one call per reported overlap; the reference's overlap_create skips a pair
+ * whose contact exists already (contact_exists, dom.c:333-346), as hybrid can
+ * report a pair more than once: the detected pairs are recorded and counted
+ * once at the end */
+static void hyb_overlap (void *data, BOX *one, BOX *two)
+{
+  hyb_state *h = data;
+  SPHERE *a = one->sgp->gobj, *b = two->sgp->gobj;
+  const long long i = a - h->sph, j = b - h->sph;
+  double onepnt [3], twopnt [3], normal [3], gap, area;
+  int spair [2], ntri = 0;
+  TRI *tri = NULL;
+  if (h->body [i] == h->body [j]) return;
+  if (gobjcontact (CONTACT_DETECT, AABB_SPHERE_SPHERE, NULL, a, NULL, b, onepnt, twopnt, normal, &gap, &area, spair,
+                   &tri, &ntri))
+  {
+    if (h->n == h->cap) { h->cap = h->cap ? 2 * h->cap : 1024; h->pair = realloc (h->pair, sizeof (long long) * h->cap); }
+    h->pair [h->n ++] = i < j ? (i << 32) | j : (j << 32) | i;
+  }
+  free (tri);
+}
+
+static int llcmp (const void *x, const void *y)
+{
+  const long long a = *(const long long *) x, b = *(const long long *) y;
+  return a < b ? -1 : a > b;
+}
+
+long long ref_detect_spheres_hybrid (int n, const double *centre, const double *radius, const int *body,
+                                     long long *pairs, long long cap)
+{
+  SPHERE *sph = calloc ((size_t) n + 1, sizeof (SPHERE));
+  SGP *sgp = calloc ((size_t) n + 1, sizeof (SGP));
+  BOX *box = calloc ((size_t) n + 1, sizeof (BOX));
+  BOX **ptr = calloc ((size_t) n + 1, sizeof (BOX *));
+  hyb_state h = {sph, body, NULL, 0, 0};
+  long long count = 0;
+  for (int i = 0; i < n; i ++)
+  {
+    memcpy (sph [i].cur_center, centre + 3 * (size_t) i, sizeof (double [3]));
+    sph [i].cur_radius = radius [i];
+    sgp [i].gobj = &sph [i];
+    sgp [i].kind = GOBJ_SPHERE;
+    sgp [i].box = &box [i];
+    box [i].kind = GOBJ_SPHERE;
+    box [i].sgp = &sgp [i];
+    SPHERE_Extents (NULL, &sph [i], box [i].extents);
+    ptr [i] = &box [i];
+  }
+  hybrid (ptr, n, &h, hyb_overlap);
+  qsort (h.pair, h.n, sizeof (long long), llcmp);
+  for (size_t k = 0; k < h.n; k ++)
+    if (k == 0 || h.pair [k] != h.pair [k - 1])
+    {
+      if (pairs && count < cap) pairs [count] = h.pair [k];
+      count ++;
+    }
+  free (h.pair); free (ptr); free (box); free (sgp); free (sph);
+  return count;
 }
 
 /* ---- link stubs: code the sphere and convex paths of goc.c do not reach ---- */

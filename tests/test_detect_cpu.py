@@ -346,3 +346,17 @@ def test_convex_contacts_pinned_to_reference_gobjcontact():
             if (i, c) not in seen:
                 ver, fac, surf = walls[c]
                 assert oracle.ref_gobj_convex_sphere(ver, fac, surf, cur[i], 0.05, 0)[0] == 0
+
+
+@pytest.mark.skipif(not oracle.geo_available(), reason='reference build unavailable')
+def test_reference_broad_phase_finds_the_oracle_pairs(scene_cache):
+    """The reference's own broad phase (hyb.c hybrid over the eps-inflated
+    sphere boxes) with detect_sphere_sphere per overlap finds exactly the
+    oracle's sphere pairs on the settled lattice and on an overlapping grid."""
+    for sc in (scene_cache('spheres_lattice'), scenes.spheres_grid(12)):
+        sp = scenes.sphere_shapes(sc, friction=0.3)
+        out = oracle.detect_spheres(sp['body'], sp['centre'], sp['radius'], sp['surface'], sc.rot, sc.x, sc.x0,
+                                    sc.obstacle, MAT)
+        cur = oracle.sphere_centres(sp['body'], sp['centre'], sc.rot, sc.x, sc.x0)
+        ref = oracle.ref_detect_spheres_hybrid(cur, sp['radius'], sp['body'], pairs=True)
+        assert ref.shape[0] > 1000 and np.array_equal(ref, out['key'])
