@@ -8,10 +8,11 @@ a step is
 
     step_begin -> LOCDYN update (device bodies) -> GAUSS_SEIDEL solve -> step_end
 
-without the bodies leaving the device. Contact detection is not part of this
-path: run_fixed_contacts keeps the uploaded contacts (referential points,
-frames, gaps, materials) for every step, which is exact for contacts that stay
-attached to the same material points, e.g. a block sliding on a flat table.
+without the bodies leaving the device. run_fixed_contacts keeps the uploaded
+contacts (referential points, frames, gaps, materials) for every step, which is
+exact for contacts that stay attached to the same material points, e.g. a
+block sliding on a flat table; for spheres and convex obstacles,
+detect.run_spheres detects and updates the contacts on the device every step.
 
 Schemes: 'RIG_NEG' (NEW2, the reference's default) and 'RIG_POS' (NEW1);
 'RIG_IMP' (NEW3) is not supported and raises.
