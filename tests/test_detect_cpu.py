@@ -360,3 +360,61 @@ def test_reference_broad_phase_finds_the_oracle_pairs(scene_cache):
         cur = oracle.sphere_centres(sp['body'], sp['centre'], sc.rot, sc.x, sc.x0)
         ref = oracle.ref_detect_spheres_hybrid(cur, sp['radius'], sp['body'], pairs=True)
         assert ref.shape[0] > 1000 and np.array_equal(ref, out['key'])
+
+
+# ---------------------------------------------------------------- golden vectors of the reference's gobjcontact
+
+def _unhex(v):
+    return np.array([float.fromhex(x) for x in v])
+
+
+def _golden():
+    import json
+    import os
+    return json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'detect_ref.json')))
+
+
+def test_oracle_sphere_pairs_match_golden_gobjcontact():
+    """tests/golden/detect_ref.json (made by make_detect_golden.py from the
+    reference's own gobjcontact): each sphere pair, detected fresh or updated
+    with the first sphere as the slave, gives the oracle's contact bit for bit."""
+    eye = np.tile(np.eye(3).reshape(9), (2, 1))
+    z = np.zeros((2, 3))
+    for case in _golden()['sphere_sphere']:
+        a, b = _unhex(case['a']), _unhex(case['b'])
+        ra, rb = _unhex(case['ra'])[0], _unhex(case['rb'])[0]
+        prev = dict(key=np.array([1], np.int64), slave_lo=np.array([1], np.int32)) if case['update'] else None
+        out = oracle.detect_spheres([0, 1], np.stack([a, b]), [ra, rb], [0, 0], eye, z, z, [0, 0], MAT, prev)
+        if case['state'] == 0:
+            assert out['key'].shape[0] == 0
+            continue
+        assert out['key'].shape[0] == 1
+        st = case['state']
+        assert out['master'][0] == (1 if st == 1 else 0)
+        assert _same_bits(out['base'][0, 6:9], _unhex(case['normal'])) and _same_bits(out['gap'], _unhex(case['gap']))
+        assert _same_bits(out['point'][0], _unhex(case['twopnt'] if st == 1 else case['onepnt']))
+
+
+def test_oracle_convex_sphere_matches_golden_gobjcontact():
+    """Each convex-sphere case of the fixture (convex or sphere first, detect
+    or update, centres near faces, edges and inside) gives the oracle's contact
+    bit for bit: normal, gap, master point, and the convex point."""
+    eye = np.tile(np.eye(3).reshape(9), (2, 1))
+    z = np.zeros((2, 3))
+    for case in _golden()['convex_sphere']:
+        ver = _unhex(case['ver']).reshape(-1, 3)
+        fac = np.array(case['fac'], np.int32)
+        surf = np.array(case['surf'], np.int32)
+        c, r = _unhex(case['c']), _unhex(case['r'])[0]
+        cv = dict(body=[1], vptr=[0, ver.shape[0]], vert=ver, fptr=[0, fac.shape[0]], fac=fac, sptr=[0, surf.shape[0]],
+                  surf=surf)
+        mat = np.zeros((16, 16, 2))
+        out = oracle.detect_spheres([0], c[None], [r], [3], eye, z, z, [0, 1], mat, None, convex=cv)
+        if case['state'] == 0:
+            assert out['key'].shape[0] == 0
+            continue
+        assert out['key'].shape[0] == 1 and out['master'][0] == 0 and out['slave'][0] == 1
+        mpt, cpt = (case['onepnt'], case['twopnt']) if case['sphere_first'] else (case['twopnt'], case['onepnt'])
+        assert _same_bits(out['base'][0, 6:9], _unhex(case['normal'])) and _same_bits(out['gap'], _unhex(case['gap']))
+        assert _same_bits(out['point'][0], _unhex(mpt))
+        assert _same_bits(out['spnt'][0], _unhex(cpt))   # referential = spatial here
