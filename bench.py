@@ -367,7 +367,10 @@ def detect_timing(grid=DETECT_GRID):
         ms = float(np.median(ts)) * 1e3
         nb = DETECT_BYTES_SPHERE * s.nsph + DETECT_BYTES_CONTACT * s.ncon
         peak = _peaks()[0]
-        cpu = detect_cpu_baseline()
+        try:
+            cpu = detect_cpu_baseline()
+        except Exception as e:  # the reference build is test infrastructure: its absence costs only this figure
+            cpu = {'error': str(e)[:200]}
         return {'workload': 'spheres-grid-%d: %d^3 spheres, pitch 0.0999, radius 0.05' % (s.nsph, grid),
                 'spheres': s.nsph, 'contacts': int(s.ncon), 'new_first_call': int(nn),
                 'first_call_ms': round(first * 1e3, 3), 'update_call_ms': round(ms, 3),
