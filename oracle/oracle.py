@@ -41,6 +41,9 @@ def _load(name):
         lib.ref_gobj_sphere_sphere.restype = C.c_int
         lib.ref_gobj_sphere_sphere.argtypes = [C.c_int, _dp, C.c_double, C.c_int, _dp, C.c_double, C.c_int,
                                                _dp, _dp, _dp, _dp, _ip]
+        lib.ref_gobj_convex_convex.restype = C.c_int
+        lib.ref_gobj_convex_convex.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _ip, _ip, C.c_int, _dp, C.c_int, _ip,
+                                               _ip, _dp, _dp, _dp, _dp, _dp, _ip]
         lib.ref_detect_spheres_hybrid.restype = C.c_longlong
         lib.ref_detect_spheres_hybrid.argtypes = [C.c_int, _dp, _dp, _ip, C.c_void_p, C.c_longlong]
         lib.ref_gobj_convex_sphere.restype = C.c_int
@@ -402,3 +405,18 @@ def ref_detect_spheres_hybrid(centre, radius, body, pairs=False):
         out = np.zeros(m, np.int64)
         m = int(lib.ref_detect_spheres_hybrid(*args, out.ctypes.data_as(C.c_void_p), m))
     return out[:m]
+
+
+def ref_gobj_convex_convex(va, fa, sa, vb, fb, sb, update=False):
+    """gobjcontact of the reference for two convexes (detect_convex_convex,
+    goc.c:280-306): (state, onepnt, twopnt, normal, gap, area, spair)."""
+    lib = _load('geo')
+    va = np.ascontiguousarray(va, dtype=np.float64).reshape(-1)
+    vb = np.ascontiguousarray(vb, dtype=np.float64).reshape(-1)
+    fa, fb = np.ascontiguousarray(fa, dtype=np.int32), np.ascontiguousarray(fb, dtype=np.int32)
+    sa, sb = np.ascontiguousarray(sa, dtype=np.int32), np.ascontiguousarray(sb, dtype=np.int32)
+    one, two, nrm, gap, area, sp = (np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(1), np.zeros(1),
+                                    np.zeros(2, np.int32))
+    st = lib.ref_gobj_convex_convex(int(update), va.shape[0] // 3, va, sa.shape[0], fa, sa, vb.shape[0] // 3, vb,
+                                    sb.shape[0], fb, sb, one, two, nrm, gap, area, sp)
+    return st, one, two, nrm, gap[0], area[0], sp

@@ -68,6 +68,26 @@ int ref_gobj_convex_sphere (int action, int sphere_first, int nver, const double
   return state;
 }
 
+/* two convexes (vertices, faces as count then vertex indices, surface per face):
+ * gobjcontact for AABB_CONVEX_CONVEX (detect_convex_convex, goc.c:280-306, or
+ * update_convex_convex): state, points, normal, gap, area and surface pair */
+int ref_gobj_convex_convex (int action, int nva, const double *va, int nfa, const int *fa, const int *sa,
+                            int nvb, const double *vb, int nfb, const int *fb, const int *sb,
+                            double *onepnt, double *twopnt, double *normal, double *gap, double *area, int *spair)
+{
+  CONVEX *a = CONVEX_Create (NULL, (double *) va, nva, (int *) fa, nfa, (int *) sa, 0);
+  CONVEX *b = CONVEX_Create (NULL, (double *) vb, nvb, (int *) fb, nfb, (int *) sb, 0);
+  TRI *tri = NULL;
+  int ntri = 0, state;
+  *area = 0.0;
+  state = gobjcontact (action ? CONTACT_UPDATE : CONTACT_DETECT, AABB_CONVEX_CONVEX, NULL, a, NULL, b,
+                       onepnt, twopnt, normal, gap, area, spair, &tri, &ntri);
+  free (tri);
+  CONVEX_Destroy (a);
+  CONVEX_Destroy (b);
+  return state;
+}
+
 /* ---- the reference's CPU detection of a sphere set: its hybrid broad phase
  * (hyb.c:317) over the spheres' boxes (SPHERE_Extents, sph.c:240-252) and
  * detect_sphere_sphere (gobjcontact) for every overlap of spheres of different
