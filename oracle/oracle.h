@@ -124,6 +124,10 @@ int orc_detect_spheres (int nsph, const int *sbody, const double *sref, const do
  * vertices a[3 na], nearest hull point q. */
 double orc_gjk_convex_point (const double *a, int na, const double *p, double *q);
 
+/* gjk (gjk.c:340-391): distance of the hulls of two vertex sets, nearest points
+ * p (on a) and q (on b). */
+double orc_gjk_polytopes (const double *a, int na, const double *b, int nb, double *p, double *q);
+
 /* computeplanes (cvx.c:72-89) with CONVEX_Planes' layout (cvx.c:1412-1427):
  * per face its unit normal and its first vertex, pla[6 nfac]. */
 void orc_convex_planes (int nfac, const int *fac, const double *cur, double *pla);

@@ -222,6 +222,8 @@ def _detect_sigs(lib):
                                         _lp, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip])
     lib.orc_gjk_convex_point.restype = C.c_double
     lib.orc_gjk_convex_point.argtypes = [_dp, C.c_int, _dp, _dp]
+    lib.orc_gjk_polytopes.restype = C.c_double
+    lib.orc_gjk_polytopes.argtypes = [_dp, C.c_int, _dp, C.c_int, _dp, _dp]
     lib.orc_convex_planes.restype = None
     lib.orc_convex_planes.argtypes = [C.c_int, _ip, _dp, _dp]
     lib.orc_detect.restype = C.c_int
@@ -260,6 +262,24 @@ def gjk_convex_point(a, p, which='oracle'):
     q = np.zeros(3)
     d = f(a, a.shape[0] // 3, np.ascontiguousarray(p, dtype=np.float64), q)
     return d, q
+
+
+def gjk_polytopes(a, b, which='oracle'):
+    """(distance, p, q) of gjk for two vertex sets: the restatement, or the
+    reference's gjk.c compiled into _ref (which='ref')."""
+    lib = _load(which)
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1)
+    if which == 'oracle':
+        _detect_sigs(lib)
+        f = lib.orc_gjk_polytopes
+    else:
+        f = lib.gjk
+        f.restype = C.c_double
+        f.argtypes = [_dp, C.c_int, _dp, C.c_int, _dp, _dp]
+    p, q = np.zeros(3), np.zeros(3)
+    d = f(a, a.shape[0] // 3, b, b.shape[0] // 3, p, q)
+    return d, p, q
 
 
 def convex_planes(fac, cur):

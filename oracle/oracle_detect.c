@@ -84,7 +84,7 @@ double orc_gjk_sphere_sphere (const double *a, double ra, const double *b, doubl
  * the first whose barycentric weights (delta) are positive on its members and
  * non-positive off them gives the projection of the origin. */
 
-typedef struct { double w[3]; const double *a; } simplex_pt;
+typedef struct { double w[3]; const double *a, *b; } simplex_pt;
 
 /* sub-simplex masks in the order they are tried (bit i = simplex vertex i) and
  * how many of them a simplex of n vertices tries */
@@ -202,6 +202,62 @@ double orc_gjk_convex_point (const double *a, int na, const double *p, double *q
       for (int c = 0; c < 3; c++) q[c] = q[c] + l[n] * w[n].a[c];
   }
   else { q[0] = a[0]; q[1] = a[1]; q[2] = a[2]; }
+  return vlen;
+}
+
+/* gjk (gjk.c:340-391): distance of two polytopes (vertex sets a, b) and their
+ * nearest points p in a and q in b; the support points are the first vertex
+ * with the smallest (a) or largest (b) projection on the search direction */
+double orc_gjk_polytopes (const double *a, int na, const double *b, int nb, double *p, double *q)
+{
+  simplex_pt w[4];
+  double v[3], vlen, delta, mi = 0.0, l[4];
+  int toofar = 1, n = 0, j = 0;
+  const int k = (na + nb) * (na + nb);
+  v[0] = a[0] - b[0]; v[1] = a[1] - b[1]; v[2] = a[2] - b[2];
+  vlen = sqrt (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  while (toofar && vlen > GEPS && n < 4 && j++ < k)
+  {
+    double dmin = DBL_MAX, dmax = -DBL_MAX;
+    const double *sa = NULL, *sb = NULL;
+    for (int t = 0; t < na; t++)
+    {
+      const double *c = a + 3 * t, d = c[0] * v[0] + c[1] * v[1] + c[2] * v[2];
+      if (d < dmin) { dmin = d; sa = c; }
+    }
+    for (int t = 0; t < nb; t++)
+    {
+      const double *c = b + 3 * t, d = c[0] * v[0] + c[1] * v[1] + c[2] * v[2];
+      if (d > dmax) { dmax = d; sb = c; }
+    }
+    w[n].a = sa;
+    w[n].b = sb;
+    w[n].w[0] = sa[0] - sb[0]; w[n].w[1] = sa[1] - sb[1]; w[n].w[2] = sa[2] - sb[2];
+    delta = (v[0] * w[n].w[0] + v[1] * w[n].w[1] + v[2] * w[n].w[2]) / vlen;
+    mi = mi > delta ? mi : delta;
+    toofar = (vlen - mi) > GEPS;
+    if (toofar)
+    {
+      n = johnson (w, n + 1, l, v);
+      vlen = sqrt (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    }
+  }
+  if (n)
+  {
+    p[0] = p[1] = p[2] = 0.0;
+    q[0] = q[1] = q[2] = 0.0;
+    for (n--; n >= 0; n--)
+      for (int c = 0; c < 3; c++)
+      {
+        p[c] = p[c] + l[n] * w[n].a[c];
+        q[c] = q[c] + l[n] * w[n].b[c];
+      }
+  }
+  else
+  {
+    p[0] = a[0]; p[1] = a[1]; p[2] = a[2];
+    q[0] = b[0]; q[1] = b[1]; q[2] = b[2];
+  }
   return vlen;
 }
 

@@ -418,3 +418,21 @@ def test_oracle_convex_sphere_matches_golden_gobjcontact():
         assert _same_bits(out['base'][0, 6:9], _unhex(case['normal'])) and _same_bits(out['gap'], _unhex(case['gap']))
         assert _same_bits(out['point'][0], _unhex(mpt))
         assert _same_bits(out['spnt'][0], _unhex(cpt))   # referential = spatial here
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason='reference build unavailable')
+def test_gjk_polytopes_pinned_to_reference():
+    """gjk of two polytopes (the first step of the reference's convex-convex
+    intersection, cvi.c:131) restated bit for bit: separated, touching and
+    overlapping pairs of perturbed, rotated hexahedra."""
+    rng = np.random.default_rng(13)
+    base = np.array([[x, y, z] for x in (0, 1) for y in (0, 1) for z in (0, 1)], float)
+    for t in range(2000):
+        def hexa():
+            h = base * rng.uniform(0.2, 2, 3) + rng.normal(size=(8, 3)) * 0.05
+            return h @ np.linalg.qr(rng.normal(size=(3, 3)))[0].T
+        a, b = hexa(), hexa()
+        b += a.mean(0) - b.mean(0) + rng.normal(size=3) * [0.3, 1.0, 3.0][t % 3]
+        d1, p1, q1 = oracle.gjk_polytopes(a, b, 'oracle')
+        d2, p2, q2 = oracle.gjk_polytopes(a, b, 'ref')
+        assert _bits([d1]) == _bits([d2]) and np.array_equal(_bits(p1), _bits(p2)) and np.array_equal(_bits(q1), _bits(q2))
