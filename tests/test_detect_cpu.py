@@ -436,3 +436,19 @@ def test_gjk_polytopes_pinned_to_reference():
         d1, p1, q1 = oracle.gjk_polytopes(a, b, 'oracle')
         d2, p2, q2 = oracle.gjk_polytopes(a, b, 'ref')
         assert _bits([d1]) == _bits([d2]) and np.array_equal(_bits(p1), _bits(p2)) and np.array_equal(_bits(q1), _bits(q2))
+
+
+def test_clumps_of_spheres():
+    """Bodies made of several spheres (clumps): spheres of one body never touch
+    each other (box.c:107-108), and two bodies touching through two sphere
+    pairs get two contacts between the same bodies."""
+    nb = 2
+    rot = np.tile(np.eye(3).reshape(9), (nb, 1))
+    # body 0: spheres at x = 0 and x = 0.9 (overlapping each other); body 1: the same shifted up by 0.95
+    sref = np.array([[0, 0, 0], [0.9, 0, 0], [0, 0, 0.95], [0.9, 0, 0.95]], float)
+    out = oracle.detect_spheres([0, 0, 1, 1], sref, np.full(4, 0.5), np.zeros(4, np.int32), rot, np.zeros((2, 3)),
+                                np.zeros((2, 3)), np.zeros(2, np.int32), MAT)
+    pairs = [(int(k >> 32), int(k & 0xFFFFFFFF)) for k in out['key']]
+    assert (0, 1) not in pairs and (2, 3) not in pairs
+    assert (0, 2) in pairs and (1, 3) in pairs
+    assert set(zip(out['master'].tolist(), out['slave'].tolist())) <= {(0, 1), (1, 0)}
