@@ -23,6 +23,7 @@
 #include "fem.h"
 #include "mat.h"
 #include "hyb.h"
+#include "ext/predicates.h"
 
 /* action: 0 CONTACT_DETECT, 1 CONTACT_UPDATE; sphere a is the first object */
 int ref_gobj_sphere_sphere (int action, const double *ca, double ra, int sa, const double *cb, double rb, int sb,
@@ -68,6 +69,14 @@ int ref_gobj_convex_sphere (int action, int sphere_first, int nver, const double
   return state;
 }
 
+/* the reference initialises the robust predicates once at start-up
+ * (solfec.c:295); the hull of the convex-convex path depends on them */
+static void predicates_ready (void)
+{
+  static int done = 0;
+  if (!done) { exactinit (); done = 1; }
+}
+
 /* two convexes (vertices, faces as count then vertex indices, surface per face):
  * gobjcontact for AABB_CONVEX_CONVEX (detect_convex_convex, goc.c:280-306, or
  * update_convex_convex): state, points, normal, gap, area and surface pair */
@@ -75,6 +84,7 @@ int ref_gobj_convex_convex (int action, int nva, const double *va, int nfa, cons
                             int nvb, const double *vb, int nfb, const int *fb, const int *sb,
                             double *onepnt, double *twopnt, double *normal, double *gap, double *area, int *spair)
 {
+  predicates_ready ();
   CONVEX *a = CONVEX_Create (NULL, (double *) va, nva, (int *) fa, nfa, (int *) sa, 0);
   CONVEX *b = CONVEX_Create (NULL, (double *) vb, nvb, (int *) fb, nfb, (int *) sb, 0);
   TRI *tri = NULL;
