@@ -120,10 +120,12 @@ int b2dev_rigid_get(b2dev_ctx* ctx, double* rot, double* x, double* velo, double
  *     where the spheres separated; every other pair of spheres of different
  *     bodies, not both obstacles, whose gap (gjk.c:560-584) is below
  *     GEOMETRIC_EPSILON becomes a new contact (detect_sphere_sphere,
- *     goc.c:421-456; insert_contact, dom.c:315-330); new contacts with a
+ *     goc.c:421-456; insert_contact, dom.c:315-330), and so does every sphere
+ *     within r + GEOMETRIC_EPSILON of a convex of b2dev_convexes_setup
+ *     (detect_convex_sphere, goc.c:308-349); new contacts with a
  *     duplicate point are removed (sparsify_contacts, dom.c:2956-3054). The
- *     result replaces the scene's contacts, listed by sphere pair (i < j)
- *     ascending; *ncon and *nnew (either may be NULL) receive the number of
+ *     result replaces the scene's contacts, listed by pair (sphere i, then its
+ *     partner j > i, a convex c counting as nsph + c) ascending; *ncon and *nnew (either may be NULL) receive the number of
  *     contacts and of new ones. Updated contacts carry their R and U from the
  *     last solve, new ones start from zero.
  *   b2dev_detect_carry_state: after b2dev_assemble of the detected contacts,
