@@ -63,7 +63,7 @@ WORKLOAD = 'hexahedra-100k: 100x100x10 perturbed rigid hexahedra (side 0.04 m, +
 BYTES_BLOCK = {'fp64': 100, 'mixed': 52}
 BYTES_ROW = {'fp64': 316, 'mixed': 328}
 # DRAM bytes (read + write) per algorithmic byte of k_solve, measured by ncu on the 100x100x6 lattice
-# (profiles/k_solve_hexahedra100k.md); DRAM traffic grows in proportion to blocks, rows and passes
+# (one --set full capture per precision); DRAM traffic grows in proportion to blocks, rows and passes
 TRAFFIC_RATIO = {'fp64': 1178.1 / 1363.6, 'mixed': 647.1 / 739.2}
 
 

@@ -213,7 +213,10 @@ int b2dev_get_trace(b2dev_ctx* ctx, double* out);
  * timeout flag, colour-overflow flag, number of colours, rounds). n above the
  * maximum is rejected with B2DEV_EINVAL before anything is queued.
  * The first call on a device looks up the array's device address and the
- * kernel's residency; make that first call before any stream capture. Every
+ * kernel's residency; make that first call before any stream capture. That
+ * set-up is kept for the life of the process: a cudaDeviceReset of the device
+ * afterwards invalidates it, so a process that resets a device must not call
+ * this entry point for that device again. Every
  * call shares the one array, so calls whose work overlaps on the GPU (other
  * streams, other threads) race: queue them on one stream or serialise them. */
 int b2dev_colour_noalloc(int device, void* stream, int n, const int* adjptr, const int* adjcol, uint64_t seed,

@@ -18,7 +18,7 @@
  * (con->R, con->U, con->merit, dom->merit; dom.h:79-92).
  *
  * The structs here are flat arrays (no linked lists); a Solfec build binds
- * them by walking its LOCDYN/DOM lists once per step (see INTEGRATION.md).
+ * them by walking its LOCDYN/DOM lists once per step.
  * Only CONTACT constraints with SIGNORINI_COULOMB materials on RIG/OBS bodies
  * are on this path; anything else is rejected with B2GS_EUNSUPPORTED.
  */
@@ -118,6 +118,7 @@ void b2gs_set_precision (b2gs_solver *gs, int precision);
 void b2gs_set_grid (b2gs_solver *gs, int blocks);      /* persistent grid size (0 = automatic) */
 void b2gs_set_stage_blocks (b2gs_solver *gs, int blocks); /* staging window per warp (0 = automatic) */
 /* device options of the next solve (b2dev_solve_opts of b2_device.h), e.g. for b2dev_solve_batch */
+struct b2dev_solve_opts;
 int b2gs_get_opts (b2gs_solver *gs, struct b2dev_solve_opts *opts);
 int b2gs_get_iters_mixed (b2gs_solver *gs);           /* FP32 iterations of the last mixed solve */
 double b2gs_get_solve_ms (b2gs_solver *gs);           /* device time of the last solve */

@@ -77,7 +77,7 @@ def _load(name):
 
 
 def ref_available() -> bool:
-    return os.path.exists(os.path.join(HERE, '_ref/libref_bgs.so')) or os.path.isdir('/root/reference')
+    return os.path.exists(os.path.join(HERE, '_ref/libref_bgs.so'))
 
 
 class LocalDynamics:
@@ -379,7 +379,7 @@ def detect_spheres(sbody, sref, radius, surface, rot, x, x0, obstacle, material,
 # ---------------------------------------------------------------- the reference's own contact geometry
 
 def geo_available() -> bool:
-    return os.path.exists(os.path.join(HERE, '_ref/libref_geo.so')) or os.path.isdir('/root/reference')
+    return os.path.exists(os.path.join(HERE, '_ref/libref_geo.so'))
 
 
 def ref_gobj_sphere_sphere(ca, ra, sa, cb, rb, sb, update=False):

@@ -448,6 +448,16 @@ __global__ void k_add_counts(int n, const int* a, int* b) {
   if (i < n) b[i] += a[i];
 }
 
+// Sum of the per-sphere pair counts in 64 bits (the scan that follows runs in
+// int, so the host checks this total first): one atomic per warp.
+__global__ void k_count_total(int n, const int* cnt, unsigned long long* total) {
+  unsigned long long s = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += (unsigned)cnt[i];
+#pragma unroll
+  for (int d = 16; d >= 1; d >>= 1) s += __shfl_down_sync(0xffffffffu, s, d);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(total, s);
+}
+
 __global__ void k_sph_sort_seg(int nsph, const int* off, int* pj, int* pi) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsph) return;

@@ -204,7 +204,7 @@ struct b2dev_ctx {
   int nsph = 0, nsurf = 0;
   std::vector<double> sph_mat_h;
   Buf sph_body, sph_ref, sph_rad, sph_surf, sph_mat, sph_cur, sph_cell, sph_hkey, sph_hkey_s, sph_idx, sph_sorted,
-      sph_bstart, sph_bend, sph_cnt, sph_off, sph_pi, sph_pj, sph_rmax, sph_keep, sph_pos, sph_bcnt, sph_bptr,
+      sph_bstart, sph_bend, sph_cnt, sph_off, sph_pi, sph_pj, sph_rmax, sph_total, sph_keep, sph_pos, sph_bcnt, sph_bptr,
       sph_blist, sph_pkey, sph_pslo, sph_pR, sph_pU, sph_ccnt;
   Buf st_master, st_slave, st_point, st_mpnt, st_spnt, st_base, st_gap, st_fric, st_rest, st_coh, st_R0, st_U0,
       st_key, st_slo, st_new;
@@ -828,7 +828,17 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->R64[0], &c->R64[1], &c->R64[2], &c->R32[0], &c->R32[1], &c->R32[2], &c->Us[0], &c->Us[1],
                 &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tilek, &c->rtile, &c->dcnt, &c->depE_ptr, &c->depL_ptr, &c->depE, &c->depL, &c->tile_done, &c->rb_x, &c->rb_J, &c->rb_mass, &c->rb_scheme, &c->rb_fext, &c->rb_aux, &c->rb_loads, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec, &c->gptr_prev, &c->gcol_prev,
                 &c->part, &c->rer,
-                &c->mer, &c->failkey, &c->failcount, &c->sctrl, &c->io, &c->cub_tmp, &c->trace};
+                &c->mer, &c->failkey, &c->failcount, &c->sctrl, &c->io, &c->cub_tmp, &c->trace,
+                // contact detection: spheres, grid, pairs, staged and detected contacts, convexes
+                &c->sph_body, &c->sph_ref, &c->sph_rad, &c->sph_surf, &c->sph_mat, &c->sph_cur, &c->sph_cell,
+                &c->sph_hkey, &c->sph_hkey_s, &c->sph_idx, &c->sph_sorted, &c->sph_bstart, &c->sph_bend,
+                &c->sph_cnt, &c->sph_off, &c->sph_pi, &c->sph_pj, &c->sph_rmax, &c->sph_total, &c->sph_keep,
+                &c->sph_pos, &c->sph_bcnt, &c->sph_bptr, &c->sph_blist, &c->sph_pkey, &c->sph_pslo, &c->sph_pR,
+                &c->sph_pU, &c->sph_ccnt, &c->st_master, &c->st_slave, &c->st_point, &c->st_mpnt, &c->st_spnt,
+                &c->st_base, &c->st_gap, &c->st_fric, &c->st_rest, &c->st_coh, &c->st_R0, &c->st_U0, &c->st_key,
+                &c->st_slo, &c->st_new, &c->det_point, &c->det_R0, &c->det_U0, &c->det_key, &c->det_slo,
+                &c->det_new, &c->cvx_body, &c->cvx_vptr, &c->cvx_vert, &c->cvx_fptr, &c->cvx_fac, &c->cvx_sptr,
+                &c->cvx_surf, &c->cvx_ns, &c->cvx_cur, &c->cvx_pla, &c->cvx_box};
   for (Buf* b : all)
     if (b->p) cudaFree(b->p);
   if (c->graph) cudaGraphExecDestroy(c->graph);
@@ -1360,11 +1370,25 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
       k_add_counts<<<blocks_for(ns, T), T, 0, st>>>(ns, ptr<int>(c->sph_cnt), ptr<int>(c->sph_ccnt));
       pair_count = ptr<int>(c->sph_ccnt);
     }
-    B2_TRY(scan_exclusive(c, pair_count, ptr<int>(c->sph_off), ns + 1));
-    B2_CK(cudaMemcpyAsync(&npair, ptr<int>(c->sph_off) + ns, sizeof(int), cudaMemcpyDeviceToHost, st));
+    // the pair total in 64 bits before the int scan: offsets, pair indices and
+    // the body lists (two entries per contact) are int
+    unsigned long long total = 0;
+    B2_TRY(ensure(c->sph_total, sizeof(unsigned long long)));
+    B2_CK(cudaMemsetAsync(c->sph_total.p, 0, sizeof(unsigned long long), st));
+    c->launches++;
+    k_count_total<<<std::min(blocks_for(ns, T), 4 * c->sms), T, 0, st>>>(ns, pair_count,
+                                                                         ptr<unsigned long long>(c->sph_total));
+    B2_CK(cudaMemcpyAsync(&total, c->sph_total.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     B2_CK(cudaMemcpyAsync(&bad, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     B2_CK(cudaStreamSynchronize(st));
     if (bad) { set_err("detect: %s", detect_bad_text(bad)); return B2DEV_EINVAL; }
+    if (total > (unsigned long long)(INT_MAX / 2 - 1)) {
+      set_err("detect: %llu candidate pairs exceed the supported %d", total, INT_MAX / 2 - 1);
+      return B2DEV_EINVAL;
+    }
+    B2_TRY(scan_exclusive(c, pair_count, ptr<int>(c->sph_off), ns + 1));
+    B2_CK(cudaMemcpyAsync(&npair, ptr<int>(c->sph_off) + ns, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaStreamSynchronize(st));
   }
 
   // contacts of the pairs, in pair order

@@ -2,19 +2,21 @@
 fixtures: tests/block-sliding.py:64-80 (position x and velocity v_x of the
 block at given callback indices, 1e-3 relative tolerance) into
 block_sliding_ref.json, and tests/projectile.py:47-50 (the x distance in
-inches at the end, 0.5% relative tolerance) into projectile_ref.json. Run in
-a container where the reference sources are at REFERENCE (default
-/root/reference); the tests read only the JSON."""
+inches at the end, 0.5% relative tolerance) into projectile_ref.json. Run with
+the environment variable REFERENCE set to the reference source tree; the
+tests read only the JSON."""
 import ast
 import json
 import os
 import re
 import sys
 
-REFERENCE = os.environ.get('REFERENCE', '/root/reference')
+REFERENCE = os.environ.get('REFERENCE')
 
 
 def main():
+    if not REFERENCE or not os.path.isdir(REFERENCE):
+        sys.exit('set REFERENCE to the reference source tree')
     src = open(os.path.join(REFERENCE, 'tests', 'block-sliding.py')).read()
     m = re.search(r'REF\s*=\s*(\[[^\]]*\])', src)  # the test is Python 2: read the list literal alone
     if not m:

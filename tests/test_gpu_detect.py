@@ -225,3 +225,56 @@ def test_box_time_loop_matches_oracle_every_step():
     assert walls >= 16   # the lowest layer rests on the floor
     assert np.all(dyn.state()['x'][:sp['body'].shape[0], 2] > 0.04)
     ldy.close()
+
+
+def _clump_scene(offsets0, offsets1, dz):
+    """spheres_on_bed with bodies 0 and 1 made clumps (several spheres each,
+    at the given offsets from the body's centre) and body 1 placed dz above
+    body 0; every rotation the identity, so referential and current centres
+    agree. Bodies 2 and 3 carry no shapes; the bed spheres keep theirs."""
+    sc, sp, J, mass = scenes.spheres_on_bed(seed=7, n_side=2, layers=1)
+    nb = sc.nbod
+    x = sc.x.copy()
+    x[1] = x[0] + np.array([0.0, 0.0, dz])
+    sc = dataclasses.replace(sc, rot=np.tile(np.eye(3).reshape(9), (nb, 1)), x=x, x0=x.copy())
+    o0, o1 = np.asarray(offsets0, float), np.asarray(offsets1, float)
+    bed = np.arange(4, nb)
+    body = np.concatenate([np.zeros(len(o0)), np.ones(len(o1)), bed]).astype(np.int32)
+    centre = np.concatenate([x[0] + o0, x[1] + o1, x[bed]])
+    radius = np.concatenate([np.full(len(o0) + len(o1), 0.05), sp['radius'][bed]])
+    sp = dict(sp, body=body, centre=centre, radius=radius, surface=np.zeros(body.shape[0], np.int32))
+    return sc, sp, J, mass
+
+
+@pytest.mark.parametrize('variant', ['two_contacts', 'duplicate_points'])
+def test_clumps_match_oracle(variant):
+    """Bodies made of several spheres: spheres of one body never touch each
+    other (box.c:107-108); two bodies touching through two sphere pairs get
+    two contacts between the same bodies; when those two contact points lie
+    within 2 mindist of each other the sparsification removes one (the
+    compaction path; otherwise the staged arrays are taken over). Every array
+    equals the oracle's bit for bit."""
+    if variant == 'two_contacts':  # overlapping spheres inside each body, two body-to-body contacts
+        sc, sp, J, mass = _clump_scene([[0, 0, 0], [-0.09, 0, 0]], [[0, 0, 0], [-0.09, 0, 0]], 0.099)
+    else:                          # body 0's two spheres 1e-7 apart: duplicate contact points with body 1
+        sc, sp, J, mass = _clump_scene([[0, 0, 0], [1e-7, 0, 0]], [[0, 0, 0]], 0.099)
+    ldy = _setup(sc, J, mass)
+    s = SPHERES(ldy, **sp)
+    nc, nn = s.detect()
+    dev = s.contacts()
+    orc = _oracle(sp, sc.rot, sc.x, sc.x0, sc.obstacle)
+    _same(dev, orc)
+    body = sp['body']
+    pi, pj = dev['key'] >> 32, dev['key'] & 0xFFFFFFFF
+    assert not np.any(body[pi] == body[pj])                       # no contact inside a clump
+    assert set(zip(dev['master'].tolist(), dev['slave'].tolist())) <= {(0, 1), (1, 0)}
+    if variant == 'two_contacts':
+        assert nc == nn == 2 and pi.tolist() == [0, 1] and pj.tolist() == [2, 3]
+    else:
+        assert nc == nn == 1                                      # of two touching pairs, one contact is kept
+    # a second detection updates the kept contacts with their roles
+    nc2, nn2 = s.detect()
+    assert nc2 == nc and nn2 == 0
+    _same(s.contacts(), _oracle(sp, sc.rot, sc.x, sc.x0, sc.obstacle,
+                                dict(key=dev['key'], slave_lo=dev['slave_lo'])))
+    ldy.close()
