@@ -1,21 +1,30 @@
 """Benchmark of the B200 contact-solve path (one JSON line on rank 0).
 
 Workload: the 100,000-body perturbed-hexahedra scene (rigid convex hexahedra,
-side 0.04 m, vertices +-10%, density 2000, friction 0.4, h = 5e-4), one
-contact step = LOCDYN_Update_Begin (W_ii, rho, A, B, V, W_ij, colouring,
-colour-sorted layout) + GAUSS_SEIDEL_Solve to merit 1e-4 (meritval 1e-4 with
+side 0.04 m, vertices +-10%, density 2000, friction 0.4, h = 5e-4) in a time
+loop from rest under gravity, all on the device: every step is
+BODY_Dynamic_Step_Begin, LOCDYN_Update_Begin on the device bodies (W_ii, rho,
+A, B, V, W_ij, colouring reused while the contact graph is unchanged,
+colour-sorted layout), GAUSS_SEIDEL_Solve to merit 1e-4 (meritval 1e-4 with
 the relative-error test non-binding, epsilon = 1; maxiter 1000,
-SEMISMOOTH_NEWTON), warm-started from the reactions of the previous step, as
-a time-stepping run does.
+SEMISMOOTH_NEWTON) warm-started from the previous step's reactions, and
+BODY_Dynamic_Step_End. W steps run untimed, then K consecutive steps are
+timed (each a different step of the run).
 
-`value` is the per-step time of the product mode named by the metric: mixed
-precision (FP32 off-diagonal sweeps, FP64 diagonal solves / merit / closing
-refinement) started from the learned warm start (BF16 network on the tensor
-cores, kept only when its merit is below the previous-step start's), with all
-inputs resident in HBM; the plain FP64 and plain mixed modes are reported
-beside it. `e2e` is the same step through the C ABI with host (pinned)
-buffers: scene upload, assembly, warm-start upload, network start, solve and
-the read-back of R, U and the per-contact merit.
+`value` is the per-step time of the mixed-precision mode (FP32 off-diagonal
+sweeps, FP64 diagonal solves / merit / closing refinement) with the learned
+warm start (BF16 network on the tensor cores, kept only when its merit is
+below the previous-step start's), inputs resident in HBM; the plain FP64 and
+plain mixed modes, and both with the reference's own stopping rule
+(epsilon = meritval = 1e-4), are reported beside it, with the iterations of
+every timed step. `e2e` replays the same steps through the C ABI from pinned
+host buffers: each step's bodies and contacts and the previous result
+uploaded, assembly, learned warm start, solve, and the read-back of R, U and
+the per-contact merit. `mixed_vs_fp64_converged` compares mixed precision and
+FP64 run to merit 1e-7 on the last step's local dynamics. The configs key
+(single-GPU runs) carries per-step times of configs 1 and 2 (device time
+loops of the settled sphere packings) and the batched config 4, whose scenes
+a spawned process generates on the host meanwhile.
 
 --workload batched runs the batched workload instead: 256 independent uneven
 sphere scenes (bodies log-uniform in [50, 2000], radius U[0.02, 0.05],
@@ -154,32 +163,58 @@ class ClockSampler:
                 'reasons': sorted(reasons), 'samples': len(sm)}
 
 
-def make_step_inputs(rank):
-    """Scene of the timed step and the warm start from the previous step.
-    The previous step is solved once (FP64, untimed) and the bodies advanced
-    by one velocity step with its reactions."""
-    from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN, scenes
-    sc0 = scenes.hexahedra_lattice(seed=replica_seed(rank), **SCENE)
-    ldy = LOCDYN()
-    ldy.update_begin(sc0)
-    gs = GAUSS_SEIDEL_SOLVER(**SOLVE)
-    gs.solve(ldy)
-    R0, U0, _ = ldy.get_state()
-    sc1 = scenes.advance_velocities(sc0, R0)
-    ldy.close()
-    return sc1, R0, U0, gs.iters
+# the time loop of the bench: gravity on every body, the scene's contacts kept
+# (referential points, frames, gaps, materials), the reactions of each step
+# the warm start of the next, as in a time-stepping run of the reference
+STEP_GRAVITY = (0.0, 0.0, -9.81)
+# the reference's own stopping rule at the metric's tolerance (reported beside the merit-decided modes)
+SOLVE_REF_RULE = dict(epsilon=1e-4, maxiter=1000, meritval=1e-4)
+# converged comparison of the mixed precision with FP64 (the stack stalls near merit 4e-8)
+CONVERGED_MERIT = 1e-7
+CONVERGED_SEED = 12345   # seeded colouring: another valid row order for the FP64 spread
+
+
+def body_resultants(rot, x, sc, R):
+    """Force and torque of the contact reactions on every moving body (global
+    frame), as rig_constraints_force (bod.c:390-439) sums them."""
+    base = sc.base.reshape(-1, 3, 3)
+    f = np.einsum('kji,kj->ki', base, R)
+    M = rot.reshape(-1, 3, 3).transpose(0, 2, 1)
+    m, s = sc.master, sc.slave
+    p = x[m] + np.einsum('kij,kj->ki', M[m], sc.mpnt - sc.x0[m])
+    F = np.zeros((sc.nbod, 3)); T = np.zeros((sc.nbod, 3))
+    np.add.at(F, m, f); np.add.at(T, m, np.cross(p - x[m], f))
+    ok = s >= 0
+    np.add.at(F, s[ok], -f[ok]); np.add.at(T, s[ok], -np.cross(p[ok] - x[s[ok]], f[ok]))
+    mov = sc.obstacle == 0
+    return F[mov], T[mov]
+
+
+def _rel2(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
 
 
 def bench_product(args, ws, rank, local):
+    """Time loop of the hexahedra scene on the device, one run per mode from
+    the same initial state (bodies at rest, zero reactions). Every step is
+    BODY_Dynamic_Step_Begin (device) -> LOCDYN_Update_Begin on the device
+    bodies -> warm start from the previous step's R, U (device) [-> learned
+    warm start] -> GAUSS_SEIDEL_Solve -> R, U kept on the device ->
+    BODY_Dynamic_Step_End (device): no host round trip of bodies or state.
+    W untimed steps, then K timed steps, each a different step of the run."""
     import torch
     import ctypes as C
-    from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN
+    from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN, learn, scenes
     from solfec_b200._lib import b2gs_bodies, b2gs_contacts, lib
+    from solfec_b200.dynamics import RIGID_DYNAMICS
 
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
-    sc, R0, U0, iters_prev = make_step_inputs(rank)
+    sc = scenes.hexahedra_lattice(seed=replica_seed(rank), **SCENE)
+    J, mass = _rigid_inertia(sc)
+    h, dflag = float(sc.step), int(sc.dynamic)
     stream = torch.cuda.current_stream()
+    n, nb = sc.ncon, sc.nbod
 
     def tens(a, dtype):
         return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype))
@@ -189,93 +224,174 @@ def bench_product(args, ws, rank, local):
             tens(sc.master, np.int32), tens(sc.slave, np.int32), tens(sc.mpnt, np.float64), tens(sc.spnt, np.float64),
             tens(sc.base, np.float64), tens(sc.gap, np.float64), tens(sc.friction, np.float64),
             tens(sc.restitution, np.float64), tens(sc.cohesion, np.float64)]
+    devt = [t.to(dev) for t in host]   # the initial scene, kept on the device for each mode's start
     pinned = [t.pin_memory() for t in host]
-    devt = [t.to(dev) for t in host]
-    Rd, Ud = tens(R0, np.float64).to(dev), tens(U0, np.float64).to(dev)
-    Rh, Uh = tens(R0, np.float64).pin_memory(), tens(U0, np.float64).pin_memory()
-    n = sc.ncon
-    Rout_h = torch.empty(3 * n, dtype=torch.float64).pin_memory()
-    Uout_h = torch.empty(3 * n, dtype=torch.float64).pin_memory()
-    Cout_h = torch.empty(n, dtype=torch.float64).pin_memory()
-    h2d_bytes = sum(t.numel() * t.element_size() for t in host) + 2 * Rh.numel() * 8
-    d2h_bytes = (Rout_h.numel() + Uout_h.numel() + Cout_h.numel()) * 8
 
     def structs(ts, on_device):
         p = [C.c_void_p(t.data_ptr()) for t in ts]
-        return (b2gs_bodies(sc.nbod, *p[:7], on_device), b2gs_contacts(sc.ncon, *p[7:], on_device))
+        return (b2gs_bodies(nb, *p[:7], on_device), b2gs_contacts(n, *p[7:], on_device))
 
     bd, cd = structs(devt, 1)
     bh, ch = structs(pinned, 0)
     ldy = LOCDYN(device=local, stream=stream.cuda_stream)
     ctx = ldy.device_context
-
-    def step_device(gs):
-        ldy.update_begin_arrays(bd, cd, sc.step, sc.dynamic)
-        ldy.set_state_ptr(C.c_void_p(Rd.data_ptr()), C.c_void_p(Ud.data_ptr()), 1)
-        gs.solve(ldy)
-
-    from solfec_b200 import learn
     net = learn.WarmStartNet.load(device=local)
-    nn_reps = []
+    Rd = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    Ud = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    rot_d = torch.empty(9 * nb, dtype=torch.float64, device=dev)
+    x_d = torch.empty(3 * nb, dtype=torch.float64, device=dev)
+    vel_d = torch.empty(6 * nb, dtype=torch.float64, device=dev)
+    vel0_d = torch.empty(6 * nb, dtype=torch.float64, device=dev)
 
-    def step_device_nn(gs):
-        ldy.update_begin_arrays(bd, cd, sc.step, sc.dynamic)
-        ldy.set_state_ptr(C.c_void_p(Rd.data_ptr()), C.c_void_p(Ud.data_ptr()), 1)
-        nn_reps.append(learn.warm_start(ldy, net))
-        gs.solve(ldy)
+    def check(rc, what):
+        if rc != 0:
+            from solfec_b200._lib import last_error
+            raise RuntimeError('%s failed: %s' % (what, last_error()))
 
-    def step_e2e(gs):
-        ldy.update_begin_arrays(bh, ch, sc.step, sc.dynamic)
-        ldy.set_state_ptr(C.c_void_p(Rh.data_ptr()), C.c_void_p(Uh.data_ptr()), 0)
-        learn.warm_start(ldy, net)
-        gs.solve(ldy)
-        ldy.get_state_ptr(C.c_void_p(Rout_h.data_ptr()), C.c_void_p(Uout_h.data_ptr()),
-                          C.c_void_p(Cout_h.data_ptr()), 0)
+    def reset():
+        ldy.update_begin_arrays(bd, cd, h, dflag)
+        Rd.zero_(); Ud.zero_()
+        return RIGID_DYNAMICS(ldy, J, mass, sc.x)
 
     def barrier():
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    def timed(fn, gs, steps, warmup):
-        for _ in range(warmup):
-            fn(gs)
+    snaps = []   # per timed step of the mixed+NN run: the bodies the assembly read and the warm start
+
+    def run(solve_kw, precision, nn, record=False):
+        dyn = reset()
+        gs = GAUSS_SEIDEL_SOLVER(**solve_kw)
+        gs.precision = precision
+        nn_reps, reps, its = [], [], []
+
+        def step(timed):
+            dyn.step_begin(h, STEP_GRAVITY)
+            check(lib().b2gs_locdyn_update_begin_resident(ldy.handle, h, dflag), 'LOCDYN update on the device bodies')
+            if record and timed:
+                check(lib().b2dev_rigid_get(ctx, C.c_void_p(rot_d.data_ptr()), None, C.c_void_p(vel_d.data_ptr()),
+                                            C.c_void_p(vel0_d.data_ptr()), 1), 'b2dev_rigid_get')
+                snaps.append([t.clone() for t in (rot_d, vel_d, vel0_d, Rd, Ud)])
+            ldy.set_state_ptr(C.c_void_p(Rd.data_ptr()), C.c_void_p(Ud.data_ptr()), 1)
+            if nn:
+                nn_reps.append(learn.warm_start(ldy, net))
+            gs.solve(ldy)
+            ldy.get_state_ptr(C.c_void_p(Rd.data_ptr()), C.c_void_p(Ud.data_ptr()), None, 1)
+            dyn.step_end(h)
+            if timed:
+                reps.append(gs.report)
+                its.append(gs.iters)
+
+        for _ in range(args.warmup):
+            step(False)
         barrier()
         l0 = lib().b2dev_launch_count(ctx)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = []
         ev0.record(stream)
-        for _ in range(steps):
-            fn(gs)
-            reps.append(gs.report)
+        for _ in range(args.steps):
+            step(True)
         ev1.record(stream)
         barrier()
-        ms = max_over_ranks(ev0.elapsed_time(ev1) / steps, dev)
-        launches = lib().b2dev_launch_count(ctx) - l0
-        return ms, reps, launches
+        ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dev)
+        check(lib().b2dev_rigid_get(ctx, C.c_void_p(rot_d.data_ptr()), C.c_void_p(x_d.data_ptr()), None, None, 1),
+              'b2dev_rigid_get')
+        return dict(ms=ms, iters=its, reps=reps, nn=nn_reps, launches=lib().b2dev_launch_count(ctx) - l0,
+                    R=Rd.cpu().numpy().reshape(-1, 3).copy(), merit=ldy.merit, error=gs.error,
+                    assemble_ms=ldy.assemble_ms,
+                    rot=rot_d.cpu().numpy().reshape(-1, 9).copy(), x=x_d.cpu().numpy().reshape(-1, 3).copy())
 
     results = {}
     with ClockSampler(local) as clk:
-        for mode in ('fp64', 'mixed', 'mixed_nn'):
-            gs = GAUSS_SEIDEL_SOLVER(**SOLVE)
-            gs.precision = 'FP64' if mode == 'fp64' else 'MIXED'
-            ms, reps, launches = timed(step_device_nn if mode == 'mixed_nn' else step_device, gs, args.steps,
-                                       args.warmup)
-            r = reps[-1]
-            results[mode] = dict(ms=ms, iters=gs.iters, iters_mixed=gs.iters_mixed, merit=ldy.merit, report=r,
-                                 launches=launches, assemble_ms=ldy.assemble_ms, error=gs.error,
-                                 R=ldy.get_state()[0])  # the last step's reactions (outside the timed region)
+        results['fp64'] = run(SOLVE, 'FP64', False)
+        results['mixed'] = run(SOLVE, 'MIXED', False)
+        results['mixed_nn'] = run(SOLVE, 'MIXED', True)
+        results['fp64_ref_rule'] = run(SOLVE_REF_RULE, 'FP64', False)
+        results['mixed_nn_ref_rule'] = run(SOLVE_REF_RULE, 'MIXED', True)
+        run(SOLVE, 'MIXED', True, record=True)   # untimed: the mixed+NN steps' inputs for the end-to-end leg
+        results['mixed_nn']['R_last'] = Rd.cpu().numpy().reshape(-1, 3).copy()
+        # end to end through the C ABI from pinned host buffers: the mixed+NN run's
+        # timed steps replayed (each step's bodies and the previous step's result
+        # uploaded, the step's R, U and per-contact merit read back)
+        Rh = torch.empty(3 * n, dtype=torch.float64).pin_memory()
+        Uh = torch.empty(3 * n, dtype=torch.float64).pin_memory()
+        Ch = torch.empty(n, dtype=torch.float64).pin_memory()
+        snaps_h = [[t.cpu().pin_memory() for t in sn] for sn in snaps]
+        # each step's host bodies: its rotations and velocities, the fixed arrays of the scene
+        step_bodies = [structs([sn[0], pinned[1], pinned[2], pinned[3], sn[1], sn[2], pinned[6]] + pinned[7:], 0)[0]
+                       for sn in snaps_h]
         gs = GAUSS_SEIDEL_SOLVER(**SOLVE)
         gs.precision = 'MIXED'
-        e2e_ms, _, _ = timed(step_e2e, gs, args.steps, args.warmup)
+        Rh.copy_(snaps_h[0][3]); Uh.copy_(snaps_h[0][4])
+
+        def e2e_step(k):
+            ldy.update_begin_arrays(step_bodies[k], ch, h, dflag)
+            ldy.set_state_ptr(C.c_void_p(Rh.data_ptr()), C.c_void_p(Uh.data_ptr()), 0)
+            learn.warm_start(ldy, net)
+            gs.solve(ldy)
+            ldy.get_state_ptr(C.c_void_p(Rh.data_ptr()), C.c_void_p(Uh.data_ptr()), C.c_void_p(Ch.data_ptr()), 0)
+
+        for k in range(min(args.warmup, len(snaps_h))):
+            e2e_step(k)
+        Rh.copy_(snaps_h[0][3]); Uh.copy_(snaps_h[0][4])
+        barrier()
+        t0 = time.perf_counter()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for k in range(len(snaps_h)):
+            e2e_step(k)
+        ev1.record(stream)
+        barrier()
+        e2e_ms = max_over_ranks(max(ev0.elapsed_time(ev1), 1e3 * (time.perf_counter() - t0)) / len(snaps_h), dev)
+    h2d = sum(t.numel() * t.element_size() for t in host) + 2 * 3 * n * 8
+    d2h = (2 * 3 * n + n) * 8
     nrows, K, ncol, fe = ldy.sizes()
+    conv = converged_comparison(ldy, results['mixed_nn'], sc, dev)
     rigid = rigid_step_timing(ldy, sc, bd, cd, stream, barrier, dev)
-    results['mixed_nn']['nn'] = nn_reps[-1] if nn_reps else None
-    results['mixed_nn']['nn_used_steps'] = sum(1 for r in nn_reps if r['used_nn'])
-    results['mixed_nn']['nn_steps'] = len(nn_reps)
     net.close()
-    return dict(results=results, e2e_ms=e2e_ms, h2d=h2d_bytes, d2h=d2h_bytes, n=nrows, K=K, ncolours=ncol,
-                clocks=clk.summary(), iters_prev=iters_prev, nbod=sc.nbod, scene=sc, R0=R0, U0=U0, rigid=rigid)
+    ldy.close()
+    return dict(results=results, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h, n=nrows, K=K, ncolours=ncol,
+                clocks=clk.summary(), nbod=sc.nbod, scene=sc, rigid=rigid, converged=conv)
+
+
+def converged_comparison(ldy, last, sc, dev):
+    """The last timed step's local dynamics (still in the context) solved to
+    merit 1e-7 from zero reactions by FP64 and by mixed precision in the same
+    row order, and by FP64 in another valid row order (seeded colouring):
+    relative 2-norm differences of the reactions, of the relative velocities
+    and of the per-body force and torque resultants. On this hyperstatic stack
+    the contact reactions are not unique; the resultants are what moves the
+    bodies."""
+    from types import SimpleNamespace
+    from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN
+    d = ldy.download()
+    ld = SimpleNamespace(W=d['W'], A=d['A'], rho=d['rho'], B=d['B'], V=d['V'], gap=sc.gap, friction=sc.friction,
+                         restitution=sc.restitution, cohesion=sc.cohesion, adjptr=d['adjptr'], adjcol=d['adjcol'],
+                         Woff=d['Woff'], free_energy=d['free_energy'], step=sc.step, dynamic=sc.dynamic)
+    kw = dict(epsilon=1.0, maxiter=20000, meritval=CONVERGED_MERIT)
+    out = {}
+    for key, prec, seed in (('fp64', 'FP64', None), ('mixed', 'MIXED', None), ('fp64_other_order', 'FP64',
+                                                                               CONVERGED_SEED)):
+        l2 = LOCDYN(device=dev.index)
+        if seed is not None:
+            l2.set_colour_seed(seed)
+        l2.set(ld)
+        gs = GAUSS_SEIDEL_SOLVER(**kw)
+        gs.precision = prec
+        gs.solve(l2)
+        R, U, _ = l2.get_state()
+        out[key] = dict(R=R, U=U, iters=gs.iters, merit=l2.merit)
+        l2.close()
+    F0, T0 = body_resultants(last['rot'], last['x'], sc, out['fp64']['R'])
+    res = dict(merit_target=CONVERGED_MERIT, fp64_iters=out['fp64']['iters'], fp64_merit=out['fp64']['merit'],
+               note='relative 2-norm differences from the FP64 solve in the same row order')
+    for key in ('mixed', 'fp64_other_order'):
+        F, T = body_resultants(last['rot'], last['x'], sc, out[key]['R'])
+        res[key] = dict(iters=out[key]['iters'], merit=out[key]['merit'],
+                        reactions=_rel2(out[key]['R'], out['fp64']['R']),
+                        velocities=_rel2(out[key]['U'], out['fp64']['U']),
+                        body_forces=_rel2(F, F0), body_torques=_rel2(T, T0))
+    return res
 
 
 # Algorithmic bytes of the rigid time integration kernels (csrc/b2_rigid.cuh),
@@ -456,7 +572,7 @@ BATCH_SOLVE = dict(epsilon=1e-4, maxiter=1000, meritval=1e-4)
 BATCH_METRIC = 'batched contact solve: contacts solved per second (256 uneven sphere scenes, one persistent launch)'
 
 
-def bench_batched(args, ws, rank, local):
+def bench_batched(args, ws, rank, local, scs=None):
     """Config of the batched workload: every rank solves its own batch."""
     import ctypes as C
     import torch
@@ -466,7 +582,8 @@ def bench_batched(args, ws, rank, local):
     kw = dict(BATCH)
     kw['seed'] = BATCH['seed'] + 1000 * rank
     t0 = time.perf_counter()
-    scs = scenes.batched_scenes(workers=min(32, os.cpu_count() or 1), **kw)
+    if scs is None:
+        scs = scenes.batched_scenes(workers=min(32, os.cpu_count() or 1), **kw)
     gen_s = time.perf_counter() - t0
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
@@ -560,16 +677,160 @@ def batched_line(args, ws, out):
     }
 
 
-def roofline(mode, r, n, K, peak):
-    rep = r['report']
-    sweeps = rep['sweeps_launch'][0]
-    ms = rep['ms_kernel'][0]
-    bytes_launch = sweeps * (K * BYTES_BLOCK[mode] + n * BYTES_ROW[mode])
-    gbs = bytes_launch / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+CONFIG_SOLVE = {'config1': dict(epsilon=1e-4, maxiter=1000, meritval=1e-4),
+                'config2': dict(epsilon=1e-6, maxiter=1000, meritval=1e-6)}
+
+
+def _generate_config_scenes(queue, batch_seed, workers):
+    """Host generation of the scenes of configs 1, 2 and 4 (runs in a spawned
+    process while the GPU runs the headline workload)."""
+    sys.path.insert(0, os.path.join(ROOT, 'solfec-1.0_b200'))
+    from solfec_b200 import scenes
+    t0 = time.perf_counter()
+    c1 = scenes.spheres_lattice()
+    c2 = scenes.spheres_polydisperse(seed=2, n=20000)
+    kw = dict(BATCH)
+    kw['seed'] = batch_seed
+    c4 = scenes.batched_scenes(workers=workers, **kw)
+    queue.put((c1, c2, c4, time.perf_counter() - t0))
+
+
+class _ConfigScenes:
+    """Scenes of configs 1, 2 and 4, generated by a spawned process."""
+
+    def __init__(self, batch_seed):
+        import multiprocessing as mp
+        ctx = mp.get_context('spawn')
+        self.q = ctx.Queue()
+        self.p = ctx.Process(target=_generate_config_scenes,
+                             args=(self.q, batch_seed, max(1, min(16, (os.cpu_count() or 2) - 1))))
+        self.p.start()
+
+    def result(self, timeout=900):
+        try:
+            out = self.q.get(timeout=timeout)   # read before joining: the child flushes its result into the pipe
+        finally:
+            self.close()
+        return out
+
+    def close(self):
+        """Ends the generator (it may still be writing when the run fails early)."""
+        if self.p.is_alive():
+            self.p.terminate()
+        self.p.join(timeout=30)
+
+
+def start_scene_generation(args):
+    """Configs 1, 2 and 4 ride along the default run (rank 0 only)."""
+    ws, rank, _ = _dist()
+    if ws > 1 or args.no_configs or args.scene:  # single-GPU runs only (the legs take no collective)
+        return None
+    return _ConfigScenes(BATCH['seed'])
+
+
+def sphere_time_loop(sc, solve_kw, args, dev, precision='FP64'):
+    """Device time loop of a sphere scene with the scene's contacts kept
+    (gravity, warm start from the previous step, bodies and state on the
+    device): W untimed steps, then K timed steps; per-step time by CUDA events."""
+    import torch
+    import ctypes as C
+    from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN
+    from solfec_b200._lib import lib
+    from solfec_b200.dynamics import RIGID_DYNAMICS
+    stream = torch.cuda.current_stream()
+    J, mass = _rigid_inertia(sc)
+    ldy = LOCDYN(device=dev.index, stream=stream.cuda_stream)
+    ldy.update_begin(sc)
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    n = sc.ncon
+    Rd = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    Ud = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    gs = GAUSS_SEIDEL_SOLVER(**solve_kw)
+    gs.precision = precision
+    h, dflag = float(sc.step), int(sc.dynamic)
+    its, kms = [], []
+
+    def step(timed):
+        dyn.step_begin(h, STEP_GRAVITY)
+        if lib().b2gs_locdyn_update_begin_resident(ldy.handle, h, dflag) != 0:
+            raise RuntimeError('LOCDYN update failed')
+        ldy.set_state_ptr(C.c_void_p(Rd.data_ptr()), C.c_void_p(Ud.data_ptr()), 1)
+        gs.solve(ldy)
+        ldy.get_state_ptr(C.c_void_p(Rd.data_ptr()), C.c_void_p(Ud.data_ptr()), None, 1)
+        dyn.step_end(h)
+        if timed:
+            its.append(gs.iters)
+            r = gs.report
+            kms.append(r['ms_kernel'][0] + r['ms_kernel'][1])
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    nrows, K, ncol, _ = ldy.sizes()
+    out = {'ms_per_step': round(ms, 4), 'contacts': nrows, 'blocks': K, 'colours': ncol, 'bodies': sc.nbod,
+           'iters_per_step': its, 'solve_kernel_ms_mean': round(float(np.mean(kms)), 4),
+           'us_per_sweep': round(1e3 * float(np.sum(kms)) / max(1, sum(its) + len(its)), 2),
+           'precision': precision,
+           'last_merit': ldy.merit, 'last_error': gs.error,
+           'solver': 'GAUSS_SEIDEL_SOLVER(epsilon=%g, maxiter=%d, meritval=%g)' % (
+               solve_kw['epsilon'], solve_kw['maxiter'], solve_kw['meritval'])}
+    ldy.close()
+    return out
+
+
+def run_config_legs(args, ws, rank, local, extra):
+    """Per-step times of configs 1 and 2 (device time loops of the settled
+    sphere packings) and the batched config 4, for the default line."""
+    if extra is None:
+        return None
+    import torch
+    dev = torch.device('cuda', local)
+    try:
+        c1, c2, c4, gen_s = extra.result()
+    except Exception as e:
+        return {'error': 'scene generation: %s' % str(e)[:200]}
+    out = {'scene_generation_s': round(gen_s, 1)}
+    for key, sc, name in (('config1', c1, '1000 spheres r=0.05 on a 10^3 lattice, settled, friction 0.3, h=1e-3'),
+                          ('config2', c2, '20000 polydisperse spheres r~U[0.03,0.06], settled, friction 0.5, '
+                                          'h=5e-4')):
+        try:
+            out[key] = dict(sphere_time_loop(sc, CONFIG_SOLVE[key], args, dev), workload=name)
+        except Exception as e:
+            out[key] = {'error': str(e)[:300]}
+    try:
+        b = bench_batched(args, 1, 0, local, scs=c4)
+        line = batched_line(args, 1, b)
+        out['config4'] = {k: line[k] for k in ('value', 'unit', 'ms_per_step', 'per_scene_ms_to_decision',
+                                                'per_scene_iters', 'e2e', 'gpu_launches')}
+        out['config4']['metric'] = BATCH_METRIC
+        out['config4']['contacts'] = b['contacts']
+        out['config4']['autotuned'] = line['config']['autotuned']
+    except Exception as e:
+        out['config4'] = {'error': str(e)[:300]}
+    return out
+
+
+def roofline(mode, reps, n, K, peak):
+    """Achieved bandwidth of the dominant kernel (the solve launch of the FP32
+    sweeps in mixed precision, the FP64 solve launch otherwise) over the timed
+    steps: algorithmic bytes of all its fused passes / its CUDA-event time."""
+    sweeps = sum(r['sweeps_launch'][0] for r in reps)
+    ms = sum(r['ms_kernel'][0] for r in reps)
+    bytes_all = sweeps * (K * BYTES_BLOCK[mode] + n * BYTES_ROW[mode])
+    gbs = bytes_all / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+    nl = max(len(reps), 1)
     return dict(bound='hbm', achieved=round(gbs, 1), peak=peak, unit='GB/s', frac=round(gbs / peak, 3),
-                traffic=int(bytes_launch * TRAFFIC_RATIO[mode]), traffic_source='ncu, 100x100x6 lattice, scaled',
+                traffic=int(bytes_all / nl * TRAFFIC_RATIO[mode]), traffic_source='ncu, 100x100x6 lattice, scaled',
                 kernel='k_solve<%s>' % ('true' if mode == 'mixed' else 'false'),
-                bytes_per_launch=int(bytes_launch), sweeps_per_launch=sweeps, kernel_ms=round(ms, 4))
+                bytes_per_launch=int(bytes_all / nl), sweeps_per_launch=round(sweeps / nl, 2),
+                kernel_ms_per_launch=round(ms / nl, 4), launches=len(reps))
 
 
 # FP64 iterations of the bench step (seed of rank 0) to merit 1e-4. The FP64
@@ -643,6 +904,7 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='product', choices=['product', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-configs', action='store_true', help='skip the configs 1, 2 and 4 legs of the default line')
     ap.add_argument('--scene', default=None, help='NXxNYxNZ lattice of a smaller case (profiling)')
     ap.add_argument('--maxiter', type=int, default=None, help='iteration cap of a smaller case (profiling)')
     ap.add_argument('--workload', default='hexahedra', choices=['hexahedra', 'batched', 'detect'])
@@ -682,23 +944,30 @@ def main():
             torch.distributed.barrier()
             torch.distributed.destroy_process_group()
         return
-    out = bench_product(args, ws, rank, local)
+    extra = start_scene_generation(args)          # configs 1, 2 and 4 are generated on the host meanwhile
+    try:
+        out = bench_product(args, ws, rank, local)
+        configs = run_config_legs(args, ws, rank, local, extra)
+    finally:
+        if extra is not None:
+            extra.close()
     peak, peak_kind = _peaks()
     if rank == 0:
         res = out['results']
         mixed, fp64, mnn = res['mixed'], res['fp64'], res['mixed_nn']
-        roof = roofline('mixed', mnn, out['n'], out['K'], peak)
-        roof64 = roofline('fp64', fp64, out['n'], out['K'], peak)
+        roof = roofline('mixed', mnn['reps'], out['n'], out['K'], peak)
+        roof64 = roofline('fp64', fp64['reps'], out['n'], out['K'], peak)
         roof['peak_kind'] = peak_kind
+        fp64_iters = float(np.mean(fp64['iters']))
         cpu = None
         if not args.no_cpu_baseline:
-            t = cpu_reference_step(out['scene'], out['R0'], out['U0'], fp64['iters'])
+            t = cpu_reference_step(out['scene'], None, None, fp64_iters)
             cpu = {'value': round(t['ms'], 3), 'unit': 'ms', 'cores': 1,
                    'kind': 'reference' if t['impl'] == 'ref' else 'port',
-                   'sample': 'the bench step (%d contacts): restated assembly timed in full + %d iterations of the '
-                             'reference serial GAUSS_SEIDEL_Solve from the same warm start, scaled to the %d '
-                             'iterations the step takes (the FP64 GPU path takes the same iterates)'
-                             % (out['n'], t['sample_iters'], fp64['iters']),
+                   'sample': 'a step of the bench scene (%d contacts): restated assembly timed in full + %d '
+                             'iterations of the reference serial GAUSS_SEIDEL_Solve, scaled to the %.1f iterations '
+                             'a timed step takes on average (the FP64 GPU path takes the same iterates)'
+                             % (out['n'], t['sample_iters'], fp64_iters),
                    'assemble_ms': round(t['assemble_ms'], 3), 'per_iteration_ms': round(t['per_iter_ms'], 3)}
         rg = out['rigid']
         gb = rg['begin_bytes'] / (rg['begin_ms'] * 1e-3) / 1e9
@@ -713,6 +982,19 @@ def main():
                            'solve whose reactions and layout it reads back from L2 (end_frac > 1 reflects that)',
                  'cpu_port_ms_per_1k_bodies': None if args.no_cpu_baseline
                  else round(rigid_cpu_sample(out['scene']), 3)}
+
+        def mode_summary(r):
+            reps = r['reps']
+            return {'ms_per_step': round(r['ms'], 4), 'iters_per_step': r['iters'],
+                    'iters_mean': round(float(np.mean(r['iters'])), 2),
+                    'iters_fp32_per_step': [x['iters_mixed'] for x in reps],
+                    'solve_kernel_ms_mean': [round(float(np.mean([x['ms_kernel'][j] for x in reps])), 4)
+                                             for j in (0, 1)],
+                    'sweeps_per_step': [x['sweeps_launch'] for x in reps], 'grid': reps[-1]['grid'],
+                    'last_merit': r['merit'], 'last_error': r['error'],
+                    'assemble_ms_last': round(r['assemble_ms'], 4),
+                    'reaction_rel_diff_vs_fp64_last_step': _rel2(r['R'], fp64['R'])}
+        nn = mnn['nn']
         line = {
             'metric': METRIC, 'value': round(mnn['ms'], 4), 'unit': 'ms', 'n_gpus': ws, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': round(mnn['ms'], 4), 'higher_is_better': False,
@@ -720,36 +1002,39 @@ def main():
             'data': 'synthetic (seeded scene generator)',
             'config': {'workload': WORKLOAD, 'contacts': out['n'], 'blocks': out['K'], 'bodies': out['nbod'],
                        'colours': out['ncolours'],
+                       'run': 'time loop from rest under gravity: %d untimed steps, then %d timed consecutive steps; '
+                              'each step = BODY_Dynamic_Step_Begin + LOCDYN_Update_Begin + solve + '
+                              'BODY_Dynamic_Step_End on the device, warm start = the previous step\'s R, U'
+                              % (args.warmup, args.steps),
                        'mode': 'mixed+NN: learned warm start (kept when its merit is lower), FP32 sweeps, '
                                'FP64 diagonal/merit/refinement',
-                       'solver': 'GAUSS_SEIDEL_SOLVER(epsilon=%g, maxiter=%d, meritval=%g, SEMISMOOTH_NEWTON), '
-                                 'warm start from the previous step' % (SOLVE['epsilon'], SOLVE['maxiter'],
-                                                                         SOLVE['meritval']),
+                       'solver': 'GAUSS_SEIDEL_SOLVER(epsilon=%g, maxiter=%d, meritval=%g, SEMISMOOTH_NEWTON): '
+                                 'the merit test decides (time to merit 1e-4); the modes *_ref_rule use the '
+                                 'reference\'s epsilon = meritval = 1e-4' % (SOLVE['epsilon'], SOLVE['maxiter'],
+                                                                          SOLVE['meritval']),
                        'l2': 'sweep working set > 126 MB L2 (W planes %.0f MB FP64 / %.0f MB FP32)'
                              % (out['K'] * 72 / 1e6, out['K'] * 36 / 1e6),
                        'parallelism': 'replicas' if ws > 1 else 'single GPU'},
-            'modes': {m: {'ms_per_step': round(r['ms'], 4), 'iters': r['iters'], 'iters_fp32': r['iters_mixed'],
-                          'merit': r['merit'], 'error': r['error'], 'assemble_ms': round(r['assemble_ms'], 4),
-                          'solve_kernel_ms': [round(x, 4) for x in r['report']['ms_kernel']],
-                          'sweeps': r['report']['sweeps_launch'], 'grid': r['report']['grid'],
-                          'reaction_rel_diff_vs_fp64': float(np.linalg.norm(r['R'] - fp64['R'])
-                                                             / max(np.linalg.norm(fp64['R']), 1e-300))}
-                      for m, r in res.items()},
-            'reaction_diff_note': 'relative 2-norm difference of the final reactions from the FP64 solve; the '
-                                  'stack is hyperstatic, so merit-1e-4 solutions need not coincide',
+            'modes': {m: mode_summary(r) for m, r in res.items()},
             'speedup_mixed_vs_fp64': round(fp64['ms'] / mixed['ms'], 3),
             'speedup_mixed_nn_vs_fp64': round(fp64['ms'] / mnn['ms'], 3),
-            'warm_start': None if not mnn.get('nn') else {
-                'network_start_used_steps': mnn['nn_used_steps'], 'steps': mnn['nn_steps'],
-                'merit_network_start': mnn['nn']['merit_nn'], 'merit_previous_step_start': mnn['nn']['merit_plain'],
-                'network_and_merit_ms': round(mnn['nn']['ms'], 4)},
+            'mixed_vs_fp64_converged': out['converged'],
+            'warm_start': None if not nn else {
+                'network_start_used_steps': sum(1 for q in nn if q['used_nn']), 'steps': len(nn),
+                'merit_network_start': [q['merit_nn'] for q in nn],
+                'merit_previous_step_start': [q['merit_plain'] for q in nn],
+                'network_and_merit_ms_mean': round(float(np.mean([q['ms'] for q in nn])), 4)},
             'roofline': roof, 'roofline_fp64': roof64,
             'cpu_baseline': cpu,
             'e2e': {'value': round(out['e2e_ms'], 4), 'unit': 'ms', 'h2d_bytes_per_step': out['h2d'],
-                    'd2h_bytes_per_step': out['d2h']},
+                    'd2h_bytes_per_step': out['d2h'],
+                    'what': 'the timed steps of the mixed+NN run replayed through the C ABI from pinned host '
+                            'buffers: bodies, contacts and the previous result up, assembly, learned warm start, '
+                            'solve, R, U and per-contact merit down'},
             'gpu_launches': int(mnn['launches']),
             'clocks': out['clocks'],
             'rigid_step': rigid,
+            'configs': configs,
         }
         try:
             line['detect'] = detect_timing()

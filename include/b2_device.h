@@ -266,6 +266,13 @@ int b2dev_problem_free_energy(b2dev_ctx* ctx, double* out);
  * parallel work to small problems; the autotuner chooses it. */
 int b2dev_set_tile_rows(b2dev_ctx* ctx, int rows);
 int b2dev_tile_rows(b2dev_ctx* ctx);
+/* Limit, in seconds, of every bounded wait of the solver kernels on a flag
+ * that another warp sets (0 restores the default of 2 s). A wait that runs
+ * out ends the launch and the solve returns B2DEV_ETIMEOUT; the context keeps
+ * its state and stays usable. No counterpart in the reference (its solver
+ * never waits on another thread); meant for tests of that path. */
+int b2dev_set_wait_limit(b2dev_ctx* ctx, double seconds);
+
 /* Solve every problem (FP64 sweeps). use_graph: capture the launch sequence
  * into a CUDA graph and replay it while its arguments are unchanged.
  * reps[nprob]; rerhist/merhist NULL or nprob * opts->maxiter doubles;

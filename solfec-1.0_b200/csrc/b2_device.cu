@@ -216,6 +216,7 @@ struct b2dev_ctx {
   bool det_assembled = false;   // ... and the local dynamics was assembled from them
   std::vector<int> ptile_count;  // tiles per problem
   int trace_sweep = -1;  // sweep of the next solve whose diagonal solves are recorded
+  unsigned long long wait_ns = kBarrierLimitNs;  // limit of the solver's bounded waits
 
   int n = 0;
   long long K = 0, kstride = 0;
@@ -682,6 +683,7 @@ int solve_setup(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter
   A.u0_from_merit = u0_from_merit;
   A.gcap = gcap;
   A.warp_smem = (int)wsm;
+  A.wait_ns = c->wait_ns;
   if (c->trace_sweep >= 0 && iter0 == 0) {
     A.trace = ptr<double>(c->trace);
     A.trace_sweep = c->trace_sweep;
@@ -726,6 +728,13 @@ int solve_enqueue(b2dev_ctx* c, bool mixed, const SolveArgs& a, int grid, size_t
   B2_CK(cudaLaunchKernelExC(&cfg, fn, args));
   return B2DEV_OK;
 }
+
+// Floors of the FP32 sweeps' stopping rule in mixed precision: FP32 products
+// carry relative rounding of about 6e-8, so iterate differences (the relative
+// error) and merits (quadratic in the velocity residual) below these are not
+// resolved by them; a tighter caller rule is met by the FP64 sweeps.
+constexpr double kMixedEpsilonFloor = 1e-5;
+constexpr double kMixedMeritFloor = 1e-10;
 
 // One persistent solve launch, synchronised: per-problem outcomes in pc.
 int solve_launch(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter, int iter0, int in,
@@ -1626,7 +1635,13 @@ int b2dev_solve(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_solve_report* rep
     c->launches++;
     k_shadow<<<blocks_for(c->n, 256), 256, 0, st>>>(c->n, ptr<double4>(c->R64[c->state_r]),
                                                     ptr<float4>(c->R32[c->state_r]));
-    B2_TRY(solve_launch(c, true, o, maxiter - 1, 0, c->state_r, 0, o->grid, &g1, q1, &rep->ms_kernel[0], &rep->grid));
+    // The FP32 sweeps stop at the caller's rule or, when that asks for more
+    // than FP32 products resolve, at the FP32 floors; the FP64 sweeps that
+    // follow continue to the caller's epsilon and meritval.
+    b2dev_solve_opts o32 = *o;
+    o32.epsilon = std::max(o->epsilon, kMixedEpsilonFloor);
+    if (!o->nomerit) o32.meritval = std::max(o->meritval, kMixedMeritFloor);
+    B2_TRY(solve_launch(c, true, &o32, maxiter - 1, 0, c->state_r, 0, o->grid, &g1, q1, &rep->ms_kernel[0], &rep->grid));
     const ProblemControl& s1 = q1[0];
     rep->sweeps_launch[0] = g1.sweeps;
     rep->merit_input = s1.merit_input;
@@ -1728,6 +1743,12 @@ int b2dev_set_tile_rows(b2dev_ctx* c, int rows) {
 }
 
 int b2dev_tile_rows(b2dev_ctx* c) { return c ? c->tile_rows : 0; }
+
+int b2dev_set_wait_limit(b2dev_ctx* c, double seconds) {
+  if (!c || !(seconds >= 0.0) || seconds > 60.0) { set_err("set_wait_limit: 0 <= seconds <= 60"); return B2DEV_EINVAL; }
+  c->wait_ns = seconds == 0.0 ? kBarrierLimitNs : std::max(1ull, (unsigned long long)(seconds * 1e9));
+  return B2DEV_OK;
+}
 
 // Batched solve: one persistent launch over every problem of the context, each
 // an independent GAUSS_SEIDEL_Solve with its own stopping decision (FP64

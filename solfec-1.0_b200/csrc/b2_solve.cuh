@@ -55,7 +55,7 @@ constexpr int kSolveWarps = kSolveThreads / kWarp;
 template <bool MIXED>
 __host__ __device__ constexpr int chunk_unroll() { return MIXED ? 1 : 2; }
 constexpr int kTileHeader = 256;                     // bytes of per-warp shared memory before the staging
-constexpr uint64_t kBarrierLimitNs = 2000000000ull;  // 2 s per bounded wait
+constexpr uint64_t kBarrierLimitNs = 2000000000ull;  // 2 s per bounded wait (default of SolveArgs::wait_ns)
 
 enum { DECIDE_NONE = 0, DECIDE_CONTINUE = 1, DECIDE_STOP = 2 };
 
@@ -140,6 +140,7 @@ struct SolveArgs {
   int u0_from_merit;        // sweep 0 hands the merit U (not Us) to the diagonal solver
   int gcap;                 // Gauss-Seidel products staged per tile window
   int warp_smem;            // bytes of dynamic shared memory per warp
+  unsigned long long wait_ns;  // limit of every wait on a flag another warp sets (ns)
 };
 
 // trace record per row: B'[3], U in[3], R in[3], U out[3], R out[3], kind
@@ -159,27 +160,27 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 // the wait ran out (the timeout is recorded in ctrl). The first check is
 // inlined; only the spin is out of line (a call site saves live registers, so
 // the common case must not be a call).
-__device__ __noinline__ bool wait_at_least_spin(const int* p, int need, SolveControl* ctrl) {
+__device__ __noinline__ bool wait_at_least_spin(const int* p, int need, SolveControl* ctrl, uint64_t limit) {
   const uint64_t t0 = globaltimer_ns();
   volatile int* stop = &ctrl->stop;
   volatile int* to = &ctrl->timeout;
   while (ld_acquire(p) < need) {
     if (*stop || *to) return false;
-    if (globaltimer_ns() - t0 > kBarrierLimitNs) { *to = 1; return false; }
+    if (globaltimer_ns() - t0 > limit) { *to = 1; return false; }
     __nanosleep(64);
   }
   return true;
 }
-__device__ __forceinline__ bool wait_at_least(const int* p, int need, SolveControl* ctrl) {
+__device__ __forceinline__ bool wait_at_least(const int* p, int need, SolveControl* ctrl, uint64_t limit) {
   if (ld_acquire(p) >= need) return true;
-  return wait_at_least_spin(p, need, ctrl);
+  return wait_at_least_spin(p, need, ctrl, limit);
 }
 
 // Gate of a tile of sweep s >= 2 of one problem: 1 = run (the decision after
 // sweep s-2 is to continue), 2 = skip (the problem has taken its final
 // decision, so later sweeps are discarded), 0 = the solve is ending or the
 // bounded wait gave up.
-__device__ __noinline__ int gate_wait_spin(const int* decided_s2, const int* pstop, SolveControl* ctrl) {
+__device__ __noinline__ int gate_wait_spin(const int* decided_s2, const int* pstop, SolveControl* ctrl, uint64_t limit) {
   const uint64_t t0 = globaltimer_ns();
   volatile int* stop = &ctrl->stop;
   volatile int* to = &ctrl->timeout;
@@ -189,13 +190,13 @@ __device__ __noinline__ int gate_wait_spin(const int* decided_s2, const int* pst
     if (d == DECIDE_STOP) return 2;
     if (*(volatile const int*)pstop) return 2;
     if (*stop || *to) return 0;
-    if (globaltimer_ns() - t0 > kBarrierLimitNs) { *to = 1; return 0; }
+    if (globaltimer_ns() - t0 > limit) { *to = 1; return 0; }
     __nanosleep(64);
   }
 }
-__device__ __forceinline__ int gate_wait(const int* decided_s2, const int* pstop, SolveControl* ctrl) {
+__device__ __forceinline__ int gate_wait(const int* decided_s2, const int* pstop, SolveControl* ctrl, uint64_t limit) {
   if (ld_acquire(decided_s2) == DECIDE_CONTINUE) return 1;
-  return gate_wait_spin(decided_s2, pstop, ctrl);
+  return gate_wait_spin(decided_s2, pstop, ctrl, limit);
 }
 
 // Bounded wait until every tile of list[lo, hi) has completed `need` sweeps:
@@ -204,9 +205,9 @@ __device__ __forceinline__ int gate_wait(const int* decided_s2, const int* pstop
 // all of them (each tile publishes its rows with one release after its own
 // warp barrier).
 __device__ __forceinline__ bool wait_tiles(const int* list, int lo, int hi, const int* tile_done, int need,
-                                           SolveControl* ctrl, int lane) {
+                                           SolveControl* ctrl, uint64_t limit, int lane) {
   bool ok = true;
-  for (int i = lo + lane; i < hi; i += kWarp) ok = wait_at_least(tile_done + __ldg(list + i), need, ctrl) && ok;
+  for (int i = lo + lane; i < hi; i += kWarp) ok = wait_at_least(tile_done + __ldg(list + i), need, ctrl, limit) && ok;
   return ok;
 }
 
@@ -449,12 +450,12 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   const bool by_tile = a.tile_done != nullptr;
   if (!f.prev_done) {  // the rows and all neighbours of this tile have completed the previous sweep
     if (by_tile) {
-      if (lane == 0) ok = wait_at_least(a.tile_done + tile, s, a.ctrl);
-      ok = wait_tiles(a.depE, __ldg(a.depE_ptr + tile), __ldg(a.depE_ptr + tile + 1), a.tile_done, s, a.ctrl, lane) && ok;
-      ok = wait_tiles(a.depL, __ldg(a.depL_ptr + tile), __ldg(a.depL_ptr + tile + 1), a.tile_done, s, a.ctrl, lane) && ok;
+      if (lane == 0) ok = wait_at_least(a.tile_done + tile, s, a.ctrl, a.wait_ns);
+      ok = wait_tiles(a.depE, __ldg(a.depE_ptr + tile), __ldg(a.depE_ptr + tile + 1), a.tile_done, s, a.ctrl, a.wait_ns, lane) && ok;
+      ok = wait_tiles(a.depL, __ldg(a.depL_ptr + tile), __ldg(a.depL_ptr + tile + 1), a.tile_done, s, a.ctrl, a.wait_ns, lane) && ok;
       __syncwarp();
     } else if (own) {
-      ok = wait_at_least(a.done + p, s, a.ctrl);
+      ok = wait_at_least(a.done + p, s, a.ctrl, a.wait_ns);
     }
   }
 
@@ -505,7 +506,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
       const int j = col_s[k - a0];
       const bool earlier = f.backward ? (j >= ce) : (j < cs);
       if (f.merit || (f.gs && !earlier)) {
-        if (!f.prev_done && !by_tile) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
+        if (!f.prev_done && !by_tile) ok = wait_at_least(a.done + j, s, a.ctrl, a.wait_ns) && ok;
         cp_async16(smem_addr(slot + (k - wb)), a.R32[rin] + j);
       }
     }
@@ -530,7 +531,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
               const float4 v = slot[g];
               ro0 = v.x; ro1 = v.y; ro2 = v.z;
             } else {
-              if (!f.prev_done && !by_tile) ok = wait_at_least(a.done + j, s, a.ctrl) && ok;
+              if (!f.prev_done && !by_tile) ok = wait_at_least(a.done + j, s, a.ctrl, a.wait_ns) && ok;
               load_r<MIXED, real>(a, rin, j, ro0, ro1, ro2);
             }
             const real* Wk = w[u];
@@ -564,7 +565,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
     if (by_tile && win == 0) {  // every tile holding an earlier neighbour has completed this sweep
       const int* ptr = f.backward ? a.depL_ptr : a.depE_ptr;
       ok = wait_tiles(f.backward ? a.depL : a.depE, __ldg(ptr + tile), __ldg(ptr + tile + 1), a.tile_done, s + 1,
-                      a.ctrl, lane) && ok;
+                      a.ctrl, a.wait_ns, lane) && ok;
       __syncwarp();
     }
     // ---- pass 2: neighbours earlier in this sweep (their new reactions)
@@ -600,7 +601,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
           const int j = col_s[k - a0];
           const bool earlier = f.backward ? (j >= ce) : (j < cs);
           if (earlier) {
-            if (!by_tile) ok = wait_at_least(a.done + j, s + 1, a.ctrl) && ok;
+            if (!by_tile) ok = wait_at_least(a.done + j, s + 1, a.ctrl, a.wait_ns) && ok;
             real Wk[9];
 #pragma unroll
             for (int q = 0; q < 9; q++) {
@@ -677,7 +678,7 @@ __device__ __noinline__ void finalize_sweep(const SolveArgs& a, int prob, int s)
   int prev = DECIDE_CONTINUE;
   if (s >= 1) {
     bool ok = true;
-    if (lane == 0) ok = wait_at_least((const int*)decided + s - 1, DECIDE_CONTINUE, a.ctrl);
+    if (lane == 0) ok = wait_at_least((const int*)decided + s - 1, DECIDE_CONTINUE, a.ctrl, a.wait_ns);
     ok = __shfl_sync(0xffffffffu, ok, 0);
     if (!ok) return;
     prev = decided[s - 1];
@@ -800,7 +801,7 @@ __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constan
     volatile int* decided = a.decided + (size_t)prob * a.pstride;
     if (s >= 2) {  // sweep s reuses the buffers of iterate s-3: wait for the decision after sweep s-2
       int gate = 0;
-      if (lane == 0) gate = gate_wait((const int*)decided + s - 2, &a.pctl[prob].stop, a.ctrl);
+      if (lane == 0) gate = gate_wait((const int*)decided + s - 2, &a.pctl[prob].stop, a.ctrl, a.wait_ns);
       gate = __shfl_sync(0xffffffffu, gate, 0);
       if (gate == 0) break;
       if (gate == 2) continue;  // this problem has finished: its later sweeps are not run

@@ -110,6 +110,7 @@ _SIGNATURES = {
     'b2dev_problem_free_energy': (C.c_int, [C.c_void_p, C.c_void_p]),
     'b2dev_set_tile_rows': (C.c_int, [C.c_void_p, C.c_int]),
     'b2dev_tile_rows': (C.c_int, [C.c_void_p]),
+    'b2dev_set_wait_limit': (C.c_int, [C.c_void_p, C.c_double]),
     'b2dev_solve_batch': (C.c_int, [C.c_void_p, C.POINTER(b2dev_solve_opts), C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.POINTER(b2dev_solve_report), C.c_int]),
     'b2dev_autotune_batch': (C.c_int, [C.c_void_p, C.POINTER(b2dev_solve_opts), C.POINTER(b2dev_tune_result)]),

@@ -93,6 +93,10 @@ class LOCDYN:
         """Greedy colouring in list order for the next layouts (the default)."""
         _check(lib().b2dev_set_colour_order(self.device_context, 1), 'b2dev_set_colour_order')
 
+    def set_wait_limit(self, seconds: float):
+        """Limit of the solver's bounded device-side waits (0: the default 2 s)."""
+        _check(lib().b2dev_set_wait_limit(self.device_context, float(seconds)), 'b2dev_set_wait_limit')
+
     def colour_reuse_count(self) -> int:
         """Layouts that reused the previous colouring (unchanged contact graph)."""
         return int(lib().b2dev_colour_reuse_count(self.device_context))
