@@ -1652,17 +1652,26 @@ int b2dev_solve(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_solve_report* rep
     error = s1.error;
     rep->iters_mixed = iters;
     rep->sweeps = g1.sweeps;
-    if (!thrown) {  // closing FP64 refinement, continuing the iteration count
-      B2_TRY(solve_launch(c, false, o, maxiter - iters, iters, c->state_r, o->nomerit ? 0 : 1, o->grid, &g2, q2,
-                          &rep->ms_kernel[1], &rep->grid));
+    // closing FP64 refinement, continuing the iteration count: one FP64
+    // sweep and the FP64 merit of its iterate (a merit-only pass, no
+    // speculative sweeps); if that iterate does not meet the caller's rule,
+    // FP64 sweeps continue until it does or maxiter is reached
+    for (int pass = 0; !thrown && iters < maxiter; pass++) {
+      const int budget = pass == 0 ? 1 : maxiter - iters;
+      float ms = 0.f;
+      B2_TRY(solve_launch(c, false, o, budget, iters, c->state_r, o->nomerit ? 0 : 1, o->grid, &g2, q2, &ms,
+                          &rep->grid));
       const ProblemControl& s2 = q2[0];
-      rep->sweeps_launch[1] = g2.sweeps;
+      rep->ms_kernel[1] += ms;
+      rep->sweeps_launch[1] += g2.sweeps;
       ranges.push_back({iters, iters + s2.final_iter});
       iters += s2.iters;
       thrown = s2.thrown != 0;
       merit = s2.merit;
       error = s2.error;
       rep->sweeps += g2.sweeps;
+      const bool meets = o->nomerit ? !(error > o->epsilon) : !(error > o->epsilon || merit > o->meritval);
+      if (meets || pass > 0) break;
     }
   } else {
     B2_TRY(solve_launch(c, false, o, maxiter, 0, c->state_r, 0, o->grid, &g1, q1, &rep->ms_kernel[0], &rep->grid));

@@ -136,7 +136,8 @@ __global__ void k_merit_rows(int n, const int* __restrict__ rowptr, const int* _
                              const double* __restrict__ coh, double step, int dynamic, const double4* __restrict__ Ra,
                              const double4* __restrict__ Rb, double* __restrict__ upa, double* __restrict__ upb) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
+  double ua = 0.0, ub = 0.0;
+  if (p < n) {
   double B[3], W[9], A[9], V[3], Ua[3], Ub[3];
   const double4 ra = Ra[p], rb = Rb[p];
   const double Rpa[3] = {ra.x, ra.y, ra.z}, Rpb[3] = {rb.x, rb.y, rb.z};
@@ -162,8 +163,24 @@ __global__ void k_merit_rows(int n, const int* __restrict__ rowptr, const int* _
   ContactParams cp;
   cp.friction = fric[p]; cp.restitution = rest[p]; cp.cohesion = coh[p]; cp.gap = gap[p]; cp.step = step;
   cp.dynamic = dynamic;
-  upa[p] = merit_row(cp, A, V, Ua, Rpa);
-  upb[p] = merit_row(cp, A, V, Ub, Rpb);
+  ua = merit_row(cp, A, V, Ua, Rpa);
+  ub = merit_row(cp, A, V, Ub, Rpb);
+  }
+  // block partials in a fixed order (lanes, then warps): upa[blockIdx.x], upb[blockIdx.x]
+  __shared__ double red[2][32];
+#pragma unroll
+  for (int d = 16; d >= 1; d >>= 1) {
+    ua += __shfl_down_sync(0xffffffffu, ua, d);
+    ub += __shfl_down_sync(0xffffffffu, ub, d);
+  }
+  if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = ua; red[1][threadIdx.x >> 5] = ub; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sa = 0.0, sb = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { sa += red[0][w]; sb += red[1][w]; }
+    upa[blockIdx.x] = sa;
+    upb[blockIdx.x] = sb;
+  }
 }
 
 }  // namespace
@@ -427,19 +444,20 @@ NnRows nn_rows(b2dev_ctx* c) {
 int merit_of2(b2dev_ctx* c, const double4* Ra, const double4* Rb, double* outa, double* outb) {
   const int n = c->n;
   cudaStream_t st = c->stream;
-  B2_TRY(ensure(c->fe_part, sizeof(double) * 2 * (n + 1)));
+  const int nb = blocks_for(n, 128);
+  B2_TRY(ensure(c->fe_part, sizeof(double) * 2 * (nb + 1)));
   double* pa = ptr<double>(c->fe_part);
-  double* pb = pa + (n + 1);
+  double* pb = pa + (nb + 1);
   c->launches++;
-  k_merit_rows<<<blocks_for(n, 128), 128, 0, st>>>(n, ptr<int>(c->rowptr), ptr<int>(c->col), ptr<double>(c->W64),
+  k_merit_rows<<<nb, 128, 0, st>>>(n, ptr<int>(c->rowptr), ptr<int>(c->col), ptr<double>(c->W64),
                                                    c->kstride, ptr<double>(c->Wd), ptr<double>(c->Ad),
                                                    ptr<double>(c->Bv), ptr<double>(c->Vv), ptr<double>(c->gap),
                                                    ptr<double>(c->fric), ptr<double>(c->rest), ptr<double>(c->coh),
                                                    c->step, c->dynamic, Ra, Rb, pa, pb);
   B2_TRY(ensure(c->io, sizeof(double) * 2));
   c->launches += 2;
-  k_sum_partials<<<1, 1024, 0, st>>>(pa, n, ptr<double>(c->io));  // 0.5 sum up
-  k_sum_partials<<<1, 1024, 0, st>>>(pb, n, ptr<double>(c->io) + 1);
+  k_sum_partials<<<1, 1024, 0, st>>>(pa, nb, ptr<double>(c->io));  // 0.5 sum up
+  k_sum_partials<<<1, 1024, 0, st>>>(pb, nb, ptr<double>(c->io) + 1);
   double half[2] = {0.0, 0.0};
   B2_CK(cudaMemcpyAsync(half, c->io.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
   B2_CK(cudaStreamSynchronize(st));

@@ -118,3 +118,50 @@ def test_bench_step_bounded_fp64_bitwise():
     o = reference_in_order(ld, g['order'], 'oracle', **kw)
     assert ld.n == 302000 and g['iters'] == o['iters'] == 5
     assert same_bits(g['R'], o['R']) and same_bits(g['U'], o['U'])
+
+
+def test_hexahedra_lattice_mixed_against_fp64_oracle():
+    """A 40 x 40 x 8 hexahedra lattice settled by a 20-step device time loop
+    (gravity, warm starts, the device integrator); the last step's local
+    dynamics solved from zero reactions to merit 1e-7 (the stack's merit
+    stalls near 4e-8) by mixed precision on the GPU and by the FP64 oracle in
+    the same row order: reactions and per-body resultants within 1e-4."""
+    from types import SimpleNamespace
+    import ctypes as C
+    import bench
+    from solfec_b200._lib import lib
+    from solfec_b200.dynamics import RIGID_DYNAMICS
+    sc = scenes.hexahedra_lattice(seed=5, nx=40, ny=40, nz=8)
+    J, mass = bench._rigid_inertia(sc)
+    ldy = LOCDYN()
+    ldy.update_begin(sc)
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    gs = GAUSS_SEIDEL_SOLVER(epsilon=1.0, maxiter=1000, meritval=1e-4)
+    R = np.zeros((sc.ncon, 3)); U = np.zeros((sc.ncon, 3))
+    for _ in range(20):
+        dyn.step_begin(sc.step, (0.0, 0.0, -9.81))
+        assert lib().b2gs_locdyn_update_begin_resident(ldy.handle, sc.step, 1) == 0
+        ldy.set_state(R, U)
+        gs.solve(ldy)
+        R, U, _ = ldy.get_state()
+        dyn.step_end(sc.step)
+    dyn.step_begin(sc.step, (0.0, 0.0, -9.81))
+    assert lib().b2gs_locdyn_update_begin_resident(ldy.handle, sc.step, 1) == 0
+    st = dyn.state()
+    d = ldy.download()
+    ldy.close()
+    ld = SimpleNamespace(W=d['W'], A=d['A'], rho=d['rho'], B=d['B'], V=d['V'], gap=sc.gap, friction=sc.friction,
+                         restitution=sc.restitution, cohesion=sc.cohesion, adjptr=d['adjptr'], adjcol=d['adjcol'],
+                         Woff=d['Woff'], free_energy=d['free_energy'], step=sc.step, dynamic=sc.dynamic)
+    ldo = O.LocalDynamics(ld.W, ld.A, ld.rho, ld.B, ld.V, ld.gap, ld.friction, ld.restitution, ld.cohesion, ld.adjptr,
+                          ld.adjcol, ld.Woff, ld.free_energy, ld.step, ld.dynamic)
+    kw = dict(epsilon=1.0, maxiter=20000, meritval=1e-7)
+    g = device_solve(ldo, precision='MIXED', **kw)
+    o = reference_in_order(ldo, g['order'], 'oracle', **kw)
+    assert o['error'] == 0 and g['error'] == 'OK' and g['merit'] <= 1e-7 and o['merit'] <= 1e-7
+    assert rel2(g['R'], o['R']) <= MIXED_TOL, rel2(g['R'], o['R'])
+    rs = SimpleNamespace(base=sc.base, rot=st['rot'], x=st['x'], master=sc.master, slave=sc.slave, mpnt=sc.mpnt,
+                         x0=sc.x0, nbod=sc.nbod, obstacle=sc.obstacle)
+    Fg, Tg = body_resultants(rs, g['R'])
+    Fo, To = body_resultants(rs, o['R'])
+    assert rel2(Fg, Fo) <= MIXED_TOL and rel2(Tg, To) <= 10 * MIXED_TOL, (rel2(Fg, Fo), rel2(Tg, To))
