@@ -153,16 +153,21 @@ __global__ void k_sorted_degree(int n, const int* perm, const int* adjptr, int* 
 // the sorted row offsets.
 __global__ void k_offdiag_assembled(int n, long long K, const int* perm, const int* iperm, const int* adjptr,
                                     const int* adjcol, const int* adjbod, const int* master, const double* factors,
-                                    double step, const int* rowptr, int* col, double* W64, float* W32,
-                                    long long kstride) {
+                                    double step, const int* rowptr, const int* brow, int* col, double* W64,
+                                    float* W32, long long kstride) {
   const long long qo = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (qo >= K) return;
-  int lo_r = 0, hi_r = n;  // rowptr[lo_r] <= qo < rowptr[hi_r]
-  while (hi_r - lo_r > 1) {
-    const int mid = (lo_r + hi_r) >> 1;
-    if (rowptr[mid] <= qo) lo_r = mid; else hi_r = mid;
+  int p;
+  if (brow) {
+    p = brow[qo];
+  } else {
+    int lo_r = 0, hi_r = n;  // rowptr[lo_r] <= qo < rowptr[hi_r]
+    while (hi_r - lo_r > 1) {
+      const int mid = (lo_r + hi_r) >> 1;
+      if (rowptr[mid] <= qo) lo_r = mid; else hi_r = mid;
+    }
+    p = lo_r;
   }
-  const int p = lo_r;
   const int i = perm[p];
   const int t = (int)(qo - rowptr[p]);
   {
@@ -189,6 +194,27 @@ __global__ void k_offdiag_assembled(int n, long long K, const int* perm, const i
         W32[(3 * c + r) * kstride + qo] = (float)v;
       }
   }
+}
+
+// Sorted row of every off-diagonal block of the colour-sorted CSR (thread per
+// row), kept with the layout so the per-step block kernel needs no search.
+__global__ void k_block_rows(int n, const int* rowptr, int* brow) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  for (int k = rowptr[p]; k < rowptr[p + 1]; k++) brow[k] = p;
+}
+
+// Sets *diff if the contact topology (master and slave of every contact, the
+// obstacle flag of every body) differs from the copy kept with the last
+// contact graph.
+__global__ void k_topology_diff(int n, int nb, const int* master, const int* slave, const int* obst, const int* pm,
+                                const int* ps, const int* po, int* diff) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int stride = gridDim.x * blockDim.x;
+  bool d = false;
+  for (int i = t; i < n; i += stride) d |= master[i] != pm[i] || slave[i] != ps[i];
+  for (int b = t; b < nb; b += stride) d |= obst[b] != po[b];
+  if (__any_sync(0xffffffffu, d) && (threadIdx.x & 31) == 0) atomicExch(diff, 1);
 }
 
 // Tile of every sorted row (forward tile numbering).

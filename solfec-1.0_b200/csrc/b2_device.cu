@@ -217,6 +217,12 @@ struct b2dev_ctx {
   std::vector<int> ptile_count;  // tiles per problem
   int trace_sweep = -1;  // sweep of the next solve whose diagonal solves are recorded
   unsigned long long wait_ns = kBarrierLimitNs;  // limit of the solver's bounded waits
+  // the contact topology (master, slave, obstacle flags) of the last contact
+  // graph built by b2dev_assemble: an unchanged topology keeps that graph
+  Buf topo_m, topo_s, topo_o, topo_flag;
+  int topo_n = -1, topo_nb = -1;
+  bool topo_valid = false;
+  Buf blkrow;  // sorted row of every off-diagonal block (with the layout)
 
   int n = 0;
   long long K = 0, kstride = 0;
@@ -361,7 +367,9 @@ int build_tiles(b2dev_ctx* c, int rows) {
 
 // Colour the caller-order graph (adjptr/adjcol) and build the colour-sorted
 // layout; row data must already sit in the caller-order buffers.
-int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
+// same_graph: the caller knows the contact graph is that of the last layout
+// (an unchanged contact topology), so the comparison pass is skipped.
+int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled, bool same_graph) {
   const int n = c->n;
   cudaStream_t st = c->stream;
   const int T = 256;
@@ -380,6 +388,9 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   memset(&cc, 0, sizeof cc);
   bool reuse = false;
   if (c->colour_valid && c->colour_n == n && c->colour_K == c->K && c->colour_mode == c->colour_list &&
+      (c->colour_list || c->colour_seed_prev == seed) && n > 0 && same_graph) {
+    reuse = true;
+  } else if (c->colour_valid && c->colour_n == n && c->colour_K == c->K && c->colour_mode == c->colour_list &&
       (c->colour_list || c->colour_seed_prev == seed) && n > 0) {  // same graph as the last colouring?
     B2_CK(cudaMemsetAsync(c->bad.p, 0, sizeof(int), st));
     c->launches++;
@@ -459,6 +470,11 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
   c->launches++;
   k_set_last_zero<<<1, 32, 0, st>>>(ptr<int>(c->sdeg), n);
   B2_TRY(scan_exclusive(c, ptr<int>(c->sdeg), ptr<int>(c->rowptr), n + 1));
+  B2_TRY(ensure(c->blkrow, sizeof(int) * ((size_t)c->K + 1)));
+  if (n > 0 && c->K > 0) {
+    c->launches++;
+    k_block_rows<<<blocks_for(n, T), T, 0, st>>>(n, ptr<int>(c->rowptr), ptr<int>(c->blkrow));
+  }
 
   c->colptr_h.assign(c->ncolours + 1, 0);
   if (c->ncolours > 0) {
@@ -478,8 +494,8 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled) {
       c->launches++;
       k_offdiag_assembled<<<blocks_for(K, 256), 256, 0, st>>>(
           n, K, ptr<int>(c->perm), ptr<int>(c->iperm), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<int>(c->adjbod),
-          ptr<int>(c->master), ptr<double>(c->factors), c->step, ptr<int>(c->rowptr), ptr<int>(c->col),
-          ptr<double>(c->W64), ptr<float>(c->W32), c->kstride);
+          ptr<int>(c->master), ptr<double>(c->factors), c->step, ptr<int>(c->rowptr), ptr<int>(c->blkrow),
+          ptr<int>(c->col), ptr<double>(c->W64), ptr<float>(c->W32), c->kstride);
     } else {
       c->launches++;
       k_offdiag_copy<<<blocks_for(n, wpb), wpb * kWarp, 0, st>>>(
@@ -847,7 +863,8 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->st_base, &c->st_gap, &c->st_fric, &c->st_rest, &c->st_coh, &c->st_R0, &c->st_U0, &c->st_key,
                 &c->st_slo, &c->st_new, &c->det_point, &c->det_R0, &c->det_U0, &c->det_key, &c->det_slo,
                 &c->det_new, &c->cvx_body, &c->cvx_vptr, &c->cvx_vert, &c->cvx_fptr, &c->cvx_fac, &c->cvx_sptr,
-                &c->cvx_surf, &c->cvx_ns, &c->cvx_cur, &c->cvx_pla, &c->cvx_box};
+                &c->cvx_surf, &c->cvx_ns, &c->cvx_cur, &c->cvx_pla, &c->cvx_box,
+                &c->topo_m, &c->topo_s, &c->topo_o, &c->topo_flag, &c->blkrow};
   for (Buf* b : all)
     if (b->p) cudaFree(b->p);
   if (c->graph) cudaGraphExecDestroy(c->graph);
@@ -919,6 +936,17 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
   const int rb = blocks_for(n, T);
   B2_TRY(ensure(c->fe_part, sizeof(double) * rb));
   B2_CK(cudaMemsetAsync(c->bad.p, 0, sizeof(int), st));
+  // is the contact topology that of the last contact graph? (checked with the
+  // body indices below, in one synchronisation)
+  const bool topo_cand = c->topo_valid && c->topo_n == n && c->topo_nb == nb && n > 0;
+  if (topo_cand) {
+    B2_TRY(ensure(c->topo_flag, sizeof(int)));
+    B2_CK(cudaMemsetAsync(c->topo_flag.p, 0, sizeof(int), st));
+    c->launches++;
+    k_topology_diff<<<std::max(1, std::min(4 * c->sms, blocks_for(std::max(n, nb), T))), T, 0, st>>>(
+        n, nb, ptr<int>(c->master), ptr<int>(c->slave), ptr<int>(c->obst), ptr<int>(c->topo_m), ptr<int>(c->topo_s),
+        ptr<int>(c->topo_o), ptr<int>(c->topo_flag));
+  }
 
   SceneDev sc;
   sc.nbod = nb; sc.ncon = n;
@@ -942,12 +970,24 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
     k_problem_free_energy<<<c->nprob, 256, 0, st>>>(ptr<int>(c->pvec), ptr<double>(c->Aii), ptr<double>(c->B_c),
                                                     ptr<double>(c->pfe));
   }
+  bool same_topo = false;
   {  // body indices are checked before any kernel indexes per-body arrays with them
-    int bad0 = 0;
-    B2_CK(cudaMemcpyAsync(&bad0, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int flags[2] = {0, 1};
+    B2_CK(cudaMemcpyAsync(&flags[0], c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (topo_cand) B2_CK(cudaMemcpyAsync(&flags[1], c->topo_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaMemcpyAsync(&c->free_energy, c->fe_dev.p, sizeof(double), cudaMemcpyDeviceToHost, st));
     B2_CK(cudaStreamSynchronize(st));
-    if (bad0) { set_err("assemble: self-contact or invalid body index (outside the rigid contact path)"); return B2DEV_EUNSUPPORTED; }
+    if (flags[0]) { set_err("assemble: self-contact or invalid body index (outside the rigid contact path)"); return B2DEV_EUNSUPPORTED; }
+    same_topo = topo_cand && flags[1] == 0;
   }
+  if (same_topo) {  // the contact graph of the last assembly holds (adjptr, adjcol, adjbod, K)
+    B2_TRY(prepare_layout(c, colour_seed, true, true));
+    B2_CK(cudaEventRecord(c->ev[1], st));
+    B2_CK(cudaEventSynchronize(c->ev[1]));
+    cudaEventElapsedTime(&c->assemble_ms, c->ev[0], c->ev[1]);
+    return B2DEV_OK;
+  }
+  c->topo_valid = false;
 
   // contact graph through shared non-obstacle bodies
   B2_TRY(ensure(c->bdeg, sizeof(int) * (nb + 1)));
@@ -985,7 +1025,19 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
   c->launches++;
   k_adj_fill<<<rb, T, 0, st>>>(n, ptr<int>(c->master), ptr<int>(c->slave), ptr<int>(c->obst), ptr<int>(c->bptr),
                                ptr<int>(c->brow), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<int>(c->adjbod));
-  B2_TRY(prepare_layout(c, colour_seed, true));
+  // the topology this graph belongs to
+  B2_TRY(ensure(c->topo_m, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->topo_s, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->topo_o, sizeof(int) * (nb + 1)));
+  if (n > 0) {
+    B2_CK(cudaMemcpyAsync(c->topo_m.p, c->master.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
+    B2_CK(cudaMemcpyAsync(c->topo_s.p, c->slave.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
+  }
+  if (nb > 0) B2_CK(cudaMemcpyAsync(c->topo_o.p, c->obst.p, sizeof(int) * nb, cudaMemcpyDeviceToDevice, st));
+  c->topo_n = n;
+  c->topo_nb = nb;
+  c->topo_valid = true;
+  B2_TRY(prepare_layout(c, colour_seed, true, false));
   B2_CK(cudaEventRecord(c->ev[1], st));
   B2_CK(cudaEventSynchronize(c->ev[1]));
   cudaEventElapsedTime(&c->assemble_ms, c->ev[0], c->ev[1]);
@@ -1040,7 +1092,8 @@ int b2dev_upload_locdyn(b2dev_ctx* c, int n, const double* W, const double* A, c
     B2_CK(cudaStreamSynchronize(c->stream));
     if (bad) { set_err("adjptr/adjcol out of range"); return B2DEV_EINVAL; }
   }
-  return prepare_layout(c, colour_seed, false);
+  c->topo_valid = false;  // the contact graph buffers now hold the uploaded one
+  return prepare_layout(c, colour_seed, false, false);
 }
 
 int b2dev_set_state(b2dev_ctx* c, const double* R, const double* U, int on_device) {
