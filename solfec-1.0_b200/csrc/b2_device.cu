@@ -604,7 +604,7 @@ int solve_setup(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter
                 int u0_from_merit, int grid_req, SolveArgs* a, int* grid, size_t* smem) {
   const int n = c->n;
   const int P = c->nprob;
-  const void* fn = mixed ? (const void*)k_solve<true> : (const void*)k_solve<false>;
+  const void* fn = mixed ? (const void*)k_solve_fp32 : (const void*)k_solve<false>;
   // enough warps for the tiles of about two sweeps in flight, capped by residency
   const int want = grid_req > 0 ? grid_req : blocks_for(2LL * c->ntiles, kSolveWarps);
   // staging window: the largest tile if the shared memory of the blocks that
@@ -726,7 +726,7 @@ int solve_enqueue(b2dev_ctx* c, bool mixed, const SolveArgs& a, int grid, size_t
     B2_CK(cudaMemsetAsync(ptr<unsigned>(c->failcount) + a.iter0, 0, sizeof(unsigned) * (a.pstride - a.iter0), st));
   }
   if (a.trace) B2_CK(cudaMemsetAsync(a.trace, 0, sizeof(double) * kTraceStride * (n + 1), st));
-  const void* fn = mixed ? (const void*)k_solve<true> : (const void*)k_solve<false>;
+  const void* fn = mixed ? (const void*)k_solve_fp32 : (const void*)k_solve<false>;
   SolveArgs arg = a;
   void* args[] = {&arg};
   cudaLaunchConfig_t cfg;

@@ -188,7 +188,7 @@ __device__ __forceinline__ void scf_linearize(const ContactParams& cp, const dou
 }
 
 // projected_gradient (dbs.c:35-94)
-__device__ __noinline__ int projected_gradient(const ContactParams& cp, double epsilon, int maxiter, double rho,
+static __device__ __noinline__ int projected_gradient(const ContactParams& cp, double epsilon, int maxiter, double rho,
                                                const double* W, const double* B, const double* V, double* U,
                                                double* R) {
   if (cp.dynamic && cp.gap > 0) {
@@ -221,7 +221,7 @@ __device__ __noinline__ int projected_gradient(const ContactParams& cp, double e
 }
 
 // de_saxce_feng (dbs.c:96-140)
-__device__ __noinline__ int de_saxce_feng(const ContactParams& cp, double epsilon, int maxiter, double rho,
+static __device__ __noinline__ int de_saxce_feng(const ContactParams& cp, double epsilon, int maxiter, double rho,
                                           const double* W, const double* B, const double* V, double* U, double* R) {
   if (cp.dynamic && cp.gap > 0) {
     R[0] = R[1] = R[2] = 0.0;
@@ -342,7 +342,7 @@ __device__ __forceinline__ int semismooth_newton(const ContactParams& cp, double
 }
 
 // projected_newton (dbs.c:305-326)
-__device__ __noinline__ int projected_newton(const ContactParams& cp, double epsilon, int maxiter, const double* W,
+static __device__ __noinline__ int projected_newton(const ContactParams& cp, double epsilon, int maxiter, const double* W,
                                              const double* B, const double* V, double* U, double* R) {
   double T[9], X[9], Y[9], Cv[3];
   int iter = 0;
@@ -391,7 +391,7 @@ struct RowState {
 // PN, each from the previous reaction R0; if all fail the previous reaction is
 // kept (U keeps the last attempt's value). Returns the failure kind of the
 // first attempt: 0 none, 1 diverged (iterations >= maxiter), 2 failed (< 0).
-__device__ __noinline__ int diagonal_solve_row_slow(int solver, int failure, double epsilon, int maxiter, double rho,
+static __device__ __noinline__ int diagonal_solve_row_slow(int solver, int failure, double epsilon, int maxiter, double rho,
                                                     int it, RowState& st) {
   if (solver != DS_SEMISMOOTH_NEWTON) {
     it = diagonal_solve(solver, st.cp, epsilon, maxiter, rho, st.W, st.B, st.V, st.U, st.R);

@@ -160,7 +160,7 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 // the wait ran out (the timeout is recorded in ctrl). The first check is
 // inlined; only the spin is out of line (a call site saves live registers, so
 // the common case must not be a call).
-__device__ __noinline__ bool wait_at_least_spin(const int* p, int need, SolveControl* ctrl, uint64_t limit) {
+static __device__ __noinline__ bool wait_at_least_spin(const int* p, int need, SolveControl* ctrl, uint64_t limit) {
   const uint64_t t0 = globaltimer_ns();
   volatile int* stop = &ctrl->stop;
   volatile int* to = &ctrl->timeout;
@@ -180,7 +180,7 @@ __device__ __forceinline__ bool wait_at_least(const int* p, int need, SolveContr
 // sweep s-2 is to continue), 2 = skip (the problem has taken its final
 // decision, so later sweeps are discarded), 0 = the solve is ending or the
 // bounded wait gave up.
-__device__ __noinline__ int gate_wait_spin(const int* decided_s2, const int* pstop, SolveControl* ctrl, uint64_t limit) {
+static __device__ __noinline__ int gate_wait_spin(const int* decided_s2, const int* pstop, SolveControl* ctrl, uint64_t limit) {
   const uint64_t t0 = globaltimer_ns();
   volatile int* stop = &ctrl->stop;
   volatile int* to = &ctrl->timeout;
@@ -250,7 +250,7 @@ __device__ __forceinline__ bool stage_try_wait(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait for the staging copies of the given phase.
-__device__ __noinline__ bool stage_wait_spin(uint32_t bar, uint32_t parity, SolveControl* ctrl) {
+static __device__ __noinline__ bool stage_wait_spin(uint32_t bar, uint32_t parity, SolveControl* ctrl) {
   const uint64_t t0 = globaltimer_ns();
   while (!stage_try_wait(bar, parity)) {
     if (globaltimer_ns() - t0 > kBarrierLimitNs) { *(volatile int*)&ctrl->timeout = 1; return false; }
@@ -671,7 +671,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
 // the problem's last tile of the sweep: sums the problem's tile partials in
 // tile order and applies the reference's stopping rule (bgs.c:1028-1036,
 // mrf.c:176-184). Decisions of a problem are taken in sweep order.
-__device__ __noinline__ void finalize_sweep(const SolveArgs& a, int prob, int s) {
+static __device__ __noinline__ void finalize_sweep(const SolveArgs& a, int prob, int s) {
   const int lane = threadIdx.x & (kWarp - 1);
   ProblemControl* pc = a.pctl + prob;
   volatile int* decided = a.decided + (size_t)prob * a.pstride;
@@ -766,7 +766,7 @@ __device__ __noinline__ void finalize_sweep(const SolveArgs& a, int prob, int s)
 // list-order colouring a sweep has about six levels of ~1.5k tiles each, so
 // 1,776 resident warps hold a whole level in one wave.
 template <bool MIXED>
-__global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constant__ SolveArgs a) {
+__device__ __forceinline__ void solve_persistent(const SolveArgs& a) {
   extern __shared__ __align__(16) unsigned char solve_smem[];
   const int warp = threadIdx.x / kWarp;
   const int lane = threadIdx.x & (kWarp - 1);
@@ -837,5 +837,18 @@ __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constan
     }
   }
 }
+
+// FP64 sweeps (bitwise the reference's arithmetic: this translation unit is
+// built without fused multiply-adds).
+template <bool MIXED>
+__global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constant__ SolveArgs a) {
+  solve_persistent<MIXED>(a);
+}
+
+// FP32 sweeps of mixed precision, defined in b2_solve_fp32.cu: that
+// translation unit is built with fused multiply-adds, which the FP32 products
+// and the FP64 diagonal solves and merit of these sweeps may use (their results
+// are not bitwise the reference's anyway; the closing FP64 sweep is).
+__global__ void __launch_bounds__(kSolveThreads, 6) k_solve_fp32(const __grid_constant__ SolveArgs a);
 
 }  // namespace b2
