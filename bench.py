@@ -73,7 +73,7 @@ BYTES_BLOCK = {'fp64': 100, 'mixed': 52}
 BYTES_ROW = {'fp64': 316, 'mixed': 328}
 # DRAM bytes (read + write) per algorithmic byte of k_solve, measured by ncu on the 100x100x6 lattice
 # (one --set full capture per precision); DRAM traffic grows in proportion to blocks, rows and passes
-TRAFFIC_RATIO = {'fp64': 1178.1 / 1363.6, 'mixed': 647.1 / 739.2}
+TRAFFIC_RATIO = {'fp64': 1184.6 / 1363.6, 'mixed': 646.5 / 739.2}
 
 
 def _dist():
@@ -833,7 +833,7 @@ def roofline(mode, reps, n, K, peak):
     nl = max(len(reps), 1)
     return dict(bound='hbm', achieved=round(gbs, 1), peak=peak, unit='GB/s', frac=round(gbs / peak, 3),
                 traffic=int(bytes_all / nl * TRAFFIC_RATIO[mode]), traffic_source='ncu, 100x100x6 lattice, scaled',
-                kernel='k_solve<%s>' % ('true' if mode == 'mixed' else 'false'),
+                kernel='k_solve_fp32' if mode == 'mixed' else 'k_solve<false>',
                 bytes_per_launch=int(bytes_all / nl), sweeps_per_launch=round(sweeps / nl, 2),
                 kernel_ms_per_launch=round(ms / nl, 4), launches=len(reps))
 
