@@ -477,6 +477,67 @@ def block_sliding(step: float = 1e-3, friction: float = 0.8, density: float = 11
     return scene, J, mass
 
 
+def masonry_arch(ratio: float, step: float = 1e-3, friction: float = 0.5, density: float = 1.0, n: int = 27,
+                 radius: float = 10.0, width: float = 5.0):
+    """The scene of the reference's tests/arch.py as a fixed contact set: a
+    semicircular arch of n voussoirs (angle pi/n each, radius 10, thickness
+    ratio * radius, width 5, density 1) between two obstacle bases of one
+    voussoir each. The test meshes every voussoir 3 x 2 x 1, with radial cells
+    of relative sizes 0.05, 1.9, 0.05 (from the extrados) and two equal cells
+    across the width, so two touching voussoirs meet face to face on six cell
+    faces; the reference's convex-convex contact of two touching cells sits at
+    the centre of their common face. Each interface therefore carries six
+    contacts, at the cell-face centres, with the interface's normal (from the
+    voussoir at the lower angle to the one at the higher), gap 0, friction
+    0.5, no restitution or cohesion. Angles are measured from the vertical
+    (x = r sin a, z = r cos a). Returns (scene, J, mass)."""
+    dalpha = math.pi / n
+    t = ratio * radius
+
+    def hexahedron(alpha):  # the test's node order: far/near at the lower angle, then at the upper angle
+        out = []
+        for a in (alpha, alpha + dalpha):
+            for rr, y in ((radius + t / 2, -width / 2), (radius - t / 2, -width / 2), (radius - t / 2, width / 2),
+                          (radius + t / 2, width / 2)):
+                out.append([rr * math.sin(a), y, rr * math.cos(a)])
+        return np.array(out)
+
+    lows = [-0.5 * math.pi - dalpha, 0.5 * math.pi] + [-0.5 * math.pi + i * dalpha for i in range(n)]
+    nodes = np.stack([hexahedron(a) for a in lows])
+    corners = nodes[:, [0, 1, 3, 2, 4, 5, 7, 6]]          # unit-cube corner order (radial, width, angle)
+    vol, xc, Jc, mass = _hexahedron_mass(corners, density)
+    if np.any(vol <= 0):
+        vol, xc, Jc, mass = _hexahedron_mass(corners[:, [1, 0, 3, 2, 5, 4, 7, 6]], density)
+    nb = n + 2
+    obstacle = np.zeros(nb, dtype=np.int32); obstacle[:2] = 1
+    J = Jc.reshape(nb, 9)
+    jinv = np.stack([np.linalg.inv(Ji.reshape(3, 3)).T.reshape(9) for Ji in J])
+    jinv[obstacle != 0] = 0.0
+    minv = np.where(obstacle != 0, 0.0, 1.0 / mass)
+    # interfaces k = 0 .. n at angle -pi/2 + k dalpha: slave = the body below, master = the body above
+    below = [0] + [2 + i for i in range(n)]
+    above = [2 + i for i in range(n)] + [1]
+    fr = [0.0125, 0.5, 0.9875]                            # cell-face centres, fraction of t from the extrados
+    pts, nrm, master, slave = [], [], [], []
+    for k in range(n + 1):
+        a = -0.5 * math.pi + k * dalpha
+        for f in fr:
+            rr = radius + t / 2 - f * t
+            for y in (-width / 4, width / 4):
+                pts.append([rr * math.sin(a), y, rr * math.cos(a)])
+                nrm.append([math.cos(a), 0.0, -math.sin(a)])
+                master.append(above[k]); slave.append(below[k])
+    pts = np.array(pts); nc = pts.shape[0]
+    scene = Scene(name='masonry-arch-%g' % ratio, step=step, dynamic=1, rot=np.tile(np.eye(3).reshape(9), (nb, 1)),
+                  x=xc.copy(), x0=xc.copy(), jinv=jinv, minv=minv, velo=np.zeros((nb, 6)), velo0=np.zeros((nb, 6)),
+                  obstacle=obstacle, master=np.array(master, dtype=np.int32), slave=np.array(slave, dtype=np.int32),
+                  mpnt=pts.copy(), spnt=pts.copy(), base=local_base(np.array(nrm)), gap=np.zeros(nc),
+                  friction=np.full(nc, friction), restitution=np.zeros(nc), cohesion=np.zeros(nc), mass=mass)
+    Jr = J.copy(); Jr[obstacle != 0] = np.eye(3).reshape(9)
+    massr = np.where(obstacle != 0, 1.0, mass)
+    return scene, Jr, massr
+
+
 def block_sliding_loads(t: float) -> np.ndarray:
     """The test's block_force callback, 8 cos(t) along x on the block, as the
     (nbod, 9) load triples RIGID_DYNAMICS.step_begin takes."""

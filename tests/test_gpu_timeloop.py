@@ -34,8 +34,9 @@ def inertia(sc):
     return J, mass
 
 
-def time_loop_parity(sc, steps, **kw):
-    J, mass = inertia(sc)
+def time_loop_parity(sc, steps, J=None, mass=None, **kw):
+    if J is None:
+        J, mass = inertia(sc)
     h = float(sc.step)
     ldy = LOCDYN()
     ldy.update_begin(sc)
@@ -72,19 +73,34 @@ def time_loop_parity(sc, steps, **kw):
     for key in ('rot', 'x', 'velo'):
         assert same_bits(st[key], np.array(getattr(bd, key))), key
     ldy.close()
-    return iters
+    return iters, bd
 
 
 def test_config1_time_loop(scene_cache):
     """The 1000-sphere lattice of config 1 (FP64, epsilon = meritval = 1e-4),
     20 steps under gravity from its settled state."""
-    iters = time_loop_parity(scene_cache('spheres_lattice'), 20, epsilon=1e-4, maxiter=1000, meritval=1e-4)
+    iters, _ = time_loop_parity(scene_cache('spheres_lattice'), 20, epsilon=1e-4, maxiter=1000, meritval=1e-4)
     assert len(iters) == 20 and min(iters) >= 1
 
 
 def test_hexahedra_time_loop(scene_cache):
     """A 12 x 12 x 4 hexahedra lattice (the bench's scene shape), 15 steps
     from rest with the bench's stopping rule (merit 1e-4 decides)."""
-    iters = time_loop_parity(scene_cache('hexahedra_lattice', nx=12, ny=12, nz=4), 15, epsilon=1.0, maxiter=1000,
-                             meritval=1e-4)
+    iters, _ = time_loop_parity(scene_cache('hexahedra_lattice', nx=12, ny=12, nz=4), 15, epsilon=1.0,
+                                maxiter=1000, meritval=1e-4)
     assert iters[0] > iters[-1]
+
+
+def test_masonry_arch_threshold():
+    """The reference's tests/arch.py on the device: 750 steps of each arch,
+    GAUSS_SEIDEL_SOLVER (1E-4, 10000), bitwise with the CPU restatements at
+    every step, and its pass criterion (tests/arch.py:132): thickness ratio
+    0.1095 ends at rest (kinetic energy below 1e-4), 0.1094 collapses (above
+    1e-3)."""
+    energy = {}
+    for ratio in (0.1095, 0.1094):
+        sc, J, mass = scenes.masonry_arch(ratio)
+        iters, bd = time_loop_parity(sc, 750, J=J, mass=mass, epsilon=1e-4, maxiter=10000)
+        assert max(iters) > 1000  # the first steps of an arch at rest need thousands of sweeps
+        energy[ratio] = sum(ro.kinetic_energy(bd, b) for b in range(bd.nbod) if not bd.obstacle[b])
+    assert energy[0.1095] < 1e-4 and energy[0.1094] > 1e-3, energy

@@ -53,6 +53,37 @@ def test_block_sliding_pins_cpu(impl):
     check_pins(X, V)
 
 
+def run_arch_cpu(ratio, nsteps=750, impl='oracle'):
+    """The masonry arch of tests/arch.py as fixed contacts: 750 steps of 1 ms
+    under gravity, GAUSS_SEIDEL_SOLVER (1E-4, 10000) warm-started from the
+    previous reactions. Returns the kinetic energy of the voussoirs after the
+    last step (ENERGY (solfec) [0])."""
+    sc, J, mass = scenes.masonry_arch(ratio)
+    bd = ro.Bodies(sc.rot, sc.x, sc.velo, J, sc.jinv, mass, sc.minv, sc.x0, sc.obstacle)
+    R = np.zeros(3 * sc.ncon)
+    U = np.zeros(3 * sc.ncon)
+    for _ in range(nsteps):
+        ro.step_begin(bd, sc.step, (0.0, 0.0, -9.81))
+        cur = dataclasses.replace(sc, rot=np.array(bd.rot), x=np.array(bd.x), velo=np.array(bd.velo),
+                                  velo0=np.array(bd.velo0))
+        out = oracle.solve(oracle.assemble(cur), R, U, epsilon=1e-4, maxiter=10000, impl=impl)
+        R, U = out['R'], out['U']
+        ro.step_end(bd, sc.step, sc.master, sc.slave, sc.mpnt, sc.spnt, sc.base, R.reshape(-1, 3))
+    return sum(ro.kinetic_energy(bd, b) for b in range(bd.nbod) if not bd.obstacle[b])
+
+
+@pytest.mark.parametrize('impl', ['oracle', 'ref'])
+def test_masonry_arch_threshold_cpu(impl):
+    """The reference's pass criterion (tests/arch.py:132): after 750 steps the
+    arch of thickness ratio 0.1095 is at rest (kinetic energy below 1e-4) and
+    the one of ratio 0.1094 collapses (above 1e-3)."""
+    if impl == 'ref' and not oracle.ref_available():
+        pytest.skip('compiled reference solver not built')
+    e1 = run_arch_cpu(0.1095, impl=impl)
+    e2 = run_arch_cpu(0.1094, impl=impl)
+    assert e1 < 1e-4 and e2 > 1e-3, (e1, e2)
+
+
 def test_projectile_pin_cpu():
     """The reference's tests/projectile.py: drag load -m v and gravity, no
     contacts; the x distance after the run in inches within 0.5% of 86.138
