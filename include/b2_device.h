@@ -148,6 +148,28 @@ int b2dev_detect_spheres(b2dev_ctx* ctx, int* ncon, int* nnew);
  * Host memory; validated here. nconv = 0 removes them. */
 int b2dev_convexes_setup(b2dev_ctx* ctx, int nconv, const int* body, const int* vptr, const double* vert,
                          const int* fptr, const int* fac, const int* sptr, const int* surf);
+/* Convex-convex contacts (detect_convex_convex and update_convex_convex,
+ * goc.c:280-306 and 527-553, with cvi.c, hul.c and tri.c): b2dev_detect_spheres
+ * also pairs the convexes of b2dev_convexes_setup with one another (bodies
+ * different, not both obstacles; a convex c counts as object nsph + c, the
+ * pair key is (nsph + c1) << 32 | (nsph + c2) with c1 < c2). The lower convex
+ * is the reference's first object: the slave, whose outward normal the
+ * contact takes. Each pair is one contact at the area centre of the surface of
+ * the two convexes' intersection, with its normal, gap, area and surface pair;
+ * a pair with more than 32 face planes together is an error. Convexes of one
+ * body within GEOMETRIC_EPSILON of each other when set up are adjacent
+ * (cvx.c:575-589) for the sparsification.
+ *   b2dev_contact_sparsify: CONTACT_SPARSIFY (lng.c:8875-8899) threshold in
+ *     [0, 1] (default 0.01), minarea >= 0 (0), mindist >= 0
+ *     (GEOMETRIC_EPSILON), used by sparsify_contacts (dom.c:2956-3054): a new
+ *     contact of area below minarea goes; one of area below threshold times
+ *     that of another contact of the same two bodies goes when their objects
+ *     are adjacent; otherwise one within 2 mindist (max-norm) of another
+ *     contact's point goes when that one is old or later in key order.
+ *   b2dev_get_contact_area: the area of every detected contact (1 for sphere
+ *     contacts, goc.c:341 and 436). */
+int b2dev_contact_sparsify(b2dev_ctx* ctx, double threshold, double minarea, double mindist);
+int b2dev_get_contact_area(b2dev_ctx* ctx, double* area, int on_device);
 int b2dev_detect_carry_state(b2dev_ctx* ctx);
 int b2dev_get_contacts(b2dev_ctx* ctx, int* master, int* slave, double* point, double* mpnt, double* spnt,
                        double* base, double* gap, double* friction, double* restitution, long long* key,

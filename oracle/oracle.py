@@ -408,6 +408,23 @@ def ref_gobj_convex_sphere(ver, fac, surf, c, r, s, sphere_first=False, update=F
     return st, one, two, nrm, gap[0], sp
 
 
+def ref_gobj_convex_convex(va, fa, sa, vb, fb, sb, update=False, spair=(0, 0)):
+    """gobjcontact (goc.c:1362) of the reference for two convexes a (first)
+    and b, each as vertices, reference face layout (count, then indices) and
+    a surface per face: (state, onepnt, normal, gap, area, spair). For an
+    update, spair is the contact's current surface pair."""
+    lib = _load('geo')
+    va = np.ascontiguousarray(va, dtype=np.float64).reshape(-1)
+    vb = np.ascontiguousarray(vb, dtype=np.float64).reshape(-1)
+    fa = np.ascontiguousarray(fa, dtype=np.int32); fb = np.ascontiguousarray(fb, dtype=np.int32)
+    sa = np.ascontiguousarray(sa, dtype=np.int32); sb = np.ascontiguousarray(sb, dtype=np.int32)
+    one, two, nrm, gap, area = np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(1), np.zeros(1)
+    sp = np.array(spair, np.int32)
+    st = lib.ref_gobj_convex_convex(int(update), va.shape[0] // 3, va, sa.shape[0], fa, sa, vb.shape[0] // 3, vb,
+                                    sb.shape[0], fb, sb, one, two, nrm, gap, area, sp)
+    return st, one, nrm, gap[0], area[0], sp
+
+
 def ref_detect_spheres_hybrid(centre, radius, body, pairs=False):
     """The reference's CPU detection of a sphere set (hyb.c hybrid broad phase
     and detect_sphere_sphere per overlap): the number of contacts, or with
@@ -426,17 +443,3 @@ def ref_detect_spheres_hybrid(centre, radius, body, pairs=False):
         m = int(lib.ref_detect_spheres_hybrid(*args, out.ctypes.data_as(C.c_void_p), m))
     return out[:m]
 
-
-def ref_gobj_convex_convex(va, fa, sa, vb, fb, sb, update=False):
-    """gobjcontact of the reference for two convexes (detect_convex_convex,
-    goc.c:280-306): (state, onepnt, twopnt, normal, gap, area, spair)."""
-    lib = _load('geo')
-    va = np.ascontiguousarray(va, dtype=np.float64).reshape(-1)
-    vb = np.ascontiguousarray(vb, dtype=np.float64).reshape(-1)
-    fa, fb = np.ascontiguousarray(fa, dtype=np.int32), np.ascontiguousarray(fb, dtype=np.int32)
-    sa, sb = np.ascontiguousarray(sa, dtype=np.int32), np.ascontiguousarray(sb, dtype=np.int32)
-    one, two, nrm, gap, area, sp = (np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(1), np.zeros(1),
-                                    np.zeros(2, np.int32))
-    st = lib.ref_gobj_convex_convex(int(update), va.shape[0] // 3, va, sa.shape[0], fa, sa, vb.shape[0] // 3, vb,
-                                    sb.shape[0], fb, sb, one, two, nrm, gap, area, sp)
-    return st, one, two, nrm, gap[0], area[0], sp

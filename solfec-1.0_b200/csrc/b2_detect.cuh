@@ -44,9 +44,10 @@
 #include <cfloat>
 #include <cstdint>
 
-namespace b2 {
+#include "b2_cvi.cuh"
+#include "b2_gjk.cuh"
 
-constexpr double kGeomEps = 1e-6;  // GEOMETRIC_EPSILON, alg.c:24
+namespace b2 {
 
 struct SphereDev {
   int nsph, nbod;
@@ -149,112 +150,6 @@ struct ConvexDev {
   double* pla;         // per face unit normal and first vertex [6]
   double* box;         // per convex min[3], max[3] of the current vertices
 };
-
-// Johnson's sub-algorithm as gjk.c:213-330 evaluates it: sub-simplices tried
-// in a fixed order (singletons, pairs, triples, the whole simplex), the first
-// whose barycentric weights are positive on its members and non-positive off
-// them gives the projection of the origin. w[i] holds a Minkowski point and
-// wa[i] the index of its hull vertex.
-__device__ int johnson_project(double (*w)[3], int* wa, int n, double* l, double* v) {
-  const int sub_mask[15] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 11, 13, 14, 15};
-  const int sub_count[5] = {0, 0, 3, 7, 15};
-  double dot[4][4], delta[16][4];
-  if (n == 1) {
-    l[0] = 1.0;
-    v[0] = w[0][0]; v[1] = w[0][1]; v[2] = w[0][2];
-    return 1;
-  }
-  for (int i = 0; i < n; i++)
-    for (int j = i; j < n; j++) {
-      dot[i][j] = w[i][0] * w[j][0] + w[i][1] * w[j][1] + w[i][2] * w[j][2];
-      dot[j][i] = dot[i][j];
-    }
-  for (int m = 0; m < sub_count[n]; m++) {
-    const int s = sub_mask[m];
-    bool ok = true;
-    int k = -1;
-    if (__popc(s) == 1) {
-      for (int i = 0; i < n; i++)
-        if (s & (1 << i)) { delta[s][i] = 1.0; k = i; break; }
-      for (int j = 0; j < n; j++)
-        if (!(s & (1 << j))) {
-          delta[s][j] = dot[k][k] - dot[k][j];
-          if (delta[s][j] > 0.0) ok = false;
-        }
-    } else {
-      for (int i = 0; i < n; i++)
-        if (s & (1 << i)) {
-          if (k < 0) k = i;
-          delta[s][i] = delta[s & ~(1 << i)][i];
-          if (delta[s][i] <= 0.0) ok = false;
-        }
-      for (int j = 0; j < n; j++)
-        if (!(s & (1 << j))) {
-          delta[s][j] = 0.0;
-          for (int i = 0; i < n; i++)
-            if (s & (1 << i)) delta[s][j] += delta[s][i] * (dot[i][k] - dot[i][j]);
-          if (delta[s][j] > 0.0) ok = false;
-        }
-    }
-    if (ok) {
-      int o = 0;
-      double sum = 0.0;
-      for (int i = 0; i < n; i++)
-        if (s & (1 << i)) {
-          w[o][0] = w[i][0]; w[o][1] = w[i][1]; w[o][2] = w[i][2];
-          wa[o] = wa[i];
-          l[o] = delta[s][i];
-          sum += l[o];
-          o++;
-        }
-      v[0] = v[1] = v[2] = 0.0;
-      for (int i = 0; i < o; i++) {
-        l[i] /= sum;
-        for (int c = 0; c < 3; c++) v[c] = v[c] + l[i] * w[i][c];
-      }
-      return o;
-    }
-  }
-  return 0;
-}
-
-// gjk_convex_point, gjk.c:510-556: distance from p to the hull of the na
-// vertices a[3 na] and the nearest hull point q (an upper bound of the exact
-// distance within GEOMETRIC_EPSILON)
-__device__ double gjk_convex_point(const double* a, int na, const double* p, double* q) {
-  double w[4][3], v[3], l[4], mi = 0.0;
-  int wa[4];
-  int n = 0, j = 0;
-  bool toofar = true;
-  const int k = 4 * na * na;
-  v[0] = a[0] - p[0]; v[1] = a[1] - p[1]; v[2] = a[2] - p[2];
-  double vlen = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-  while (toofar && vlen > kGeomEps && n < 4 && j++ < k) {
-    double dmin = DBL_MAX;
-    int best = 0;
-    for (int t = 0; t < na; t++) {
-      const double d = a[3 * t] * v[0] + a[3 * t + 1] * v[1] + a[3 * t + 2] * v[2];
-      if (d < dmin) { dmin = d; best = t; }
-    }
-    wa[n] = best;
-    w[n][0] = a[3 * best] - p[0]; w[n][1] = a[3 * best + 1] - p[1]; w[n][2] = a[3 * best + 2] - p[2];
-    const double delta = (v[0] * w[n][0] + v[1] * w[n][1] + v[2] * w[n][2]) / vlen;
-    mi = mi > delta ? mi : delta;
-    toofar = (vlen - mi) > kGeomEps;
-    if (toofar) {
-      n = johnson_project(w, wa, n + 1, l, v);
-      vlen = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-    }
-  }
-  if (n) {
-    q[0] = q[1] = q[2] = 0.0;
-    for (n--; n >= 0; n--)
-      for (int c = 0; c < 3; c++) q[c] = q[c] + l[n] * a[3 * wa[n] + c];
-  } else {
-    q[0] = a[0]; q[1] = a[1]; q[2] = a[2];
-  }
-  return vlen;
-}
 
 // computeplanes (cvx.c:72-89) in CONVEX_Planes' layout, current vertices from
 // the body (CONVEX_Update, cvx.c:1362-1396) and the bounding box: one thread
@@ -474,6 +369,7 @@ __global__ void k_sph_sort_seg(int nsph, const int* off, int* pj, int* pi) {
 struct ContactOut {
   int* master; int* slave; double* point; double* mpnt; double* spnt; double* base; double* gap;
   double* fric; double* rest; double* coh; double* R0; double* U0; long long* key; int* slave_lo; int* isnew;
+  double* area;
 };
 
 __global__ void k_sph_contacts(int npair, SphereDev s, ConvexDev cv, const int* pi, const int* pj, const double* rot,
@@ -545,6 +441,7 @@ __global__ void k_sph_contacts(int npair, SphereDev s, ConvexDev cv, const int* 
       o.rest[k] = mat[2 * t + 1];
     }
     o.coh[k] = 0.0;
+    o.area[k] = 1.0;  // detect_convex_sphere, goc.c:341
     for (int v = 0; v < 3; v++) {
       o.R0[3 * (size_t)k + v] = hit >= 0 ? prevR[3 * (size_t)hit + v] : 0.0;
       o.U0[3 * (size_t)k + v] = hit >= 0 ? prevU[3 * (size_t)hit + v] : 0.0;
@@ -599,6 +496,135 @@ __global__ void k_sph_contacts(int npair, SphereDev s, ConvexDev cv, const int* 
     o.rest[k] = mat[2 * t + 1];
   }
   o.coh[k] = 0.0;
+  o.area[k] = 1.0;  // detect_sphere_sphere, goc.c:436
+  for (int v = 0; v < 3; v++) {
+    o.R0[3 * (size_t)k + v] = hit >= 0 ? prevR[3 * (size_t)hit + v] : 0.0;
+    o.U0[3 * (size_t)k + v] = hit >= 0 ? prevU[3 * (size_t)hit + v] : 0.0;
+  }
+}
+
+// ---- convex-convex pairs (detect_convex_convex / update_convex_convex) ----
+//
+// Broad phase: a sweep along x over the convexes' boxes inflated by
+// GEOMETRIC_EPSILON (CONVEX_Extents, cvx.c:1236-1260), sorted by their lower
+// x; a pair whose convexes are within GEOMETRIC_EPSILON of each other has
+// overlapping inflated boxes, so the sweep finds every pair that can touch.
+// Pairs of one body and pairs of two obstacles are left out (box.c:104-108).
+// A pair is keyed by its convexes c1 < c2 as (nsph + c1) << 32 | (nsph + c2);
+// the first object of the reference's gobjcontact is c1 (the slave, holding
+// the outward normal), the second c2 (the master), in detection and update
+// alike (overlap_create, dom.c:392-399; update_contact, dom.c:446-450).
+
+__global__ void k_cc_sweep_keys(ConvexDev cv, double* lox, int* idx) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cv.n) return;
+  lox[c] = cv.box[6 * c] - kGeomEps;
+  idx[c] = c;
+}
+
+// WRITE = false: cnt[p] = candidate pairs found from sorted position p;
+// WRITE = true: their keys from off[p]
+template <bool WRITE>
+__global__ void k_cc_pairs(ConvexDev cv, const int* obst, int nsph, const double* slox, const int* sidx, int* cnt,
+                           const int* off, long long* keys) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= cv.n) return;
+  const int i = sidx[p], bi = cv.body[i];
+  const double* bx = cv.box + 6 * i;
+  const double ilo[3] = {bx[0] - kGeomEps, bx[1] - kGeomEps, bx[2] - kGeomEps};
+  const double ihi[3] = {bx[3] + kGeomEps, bx[4] + kGeomEps, bx[5] + kGeomEps};
+  int found = 0, w = WRITE ? off[p] : 0;
+  for (int q = p + 1; q < cv.n && slox[q] <= ihi[0]; q++) {
+    const int j = sidx[q], bj = cv.body[j];
+    if (bj == bi || (obst[bi] && obst[bj])) continue;
+    const double* by = cv.box + 6 * j;
+    bool over = true;
+    for (int a = 1; a < 3 && over; a++)
+      over = by[a] - kGeomEps <= ihi[a] && ilo[a] <= by[3 + a] + kGeomEps;
+    if (!over) continue;
+    if (WRITE) {
+      const long long lo = nsph + (i < j ? i : j), hi = nsph + (i < j ? j : i);
+      keys[w++] = (lo << 32) | hi;
+    } else {
+      found++;
+    }
+  }
+  if (!WRITE) cnt[p] = found;
+}
+
+// the contact of candidate pair t (slot k0 + t of the staged arrays): the
+// polyhedral intersection of its convexes (b2_cvi.cuh); a pair without a
+// contact keeps master = slave = -1 and is dropped by the sparsification. Bad
+// flags: 8 a surface id out of the material table, 64 a pair over the
+// intersection's capacity (32 planes of both convexes together).
+__global__ void __launch_bounds__(64) k_cc_contacts(int ncc, int k0, int nsph, ConvexDev cv, const long long* ckey,
+                                                    const double* rot, const double* xb, const double* x0, int nsurf,
+                                                    const double* mat, int nprev, const long long* prevkey,
+                                                    const double* prevR, const double* prevU, ContactOut o, int* bad) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncc) return;
+  const int k = k0 + t;
+  const long long key = ckey[t];
+  const int c1 = (int)(key >> 32) - nsph, c2 = (int)(key & 0xFFFFFFFFLL) - nsph;
+  int hit = -1;
+  {
+    int lo = 0, hi = nprev - 1;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      const long long v = prevkey[mid];
+      if (v == key) { hit = mid; break; }
+      if (v < key) lo = mid + 1; else hi = mid - 1;
+    }
+  }
+  o.key[k] = key;
+  o.slave_lo[k] = 1;
+  o.isnew[k] = hit < 0;
+  o.master[k] = o.slave[k] = -1;
+  cvi::Convex A, B;
+  const int cc[2] = {c1, c2};
+  for (int e = 0; e < 2; e++) {
+    cvi::Convex& X = e ? B : A;
+    const int c = cc[e];
+    X.v = cv.cur + 3 * (size_t)cv.vptr[c];
+    X.nv = cv.vptr[c + 1] - cv.vptr[c];
+    X.pla = cv.pla + 6 * (size_t)cv.sptr[c];
+    X.np = cv.sptr[c + 1] - cv.sptr[c];
+    X.sur = cv.surf + cv.sptr[c];
+    X.ns = cv.nsurf_face[c];
+  }
+  cvi::Scratch scratch;
+  cvi::Contact ct;
+  // update_convex_convex differs from detect_convex_convex only in its return
+  // value (2 when the surface pair changed); the contact data are the same
+  const int state = cvi::convex_convex(A, B, false, ct, scratch);
+  if (state <= 0) {
+    if (state == cvi::kCviOverflow) atomicOr(bad, 64);
+    return;
+  }
+  const int bs = cv.body[c1], bm = cv.body[c2];
+  o.master[k] = bm;
+  o.slave[k] = bs;
+  for (int v = 0; v < 3; v++) o.point[3 * (size_t)k + v] = ct.point[v];
+  double X[3];
+  ref_point(rot + 9 * (size_t)bm, xb + 3 * (size_t)bm, x0 + 3 * (size_t)bm, ct.point, X);
+  for (int v = 0; v < 3; v++) o.mpnt[3 * (size_t)k + v] = X[v];
+  ref_point(rot + 9 * (size_t)bs, xb + 3 * (size_t)bs, x0 + 3 * (size_t)bs, ct.point, X);
+  for (int v = 0; v < 3; v++) o.spnt[3 * (size_t)k + v] = X[v];
+  double loc[9];
+  local_base(ct.normal, loc);
+  for (int v = 0; v < 9; v++) o.base[9 * (size_t)k + v] = loc[v];
+  o.gap[k] = ct.gap;
+  o.area[k] = ct.area;
+  const int s1 = ct.spair[0], s2 = ct.spair[1];
+  if (s1 < 0 || s1 >= nsurf || s2 < 0 || s2 >= nsurf) {
+    atomicOr(bad, 8);
+    o.fric[k] = o.rest[k] = 0.0;
+  } else {
+    const size_t u = (size_t)s1 * nsurf + s2;
+    o.fric[k] = mat[2 * u];
+    o.rest[k] = mat[2 * u + 1];
+  }
+  o.coh[k] = 0.0;
   for (int v = 0; v < 3; v++) {
     o.R0[3 * (size_t)k + v] = hit >= 0 ? prevR[3 * (size_t)hit + v] : 0.0;
     o.U0[3 * (size_t)k + v] = hit >= 0 ? prevU[3 * (size_t)hit + v] : 0.0;
@@ -612,6 +638,7 @@ __global__ void k_sph_body_count(int n, int nb, const int* master, const int* sl
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const int m = master[k], s = slave[k];
+  if (m == -1 && s == -1) return;  // a convex pair without a contact
   if (m < 0 || m >= nb || s < 0 || s >= nb) { atomicOr(bad, 16); return; }
   atomicAdd(bcnt + m, 1);
   atomicAdd(bcnt + s, 1);
@@ -626,21 +653,63 @@ __global__ void k_sph_body_fill(int n, int nb, const int* master, const int* sla
   blist[atomicAdd(cursor + s, 1)] = k;
 }
 
-// keep[k] = 0 for a new contact with a duplicate point (the decision does not
-// depend on the order of the body lists)
+// the objects of a contact as keyed (sphere i, or convex c as nsph + c): the
+// slave's and the master's
+__device__ __forceinline__ void contact_objects(long long key, int slave_lo, int& sobj, int& mobj) {
+  const int i = (int)(key >> 32), j = (int)(key & 0xFFFFFFFFLL);
+  sobj = slave_lo ? i : j;
+  mobj = slave_lo ? j : i;
+}
+
+// gobj_adjacent for two objects: convexes of one body that touched when they
+// were set up (CONVEX_Adjacent, cvx.c:1399-1409); spheres have no adjacency here
+__device__ __forceinline__ bool objects_adjacent(int x, int y, int nsph, const int* aptr, const int* alist) {
+  if (x < nsph || y < nsph || !aptr) return false;
+  const int cy = y - nsph;
+  for (int u = aptr[cy]; u < aptr[cy + 1]; u++)
+    if (alist[u] == x - nsph) return true;
+  return false;
+}
+
+// sparsify_contacts, dom.c:2956-3054: keep[k] = 0 for a convex pair without a
+// contact and for a new contact whose area is below minarea; a new contact
+// whose area is below threshold times that of another contact of its bodies
+// goes when the two contacts join the same pair of bodies through adjacent
+// objects; otherwise it goes when its point lies within margin (max-norm) of
+// the other contact's point and the other one is old or comes later in key
+// order (the reference compares contact ids, given in creation order). The
+// decision does not depend on the order of the body lists.
 __global__ void k_sph_sparsify(int n, int nb, const int* master, const int* slave, const int* isnew,
-                               const double* point, const int* bptr, const int* blist, double margin, int* keep) {
+                               const double* point, const double* area, const long long* key, const int* slave_lo,
+                               int nsph, const int* aptr, const int* alist, const int* bptr, const int* blist,
+                               double margin, double threshold, double minarea, int* keep) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   int kp = 1;
   const int m = master[k], s = slave[k];
-  if (isnew[k] && m >= 0 && m < nb && s >= 0 && s < nb) {
+  if (m == -1 && s == -1) {
+    kp = 0;
+  } else if (isnew[k] && m >= 0 && m < nb && s >= 0 && s < nb) {
     const double p0 = point[3 * (size_t)k], p1 = point[3 * (size_t)k + 1], p2 = point[3 * (size_t)k + 2];
+    const double ak = area[k];
+    int so, mo;
+    contact_objects(key[k], slave_lo[k], so, mo);
+    if (ak < minarea) kp = 0;
     const int bb[2] = {m, s};
     for (int t = 0; t < 2 && kp; t++)
       for (int u = bptr[bb[t]]; u < bptr[bb[t] + 1]; u++) {
         const int a = blist[u];
         if (a == k || a < 0 || a >= n) continue;
+        if (ak < threshold * area[a]) {
+          int sa, ma;
+          contact_objects(key[a], slave_lo[a], sa, ma);
+          if (m == master[a] && s == slave[a]) {
+            if (objects_adjacent(mo, ma, nsph, aptr, alist)) { kp = 0; break; }
+          } else if (m == slave[a] && s == master[a]) {
+            if (objects_adjacent(mo, sa, nsph, aptr, alist)) { kp = 0; break; }
+          }
+          continue;
+        }
         const double e0 = fabs(p0 - point[3 * (size_t)a]), e1 = fabs(p1 - point[3 * (size_t)a + 1]),
                      e2 = fabs(p2 - point[3 * (size_t)a + 2]);
         double mx = 0.0;
@@ -667,6 +736,7 @@ __global__ void k_sph_compact(int n, const int* keep, const int* pos, ContactOut
   out.fric[d] = in.fric[k];
   out.rest[d] = in.rest[k];
   out.coh[d] = in.coh[k];
+  out.area[d] = in.area[k];
   for (int v = 0; v < 3; v++) {
     out.point[3 * (size_t)d + v] = in.point[3 * (size_t)k + v];
     out.mpnt[3 * (size_t)d + v] = in.mpnt[3 * (size_t)k + v];

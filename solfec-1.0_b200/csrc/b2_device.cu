@@ -207,11 +207,17 @@ struct b2dev_ctx {
       sph_bstart, sph_bend, sph_cnt, sph_off, sph_pi, sph_pj, sph_rmax, sph_total, sph_keep, sph_pos, sph_bcnt, sph_bptr,
       sph_blist, sph_pkey, sph_pslo, sph_pR, sph_pU, sph_ccnt;
   Buf st_master, st_slave, st_point, st_mpnt, st_spnt, st_base, st_gap, st_fric, st_rest, st_coh, st_R0, st_U0,
-      st_key, st_slo, st_new;
-  Buf det_point, det_R0, det_U0, det_key, det_slo, det_new;
-  // convex obstacles of the detection (b2dev_convexes_setup)
+      st_key, st_slo, st_new, st_area;
+  Buf det_point, det_R0, det_U0, det_key, det_slo, det_new, det_area;
+  // convexes of the detection (b2dev_convexes_setup): their data, the
+  // adjacency of convexes of one body, and the convex-convex sweep
   int nconv = 0;
-  Buf cvx_body, cvx_vptr, cvx_vert, cvx_fptr, cvx_fac, cvx_sptr, cvx_surf, cvx_ns, cvx_cur, cvx_pla, cvx_box;
+  Buf cvx_body, cvx_vptr, cvx_vert, cvx_fptr, cvx_fac, cvx_sptr, cvx_surf, cvx_ns, cvx_cur, cvx_pla, cvx_box,
+      cvx_aptr, cvx_adj;
+  bool cvx_have_adj = false;
+  Buf cc_lox, cc_lox_s, cc_idx, cc_sidx, cc_cnt, cc_off, cc_keys, cc_keys_s;
+  // CONTACT_SPARSIFY (dom.c:3107-3109 defaults)
+  double sp_threshold = 0.01, sp_minarea = 0.0, sp_mindist = kGeomEps;
   bool det_valid = false;       // the scene's contacts are those of the last detection
   bool det_assembled = false;   // ... and the local dynamics was assembled from them
   std::vector<int> ptile_count;  // tiles per problem
@@ -863,7 +869,9 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->st_base, &c->st_gap, &c->st_fric, &c->st_rest, &c->st_coh, &c->st_R0, &c->st_U0, &c->st_key,
                 &c->st_slo, &c->st_new, &c->det_point, &c->det_R0, &c->det_U0, &c->det_key, &c->det_slo,
                 &c->det_new, &c->cvx_body, &c->cvx_vptr, &c->cvx_vert, &c->cvx_fptr, &c->cvx_fac, &c->cvx_sptr,
-                &c->cvx_surf, &c->cvx_ns, &c->cvx_cur, &c->cvx_pla, &c->cvx_box,
+                &c->cvx_surf, &c->cvx_ns, &c->cvx_cur, &c->cvx_pla, &c->cvx_box, &c->cvx_aptr, &c->cvx_adj,
+                &c->cc_lox, &c->cc_lox_s, &c->cc_idx, &c->cc_sidx, &c->cc_cnt, &c->cc_off, &c->cc_keys,
+                &c->cc_keys_s, &c->st_area, &c->det_area,
                 &c->topo_m, &c->topo_s, &c->topo_o, &c->topo_flag, &c->blkrow};
   for (Buf* b : all)
     if (b->p) cudaFree(b->p);
@@ -1298,6 +1306,36 @@ int b2dev_convexes_setup(b2dev_ctx* c, int nconv, const int* body, const int* vp
   B2_TRY(upload(c, c->cvx_sptr, sptr, (size_t)nconv + (nconv > 0), 0));
   B2_TRY(upload(c, c->cvx_surf, surf, (size_t)nft, 0));
   B2_TRY(upload(c, c->cvx_ns, ns.data(), (size_t)nconv, 0));
+  // adjacency of the convexes of one body: those within GEOMETRIC_EPSILON of
+  // each other as set up (the overlap callback of cvx.c:575-589); a rigid
+  // body's convexes keep it
+  {
+    std::vector<std::vector<int>> of_body(c->nbod);
+    for (int k = 0; k < nconv; k++) of_body[body[k]].push_back(k);
+    std::vector<std::vector<int>> adj(std::max(nconv, 1));
+    bool any = false;
+    for (const auto& list : of_body)
+      for (size_t a = 0; a < list.size(); a++)
+        for (size_t b = a + 1; b < list.size(); b++) {
+          const int x = list[a], y = list[b];
+          double p[3], q[3];
+          if (gjk_polytopes(vert + 3 * (size_t)vptr[x], vptr[x + 1] - vptr[x], vert + 3 * (size_t)vptr[y],
+                            vptr[y + 1] - vptr[y], p, q) < kGeomEps) {
+            adj[x].push_back(y);
+            adj[y].push_back(x);
+            any = true;
+          }
+        }
+    std::vector<int> aptr(nconv + 1, 0), alist;
+    for (int k = 0; k < nconv; k++) {
+      aptr[k + 1] = aptr[k] + (int)adj[k].size();
+      alist.insert(alist.end(), adj[k].begin(), adj[k].end());
+    }
+    alist.push_back(0);
+    B2_TRY(upload(c, c->cvx_aptr, aptr.data(), aptr.size(), 0));
+    B2_TRY(upload(c, c->cvx_adj, alist.data(), alist.size(), 0));
+    c->cvx_have_adj = any;
+  }
   B2_TRY(ensure(c->cvx_cur, sizeof(double) * 3 * (nvt + 1)));
   B2_TRY(ensure(c->cvx_pla, sizeof(double) * 6 * (nft + 1)));
   B2_TRY(ensure(c->cvx_box, sizeof(double) * 6 * (nconv + 1)));
@@ -1322,6 +1360,7 @@ static const char* detect_bad_text(int bad) {
   if (bad & 2) return "a sphere centre is too far from the origin for the detection grid";
   if (bad & 4) return "two sphere centres coincide (no contact normal)";
   if (bad & 32) return "a convex has no finite face plane";
+  if (bad & 64) return "a convex pair has more than 32 face planes together (intersection capacity)";
   return "a surface id is out of the material table";
 }
 
@@ -1332,7 +1371,21 @@ static ContactOut staged(b2dev_ctx* c) {
   o.gap = ptr<double>(c->st_gap); o.fric = ptr<double>(c->st_fric); o.rest = ptr<double>(c->st_rest);
   o.coh = ptr<double>(c->st_coh); o.R0 = ptr<double>(c->st_R0); o.U0 = ptr<double>(c->st_U0);
   o.key = ptr<long long>(c->st_key); o.slave_lo = ptr<int>(c->st_slo); o.isnew = ptr<int>(c->st_new);
+  o.area = ptr<double>(c->st_area);
   return o;
+}
+
+int b2dev_contact_sparsify(b2dev_ctx* c, double threshold, double minarea, double mindist) {
+  if (!c) { set_err("contact_sparsify: null context"); return B2DEV_EINVAL; }
+  // lng.c:8875-8899 (CONTACT_SPARSIFY): threshold in [0, 1], minarea and mindist not negative
+  if (!(threshold >= 0.0 && threshold <= 1.0) || !(minarea >= 0.0) || !(mindist >= 0.0)) {
+    set_err("contact_sparsify: threshold must lie in [0, 1], minarea and mindist must not be negative");
+    return B2DEV_EINVAL;
+  }
+  c->sp_threshold = threshold;
+  c->sp_minarea = minarea;
+  c->sp_mindist = mindist;
+  return B2DEV_OK;
 }
 
 int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
@@ -1396,16 +1449,16 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
   sd.hkey = ptr<unsigned int>(c->sph_hkey);
   const ConvexDev cvd = convex_view(c);
   int npair = 0, bad = 0;
+  if (c->nconv > 0) {
+    c->launches++;
+    k_cvx_update<<<blocks_for(c->nconv, 64), 64, 0, st>>>(cvd, ptr<double>(c->rot), ptr<double>(c->rb_x),
+                                                        ptr<double>(c->x0));
+  }
   if (ns > 0) {
     c->launches += 2;
     k_sph_centres<<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<double>(c->rot), ptr<double>(c->rb_x),
                                                    ptr<double>(c->x0), ptr<unsigned long long>(c->sph_rmax),
                                                    ptr<int>(c->bad));
-    if (c->nconv > 0) {
-      c->launches++;
-      k_cvx_update<<<blocks_for(c->nconv, 64), 64, 0, st>>>(cvd, ptr<double>(c->rot), ptr<double>(c->rb_x),
-                                                          ptr<double>(c->x0));
-    }
     k_sph_cells<<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<unsigned long long>(c->sph_rmax), M - 1,
                                                  ptr<int>(c->sph_idx), ptr<int>(c->bad));
     size_t bytes = 0;
@@ -1452,6 +1505,61 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     B2_CK(cudaMemcpyAsync(&npair, ptr<int>(c->sph_off) + ns, sizeof(int), cudaMemcpyDeviceToHost, st));
     B2_CK(cudaStreamSynchronize(st));
   }
+  const int nps = npair;  // pairs with a sphere; the convex-convex candidates follow (their keys are larger)
+
+  // convex-convex candidates: a sweep over the x-sorted inflated boxes, the
+  // keys then sorted
+  int ncc = 0;
+  const int nv = c->nconv;
+  if (nv > 1) {
+    B2_TRY(ensure(c->cc_lox, sizeof(double) * (nv + 1)));
+    B2_TRY(ensure(c->cc_lox_s, sizeof(double) * (nv + 1)));
+    B2_TRY(ensure(c->cc_idx, sizeof(int) * (nv + 1)));
+    B2_TRY(ensure(c->cc_sidx, sizeof(int) * (nv + 1)));
+    B2_TRY(ensure(c->cc_cnt, sizeof(int) * (nv + 1)));
+    B2_TRY(ensure(c->cc_off, sizeof(int) * (nv + 1)));
+    B2_TRY(ensure(c->sph_total, sizeof(unsigned long long)));
+    c->launches++;
+    k_cc_sweep_keys<<<blocks_for(nv, T), T, 0, st>>>(cvd, ptr<double>(c->cc_lox), ptr<int>(c->cc_idx));
+    size_t bytes = 0;
+    B2_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, ptr<double>(c->cc_lox), ptr<double>(c->cc_lox_s),
+                                          ptr<int>(c->cc_idx), ptr<int>(c->cc_sidx), nv, 0, 64, st));
+    B2_TRY(ensure(c->cub_tmp, bytes));
+    B2_CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, bytes, ptr<double>(c->cc_lox), ptr<double>(c->cc_lox_s),
+                                          ptr<int>(c->cc_idx), ptr<int>(c->cc_sidx), nv, 0, 64, st));
+    c->launches += 2;
+    k_cc_pairs<false><<<blocks_for(nv, T), T, 0, st>>>(cvd, ptr<int>(c->obst), ns, ptr<double>(c->cc_lox_s),
+                                                       ptr<int>(c->cc_sidx), ptr<int>(c->cc_cnt), nullptr, nullptr);
+    unsigned long long total = 0;
+    B2_CK(cudaMemsetAsync(c->sph_total.p, 0, sizeof(unsigned long long), st));
+    k_count_total<<<std::min(blocks_for(nv, T), 4 * c->sms), T, 0, st>>>(nv, ptr<int>(c->cc_cnt),
+                                                                         ptr<unsigned long long>(c->sph_total));
+    B2_CK(cudaMemcpyAsync(&total, c->sph_total.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaMemcpyAsync(&bad, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2_CK(cudaStreamSynchronize(st));
+    if (bad) { set_err("detect: %s", detect_bad_text(bad)); return B2DEV_EINVAL; }
+    if (total + (unsigned long long)nps > (unsigned long long)(INT_MAX / 2 - 1)) {
+      set_err("detect: %llu candidate pairs exceed the supported %d", total + nps, INT_MAX / 2 - 1);
+      return B2DEV_EINVAL;
+    }
+    ncc = (int)total;
+    if (ncc > 0) {
+      B2_TRY(scan_exclusive(c, ptr<int>(c->cc_cnt), ptr<int>(c->cc_off), nv));
+      B2_TRY(ensure(c->cc_keys, sizeof(long long) * (ncc + 1)));
+      B2_TRY(ensure(c->cc_keys_s, sizeof(long long) * (ncc + 1)));
+      c->launches++;
+      k_cc_pairs<true><<<blocks_for(nv, T), T, 0, st>>>(cvd, ptr<int>(c->obst), ns, ptr<double>(c->cc_lox_s),
+                                                        ptr<int>(c->cc_sidx), nullptr, ptr<int>(c->cc_off),
+                                                        ptr<long long>(c->cc_keys));
+      bytes = 0;
+      B2_CK(cub::DeviceRadixSort::SortKeys(nullptr, bytes, ptr<unsigned long long>(c->cc_keys),
+                                           ptr<unsigned long long>(c->cc_keys_s), ncc, 0, 64, st));
+      B2_TRY(ensure(c->cub_tmp, bytes));
+      B2_CK(cub::DeviceRadixSort::SortKeys(c->cub_tmp.p, bytes, ptr<unsigned long long>(c->cc_keys),
+                                           ptr<unsigned long long>(c->cc_keys_s), ncc, 0, 64, st));
+    }
+  }
+  npair = nps + ncc;
 
   // contacts of the pairs, in pair order
   const size_t np1 = (size_t)npair + 1;
@@ -1472,6 +1580,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
   B2_TRY(ensure(c->st_key, sizeof(long long) * np1));
   B2_TRY(ensure(c->st_slo, sizeof(int) * np1));
   B2_TRY(ensure(c->st_new, sizeof(int) * np1));
+  B2_TRY(ensure(c->st_area, sizeof(double) * np1));
   B2_TRY(ensure(c->sph_keep, sizeof(int) * np1));
   B2_TRY(ensure(c->sph_pos, sizeof(int) * np1));
   B2_TRY(ensure(c->sph_bcnt, sizeof(int) * (nb + 1)));
@@ -1480,22 +1589,31 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
   const ContactOut so = staged(c);
   int nkeep = 0, nfresh = 0;
   if (npair > 0) {
-    c->launches += 3;
-    k_sph_pairs<true><<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<int>(c->obst), ptr<int>(c->sph_sorted),
-                                                       ptr<int>(c->sph_bstart), ptr<int>(c->sph_bend), M - 1,
-                                                       nullptr, ptr<int>(c->sph_off), ptr<int>(c->sph_pj));
-    if (c->nconv > 0) {  // after the sphere partners (sph_cnt still holds their count)
-      c->launches++;
-      k_cvx_pairs<true><<<blocks_for(ns, 128), 128, 0, st>>>(sd, cvd, ptr<int>(c->obst), nullptr,
-                                                              ptr<int>(c->sph_off), ptr<int>(c->sph_cnt),
-                                                              ptr<int>(c->sph_pj));
+    if (nps > 0) {
+      c->launches += 3;
+      k_sph_pairs<true><<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<int>(c->obst), ptr<int>(c->sph_sorted),
+                                                         ptr<int>(c->sph_bstart), ptr<int>(c->sph_bend), M - 1,
+                                                         nullptr, ptr<int>(c->sph_off), ptr<int>(c->sph_pj));
+      if (c->nconv > 0) {  // after the sphere partners (sph_cnt still holds their count)
+        c->launches++;
+        k_cvx_pairs<true><<<blocks_for(ns, 128), 128, 0, st>>>(sd, cvd, ptr<int>(c->obst), nullptr,
+                                                                ptr<int>(c->sph_off), ptr<int>(c->sph_cnt),
+                                                                ptr<int>(c->sph_pj));
+      }
+      k_sph_sort_seg<<<blocks_for(ns, T), T, 0, st>>>(ns, ptr<int>(c->sph_off), ptr<int>(c->sph_pj),
+                                                      ptr<int>(c->sph_pi));
+      k_sph_contacts<<<blocks_for(nps, T), T, 0, st>>>(
+          nps, sd, cvd, ptr<int>(c->sph_pi), ptr<int>(c->sph_pj), ptr<double>(c->rot), ptr<double>(c->rb_x),
+          ptr<double>(c->x0), c->nsurf, ptr<double>(c->sph_mat), nprev, ptr<long long>(c->sph_pkey),
+          ptr<int>(c->sph_pslo), ptr<double>(c->sph_pR), ptr<double>(c->sph_pU), so, ptr<int>(c->bad));
     }
-    k_sph_sort_seg<<<blocks_for(ns, T), T, 0, st>>>(ns, ptr<int>(c->sph_off), ptr<int>(c->sph_pj),
-                                                    ptr<int>(c->sph_pi));
-    k_sph_contacts<<<blocks_for(npair, T), T, 0, st>>>(
-        npair, sd, cvd, ptr<int>(c->sph_pi), ptr<int>(c->sph_pj), ptr<double>(c->rot), ptr<double>(c->rb_x),
-        ptr<double>(c->x0), c->nsurf, ptr<double>(c->sph_mat), nprev, ptr<long long>(c->sph_pkey),
-        ptr<int>(c->sph_pslo), ptr<double>(c->sph_pR), ptr<double>(c->sph_pU), so, ptr<int>(c->bad));
+    if (ncc > 0) {
+      c->launches++;
+      k_cc_contacts<<<blocks_for(ncc, 64), 64, 0, st>>>(
+          ncc, nps, ns, cvd, ptr<long long>(c->cc_keys_s), ptr<double>(c->rot), ptr<double>(c->rb_x),
+          ptr<double>(c->x0), c->nsurf, ptr<double>(c->sph_mat), nprev, ptr<long long>(c->sph_pkey),
+          ptr<double>(c->sph_pR), ptr<double>(c->sph_pU), so, ptr<int>(c->bad));
+    }
     // sparsification neighbourhoods: the contacts of each body
     B2_CK(cudaMemsetAsync(c->sph_bcnt.p, 0, sizeof(int) * (nb + 1), st));
     c->launches++;
@@ -1506,9 +1624,10 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     c->launches += 2;
     k_sph_body_fill<<<blocks_for(npair, T), T, 0, st>>>(npair, nb, so.master, so.slave, ptr<int>(c->sph_bcnt),
                                                         ptr<int>(c->sph_blist));
-    k_sph_sparsify<<<blocks_for(npair, T), T, 0, st>>>(npair, nb, so.master, so.slave, so.isnew, so.point,
-                                                       ptr<int>(c->sph_bptr), ptr<int>(c->sph_blist),
-                                                       2.0 * kGeomEps, ptr<int>(c->sph_keep));
+    k_sph_sparsify<<<blocks_for(npair, T), T, 0, st>>>(
+        npair, nb, so.master, so.slave, so.isnew, so.point, so.area, so.key, so.slave_lo, ns,
+        c->cvx_have_adj ? ptr<int>(c->cvx_aptr) : nullptr, ptr<int>(c->cvx_adj), ptr<int>(c->sph_bptr),
+        ptr<int>(c->sph_blist), 2.0 * c->sp_mindist, c->sp_threshold, c->sp_minarea, ptr<int>(c->sph_keep));
     B2_TRY(scan_exclusive(c, ptr<int>(c->sph_keep), ptr<int>(c->sph_pos), npair));
     int lastpos = 0, lastkeep = 0;
     B2_CK(cudaMemcpyAsync(&lastpos, ptr<int>(c->sph_pos) + npair - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1529,6 +1648,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     std::swap(c->gap_c, c->st_gap); std::swap(c->fric_c, c->st_fric); std::swap(c->rest_c, c->st_rest);
     std::swap(c->coh_c, c->st_coh); std::swap(c->det_R0, c->st_R0); std::swap(c->det_U0, c->st_U0);
     std::swap(c->det_key, c->st_key); std::swap(c->det_slo, c->st_slo); std::swap(c->det_new, c->st_new);
+    std::swap(c->det_area, c->st_area);
   } else {
     B2_TRY(ensure(c->master, sizeof(int) * nk1));
     B2_TRY(ensure(c->slave, sizeof(int) * nk1));
@@ -1545,6 +1665,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     B2_TRY(ensure(c->det_key, sizeof(long long) * nk1));
     B2_TRY(ensure(c->det_slo, sizeof(int) * nk1));
     B2_TRY(ensure(c->det_new, sizeof(int) * nk1));
+    B2_TRY(ensure(c->det_area, sizeof(double) * nk1));
     if (npair > 0) {
       ContactOut d;
       d.master = ptr<int>(c->master); d.slave = ptr<int>(c->slave); d.point = ptr<double>(c->det_point);
@@ -1552,6 +1673,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
       d.gap = ptr<double>(c->gap_c); d.fric = ptr<double>(c->fric_c); d.rest = ptr<double>(c->rest_c);
       d.coh = ptr<double>(c->coh_c); d.R0 = ptr<double>(c->det_R0); d.U0 = ptr<double>(c->det_U0);
       d.key = ptr<long long>(c->det_key); d.slave_lo = ptr<int>(c->det_slo); d.isnew = ptr<int>(c->det_new);
+      d.area = ptr<double>(c->det_area);
       c->launches++;
       k_sph_compact<<<blocks_for(npair, T), T, 0, st>>>(npair, ptr<int>(c->sph_keep), ptr<int>(c->sph_pos), so,
                                                          d);
@@ -1609,6 +1731,17 @@ int b2dev_get_contacts(b2dev_ctx* c, int* master, int* slave, double* point, dou
     if (U0) B2_CK(cudaMemcpyAsync(U0, c->det_U0.p, sizeof(double) * 3 * n, kd, st));
   }
   B2_CK(cudaStreamSynchronize(st));
+  return B2DEV_OK;
+}
+
+int b2dev_get_contact_area(b2dev_ctx* c, double* area, int on_device) {
+  if (!c || !c->det_valid) { set_err("get_contact_area: no detection"); return B2DEV_ESTATE; }
+  if (!area) { set_err("get_contact_area: null output"); return B2DEV_EINVAL; }
+  DeviceGuard g(c->device);
+  if (c->ncon > 0)
+    B2_CK(cudaMemcpyAsync(area, c->det_area.p, sizeof(double) * c->ncon,
+                          on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
+  B2_CK(cudaStreamSynchronize(c->stream));
   return B2DEV_OK;
 }
 

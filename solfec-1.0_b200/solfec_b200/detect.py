@@ -20,6 +20,15 @@ reference's detect_convex_sphere does: the closest hull point by GJK
 (gjk_convex_point), the convex as the slave, the material of the nearest face's
 surface.
 
+Convexes of different bodies collide with one another as the reference's
+detect_convex_convex and update_convex_convex do (goc.c:280-306, 527-553): one
+contact per pair at the area centre of the surface of the convexes'
+intersection polytope (cvi.c, hul.c, tri.c, restated in csrc/b2_cvi.cuh), with
+its normal, gap, area and surface pair. Pairs come from a sweep over the
+convexes' eps-inflated boxes; the lower convex of a pair is the slave. A
+scene of convex bodies alone is a SPHERES with no spheres (CONVEXES).
+Sparsification follows CONTACT_SPARSIFY (sparsify).
+
 Materials: a symmetric table (nsurf, nsurf, 2) of friction and restitution per
 surface pair (SPSET_Find resolved by the caller). Cohesion is not supported:
 the reference gives it only to contacts created at time zero and updates
@@ -105,6 +114,12 @@ class SPHERES:
                'b2dev_convexes_setup')
         self.nconv = nc
 
+    def sparsify(self, threshold=0.01, minarea=0.0, mindist=1e-6):
+        """CONTACT_SPARSIFY (lng.c:8875-8899) for the sparsification of new
+        contacts (sparsify_contacts, dom.c:2956-3054)."""
+        _check(lib().b2dev_contact_sparsify(self.ldy.device_context, float(threshold), float(minarea),
+                                            float(mindist)), 'CONTACT_SPARSIFY')
+
     def detect(self):
         """Update and detection of the contacts; returns (contacts, new contacts)."""
         nc, nn = C.c_int(0), C.c_int(0)
@@ -128,12 +143,23 @@ class SPHERES:
                  'slave_lo', 'isnew', 'R', 'U']
         _check(lib().b2dev_get_contacts(self.ldy.device_context, *[ptr(out[k]) for k in names], 0),
                'b2dev_get_contacts')
+        out['area'] = np.zeros(m)
+        if n > 0:
+            _check(lib().b2dev_get_contact_area(self.ldy.device_context, ptr(out['area']), 0),
+                   'b2dev_get_contact_area')
         return {k: v[:n] for k, v in out.items()}
 
     def centres(self) -> np.ndarray:
         cur = np.zeros((max(self.nsph, 1), 3))
         _check(lib().b2dev_sphere_centres(self.ldy.device_context, ptr(cur), 0), 'b2dev_sphere_centres')
         return cur[:self.nsph]
+
+
+def CONVEXES(ldy: LOCDYN, convex: dict, material=(0.0, 0.0)) -> SPHERES:
+    """Convex shapes of the bodies of a LOCDYN's device scene, no spheres:
+    convex = the keyword arguments of SPHERES.set_convexes."""
+    e = np.zeros(0)
+    return SPHERES(ldy, np.zeros(0, np.int32), np.zeros((0, 3)), e, material=material, convex=convex)
 
 
 def bodies_only(scene):

@@ -720,6 +720,109 @@ def box_convex(lo, hi):
     return v, np.array(fac, np.int32)
 
 
+def _convex_arrays(convexes, bodies):
+    """set_convexes arguments from a list of (vertices (nv, 3), faces as vertex
+    index lists, surface id per face) and a body per convex."""
+    vptr, fptr, sptr, vert, fac, surf = [0], [0], [0], [], [], []
+    for (v, faces, sids) in convexes:
+        vert.append(np.asarray(v, float))
+        for f in faces:
+            fac += [len(f)] + list(f)
+        surf += list(sids)
+        vptr.append(vptr[-1] + len(v)); fptr.append(len(fac)); sptr.append(len(surf))
+    return dict(body=np.asarray(bodies, np.int32), vptr=np.array(vptr, np.int32), vert=np.concatenate(vert),
+                fptr=np.array(fptr, np.int32), fac=np.array(fac, np.int32), sptr=np.array(sptr, np.int32),
+                surf=np.array(surf, np.int32))
+
+
+def convex_list(cv):
+    """Per convex of set_convexes arguments: (vertices (nv, 3), reference face
+    layout (count, then indices), surface ids)."""
+    out = []
+    for c in range(cv['body'].shape[0]):
+        out.append((cv['vert'][cv['vptr'][c]:cv['vptr'][c + 1]], cv['fac'][cv['fptr'][c]:cv['fptr'][c + 1]],
+                    cv['surf'][cv['sptr'][c]:cv['sptr'][c + 1]]))
+    return out
+
+
+def hull_faces(points):
+    """Triangles of the convex hull of points, counter-clockwise seen from
+    outside: (vertices used, faces as index triples)."""
+    from scipy.spatial import ConvexHull
+    P = np.asarray(points, float)
+    H = ConvexHull(P)
+    used = sorted(set(H.simplices.ravel()))
+    remap = {u: i for i, u in enumerate(used)}
+    V = P[used]
+    cen = V.mean(axis=0)
+    faces = []
+    for s in H.simplices:
+        a, b, c = (remap[i] for i in s)
+        if np.dot(np.cross(V[b] - V[a], V[c] - V[b]), V[a] - cen) < 0:
+            b, c = c, b
+        faces.append((a, b, c))
+    return V, faces
+
+
+def convex_pile(seed: int = 1, nx: int = 5, ny: int = 4, nz: int = 3, hulls: int = 20, nsurf: int = 7):
+    """Convex bodies for contact detection checks, every body at the origin
+    with the identity rotation (its convex's vertices are its current ones):
+    an nx x ny x nz lattice of unit boxes on a floor obstacle, a third of them
+    exact (faces touching exactly), the rest with sizes and positions jittered
+    by a few thousandths (touching, slightly overlapping or slightly apart),
+    some of those turned by up to 3 degrees; `hulls` random convex hulls of 6 to
+    8 points dropped over the top layer and among the boxes. Surface ids are
+    seeded per face in 0 .. nsurf - 1.
+
+    Returns (scene without contacts, set_convexes arguments)."""
+    rng = np.random.default_rng(seed)
+    convexes, kinds = [], []
+
+    def box(c, h, R=None):
+        v = np.array([[(-h[0], h[0])[i], (-h[1], h[1])[j], (-h[2], h[2])[k]] for k in (0, 1) for j in (0, 1)
+                      for i in (0, 1)])
+        if R is not None:
+            v = v @ R.T
+        return v + c
+
+    def turn(angle):
+        w = rng.normal(size=3)
+        w *= angle / np.linalg.norm(w)
+        K = np.array([[0, -w[2], w[1]], [w[2], 0, -w[0]], [-w[1], w[0], 0]])
+        a = np.linalg.norm(w)
+        return np.eye(3) + np.sin(a) / a * K + (1 - np.cos(a)) / a ** 2 * K @ K
+
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                c = np.array([i, j, k + 0.5], float)
+                t = rng.integers(3)
+                if t == 0:
+                    v = box(c, np.full(3, 0.5))
+                elif t == 1:
+                    v = box(c + rng.uniform(-2e-3, 2e-3, 3), 0.5 * (1 + rng.uniform(-3e-3, 3e-3, 3)))
+                else:
+                    v = box(c + rng.uniform(-2e-3, 2e-3, 3), 0.5 * (1 + rng.uniform(-3e-3, 3e-3, 3)),
+                            turn(rng.uniform(0, np.radians(3))))
+                convexes.append((v, HEX_FACES, rng.integers(nsurf, size=6)))
+    for _ in range(hulls):
+        c = np.array([rng.uniform(0, nx - 1), rng.uniform(0, ny - 1), rng.uniform(nz - 0.6, nz + 0.3)])
+        V, faces = hull_faces(c + rng.normal(size=(int(rng.integers(6, 9)), 3)) * 0.3)
+        convexes.append((V, faces, rng.integers(nsurf, size=len(faces))))
+    floor = box(np.array([(nx - 1) / 2, (ny - 1) / 2, -0.25]), np.array([nx / 2 + 1, ny / 2 + 1, 0.25]))
+    convexes.append((floor, HEX_FACES, rng.integers(nsurf, size=6)))
+    nb = len(convexes)
+    obstacle = np.zeros(nb, np.int32); obstacle[-1] = 1
+    e = np.zeros(0)
+    eye = np.tile(np.eye(3).reshape(9), (nb, 1))
+    sc = Scene(name='convex-pile-%d' % nb, step=1e-3, dynamic=1, rot=eye.copy(), x=np.zeros((nb, 3)),
+               x0=np.zeros((nb, 3)), jinv=np.where(obstacle[:, None] != 0, 0.0, eye), minv=1.0 - obstacle,
+               velo=np.zeros((nb, 6)), velo0=np.zeros((nb, 6)), obstacle=obstacle, master=np.zeros(0, np.int32),
+               slave=np.zeros(0, np.int32), mpnt=np.zeros((0, 3)), spnt=np.zeros((0, 3)), base=np.zeros((0, 9)),
+               gap=e, friction=e, restitution=e, cohesion=e, mass=np.ones(nb))
+    return sc, _convex_arrays(convexes, np.arange(nb))
+
+
 def spheres_in_box(seed: int = 9, n_side: int = 5, layers: int = 3, radius: float = 0.05, pitch: float = 0.11,
                    wall: float = 0.05, clearance: float = 0.002, density: float = 2000.0, friction: float = 0.3,
                    step: float = 1e-3):

@@ -3,6 +3,8 @@ gjk_sphere_sphere pinned bit for bit to the reference's own gjk.c (compiled
 into oracle/_ref), the restated contact formulas against an independent
 vectorised restatement, and the update, filter and sparsification rules of
 dom.c and box.c on hand-built cases."""
+import os
+
 import numpy as np
 import pytest
 
@@ -452,3 +454,22 @@ def test_clumps_of_spheres():
     assert (0, 1) not in pairs and (2, 3) not in pairs
     assert (0, 2) in pairs and (1, 3) in pairs
     assert set(zip(out['master'].tolist(), out['slave'].tolist())) <= {(0, 1), (1, 0)}
+
+
+@pytest.mark.skipif(not oracle.geo_available(), reason='reference build unavailable')
+def test_convex_convex_golden_pinned_to_reference():
+    """tests/golden/convex/pile_ref.npz (make_cvi_golden.py) holds exactly the
+    reference's gobjcontact results (detect_convex_convex, goc.c:280-306) for
+    every convex pair of the seeded convex piles, bit for bit."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location('make_cvi_golden', os.path.join(os.path.dirname(
+        os.path.abspath(__file__)), 'golden', 'make_cvi_golden.py'))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'convex', 'pile_ref.npz'))
+    for seed, kw in gen.CASES:
+        now = gen.reference_pairs(seed, kw)
+        assert now['keys'].shape[0] > 20
+        for name, v in now.items():
+            stored = g['s%d_%s' % (seed, name)]
+            assert stored.shape == v.shape and np.array_equal(stored.view(np.uint8), v.view(np.uint8)), (seed, name)
