@@ -504,6 +504,80 @@ def detect_timing(grid=DETECT_GRID):
         ldy.close()
 
 
+CONVEX_LATTICE = dict(nx=50, ny=50, nz=10)
+CONVEX_CPU_PAIRS = 1500
+
+
+def detect_convex_timing():
+    """Host call time of the convex-convex contact update and detection
+    (b2dev_detect_spheres with convexes only: k_cvx_update, the sweep over the
+    inflated boxes, k_cc_contacts, sparsification) on a lattice of boxes with
+    exact, jittered and turned members on a floor obstacle: the first call
+    detects every contact, the timed calls (after 3 warm-up calls) update them
+    all. CPU baseline: the reference's own gobjcontact (detect_convex_convex,
+    oracle/_ref) on a sample of the contact pairs, one host core; its broad
+    phase and the domain insertion are not timed, which favours it."""
+    import time
+    import torch
+    from solfec_b200 import LOCDYN, scenes
+    from solfec_b200.detect import CONVEXES, bodies_only
+    from solfec_b200.dynamics import RIGID_DYNAMICS
+    sc, cv = scenes.convex_lattice(**CONVEX_LATTICE)
+    J = np.tile(np.eye(3).reshape(9), (sc.nbod, 1))
+    ldy = LOCDYN()
+    try:
+        ldy.update_begin(bodies_only(sc))
+        RIGID_DYNAMICS(ldy, J, np.ones(sc.nbod), sc.x)
+        nsurf = int(cv['surf'].max()) + 1
+        mat = np.zeros((nsurf, nsurf, 2))
+        mat[..., 0] = 0.5
+        det = CONVEXES(ldy, cv, mat)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        nc, nn = det.detect()
+        first = time.perf_counter() - t0
+        for _ in range(3):
+            det.detect()
+        ts = []
+        for _ in range(DETECT_REPS):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            det.detect()
+            ts.append(time.perf_counter() - t0)
+        ms = float(np.median(ts)) * 1e3
+        keys = det.contacts()['key']
+        out = {'workload': 'convex-lattice-%d: %dx%dx%d unit boxes (a third exact, a third jittered, a third '
+                           'also turned) on a floor' % (sc.nbod - 1, CONVEX_LATTICE['nx'], CONVEX_LATTICE['ny'],
+                                                      CONVEX_LATTICE['nz']),
+               'convexes': int(sc.nbod), 'contacts': int(nc), 'new_first_call': int(nn),
+               'first_call_ms': round(first * 1e3, 3), 'update_call_ms': round(ms, 3),
+               'contacts_per_s': round(nc / (ms * 1e-3), 1),
+               'timing': 'host call time, median of %d' % DETECT_REPS}
+        try:
+            sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+            import oracle as O
+            if not O.geo_available():
+                raise RuntimeError('reference geometry build unavailable')
+            conv = scenes.convex_list(cv)
+            rng = np.random.default_rng(0)
+            sample = keys[rng.choice(keys.shape[0], min(CONVEX_CPU_PAIRS, keys.shape[0]), replace=False)]
+            args = [(conv[int(k >> 32)], conv[int(k & 0xFFFFFFFF)]) for k in sample]
+            t0 = time.perf_counter()
+            for a, b in args:
+                O.ref_gobj_convex_convex(*a, *b)
+            dt = time.perf_counter() - t0
+            out['cpu_baseline'] = {'value': round(len(args) / dt, 1), 'unit': 'contacts/s', 'cores': 1,
+                                   'kind': 'reference',
+                                   'sample': '%d contact pairs of the same lattice through the reference gobjcontact '
+                                             '(detect_convex_convex), %.2f s; broad phase and insertion untimed'
+                                             % (len(args), dt)}
+        except Exception as e:  # the reference build is test infrastructure: its absence costs only this figure
+            out['cpu_baseline'] = {'error': str(e)[:200]}
+        return out
+    finally:
+        ldy.close()
+
+
 def _rigid_inertia(sc, k=None):
     k = sc.nbod if k is None else k
     ob = sc.obstacle[:k] != 0  # walls: zero inverse inertia and mass (never accelerated)
@@ -930,7 +1004,8 @@ def main():
     ap.add_argument('--no-configs', action='store_true', help='skip the configs 1, 2 and 4 legs of the default line')
     ap.add_argument('--scene', default=None, help='NXxNYxNZ lattice of a smaller case (profiling)')
     ap.add_argument('--maxiter', type=int, default=None, help='iteration cap of a smaller case (profiling)')
-    ap.add_argument('--workload', default='hexahedra', choices=['hexahedra', 'batched', 'detect'])
+    ap.add_argument('--workload', default='hexahedra', choices=['hexahedra', 'batched', 'detect', 'detect-convex'])
+    ap.add_argument('--convex-lattice', default=None, help='NXxNYxNZ boxes of the convex detection case')
     ap.add_argument('--detect-grid', type=int, default=DETECT_GRID, help='spheres per grid side (--workload detect)')
     args = ap.parse_args()
     global WORKLOAD
@@ -955,6 +1030,17 @@ def main():
         d = detect_timing(args.detect_grid)
         if rank == 0:
             print(json.dumps(dict(d, metric='sphere contact update call time', impl='product')), flush=True)
+        if ws > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return
+    if args.workload == 'detect-convex':  # convex-convex contact detection alone (profiling)
+        torch.cuda.set_device(local)
+        if args.convex_lattice:
+            CONVEX_LATTICE.update(zip(('nx', 'ny', 'nz'), (int(v) for v in args.convex_lattice.lower().split('x'))))
+        d = detect_convex_timing()
+        if rank == 0:
+            print(json.dumps(dict(d, metric='convex contact update call time', impl='product')), flush=True)
         if ws > 1:
             torch.distributed.barrier()
             torch.distributed.destroy_process_group()
@@ -1068,6 +1154,10 @@ def main():
             line['detect'] = detect_timing()
         except Exception as e:  # the headline line is printed whatever happens here
             line['detect'] = {'error': str(e)[:300]}
+        try:
+            line['detect_convex'] = detect_convex_timing()
+        except Exception as e:
+            line['detect_convex'] = {'error': str(e)[:300]}
         print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.barrier()

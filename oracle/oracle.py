@@ -216,6 +216,8 @@ def _detect_sigs(lib):
     lib.orc_localbase.argtypes = [_dp, _dp]
     lib.orc_sphere_centres.restype = None
     lib.orc_sphere_centres.argtypes = [C.c_int, _ip, _dp, _dp, _dp, _dp, _dp]
+    lib.orc_ref_points.restype = None
+    lib.orc_ref_points.argtypes = [C.c_int, _ip, _dp, _dp, _dp, _dp, _dp]
     lib.orc_detect_spheres.restype = C.c_int
     lib.orc_detect_spheres.argtypes = ([C.c_int, _ip, _dp, _dp, _ip, C.c_int, _dp, _dp, _dp, _ip, C.c_int, _dp,
                                         C.c_int, _lp, _ip, _dp, _dp, C.c_int,
@@ -314,6 +316,19 @@ def sphere_centres(sbody, sref, rot, x, x0):
                            np.ascontiguousarray(x, dtype=np.float64).reshape(-1),
                            np.ascontiguousarray(x0, dtype=np.float64).reshape(-1), cur)
     return cur
+
+
+def ref_points(body, pts, rot, x, x0):
+    """BODY_Ref_Point (bod.c:1736-1750) of spatial points pts[k] on bodies body[k]."""
+    lib = _load('oracle')
+    _detect_sigs(lib)
+    body = np.ascontiguousarray(body, dtype=np.int32)
+    out = np.zeros((body.shape[0], 3))
+    lib.orc_ref_points(body.shape[0], body, np.ascontiguousarray(pts, dtype=np.float64).reshape(-1),
+                       np.ascontiguousarray(rot, dtype=np.float64).reshape(-1),
+                       np.ascontiguousarray(x, dtype=np.float64).reshape(-1),
+                       np.ascontiguousarray(x0, dtype=np.float64).reshape(-1), out)
+    return out
 
 
 def detect_spheres(sbody, sref, radius, surface, rot, x, x0, obstacle, material, prev=None, convex=None):

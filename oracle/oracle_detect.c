@@ -372,6 +372,17 @@ void orc_sphere_centres (int nsph, const int *sbody, const double *sref, const d
   }
 }
 
+/* BODY_Ref_Point for a list of spatial points, each of its body */
+void orc_ref_points (int n, const int *body, const double *pts, const double *rot, const double *x,
+                     const double *x0, double *out)
+{
+  for (int k = 0; k < n; k++)
+  {
+    const int b = body[k];
+    ref_point (rot + 9 * (size_t) b, x + 3 * (size_t) b, x0 + 3 * (size_t) b, pts + 3 * (size_t) k, out + 3 * (size_t) k);
+  }
+}
+
 typedef struct { long long key; int slave_lo; double R[3], U[3]; } prevrec;
 
 static int prevcmp (const void *a, const void *b)

@@ -505,51 +505,128 @@ __global__ void k_sph_contacts(int npair, SphereDev s, ConvexDev cv, const int* 
 
 // ---- convex-convex pairs (detect_convex_convex / update_convex_convex) ----
 //
-// Broad phase: a sweep along x over the convexes' boxes inflated by
-// GEOMETRIC_EPSILON (CONVEX_Extents, cvx.c:1236-1260), sorted by their lower
-// x; a pair whose convexes are within GEOMETRIC_EPSILON of each other has
-// overlapping inflated boxes, so the sweep finds every pair that can touch.
-// Pairs of one body and pairs of two obstacles are left out (box.c:104-108).
-// A pair is keyed by its convexes c1 < c2 as (nsph + c1) << 32 | (nsph + c2);
-// the first object of the reference's gobjcontact is c1 (the slave, holding
-// the outward normal), the second c2 (the master), in detection and update
-// alike (overlap_create, dom.c:392-399; update_contact, dom.c:446-450).
+// Broad phase: a uniform grid over the centres of the convexes' boxes, its
+// cell edge the largest box side of the ordinary convexes plus
+// 2 GEOMETRIC_EPSILON; convexes whose box side exceeds kLargeConvex times the
+// mean (floors, walls) are listed apart and tested against every convex.
+// Two convexes within GEOMETRIC_EPSILON of each other have overlapping
+// eps-inflated boxes (CONVEX_Extents, cvx.c:1236-1260), so their centres lie
+// in neighbouring cells; a candidate pair then passes the box test and the
+// GJK distance test of cvi (cvi.c:128-129, gjk of the lower convex first),
+// which leaves the narrow phase only pairs that touch. Pairs of one body and
+// pairs of two obstacles are left out (box.c:104-108). A pair is keyed by its
+// convexes c1 < c2 as (nsph + c1) << 32 | (nsph + c2); the first object of the
+// reference's gobjcontact is c1 (the slave, holding the outward normal), the
+// second c2 (the master), in detection and update alike (overlap_create,
+// dom.c:392-399; update_contact, dom.c:446-450).
 
-__global__ void k_cc_sweep_keys(ConvexDev cv, double* lox, int* idx) {
+constexpr double kLargeConvex = 4.0;
+
+// ext[c] = the largest side of convex c's box; sum += ext[c]
+__global__ void k_cc_extent(ConvexDev cv, double* ext, double* sum) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cv.n) return;
-  lox[c] = cv.box[6 * c] - kGeomEps;
-  idx[c] = c;
+  const double* b = cv.box + 6 * c;
+  double e = b[3] - b[0];
+  if (b[4] - b[1] > e) e = b[4] - b[1];
+  if (b[5] - b[2] > e) e = b[5] - b[2];
+  ext[c] = e;
+  atomicAdd(sum, e);
 }
 
-// WRITE = false: cnt[p] = candidate pairs found from sorted position p;
-// WRITE = true: their keys from off[p]
+__device__ __forceinline__ bool cc_large(const double* ext, const double* sum, int n, int c) {
+  return ext[c] > kLargeConvex * (*sum / n);
+}
+
+// the largest side among ordinary convexes (bits of a non-negative double);
+// the large ones listed
+__global__ void k_cc_classify(int n, const double* ext, const double* sum, unsigned long long* emax, int* large,
+                              int* nlarge) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  if (cc_large(ext, sum, n, c)) large[atomicAdd(nlarge, 1)] = c;
+  else atomicMax(emax, (unsigned long long)__double_as_longlong(ext[c]));
+}
+
+// grid cell of an ordinary convex's box centre and its bucket; a large
+// convex goes to bucket mask + 1, which no cell probes. Bad flag 2: a centre
+// too far from the origin for the grid.
+__global__ void k_cc_cells(ConvexDev cv, const double* ext, const double* sum, const unsigned long long* emax,
+                           unsigned int mask, int4* cell, unsigned int* hkey, int* idx, int* bad) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cv.n) return;
+  idx[c] = c;
+  if (cc_large(ext, sum, cv.n, c)) {
+    cell[c] = make_int4(0, 0, 0, 1);
+    hkey[c] = mask + 1;
+    return;
+  }
+  const double h = __longlong_as_double((long long)*emax) + 2.0 * kGeomEps;
+  const double* b = cv.box + 6 * c;
+  int q[3];
+  for (int k = 0; k < 3; k++) {
+    const double f = floor(0.5 * (b[k] + b[3 + k]) / h);
+    if (!(fabs(f) < 1.0e9)) { atomicOr(bad, 2); q[k] = 0; }
+    else q[k] = (int)f;
+  }
+  cell[c] = make_int4(q[0], q[1], q[2], 0);
+  hkey[c] = cell_hash(q[0], q[1], q[2], mask);
+}
+
+__device__ __forceinline__ bool cc_candidate(const ConvexDev& cv, const int* obst, int i, int j) {
+  const int bi = cv.body[i], bj = cv.body[j];
+  if (bi == bj || (obst[bi] && obst[bj])) return false;
+  const double* a = cv.box + 6 * i;
+  const double* b = cv.box + 6 * j;
+  for (int k = 0; k < 3; k++)
+    if (!(b[k] - kGeomEps <= a[3 + k] + kGeomEps && a[k] - kGeomEps <= b[3 + k] + kGeomEps)) return false;
+  const int lo = i < j ? i : j, hi = i < j ? j : i;
+  double p[3], q[3];
+  return gjk_polytopes(cv.cur + 3 * (size_t)cv.vptr[lo], cv.vptr[lo + 1] - cv.vptr[lo],
+                       cv.cur + 3 * (size_t)cv.vptr[hi], cv.vptr[hi + 1] - cv.vptr[hi], p, q) <= kGeomEps;
+}
+
+// per sorted position t (convex i = sorted[t]): its partners j > i of the 27
+// cells around it (ordinary convexes), and the large convexes l (a large i
+// pairs only with large l > i). WRITE = false: cnt[t]; WRITE = true: the keys
+// from off[t].
 template <bool WRITE>
-__global__ void k_cc_pairs(ConvexDev cv, const int* obst, int nsph, const double* slox, const int* sidx, int* cnt,
-                           const int* off, long long* keys) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= cv.n) return;
-  const int i = sidx[p], bi = cv.body[i];
-  const double* bx = cv.box + 6 * i;
-  const double ilo[3] = {bx[0] - kGeomEps, bx[1] - kGeomEps, bx[2] - kGeomEps};
-  const double ihi[3] = {bx[3] + kGeomEps, bx[4] + kGeomEps, bx[5] + kGeomEps};
-  int found = 0, w = WRITE ? off[p] : 0;
-  for (int q = p + 1; q < cv.n && slox[q] <= ihi[0]; q++) {
-    const int j = sidx[q], bj = cv.body[j];
-    if (bj == bi || (obst[bi] && obst[bj])) continue;
-    const double* by = cv.box + 6 * j;
-    bool over = true;
-    for (int a = 1; a < 3 && over; a++)
-      over = by[a] - kGeomEps <= ihi[a] && ilo[a] <= by[3 + a] + kGeomEps;
-    if (!over) continue;
+__global__ void k_cc_pairs(ConvexDev cv, const int* obst, int nsph, const int* sorted, const int4* cell,
+                           const int* bstart, const int* bend, unsigned int mask, const int* large, int nlarge,
+                           int* cnt, const int* off, long long* keys) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cv.n) return;
+  const int i = sorted[t];
+  const int4 ci = cell[i];
+  int found = 0, w = WRITE ? off[t] : 0;
+  auto emit = [&](int j) {
     if (WRITE) {
       const long long lo = nsph + (i < j ? i : j), hi = nsph + (i < j ? j : i);
       keys[w++] = (lo << 32) | hi;
-    } else {
-      found++;
     }
+    found++;
+  };
+  if (ci.w == 0) {
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+          const int nx = ci.x + dx, ny = ci.y + dy, nz = ci.z + dz;
+          const unsigned int hb = cell_hash(nx, ny, nz, mask);
+          for (int u = bstart[hb]; u < bend[hb]; u++) {
+            const int j = sorted[u];
+            if (j <= i) continue;
+            const int4 cj = cell[j];
+            if (cj.x != nx || cj.y != ny || cj.z != nz) continue;  // another cell in the same bucket
+            if (cc_candidate(cv, obst, i, j)) emit(j);
+          }
+        }
   }
-  if (!WRITE) cnt[p] = found;
+  for (int u = 0; u < nlarge; u++) {
+    const int l = large[u];
+    if (l == i || (ci.w != 0 && l < i)) continue;
+    if (cc_candidate(cv, obst, i, l)) emit(l);
+  }
+  if (!WRITE) cnt[t] = found;
 }
 
 // the contact of candidate pair t (slot k0 + t of the staged arrays): the

@@ -215,7 +215,8 @@ struct b2dev_ctx {
   Buf cvx_body, cvx_vptr, cvx_vert, cvx_fptr, cvx_fac, cvx_sptr, cvx_surf, cvx_ns, cvx_cur, cvx_pla, cvx_box,
       cvx_aptr, cvx_adj;
   bool cvx_have_adj = false;
-  Buf cc_lox, cc_lox_s, cc_idx, cc_sidx, cc_cnt, cc_off, cc_keys, cc_keys_s;
+  Buf cc_lox, cc_idx, cc_sidx, cc_cnt, cc_off, cc_keys, cc_keys_s, cc_cell, cc_hkey, cc_hkey_s, cc_large,
+      cc_bstart, cc_bend, cc_misc;
   // CONTACT_SPARSIFY (dom.c:3107-3109 defaults)
   double sp_threshold = 0.01, sp_minarea = 0.0, sp_mindist = kGeomEps;
   bool det_valid = false;       // the scene's contacts are those of the last detection
@@ -870,8 +871,9 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->st_slo, &c->st_new, &c->det_point, &c->det_R0, &c->det_U0, &c->det_key, &c->det_slo,
                 &c->det_new, &c->cvx_body, &c->cvx_vptr, &c->cvx_vert, &c->cvx_fptr, &c->cvx_fac, &c->cvx_sptr,
                 &c->cvx_surf, &c->cvx_ns, &c->cvx_cur, &c->cvx_pla, &c->cvx_box, &c->cvx_aptr, &c->cvx_adj,
-                &c->cc_lox, &c->cc_lox_s, &c->cc_idx, &c->cc_sidx, &c->cc_cnt, &c->cc_off, &c->cc_keys,
-                &c->cc_keys_s, &c->st_area, &c->det_area,
+                &c->cc_lox, &c->cc_idx, &c->cc_sidx, &c->cc_cnt, &c->cc_off, &c->cc_keys, &c->cc_keys_s,
+                &c->cc_cell, &c->cc_hkey, &c->cc_hkey_s, &c->cc_large, &c->cc_bstart, &c->cc_bend, &c->cc_misc,
+                &c->st_area, &c->det_area,
                 &c->topo_m, &c->topo_s, &c->topo_o, &c->topo_flag, &c->blkrow};
   for (Buf* b : all)
     if (b->p) cudaFree(b->p);
@@ -1507,29 +1509,59 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
   }
   const int nps = npair;  // pairs with a sphere; the convex-convex candidates follow (their keys are larger)
 
-  // convex-convex candidates: a sweep over the x-sorted inflated boxes, the
-  // keys then sorted
+  // convex-convex candidates: the grid over the box centres of ordinary
+  // convexes and the list of large ones, counted, written, the keys sorted
   int ncc = 0;
   const int nv = c->nconv;
   if (nv > 1) {
+    unsigned int Mc = 1024;
+    while (Mc < 2u * (unsigned int)nv) Mc *= 2;
+    int cbits = 0;
+    while ((1u << cbits) <= Mc) cbits++;  // keys up to Mc (the large convexes' bucket)
     B2_TRY(ensure(c->cc_lox, sizeof(double) * (nv + 1)));
-    B2_TRY(ensure(c->cc_lox_s, sizeof(double) * (nv + 1)));
     B2_TRY(ensure(c->cc_idx, sizeof(int) * (nv + 1)));
     B2_TRY(ensure(c->cc_sidx, sizeof(int) * (nv + 1)));
     B2_TRY(ensure(c->cc_cnt, sizeof(int) * (nv + 1)));
     B2_TRY(ensure(c->cc_off, sizeof(int) * (nv + 1)));
+    B2_TRY(ensure(c->cc_cell, sizeof(int4) * (nv + 1)));
+    B2_TRY(ensure(c->cc_hkey, sizeof(unsigned int) * (nv + 1)));
+    B2_TRY(ensure(c->cc_hkey_s, sizeof(unsigned int) * (nv + 1)));
+    B2_TRY(ensure(c->cc_large, sizeof(int) * (nv + 1)));
+    B2_TRY(ensure(c->cc_bstart, sizeof(int) * (Mc + 1)));
+    B2_TRY(ensure(c->cc_bend, sizeof(int) * (Mc + 1)));
+    B2_TRY(ensure(c->cc_misc, 32));  // extent sum (double), largest ordinary side (bits), large count (int)
     B2_TRY(ensure(c->sph_total, sizeof(unsigned long long)));
-    c->launches++;
-    k_cc_sweep_keys<<<blocks_for(nv, T), T, 0, st>>>(cvd, ptr<double>(c->cc_lox), ptr<int>(c->cc_idx));
+    double* esum = ptr<double>(c->cc_misc);
+    unsigned long long* emax = ptr<unsigned long long>(c->cc_misc) + 1;
+    int* nlarge_d = reinterpret_cast<int*>(ptr<unsigned long long>(c->cc_misc) + 2);
+    B2_CK(cudaMemsetAsync(c->cc_misc.p, 0, 32, st));
+    B2_CK(cudaMemsetAsync(c->cc_bstart.p, 0, sizeof(int) * (Mc + 1), st));
+    B2_CK(cudaMemsetAsync(c->cc_bend.p, 0, sizeof(int) * (Mc + 1), st));
+    c->launches += 3;
+    k_cc_extent<<<blocks_for(nv, T), T, 0, st>>>(cvd, ptr<double>(c->cc_lox), esum);
+    k_cc_classify<<<blocks_for(nv, T), T, 0, st>>>(nv, ptr<double>(c->cc_lox), esum, emax, ptr<int>(c->cc_large),
+                                                   nlarge_d);
+    k_cc_cells<<<blocks_for(nv, T), T, 0, st>>>(cvd, ptr<double>(c->cc_lox), esum, emax, Mc - 1,
+                                                ptr<int4>(c->cc_cell), ptr<unsigned int>(c->cc_hkey),
+                                                ptr<int>(c->cc_idx), ptr<int>(c->bad));
     size_t bytes = 0;
-    B2_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, ptr<double>(c->cc_lox), ptr<double>(c->cc_lox_s),
-                                          ptr<int>(c->cc_idx), ptr<int>(c->cc_sidx), nv, 0, 64, st));
+    B2_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, ptr<unsigned int>(c->cc_hkey),
+                                          ptr<unsigned int>(c->cc_hkey_s), ptr<int>(c->cc_idx),
+                                          ptr<int>(c->cc_sidx), nv, 0, cbits, st));
     B2_TRY(ensure(c->cub_tmp, bytes));
-    B2_CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, bytes, ptr<double>(c->cc_lox), ptr<double>(c->cc_lox_s),
-                                          ptr<int>(c->cc_idx), ptr<int>(c->cc_sidx), nv, 0, 64, st));
+    B2_CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, bytes, ptr<unsigned int>(c->cc_hkey),
+                                          ptr<unsigned int>(c->cc_hkey_s), ptr<int>(c->cc_idx),
+                                          ptr<int>(c->cc_sidx), nv, 0, cbits, st));
+    int nlarge = 0;
+    B2_CK(cudaMemcpyAsync(&nlarge, nlarge_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+    c->launches++;
+    k_sph_buckets<<<blocks_for(nv, T), T, 0, st>>>(nv, ptr<unsigned int>(c->cc_hkey_s), ptr<int>(c->cc_bstart),
+                                                   ptr<int>(c->cc_bend));
+    B2_CK(cudaStreamSynchronize(st));
     c->launches += 2;
-    k_cc_pairs<false><<<blocks_for(nv, T), T, 0, st>>>(cvd, ptr<int>(c->obst), ns, ptr<double>(c->cc_lox_s),
-                                                       ptr<int>(c->cc_sidx), ptr<int>(c->cc_cnt), nullptr, nullptr);
+    k_cc_pairs<false><<<blocks_for(nv, 128), 128, 0, st>>>(
+        cvd, ptr<int>(c->obst), ns, ptr<int>(c->cc_sidx), ptr<int4>(c->cc_cell), ptr<int>(c->cc_bstart),
+        ptr<int>(c->cc_bend), Mc - 1, ptr<int>(c->cc_large), nlarge, ptr<int>(c->cc_cnt), nullptr, nullptr);
     unsigned long long total = 0;
     B2_CK(cudaMemsetAsync(c->sph_total.p, 0, sizeof(unsigned long long), st));
     k_count_total<<<std::min(blocks_for(nv, T), 4 * c->sms), T, 0, st>>>(nv, ptr<int>(c->cc_cnt),
@@ -1548,9 +1580,10 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
       B2_TRY(ensure(c->cc_keys, sizeof(long long) * (ncc + 1)));
       B2_TRY(ensure(c->cc_keys_s, sizeof(long long) * (ncc + 1)));
       c->launches++;
-      k_cc_pairs<true><<<blocks_for(nv, T), T, 0, st>>>(cvd, ptr<int>(c->obst), ns, ptr<double>(c->cc_lox_s),
-                                                        ptr<int>(c->cc_sidx), nullptr, ptr<int>(c->cc_off),
-                                                        ptr<long long>(c->cc_keys));
+      k_cc_pairs<true><<<blocks_for(nv, 128), 128, 0, st>>>(
+          cvd, ptr<int>(c->obst), ns, ptr<int>(c->cc_sidx), ptr<int4>(c->cc_cell), ptr<int>(c->cc_bstart),
+          ptr<int>(c->cc_bend), Mc - 1, ptr<int>(c->cc_large), nlarge, nullptr, ptr<int>(c->cc_off),
+          ptr<long long>(c->cc_keys));
       bytes = 0;
       B2_CK(cub::DeviceRadixSort::SortKeys(nullptr, bytes, ptr<unsigned long long>(c->cc_keys),
                                            ptr<unsigned long long>(c->cc_keys_s), ncc, 0, 64, st));

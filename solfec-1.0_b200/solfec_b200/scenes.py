@@ -823,6 +823,126 @@ def convex_pile(seed: int = 1, nx: int = 5, ny: int = 4, nz: int = 3, hulls: int
     return sc, _convex_arrays(convexes, np.arange(nb))
 
 
+def convex_lattice(seed: int = 11, nx: int = 50, ny: int = 50, nz: int = 10, nsurf: int = 4):
+    """Convex bodies for detection timing, as convex_pile without hulls: an
+    nx x ny x nz lattice of unit boxes on a floor obstacle, a third exact
+    (faces, edges and corners of exact neighbours touching), a third with
+    sizes and positions jittered by a few thousandths, a third also turned by
+    up to 3 degrees; every body at the origin with the identity rotation.
+
+    Returns (scene without contacts, set_convexes arguments)."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    I, J_, K = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing='ij')
+    c = np.stack([I.ravel(), J_.ravel(), K.ravel() + 0.5], axis=1).astype(float)
+    kind = rng.integers(3, size=n)
+    h = np.full((n, 3), 0.5)
+    jit = kind > 0
+    h[jit] = 0.5 * (1 + rng.uniform(-3e-3, 3e-3, (int(jit.sum()), 3)))
+    c[jit] += rng.uniform(-2e-3, 2e-3, (int(jit.sum()), 3))
+    corners = np.array([[i, j, k] for k in (0, 1) for j in (0, 1) for i in (0, 1)], float) * 2 - 1
+    v = corners[None] * h[:, None, :]
+    rot = kind == 2
+    if rot.any():
+        m = int(rot.sum())
+        w = rng.normal(size=(m, 3))
+        w *= (rng.uniform(0, np.radians(3), m) / np.linalg.norm(w, axis=1))[:, None]
+        a = np.linalg.norm(w, axis=1)
+        Kx = np.zeros((m, 3, 3))
+        Kx[:, 0, 1], Kx[:, 0, 2], Kx[:, 1, 2] = -w[:, 2], w[:, 1], -w[:, 0]
+        Kx[:, 1, 0], Kx[:, 2, 0], Kx[:, 2, 1] = w[:, 2], -w[:, 1], w[:, 0]
+        R = np.eye(3)[None] + (np.sin(a) / a)[:, None, None] * Kx + ((1 - np.cos(a)) / a ** 2)[:, None, None] * (Kx @ Kx)
+        v[rot] = np.einsum('nij,nkj->nki', R, v[rot])
+    v += c[:, None, :]
+    fh = np.array([nx / 2 + 1, ny / 2 + 1, 0.25])
+    floor = corners * fh + np.array([(nx - 1) / 2, (ny - 1) / 2, -0.25])
+    vert = np.concatenate([v.reshape(-1, 3), floor])
+    nb = n + 1
+    fac1 = np.array(sum(([4] + list(f) for f in HEX_FACES), []), np.int32)
+    cv = dict(body=np.arange(nb, dtype=np.int32), vptr=np.arange(nb + 1, dtype=np.int32) * 8, vert=vert,
+              fptr=np.arange(nb + 1, dtype=np.int32) * fac1.shape[0], fac=np.tile(fac1, nb),
+              sptr=np.arange(nb + 1, dtype=np.int32) * 6, surf=rng.integers(nsurf, size=6 * nb).astype(np.int32))
+    obstacle = np.zeros(nb, np.int32); obstacle[-1] = 1
+    e = np.zeros(0)
+    eye = np.tile(np.eye(3).reshape(9), (nb, 1))
+    sc = Scene(name='convex-lattice-%d' % n, step=1e-3, dynamic=1, rot=eye.copy(), x=np.zeros((nb, 3)),
+               x0=np.zeros((nb, 3)), jinv=np.where(obstacle[:, None] != 0, 0.0, eye), minv=1.0 - obstacle,
+               velo=np.zeros((nb, 6)), velo0=np.zeros((nb, 6)), obstacle=obstacle, master=np.zeros(0, np.int32),
+               slave=np.zeros(0, np.int32), mpnt=np.zeros((0, 3)), spnt=np.zeros((0, 3)), base=np.zeros((0, 9)),
+               gap=e, friction=e, restitution=e, cohesion=e, mass=np.ones(nb))
+    return sc, cv
+
+
+def convex_drop(seed: int = 5, nx: int = 3, ny: int = 2, nz: int = 2, hulls: int = 2, gap: float = 1.5e-3,
+                density: float = 1000.0, nsurf: int = 3, step: float = 1e-3):
+    """Convex bodies dropped onto a floor obstacle: an nx x ny x nz stack of
+    boxes of side about 1, 1 cm apart sideways (sizes and positions jittered
+    by a few thousandths, turned by up to 0.3 degrees), each layer `gap` above
+    the highest vertex of the one below it, and
+    `hulls` random hulls of 7 points above the stack; every body's mass centre
+    at its vertices' mean, inertia that of its bounding box. Surface ids are
+    seeded per face.
+
+    Returns (scene without contacts, set_convexes arguments, J, mass)."""
+    rng = np.random.default_rng(seed)
+    convexes = []
+
+    def turn(angle):
+        w = rng.normal(size=3)
+        w *= angle / np.linalg.norm(w)
+        K = np.array([[0, -w[2], w[1]], [w[2], 0, -w[0]], [-w[1], w[0], 0]])
+        a = np.linalg.norm(w)
+        return np.eye(3) + np.sin(a) / a * K + (1 - np.cos(a)) / a ** 2 * K @ K
+
+    top = 0.0
+    for k in range(nz):
+        layer = []
+        for j in range(ny):
+            for i in range(nx):
+                h = 0.5 * (1 + rng.uniform(-3e-3, 3e-3, 3))
+                v = np.array([[(-h[0], h[0])[a], (-h[1], h[1])[b], (-h[2], h[2])[c]] for c in (0, 1)
+                              for b in (0, 1) for a in (0, 1)]) @ turn(rng.uniform(0, np.radians(0.3))).T
+                v += np.array([i * 1.01, j * 1.01, 0.0]) + rng.uniform(-1e-3, 1e-3, 3)
+                v[:, 2] += top + gap - v[:, 2].min()
+                layer.append(v)
+                convexes.append((v, HEX_FACES, rng.integers(nsurf, size=6)))
+        top = max(v[:, 2].max() for v in layer)
+    for _ in range(hulls):
+        P = rng.normal(size=(7, 3)) * 0.3
+        V, faces = hull_faces(P)
+        V = V + np.array([rng.uniform(0, nx - 1), rng.uniform(0, ny - 1), 0.0])
+        V[:, 2] += top + gap - V[:, 2].min()
+        convexes.append((V, faces, rng.integers(nsurf, size=len(faces))))
+    floor_h = np.array([nx / 2 + 1, ny / 2 + 1, 0.25])
+    floor_c = np.array([(nx - 1) / 2, (ny - 1) / 2, -0.25])
+    floor = np.array([[(-floor_h[0], floor_h[0])[a], (-floor_h[1], floor_h[1])[b], (-floor_h[2], floor_h[2])[c]]
+                      for c in (0, 1) for b in (0, 1) for a in (0, 1)]) + floor_c
+    convexes.append((floor, HEX_FACES, rng.integers(nsurf, size=6)))
+    nb = len(convexes)
+    obstacle = np.zeros(nb, np.int32); obstacle[-1] = 1
+    x = np.array([v.mean(axis=0) for v, _, _ in convexes])
+    ext = np.array([v.max(axis=0) - v.min(axis=0) for v, _, _ in convexes])
+    mass = density * ext.prod(axis=1)
+    J = np.zeros((nb, 9))
+    J[:, 0] = mass * (ext[:, 1] ** 2 + ext[:, 2] ** 2) / 12
+    J[:, 4] = mass * (ext[:, 0] ** 2 + ext[:, 2] ** 2) / 12
+    J[:, 8] = mass * (ext[:, 0] ** 2 + ext[:, 1] ** 2) / 12
+    jinv = np.zeros((nb, 9))
+    jinv[:, 0], jinv[:, 4], jinv[:, 8] = 1 / J[:, 0], 1 / J[:, 4], 1 / J[:, 8]
+    jinv[obstacle != 0] = 0.0
+    minv = np.where(obstacle != 0, 0.0, 1.0 / mass)
+    J[obstacle != 0] = np.eye(3).reshape(9)
+    mass = np.where(obstacle != 0, 1.0, mass)
+    e = np.zeros(0)
+    eye = np.tile(np.eye(3).reshape(9), (nb, 1))
+    sc = Scene(name='convex-drop-%d' % nb, step=step, dynamic=1, rot=eye, x=x.copy(), x0=x.copy(), jinv=jinv,
+               minv=minv, velo=np.zeros((nb, 6)), velo0=np.zeros((nb, 6)), obstacle=obstacle,
+               master=np.zeros(0, np.int32), slave=np.zeros(0, np.int32), mpnt=np.zeros((0, 3)),
+               spnt=np.zeros((0, 3)), base=np.zeros((0, 9)), gap=e, friction=e, restitution=e, cohesion=e,
+               mass=mass)
+    return sc, _convex_arrays(convexes, np.arange(nb)), J, mass
+
+
 def spheres_in_box(seed: int = 9, n_side: int = 5, layers: int = 3, radius: float = 0.05, pitch: float = 0.11,
                    wall: float = 0.05, clearance: float = 0.002, density: float = 2000.0, friction: float = 0.3,
                    step: float = 1e-3):

@@ -15,7 +15,9 @@ import os
 import numpy as np
 import pytest
 
-from solfec_b200 import LOCDYN, scenes
+import oracle
+from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN, scenes
+from solfec_b200._lib import lib
 from solfec_b200.detect import CONVEXES, bodies_only
 from solfec_b200.dynamics import RIGID_DYNAMICS
 
@@ -129,3 +131,111 @@ def test_convex_lattice_contacts_equal_reference():
 def test_convex_pile_contacts_equal_reference(seed):
     sc, cv = scenes.convex_pile(seed=seed, nx=4, ny=3, nz=2, hulls=12)
     check_scene(seed, sc, cv, min_contacts=25)
+
+
+def expected_step(sc, cv, st, prev, mat, threshold=0.01, mindist=1e-6):
+    """The contacts the reference's DOM_Update_Begin makes of the convexes at
+    the device's body state st (rotations, mass centres): gobjcontact of the
+    compiled reference for every pair on the current vertices (cur_point of
+    the oracle), kept contacts carrying their R and U, new ones sparsified."""
+    if not oracle.geo_available():
+        pytest.skip('reference geometry build unavailable')
+    vbody = np.repeat(cv['body'], np.diff(cv['vptr']))
+    cur = oracle.sphere_centres(vbody, cv['vert'], st['rot'], st['x'], sc.x0)
+    conv = [(cur[cv['vptr'][c]:cv['vptr'][c + 1]], f, s_) for c, (_, f, s_) in enumerate(scenes.convex_list(cv))]
+    found = {}
+    for i in range(len(conv)):
+        for j in range(i + 1, len(conv)):
+            if sc.obstacle[cv['body'][i]] and sc.obstacle[cv['body'][j]]:
+                continue
+            r = oracle.ref_gobj_convex_convex(*conv[i], *conv[j])
+            if r[0] > 0:
+                found[(i, j)] = r
+    keys = sorted(found)
+    pkeys = {} if prev is None else {int(k): t for t, k in enumerate(prev['key'])}
+    key64 = [(i << 32) | j for i, j in keys]
+    isnew = [k not in pkeys for k in key64]
+    body = {key: (cv['body'][key[1]], cv['body'][key[0]]) for key in keys}
+    keep = []
+    for t, key in enumerate(keys):
+        ok = True
+        if isnew[t]:
+            m, s_ = body[key]
+            for a, other in enumerate(keys):
+                if a == t or not (set(body[other]) & {m, s_}):
+                    continue
+                if found[key][4] < threshold * found[other][4]:
+                    continue
+                if np.abs(found[key][1] - found[other][1]).max() < 2 * mindist and (t < a or not isnew[a]):
+                    ok = False
+                    break
+        keep.append(ok)
+    out = {n: [] for n in ('key', 'slave_lo', 'master', 'slave', 'point', 'mpnt', 'spnt', 'base', 'gap', 'area',
+                           'friction', 'restitution', 'R', 'U', 'isnew')}
+    for t, key in enumerate(keys):
+        if not keep[t]:
+            continue
+        st_, pt, nrm, gap, area, sp = found[key]
+        m, s_ = body[key]
+        out['key'].append(key64[t]); out['slave_lo'].append(1); out['master'].append(m); out['slave'].append(s_)
+        out['point'].append(pt)
+        out['mpnt'].append(oracle.ref_points([m], [pt], st['rot'], st['x'], sc.x0)[0])
+        out['spnt'].append(oracle.ref_points([s_], [pt], st['rot'], st['x'], sc.x0)[0])
+        out['base'].append(oracle.localbase(nrm)); out['gap'].append(gap); out['area'].append(area)
+        out['friction'].append(mat[sp[0], sp[1], 0]); out['restitution'].append(mat[sp[0], sp[1], 1])
+        hit = pkeys.get(key64[t])
+        out['R'].append(np.zeros(3) if hit is None or 'R' not in prev else prev['R'][hit])
+        out['U'].append(np.zeros(3) if hit is None or 'U' not in prev else prev['U'][hit])
+        out['isnew'].append(int(hit is None))
+    return {k: np.array(v) for k, v in out.items()}
+
+
+def same_contacts(dev, exp):
+    assert dev['key'].shape[0] == exp['key'].shape[0], (dev['key'].shape, exp['key'].shape)
+    if exp['key'].shape[0] == 0:
+        return
+    for k, b in exp.items():
+        a = np.asarray(dev[k])
+        if a.dtype.kind == 'f':
+            assert np.array_equal(a.view(np.uint64), np.ascontiguousarray(b, np.float64).reshape(a.shape)
+                                  .view(np.uint64)), k
+        else:
+            assert np.array_equal(a.astype(np.int64), b.astype(np.int64).reshape(a.shape)), k
+
+
+def test_convex_time_loop_matches_reference_every_step():
+    """Boxes and hulls dropped onto a floor: at every step the device's
+    contact update and detection on its own body state equals the reference's
+    gobjcontact over all pairs, with the R and U of the device solve carried
+    for kept contacts, as the bodies fall, land, settle and rotate."""
+    sc, cv, J, mass = scenes.convex_drop()
+    mat = np.zeros((3, 3, 2))
+    mat[..., 0] = [[0.3, 0.4, 0.5], [0.4, 0.6, 0.7], [0.5, 0.7, 0.2]]
+    ldy = LOCDYN()
+    ldy.update_begin(bodies_only(sc))
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    det = CONVEXES(ldy, cv, mat)
+    gs = GAUSS_SEIDEL_SOLVER(1e-6, 300)
+    prev = None
+    counts = []
+    h = sc.step
+    for k in range(60):
+        dyn.step_begin(h, (0.0, 0.0, -9.81))
+        st = dyn.state()
+        nc, nn = det.detect()
+        dev = det.contacts()
+        same_contacts(dev, expected_step(sc, cv, st, prev, mat))
+        counts.append((nc, nn))
+        if nc > 0:
+            assert lib().b2gs_locdyn_update_begin_resident(ldy.handle, h, 1) == 0
+            det.carry_state()
+            gs.solve(ldy)
+            R, U, _ = ldy.get_state()
+            prev = dict(key=dev['key'], R=R, U=U)
+        else:
+            prev = dict(key=dev['key'])
+        dyn.step_end(h)
+    kept = sum(nc - nn for nc, nn in counts)
+    assert max(nc for nc, _ in counts) >= 8 and kept > 100, counts
+    assert np.all(dyn.state()['x'][sc.obstacle == 0, 2] > 0.3)   # resting on the floor, not through it
+    ldy.close()
