@@ -109,7 +109,7 @@ B2_HD inline int add_det3(double* h, int n, double s, const double* p, const dou
 
 // exact sign of orient3d (a, b, c, d) = det [a - d; b - d; c - d], which is the
 // 4 x 4 determinant with rows (x, 1) expanded along its last column
-B2_HD inline double orient3d_exact_sign(const double* a, const double* b, const double* c, const double* d) {
+B2_HD B2_NOINLINE static double orient3d_exact_sign(const double* a, const double* b, const double* c, const double* d) {
   double h[160];  // a non-overlapping expansion of doubles spans at most ~2100 bits / component
   int n = 0;
   n = add_det3(h, n, -1.0, b, c, d);
@@ -250,7 +250,7 @@ struct Hull {
 
   // mendface, hul.c:150-228: a face whose vertices are colinear is flipped
   // with its neighbour across the edge that contains the middle vertex
-  B2_HD bool mendface(int f) {
+  B2_HD B2_NOINLINE bool mendface(int f) {
     int e, c = -1;
     for (e = face[f].e; e >= 0; e = edge[e].n) {
       const int a = edge[e].v0, b = edge[e].v1;
@@ -294,7 +294,7 @@ struct Hull {
   // glibc's qsort orders equal keys), points inside the 10 eps box of an
   // earlier sorted point dropped, then four well separated points in input
   // order; the rest (input order) pushed onto a list, so it runs backwards
-  B2_HD bool simplex_vertices(int sv[4], int& list) {
+  B2_HD B2_NOINLINE bool simplex_vertices(int sv[4], int& list) {
     short order[kMaxPlanes];
     bool alive[kMaxPlanes];
     for (int i = 0; i < n; i++) { order[i] = (short)i; alive[i] = true; }
@@ -368,7 +368,7 @@ struct Hull {
 
   // simplex, hul.c:346-456: four faces (a b c), (b d c), (d a c), (d b a), each
   // turned over when the remaining vertex is in front of it
-  B2_HD int simplex(int a, int b, int c, int d) {
+  B2_HD B2_NOINLINE int simplex(int a, int b, int c, int d) {
     int e[12], f[4];
     for (int i = 0; i < 12; i++) e[i] = new_edge();
     for (int i = 0; i < 4; i++) f[i] = new_face();
@@ -413,7 +413,7 @@ struct Hull {
   }
 
   // testsimplex, hul.c:527-553
-  B2_HD bool testsimplex(int h) const {
+  B2_HD B2_NOINLINE bool testsimplex(int h) const {
     for (; h >= 0; h = face[h].n)
       for (int e = face[h].e; e >= 0; e = edge[e].n)
         for (int i = 0; i < 2; i++) {
@@ -427,7 +427,7 @@ struct Hull {
 
   // mark, hul.c:460-471: faces visible from point v, depth first through the
   // edges in list order; g = the last face met that v does not see
-  B2_HD void mark(int f0, int v, int& g) {
+  B2_HD B2_NOINLINE void mark(int f0, int v, int& g) {
     short fs[kMaxFaces], es[kMaxFaces];
     int top = 0;
     const double d0 = orient(f0, v);
@@ -471,7 +471,7 @@ struct Hull {
   // the points of the list l above face f go to f's outside set: the last of
   // them becomes f->w and the earlier choices move to f->v (hul.c:580-603 and
   // 683-708, whose running maximum stays 0)
-  B2_HD void take_outside(int f, short& l) {
+  B2_HD B2_NOINLINE void take_outside(int f, short& l) {
     int z = -1, x = l;
     while (x >= 0) {
       const int yv = vert[x].n;
@@ -492,7 +492,7 @@ struct Hull {
 
   // hull, hul.c:560-779: the hull's faces as triangles, counter-clockwise
   // seen from outside, with their adjacency; returns the count or -1
-  B2_HD int build(const double* pts, int npts, OutTri* tri) {
+  B2_HD B2_NOINLINE int build(const double* pts, int npts, OutTri* tri) {
     y = pts; n = npts;
     nfree_face = nfree_edge = used_face = used_edge = used_vert = 0;
     overflow = false;
@@ -633,7 +633,7 @@ struct Polar {
 // order, listing the hull triangles around it (from the first triangle that
 // holds it); the polar vertex of triangle t is out / -d, d the smallest
 // -<out, ver> over its vertices, clamped to -eps
-B2_HD inline bool polarise(const OutTri* tri, int m, const double* y, double* w, Polar& P, int npts) {
+B2_HD B2_NOINLINE static bool polarise(const OutTri* tri, int m, const double* y, double* w, Polar& P, int npts) {
   short first[kMaxPlanes];
   for (int i = 0; i < npts; i++) first[i] = -1;
   int cnt = 0;
@@ -717,7 +717,7 @@ struct Scratch {
 // detect_convex_convex (update = false) and update_convex_convex (update =
 // true, c.spair holds the current pair): 0 no contact; 1, or 2 when an update
 // changed the surface pair; kCviOverflow past the capacities above
-B2_HD inline int convex_convex(const Convex& A, const Convex& B, bool update, Contact& c, Scratch& s) {
+B2_HD B2_NOINLINE static int convex_convex(const Convex& A, const Convex& B, bool update, Contact& c, Scratch& s) {
   double p[3], q[3];
   // cvi, cvi.c:118-230 (NON_REGULARIZED: the closest point p is not refined)
   const double dist = gjk_polytopes(A.v, A.nv, B.v, B.nv, p, q);

@@ -10,8 +10,10 @@
 
 #if defined(__CUDACC__)
 #define B2_HD __host__ __device__
+#define B2_NOINLINE __noinline__
 #else
 #define B2_HD
+#define B2_NOINLINE __attribute__((noinline))
 #endif
 
 namespace b2 {
@@ -23,7 +25,7 @@ constexpr double kGeomEps = 1e-6;  // GEOMETRIC_EPSILON, alg.c:24
 // whose barycentric weights are positive on its members and non-positive off
 // them gives the projection of the origin. w[i] holds a Minkowski point and
 // wa[i] the index of its hull vertex.
-B2_HD inline int johnson_project(double (*w)[3], int* wa, int n, double* l, double* v) {
+B2_HD B2_NOINLINE static int johnson_project(double (*w)[3], int* wa, int n, double* l, double* v) {
   const int sub_mask[15] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 11, 13, 14, 15};
   const int sub_count[5] = {0, 0, 3, 7, 15};
   double dot[4][4], delta[16][4];
@@ -89,7 +91,7 @@ B2_HD inline int johnson_project(double (*w)[3], int* wa, int n, double* l, doub
 // gjk_convex_point, gjk.c:510-556: distance from p to the hull of the na
 // vertices a[3 na] and the nearest hull point q (an upper bound of the exact
 // distance within GEOMETRIC_EPSILON)
-B2_HD inline double gjk_convex_point(const double* a, int na, const double* p, double* q) {
+B2_HD B2_NOINLINE static double gjk_convex_point(const double* a, int na, const double* p, double* q) {
   double w[4][3], v[3], l[4], mi = 0.0;
   int wa[4];
   int n = 0, j = 0;
@@ -128,7 +130,7 @@ B2_HD inline double gjk_convex_point(const double* a, int na, const double* p, d
 // nb vertices b[3 nb] and their nearest points p (in a) and q (in b). The
 // support points are the first vertex of a with the smallest, and of b with
 // the largest, projection on the search direction.
-B2_HD inline double gjk_polytopes(const double* a, int na, const double* b, int nb, double* p, double* q) {
+B2_HD B2_NOINLINE static double gjk_polytopes(const double* a, int na, const double* b, int nb, double* p, double* q) {
   double w[4][3], v[3], l[4], mi = 0.0;
   int wa[4], wb[4];
   int n = 0, j = 0;
