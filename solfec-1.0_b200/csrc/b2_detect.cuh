@@ -511,9 +511,9 @@ __global__ void k_sph_contacts(int npair, SphereDev s, ConvexDev cv, const int* 
 // mean (floors, walls) are listed apart and tested against every convex.
 // Two convexes within GEOMETRIC_EPSILON of each other have overlapping
 // eps-inflated boxes (CONVEX_Extents, cvx.c:1236-1260), so their centres lie
-// in neighbouring cells; a candidate pair then passes the box test and the
-// GJK distance test of cvi (cvi.c:128-129, gjk of the lower convex first),
-// which leaves the narrow phase only pairs that touch. Pairs of one body and
+// in neighbouring cells; a candidate pair then passes the box test and, in
+// k_cc_gjk, the GJK distance test of cvi (cvi.c:128-129, gjk of the lower
+// convex first), which leaves the narrow phase only pairs that touch. Pairs of one body and
 // pairs of two obstacles are left out (box.c:104-108). A pair is keyed by its
 // convexes c1 < c2 as (nsph + c1) << 32 | (nsph + c2); the first object of the
 // reference's gobjcontact is c1 (the slave, holding the outward normal), the
@@ -580,10 +580,19 @@ __device__ __forceinline__ bool cc_candidate(const ConvexDev& cv, const int* obs
   const double* b = cv.box + 6 * j;
   for (int k = 0; k < 3; k++)
     if (!(b[k] - kGeomEps <= a[3 + k] + kGeomEps && a[k] - kGeomEps <= b[3 + k] + kGeomEps)) return false;
-  const int lo = i < j ? i : j, hi = i < j ? j : i;
+  return true;
+}
+
+// keep[t] = 1 when the convexes of candidate key t are within GEOMETRIC_EPSILON
+// (gjk with the lower convex first, as cvi calls it)
+__global__ void k_cc_gjk(int n, int nsph, ConvexDev cv, const long long* keys, unsigned char* keep) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const long long key = keys[t];
+  const int lo = (int)(key >> 32) - nsph, hi = (int)(key & 0xFFFFFFFFLL) - nsph;
   double p[3], q[3];
-  return gjk_polytopes(cv.cur + 3 * (size_t)cv.vptr[lo], cv.vptr[lo + 1] - cv.vptr[lo],
-                       cv.cur + 3 * (size_t)cv.vptr[hi], cv.vptr[hi + 1] - cv.vptr[hi], p, q) <= kGeomEps;
+  keep[t] = gjk_polytopes(cv.cur + 3 * (size_t)cv.vptr[lo], cv.vptr[lo + 1] - cv.vptr[lo],
+                          cv.cur + 3 * (size_t)cv.vptr[hi], cv.vptr[hi + 1] - cv.vptr[hi], p, q) <= kGeomEps;
 }
 
 // per sorted position t (convex i = sorted[t]): its partners j > i of the 27

@@ -216,7 +216,7 @@ struct b2dev_ctx {
       cvx_aptr, cvx_adj;
   bool cvx_have_adj = false;
   Buf cc_lox, cc_idx, cc_sidx, cc_cnt, cc_off, cc_keys, cc_keys_s, cc_cell, cc_hkey, cc_hkey_s, cc_large,
-      cc_bstart, cc_bend, cc_misc;
+      cc_bstart, cc_bend, cc_misc, cc_keep;
   // CONTACT_SPARSIFY (dom.c:3107-3109 defaults)
   double sp_threshold = 0.01, sp_minarea = 0.0, sp_mindist = kGeomEps;
   bool det_valid = false;       // the scene's contacts are those of the last detection
@@ -872,7 +872,7 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->det_new, &c->cvx_body, &c->cvx_vptr, &c->cvx_vert, &c->cvx_fptr, &c->cvx_fac, &c->cvx_sptr,
                 &c->cvx_surf, &c->cvx_ns, &c->cvx_cur, &c->cvx_pla, &c->cvx_box, &c->cvx_aptr, &c->cvx_adj,
                 &c->cc_lox, &c->cc_idx, &c->cc_sidx, &c->cc_cnt, &c->cc_off, &c->cc_keys, &c->cc_keys_s,
-                &c->cc_cell, &c->cc_hkey, &c->cc_hkey_s, &c->cc_large, &c->cc_bstart, &c->cc_bend, &c->cc_misc,
+                &c->cc_cell, &c->cc_hkey, &c->cc_hkey_s, &c->cc_large, &c->cc_bstart, &c->cc_bend, &c->cc_misc, &c->cc_keep,
                 &c->st_area, &c->det_area,
                 &c->topo_m, &c->topo_s, &c->topo_o, &c->topo_flag, &c->blkrow};
   for (Buf* b : all)
@@ -1529,7 +1529,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     B2_TRY(ensure(c->cc_large, sizeof(int) * (nv + 1)));
     B2_TRY(ensure(c->cc_bstart, sizeof(int) * (Mc + 1)));
     B2_TRY(ensure(c->cc_bend, sizeof(int) * (Mc + 1)));
-    B2_TRY(ensure(c->cc_misc, 32));  // extent sum (double), largest ordinary side (bits), large count (int)
+    B2_TRY(ensure(c->cc_misc, 32));  // extent sum, largest ordinary side (bits), large count, selected count
     B2_TRY(ensure(c->sph_total, sizeof(unsigned long long)));
     double* esum = ptr<double>(c->cc_misc);
     unsigned long long* emax = ptr<unsigned long long>(c->cc_misc) + 1;
@@ -1574,22 +1574,38 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
       set_err("detect: %llu candidate pairs exceed the supported %d", total + nps, INT_MAX / 2 - 1);
       return B2DEV_EINVAL;
     }
-    ncc = (int)total;
-    if (ncc > 0) {
+    const int nbox = (int)total;  // pairs whose inflated boxes overlap
+    if (nbox > 0) {
       B2_TRY(scan_exclusive(c, ptr<int>(c->cc_cnt), ptr<int>(c->cc_off), nv));
-      B2_TRY(ensure(c->cc_keys, sizeof(long long) * (ncc + 1)));
-      B2_TRY(ensure(c->cc_keys_s, sizeof(long long) * (ncc + 1)));
-      c->launches++;
+      B2_TRY(ensure(c->cc_keys, sizeof(long long) * (nbox + 1)));
+      B2_TRY(ensure(c->cc_keys_s, sizeof(long long) * (nbox + 1)));
+      B2_TRY(ensure(c->cc_keep, nbox + 1));
+      c->launches += 2;
       k_cc_pairs<true><<<blocks_for(nv, 128), 128, 0, st>>>(
           cvd, ptr<int>(c->obst), ns, ptr<int>(c->cc_sidx), ptr<int4>(c->cc_cell), ptr<int>(c->cc_bstart),
           ptr<int>(c->cc_bend), Mc - 1, ptr<int>(c->cc_large), nlarge, nullptr, ptr<int>(c->cc_off),
           ptr<long long>(c->cc_keys));
+      k_cc_gjk<<<blocks_for(nbox, 128), 128, 0, st>>>(nbox, ns, cvd, ptr<long long>(c->cc_keys),
+                                                      ptr<unsigned char>(c->cc_keep));
+      // the touching pairs, then sorted by key
+      int* nsel = reinterpret_cast<int*>(ptr<unsigned long long>(c->cc_misc) + 3);
       bytes = 0;
-      B2_CK(cub::DeviceRadixSort::SortKeys(nullptr, bytes, ptr<unsigned long long>(c->cc_keys),
-                                           ptr<unsigned long long>(c->cc_keys_s), ncc, 0, 64, st));
+      B2_CK(cub::DeviceSelect::Flagged(nullptr, bytes, ptr<long long>(c->cc_keys), ptr<unsigned char>(c->cc_keep),
+                                       ptr<long long>(c->cc_keys_s), nsel, nbox, st));
       B2_TRY(ensure(c->cub_tmp, bytes));
-      B2_CK(cub::DeviceRadixSort::SortKeys(c->cub_tmp.p, bytes, ptr<unsigned long long>(c->cc_keys),
-                                           ptr<unsigned long long>(c->cc_keys_s), ncc, 0, 64, st));
+      B2_CK(cub::DeviceSelect::Flagged(c->cub_tmp.p, bytes, ptr<long long>(c->cc_keys),
+                                       ptr<unsigned char>(c->cc_keep), ptr<long long>(c->cc_keys_s), nsel, nbox,
+                                       st));
+      B2_CK(cudaMemcpyAsync(&ncc, nsel, sizeof(int), cudaMemcpyDeviceToHost, st));
+      B2_CK(cudaStreamSynchronize(st));
+      if (ncc > 0) {
+        bytes = 0;
+        B2_CK(cub::DeviceRadixSort::SortKeys(nullptr, bytes, ptr<unsigned long long>(c->cc_keys_s),
+                                             ptr<unsigned long long>(c->cc_keys), ncc, 0, 64, st));
+        B2_TRY(ensure(c->cub_tmp, bytes));
+        B2_CK(cub::DeviceRadixSort::SortKeys(c->cub_tmp.p, bytes, ptr<unsigned long long>(c->cc_keys_s),
+                                             ptr<unsigned long long>(c->cc_keys), ncc, 0, 64, st));
+      }
     }
   }
   npair = nps + ncc;
@@ -1643,7 +1659,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     if (ncc > 0) {
       c->launches++;
       k_cc_contacts<<<blocks_for(ncc, 64), 64, 0, st>>>(
-          ncc, nps, ns, cvd, ptr<long long>(c->cc_keys_s), ptr<double>(c->rot), ptr<double>(c->rb_x),
+          ncc, nps, ns, cvd, ptr<long long>(c->cc_keys), ptr<double>(c->rot), ptr<double>(c->rb_x),
           ptr<double>(c->x0), c->nsurf, ptr<double>(c->sph_mat), nprev, ptr<long long>(c->sph_pkey),
           ptr<double>(c->sph_pR), ptr<double>(c->sph_pU), so, ptr<int>(c->bad));
     }
