@@ -473,3 +473,135 @@ def test_convex_convex_golden_pinned_to_reference():
         for name, v in now.items():
             stored = g['s%d_%s' % (seed, name)]
             assert stored.shape == v.shape and np.array_equal(stored.view(np.uint8), v.view(np.uint8)), (seed, name)
+
+
+def _cvi_host_lib(tmp_path_factory):
+    """tests/cvi_host_harness.cpp: csrc/b2_cvi.cuh built for the host with
+    g++ (no fused multiply-adds, as the device build)."""
+    import ctypes as C
+    import subprocess
+    here = os.path.dirname(os.path.abspath(__file__))
+    csrc = os.path.join(os.path.dirname(here), 'solfec-1.0_b200', 'csrc')
+    out = str(tmp_path_factory.mktemp('cvi') / 'libcvi_host.so')
+    subprocess.check_call(['g++', '-O2', '-ffp-contract=off', '-fPIC', '-shared', '-I', csrc, '-o', out,
+                           os.path.join(here, 'cvi_host_harness.cpp')])
+    lib = C.CDLL(out)
+    dp = np.ctypeslib.ndpointer(np.float64, flags='C')
+    ip = np.ctypeslib.ndpointer(np.int32, flags='C')
+    lib.cvi_host_pair.restype = C.c_int
+    lib.cvi_host_pair.argtypes = [C.c_int, C.c_int, dp, C.c_int, ip, ip, C.c_int, dp, C.c_int, ip, ip, dp, dp, dp,
+                                  dp, ip]
+    lib.cvi_host_orient3d.restype = C.c_double
+    lib.cvi_host_orient3d.argtypes = [dp, dp, dp, dp]
+    return lib
+
+
+@pytest.fixture(scope='module')
+def cvi_host(tmp_path_factory):
+    return _cvi_host_lib(tmp_path_factory)
+
+
+def test_cvi_orientation_sign_exact(cvi_host):
+    """The hull's orientation test (csrc/b2_cvi.cuh orient3d) has the exact
+    sign of the determinant on near-degenerate inputs, against rational
+    arithmetic: coplanar points, points a rounding away from a plane,
+    collinear points, widely scaled points."""
+    from fractions import Fraction as F
+    rng = np.random.default_rng(3)
+    zeros = 0
+    for t in range(4000):
+        k = t % 4
+        if k == 0:
+            pts = [np.array([rng.uniform(-1, 1) * 10.0 ** rng.integers(-3, 6), rng.uniform(-1, 1), 0.3])
+                   for _ in range(4)]
+        elif k == 1:
+            a, b, c = (rng.normal(size=3) * 1e4 for _ in range(3))
+            u, v = rng.uniform(size=2)
+            d = a + u * (b - a) + v * (c - a)
+            pts = [a, b, c, d + rng.choice([0.0, 1e-12, -1e-12]) * rng.normal(size=3)]
+        elif k == 2:
+            a, dv = rng.normal(size=3), rng.normal(size=3)
+            pts = [a + s * dv for s in rng.uniform(-1, 1, 4)]
+        else:
+            pts = [rng.normal(size=3) * 10.0 ** rng.integers(-6, 6) for _ in range(4)]
+        pts = [np.ascontiguousarray(p, float) for p in pts]
+        M = [[F(x) - F(y) for x, y in zip(p, pts[3])] for p in pts[:3]]
+        e = (M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0])
+             + M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]))
+        s = cvi_host.cvi_host_orient3d(*pts)
+        zeros += e == 0
+        assert ((e > 0) - (e < 0)) == ((s > 0) - (s < 0)), t
+    assert zeros > 500
+
+
+def _random_hull(rng, centre, npts):
+    V, faces = scenes.hull_faces(centre + rng.normal(size=(npts, 3)) * 0.5)
+    fac = np.array(sum(([3] + list(f) for f in faces), []), np.int32)
+    return V, fac, len(faces)
+
+
+@pytest.mark.skipif(not oracle.geo_available(), reason='reference build unavailable')
+def test_cvi_restatement_equals_reference_on_random_pairs(cvi_host):
+    """csrc/b2_cvi.cuh, built for the host, against the reference's own
+    gobjcontact (detect_convex_convex and update_convex_convex) on random
+    pairs: stacked and offset boxes (touching exactly, within and past eps,
+    overlapping), perturbed hexahedra side by side, turned boxes, coincident
+    side planes, and random hulls of 5 to 8 points. State, point, normal, gap,
+    area and surface pair equal bit for bit."""
+    rng = np.random.default_rng(7)
+    fac_box = np.array(sum(([4] + list(f) for f in scenes.HEX_FACES), []), np.int32)
+
+    def box(c, h, pert=0.0, R=None):
+        v = np.array([[(-h[0], h[0])[i], (-h[1], h[1])[j], (-h[2], h[2])[k]] for k in (0, 1) for j in (0, 1)
+                      for i in (0, 1)])
+        v = v + rng.uniform(-pert, pert, v.shape) * h
+        return (v @ R.T if R is not None else v) + c
+
+    def turn():
+        w = rng.normal(size=3)
+        a = np.linalg.norm(w)
+        K = np.array([[0, -w[2], w[1]], [w[2], 0, -w[0]], [-w[1], w[0], 0]])
+        return np.eye(3) + np.sin(a) / a * K + (1 - np.cos(a)) / a ** 2 * K @ K
+
+    contacts = 0
+    for t in range(1200):
+        kind = t % 5
+        h = 0.5 * rng.uniform(0.5, 1.5, 3)
+        if kind == 0:
+            a = box(np.zeros(3), h)
+            b = box(np.array([rng.uniform(-.5, .5), rng.uniform(-.5, .5),
+                              2 * h[2] + rng.choice([0.0, -1e-3, -1e-2, 1e-7, -1e-7])]), h)
+            fa = fb = fac_box
+        elif kind == 1:
+            a = box(np.zeros(3), h, 0.1)
+            b = box(np.array([2 * h[0] + rng.uniform(-0.05, 0.02), rng.uniform(-0.1, 0.1), 0.0]), h, 0.1)
+            fa = fb = fac_box
+        elif kind == 2:
+            a = box(np.zeros(3), h, R=turn())
+            b = box(rng.uniform(-1.2, 1.2, 3), h, R=turn())
+            fa = fb = fac_box
+        elif kind == 3:
+            a = box(np.zeros(3), h)
+            b = box(np.array([0.0, 0.0, 2 * h[2] - rng.choice([0.0, 1e-3, 0.25])]), h)
+            fa = fb = fac_box
+        else:
+            a, fa, _ = _random_hull(rng, np.zeros(3), int(rng.integers(5, 9)))
+            b, fb, _ = _random_hull(rng, rng.uniform(-0.8, 0.8, 3), int(rng.integers(5, 9)))
+        sa = np.arange(1, 1 + (6 if fa is fac_box else fa.shape[0] // 4), dtype=np.int32)
+        sb = np.arange(11, 11 + (6 if fb is fac_box else fb.shape[0] // 4), dtype=np.int32)
+        for update in (False, True):
+            r = oracle.ref_gobj_convex_convex(a, fa, sa, b, fb, sb, update=update, spair=(sa[0], sb[0]))
+            va = np.ascontiguousarray(a, float).ravel()
+            vb = np.ascontiguousarray(b, float).ravel()
+            pt, nr, g, ar = np.zeros(3), np.zeros(3), np.zeros(1), np.zeros(1)
+            sp = np.array([sa[0], sb[0]], np.int32)
+            st = cvi_host.cvi_host_pair(int(update), va.size // 3, va, sa.size, fa, sa, vb.size // 3, vb, sb.size,
+                                        fb, sb, pt, nr, g, ar, sp)
+            assert st == r[0], (t, update)
+            if st > 0:
+                contacts += 1
+                for mine, ref in ((pt, r[1]), (nr, r[2]), (g[0], r[3]), (ar[0], r[4])):
+                    assert np.array_equal(np.asarray(mine, float).view(np.uint64),
+                                          np.asarray(ref, float).view(np.uint64)), (t, update)
+                assert np.array_equal(sp, r[5]), (t, update)
+    assert contacts > 1500
