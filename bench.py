@@ -198,14 +198,19 @@ def _rel2(a, b):
     return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
 
 
-def bench_product(args, ws, rank, local):
+ALL_MODES = ('fp64', 'mixed', 'mixed_nn', 'fp64_ref_rule', 'mixed_nn_ref_rule')
+
+
+def bench_product(args, ws, rank, local, scene=None, modes=ALL_MODES, full=True):
     """Time loop of the hexahedra scene on the device, one run per mode from
     the same initial state (bodies at rest, zero reactions). Every step is
     BODY_Dynamic_Step_Begin (device) -> LOCDYN_Update_Begin on the device
     bodies -> warm start from the previous step's R, U (device) [-> learned
     warm start] -> GAUSS_SEIDEL_Solve -> R, U kept on the device ->
     BODY_Dynamic_Step_End (device): no host round trip of bodies or state.
-    W untimed steps, then K timed steps, each a different step of the run."""
+    W untimed steps, then K timed steps, each a different step of the run.
+    scene replaces the hexahedra scene; modes picks the runs; full = False
+    leaves out the end-to-end replay and the rigid-step timing."""
     import torch
     import ctypes as C
     from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN, learn, scenes
@@ -214,7 +219,7 @@ def bench_product(args, ws, rank, local):
 
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
-    sc = scenes.hexahedra_lattice(seed=replica_seed(rank), **SCENE)
+    sc = scene if scene is not None else scenes.hexahedra_lattice(seed=replica_seed(rank), **SCENE)
     J, mass = _rigid_inertia(sc)
     h, dflag = float(sc.step), int(sc.dynamic)
     stream = torch.cuda.current_stream()
@@ -307,12 +312,18 @@ def bench_product(args, ws, rank, local):
                     rot=rot_d.cpu().numpy().reshape(-1, 9).copy(), x=x_d.cpu().numpy().reshape(-1, 3).copy())
 
     results = {}
+    mode_args = dict(fp64=(SOLVE, 'FP64', False), mixed=(SOLVE, 'MIXED', False), mixed_nn=(SOLVE, 'MIXED', True),
+                     fp64_ref_rule=(SOLVE_REF_RULE, 'FP64', False), mixed_nn_ref_rule=(SOLVE_REF_RULE, 'MIXED', True))
     with ClockSampler(local) as clk:
-        results['fp64'] = run(SOLVE, 'FP64', False)
-        results['mixed'] = run(SOLVE, 'MIXED', False)
-        results['mixed_nn'] = run(SOLVE, 'MIXED', True)
-        results['fp64_ref_rule'] = run(SOLVE_REF_RULE, 'FP64', False)
-        results['mixed_nn_ref_rule'] = run(SOLVE_REF_RULE, 'MIXED', True)
+        for m in modes:
+            results[m] = run(*mode_args[m])
+        if not full:
+            nrows, K, ncol, fe = ldy.sizes()
+            conv = converged_comparison(ldy, results[HEADLINE], sc, dev)
+            net.close()
+            ldy.close()
+            return dict(results=results, n=nrows, K=K, ncolours=ncol, clocks=clk.summary(), nbod=sc.nbod,
+                        scene=sc, converged=conv)
         head_nn = HEADLINE == 'mixed_nn'
         run(SOLVE, 'MIXED', head_nn, record=True)   # untimed: the headline steps' inputs for the end-to-end leg
         # end to end through the C ABI from pinned host buffers: the headline
@@ -358,6 +369,39 @@ def bench_product(args, ws, rank, local):
     ldy.close()
     return dict(results=results, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h, n=nrows, K=K, ncolours=ncol,
                 clocks=clk.summary(), nbod=sc.nbod, scene=sc, rigid=rigid, converged=conv)
+
+
+def bench_detected_hexahedra(args, ws, rank, local):
+    """Config 3 with the contacts the reference's own contact model makes: the
+    bodies of the bench scene (the same seeded perturbed cubes and walls), their
+    contacts detected once on the device as detect_convex_convex makes them
+    (the k_cc_* kernels, bitwise with the reference's gobjcontact), then the
+    bench's time loop in FP64 and mixed precision. The headline keeps the
+    scene generator's face-pair contacts, whose iteration counts the reference
+    arm scales to."""
+    import torch
+    from solfec_b200 import scenes
+    from solfec_b200.detect import detected_scene
+    sc = scenes.hexahedra_lattice(seed=replica_seed(rank), **SCENE)
+    cv = scenes.hexahedra_geometry(seed=replica_seed(rank), nx=SCENE['nx'], ny=SCENE['ny'], nz=SCENE['nz'])
+    J, mass = _rigid_inertia(sc)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    det, con = detected_scene(sc, cv, J, mass, material=(0.4, 0.0))
+    detect_s = time.perf_counter() - t0
+    out = bench_product(args, ws, rank, local, scene=det, modes=('fp64', 'mixed'), full=False)
+    res = out['results']
+    face = np.abs(np.asarray(con['base'])[:, 6:9]).max(axis=1) > 0.999   # normal along a lattice axis
+    return {'workload': 'the bench scene\'s %d bodies with the contacts of the convex detection (goc.c '
+                        'detect_convex_convex restated on the device)' % sc.nbod,
+            'contacts': int(det.ncon), 'contacts_generator': int(sc.ncon), 'blocks': int(out['K']),
+            'colours': int(out['ncolours']), 'axis_normals': int(face.sum()),
+            'gap_median': float(np.median(det.gap)), 'gap_min': float(det.gap.min()),
+            'detect_call_s': round(detect_s, 3),
+            'modes': {m: {'ms_per_step': round(r['ms'], 4), 'iters_per_step': r['iters'],
+                          'iters_mean': round(float(np.mean(r['iters'])), 2)} for m, r in res.items()},
+            'speedup_mixed_vs_fp64': round(res['fp64']['ms'] / res['mixed']['ms'], 3),
+            'mixed_vs_fp64_converged': out['converged'], 'clocks': out['clocks']}
 
 
 def converged_comparison(ldy, last, sc, dev):
@@ -1057,6 +1101,7 @@ def main():
     try:
         out = bench_product(args, ws, rank, local)
         configs = run_config_legs(args, ws, rank, local, extra)
+        detected = None if args.no_configs else bench_detected_hexahedra(args, ws, rank, local)
     finally:
         if extra is not None:
             extra.close()
@@ -1149,6 +1194,7 @@ def main():
             'clocks': out['clocks'],
             'rigid_step': rigid,
             'configs': configs,
+            'config3_detected': detected,
         }
         try:
             line['detect'] = detect_timing()

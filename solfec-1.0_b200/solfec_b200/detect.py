@@ -162,6 +162,29 @@ def CONVEXES(ldy: LOCDYN, convex: dict, material=(0.0, 0.0)) -> SPHERES:
     return SPHERES(ldy, np.zeros(0, np.int32), np.zeros((0, 3)), e, material=material, convex=convex)
 
 
+def detected_scene(scene, convex: dict, J, mass, material=(0.0, 0.0), sparsify=None):
+    """The scene's bodies with the contacts of one device detection of their
+    convexes (the contact part of DOM_Update_Begin at the scene's state):
+    master, slave, referential points, local bases, gaps and materials of the
+    detected contacts, cohesion 0. Returns (scene, contacts dict with areas)."""
+    ldy = LOCDYN()
+    try:
+        ldy.update_begin(bodies_only(scene))
+        RIGID_DYNAMICS(ldy, J, mass, scene.x)
+        det = CONVEXES(ldy, convex, material)
+        if sparsify:
+            det.sparsify(**sparsify)
+        det.detect()
+        con = det.contacts()
+    finally:
+        ldy.close()
+    n = con['key'].shape[0]
+    out = dataclasses.replace(scene, master=con['master'].astype(np.int32), slave=con['slave'].astype(np.int32),
+                              mpnt=con['mpnt'], spnt=con['spnt'], base=con['base'], gap=con['gap'],
+                              friction=con['friction'], restitution=con['restitution'], cohesion=np.zeros(n))
+    return out, con
+
+
 def bodies_only(scene):
     """The scene's bodies with no contacts (what detection starts from)."""
     e = np.zeros(0)

@@ -340,6 +340,44 @@ def _hexahedron_mass(verts: np.ndarray, density: float):
     return vol, o + c_rel, J, density * vol
 
 
+def _hexahedra_vertices(rng, nx, ny, nz, side, perturb):
+    """Lattice indices (n, 3) and vertices (n, 8, 3) of the perturbed cubes of
+    hexahedra_lattice (vertex v = i + 2 j + 4 k at corner (x_i, y_j, z_k))."""
+    n = nx * ny * nz
+    corners = np.array([[i, j, k] for k in (0, 1) for j in (0, 1) for i in (0, 1)], float) - 0.5
+    I, J_, K = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing='ij')
+    idx = np.stack([I.ravel(), J_.ravel(), K.ravel()], axis=1)
+    lat = np.stack([(idx[:, 0] - (nx - 1) / 2.0) * side, (idx[:, 1] - (ny - 1) / 2.0) * side,
+                    (idx[:, 2] + 0.5) * side], axis=1)
+    return idx, lat[:, None, :] + side * (corners[None] + rng.uniform(-perturb, perturb, (n, 8, 3)))
+
+
+def hexahedra_geometry(seed: int = 3, nx: int = 100, ny: int = 100, nz: int = 10, side: float = 0.04,
+                       perturb: float = 0.1, nsurf: int = 1):
+    """The bodies of hexahedra_lattice as convexes for contact detection: per
+    hexahedron its 8 perturbed vertices (the same seeded values) with the
+    faces of HEX_FACES, and the floor and four side walls as obstacle boxes
+    0.1 m thick whose inner faces are the walls' planes. Referential vertices
+    are spatial ones (rotations identity, mass centres as in the scene).
+
+    Returns set_convexes arguments."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    _, verts = _hexahedra_vertices(rng, nx, ny, nz, side, perturb)
+    halfx, halfy = nx * side / 2.0 + 0.5 * side * perturb, ny * side / 2.0 + 0.5 * side * perturb
+    t, top = 0.1, (nz + 2) * side
+    walls = [([-halfx - t, -halfy - t, -t], [halfx + t, halfy + t, 0.0]),     # floor
+             ([-halfx - t, -halfy - t, 0.0], [-halfx, halfy + t, top]),      # -x
+             ([halfx, -halfy - t, 0.0], [halfx + t, halfy + t, top]),        # +x
+             ([-halfx, -halfy - t, 0.0], [halfx, -halfy, top]),              # -y
+             ([-halfx, halfy, 0.0], [halfx, halfy + t, top])]                # +y
+    convexes = [(v, HEX_FACES, np.zeros(6, np.int32)) for v in verts]
+    for lo, hi in walls:
+        v, _ = box_convex(lo, hi)
+        convexes.append((v, HEX_FACES, np.zeros(6, np.int32)))
+    return _convex_arrays(convexes, np.arange(n + len(walls)))
+
+
 def hexahedra_lattice(seed: int = 3, nx: int = 100, ny: int = 100, nz: int = 10, side: float = 0.04,
                       perturb: float = 0.1, density: float = 2000.0, friction: float = 0.4, step: float = 5e-4,
                       vel_sigma: float = 0.02) -> Scene:
@@ -355,12 +393,7 @@ def hexahedra_lattice(seed: int = 3, nx: int = 100, ny: int = 100, nz: int = 10,
     normals and a settled interpenetration gap drawn from -|N(0, 2e-5)| m."""
     rng = np.random.default_rng(seed)
     n = nx * ny * nz
-    corners = np.array([[i, j, k] for k in (0, 1) for j in (0, 1) for i in (0, 1)], float) - 0.5
-    I, J_, K = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing='ij')
-    idx = np.stack([I.ravel(), J_.ravel(), K.ravel()], axis=1)
-    lat = np.stack([(idx[:, 0] - (nx - 1) / 2.0) * side, (idx[:, 1] - (ny - 1) / 2.0) * side,
-                    (idx[:, 2] + 0.5) * side], axis=1)
-    verts = lat[:, None, :] + side * (corners[None] + rng.uniform(-perturb, perturb, (n, 8, 3)))
+    idx, verts = _hexahedra_vertices(rng, nx, ny, nz, side, perturb)
     vol, xc, Jt, mass_b = _hexahedron_mass(verts, density)
     # face vertex sets (outward): -x, +x, -y, +y, -z, +z
     fv = {0: [0, 2, 6, 4], 1: [1, 5, 7, 3], 2: [0, 4, 5, 1], 3: [2, 3, 7, 6], 4: [0, 1, 3, 2], 5: [4, 6, 7, 5]}

@@ -239,3 +239,23 @@ def test_convex_time_loop_matches_reference_every_step():
     assert max(nc for nc, _ in counts) >= 8 and kept > 100, counts
     assert np.all(dyn.state()['x'][sc.obstacle == 0, 2] > 0.3)   # resting on the floor, not through it
     ldy.close()
+
+
+def test_hexahedra_geometry_contacts_equal_reference():
+    """The perturbed cubes and walls of the config-3 scene (8 x 8 x 3 of them):
+    the device detection at the scene's state equals the reference's
+    gobjcontact over all pairs, face, edge and corner contacts alike."""
+    sc = scenes.hexahedra_lattice(nx=8, ny=8, nz=3)
+    cv = scenes.hexahedra_geometry(nx=8, ny=8, nz=3)
+    J = np.tile(np.eye(3).reshape(9), (sc.nbod, 1))
+    mat = np.zeros((1, 1, 2)); mat[0, 0, 0] = 0.4
+    ldy = LOCDYN()
+    ldy.update_begin(bodies_only(sc))
+    dyn = RIGID_DYNAMICS(ldy, J, np.ones(sc.nbod), sc.x)
+    det = CONVEXES(ldy, cv, mat)
+    det.detect()
+    dev = det.contacts()
+    exp = expected_step(sc, cv, dyn.state(), None, mat)
+    same_contacts(dev, exp)
+    assert dev['key'].shape[0] > 400
+    ldy.close()

@@ -104,3 +104,17 @@ def test_masonry_arch_threshold():
         assert max(iters) > 1000  # the first steps of an arch at rest need thousands of sweeps
         energy[ratio] = sum(ro.kinetic_energy(bd, b) for b in range(bd.nbod) if not bd.obstacle[b])
     assert energy[0.1095] < 1e-4 and energy[0.1094] > 1e-3, energy
+
+
+def test_detected_hexahedra_time_loop():
+    """The config-3 bodies (8 x 8 x 3 perturbed cubes and their walls) with
+    the contacts of the device's convex detection: 8 steps from rest, the
+    assembly and solve bitwise with the CPU restatements at every step."""
+    from solfec_b200.detect import detected_scene
+    sc = scenes.hexahedra_lattice(nx=8, ny=8, nz=3)
+    cv = scenes.hexahedra_geometry(nx=8, ny=8, nz=3)
+    J, mass = inertia(sc)
+    det, con = detected_scene(sc, cv, J, mass, material=(0.4, 0.0))
+    assert det.ncon > 400 and np.median(det.gap) < 0.0
+    iters, _ = time_loop_parity(det, 8, epsilon=1.0, maxiter=1000, meritval=1e-4)
+    assert min(iters) >= 1
