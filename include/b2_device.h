@@ -92,7 +92,13 @@ int b2dev_assemble(b2dev_ctx* ctx, double step, int dynamic, uint64_t colour_see
  * next b2dev_assemble reads them without a host round trip.
  *   b2dev_rigid_setup: referential inertia J[9] (column-major), mass, current
  *     mass centre x[3] and scheme per body (0 = RIG_POS, 1 = RIG_NEG, the
- *     reference's default; NULL = all RIG_NEG; RIG_IMP is not supported).
+ *     reference's default, 2 = RIG_IMP, NEW3's Newton solve of bod.c:163-209;
+ *     NULL = all RIG_NEG). A failed NEW3 solve (singular Jacobian, or 50
+ *     Newton steps, where the reference stops the program) is reported by
+ *     the next b2dev_rigid_step_begin or b2dev_rigid_get.
+ *   b2dev_rigid_flags: BODY_* flags per body (bod.h:140-152); BODY_DISABLE_ROTATION
+ *     (4) zeroes the angular velocity at both ends of the step (bod.c:1337-1340,
+ *     1450-1453); NULL clears them.
  *   b2dev_rigid_step_begin: velo0 <- velo, half step of position and rotation,
  *     free velocity with gravity (m g) and the bodies' point loads at
  *     t + step/2 (loads: [nbod][9] linear force, spatial torque, referential
@@ -103,6 +109,7 @@ int b2dev_assemble(b2dev_ctx* ctx, double step, int dynamic, uint64_t colour_see
  *   b2dev_rigid_get: rot[9], x[3], velo[6], velo0[6] per body (any may be NULL). */
 int b2dev_rigid_setup(b2dev_ctx* ctx, const double* J, const double* mass, const double* x, const int* scheme,
                       int on_device);
+int b2dev_rigid_flags(b2dev_ctx* ctx, const int* flags, int on_device);
 int b2dev_rigid_step_begin(b2dev_ctx* ctx, double step, const double* gravity, const double* loads, int on_device);
 int b2dev_rigid_step_end(b2dev_ctx* ctx, double step);
 int b2dev_rigid_get(b2dev_ctx* ctx, double* rot, double* x, double* velo, double* velo0, int on_device);

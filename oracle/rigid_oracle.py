@@ -29,7 +29,8 @@ import math
 
 import numpy as np
 
-SCH_RIG_POS, SCH_RIG_NEG = 0, 1
+SCH_RIG_POS, SCH_RIG_NEG, SCH_RIG_IMP = 0, 1, 2
+BODY_DISABLE_ROTATION = 0x0004  # bod.h:144
 DEG_10_SQ = 3.0461741978671E-02
 
 
@@ -60,6 +61,131 @@ def expmap(w):
     R[5] = c12 + s0
     R[7] = c12 - s0
     return R
+
+
+def expmap123(w):
+    """EXPMAP123 (alg.h:1280-1382): the derivatives of exp[w] with respect to
+    w[0], w[1], w[2], column-major lists of 9."""
+    x = w[0] * w[0] + w[1] * w[1] + w[2] * w[2]
+    if x < 1E-16 * DEG_10_SQ:
+        R0, R1, R2 = [0.0] * 9, [0.0] * 9, [0.0] * 9
+        R0[5], R0[7] = 1.0, -1.0
+        R1[2], R1[6] = -1.0, 1.0
+        R2[1], R2[3] = 1.0, -1.0
+        return R0, R1, R2
+    c = 1.0 / x
+    if x < DEG_10_SQ:
+        a = 1.0 + (-1.666666666666667E-1 + (8.333333333333333E-3 + (-1.984126984126984E-4 + (
+            2.755731922398589E-6 + (-2.505210838544172E-8 + 1.605904383682161E-10 * x) * x) * x) * x) * x) * x
+        b = c - 0.5 + (4.166666666666667E-2 + (-1.388888888888889E-3 + (2.480158730158730E-5 + (
+            -2.755731922398589E-7 + (2.087675698786810E-9 - 1.147074559772972E-11 * x) * x) * x) * x) * x) * x
+    else:
+        x = math.sqrt(x)
+        a = math.sin(x) / x
+        b = c * math.cos(x)
+    b_ac = b - a * c
+    ac_2cc_2bc = (a - 2.0 * (c - b)) * c
+    c_b = c - b
+    aux = [w[i] * w[j] for j in range(3) for i in range(3)]
+    aux = [v * ac_2cc_2bc for v in aux]
+    t = [w[0] * b_ac, w[1] * b_ac, w[2] * b_ac]
+    aux[0] -= a; aux[1] += t[2]; aux[2] -= t[1]
+    aux[3] -= t[2]; aux[4] -= a; aux[5] += t[0]
+    aux[6] += t[1]; aux[7] -= t[0]; aux[8] -= a
+    t = [w[0] * c_b, w[1] * c_b, w[2] * c_b]
+    R0 = [aux[0] * w[0] + 2.0 * t[0], aux[1] * w[0] + t[1], aux[2] * w[0] + t[2],
+          aux[3] * w[0] + t[1], aux[4] * w[0], aux[5] * w[0] + a,
+          aux[6] * w[0] + t[2], aux[7] * w[0] - a, aux[8] * w[0]]
+    R1 = [aux[0] * w[1], aux[1] * w[1] + t[0], aux[2] * w[1] - a,
+          aux[3] * w[1] + t[0], aux[4] * w[1] + 2.0 * t[1], aux[5] * w[1] + t[2],
+          aux[6] * w[1] + a, aux[7] * w[1] + t[2], aux[8] * w[1]]
+    R2 = [aux[0] * w[2], aux[1] * w[2] + a, aux[2] * w[2] + t[0],
+          aux[3] * w[2] - a, aux[4] * w[2], aux[5] * w[2] + t[1],
+          aux[6] * w[2] + t[0], aux[7] * w[2] + t[1], aux[8] * w[2] + 2.0 * t[2]]
+    return R0, R1, R2
+
+
+def dgesv3(a, b):
+    """Solve a x = b in place (a column-major list of 9, b a list of 3) in
+    the arithmetic of LAPACK dgetf2 / dgetrs (as oracle/lu_small.c); returns
+    LAPACK's info (0, or k > 0 for an exactly zero U(k,k))."""
+    n, info, ipiv = 3, 0, [0, 0, 0]
+    for j in range(n):
+        p, amax = j, abs(a[j + j * n])
+        for i in range(j + 1, n):
+            if abs(a[i + j * n]) > amax:
+                amax, p = abs(a[i + j * n]), i
+        ipiv[j] = p
+        if a[p + j * n] != 0.0:
+            if p != j:
+                for c in range(n):
+                    a[j + c * n], a[p + c * n] = a[p + c * n], a[j + c * n]
+            piv = a[j + j * n]
+            if abs(piv) >= 2.2250738585072014e-308:
+                r = 1.0 / piv
+                for i in range(j + 1, n):
+                    a[i + j * n] *= r
+            else:
+                for i in range(j + 1, n):
+                    a[i + j * n] /= piv
+        elif info == 0:
+            info = j + 1
+        for c in range(j + 1, n):
+            u = a[j + c * n]
+            if u != 0.0:
+                t = -u
+                for i in range(j + 1, n):
+                    a[i + c * n] += a[i + j * n] * t
+    if info:
+        return info
+    for i in range(n):
+        p = ipiv[i]
+        if p != i:
+            b[i], b[p] = b[p], b[i]
+    for k in range(n):
+        if b[k] != 0.0:
+            for i in range(k + 1, n):
+                b[i] -= b[k] * a[i + k * n]
+    for k in range(n - 1, -1, -1):
+        if b[k] != 0.0:
+            b[k] /= a[k + k * n]
+            for i in range(k):
+                b[i] -= b[k] * a[i + k * n]
+    return 0
+
+
+def new3_solve(h, J, W, G):
+    """SOLVE (bod.c:163-209, NEW3): W with exp[hW] J W = G by Newton's method
+    from W; returns (W, A = exp[hW], code), code 1 for a singular Jacobian, 2
+    after 50 Newton steps (the reference stops there), else 0."""
+    W = list(W)
+    O = [W[0] * h, W[1] * h, W[2] * h]
+    A = expmap(O)
+    B = mat_mul(A, J)
+    R = mat_vec(B, W)
+    R = [R[i] - G[i] for i in range(3)]
+    level = 1E-12 * h
+    error = max(abs(R[0]), abs(R[1]), abs(R[2]))
+    i = 0
+    while error > level:
+        JW = mat_vec(J, W)
+        Z0, Z1, Z2 = expmap123(O)
+        Z = mat_vec(Z0, JW) + mat_vec(Z1, JW) + mat_vec(Z2, JW)
+        Z = [v * h for v in Z]
+        Z = [Z[q] + B[q] for q in range(9)]
+        if dgesv3(Z, R):
+            return W, A, 1
+        W = [W[k] - R[k] for k in range(3)]
+        O = [W[0] * h, W[1] * h, W[2] * h]
+        A = expmap(O)
+        B = mat_mul(A, J)
+        R = mat_vec(B, W)
+        R = [R[k] - G[k] for k in range(3)]
+        error = max(abs(R[0]), abs(R[1]), abs(R[2]))
+        i += 1
+        if not i < 50:
+            return W, A, 2
+    return W, A, 0
 
 
 def mat_mul(A, B):  # NNMUL
@@ -105,7 +231,7 @@ class Bodies:
     velo0[6], J[9], jinv[9], mass, minv, scheme, obstacle, x0[3] (referential
     mass centre), fext[6], aux[3]."""
 
-    def __init__(self, rot, x, velo, J, jinv, mass, minv, x0, obstacle, scheme=None):
+    def __init__(self, rot, x, velo, J, jinv, mass, minv, x0, obstacle, scheme=None, flags=None):
         nb = len(mass)
         f = lambda a, k: [list(map(float, np.asarray(a, dtype=np.float64).reshape(nb, k)[b])) for b in range(nb)]
         self.rot, self.x, self.velo = f(rot, 9), f(x, 3), f(velo, 6)
@@ -115,6 +241,8 @@ class Bodies:
         self.minv = [float(v) for v in np.asarray(minv, dtype=np.float64)]
         self.obstacle = [int(v) for v in obstacle]
         self.scheme = [SCH_RIG_NEG] * nb if scheme is None else [int(v) for v in scheme]
+        self.flags = [0] * nb if flags is None else [int(v) for v in flags]
+        self.failures = 0
         self.fext = [[0.0] * 6 for _ in range(nb)]
         self.aux = [[0.0] * 3 for _ in range(nb)]
 
@@ -128,6 +256,8 @@ def step_begin(bd: Bodies, step, gravity=(0.0, 0.0, 0.0), loads=None):
     half = 0.5 * step
     for b in range(bd.nbod):
         u = bd.velo[b]
+        if bd.flags[b] & BODY_DISABLE_ROTATION:
+            u[0] = u[1] = u[2] = 0.0
         bd.velo0[b] = list(u)
         J, I, Rold = bd.J[b], bd.jinv[b], bd.rot[b]
         W = u[0:3]
@@ -200,6 +330,8 @@ def step_end(bd: Bodies, step, master, slave, mpnt, spnt, base, R):
         x = bd.x[b]
         for i in range(3):
             x[i] = x[i] + half * u[3 + i]
+        if bd.flags[b] & BODY_DISABLE_ROTATION:
+            u[0] = u[1] = u[2] = 0.0
         sch = bd.scheme[b]
         DR = None
         if sch <= SCH_RIG_NEG:
@@ -211,6 +343,11 @@ def step_end(bd: Bodies, step, master, slave, mpnt, spnt, base, R):
             if sch == SCH_RIG_NEG:
                 W = mat_vec(I, matt_vec(DR, A))
                 u[0], u[1], u[2] = W[0], W[1], W[2]
+            else:  # NEW3
+                W, DR, code = new3_solve(half, bd.J[b], u[0:3], A)
+                bd.failures |= code
+                u[0], u[1], u[2] = W[0], W[1], W[2]
+                bd.rot[b] = mat_mul(Rb, DR)
 
 
 def kinetic_energy(bd: Bodies, b):

@@ -195,8 +195,10 @@ struct b2dev_ctx {
   bool deps_valid = false;
   // rigid time integration (b2dev_rigid_*): mass centre, inertia, mass, scheme,
   // external force of the step, NEW2 auxiliary vector, per-step loads
-  Buf rb_x, rb_J, rb_mass, rb_scheme, rb_fext, rb_aux, rb_loads;
+  Buf rb_x, rb_J, rb_mass, rb_scheme, rb_fext, rb_aux, rb_loads, rb_flags, rb_fail;
   bool have_rigid = false;
+  bool rb_imp = false;        // some body integrates with NEW3 (its Newton solve can fail)
+  bool rb_have_flags = false;
   // sphere contact detection (b2dev_spheres_setup, b2dev_detect_spheres): the
   // spheres, the grid, the pair lists, the contacts before sparsification
   // (st_*), and per contact of the last detection its sphere pair key, role
@@ -858,7 +860,7 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->cctrl, &c->keys_out, &c->iota, &c->perm, &c->iperm, &c->colptr, &c->sdeg, &c->rowptr, &c->col,
                 &c->W64, &c->W32, &c->Wd, &c->Ad, &c->Bv, &c->Vv, &c->rho, &c->gap, &c->fric, &c->rest, &c->coh,
                 &c->R64[0], &c->R64[1], &c->R64[2], &c->R32[0], &c->R32[1], &c->R32[2], &c->Us[0], &c->Us[1],
-                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tilek, &c->rtile, &c->dcnt, &c->depE_ptr, &c->depL_ptr, &c->depE, &c->depL, &c->tile_done, &c->rb_x, &c->rb_J, &c->rb_mass, &c->rb_scheme, &c->rb_fext, &c->rb_aux, &c->rb_loads, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec, &c->gptr_prev, &c->gcol_prev,
+                &c->Um[0], &c->Um[1], &c->conmerit[0], &c->conmerit[1], &c->done, &c->decided, &c->tiles, &c->tilek, &c->rtile, &c->dcnt, &c->depE_ptr, &c->depL_ptr, &c->depE, &c->depL, &c->tile_done, &c->rb_x, &c->rb_J, &c->rb_mass, &c->rb_scheme, &c->rb_fext, &c->rb_aux, &c->rb_loads, &c->rb_flags, &c->rb_fail, &c->tile_prob, &c->ptile_ptr, &c->ptile, &c->row_prob, &c->pctl, &c->pfe, &c->pvec, &c->gptr_prev, &c->gcol_prev,
                 &c->part, &c->rer,
                 &c->mer, &c->failkey, &c->failcount, &c->sctrl, &c->io, &c->cub_tmp, &c->trace,
                 // contact detection: spheres, grid, pairs, staged and detected contacts, convexes
@@ -1140,7 +1142,33 @@ static RigidDev rigid_view(b2dev_ctx* c) {
   d.velo0 = ptr<double>(c->velo0); d.fext = ptr<double>(c->rb_fext); d.aux = ptr<double>(c->rb_aux);
   d.J = ptr<double>(c->rb_J); d.jinv = ptr<double>(c->jinv); d.mass = ptr<double>(c->rb_mass);
   d.minv = ptr<double>(c->minv); d.scheme = ptr<int>(c->rb_scheme); d.obstacle = ptr<int>(c->obst);
+  d.flags = c->rb_have_flags ? ptr<int>(c->rb_flags) : nullptr;
+  d.fail = ptr<int>(c->rb_fail);
   return d;
+}
+
+// a failed NEW3 Newton solve of an earlier step end (bod.c:196, 206)
+static int rigid_failures(b2dev_ctx* c) {
+  if (!c->rb_imp) return B2DEV_OK;
+  int fail = 0;
+  B2_CK(cudaMemcpyAsync(&fail, c->rb_fail.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  B2_CK(cudaStreamSynchronize(c->stream));
+  if (fail) {
+    set_err("BODY_Dynamic_Step_End: NEW3 (RIG_IMP) %s", (fail & 1) ? "singular Jacobian in the Newton solve"
+                                                                   : "Newton solve not converged in 50 steps");
+    return B2DEV_EINVAL;
+  }
+  return B2DEV_OK;
+}
+
+int b2dev_rigid_flags(b2dev_ctx* c, const int* flags, int on_device) {
+  if (!c || !c->have_rigid) { set_err("rigid_flags: no rigid bodies set up"); return B2DEV_ESTATE; }
+  DeviceGuard g(c->device);
+  if (!flags) { c->rb_have_flags = false; return B2DEV_OK; }
+  B2_TRY(upload(c, c->rb_flags, flags, (size_t)c->nbod, on_device));
+  B2_CK(cudaStreamSynchronize(c->stream));
+  c->rb_have_flags = true;
+  return B2DEV_OK;
 }
 
 int b2dev_rigid_setup(b2dev_ctx* c, const double* J, const double* mass, const double* x, const int* scheme,
@@ -1157,11 +1185,13 @@ int b2dev_rigid_setup(b2dev_ctx* c, const double* J, const double* mass, const d
       std::copy(scheme, scheme + nb, sch.begin());
     }
     for (int b = 0; b < nb; b++)
-      if (sch[b] != SCH_RIG_POS && sch[b] != SCH_RIG_NEG) {
-        set_err("rigid_setup: body %d: scheme %d is not RIG_POS (0) or RIG_NEG (1)", b, sch[b]);
+      if (sch[b] != SCH_RIG_POS && sch[b] != SCH_RIG_NEG && sch[b] != SCH_RIG_IMP) {
+        set_err("rigid_setup: body %d: scheme %d is not RIG_POS (0), RIG_NEG (1) or RIG_IMP (2)", b, sch[b]);
         return B2DEV_EUNSUPPORTED;
       }
   }
+  c->rb_imp = std::find(sch.begin(), sch.end(), (int)SCH_RIG_IMP) != sch.end();
+  c->rb_have_flags = false;
   B2_TRY(upload(c, c->rb_J, J, (size_t)9 * nb, on_device));
   B2_TRY(upload(c, c->rb_mass, mass, (size_t)nb, on_device));
   B2_TRY(upload(c, c->rb_x, x, (size_t)3 * nb, on_device));
@@ -1169,6 +1199,8 @@ int b2dev_rigid_setup(b2dev_ctx* c, const double* J, const double* mass, const d
   B2_TRY(ensure(c->rb_fext, sizeof(double) * 6 * (nb + 1)));
   B2_TRY(ensure(c->rb_aux, sizeof(double) * 3 * (nb + 1)));
   B2_CK(cudaMemsetAsync(c->rb_aux.p, 0, sizeof(double) * 3 * (nb + 1), c->stream));
+  B2_TRY(ensure(c->rb_fail, sizeof(int)));
+  B2_CK(cudaMemsetAsync(c->rb_fail.p, 0, sizeof(int), c->stream));
   B2_CK(cudaStreamSynchronize(c->stream));
   c->have_rigid = true;
   return B2DEV_OK;
@@ -1178,6 +1210,7 @@ int b2dev_rigid_step_begin(b2dev_ctx* c, double step, const double* gravity, con
   if (!c || !c->have_rigid) { set_err("rigid_step_begin: no rigid bodies set up"); return B2DEV_ESTATE; }
   if (!(step > 0.0)) { set_err("rigid_step_begin: step must be positive"); return B2DEV_EINVAL; }
   DeviceGuard g(c->device);
+  B2_TRY(rigid_failures(c));
   const int nb = c->nbod;
   if (nb == 0) return B2DEV_OK;
   const double* dl = nullptr;
@@ -1228,7 +1261,7 @@ int b2dev_rigid_get(b2dev_ctx* c, double* rot, double* x, double* velo, double* 
     if (velo0) B2_CK(cudaMemcpyAsync(velo0, c->velo0.p, sizeof(double) * 6 * nb, kd, st));
   }
   B2_CK(cudaStreamSynchronize(st));
-  return B2DEV_OK;
+  return rigid_failures(c);
 }
 
 // ---- contact update and detection between spheres (dom.c:3700-3790) ----

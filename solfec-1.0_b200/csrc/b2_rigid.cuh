@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include "b2_common.cuh"
 #include "b2_assemble.cuh"
+#include "b2_diag.cuh"
 
 namespace b2 {
 
@@ -97,6 +98,106 @@ __device__ __forceinline__ void add_minv_force(const double* jinv, double minv, 
   for (int i = 0; i < 3; i++) u[3 + i] = u[3 + i] + (step * f[3 + i]) * minv;
 }
 
+// EXPMAP123, alg.h:1280-1382: the derivatives R0, R1, R2 of exp[w] with
+// respect to w[0], w[1], w[2] (column-major); below ten degrees the Taylor
+// polynomials of EXPMAP, above them sin and cos
+__device__ __noinline__ void expmap123(const double* w, double* R0, double* R1, double* R2) {
+  double x = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+  if (x < 1E-16 * 3.0461741978671E-02) {
+    for (int q = 0; q < 9; q++) R0[q] = R1[q] = R2[q] = 0.0;
+    R0[5] = 1.0; R0[7] = -1.0;
+    R1[2] = -1.0; R1[6] = 1.0;
+    R2[1] = 1.0; R2[3] = -1.0;
+    return;
+  }
+  const double c = 1.0 / x;
+  double a, b;
+  if (x < 3.0461741978671E-02) {
+    a = 1.0 + (-1.666666666666667E-1 +
+               (8.333333333333333E-3 +
+                (-1.984126984126984E-4 + (2.755731922398589E-6 + (-2.505210838544172E-8 + 1.605904383682161E-10 * x) * x) * x) *
+                    x) *
+                   x) *
+                  x;
+    b = c - 0.5 +
+        (4.166666666666667E-2 +
+         (-1.388888888888889E-3 +
+          (2.480158730158730E-5 + (-2.755731922398589E-7 + (2.087675698786810E-9 - 1.147074559772972E-11 * x) * x) * x) * x) *
+             x) *
+            x;
+  } else {
+    x = sqrt(x);
+    a = sin(x) / x;
+    b = c * cos(x);
+  }
+  const double b_ac = b - a * c;
+  const double ac_2cc_2bc = (a - 2.0 * (c - b)) * c;
+  const double c_b = c - b;
+  double aux[9];
+  for (int j = 0; j < 3; j++)
+    for (int i = 0; i < 3; i++) aux[3 * j + i] = w[i] * w[j];
+  for (int q = 0; q < 9; q++) aux[q] *= ac_2cc_2bc;
+  double t[3] = {w[0] * b_ac, w[1] * b_ac, w[2] * b_ac};
+  aux[0] -= a; aux[1] += t[2]; aux[2] -= t[1];
+  aux[3] -= t[2]; aux[4] -= a; aux[5] += t[0];
+  aux[6] += t[1]; aux[7] -= t[0]; aux[8] -= a;
+  t[0] = w[0] * c_b; t[1] = w[1] * c_b; t[2] = w[2] * c_b;
+  R0[0] = aux[0] * w[0] + 2.0 * t[0]; R0[1] = aux[1] * w[0] + t[1]; R0[2] = aux[2] * w[0] + t[2];
+  R0[3] = aux[3] * w[0] + t[1]; R0[4] = aux[4] * w[0]; R0[5] = aux[5] * w[0] + a;
+  R0[6] = aux[6] * w[0] + t[2]; R0[7] = aux[7] * w[0] - a; R0[8] = aux[8] * w[0];
+  R1[0] = aux[0] * w[1]; R1[1] = aux[1] * w[1] + t[0]; R1[2] = aux[2] * w[1] - a;
+  R1[3] = aux[3] * w[1] + t[0]; R1[4] = aux[4] * w[1] + 2.0 * t[1]; R1[5] = aux[5] * w[1] + t[2];
+  R1[6] = aux[6] * w[1] + a; R1[7] = aux[7] * w[1] + t[2]; R1[8] = aux[8] * w[1];
+  R2[0] = aux[0] * w[2]; R2[1] = aux[1] * w[2] + a; R2[2] = aux[2] * w[2] + t[0];
+  R2[3] = aux[3] * w[2] - a; R2[4] = aux[4] * w[2]; R2[5] = aux[5] * w[2] + t[1];
+  R2[6] = aux[6] * w[2] + t[0]; R2[7] = aux[7] * w[2] + t[1]; R2[8] = aux[8] * w[2] + 2.0 * t[2];
+}
+
+__device__ __forceinline__ double maxabs3(const double* r) {  // MAXABS, alg.h:434-442
+  double m = r[0] > 0 ? r[0] : -r[0];
+  const double a1 = r[1] > 0 ? r[1] : -r[1], a2 = r[2] > 0 ? r[2] : -r[2];
+  if (m < a1) m = a1;
+  if (m < a2) m = a2;
+  return m;
+}
+
+// SOLVE, bod.c:163-209 (NEW3): W with exp[hW] J W = G by Newton's method from
+// the given W, A = exp[hW]; the Jacobian dexp[hW] h J W + exp[hW] J is solved
+// by LU as LAPACK dgesv does. Returns 0, 1 for a singular Jacobian
+// (ERR_BOD_NEW3_SINGULAR_JACOBIAN) or 2 after 50 Newton steps
+// (ERR_BOD_NEW3_NEWTON_DIVERGENCE); the reference stops the program there.
+__device__ __noinline__ int rig_new3_solve(double h, const double* J, double* W, const double* G, double* A) {
+  double O[3], B[9], R[3];
+  int i = 0;
+  O[0] = W[0] * h; O[1] = W[1] * h; O[2] = W[2] * h;
+  expmap(O, A);
+  mat_mul(A, J, B);
+  mat_vec(B, W, R);
+  R[0] = R[0] - G[0]; R[1] = R[1] - G[1]; R[2] = R[2] - G[2];
+  const double level = 1E-12 * h;
+  double error = maxabs3(R);
+  while (error > level) {
+    double JW[3], Z0[9], Z1[9], Z2[9], Z[9];
+    mat_vec(J, W, JW);
+    expmap123(O, Z0, Z1, Z2);
+    mat_vec(Z0, JW, Z);
+    mat_vec(Z1, JW, Z + 3);
+    mat_vec(Z2, JW, Z + 6);
+    for (int q = 0; q < 9; q++) Z[q] *= h;
+    for (int q = 0; q < 9; q++) Z[q] = Z[q] + B[q];
+    if (lu3_solve(Z, R)) return 1;
+    W[0] = W[0] - R[0]; W[1] = W[1] - R[1]; W[2] = W[2] - R[2];
+    O[0] = W[0] * h; O[1] = W[1] * h; O[2] = W[2] * h;
+    expmap(O, A);
+    mat_mul(A, J, B);
+    mat_vec(B, W, R);
+    R[0] = R[0] - G[0]; R[1] = R[1] - G[1]; R[2] = R[2] - G[2];
+    error = maxabs3(R);
+    if (!(++i < 50)) return 2;
+  }
+  return 0;
+}
+
 struct RigidDev {
   int nbod;
   double* rot;          // [nbod][9] R, column-major (in place)
@@ -111,7 +212,11 @@ struct RigidDev {
   const double* minv;   // [nbod]
   const int* scheme;    // [nbod]
   const int* obstacle;  // [nbod]
+  const int* flags;     // [nbod] BODY_* flags (BODY_DISABLE_ROTATION = 4 honoured), or null
+  int* fail;            // NEW3 failures (bit or of rig_new3_solve's codes)
 };
+
+constexpr int kBodyDisableRotation = 0x0004;  // BODY_DISABLE_ROTATION, bod.h:144
 
 // BODY_Dynamic_Step_Begin (bod.c:1316-1370) for every body. loads[9 b ..]:
 // linear force, spatial torque, referential torque of the body's point loads
@@ -128,6 +233,7 @@ __global__ void k_rigid_begin(RigidDev d, double step, double g0, double g1, dou
   double J[9], I[9], W[3], DR[9], O[3], Rold[9], f[6];
 #pragma unroll
   for (int q = 0; q < 9; q++) { J[q] = d.J[9 * (size_t)b + q]; I[q] = d.jinv[9 * (size_t)b + q]; Rold[q] = R[q]; }
+  if (d.flags && (d.flags[b] & kBodyDisableRotation)) u[0] = u[1] = u[2] = 0.0;
 #pragma unroll
   for (int q = 0; q < 6; q++) u0[q] = u[q];
   W[0] = u[0]; W[1] = u[1]; W[2] = u[2];
@@ -231,6 +337,7 @@ __global__ void k_rigid_end(RigidDev d, double step, const double* x0, const int
   add_minv_force(I, d.minv[b], step, f, u);                   // u(t+h) += h M^-1 r
 #pragma unroll
   for (int i = 0; i < 3; i++) x[i] = x[i] + half * u[3 + i];  // x(t+h) = x(t+h/2) + (h/2) v(t+h)
+  if (d.flags && (d.flags[b] & kBodyDisableRotation)) u[0] = u[1] = u[2] = 0.0;
   const int sch = d.scheme[b];
   double DR[9];
   if (sch <= SCH_RIG_NEG) {  // R(t+h) = R(t+h/2) exp[(h/2) W(t+h)]
@@ -252,6 +359,17 @@ __global__ void k_rigid_end(RigidDev d, double step, const double* x0, const int
       double O[3];
       matt_vec(DR, A, O);
       mat_vec(I, O, u);
+    } else {  // NEW3: exp[(h/2)W(t+h)] J W(t+h) = A, then R(t+h) = R(t+h/2) exp[(h/2)W(t+h)]
+      double J[9], W[3] = {u[0], u[1], u[2]};
+#pragma unroll
+      for (int q = 0; q < 9; q++) J[q] = d.J[9 * (size_t)b + q];
+      const int e = rig_new3_solve(half, J, W, A, DR);
+      if (e) atomicOr(d.fail, e);
+      u[0] = W[0]; u[1] = W[1]; u[2] = W[2];
+      double Rn[9];
+      mat_mul(Rb, DR, Rn);
+#pragma unroll
+      for (int q = 0; q < 9; q++) R[q] = Rn[q];
     }
   }
 }

@@ -82,6 +82,7 @@ _SIGNATURES = {
                                       C.c_void_p, C.c_int]),
     'b2dev_detect_spheres': (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     'b2dev_convexes_setup': (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 7),
+    'b2dev_rigid_flags': (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     'b2dev_contact_sparsify': (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
     'b2dev_get_contact_area': (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     'b2dev_detect_carry_state': (C.c_int, [C.c_void_p]),

@@ -24,7 +24,8 @@ import numpy as np
 from ._lib import lib, ptr
 from .solver import LOCDYN, _check
 
-SCHEMES = {'RIG_POS': 0, 'RIG_NEG': 1}
+SCHEMES = {'RIG_POS': 0, 'RIG_NEG': 1, 'RIG_IMP': 2}
+BODY_DISABLE_ROTATION = 0x0004  # bod.h:144
 
 
 def _f64(a, n):
@@ -38,10 +39,12 @@ class RIGID_DYNAMICS:
     """Device time integration of the bodies of a LOCDYN's uploaded scene.
 
     J: (nbod, 9) referential inertia (column-major); mass: (nbod,); x: (nbod, 3)
-    current mass centres; scheme: None (all 'RIG_NEG') or one name per body.
+    current mass centres; scheme: None (all 'RIG_NEG') or one name per body
+    ('RIG_POS' NEW1, 'RIG_NEG' NEW2, 'RIG_IMP' NEW3); disable_rotation: None
+    or a boolean per body (BODY_DISABLE_ROTATION).
     """
 
-    def __init__(self, ldy: LOCDYN, J, mass, x, scheme=None):
+    def __init__(self, ldy: LOCDYN, J, mass, x, scheme=None, disable_rotation=None):
         self.ldy = ldy
         self.nbod = int(np.asarray(mass).reshape(-1).shape[0])
         nb = self.nbod
@@ -55,10 +58,16 @@ class RIGID_DYNAMICS:
                 raise ValueError('one scheme per body')
             for s in names:
                 if s not in SCHEMES:
-                    raise ValueError("scheme %r is not supported on the device (RIG_POS, RIG_NEG)" % s)
+                    raise ValueError("scheme %r is not one of RIG_POS, RIG_NEG, RIG_IMP" % s)
             sch = np.array([SCHEMES[s] for s in names], dtype=np.int32)
         _check(lib().b2dev_rigid_setup(ldy.device_context, ptr(self._J), ptr(self._mass), ptr(self._x), ptr(sch), 0),
                'b2dev_rigid_setup')
+        if disable_rotation is not None:
+            flags = np.where(np.asarray(disable_rotation, bool).reshape(-1), BODY_DISABLE_ROTATION, 0).astype(np.int32)
+            if flags.shape[0] != nb:
+                raise ValueError('one disable_rotation flag per body')
+            self._flags = flags
+            _check(lib().b2dev_rigid_flags(ldy.device_context, ptr(flags), 0), 'b2dev_rigid_flags')
 
     def step_begin(self, step: float, gravity=(0.0, 0.0, 0.0), loads=None):
         """BODY_Dynamic_Step_Begin of every body. loads: None or (nbod, 9)

@@ -32,29 +32,33 @@ def _scene_with_spin(seed, omega):
     J = np.stack([np.eye(3).reshape(9) if o else np.linalg.inv(j.reshape(3, 3).T).T.reshape(9)
                   for j, o in zip(sc.jinv, ob)])
     mass = np.where(ob, 1.0, 1.0 / np.where(ob, 1.0, sc.minv))
-    schemes = ['RIG_NEG' if b % 3 else 'RIG_POS' for b in range(nb)]
+    schemes = [('RIG_POS', 'RIG_NEG', 'RIG_IMP')[b % 3] for b in range(nb)]
     loads = rng.normal(size=(nb, 9))
     return sc, J, mass, schemes, loads
 
 
-def _oracle_bodies(sc, J, mass, schemes):
+def _oracle_bodies(sc, J, mass, schemes, flags=None):
+    from solfec_b200.dynamics import SCHEMES
     return ro.Bodies(sc.rot, sc.x, sc.velo, J, sc.jinv, mass, sc.minv, sc.x0, sc.obstacle,
-                     [0 if s == 'RIG_POS' else 1 for s in schemes])
+                     [SCHEMES[s] for s in schemes], flags)
 
 
 @pytest.mark.parametrize('omega,exact', [(5.0, True), (900.0, False)])
 def test_rigid_step_parity(omega, exact):
-    """Device begin/end against the oracle on 60 bodies with both schemes,
-    obstacles, point loads and random reactions: bitwise while the rotation
-    of a half step stays below ten degrees (Taylor branch of the exponential
-    map), within 1e-12 relative above it (sin/cos of two libraries)."""
+    """Device begin/end against the oracle on 60 bodies with the three schemes
+    (NEW1, NEW2, NEW3's Newton solve), every seventh body with
+    BODY_DISABLE_ROTATION, obstacles, point loads and random reactions:
+    bitwise while the rotation of a half step stays below ten degrees (Taylor
+    branch of the exponential map and its derivatives), within 1e-12 relative
+    above it (sin/cos of two libraries)."""
     sc, J, mass, schemes, loads = _scene_with_spin(11, omega)
     h = 1e-3
     g = (0.0, 0.0, -9.81)
     ldy = LOCDYN()
     ldy.update_begin(sc)
-    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x, schemes)
-    bd = _oracle_bodies(sc, J, mass, schemes)
+    off = np.arange(sc.nbod) % 7 == 3
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x, schemes, disable_rotation=off)
+    bd = _oracle_bodies(sc, J, mass, schemes, np.where(off, ro.BODY_DISABLE_ROTATION, 0))
 
     def same(a, b):
         a, b = np.asarray(a, float), np.asarray(b, float)
@@ -81,17 +85,46 @@ def test_rigid_step_parity(omega, exact):
     ldy.close()
 
 
-def test_rigid_rejects_unsupported_scheme():
+def test_rigid_rejects_unknown_scheme():
     sc, J, mass, _, _ = _scene_with_spin(2, 1.0)
     ldy = LOCDYN()
     ldy.update_begin(sc)
     with pytest.raises(ValueError):
-        RIGID_DYNAMICS(ldy, J, mass, sc.x, 'RIG_IMP')
-    sch = np.full(sc.nbod, 2, dtype=np.int32)  # RIG_IMP through the C ABI
+        RIGID_DYNAMICS(ldy, J, mass, sc.x, 'RIG_FOO')
+    sch = np.full(sc.nbod, 3, dtype=np.int32)  # no such scheme, through the C ABI
     from solfec_b200._lib import ptr
     Jc = np.ascontiguousarray(J); mc = np.ascontiguousarray(mass); xc = np.ascontiguousarray(sc.x)
     assert lib().b2dev_rigid_setup(ldy.device_context, ptr(Jc), ptr(mc), ptr(xc), ptr(sch), 0) != 0
     ldy.close()
+
+
+def test_new3_failure_reported():
+    """A NEW3 body whose Newton Jacobian is singular (zero inertia under a
+    referential torque), where the reference stops the program
+    (ERR_BOD_NEW3_SINGULAR_JACOBIAN, bod.c:196): the device records it and the
+    next state read raises; the oracle reports the same."""
+    from solfec_b200 import DeviceError
+    sc, J, mass, _, _ = _scene_with_spin(5, 1.0)
+    J = J.copy()
+    b = int(np.nonzero(sc.obstacle == 0)[0][0])
+    J[b] = 0.0
+    loads = np.zeros((sc.nbod, 9)); loads[b, 6] = 1.0
+    sc = dataclasses.replace(sc, master=np.zeros(0, np.int32), slave=np.zeros(0, np.int32), mpnt=np.zeros((0, 3)),
+                             spnt=np.zeros((0, 3)), base=np.zeros((0, 9)), gap=np.zeros(0), friction=np.zeros(0),
+                             restitution=np.zeros(0), cohesion=np.zeros(0))
+    ldy = LOCDYN()
+    ldy.update_begin(sc)
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x, 'RIG_IMP')
+    dyn.step_begin(1e-3, (0.0, 0.0, 0.0), loads)
+    dyn.step_end(1e-3)
+    with pytest.raises(DeviceError, match='NEW3'):
+        dyn.state()
+    ldy.close()
+    bd = _oracle_bodies(sc, J, mass, ['RIG_IMP'] * sc.nbod)
+    none = (np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 9)), np.zeros((0, 3)))
+    ro.step_begin(bd, 1e-3, (0.0, 0.0, 0.0), loads)
+    ro.step_end(bd, 1e-3, [], [], *none)
+    assert bd.failures == 1
 
 
 def test_block_sliding_device():

@@ -34,14 +34,15 @@ def inertia(sc):
     return J, mass
 
 
-def time_loop_parity(sc, steps, J=None, mass=None, **kw):
+def time_loop_parity(sc, steps, J=None, mass=None, scheme=None, **kw):
     if J is None:
         J, mass = inertia(sc)
     h = float(sc.step)
     ldy = LOCDYN()
     ldy.update_begin(sc)
-    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x)
-    bd = ro.Bodies(sc.rot, sc.x, sc.velo, J, sc.jinv, mass, sc.minv, sc.x0, sc.obstacle)
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x, scheme)
+    codes = None if scheme is None else [{'RIG_POS': 0, 'RIG_NEG': 1, 'RIG_IMP': 2}[scheme]] * sc.nbod
+    bd = ro.Bodies(sc.rot, sc.x, sc.velo, J, sc.jinv, mass, sc.minv, sc.x0, sc.obstacle, codes)
     gs = GAUSS_SEIDEL_SOLVER(**kw)
     n = sc.ncon
     R = np.zeros((n, 3)); U = np.zeros((n, 3))
@@ -118,3 +119,13 @@ def test_detected_hexahedra_time_loop():
     assert det.ncon > 400 and np.median(det.gap) < 0.0
     iters, _ = time_loop_parity(det, 8, epsilon=1.0, maxiter=1000, meritval=1e-4)
     assert min(iters) >= 1
+
+
+def test_masonry_arch_new3_time_loop():
+    """The stable arch of tests/arch.py integrated with NEW3 (RIG_IMP, the
+    Newton solve of bod.c:163-209) for 300 steps: device and CPU restatement
+    bitwise at every step; the arch stays at rest."""
+    sc, J, mass = scenes.masonry_arch(0.1095)
+    iters, bd = time_loop_parity(sc, 300, J=J, mass=mass, scheme='RIG_IMP', epsilon=1e-4, maxiter=10000)
+    assert bd.failures == 0
+    assert sum(ro.kinetic_energy(bd, b) for b in range(bd.nbod) if not bd.obstacle[b]) < 1e-4
