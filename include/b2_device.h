@@ -119,7 +119,7 @@ int b2dev_rigid_get(b2dev_ctx* ctx, double* rot, double* x, double* velo, double
  * the device bodies (rotation of b2dev_upload_scene, mass centre of
  * b2dev_rigid_setup, both as moved by the b2dev_rigid_* steps).
  *   b2dev_spheres_setup: per sphere its body, referential centre[3], radius
- *     and surface id (0 .. nsurf-1); material[2 * (s1 * nsurf + s2) + {0, 1}]
+ *     and surface id (0 .. nsurf-1; with nsph = 0 the arrays may be NULL); material[2 * (s1 * nsurf + s2) + {0, 1}]
  *     = friction, restitution of a surface pair (SPSET_Find resolved by the
  *     caller; the table must be symmetric; host memory).
  *   b2dev_detect_spheres: the contacts of the last detection are updated with

@@ -1269,7 +1269,7 @@ int b2dev_rigid_get(b2dev_ctx* c, double* rot, double* x, double* velo, double* 
 int b2dev_spheres_setup(b2dev_ctx* c, int nsph, const int* body, const double* centre, const double* radius,
                         const int* surface, int nsurf, const double* material, int on_device) {
   if (!c || !c->have_scene) { set_err("spheres_setup: no scene uploaded"); return B2DEV_ESTATE; }
-  if (nsph < 0 || !body || !centre || !radius || !surface || nsurf <= 0 || !material) {
+  if (nsph < 0 || (nsph > 0 && (!body || !centre || !radius || !surface)) || nsurf <= 0 || !material) {
     set_err("spheres_setup: invalid arguments");
     return B2DEV_EINVAL;
   }
