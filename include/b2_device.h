@@ -176,6 +176,19 @@ int b2dev_convexes_setup(b2dev_ctx* ctx, int nconv, const int* body, const int* 
  *   b2dev_get_contact_area: the area of every detected contact (1 for sphere
  *     contacts, goc.c:341 and 436). */
 int b2dev_contact_sparsify(b2dev_ctx* ctx, double threshold, double minarea, double mindist);
+/* Detection controls of the reference's Python interface:
+ *   b2dev_exclude_bodies: CONTACT_EXCLUDE_BODIES (lng.c:8817-8852): body pairs
+ *     pairs[2k], pairs[2k+1] (0 .. nbod-1) never make contacts (the nobody set
+ *     of the broad-phase filter, box.c:116-118); replaces earlier pairs.
+ *   b2dev_exclude_surfaces: CONTACT_EXCLUDE_SURFACES (lng.c:8855-8872): no new
+ *     contact is created for the surface pairs (either order; dom.c:379-389);
+ *     contacts that exist are updated as before. Replaces earlier pairs.
+ *   b2dev_unphysical_penetration: UNPHYSICAL_PENETRATION (lng.c:9175-9191),
+ *     depth > 0: a detection that finds a contact with gap <= -depth fails with
+ *     an error, where the reference stops (dom.c:374, 461, 3792). */
+int b2dev_exclude_bodies(b2dev_ctx* ctx, int npairs, const int* pairs);
+int b2dev_exclude_surfaces(b2dev_ctx* ctx, int npairs, const int* pairs);
+int b2dev_unphysical_penetration(b2dev_ctx* ctx, double depth);
 int b2dev_get_contact_area(b2dev_ctx* ctx, double* area, int on_device);
 int b2dev_detect_carry_state(b2dev_ctx* ctx);
 int b2dev_get_contacts(b2dev_ctx* ctx, int* master, int* slave, double* point, double* mpnt, double* spnt,

@@ -209,6 +209,36 @@ __device__ __forceinline__ int nearest_surface_id(const double* pnt, const doubl
   return ret;
 }
 
+// CONTACT_EXCLUDE_BODIES (lng.c:8817-8852; the nobody set of box.c:116-118):
+// excluded body pairs as min << 32 | max keys in ascending order
+struct PairFilter {
+  const long long* body_pairs;
+  int n;
+};
+
+__device__ __forceinline__ bool body_pair_excluded(const PairFilter& f, int a, int b) {
+  if (f.n == 0) return false;
+  const long long key = ((long long)(a < b ? a : b) << 32) | (long long)(a < b ? b : a);
+  int lo = 0, hi = f.n - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const long long v = f.body_pairs[mid];
+    if (v == key) return true;
+    if (v < key) lo = mid + 1; else hi = mid - 1;
+  }
+  return false;
+}
+
+// CONTACT_EXCLUDE_SURFACES (lng.c:8855-8872; dom.c:379-389): a new contact of
+// an excluded surface pair is not created (nosurf[s1 * nsurf + s2], symmetric,
+// or null); UNPHYSICAL_PENETRATION (lng.c:9175-9191): a contact whose gap is
+// at or below depth (negative; -DBL_MAX unless set) sets bad flag 128, where
+// the reference stops (dom.c:374, 461, 3792)
+struct ContactRules {
+  const unsigned char* nosurf;
+  double depth;
+};
+
 __device__ __forceinline__ unsigned int cell_hash(int x, int y, int z, unsigned int mask) {
   return (((unsigned int)x * 73856093u) ^ ((unsigned int)y * 19349663u) ^ ((unsigned int)z * 83492791u)) & mask;
 }
@@ -269,8 +299,8 @@ __global__ void k_sph_buckets(int n, const unsigned int* key, int* bstart, int* 
 
 // WRITE = false: count[i] = pairs (i, j > i); WRITE = true: their j at off[i]..
 template <bool WRITE>
-__global__ void k_sph_pairs(SphereDev s, const int* obst, const int* sorted, const int* bstart, const int* bend,
-                            unsigned int mask, int* count, const int* off, int* pj) {
+__global__ void k_sph_pairs(SphereDev s, const int* obst, PairFilter pf, const int* sorted, const int* bstart,
+                            const int* bend, unsigned int mask, int* count, const int* off, int* pj) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= s.nsph) return;
   const int i = sorted[t];
@@ -294,7 +324,7 @@ __global__ void k_sph_pairs(SphereDev s, const int* obst, const int* sorted, con
           const int4 cj = s.cell[j];
           if (cj.x != nx || cj.y != ny || cj.z != nz) continue;  // another cell in the same bucket
           const int bj = s.body[j];
-          if (bj < 0 || bj >= s.nbod || bj == bi || (oi && obst[bj])) continue;
+          if (bj < 0 || bj >= s.nbod || bj == bi || (oi && obst[bj]) || body_pair_excluded(pf, bi, bj)) continue;
           const double b[3] = {s.cur[3 * (size_t)j], s.cur[3 * (size_t)j + 1], s.cur[3 * (size_t)j + 2]};
           if (gjk_spheres_gap(a, ra, b, s.rad[j]) < kGeomEps) {
             if (WRITE) pj[w++] = j;
@@ -310,7 +340,7 @@ __global__ void k_sph_pairs(SphereDev s, const int* obst, const int* sorted, con
 // gjk_convex_point distance. WRITE = false: ccount[i]; WRITE = true: written
 // after the sphere's sphere partners, at off[i] + scount[i]
 template <bool WRITE>
-__global__ void k_cvx_pairs(SphereDev s, ConvexDev cv, const int* obst, int* ccount, const int* off,
+__global__ void k_cvx_pairs(SphereDev s, ConvexDev cv, const int* obst, PairFilter pf, int* ccount, const int* off,
                             const int* scount, int* pj) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.nsph) return;
@@ -323,7 +353,7 @@ __global__ void k_cvx_pairs(SphereDev s, ConvexDev cv, const int* obst, int* cco
   int w = WRITE ? off[i] + scount[i] : 0;
   for (int c = 0; c < cv.n; c++) {
     const int bc = cv.body[c];
-    if (bc == bi || (oi && obst[bc])) continue;
+    if (bc == bi || (oi && obst[bc]) || body_pair_excluded(pf, bi, bc)) continue;
     const double* bx = cv.box + 6 * (size_t)c;
     bool near = true;
     for (int k = 0; k < 3; k++)
@@ -373,8 +403,8 @@ struct ContactOut {
 };
 
 __global__ void k_sph_contacts(int npair, SphereDev s, ConvexDev cv, const int* pi, const int* pj, const double* rot,
-                               const double* xb, const double* x0, int nsurf, const double* mat, int nprev,
-                               const long long* prevkey, const int* prevslave_lo, const double* prevR,
+                               const double* xb, const double* x0, int nsurf, const double* mat, ContactRules cr,
+                               int nprev, const long long* prevkey, const int* prevslave_lo, const double* prevR,
                                const double* prevU, ContactOut o, int* bad) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= npair) return;
@@ -432,6 +462,7 @@ __global__ void k_sph_contacts(int npair, SphereDev s, ConvexDev cv, const int* 
     local_base(n, loc);
     for (int v = 0; v < 9; v++) o.base[9 * (size_t)k + v] = loc[v];
     const int s1 = nearest_surface_id(one, pla, fs, ns), s2 = s.surf[i];
+    if (o.gap[k] <= cr.depth) atomicOr(bad, 128);
     if (s1 < 0 || s1 >= nsurf || s2 < 0 || s2 >= nsurf) {
       atomicOr(bad, 8);
       o.fric[k] = o.rest[k] = 0.0;
@@ -439,6 +470,7 @@ __global__ void k_sph_contacts(int npair, SphereDev s, ConvexDev cv, const int* 
       const size_t t = (size_t)s1 * nsurf + s2;
       o.fric[k] = mat[2 * t];
       o.rest[k] = mat[2 * t + 1];
+      if (hit < 0 && cr.nosurf && cr.nosurf[t]) o.master[k] = o.slave[k] = -1;  // an excluded surface pair
     }
     o.coh[k] = 0.0;
     o.area[k] = 1.0;  // detect_convex_sphere, goc.c:341
@@ -486,6 +518,7 @@ __global__ void k_sph_contacts(int npair, SphereDev s, ConvexDev cv, const int* 
   local_base(n, loc);
   for (int v = 0; v < 9; v++) o.base[9 * (size_t)k + v] = loc[v];
   o.gap[k] = g;
+  if (g <= cr.depth) atomicOr(bad, 128);
   const int s1 = s.surf[sv], s2 = s.surf[ms];
   if (s1 < 0 || s1 >= nsurf || s2 < 0 || s2 >= nsurf) {
     atomicOr(bad, 8);
@@ -494,6 +527,7 @@ __global__ void k_sph_contacts(int npair, SphereDev s, ConvexDev cv, const int* 
     const size_t t = (size_t)s1 * nsurf + s2;
     o.fric[k] = mat[2 * t];
     o.rest[k] = mat[2 * t + 1];
+    if (hit < 0 && cr.nosurf && cr.nosurf[t]) o.master[k] = o.slave[k] = -1;  // an excluded surface pair
   }
   o.coh[k] = 0.0;
   o.area[k] = 1.0;  // detect_sphere_sphere, goc.c:436
@@ -573,9 +607,10 @@ __global__ void k_cc_cells(ConvexDev cv, const double* ext, const double* sum, c
   hkey[c] = cell_hash(q[0], q[1], q[2], mask);
 }
 
-__device__ __forceinline__ bool cc_candidate(const ConvexDev& cv, const int* obst, int i, int j) {
+__device__ __forceinline__ bool cc_candidate(const ConvexDev& cv, const int* obst, const PairFilter& pf, int i,
+                                             int j) {
   const int bi = cv.body[i], bj = cv.body[j];
-  if (bi == bj || (obst[bi] && obst[bj])) return false;
+  if (bi == bj || (obst[bi] && obst[bj]) || body_pair_excluded(pf, bi, bj)) return false;
   const double* a = cv.box + 6 * i;
   const double* b = cv.box + 6 * j;
   for (int k = 0; k < 3; k++)
@@ -600,7 +635,7 @@ __global__ void k_cc_gjk(int n, int nsph, ConvexDev cv, const long long* keys, u
 // pairs only with large l > i). WRITE = false: cnt[t]; WRITE = true: the keys
 // from off[t].
 template <bool WRITE>
-__global__ void k_cc_pairs(ConvexDev cv, const int* obst, int nsph, const int* sorted, const int4* cell,
+__global__ void k_cc_pairs(ConvexDev cv, const int* obst, PairFilter pf, int nsph, const int* sorted, const int4* cell,
                            const int* bstart, const int* bend, unsigned int mask, const int* large, int nlarge,
                            int* cnt, const int* off, long long* keys) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -626,14 +661,14 @@ __global__ void k_cc_pairs(ConvexDev cv, const int* obst, int nsph, const int* s
             if (j <= i) continue;
             const int4 cj = cell[j];
             if (cj.x != nx || cj.y != ny || cj.z != nz) continue;  // another cell in the same bucket
-            if (cc_candidate(cv, obst, i, j)) emit(j);
+            if (cc_candidate(cv, obst, pf, i, j)) emit(j);
           }
         }
   }
   for (int u = 0; u < nlarge; u++) {
     const int l = large[u];
     if (l == i || (ci.w != 0 && l < i)) continue;
-    if (cc_candidate(cv, obst, i, l)) emit(l);
+    if (cc_candidate(cv, obst, pf, i, l)) emit(l);
   }
   if (!WRITE) cnt[t] = found;
 }
@@ -645,7 +680,8 @@ __global__ void k_cc_pairs(ConvexDev cv, const int* obst, int nsph, const int* s
 // intersection's capacity (32 planes of both convexes together).
 __global__ void __launch_bounds__(64) k_cc_contacts(int ncc, int k0, int nsph, ConvexDev cv, const long long* ckey,
                                                     const double* rot, const double* xb, const double* x0, int nsurf,
-                                                    const double* mat, int nprev, const long long* prevkey,
+                                                    const double* mat, ContactRules cr, int nprev,
+                                                    const long long* prevkey,
                                                     const double* prevR, const double* prevU, ContactOut o, int* bad) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ncc) return;
@@ -701,6 +737,7 @@ __global__ void __launch_bounds__(64) k_cc_contacts(int ncc, int k0, int nsph, C
   for (int v = 0; v < 9; v++) o.base[9 * (size_t)k + v] = loc[v];
   o.gap[k] = ct.gap;
   o.area[k] = ct.area;
+  if (ct.gap <= cr.depth) atomicOr(bad, 128);
   const int s1 = ct.spair[0], s2 = ct.spair[1];
   if (s1 < 0 || s1 >= nsurf || s2 < 0 || s2 >= nsurf) {
     atomicOr(bad, 8);
@@ -709,6 +746,7 @@ __global__ void __launch_bounds__(64) k_cc_contacts(int ncc, int k0, int nsph, C
     const size_t u = (size_t)s1 * nsurf + s2;
     o.fric[k] = mat[2 * u];
     o.rest[k] = mat[2 * u + 1];
+    if (hit < 0 && cr.nosurf && cr.nosurf[u]) o.master[k] = o.slave[k] = -1;  // an excluded surface pair
   }
   o.coh[k] = 0.0;
   for (int v = 0; v < 3; v++) {

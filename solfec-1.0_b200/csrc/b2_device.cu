@@ -221,6 +221,12 @@ struct b2dev_ctx {
       cc_bstart, cc_bend, cc_misc, cc_keep;
   // CONTACT_SPARSIFY (dom.c:3107-3109 defaults)
   double sp_threshold = 0.01, sp_minarea = 0.0, sp_mindist = kGeomEps;
+  // CONTACT_EXCLUDE_BODIES / CONTACT_EXCLUDE_SURFACES / UNPHYSICAL_PENETRATION
+  Buf ex_bodies, ex_surf;
+  int n_ex_bodies = 0;
+  std::vector<int> ex_surf_pairs;  // surface pairs (s1, s2), the table built for nsurf
+  int ex_surf_nsurf = -1;
+  double depth = -DBL_MAX;
   bool det_valid = false;       // the scene's contacts are those of the last detection
   bool det_assembled = false;   // ... and the local dynamics was assembled from them
   std::vector<int> ptile_count;  // tiles per problem
@@ -874,7 +880,7 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->det_new, &c->cvx_body, &c->cvx_vptr, &c->cvx_vert, &c->cvx_fptr, &c->cvx_fac, &c->cvx_sptr,
                 &c->cvx_surf, &c->cvx_ns, &c->cvx_cur, &c->cvx_pla, &c->cvx_box, &c->cvx_aptr, &c->cvx_adj,
                 &c->cc_lox, &c->cc_idx, &c->cc_sidx, &c->cc_cnt, &c->cc_off, &c->cc_keys, &c->cc_keys_s,
-                &c->cc_cell, &c->cc_hkey, &c->cc_hkey_s, &c->cc_large, &c->cc_bstart, &c->cc_bend, &c->cc_misc, &c->cc_keep,
+                &c->cc_cell, &c->cc_hkey, &c->cc_hkey_s, &c->cc_large, &c->cc_bstart, &c->cc_bend, &c->cc_misc, &c->cc_keep, &c->ex_bodies, &c->ex_surf,
                 &c->st_area, &c->det_area,
                 &c->topo_m, &c->topo_s, &c->topo_o, &c->topo_flag, &c->blkrow};
   for (Buf* b : all)
@@ -1396,6 +1402,7 @@ static const char* detect_bad_text(int bad) {
   if (bad & 4) return "two sphere centres coincide (no contact normal)";
   if (bad & 32) return "a convex has no finite face plane";
   if (bad & 64) return "a convex pair has more than 32 face planes together (intersection capacity)";
+  if (bad & 128) return "a contact gap is at or below the unphysical penetration depth (the reference stops, dom.c:3792)";
   return "a surface id is out of the material table";
 }
 
@@ -1408,6 +1415,57 @@ static ContactOut staged(b2dev_ctx* c) {
   o.key = ptr<long long>(c->st_key); o.slave_lo = ptr<int>(c->st_slo); o.isnew = ptr<int>(c->st_new);
   o.area = ptr<double>(c->st_area);
   return o;
+}
+
+int b2dev_exclude_bodies(b2dev_ctx* c, int npairs, const int* pairs) {
+  if (!c || npairs < 0 || (npairs > 0 && !pairs)) { set_err("exclude_bodies: invalid arguments"); return B2DEV_EINVAL; }
+  std::vector<long long> keys;
+  for (int k = 0; k < npairs; k++) {
+    const int a = pairs[2 * k], b = pairs[2 * k + 1];
+    if (a < 0 || b < 0 || a >= c->nbod || b >= c->nbod) {
+      set_err("exclude_bodies: pair %d: body out of range", k);
+      return B2DEV_EINVAL;
+    }
+    keys.push_back(((long long)std::min(a, b) << 32) | (long long)std::max(a, b));
+  }
+  std::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  DeviceGuard g(c->device);
+  B2_TRY(upload(c, c->ex_bodies, keys.data(), keys.size(), 0));
+  B2_CK(cudaStreamSynchronize(c->stream));
+  c->n_ex_bodies = (int)keys.size();
+  return B2DEV_OK;
+}
+
+int b2dev_exclude_surfaces(b2dev_ctx* c, int npairs, const int* pairs) {
+  if (!c || npairs < 0 || (npairs > 0 && !pairs)) { set_err("exclude_surfaces: invalid arguments"); return B2DEV_EINVAL; }
+  for (int k = 0; k < 2 * npairs; k++)
+    if (pairs[k] < 0) { set_err("exclude_surfaces: negative surface id"); return B2DEV_EINVAL; }
+  c->ex_surf_pairs.assign(pairs, pairs + 2 * (size_t)npairs);
+  c->ex_surf_nsurf = -1;  // the table is built for the material table's surfaces at the next detection
+  return B2DEV_OK;
+}
+
+int b2dev_unphysical_penetration(b2dev_ctx* c, double depth) {
+  if (!c) { set_err("unphysical_penetration: null context"); return B2DEV_EINVAL; }
+  if (!(depth > 0.0)) { set_err("unphysical_penetration: depth must be positive"); return B2DEV_EINVAL; }
+  c->depth = -depth;  // lng.c:9191
+  return B2DEV_OK;
+}
+
+// the excluded surface pairs as a symmetric nsurf x nsurf table (ids past the
+// material table exclude nothing)
+static int exclusion_table(b2dev_ctx* c) {
+  if (c->ex_surf_pairs.empty() || c->ex_surf_nsurf == c->nsurf) return B2DEV_OK;
+  const int n = c->nsurf;
+  std::vector<unsigned char> t((size_t)n * n, 0);
+  for (size_t k = 0; k + 1 < c->ex_surf_pairs.size(); k += 2) {
+    const int a = c->ex_surf_pairs[k], b = c->ex_surf_pairs[k + 1];
+    if (a < n && b < n) t[(size_t)a * n + b] = t[(size_t)b * n + a] = 1;
+  }
+  B2_TRY(upload(c, c->ex_surf, t.data(), t.size(), 0));
+  c->ex_surf_nsurf = n;
+  return B2DEV_OK;
 }
 
 int b2dev_contact_sparsify(b2dev_ctx* c, double threshold, double minarea, double mindist) {
@@ -1484,6 +1542,13 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
   sd.hkey = ptr<unsigned int>(c->sph_hkey);
   const ConvexDev cvd = convex_view(c);
   int npair = 0, bad = 0;
+  B2_TRY(exclusion_table(c));
+  PairFilter pf;
+  pf.body_pairs = c->n_ex_bodies ? ptr<long long>(c->ex_bodies) : nullptr;
+  pf.n = c->n_ex_bodies;
+  ContactRules cr;
+  cr.nosurf = c->ex_surf_pairs.empty() ? nullptr : ptr<unsigned char>(c->ex_surf);
+  cr.depth = c->depth;
   if (c->nconv > 0) {
     c->launches++;
     k_cvx_update<<<blocks_for(c->nconv, 64), 64, 0, st>>>(cvd, ptr<double>(c->rot), ptr<double>(c->rb_x),
@@ -1507,7 +1572,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     c->launches += 2;
     k_sph_buckets<<<blocks_for(ns, T), T, 0, st>>>(ns, ptr<unsigned int>(c->sph_hkey_s), ptr<int>(c->sph_bstart),
                                                    ptr<int>(c->sph_bend));
-    k_sph_pairs<false><<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<int>(c->obst), ptr<int>(c->sph_sorted),
+    k_sph_pairs<false><<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<int>(c->obst), pf, ptr<int>(c->sph_sorted),
                                                         ptr<int>(c->sph_bstart), ptr<int>(c->sph_bend), M - 1,
                                                         ptr<int>(c->sph_cnt), nullptr, nullptr);
     const int* pair_count = ptr<int>(c->sph_cnt);
@@ -1515,7 +1580,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
       B2_TRY(ensure(c->sph_ccnt, sizeof(int) * (ns + 1)));
       B2_CK(cudaMemsetAsync(c->sph_ccnt.p, 0, sizeof(int) * (ns + 1), st));
       c->launches += 2;
-      k_cvx_pairs<false><<<blocks_for(ns, 128), 128, 0, st>>>(sd, cvd, ptr<int>(c->obst), ptr<int>(c->sph_ccnt),
+      k_cvx_pairs<false><<<blocks_for(ns, 128), 128, 0, st>>>(sd, cvd, ptr<int>(c->obst), pf, ptr<int>(c->sph_ccnt),
                                                                nullptr, nullptr, nullptr);
       k_add_counts<<<blocks_for(ns, T), T, 0, st>>>(ns, ptr<int>(c->sph_cnt), ptr<int>(c->sph_ccnt));
       pair_count = ptr<int>(c->sph_ccnt);
@@ -1593,7 +1658,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     B2_CK(cudaStreamSynchronize(st));
     c->launches += 2;
     k_cc_pairs<false><<<blocks_for(nv, 128), 128, 0, st>>>(
-        cvd, ptr<int>(c->obst), ns, ptr<int>(c->cc_sidx), ptr<int4>(c->cc_cell), ptr<int>(c->cc_bstart),
+        cvd, ptr<int>(c->obst), pf, ns, ptr<int>(c->cc_sidx), ptr<int4>(c->cc_cell), ptr<int>(c->cc_bstart),
         ptr<int>(c->cc_bend), Mc - 1, ptr<int>(c->cc_large), nlarge, ptr<int>(c->cc_cnt), nullptr, nullptr);
     unsigned long long total = 0;
     B2_CK(cudaMemsetAsync(c->sph_total.p, 0, sizeof(unsigned long long), st));
@@ -1615,7 +1680,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
       B2_TRY(ensure(c->cc_keep, nbox + 1));
       c->launches += 2;
       k_cc_pairs<true><<<blocks_for(nv, 128), 128, 0, st>>>(
-          cvd, ptr<int>(c->obst), ns, ptr<int>(c->cc_sidx), ptr<int4>(c->cc_cell), ptr<int>(c->cc_bstart),
+          cvd, ptr<int>(c->obst), pf, ns, ptr<int>(c->cc_sidx), ptr<int4>(c->cc_cell), ptr<int>(c->cc_bstart),
           ptr<int>(c->cc_bend), Mc - 1, ptr<int>(c->cc_large), nlarge, nullptr, ptr<int>(c->cc_off),
           ptr<long long>(c->cc_keys));
       k_cc_gjk<<<blocks_for(nbox, 128), 128, 0, st>>>(nbox, ns, cvd, ptr<long long>(c->cc_keys),
@@ -1673,12 +1738,12 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
   if (npair > 0) {
     if (nps > 0) {
       c->launches += 3;
-      k_sph_pairs<true><<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<int>(c->obst), ptr<int>(c->sph_sorted),
+      k_sph_pairs<true><<<blocks_for(ns, T), T, 0, st>>>(sd, ptr<int>(c->obst), pf, ptr<int>(c->sph_sorted),
                                                          ptr<int>(c->sph_bstart), ptr<int>(c->sph_bend), M - 1,
                                                          nullptr, ptr<int>(c->sph_off), ptr<int>(c->sph_pj));
       if (c->nconv > 0) {  // after the sphere partners (sph_cnt still holds their count)
         c->launches++;
-        k_cvx_pairs<true><<<blocks_for(ns, 128), 128, 0, st>>>(sd, cvd, ptr<int>(c->obst), nullptr,
+        k_cvx_pairs<true><<<blocks_for(ns, 128), 128, 0, st>>>(sd, cvd, ptr<int>(c->obst), pf, nullptr,
                                                                 ptr<int>(c->sph_off), ptr<int>(c->sph_cnt),
                                                                 ptr<int>(c->sph_pj));
       }
@@ -1686,14 +1751,14 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
                                                       ptr<int>(c->sph_pi));
       k_sph_contacts<<<blocks_for(nps, T), T, 0, st>>>(
           nps, sd, cvd, ptr<int>(c->sph_pi), ptr<int>(c->sph_pj), ptr<double>(c->rot), ptr<double>(c->rb_x),
-          ptr<double>(c->x0), c->nsurf, ptr<double>(c->sph_mat), nprev, ptr<long long>(c->sph_pkey),
+          ptr<double>(c->x0), c->nsurf, ptr<double>(c->sph_mat), cr, nprev, ptr<long long>(c->sph_pkey),
           ptr<int>(c->sph_pslo), ptr<double>(c->sph_pR), ptr<double>(c->sph_pU), so, ptr<int>(c->bad));
     }
     if (ncc > 0) {
       c->launches++;
       k_cc_contacts<<<blocks_for(ncc, 64), 64, 0, st>>>(
           ncc, nps, ns, cvd, ptr<long long>(c->cc_keys), ptr<double>(c->rot), ptr<double>(c->rb_x),
-          ptr<double>(c->x0), c->nsurf, ptr<double>(c->sph_mat), nprev, ptr<long long>(c->sph_pkey),
+          ptr<double>(c->x0), c->nsurf, ptr<double>(c->sph_mat), cr, nprev, ptr<long long>(c->sph_pkey),
           ptr<double>(c->sph_pR), ptr<double>(c->sph_pU), so, ptr<int>(c->bad));
     }
     // sparsification neighbourhoods: the contacts of each body

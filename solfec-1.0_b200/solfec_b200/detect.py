@@ -120,6 +120,24 @@ class SPHERES:
         _check(lib().b2dev_contact_sparsify(self.ldy.device_context, float(threshold), float(minarea),
                                             float(mindist)), 'CONTACT_SPARSIFY')
 
+    def exclude_bodies(self, pairs):
+        """CONTACT_EXCLUDE_BODIES for each (body1, body2) of pairs (replaces earlier ones)."""
+        p = np.ascontiguousarray(np.asarray(pairs, dtype=np.int32).reshape(-1, 2))
+        self._ex_bodies = p
+        _check(lib().b2dev_exclude_bodies(self.ldy.device_context, int(p.shape[0]), ptr(p)),
+               'CONTACT_EXCLUDE_BODIES')
+
+    def exclude_surfaces(self, pairs):
+        """CONTACT_EXCLUDE_SURFACES for each (surf1, surf2) of pairs (replaces earlier ones)."""
+        p = np.ascontiguousarray(np.asarray(pairs, dtype=np.int32).reshape(-1, 2))
+        self._ex_surf = p
+        _check(lib().b2dev_exclude_surfaces(self.ldy.device_context, int(p.shape[0]), ptr(p)),
+               'CONTACT_EXCLUDE_SURFACES')
+
+    def unphysical_penetration(self, depth):
+        """UNPHYSICAL_PENETRATION: detection fails on a contact gap at or below -depth."""
+        _check(lib().b2dev_unphysical_penetration(self.ldy.device_context, float(depth)), 'UNPHYSICAL_PENETRATION')
+
     def detect(self):
         """Update and detection of the contacts; returns (contacts, new contacts)."""
         nc, nn = C.c_int(0), C.c_int(0)

@@ -259,3 +259,43 @@ def test_hexahedra_geometry_contacts_equal_reference():
     same_contacts(dev, exp)
     assert dev['key'].shape[0] > 400
     ldy.close()
+
+
+def test_exclusions_and_penetration_depth():
+    """CONTACT_EXCLUDE_BODIES and CONTACT_EXCLUDE_SURFACES on the seeded pile:
+    the contacts are the reference's without the excluded body pairs and
+    without new contacts of the excluded surface pairs; UNPHYSICAL_PENETRATION
+    below the pile's deepest gap fails the detection, above it passes."""
+    from solfec_b200 import DeviceError
+    sc, cv = scenes.convex_pile(seed=1)
+    ref = reference_contacts(1)
+    keys = sorted(ref)
+    body = cv['body']
+    ex_bodies = {tuple(sorted((int(body[i]), int(body[j])))) for (i, j) in keys[::7]}
+    ex_surf = {(1, 4), (2, 2)}
+    excluded = lambda key: (tuple(sorted((int(body[key[0]]), int(body[key[1]])))) in ex_bodies
+                            or tuple(sorted((int(ref[key][5][0]), int(ref[key][5][1])))) in ex_surf)
+    left = [key for key in keys if not excluded(key)]
+    assert 0 < len(left) < len(keys) - len(ex_bodies)
+    bodies = {key: (body[key[1]], body[key[0]]) for key in left}
+    keep = sparsify_keep(left, ref, bodies)
+    expect = [key for key, k in zip(left, keep) if k]
+    J = np.tile(np.eye(3).reshape(9), (sc.nbod, 1))
+    ldy = LOCDYN()
+    ldy.update_begin(bodies_only(sc))
+    RIGID_DYNAMICS(ldy, J, np.ones(sc.nbod), sc.x)
+    det = CONVEXES(ldy, cv, material())
+    det.exclude_bodies(sorted(ex_bodies))
+    det.exclude_surfaces(sorted(ex_surf))
+    det.detect()
+    dev = det.contacts()
+    assert [(int(k >> 32), int(k & 0xFFFFFFFF)) for k in dev['key']] == expect
+    for t, key in enumerate(expect):
+        assert same_bits(dev['point'][t], ref[key][1]) and same_bits(dev['gap'][t], ref[key][3])
+    deepest = -min(ref[k][3] for k in keys)
+    det.unphysical_penetration(1.5 * deepest)
+    det.detect()
+    det.unphysical_penetration(0.5 * deepest)
+    with pytest.raises(DeviceError, match='penetration'):
+        det.detect()
+    ldy.close()

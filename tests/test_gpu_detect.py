@@ -278,3 +278,30 @@ def test_clumps_match_oracle(variant):
     _same(s.contacts(), _oracle(sp, sc.rot, sc.x, sc.x0, sc.obstacle,
                                 dict(key=dev['key'], slave_lo=dev['slave_lo'])))
     ldy.close()
+
+
+def test_excluded_body_pairs_spheres(scene_cache):
+    """CONTACT_EXCLUDE_BODIES on the settled 1000-sphere lattice: the contacts
+    are the oracle's without the excluded body pairs, bit for bit."""
+    sc = scene_cache('spheres_lattice')
+    sp = scenes.sphere_shapes(sc)
+    J, mass = scenes.sphere_inertia(sc)
+    orc = _oracle(sp, sc.rot, sc.x, sc.x0, sc.obstacle)
+    key = orc['key']
+    bi = sp['body'][(key >> 32).astype(np.int64)]
+    j = (key & 0xFFFFFFFF).astype(np.int64)
+    bj = np.where(j < sp['body'].shape[0], sp['body'][np.minimum(j, sp['body'].shape[0] - 1)], -1)
+    pairs = np.stack([bi, bj], axis=1)[::5]
+    pairs = pairs[pairs[:, 1] >= 0]
+    ex = {tuple(sorted(map(int, p))) for p in pairs}
+    keep = np.array([tuple(sorted((int(a), int(b)))) not in ex for a, b in zip(bi, bj)])
+    ldy = LOCDYN()
+    ldy.update_begin(bodies_only(sc))
+    RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    sph = SPHERES(ldy, **sp)
+    sph.exclude_bodies(pairs)
+    sph.detect()
+    dev = sph.contacts()
+    _same(dev, {k: np.asarray(v)[keep] for k, v in orc.items()})
+    assert keep.sum() < keep.shape[0]
+    ldy.close()
