@@ -619,8 +619,12 @@ __device__ __forceinline__ bool cc_candidate(const ConvexDev& cv, const int* obs
 }
 
 // keep[t] = 1 when the convexes of candidate key t are within GEOMETRIC_EPSILON
-// (gjk with the lower convex first, as cvi calls it)
-__global__ void k_cc_gjk(int n, int nsph, ConvexDev cv, const long long* keys, unsigned char* keep) {
+// (gjk with the lower convex first, as cvi calls it); cls[t] = a work class of
+// the pair for the narrow phase: its plane count and how many of its face
+// normals are parallel across the two convexes (aligned boxes make coplanar
+// polar points, turned ones do not), so that a warp takes pairs of one kind
+__global__ void k_cc_gjk(int n, int nsph, ConvexDev cv, const long long* keys, unsigned char* keep,
+                         unsigned int* cls) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const long long key = keys[t];
@@ -628,6 +632,16 @@ __global__ void k_cc_gjk(int n, int nsph, ConvexDev cv, const long long* keys, u
   double p[3], q[3];
   keep[t] = gjk_polytopes(cv.cur + 3 * (size_t)cv.vptr[lo], cv.vptr[lo + 1] - cv.vptr[lo],
                           cv.cur + 3 * (size_t)cv.vptr[hi], cv.vptr[hi + 1] - cv.vptr[hi], p, q) <= kGeomEps;
+  const int na = cv.sptr[lo + 1] - cv.sptr[lo], nb = cv.sptr[hi + 1] - cv.sptr[hi];
+  const double* pa = cv.pla + 6 * (size_t)cv.sptr[lo];
+  const double* pb = cv.pla + 6 * (size_t)cv.sptr[hi];
+  int par = 0;
+  for (int a = 0; a < na; a++)
+    for (int b = 0; b < nb; b++) {
+      const double d = pa[6 * a] * pb[6 * b] + pa[6 * a + 1] * pb[6 * b + 1] + pa[6 * a + 2] * pb[6 * b + 2];
+      par += fabs(d) > 1.0 - 1e-12;
+    }
+  cls[t] = ((unsigned int)(na + nb) << 8) | (unsigned int)(par < 255 ? par : 255);
 }
 
 // per sorted position t (convex i = sorted[t]): its partners j > i of the 27
@@ -678,13 +692,15 @@ __global__ void k_cc_pairs(ConvexDev cv, const int* obst, PairFilter pf, int nsp
 // contact keeps master = slave = -1 and is dropped by the sparsification. Bad
 // flags: 8 a surface id out of the material table, 64 a pair over the
 // intersection's capacity (32 planes of both convexes together).
-__global__ void __launch_bounds__(64) k_cc_contacts(int ncc, int k0, int nsph, ConvexDev cv, const long long* ckey,
+__global__ void __launch_bounds__(64) k_cc_contacts(int ncc, int k0, int nsph, const int* order, ConvexDev cv,
+                                                    const long long* ckey,
                                                     const double* rot, const double* xb, const double* x0, int nsurf,
                                                     const double* mat, ContactRules cr, int nprev,
                                                     const long long* prevkey,
                                                     const double* prevR, const double* prevU, ContactOut o, int* bad) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ncc) return;
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= ncc) return;
+  const int t = order[w];  // pairs run in work-class order, results go to their key-order slots
   const int k = k0 + t;
   const long long key = ckey[t];
   const int c1 = (int)(key >> 32) - nsph, c2 = (int)(key & 0xFFFFFFFFLL) - nsph;

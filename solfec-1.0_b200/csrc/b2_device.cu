@@ -218,7 +218,8 @@ struct b2dev_ctx {
       cvx_aptr, cvx_adj;
   bool cvx_have_adj = false;
   Buf cc_lox, cc_idx, cc_sidx, cc_cnt, cc_off, cc_keys, cc_keys_s, cc_cell, cc_hkey, cc_hkey_s, cc_large,
-      cc_bstart, cc_bend, cc_misc, cc_keep;
+      cc_bstart, cc_bend, cc_misc, cc_keep, cc_cls, cc_order;
+  size_t cc_order_off = 0;  // the work order's offset in cc_order
   // CONTACT_SPARSIFY (dom.c:3107-3109 defaults)
   double sp_threshold = 0.01, sp_minarea = 0.0, sp_mindist = kGeomEps;
   // CONTACT_EXCLUDE_BODIES / CONTACT_EXCLUDE_SURFACES / UNPHYSICAL_PENETRATION
@@ -880,7 +881,7 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->det_new, &c->cvx_body, &c->cvx_vptr, &c->cvx_vert, &c->cvx_fptr, &c->cvx_fac, &c->cvx_sptr,
                 &c->cvx_surf, &c->cvx_ns, &c->cvx_cur, &c->cvx_pla, &c->cvx_box, &c->cvx_aptr, &c->cvx_adj,
                 &c->cc_lox, &c->cc_idx, &c->cc_sidx, &c->cc_cnt, &c->cc_off, &c->cc_keys, &c->cc_keys_s,
-                &c->cc_cell, &c->cc_hkey, &c->cc_hkey_s, &c->cc_large, &c->cc_bstart, &c->cc_bend, &c->cc_misc, &c->cc_keep, &c->ex_bodies, &c->ex_surf,
+                &c->cc_cell, &c->cc_hkey, &c->cc_hkey_s, &c->cc_large, &c->cc_bstart, &c->cc_bend, &c->cc_misc, &c->cc_keep, &c->cc_cls, &c->cc_order, &c->ex_bodies, &c->ex_surf,
                 &c->st_area, &c->det_area,
                 &c->topo_m, &c->topo_s, &c->topo_o, &c->topo_flag, &c->blkrow};
   for (Buf* b : all)
@@ -1683,9 +1684,15 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
           cvd, ptr<int>(c->obst), pf, ns, ptr<int>(c->cc_sidx), ptr<int4>(c->cc_cell), ptr<int>(c->cc_bstart),
           ptr<int>(c->cc_bend), Mc - 1, ptr<int>(c->cc_large), nlarge, nullptr, ptr<int>(c->cc_off),
           ptr<long long>(c->cc_keys));
+      B2_TRY(ensure(c->cc_cls, sizeof(unsigned int) * 2 * (nbox + 1)));
+      B2_TRY(ensure(c->cc_order, sizeof(int) * 2 * (nbox + 1)));
+      unsigned int* cls = ptr<unsigned int>(c->cc_cls);
+      unsigned int* cls_s = cls + (nbox + 1);
+      int* iota = ptr<int>(c->cc_order);
+      int* order = iota + (nbox + 1);
       k_cc_gjk<<<blocks_for(nbox, 128), 128, 0, st>>>(nbox, ns, cvd, ptr<long long>(c->cc_keys),
-                                                      ptr<unsigned char>(c->cc_keep));
-      // the touching pairs, then sorted by key
+                                                      ptr<unsigned char>(c->cc_keep), cls);
+      // the touching pairs with their work classes, then sorted by key
       int* nsel = reinterpret_cast<int*>(ptr<unsigned long long>(c->cc_misc) + 3);
       bytes = 0;
       B2_CK(cub::DeviceSelect::Flagged(nullptr, bytes, ptr<long long>(c->cc_keys), ptr<unsigned char>(c->cc_keep),
@@ -1694,16 +1701,29 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
       B2_CK(cub::DeviceSelect::Flagged(c->cub_tmp.p, bytes, ptr<long long>(c->cc_keys),
                                        ptr<unsigned char>(c->cc_keep), ptr<long long>(c->cc_keys_s), nsel, nbox,
                                        st));
+      bytes = 0;
+      B2_CK(cub::DeviceSelect::Flagged(nullptr, bytes, cls, ptr<unsigned char>(c->cc_keep), cls_s, nsel, nbox, st));
+      B2_TRY(ensure(c->cub_tmp, bytes));
+      B2_CK(cub::DeviceSelect::Flagged(c->cub_tmp.p, bytes, cls, ptr<unsigned char>(c->cc_keep), cls_s, nsel, nbox,
+                                       st));
       B2_CK(cudaMemcpyAsync(&ncc, nsel, sizeof(int), cudaMemcpyDeviceToHost, st));
       B2_CK(cudaStreamSynchronize(st));
       if (ncc > 0) {
         bytes = 0;
-        B2_CK(cub::DeviceRadixSort::SortKeys(nullptr, bytes, ptr<unsigned long long>(c->cc_keys_s),
-                                             ptr<unsigned long long>(c->cc_keys), ncc, 0, 64, st));
+        B2_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, ptr<unsigned long long>(c->cc_keys_s),
+                                              ptr<unsigned long long>(c->cc_keys), cls_s, cls, ncc, 0, 64, st));
         B2_TRY(ensure(c->cub_tmp, bytes));
-        B2_CK(cub::DeviceRadixSort::SortKeys(c->cub_tmp.p, bytes, ptr<unsigned long long>(c->cc_keys_s),
-                                             ptr<unsigned long long>(c->cc_keys), ncc, 0, 64, st));
+        B2_CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, bytes, ptr<unsigned long long>(c->cc_keys_s),
+                                              ptr<unsigned long long>(c->cc_keys), cls_s, cls, ncc, 0, 64, st));
+        // work order: the key-order positions sorted (stably) by class
+        c->launches++;
+        k_iota<<<blocks_for(ncc, T), T, 0, st>>>(ncc, iota);
+        bytes = 0;
+        B2_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, cls, cls_s, iota, order, ncc, 0, 32, st));
+        B2_TRY(ensure(c->cub_tmp, bytes));
+        B2_CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, bytes, cls, cls_s, iota, order, ncc, 0, 32, st));
       }
+      c->cc_order_off = (size_t)nbox + 1;
     }
   }
   npair = nps + ncc;
@@ -1757,7 +1777,8 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
     if (ncc > 0) {
       c->launches++;
       k_cc_contacts<<<blocks_for(ncc, 64), 64, 0, st>>>(
-          ncc, nps, ns, cvd, ptr<long long>(c->cc_keys), ptr<double>(c->rot), ptr<double>(c->rb_x),
+          ncc, nps, ns, ptr<int>(c->cc_order) + c->cc_order_off, cvd, ptr<long long>(c->cc_keys),
+          ptr<double>(c->rot), ptr<double>(c->rb_x),
           ptr<double>(c->x0), c->nsurf, ptr<double>(c->sph_mat), cr, nprev, ptr<long long>(c->sph_pkey),
           ptr<double>(c->sph_pR), ptr<double>(c->sph_pU), so, ptr<int>(c->bad));
     }
