@@ -620,9 +620,11 @@ __device__ __forceinline__ bool cc_candidate(const ConvexDev& cv, const int* obs
 
 // keep[t] = 1 when the convexes of candidate key t are within GEOMETRIC_EPSILON
 // (gjk with the lower convex first, as cvi calls it); cls[t] = a work class of
-// the pair for the narrow phase: its plane count and how many of its face
-// normals are parallel across the two convexes (aligned boxes make coplanar
-// polar points, turned ones do not), so that a warp takes pairs of one kind
+// the pair for the narrow phase: its plane count, how many of its face normals
+// are parallel across the two convexes (aligned boxes make coplanar polar
+// points, turned ones do not), along how many axes the two are offset (face,
+// edge or corner neighbours) and whether they are apart or overlap, so that a
+// warp takes pairs of one kind
 __global__ void k_cc_gjk(int n, int nsph, ConvexDev cv, const long long* keys, unsigned char* keep,
                          unsigned int* cls) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -630,8 +632,16 @@ __global__ void k_cc_gjk(int n, int nsph, ConvexDev cv, const long long* keys, u
   const long long key = keys[t];
   const int lo = (int)(key >> 32) - nsph, hi = (int)(key & 0xFFFFFFFFLL) - nsph;
   double p[3], q[3];
-  keep[t] = gjk_polytopes(cv.cur + 3 * (size_t)cv.vptr[lo], cv.vptr[lo + 1] - cv.vptr[lo],
-                          cv.cur + 3 * (size_t)cv.vptr[hi], cv.vptr[hi + 1] - cv.vptr[hi], p, q) <= kGeomEps;
+  const double dist = gjk_polytopes(cv.cur + 3 * (size_t)cv.vptr[lo], cv.vptr[lo + 1] - cv.vptr[lo],
+                                    cv.cur + 3 * (size_t)cv.vptr[hi], cv.vptr[hi + 1] - cv.vptr[hi], p, q);
+  keep[t] = dist <= kGeomEps;
+  const double* ba = cv.box + 6 * lo;
+  const double* bb = cv.box + 6 * hi;
+  int sep = 0;  // axes along which the boxes' centres are further apart than a quarter of their summed sides
+  for (int k = 0; k < 3; k++) {
+    const double da = ba[3 + k] - ba[k], db = bb[3 + k] - bb[k];
+    sep += fabs((ba[k] + ba[3 + k]) - (bb[k] + bb[3 + k])) > 0.5 * (da + db);
+  }
   const int na = cv.sptr[lo + 1] - cv.sptr[lo], nb = cv.sptr[hi + 1] - cv.sptr[hi];
   const double* pa = cv.pla + 6 * (size_t)cv.sptr[lo];
   const double* pb = cv.pla + 6 * (size_t)cv.sptr[hi];
@@ -641,7 +651,8 @@ __global__ void k_cc_gjk(int n, int nsph, ConvexDev cv, const long long* keys, u
       const double d = pa[6 * a] * pb[6 * b] + pa[6 * a + 1] * pb[6 * b + 1] + pa[6 * a + 2] * pb[6 * b + 2];
       par += fabs(d) > 1.0 - 1e-12;
     }
-  cls[t] = ((unsigned int)(na + nb) << 8) | (unsigned int)(par < 255 ? par : 255);
+  cls[t] = ((unsigned int)(na + nb) << 16) | ((unsigned int)(par < 255 ? par : 255) << 8) | ((unsigned int)sep << 1) |
+           (unsigned int)(dist > 0.0);
 }
 
 // per sorted position t (convex i = sorted[t]): its partners j > i of the 27
