@@ -205,6 +205,18 @@ int b2dev_upload_locdyn(b2dev_ctx* ctx, int n, const double* W, const double* A,
                         const double* Woff, double free_energy, double step, int dynamic, uint64_t colour_seed,
                         int on_device);
 
+/* Constraint kinds of the current problem's rows (caller order), as dom.h:98
+ * numbers them: 0 CONTACT, 1 FIXPNT, 2 FIXDIR, 3 VELODIR, 4 VELODIR3, 5 RIGLNK
+ * (SPRING, whose force comes from a Python callback, is not supported). The
+ * solve treats them as DIAGONAL_BLOCK_Solver (dbs.c:328-550) and
+ * MERIT_Function (mrf.c:88-137) do. Z[4 i ..] per row: VELODIR the prescribed
+ * normal velocity Z[0]; VELODIR3 the prescribed velocity Z[0..2]; RIGLNK the
+ * link vector in the row's local frame (base^T Z, as riglnk computes it) in
+ * Z[0..2] and the link length in Z[3]; the row's gap is RIGLNK's merit gap. n
+ * must be the problem's row count; kind NULL makes every row a contact again.
+ * Uploading a scene or local dynamics, or a detection, resets the kinds. */
+int b2dev_set_kinds(b2dev_ctx* ctx, int n, const int* kind, const double* Z, int on_device);
+
 /* Reactions and relative velocities (3 per row, caller order): initial
  * values before a solve, results after it. conmerit (may be NULL) receives
  * the per-constraint merit of the last merit evaluation. */

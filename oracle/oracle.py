@@ -161,10 +161,13 @@ def colour_order(col):
 
 
 def solve(ld: LocalDynamics, R=None, U=None, epsilon=1e-4, maxiter=1000, meritval=1.0, failure='CONTINUE',
-          diagepsilon=None, diagmaxiter=None, diagsolver='SEMISMOOTH_NEWTON', reverse=False, impl='oracle'):
+          diagepsilon=None, diagmaxiter=None, diagsolver='SEMISMOOTH_NEWTON', reverse=False, impl='oracle',
+          kinds=None, Z=None):
     """Run the restated (impl='oracle') or the compiled reference
     (impl='ref') Gauss-Seidel solve on ld in list order. Defaults of
-    diagepsilon / diagmaxiter follow lng.c:4335-4342."""
+    diagepsilon / diagmaxiter follow lng.c:4335-4342. kinds: None (all
+    contacts) or a constraint kind per row (dom.h:98), with Z[n][4] (VELODIR
+    value, VELODIR3 values, RIGLNK local link vector and length)."""
     if diagepsilon is None:
         diagepsilon = max(2.220446049250313e-16, 0.01 * min(epsilon, min(meritval, 1e-4)))
     if diagmaxiter is None:
@@ -180,16 +183,32 @@ def solve(ld: LocalDynamics, R=None, U=None, epsilon=1e-4, maxiter=1000, meritva
     merit = C.c_double(0.0)
     adjcol = ld.adjcol if ld.nblocks else np.zeros(1, np.int32)
     Woff = ld.Woff if ld.nblocks else np.zeros(9)
-    thrown = fn(n, ld.adjptr, adjcol, Woff, ld.W if n else np.zeros(9), ld.A if n else np.zeros(9),
+    setk = lib.orc_gs_set_kinds if impl == 'oracle' else lib.ref_gs_set_kinds
+    setk.restype = None
+    setk.argtypes = [C.c_void_p, C.c_void_p]
+    if kinds is not None:
+        kinds = np.ascontiguousarray(kinds, dtype=np.int32)
+        Zk = np.ascontiguousarray(np.zeros((n, 4)) if Z is None else Z, dtype=np.float64).reshape(n, 4)
+        setk(kinds.ctypes.data, Zk.ctypes.data)
+    try:
+        thrown = _gs_call(fn, n, ld, adjcol, Woff, R, U, conmerit, epsilon, maxiter, meritval, failure, diagepsilon,
+                          diagmaxiter, diagsolver, reverse, iters, err, merit, rer, mer, ncb)
+    finally:
+        setk(None, None)
+    k = iters.value
+    return dict(R=R, U=U, conmerit=conmerit[:n], iters=k, error=err.value, merit=merit.value,
+                rerhist=rer[:k].copy(), merhist=mer[:k].copy(), thrown=thrown, ncallbacks=ncb.value)
+
+
+def _gs_call(fn, n, ld, adjcol, Woff, R, U, conmerit, epsilon, maxiter, meritval, failure, diagepsilon, diagmaxiter,
+             diagsolver, reverse, iters, err, merit, rer, mer, ncb):
+    return fn(n, ld.adjptr, adjcol, Woff, ld.W if n else np.zeros(9), ld.A if n else np.zeros(9),
                 ld.rho if n else np.zeros(1), ld.B if n else np.zeros(3), ld.V if n else np.zeros(3),
                 ld.gap if n else np.zeros(1), ld.friction if n else np.zeros(1),
                 ld.restitution if n else np.zeros(1), ld.cohesion if n else np.zeros(1),
                 R if n else np.zeros(3), U if n else np.zeros(3), conmerit, ld.free_energy, ld.dynamic, ld.step,
                 epsilon, maxiter, meritval, FAIL[failure], diagepsilon, diagmaxiter, DS[diagsolver], int(reverse),
                 C.byref(iters), C.byref(err), C.byref(merit), rer, mer, C.byref(ncb))
-    k = iters.value
-    return dict(R=R, U=U, conmerit=conmerit[:n], iters=k, error=err.value, merit=merit.value,
-                rerhist=rer[:k].copy(), merhist=mer[:k].copy(), thrown=thrown, ncallbacks=ncb.value)
 
 
 def merit(ld: LocalDynamics, R):

@@ -394,6 +394,90 @@ static int projected_newton (double epsilon, int maxiter, int dynamic, double st
   return iter;
 }
 
+/* ---- bilateral constraints (dbs.c:328-450, mrf.c:88-137), kinds as dom.h:98:
+ * 1 FIXPNT, 2 FIXDIR, 3 VELODIR, 4 VELODIR3, 5 RIGLNK; Z[4] per row: VELODIR
+ * Z[0], VELODIR3 Z[0..2], RIGLNK the local link vector (base^T Z) and length */
+static const int *g_kind = NULL;
+static const double *g_Z = NULL;
+
+void orc_gs_set_kinds (const int *kind, const double *Z)
+{
+  g_kind = kind;
+  g_Z = Z;
+}
+
+static int orc_bilateral (int kind, const double *Z, int dynamic, double step, double epsilon, int maxiter,
+                          const double *W, const double *B, const double *V, double *U, double *R)
+{
+  double A[9];
+  switch (kind)
+  {
+  case 1: /* fixpnt, dbs.c:328-350 */
+    for (int q = 0; q < 9; q ++) A[q] = W[q];
+    for (int q = 0; q < 3; q ++) U[q] = dynamic ? V[q] * -1.0 : 0.0;
+    for (int q = 0; q < 3; q ++) R[q] = U[q] - B[q];
+    return orc_dposv (3, A, R) ? -1 : 0;
+  case 2: /* fixdir, dbs.c:352-369 */
+  case 3: /* velodir, dbs.c:371-379 */
+    R[0] = 0.0;
+    R[1] = 0.0;
+    if (kind == 3) R[2] = (Z[0] - B[2]) / W[8];
+    else R[2] = dynamic ? -(V[2] + B[2]) / W[8] : -B[2] / W[8];
+    for (int q = 0; q < 3; q ++) U[q] = B[q] + R[2] * W[6+q];
+    return 0;
+  case 4: /* velodir3, dbs.c:381-394 */
+    for (int q = 0; q < 9; q ++) A[q] = W[q];
+    for (int q = 0; q < 3; q ++) U[q] = Z[q];
+    for (int q = 0; q < 3; q ++) R[q] = U[q] - B[q];
+    return orc_dposv (3, A, R) ? -1 : 0;
+  case 5: /* riglnk, dbs.c:396-450 */
+  {
+    double h = dynamic ? 0.5 * step : step, len = Z[3], l = 0.0, error, X[2], C[3], D[4], L[4];
+    int ipiv[2], iter = 0;
+    R[0] = R[1] = 0.0;
+    do
+    {
+      for (int q = 0; q < 3; q ++) C[q] = B[q] + R[2] * W[6+q];
+      for (int q = 0; q < 3; q ++) D[q] = Z[q] + h * C[q];
+      X[1] = dot3 (D, D) - len*len;
+      D[3] = dot3 (W+6, D) * 2.0 * h;
+      X[0] = W[8]*R[2] + l*D[3];
+      L[0] = W[8]; L[2] = D[3];
+      L[1] = D[3]; L[3] = 0.0;
+      if (orc_dgesv (2, L, ipiv, X)) return -1;
+      R[2] -= X[0];
+      l -= X[1];
+      error = sqrt ((X[0]*X[0] + X[1]*X[1])/(R[2]*R[2] + l*l));
+    } while (error > epsilon && ++iter < maxiter);
+    if (dynamic && iter >= maxiter) { R[2] = -B[2] / W[8]; iter = 0; }
+    for (int q = 0; q < 3; q ++) U[q] = B[q] + R[2] * W[6+q];
+    return iter;
+  }
+  }
+  return -1;
+}
+
+static double orc_bilateral_merit (int kind, const double *Z, double gap, int dynamic, double step,
+                                   const double *A, const double *V, const double *U)
+{
+  double P[3], Q[3];
+  switch (kind)
+  {
+  case 1: case 4: /* FIXPNT, VELODIR3 */
+    for (int q = 0; q < 3; q ++) P[q] = kind == 1 ? (dynamic ? U[q] + V[q] : U[q]) : Z[q] - U[q];
+    Q[0] = A[0]*P[0] + A[3]*P[1] + A[6]*P[2];
+    Q[1] = A[1]*P[0] + A[4]*P[1] + A[7]*P[2];
+    Q[2] = A[2]*P[0] + A[5]*P[1] + A[8]*P[2];
+    return dot3 (Q, P);
+  case 2: P[2] = dynamic ? U[2] + V[2] : U[2]; break;
+  case 3: P[2] = Z[0] - U[2]; break;
+  case 5: P[2] = gap/(step * (dynamic ? 0.5 : 1.0)) + U[2]; break;
+  default: return 0.0;
+  }
+  Q[2] = A[8] * P[2];
+  return Q[2] * P[2];
+}
+
 int orc_diagonal_solve (int diagsolver, double diagepsilon, int diagmaxiter, int dynamic, double step,
                         double friction, double restitution, double cohesion, double gap, double rho,
                         const double *W, const double *B, const double *V, double *U, double *R)
@@ -422,12 +506,17 @@ double orc_merit (int n, const int *adjptr, const int *adjcol, const double *Wof
     nvaddmul (B + 3*i, W + 9*i, R + 3*i, Ui);
     for (int k = adjptr[i]; k < adjptr[i+1]; k ++)
       nvaddmul (Ui, Woff + 9*(size_t)k, R + 3*adjcol[k], Ui);
-    scf_linearize (dynamic, step, friction[i], restitution[i], cohesion[i], gap[i], V + 3*i, Ui, R + 3*i, P, NULL, NULL);
-    const double *Ai = A + 9*i; /* NVMUL (A, P, Q) */
-    Q[0] = Ai[0]*P[0] + Ai[3]*P[1] + Ai[6]*P[2];
-    Q[1] = Ai[1]*P[0] + Ai[4]*P[1] + Ai[7]*P[2];
-    Q[2] = Ai[2]*P[0] + Ai[5]*P[1] + Ai[8]*P[2];
-    up = dot3 (Q, P);
+    if (g_kind && g_kind[i])
+      up = orc_bilateral_merit (g_kind[i], g_Z + 4*i, gap[i], dynamic, step, A + 9*i, V + 3*i, Ui);
+    else
+    {
+      scf_linearize (dynamic, step, friction[i], restitution[i], cohesion[i], gap[i], V + 3*i, Ui, R + 3*i, P, NULL, NULL);
+      const double *Ai = A + 9*i; /* NVMUL (A, P, Q) */
+      Q[0] = Ai[0]*P[0] + Ai[3]*P[1] + Ai[6]*P[2];
+      Q[1] = Ai[1]*P[0] + Ai[4]*P[1] + Ai[7]*P[2];
+      Q[2] = Ai[2]*P[0] + Ai[5]*P[1] + Ai[8]*P[2];
+      up = dot3 (Q, P);
+    }
     if (conmerit) conmerit[i] = up;
     sum += up;
   }
@@ -470,13 +559,22 @@ int orc_gs_solve (int n, const int *adjptr, const int *adjcol, const double *Wof
 
       R0[0] = Ri[0]; R0[1] = Ri[1]; R0[2] = Ri[2];
 
-      diagiters = orc_diagonal_solve (diagsolver, diagepsilon, diagmaxiter, dynamic, step, friction[i],
-                    restitution[i], cohesion[i], gap[i], rho[i], W + 9*i, Bp, V + 3*i, Ui, Ri);
+      int kind = g_kind ? g_kind[i] : 0;
+      if (kind)
+        diagiters = orc_bilateral (kind, g_Z + 4*i, dynamic, step, diagepsilon, diagmaxiter, W + 9*i, Bp, V + 3*i,
+                                   Ui, Ri);
+      else
+        diagiters = orc_diagonal_solve (diagsolver, diagepsilon, diagmaxiter, dynamic, step, friction[i],
+                      restitution[i], cohesion[i], gap[i], rho[i], W + 9*i, Bp, V + 3*i, Ui, Ri);
 
       if (diagiters >= diagmaxiter || diagiters < 0) /* bgs.c:971-1013 */
       {
         gserror = diagiters < 0 ? GS_DIAGONAL_FAILED : GS_DIAGONAL_DIVERGED;
-        if (failure == FAIL_CONTINUE)
+        if (failure == FAIL_CONTINUE && kind) /* no fallback chain outside contacts */
+        {
+          Ri[0] = R0[0]; Ri[1] = R0[1]; Ri[2] = R0[2];
+        }
+        else if (failure == FAIL_CONTINUE)
         {
           static const int chain[4] = {DS_SSN, DS_PG, DS_DSF, DS_PN};
           for (int t = 0; t < 4; t ++)

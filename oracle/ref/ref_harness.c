@@ -25,6 +25,18 @@
 static int ncallbacks_seen;
 static void count_callback (void *data) { (void)data; ncallbacks_seen ++; }
 
+/* constraint kinds (dom.h:98) and Z[4] per row for the next ref_gs_solve
+ * (NULL: every row a contact); each row's base is the identity, so riglnk's
+ * base^T Z is Z itself */
+static const int *g_kind = NULL;
+static const double *g_Z = NULL;
+
+void ref_gs_set_kinds (const int *kind, const double *Z)
+{
+  g_kind = kind;
+  g_Z = Z;
+}
+
 int ref_gs_solve (int n, const int *adjptr, const int *adjcol, const double *Woff,
                   const double *W, const double *A, const double *rho, const double *B, const double *V,
                   const double *gap, const double *friction, const double *restitution, const double *cohesion,
@@ -70,6 +82,12 @@ int ref_gs_solve (int n, const int *adjptr, const int *adjcol, const double *Wof
     c->gap = gap[i];
     c->area = 1.0;
     c->kind = CONTACT;
+    if (g_kind && g_kind[i])
+    {
+      c->kind = g_kind[i];
+      for (int q = 0; q < 4; q ++) c->Z[q] = g_Z[4*i + q];
+      for (int q = 0; q < 9; q ++) c->base[q] = (q % 4 == 0) ? 1.0 : 0.0;
+    }
     mat[i].model = SIGNORINI_COULOMB;
     mat[i].friction = friction[i];
     mat[i].restitution = restitution[i];

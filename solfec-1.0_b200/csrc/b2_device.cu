@@ -152,6 +152,10 @@ struct b2dev_ctx {
   int nbod = 0, ncon = 0;
   Buf rot, x0, jinv, minv, velo, velo0, obst, master, slave, mpnt, spnt, base;
   Buf gap_c, fric_c, rest_c, coh_c;
+  // constraint kinds of the rows (b2dev_set_kinds): caller order, and the
+  // colour-sorted planes the KINDS solve kernels read; none = all CONTACT
+  Buf kind_c, Z_c, kind_s, Z_s;
+  bool has_kinds = false;
   bool have_scene = false;
 
   // caller-order row data and graph
@@ -385,6 +389,29 @@ int build_tiles(b2dev_ctx* c, int rows) {
 // layout; row data must already sit in the caller-order buffers.
 // same_graph: the caller knows the contact graph is that of the last layout
 // (an unchanged contact topology), so the comparison pass is skipped.
+// kind and Z of every row into the colour-sorted planes (kind_s[p], Z_s[q n + p])
+__global__ void k_kinds_permute(int n, const int* perm, const int* kind_c, const double* Z_c, int* kind_s,
+                                double* Z_s) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int i = perm[p];
+  kind_s[p] = kind_c[i];
+  for (int q = 0; q < 4; q++) Z_s[(size_t)q * n + p] = Z_c[4 * (size_t)i + q];
+}
+
+static int permute_kinds(b2dev_ctx* c) {
+  const int n = c->n;
+  B2_TRY(ensure(c->kind_s, sizeof(int) * (n + 1)));
+  B2_TRY(ensure(c->Z_s, sizeof(double) * 4 * (n + 1)));
+  if (n == 0) return B2DEV_OK;
+  c->launches++;
+  k_kinds_permute<<<blocks_for(n, 256), 256, 0, c->stream>>>(n, ptr<int>(c->perm), ptr<int>(c->kind_c),
+                                                             ptr<double>(c->Z_c), ptr<int>(c->kind_s),
+                                                             ptr<double>(c->Z_s));
+  B2_CK(cudaGetLastError());
+  return B2DEV_OK;
+}
+
 int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled, bool same_graph) {
   const int n = c->n;
   cudaStream_t st = c->stream;
@@ -535,6 +562,7 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled, bool same_graph)
       ptr<double>(c->coh_c), ptr<double>(c->Wd), ptr<double>(c->Ad), ptr<double>(c->Bv), ptr<double>(c->Vv),
       ptr<double>(c->rho), ptr<double>(c->gap), ptr<double>(c->fric), ptr<double>(c->rest), ptr<double>(c->coh));
 
+  if (c->has_kinds) B2_TRY(permute_kinds(c));
   for (int b = 0; b < 3; b++) {
     B2_TRY(ensure(c->R64[b], sizeof(double4) * (n + 1)));
     B2_TRY(ensure(c->R32[b], sizeof(float4) * (n + 1)));
@@ -620,7 +648,8 @@ int solve_setup(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter
                 int u0_from_merit, int grid_req, SolveArgs* a, int* grid, size_t* smem) {
   const int n = c->n;
   const int P = c->nprob;
-  const void* fn = mixed ? (const void*)k_solve_fp32 : (const void*)k_solve<false>;
+  const void* fn = c->has_kinds ? (mixed ? (const void*)k_solve_fp32_kinds : (const void*)k_solve_kinds<false>)
+                                 : (mixed ? (const void*)k_solve_fp32 : (const void*)k_solve<false>);
   // enough warps for the tiles of about two sweeps in flight, capped by residency
   const int want = grid_req > 0 ? grid_req : blocks_for(2LL * c->ntiles, kSolveWarps);
   // staging window: the largest tile if the shared memory of the blocks that
@@ -678,6 +707,8 @@ int solve_setup(b2dev_ctx* c, bool mixed, const b2dev_solve_opts* o, int maxiter
   A.Vv = ptr<double>(c->Vv);
   A.rho = ptr<double>(c->rho);
   A.gap = ptr<double>(c->gap);
+  A.kind = c->has_kinds ? ptr<int>(c->kind_s) : nullptr;
+  A.Zv = c->has_kinds ? ptr<double>(c->Z_s) : nullptr;
   A.fric = ptr<double>(c->fric);
   A.rest = ptr<double>(c->rest);
   A.coh = ptr<double>(c->coh);
@@ -742,7 +773,8 @@ int solve_enqueue(b2dev_ctx* c, bool mixed, const SolveArgs& a, int grid, size_t
     B2_CK(cudaMemsetAsync(ptr<unsigned>(c->failcount) + a.iter0, 0, sizeof(unsigned) * (a.pstride - a.iter0), st));
   }
   if (a.trace) B2_CK(cudaMemsetAsync(a.trace, 0, sizeof(double) * kTraceStride * (n + 1), st));
-  const void* fn = mixed ? (const void*)k_solve_fp32 : (const void*)k_solve<false>;
+  const void* fn = c->has_kinds ? (mixed ? (const void*)k_solve_fp32_kinds : (const void*)k_solve_kinds<false>)
+                                 : (mixed ? (const void*)k_solve_fp32 : (const void*)k_solve<false>);
   SolveArgs arg = a;
   void* args[] = {&arg};
   cudaLaunchConfig_t cfg;
@@ -861,7 +893,8 @@ void b2dev_destroy(b2dev_ctx* c) {
   DeviceGuard g(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   Buf* all[] = {&c->rot, &c->x0, &c->jinv, &c->minv, &c->velo, &c->velo0, &c->obst, &c->master, &c->slave,
-                &c->mpnt, &c->spnt, &c->base, &c->gap_c, &c->fric_c, &c->rest_c, &c->coh_c, &c->factors, &c->Wii,
+                &c->mpnt, &c->spnt, &c->base, &c->gap_c, &c->fric_c, &c->rest_c, &c->coh_c, &c->kind_c, &c->Z_c,
+                &c->kind_s, &c->Z_s, &c->factors, &c->Wii,
                 &c->Aii, &c->rho_c, &c->B_c, &c->V_c, &c->fe_part, &c->fe_dev, &c->bad, &c->bdeg, &c->bptr,
                 &c->cursor, &c->brow, &c->deg, &c->adjptr, &c->adjcol, &c->adjbod, &c->Woff_c, &c->colour, &c->sel,
                 &c->cctrl, &c->keys_out, &c->iota, &c->perm, &c->iperm, &c->colptr, &c->sdeg, &c->rowptr, &c->col,
@@ -925,6 +958,38 @@ int b2dev_upload_scene(b2dev_ctx* c, int nbod, const double* rot, const double* 
   c->have_rigid = false;  // b2dev_rigid_setup again for the new bodies
   c->det_valid = c->det_assembled = false;
   c->ready = false;
+  c->has_kinds = false;   // new constraints: all contacts until b2dev_set_kinds
+  return B2DEV_OK;
+}
+
+int b2dev_set_kinds(b2dev_ctx* c, int n, const int* kind, const double* Z, int on_device) {
+  if (!c) { set_err("set_kinds: null context"); return B2DEV_EINVAL; }
+  const int rows = c->ready ? c->n : c->ncon;
+  if (n != rows) { set_err("set_kinds: %d rows given, the problem has %d", n, rows); return B2DEV_EINVAL; }
+  DeviceGuard g(c->device);
+  if (!kind) { c->has_kinds = false; return B2DEV_OK; }
+  std::vector<int> k(n);
+  std::vector<double> z(4 * (size_t)n, 0.0);
+  if (on_device) {
+    if (n) B2_CK(cudaMemcpy(k.data(), kind, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    if (n && Z) B2_CK(cudaMemcpy(z.data(), Z, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost));
+  } else {
+    std::copy(kind, kind + n, k.begin());
+    if (Z) std::copy(Z, Z + 4 * (size_t)n, z.begin());
+  }
+  bool any = false;
+  for (int i = 0; i < n; i++) {
+    if (k[i] < CON_CONTACT || k[i] > CON_RIGLNK) {
+      set_err("set_kinds: row %d: kind %d is not CONTACT, FIXPNT, FIXDIR, VELODIR, VELODIR3 or RIGLNK (0-5)", i, k[i]);
+      return B2DEV_EUNSUPPORTED;
+    }
+    any = any || k[i] != CON_CONTACT;
+  }
+  B2_TRY(upload(c, c->kind_c, k.data(), (size_t)n, 0));
+  B2_TRY(upload(c, c->Z_c, z.data(), z.size(), 0));
+  c->has_kinds = any;
+  if (any && c->ready) B2_TRY(permute_kinds(c));
+  B2_CK(cudaStreamSynchronize(c->stream));
   return B2DEV_OK;
 }
 
@@ -1086,6 +1151,7 @@ int b2dev_upload_locdyn(b2dev_ctx* c, int n, const double* W, const double* A, c
   c->step = step;
   c->dynamic = dynamic ? 1 : 0;
   c->free_energy = free_energy;
+  c->has_kinds = false;  // new rows: all contacts until b2dev_set_kinds
   B2_TRY(ensure(c->pfe, sizeof(double) * 2));
   B2_CK(cudaMemcpyAsync(c->pfe.p, &c->free_energy, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   c->assembled_mode = false;
@@ -1858,6 +1924,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
   B2_CK(cudaGetLastError());
   B2_CK(cudaStreamSynchronize(st));
   c->ncon = nkeep;
+  c->has_kinds = false;
   c->det_valid = true;
   c->det_assembled = false;
   c->ready = false;  // the local dynamics must be assembled for the new contacts

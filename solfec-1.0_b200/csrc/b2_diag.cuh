@@ -450,4 +450,175 @@ __device__ __forceinline__ double merit_row(const ContactParams& cp, const doubl
   return Q0 * P[0] + Q1 * P[1] + Q2 * P[2];
 }
 
+// ---- bilateral constraints (dbs.c:328-450, mrf.c:88-137) ----
+//
+// Constraint kinds as dom.h:98 numbers them. A row of a kind other than
+// CONTACT carries Z[4]: VELODIR the prescribed normal velocity Z[0]; VELODIR3
+// the prescribed velocity Z[0..2]; RIGLNK the link vector in the row's local
+// frame (base^T Z of riglnk, dbs.c:412) in Z[0..2] and the link length Z[3].
+enum { CON_CONTACT = 0, CON_FIXPNT = 1, CON_FIXDIR = 2, CON_VELODIR = 3, CON_VELODIR3 = 4, CON_RIGLNK = 5 };
+
+// A x = b for a symmetric positive definite 3x3 A (column-major, upper
+// triangle read), Cholesky A = U^T U in the order of the 3x3 dposv the
+// reference is linked with here (oracle/lu_small.c): 0, or j + 1 for a
+// non-positive or NaN pivot
+__device__ __forceinline__ int chol3_solve(double* a, double* b) {
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    double s = a[j + 3 * j];
+    for (int k = 0; k < j; k++) s -= a[k + 3 * j] * a[k + 3 * j];
+    if (s <= 0.0 || isnan(s)) return j + 1;
+    s = sqrt(s);
+    a[j + 3 * j] = s;
+    for (int c = j + 1; c < 3; c++) {
+      double t = a[j + 3 * c];
+      for (int k = 0; k < j; k++) t -= a[k + 3 * j] * a[k + 3 * c];
+      a[j + 3 * c] = t / s;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; i++) {  // U^T y = b
+    double t = b[i];
+    for (int k = 0; k < i; k++) t -= a[k + 3 * i] * b[k];
+    b[i] = t / a[i + 3 * i];
+  }
+#pragma unroll
+  for (int i = 2; i >= 0; i--) {  // U x = y
+    double t = b[i];
+    for (int k = i + 1; k < 3; k++) t -= a[i + 3 * k] * b[k];
+    b[i] = t / a[i + 3 * i];
+  }
+  return 0;
+}
+
+// A x = b for a 2x2 A (column-major) by LU with partial pivoting in the
+// arithmetic of LAPACK dgetf2 / dgetrs; 0, or k > 0 for an exactly zero U(k,k)
+__device__ __forceinline__ int lu2_solve(double* a, double* b) {
+  int p = fabs(a[1]) > fabs(a[0]) ? 1 : 0;
+  if (a[p] == 0.0) return 1;
+  if (p) {
+    double t = a[0]; a[0] = a[1]; a[1] = t;
+    t = a[2]; a[2] = a[3]; a[3] = t;
+  }
+  const double piv = a[0];
+  if (fabs(piv) >= 2.2250738585072014e-308) a[1] *= 1.0 / piv;
+  else a[1] /= piv;
+  const double u = a[2];
+  if (u != 0.0) a[3] += a[1] * -u;
+  if (a[3] == 0.0) return 2;
+  if (p) { const double t = b[0]; b[0] = b[1]; b[1] = t; }
+  if (b[0] != 0.0) b[1] -= b[0] * a[1];
+  if (b[1] != 0.0) { b[1] /= a[3]; b[0] -= b[1] * a[2]; }
+  if (b[0] != 0.0) b[0] /= a[0];
+  return 0;
+}
+
+// DIAGONAL_BLOCK_Solver (dbs.c:492-550) for the bilateral kinds: fixpnt,
+// fixdir, velodir, velodir3, riglnk (dbs.c:328-450). Returns the iterations
+// (riglnk) or 0, and -1 when a factorisation fails.
+static __device__ __noinline__ int bilateral_solve(int kind, const double* Z, double step, int dynamic, double epsilon,
+                                                   int maxiter, const double* W, const double* B, const double* V,
+                                                   double* U, double* R) {
+  switch (kind) {
+    case CON_FIXPNT: {  // W R = -V - B (dynamic) or -B, U = -V or 0
+      double A[9];
+      for (int q = 0; q < 9; q++) A[q] = W[q];
+      if (dynamic) { U[0] = -V[0]; U[1] = -V[1]; U[2] = -V[2]; }
+      else { U[0] = U[1] = U[2] = 0.0; }
+      R[0] = U[0] - B[0]; R[1] = U[1] - B[1]; R[2] = U[2] - B[2];
+      return chol3_solve(A, R) ? -1 : 0;
+    }
+    case CON_FIXDIR:
+    case CON_VELODIR: {
+      R[0] = 0.0;
+      R[1] = 0.0;
+      if (kind == CON_VELODIR) R[2] = (Z[0] - B[2]) / W[8];
+      else R[2] = dynamic ? -(V[2] + B[2]) / W[8] : -B[2] / W[8];
+      U[0] = B[0] + R[2] * W[6]; U[1] = B[1] + R[2] * W[7]; U[2] = B[2] + R[2] * W[8];
+      return 0;
+    }
+    case CON_VELODIR3: {  // W R = Z - B, U = Z
+      double A[9];
+      for (int q = 0; q < 9; q++) A[q] = W[q];
+      U[0] = Z[0]; U[1] = Z[1]; U[2] = Z[2];
+      R[0] = U[0] - B[0]; R[1] = U[1] - B[1]; R[2] = U[2] - B[2];
+      return chol3_solve(A, R) ? -1 : 0;
+    }
+    case CON_RIGLNK: {  // min 0.5 W_NN R_N^2 subject to |Z + h (W_.N R_N + B)|^2 = d^2 (dbs.c:396-450)
+      const double h = dynamic ? step * 0.5 : step;
+      const double len = Z[3];
+      double l = 0.0, error;
+      int iter = 0;
+      R[0] = R[1] = 0.0;
+      do {
+        double C[3], D[4], X[2], L[4];
+        C[0] = B[0] + R[2] * W[6]; C[1] = B[1] + R[2] * W[7]; C[2] = B[2] + R[2] * W[8];
+        D[0] = Z[0] + h * C[0]; D[1] = Z[1] + h * C[1]; D[2] = Z[2] + h * C[2];
+        X[1] = (D[0] * D[0] + D[1] * D[1] + D[2] * D[2]) - len * len;
+        D[3] = (W[6] * D[0] + W[7] * D[1] + W[8] * D[2]) * 2.0 * h;
+        X[0] = W[8] * R[2] + l * D[3];
+        L[0] = W[8]; L[2] = D[3];
+        L[1] = D[3]; L[3] = 0.0;
+        if (lu2_solve(L, X)) return -1;
+        R[2] -= X[0];
+        l -= X[1];
+        error = sqrt((X[0] * X[0] + X[1] * X[1]) / (R[2] * R[2] + l * l));
+      } while (error > epsilon && ++iter < maxiter);
+      if (dynamic && iter >= maxiter) {  // the velocity zeroing formula
+        R[2] = -B[2] / W[8];
+        iter = 0;
+      }
+      U[0] = B[0] + R[2] * W[6]; U[1] = B[1] + R[2] * W[7]; U[2] = B[2] + R[2] * W[8];
+      return iter;
+    }
+  }
+  return -1;
+}
+
+// a bilateral row with the reference's failure handling (bgs.c:969-1013): no
+// fallback chain outside contacts; under CONTINUE a failed or diverged row
+// keeps its previous reaction. Returns 0, 1 diverged, 2 failed.
+__device__ __forceinline__ int bilateral_solve_row(int kind, const double* Z, double step, int dynamic, int failure,
+                                                   double epsilon, int maxiter, const double* W, const double* B,
+                                                   const double* V, double* U, double* R) {
+  const double r0 = R[0], r1 = R[1], r2 = R[2];
+  const int it = bilateral_solve(kind, Z, step, dynamic, epsilon, maxiter, W, B, V, U, R);
+  if (it < maxiter && it >= 0) return 0;
+  if (failure == FAIL_CONTINUE) { R[0] = r0; R[1] = r1; R[2] = r2; }
+  return it < 0 ? 2 : 1;
+}
+
+// merit numerator of a bilateral row (mrf.c:88-137, the GAUSS_SEIDEL_SOLVER
+// form for RIGLNK)
+__device__ __forceinline__ double merit_row_bilateral(int kind, const double* Z, double gap, double step, int dynamic,
+                                                      const double* A, const double* V, const double* U) {
+  switch (kind) {
+    case CON_FIXPNT:
+    case CON_VELODIR3: {
+      double P[3];
+      if (kind == CON_FIXPNT) {
+        if (dynamic) { P[0] = U[0] + V[0]; P[1] = U[1] + V[1]; P[2] = U[2] + V[2]; }
+        else { P[0] = U[0]; P[1] = U[1]; P[2] = U[2]; }
+      } else {
+        P[0] = Z[0] - U[0]; P[1] = Z[1] - U[1]; P[2] = Z[2] - U[2];
+      }
+      const double Q0 = A[0] * P[0] + A[3] * P[1] + A[6] * P[2];
+      const double Q1 = A[1] * P[0] + A[4] * P[1] + A[7] * P[2];
+      const double Q2 = A[2] * P[0] + A[5] * P[1] + A[8] * P[2];
+      return Q0 * P[0] + Q1 * P[1] + Q2 * P[2];
+    }
+    case CON_FIXDIR:
+    case CON_VELODIR:
+    case CON_RIGLNK: {
+      double P2;
+      if (kind == CON_FIXDIR) P2 = dynamic ? U[2] + V[2] : U[2];
+      else if (kind == CON_VELODIR) P2 = Z[0] - U[2];
+      else P2 = gap / (step * (dynamic ? 0.5 : 1.0)) + U[2];
+      const double Q2 = A[8] * P2;
+      return Q2 * P2;
+    }
+  }
+  return 0.0;
+}
+
 }  // namespace b2

@@ -485,6 +485,10 @@ int b2dev_nn_features(b2dev_ctx* c, float* feat, double* scale, double* rprev) {
 }
 
 int b2dev_nn_warm_start(b2dev_ctx* c, b2dev_mlp* net, double accept_ratio, b2dev_nn_report* rep) {
+  if (c && c->has_kinds) {
+    set_err("nn_warm_start: the learned start covers contact rows only; this problem has bilateral constraints");
+    return B2DEV_EUNSUPPORTED;
+  }
   using namespace b2::mlp;
   if (!c || !c->ready || !net || !rep || !(accept_ratio > 0.0 && accept_ratio <= 1.0)) {
     set_err("nn_warm_start: invalid arguments");

@@ -103,6 +103,8 @@ struct SolveArgs {
   const double* Bv;         // 3 planes of n: free velocity B
   const double* Vv;         // 3 planes of n: previous velocity V
   const double* rho;        // [n]
+  const int* kind;          // [n] constraint kind (dom.h:98), or null: all CONTACT (the KINDS kernels only)
+  const double* Zv;         // [4][n] the bilateral rows' Z (b2_diag.cuh), with kind
   const double* gap;        // [n]
   const double* fric;       // [n]
   const double* rest;       // [n]
@@ -398,7 +400,7 @@ __host__ __device__ constexpr size_t solve_smem_per_block() {
 // solves its row (diagonal solve in FP64). Tiles with more blocks than the
 // staging holds are processed in windows. Returns false if a wait gave up or
 // the solve has stopped.
-template <bool MIXED>
+template <bool MIXED, bool KINDS>
 __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags& f, int r0, int nr, int cs, int ce,
                                            int s, int rin, int rout, int prob, int kb0, int ke0, int tile,
                                            unsigned char* wsm, uint32_t& phase, double& errup, double& errlo,
@@ -466,6 +468,16 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
   cp.step = a.step;
   cp.dynamic = a.dynamic;
   cp.friction = cp.restitution = cp.cohesion = cp.gap = 0.0;
+  int ckind = CON_CONTACT;
+  double Zr[4] = {0.0, 0.0, 0.0, 0.0};
+  if constexpr (KINDS) {
+    if (own && ok) {
+      ckind = __ldg(a.kind + p);
+      if (ckind != CON_CONTACT)
+#pragma unroll
+        for (int q = 0; q < 4; q++) Zr[q] = __ldg(a.Zv + (size_t)q * n + p);
+    }
+  }
   if (own && ok) {
 #pragma unroll
     for (int q = 0; q < 3; q++) B[q] = __ldg(a.Bv + (size_t)q * n + p);
@@ -556,7 +568,9 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
       double A[9];
 #pragma unroll
       for (int q = 0; q < 9; q++) A[q] = __ldg(a.Ad + (size_t)q * n + p);
-      const double up = merit_row(cp, A, V, am, Rold);
+      double up;
+      if (KINDS && ckind != CON_CONTACT) up = merit_row_bilateral(ckind, Zr, cp.gap, a.step, a.dynamic, A, V, am);
+      else up = merit_row(cp, A, V, am, Rold);
       mnum += up;
       a.Um[s & 1][p] = make_double4(am[0], am[1], am[2], 0.0);
       if (a.conmerit[0]) a.conmerit[s & 1][p] = up;
@@ -640,8 +654,13 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
 #pragma unroll
         for (int q = 0; q < 3; q++) { tr[q] = ag[q]; tr[3 + q] = U[q]; tr[6 + q] = R[q]; }
       }
-      const int kind = diagonal_solve_row(a.diagsolver, a.failure, cp, a.diagepsilon, a.diagmaxiter, rho_row,
-                                          W, ag, V, U, R);
+      int kind;
+      if (KINDS && ckind != CON_CONTACT)
+        kind = bilateral_solve_row(ckind, Zr, a.step, a.dynamic, a.failure, a.diagepsilon, a.diagmaxiter, W, ag, V, U,
+                                   R);
+      else
+        kind = diagonal_solve_row(a.diagsolver, a.failure, cp, a.diagepsilon, a.diagmaxiter, rho_row, W, ag, V, U,
+                                  R);
       if (tr) {
 #pragma unroll
         for (int q = 0; q < 3; q++) { tr[9 + q] = U[q]; tr[12 + q] = R[q]; }
@@ -765,7 +784,7 @@ static __device__ __noinline__ void finalize_sweep(const SolveArgs& a, int prob,
 // Six blocks of two warps per SM (at most 168 registers a thread): with the
 // list-order colouring a sweep has about six levels of ~1.5k tiles each, so
 // 1,776 resident warps hold a whole level in one wave.
-template <bool MIXED>
+template <bool MIXED, bool KINDS>
 __device__ __forceinline__ void solve_persistent(const SolveArgs& a) {
   extern __shared__ __align__(16) unsigned char solve_smem[];
   const int warp = threadIdx.x / kWarp;
@@ -815,7 +834,9 @@ __device__ __forceinline__ void solve_persistent(const SolveArgs& a) {
     const int rin = (a.in + s) % 3;       // iterate s-1
     const int rout = (a.in + s + 1) % 3;  // iterate s
     double errup = 0.0, errlo = 0.0, mnum = 0.0;
-    if (!solve_tile<MIXED>(a, f, ti.x, nr, ti.z, ti.w, s, rin, rout, prob, tk.x, tk.y, tile, wsm, phase, errup, errlo, mnum)) break;
+    if (!solve_tile<MIXED, KINDS>(a, f, ti.x, nr, ti.z, ti.w, s, rin, rout, prob, tk.x, tk.y, tile, wsm, phase, errup,
+                                  errlo, mnum))
+      break;
 #pragma unroll
     for (int d = 16; d >= 1; d >>= 1) {
       errup += __shfl_down_sync(0xffffffffu, errup, d);
@@ -842,7 +863,14 @@ __device__ __forceinline__ void solve_persistent(const SolveArgs& a) {
 // built without fused multiply-adds).
 template <bool MIXED>
 __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constant__ SolveArgs a) {
-  solve_persistent<MIXED>(a);
+  solve_persistent<MIXED, false>(a);
+}
+
+// the same with rows of the bilateral kinds (a.kind, a.Zv), used only when a
+// problem has such rows, so that the contact kernels keep their registers
+template <bool MIXED>
+__global__ void __launch_bounds__(kSolveThreads, 6) k_solve_kinds(const __grid_constant__ SolveArgs a) {
+  solve_persistent<MIXED, true>(a);
 }
 
 // FP32 sweeps of mixed precision, defined in b2_solve_fp32.cu: that
@@ -850,5 +878,6 @@ __global__ void __launch_bounds__(kSolveThreads, 6) k_solve(const __grid_constan
 // and the FP64 diagonal solves and merit of these sweeps may use (their results
 // are not bitwise the reference's anyway; the closing FP64 sweep is).
 __global__ void __launch_bounds__(kSolveThreads, 6) k_solve_fp32(const __grid_constant__ SolveArgs a);
+__global__ void __launch_bounds__(kSolveThreads, 6) k_solve_fp32_kinds(const __grid_constant__ SolveArgs a);
 
 }  // namespace b2

@@ -9,7 +9,11 @@
 namespace b2 {
 
 __global__ void __launch_bounds__(kSolveThreads, 6) k_solve_fp32(const __grid_constant__ SolveArgs a) {
-  solve_persistent<true>(a);
+  solve_persistent<true, false>(a);
+}
+
+__global__ void __launch_bounds__(kSolveThreads, 6) k_solve_fp32_kinds(const __grid_constant__ SolveArgs a) {
+  solve_persistent<true, true>(a);
 }
 
 }  // namespace b2

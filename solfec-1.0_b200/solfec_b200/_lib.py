@@ -83,6 +83,7 @@ _SIGNATURES = {
     'b2dev_detect_spheres': (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     'b2dev_convexes_setup': (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 7),
     'b2dev_rigid_flags': (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    'b2dev_set_kinds': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]),
     'b2dev_exclude_bodies': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     'b2dev_exclude_surfaces': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     'b2dev_unphysical_penetration': (C.c_int, [C.c_void_p, C.c_double]),

@@ -137,6 +137,20 @@ class LOCDYN:
     def get_state_ptr(self, R_ptr, U_ptr, cm_ptr=None, on_device=1):
         _check(lib().b2gs_locdyn_get_state(self._h, R_ptr, U_ptr, cm_ptr, int(on_device)), 'b2gs_locdyn_get_state')
 
+    def set_kinds(self, kinds=None, Z=None):
+        """Constraint kinds of the rows (dom.h:98: 0 CONTACT, 1 FIXPNT, 2 FIXDIR,
+        3 VELODIR, 4 VELODIR3, 5 RIGLNK) with Z[n][4] (VELODIR value, VELODIR3
+        values, RIGLNK local link vector and length); None: all contacts. Set
+        after the rows are uploaded (an upload or a detection resets them)."""
+        n = self.sizes()[0]
+        if kinds is None:
+            _check(lib().b2dev_set_kinds(self.device_context, n, None, None, 0), 'b2dev_set_kinds')
+            return
+        k = np.ascontiguousarray(kinds, dtype=np.int32).reshape(-1)
+        z = np.ascontiguousarray(np.zeros((k.shape[0], 4)) if Z is None else Z, dtype=np.float64).reshape(-1)
+        self._kinds = (k, z)
+        _check(lib().b2dev_set_kinds(self.device_context, int(k.shape[0]), ptr(k), ptr(z), 0), 'b2dev_set_kinds')
+
     def set_state(self, R=None, U=None):
         n = self.sizes()[0]
         Rh = None if R is None else _f64(R).reshape(-1)

@@ -357,3 +357,45 @@ def test_layout_reuse_follows_tile_rows(scene_cache):
         it, R, U = solve(ldy)
         assert it == ref[0] and same_bits(R, ref[1]) and same_bits(U, ref[2])
     ldy.close()
+
+
+@pytest.mark.parametrize('dynamic', [1, 0])
+def test_bilateral_constraints_parity(ld1k, scene_cache, dynamic):
+    """FIXPNT, FIXDIR, VELODIR, VELODIR3 and RIGLNK rows among the pile's
+    contacts (b2dev_set_kinds; the KINDS solve kernels): FP64 bitwise with the
+    oracle in the GPU's row order (which equals the compiled reference, tests/
+    test_oracle.py), iterations and merit included; mixed precision reaches
+    merit 1e-4 too, its reactions within 1e-2 of FP64's at that merit."""
+    from kinds_data import bilateral_kinds, riglnk_gap
+    sc = scene_cache('spheres_lattice')
+    ld = ld1k.permuted(np.arange(ld1k.n))
+    ld.dynamic = dynamic
+    kinds, Z = bilateral_kinds(ld.n, bodies=(sc.master, sc.slave, sc.obstacle))
+    ld.gap = riglnk_gap(kinds, Z, ld.gap)
+    kw = dict(epsilon=1e-4, maxiter=1000, meritval=1e-4)
+    out = {}
+    for precision in ('FP64', 'MIXED'):
+        ldy = LOCDYN()
+        ldy.set_colour_seed(SEED)
+        ldy.set(ld)
+        ldy.set_kinds(kinds, Z)
+        gs = GAUSS_SEIDEL_SOLVER(**kw)
+        gs.precision = precision
+        gs.solve(ldy)
+        R, U, cm = ldy.get_state()
+        out[precision] = dict(R=R, U=U, cm=cm, iters=gs.iters, merit=ldy.merit, order=ldy.order(), error=gs.error)
+        ldy.close()
+    g = out['FP64']
+    order = g['order']
+    res = O.solve(ld.permuted(order), kinds=kinds[order], Z=Z[order], **kw)
+    R = np.empty((ld.n, 3)); U = np.empty((ld.n, 3))
+    R[order] = res['R'].reshape(-1, 3); U[order] = res['U'].reshape(-1, 3)
+    assert g["iters"] == res["iters"] < 1000, (g["iters"], res["iters"])
+    assert same_bits(g['R'], R) and same_bits(g['U'], U)
+    np.testing.assert_allclose(g['merit'], res['merit'], rtol=1e-13)
+    m = out['MIXED']
+    assert m['merit'] <= 1e-4 and g['merit'] <= 1e-4
+    assert rel(m['R'], g['R']) < 1e-2
+    # every row kind present, and a kinds-free solve is a different problem
+    assert set(np.unique(kinds)) == {0, 1, 2, 3, 4, 5}
+    assert not same_bits(gpu_solve(ld, **kw)['R'], g['R'])

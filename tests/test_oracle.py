@@ -18,6 +18,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from kinds_data import bilateral_kinds, riglnk_gap
 from solfec_b200 import scenes
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -203,3 +204,32 @@ def test_list_order_colouring_is_greedy_in_list_order(pile):
             c += 1
         ref[i] = c
     assert np.array_equal(col, ref) and nc == ref.max() + 1
+
+
+@pytest.mark.skipif(not O.ref_available(), reason='reference solver build (oracle/_ref) not present')
+@pytest.mark.parametrize('kw', [REF_CASES[0], REF_CASES[1], REF_CASES[2], REF_CASES[5]],
+                         ids=lambda k: '-'.join('%s=%s' % it for it in sorted(k.items())))
+@pytest.mark.parametrize('dynamic', [1, 0])
+def test_oracle_matches_compiled_reference_with_bilateral_constraints(pile, kw, dynamic):
+    """FIXPNT, FIXDIR, VELODIR, VELODIR3 and RIGLNK rows among the contacts
+    of the sphere pile (dbs.c:328-550, mrf.c:88-137): the restatement equals
+    the compiled reference bit for bit, dynamic and static."""
+    sc, ld, corder = pile
+    lp = ld.permuted(corder)
+    lp.dynamic = dynamic
+    kinds, Z = bilateral_kinds(lp.n, bodies=(sc.master[corder], sc.slave[corder], sc.obstacle))
+    lp.gap = riglnk_gap(kinds, Z, lp.gap)
+    a = O.solve(lp, impl='oracle', kinds=kinds, Z=Z, **kw)
+    b = O.solve(lp, impl='ref', kinds=kinds, Z=Z, **kw)
+    for k in ('iters', 'error', 'thrown', 'ncallbacks'):
+        assert a[k] == b[k], k
+    for k in ('R', 'U', 'conmerit', 'rerhist', 'merhist'):
+        assert same_bits(a[k], b[k]), k
+    # the bilateral rows are solved: e.g. a FIXDIR row's normal velocity vanishes (dynamic: U_N = -V_N) to the
+    # solver's tolerance (the final U holds the neighbours' later reactions)
+    fd = np.nonzero(kinds == 2)[0]
+    U = a['U'].reshape(-1, 3)
+    if kw.get('maxiter', 0) >= 200:
+        assert np.abs(U[fd, 2] + (lp.V.reshape(-1, 3)[fd, 2] if dynamic else 0.0)).max() < 1e-3
+    c = O.solve(lp, impl='oracle', **kw)   # without kinds: a different problem
+    assert not same_bits(a['R'], c['R'])
