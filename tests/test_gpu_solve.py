@@ -399,3 +399,20 @@ def test_bilateral_constraints_parity(ld1k, scene_cache, dynamic):
     # every row kind present, and a kinds-free solve is a different problem
     assert set(np.unique(kinds)) == {0, 1, 2, 3, 4, 5}
     assert not same_bits(gpu_solve(ld, **kw)['R'], g['R'])
+
+
+def test_spring_kind_rejected(ld1k):
+    """SPRING rows (kind 6) and kinds outside dom.h:98 are refused; kinds of a
+    wrong length too; None makes every row a contact again."""
+    ldy = LOCDYN()
+    ldy.set_colour_seed(SEED)
+    ldy.set(ld1k)
+    for bad in (np.full(ld1k.n, 6), np.full(ld1k.n, -1), np.zeros(ld1k.n - 1)):
+        with pytest.raises(SolfecError):
+            ldy.set_kinds(bad)
+    ldy.set_kinds(None)
+    gs = GAUSS_SEIDEL_SOLVER(1e-4, 1000, 1e-4)
+    gs.solve(ldy)
+    R, _, _ = ldy.get_state()
+    assert same_bits(R, gpu_solve(ld1k, epsilon=1e-4, maxiter=1000, meritval=1e-4)['R'])
+    ldy.close()
