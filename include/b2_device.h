@@ -114,6 +114,18 @@ int b2dev_rigid_step_begin(b2dev_ctx* ctx, double step, const double* gravity, c
 int b2dev_rigid_step_end(b2dev_ctx* ctx, double step);
 int b2dev_rigid_get(b2dev_ctx* ctx, double* rot, double* x, double* velo, double* velo0, int on_device);
 
+/* The bilateral constraints' part of DOM_Update_Begin (dom.c:3716-3732) on
+ * the device bodies, after b2dev_rigid_step_begin and before the assembly:
+ * RIGLNK rows get base, gap and the solver's local link vector Z[0..2] from
+ * the current link (update_riglnk, dom.c:524-550; Z[3] is the link length);
+ * FIXDIR rows with a slave body move their master point under the slave's
+ * and take the base from the master's current image of the referential
+ * direction in Z[0..2] (update_fixdir, dom.c:487-500). A row without a
+ * slave (slave < 0) links to the spatial point spnt. The other kinds and
+ * contacts are left as they are. Needs b2dev_rigid_setup; does nothing
+ * before b2dev_set_kinds has given bilateral rows. */
+int b2dev_update_constraints(b2dev_ctx* ctx);
+
 /* Contact update and detection between spheres held by the uploaded bodies:
  * the contact part of DOM_Update_Begin (dom.c:3700-3790) for sphere pairs, on
  * the device bodies (rotation of b2dev_upload_scene, mass centre of

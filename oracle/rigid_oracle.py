@@ -9,13 +9,15 @@ checker of the device integrator (csrc/b2_rigid.cuh):
 - rig_constraints_force, bod.c:419-439, with rig_operator_H, bod.c:216-228;
 - the exponential map of alg.h:1138-1200 (EXPMAP);
 - u += h M^-1 f as MX_Matvec on the block-diagonal inverse, mtx.c:2297-2307,
-  in the netlib dgemv order.
+  in the netlib dgemv order;
+- the bilateral constraints' update of DOM_Update_Begin (update_riglnk,
+  update_fixdir; dom.c:487-550), BODY_Cur_Point and BODY_Ref_Point.
 
 The arithmetic is written in scalar Python floats (IEEE double, no fused
 multiply-add) in the operation order of the reference's algebra macros, so it
 is bitwise comparable with the device kernels, which are built without
 multiply-add contraction, wherever the exponential map takes its small-angle
-branch. Schemes: 0 = RIG_POS (NEW1), 1 = RIG_NEG (NEW2, the default).
+branch. Schemes: 0 = RIG_POS (NEW1), 1 = RIG_NEG (NEW2, the default), 2 = RIG_IMP (NEW3).
 
 Parity of this restatement with the reference itself is not pinned bitwise:
 the reference's point-force callbacks and BLAS are site-specific. It is pinned
@@ -348,6 +350,50 @@ def step_end(bd: Bodies, step, master, slave, mpnt, spnt, base, R):
                 bd.failures |= code
                 u[0], u[1], u[2] = W[0], W[1], W[2]
                 bd.rot[b] = mat_mul(Rb, DR)
+
+
+def cur_point(bd: Bodies, b, X):
+    """BODY_Cur_Point of a rigid body or obstacle (bod.c:1702-1716, NVADDMUL)."""
+    R, c, C = bd.rot[b], bd.x[b], bd.x0[b]
+    A = [X[0] - C[0], X[1] - C[1], X[2] - C[2]]
+    return [c[i] + (R[i] * A[0] + R[3 + i] * A[1] + R[6 + i] * A[2]) for i in range(3)]
+
+
+def ref_point(bd: Bodies, b, x):
+    """BODY_Ref_Point of a rigid body or obstacle (bod.c:1736-1750, TVADDMUL)."""
+    R, c, C = bd.rot[b], bd.x[b], bd.x0[b]
+    a = [x[0] - c[0], x[1] - c[1], x[2] - c[2]]
+    return [C[i] + (R[3 * i] * a[0] + R[3 * i + 1] * a[1] + R[3 * i + 2] * a[2]) for i in range(3)]
+
+
+CON_FIXDIR, CON_RIGLNK = 2, 5  # dom.h:98
+
+
+def update_constraints(bd: Bodies, kinds, master, slave, mpnt, spnt, base, gap, Z):
+    """The bilateral constraints' part of DOM_Update_Begin (dom.c:3716-3732)
+    on the bodies at t + h/2, in place on the row arrays: RIGLNK as
+    update_riglnk (dom.c:524-550), with Z[i][0..2] the link vector in the new
+    base (the diagonal solver's TVMUL, dbs.c:409) and Z[i][3] the length;
+    FIXDIR with a slave body as update_fixdir (dom.c:487-500), the master's
+    referential direction in Z[i][0..2]. spnt is the spatial point of a row
+    without a slave."""
+    import oracle  # localbase restated in C (oracle_detect.c)
+    for i, k in enumerate(kinds):
+        m, s = int(master[i]), int(slave[i])
+        if k == CON_RIGLNK:
+            pm = cur_point(bd, m, [float(v) for v in mpnt[i]])
+            ps = cur_point(bd, s, [float(v) for v in spnt[i]]) if s >= 0 else [float(v) for v in spnt[i]]
+            v = [pm[0] - ps[0], pm[1] - ps[1], pm[2] - ps[2]]
+            ln = math.sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+            gap[i] = ln - float(Z[i][3])
+            ln = 1.0 / ln
+            b = oracle.localbase(np.array([v[0] * ln, v[1] * ln, v[2] * ln]))
+            base[i] = b
+            Z[i][:3] = matt_vec([float(q) for q in b], v)
+        elif k == CON_FIXDIR and s >= 0:
+            p = cur_point(bd, s, [float(v) for v in spnt[i]])
+            mpnt[i] = ref_point(bd, m, p)
+            base[i] = oracle.localbase(np.array(mat_vec(bd.rot[m], [float(q) for q in Z[i][:3]])))
 
 
 def kinetic_energy(bd: Bodies, b):

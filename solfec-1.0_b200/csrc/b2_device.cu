@@ -26,6 +26,7 @@
 #include "b2_colour.cuh"
 #include "b2_rigid.cuh"
 #include "b2_detect.cuh"
+#include "b2_bilateral.cuh"
 
 using namespace b2;
 
@@ -1335,6 +1336,20 @@ int b2dev_rigid_get(b2dev_ctx* c, double* rot, double* x, double* velo, double* 
   }
   B2_CK(cudaStreamSynchronize(st));
   return rigid_failures(c);
+}
+
+int b2dev_update_constraints(b2dev_ctx* c) {
+  if (!c || !c->have_rigid) { set_err("update_constraints: no rigid bodies set up"); return B2DEV_ESTATE; }
+  if (!c->has_kinds || c->ncon == 0) return B2DEV_OK;  // contacts only: nothing to update
+  DeviceGuard g(c->device);
+  c->launches++;
+  k_constraints_update<<<blocks_for(c->ncon, 128), 128, 0, c->stream>>>(
+      c->ncon, ptr<int>(c->kind_c), ptr<int>(c->master), ptr<int>(c->slave), ptr<double>(c->rot),
+      ptr<double>(c->rb_x), ptr<double>(c->x0), ptr<double>(c->mpnt), ptr<double>(c->spnt), ptr<double>(c->base),
+      ptr<double>(c->gap_c), ptr<double>(c->Z_c));
+  B2_CK(cudaGetLastError());
+  c->ready = false;  // frames and gaps changed: the local dynamics must be assembled again
+  return B2DEV_OK;
 }
 
 // ---- contact update and detection between spheres (dom.c:3700-3790) ----

@@ -14,8 +14,11 @@ exact for contacts that stay attached to the same material points, e.g. a
 block sliding on a flat table; for spheres and convex obstacles,
 detect.run_spheres detects and updates the contacts on the device every step.
 
-Schemes: 'RIG_NEG' (NEW2, the reference's default) and 'RIG_POS' (NEW1);
-'RIG_IMP' (NEW3) is not supported and raises.
+Schemes: 'RIG_NEG' (NEW2, the reference's default), 'RIG_POS' (NEW1) and
+'RIG_IMP' (NEW3). Bilateral constraints (FIXPNT, FIXDIR, VELODIR, VELODIR3,
+RIGLNK) ride along as rows of the fixed set with their kinds: every step
+updates their frames from the device bodies before the assembly, as
+DOM_Update_Begin does (dom.c:3716-3732).
 """
 from __future__ import annotations
 
@@ -78,6 +81,11 @@ class RIGID_DYNAMICS:
         _check(lib().b2dev_rigid_step_begin(self.ldy.device_context, float(step), ptr(g), ptr(L), 0),
                'BODY_Dynamic_Step_Begin')
 
+    def update_constraints(self):
+        """The bilateral constraints' update of DOM_Update_Begin on the device
+        bodies (RIGLNK frames, gaps and link vectors; FIXDIR with a slave body)."""
+        _check(lib().b2dev_update_constraints(self.ldy.device_context), 'b2dev_update_constraints')
+
     def step_end(self, step: float):
         """BODY_Dynamic_Step_End of every body with the reactions of the last solve."""
         _check(lib().b2dev_rigid_step_end(self.ldy.device_context, float(step)), 'BODY_Dynamic_Step_End')
@@ -93,27 +101,35 @@ class RIGID_DYNAMICS:
 
 
 def run_fixed_contacts(scene, gs, nsteps: int, J, mass, gravity=(0.0, 0.0, 0.0), loads=None, callback=None,
-                       scheme=None, time: float = 0.0, ldy: LOCDYN = None):
+                       scheme=None, time: float = 0.0, ldy: LOCDYN = None, kinds=None, Z=None):
     """Time loop of a scene whose contacts stay as uploaded.
 
-    Every step: bodies to t + h/2 and free velocities (device), local dynamics
+    Every step: bodies to t + h/2 and free velocities (device), the bilateral
+    constraints' frames from the moved bodies (with kinds), local dynamics
     from the device bodies, GAUSS_SEIDEL solve warm-started from the previous
     reactions (the reference keeps con->R between steps), constraint reactions
     and the second half step (device). loads(t) -> (nbod, 9) or None is called
     with t = time + h/2 of each step; callback(k, time, dyn, ldy) after step k
-    (k from 1), where a return value of False stops the loop.
-    Returns (RIGID_DYNAMICS, LOCDYN).
+    (k from 1), where a return value of False stops the loop. kinds, Z: the
+    rows' constraint kinds and values as LOCDYN.set_kinds takes them (RIGLNK:
+    Z[3] the link length; FIXDIR with a slave: Z[0..2] the master's
+    referential direction). Returns (RIGID_DYNAMICS, LOCDYN).
     """
     if ldy is None:
         ldy = LOCDYN()
     ldy.update_begin(scene)  # upload of bodies and contacts (and a first assembly)
     dyn = RIGID_DYNAMICS(ldy, J, mass, scene.x, scheme)
+    bilateral = kinds is not None and bool(np.any(np.asarray(kinds) != 0))
+    if bilateral:
+        ldy.set_kinds(kinds, Z)
     h = float(scene.step)
     R = np.zeros((scene.ncon, 3))
     U = np.zeros((scene.ncon, 3))
     t = float(time)
     for k in range(1, int(nsteps) + 1):
         dyn.step_begin(h, gravity, None if loads is None else loads(t + 0.5 * h))
+        if bilateral:
+            dyn.update_constraints()
         _check(lib().b2gs_locdyn_update_begin_resident(ldy.handle, h, int(scene.dynamic)), 'LOCDYN_Update_Begin')
         ldy.set_state(R, U)
         gs.solve(ldy)

@@ -607,6 +607,65 @@ def projectile_loads(mass: float, velo: np.ndarray) -> np.ndarray:
 PROJECTILE_GRAVITY = 9.81456
 
 
+def _one_body_rows(name, step, x, J, mass, kinds, mpnt, spnt, base, gap, Z):
+    """A scene of one rigid body (index 0) whose rows are bilateral
+    constraints without a slave body (slave -1, spnt the spatial point)."""
+    nc = len(kinds)
+    jinv = np.linalg.inv(J.reshape(3, 3).T).T.reshape(1, 9)
+    scene = Scene(name=name, step=step, dynamic=1, rot=np.eye(3).reshape(1, 9), x=x.reshape(1, 3).copy(),
+                  x0=x.reshape(1, 3).copy(), jinv=jinv, minv=np.array([1.0 / mass]), velo=np.zeros((1, 6)),
+                  velo0=np.zeros((1, 6)), obstacle=np.zeros(1, dtype=np.int32),
+                  master=np.zeros(nc, dtype=np.int32), slave=np.full(nc, -1, dtype=np.int32),
+                  mpnt=np.asarray(mpnt, float).reshape(nc, 3), spnt=np.asarray(spnt, float).reshape(nc, 3),
+                  base=np.asarray(base, float).reshape(nc, 9), gap=np.asarray(gap, float).reshape(nc),
+                  friction=np.zeros(nc), restitution=np.zeros(nc), cohesion=np.zeros(nc), mass=np.array([mass]))
+    return (scene, J.reshape(1, 9).copy(), np.array([mass]), np.asarray(kinds, dtype=np.int32),
+            np.asarray(Z, float).reshape(nc, 4))
+
+
+MATH_PENDULUM_GRAVITY = math.pi * math.pi
+
+
+def math_pendulum(step: float = 1e-3):
+    """The scene of the reference's tests/math-pendulum.py: a rigid ball of
+    mass 1 and unit inertia centred at (1, 0, 1) on a rigid link
+    (PUT_RIGID_LINK, dom.c:3379-3427) of length 1 to the fixed point (0, 0, 1),
+    at rest on the horizontal, under gravity pi^2 (MATH_PENDULUM_GRAVITY), so
+    that the period from the horizontal is 2.36 s. One RIGLNK row: master the
+    ball at its centre, no slave, spnt the fixed point; a frame with the link
+    direction as its normal, gap 0 and Z = (the link in that frame, length 1)
+    until the first step's update_riglnk (dom.c:524-550) replaces them.
+    Returns (scene, J, mass, kinds, Z)."""
+    n = np.array([[1.0, 0.0, 0.0]])
+    base = local_base(n)
+    link = base.reshape(3, 3, order='F').T @ n[0]
+    return _one_body_rows('math-pendulum', step, np.array([1.0, 0.0, 1.0]), np.eye(3).reshape(9), 1.0, [5],
+                          [[1.0, 0.0, 1.0]], [[0.0, 0.0, 1.0]], base, [0.0], [[link[0], link[1], link[2], 1.0]])
+
+
+PINNED_BAR_GRAVITY = 9.8
+
+
+def pinned_bar(step: float = 1e-3):
+    """The scene of the reference's tests/pinned-bar.py: a rigid 0.1 x 0.1 x 1
+    bar of density 1 (its mesh from z = 0 to 1, centred on the z axis),
+    turned by -30 degrees about the y axis through (0, 0, 0.75), with two
+    FIX_POINT constraints (DOM_Fix_Point, dom.c:3272-3292: identity base) at
+    (0, -0.05, 0.75) and (0, 0.05, 0.75), which make a hinge about y; gravity
+    9.8 (PINNED_BAR_GRAVITY). Released at rest, the bar swings about the
+    hinge; the test reads its angular velocity about y when the mass centre
+    passes x = 0 (2.121 rad/s). Returns (scene, J, mass, kinds, Z)."""
+    mass = 0.1 * 0.1 * 1.0
+    a = -math.radians(30.0)  # right-handed turn about +y
+    Ry = np.array([[math.cos(a), 0.0, math.sin(a)], [0.0, 1.0, 0.0], [-math.sin(a), 0.0, math.cos(a)]])
+    pivot = np.array([0.0, 0.0, 0.75])
+    x = pivot + Ry @ (np.array([0.0, 0.0, 0.5]) - pivot)
+    J = Ry @ box_inertia(mass, 0.1, 0.1, 1.0).reshape(3, 3) @ Ry.T
+    pts = [[0.0, -0.05, 0.75], [0.0, 0.05, 0.75]]
+    return _one_body_rows('pinned-bar', step, x, J.T.reshape(9), mass, [1, 1], pts, pts,
+                          np.tile(np.eye(3).reshape(9), (2, 1)), [0.0, 0.0], np.zeros((2, 4)))
+
+
 def advance_velocities(scene: Scene, R: np.ndarray) -> Scene:
     """One velocity step of the rigid bodies with the solved reactions: the new
     velocity at t is u = u_free + h M^-1 sum H^T R (bod.c:418-439 force

@@ -1,8 +1,13 @@
 """Extracts the values the reference's own rigid-body tests pin into JSON
 fixtures: tests/block-sliding.py:64-80 (position x and velocity v_x of the
 block at given callback indices, 1e-3 relative tolerance) into
-block_sliding_ref.json, and tests/projectile.py:47-50 (the x distance in
-inches at the end, 0.5% relative tolerance) into projectile_ref.json. Run with
+block_sliding_ref.json, tests/projectile.py:47-50 (the x distance in
+inches at the end, 0.5% relative tolerance) into projectile_ref.json,
+tests/math-pendulum.py:31-35 (the period from the horizontal, 1%) into
+math_pendulum_ref.json, tests/pinned-bar.py:38-42 (the angular velocity about
+y when the mass centre passes x = 0, 1%) into pinned_bar_ref.json and
+tests/double-pendulum.py:103-107 (total energy at given step indices, 1e-3
+relative to max(1, value)) into double_pendulum_ref.json. Run with
 the environment variable REFERENCE set to the reference source tree; the
 tests read only the JSON."""
 import ast
@@ -38,6 +43,26 @@ def main():
     with open(path, 'w') as f:
         json.dump(out, f, indent=1)
     print(path, exact, tol)
+    here = os.path.dirname(os.path.abspath(__file__))
+    for test, out_name, quantity in (('math-pendulum.py', 'math_pendulum_ref.json', 'period [s]'),
+                                     ('pinned-bar.py', 'pinned_bar_ref.json', 'angular velocity about y [rad/s]')):
+        src = open(os.path.join(REFERENCE, 'tests', test)).read()
+        exact = float(re.search(r'exact\s*=\s*([0-9.eE+-]+)', src).group(1))
+        tol = float(re.search(r'if \(error < ([0-9.eE+-]+)\)', src).group(1))
+        out = dict(source='tests/%s of the reference (exact, error bound)' % test, quantity=quantity, value=exact,
+                   tolerance=tol)
+        with open(os.path.join(here, out_name), 'w') as f:
+            json.dump(out, f, indent=1)
+        print(out_name, exact, tol)
+    src = open(os.path.join(REFERENCE, 'tests', 'double-pendulum.py')).read()
+    m = re.search(r'REF\s*=\s*(\[[^\]]*\])', src)
+    tol = float(re.search(r'if error > ([0-9.eE+-]+)', src).group(1))
+    values = ast.literal_eval(m.group(1))
+    out = dict(source='tests/double-pendulum.py of the reference (REF list)', quantity='total energy [J]',
+               tolerance=tol, pins=[dict(index=int(i), value=float(v)) for i, v in values])
+    with open(os.path.join(here, 'double_pendulum_ref.json'), 'w') as f:
+        json.dump(out, f, indent=1)
+    print('double_pendulum_ref.json', len(values), tol)
 
 
 if __name__ == '__main__':

@@ -20,6 +20,7 @@ import pytest
 
 import oracle as O
 from solfec_b200 import GAUSS_SEIDEL_SOLVER, LOCDYN, SolfecError, scenes
+from solfec_b200.solver import DeviceError
 
 pytestmark = pytest.mark.gpu
 
@@ -408,7 +409,7 @@ def test_spring_kind_rejected(ld1k):
     ldy.set_colour_seed(SEED)
     ldy.set(ld1k)
     for bad in (np.full(ld1k.n, 6), np.full(ld1k.n, -1), np.zeros(ld1k.n - 1)):
-        with pytest.raises(SolfecError):
+        with pytest.raises(DeviceError):
             ldy.set_kinds(bad)
     ldy.set_kinds(None)
     gs = GAUSS_SEIDEL_SOLVER(1e-4, 1000, 1e-4)

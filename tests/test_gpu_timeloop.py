@@ -129,3 +129,102 @@ def test_masonry_arch_new3_time_loop():
     iters, bd = time_loop_parity(sc, 300, J=J, mass=mass, scheme='RIG_IMP', epsilon=1e-4, maxiter=10000)
     assert bd.failures == 0
     assert sum(ro.kinetic_energy(bd, b) for b in range(bd.nbod) if not bd.obstacle[b]) < 1e-4
+
+
+def constrained_loop_parity(sc, J, mass, kinds, Z, gravity, nsteps, callback, **kw):
+    """Device time loop of a scene whose rows are bilateral constraints (step
+    begin, b2dev_update_constraints, assembly, solve with the kinds, step
+    end) against the CPU restatements, bitwise at every step; callback(k, t,
+    bd) on the restated bodies after step k stops the loop with False."""
+    h = float(sc.step)
+    ldy = LOCDYN()
+    ldy.update_begin(sc)
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    ldy.set_kinds(kinds, Z)
+    bd = ro.Bodies(sc.rot, sc.x, sc.velo, J, sc.jinv, mass, sc.minv, sc.x0, sc.obstacle)
+    mpnt, base, gap, Zc = sc.mpnt.copy(), sc.base.copy(), sc.gap.copy(), np.array(Z, dtype=float)
+    gs = GAUSS_SEIDEL_SOLVER(**kw)
+    n = sc.ncon
+    R = np.zeros((n, 3)); U = np.zeros((n, 3))
+    Ro = np.zeros((n, 3)); Uo = np.zeros((n, 3))
+    t = 0.0
+    for k in range(1, nsteps + 1):
+        dyn.step_begin(h, gravity)
+        ro.step_begin(bd, h, gravity)
+        dyn.update_constraints()
+        ro.update_constraints(bd, kinds, sc.master, sc.slave, mpnt, sc.spnt, base, gap, Zc)
+        assert lib().b2gs_locdyn_update_begin_resident(ldy.handle, h, int(sc.dynamic)) == 0
+        ldy.set_state(R, U)
+        gs.solve(ldy)
+        R, U, _ = ldy.get_state()
+        cur = dataclasses.replace(sc, rot=np.array(bd.rot), x=np.array(bd.x), velo=np.array(bd.velo),
+                                  velo0=np.array(bd.velo0), mpnt=mpnt, base=base, gap=gap)
+        order = ldy.order()
+        res = O.solve(O.assemble(cur).permuted(order), R=Ro[order].ravel(), U=Uo[order].ravel(), kinds=kinds[order],
+                      Z=Zc[order], **kw)
+        Ro = np.empty((n, 3)); Uo = np.empty((n, 3))
+        Ro[order] = res['R'].reshape(-1, 3); Uo[order] = res['U'].reshape(-1, 3)
+        assert gs.iters == res['iters'], (k, gs.iters, res['iters'])
+        assert same_bits(R, Ro) and same_bits(U, Uo), k
+        dyn.step_end(h)
+        ro.step_end(bd, h, sc.master, sc.slave, mpnt, sc.spnt, base, Ro)
+        st = dyn.state()
+        for key in ('rot', 'x', 'velo'):
+            assert same_bits(st[key], np.array(getattr(bd, key))), (k, key)
+        t += h
+        if callback(k, t, bd) is False:
+            break
+    ldy.close()
+    return k
+
+
+def test_math_pendulum_period():
+    """The reference's tests/math-pendulum.py on the device: a RIGLNK row to
+    a fixed point, updated on the device every step, bitwise with the CPU
+    restatements at every step of one full swing; the period within 1% of
+    2.36 s (the pinned value of the test)."""
+    from test_rigid_cpu import PendulumPeriod, pin
+    sc, J, mass, kinds, Z = scenes.math_pendulum()
+    cb = PendulumPeriod()
+    constrained_loop_parity(sc, J, mass, kinds, Z, (0.0, 0.0, -scenes.MATH_PENDULUM_GRAVITY), 2600, cb,
+                            epsilon=1e-3, maxiter=1000, failure='EXIT')
+    ref = pin('math_pendulum_ref.json')
+    assert cb.period is not None and abs(cb.period - ref['value']) / ref['value'] < ref['tolerance'], cb.period
+
+
+def test_pinned_bar_swing():
+    """The reference's tests/pinned-bar.py on the device: two FIXPNT rows
+    hinge a bar, bitwise with the CPU restatements at every step; the angular
+    velocity about y as the mass centre passes x = 0 within 1% of 2.121."""
+    from test_rigid_cpu import PinnedBarSwing, pin
+    sc, J, mass, kinds, Z = scenes.pinned_bar()
+    cb = PinnedBarSwing()
+    constrained_loop_parity(sc, J, mass, kinds, Z, (0.0, 0.0, -scenes.PINNED_BAR_GRAVITY), 500, cb,
+                            epsilon=1e-3, maxiter=1000, failure='EXIT')
+    ref = pin('pinned_bar_ref.json')
+    assert cb.omega is not None and abs(cb.omega - ref['value']) / ref['value'] < ref['tolerance'], cb.omega
+
+
+def test_math_pendulum_through_run_fixed_contacts():
+    """The same pendulum through the time-loop API (dynamics.run_fixed_contacts
+    with kinds), the period read from the device bodies."""
+    from solfec_b200.dynamics import run_fixed_contacts
+    from test_rigid_cpu import pin
+    sc, J, mass, kinds, Z = scenes.math_pendulum()
+    state = dict(previous=0.0, howmany=0, period=None)
+
+    def cb(k, t, dyn, ldy):
+        v = dyn.state()['velo'][0, 5]
+        if v * state['previous'] <= 0:
+            if state['howmany'] > 3:
+                state['period'] = t
+                return False
+            state['howmany'] += 1
+        state['previous'] = v
+        return True
+    gs = GAUSS_SEIDEL_SOLVER(1e-3, 1000, failure='EXIT')
+    dyn, ldy = run_fixed_contacts(sc, gs, 2600, J, mass, gravity=(0.0, 0.0, -scenes.MATH_PENDULUM_GRAVITY),
+                                  callback=cb, kinds=kinds, Z=Z)
+    ldy.close()
+    ref = pin('math_pendulum_ref.json')
+    assert state['period'] is not None and abs(state['period'] - ref['value']) / ref['value'] < ref['tolerance']

@@ -99,6 +99,114 @@ def test_projectile_pin_cpu():
     assert abs(x_in - ref['value']) / ref['value'] < ref['tolerance'], x_in
 
 
+def run_constrained_cpu(sc, J, mass, kinds, Z, gravity, nsteps, callback, impl='oracle', **kw):
+    """Time loop of a scene whose rows are bilateral constraints: step begin,
+    the constraints' update (update_riglnk / update_fixdir), assembly, the
+    solve with the constraint kinds, step end; callback(k, t, bd) after step k
+    stops the loop by returning False. Returns the last step index."""
+    bd = ro.Bodies(sc.rot, sc.x, sc.velo, J, sc.jinv, mass, sc.minv, sc.x0, sc.obstacle)
+    mpnt, base, gap, Zc = sc.mpnt.copy(), sc.base.copy(), sc.gap.copy(), np.array(Z, dtype=float)
+    R = np.zeros(3 * sc.ncon)
+    U = np.zeros(3 * sc.ncon)
+    t = 0.0
+    for k in range(1, nsteps + 1):
+        ro.step_begin(bd, sc.step, gravity)
+        ro.update_constraints(bd, kinds, sc.master, sc.slave, mpnt, sc.spnt, base, gap, Zc)
+        cur = dataclasses.replace(sc, rot=np.array(bd.rot), x=np.array(bd.x), velo=np.array(bd.velo),
+                                  velo0=np.array(bd.velo0), mpnt=mpnt, base=base, gap=gap)
+        out = oracle.solve(oracle.assemble(cur), R, U, kinds=kinds, Z=Zc, impl=impl, **kw)
+        R, U = out['R'], out['U']
+        ro.step_end(bd, sc.step, sc.master, sc.slave, mpnt, sc.spnt, base, R.reshape(-1, 3))
+        t += sc.step
+        if callback(k, t, bd) is False:
+            return k
+    return nsteps
+
+
+class PendulumPeriod:
+    """The termination callback of tests/math-pendulum.py:21-38: the time of
+    the fifth sign change of the ball's vertical velocity (velo[5]), counting
+    the start, i.e. one full period from the horizontal."""
+
+    def __init__(self):
+        self.previous, self.howmany, self.period = 0.0, 0, None
+
+    def __call__(self, k, t, bd):
+        v = bd.velo[0][5]
+        if v * self.previous <= 0:
+            if self.howmany > 3:
+                self.period = t
+                return False
+            self.howmany += 1
+        self.previous = v
+        return True
+
+
+class PinnedBarSwing:
+    """The callback of tests/pinned-bar.py:35-45: the angular velocity about
+    y (velo[1]) when the mass centre's x (conf[9]) first reaches 0."""
+
+    def __init__(self):
+        self.omega = None
+
+    def __call__(self, k, t, bd):
+        if bd.x[0][0] <= 0:
+            self.omega = bd.velo[0][1]
+            return False
+        return True
+
+
+def pin(name):
+    return json.load(open(os.path.join(HERE, 'golden', name)))
+
+
+@pytest.mark.parametrize('impl', ['oracle', 'ref'])
+def test_math_pendulum_period_cpu(impl):
+    """The reference's tests/math-pendulum.py: a ball on a rigid link
+    (RIGLNK to a fixed point) released from the horizontal under gravity pi^2,
+    GAUSS_SEIDEL_SOLVER (1E-3, 1000, failure = 'EXIT'); the period within 1%
+    of 2.36 s; the link length held to 1e-6."""
+    if impl == 'ref' and not oracle.ref_available():
+        pytest.skip('compiled reference solver not built')
+    sc, J, mass, kinds, Z = scenes.math_pendulum()
+    cb = PendulumPeriod()
+    lengths = []
+
+    def watch(k, t, bd):
+        x = bd.x[0]
+        lengths.append(math.sqrt(x[0] ** 2 + x[1] ** 2 + (x[2] - 1.0) ** 2))
+        return cb(k, t, bd)
+    run_constrained_cpu(sc, J, mass, kinds, Z, (0.0, 0.0, -scenes.MATH_PENDULUM_GRAVITY), 2600, watch, impl,
+                        epsilon=1e-3, maxiter=1000, failure='EXIT')
+    ref = pin('math_pendulum_ref.json')
+    assert cb.period is not None and abs(cb.period - ref['value']) / ref['value'] < ref['tolerance'], cb.period
+    assert np.abs(np.array(lengths) - 1.0).max() < 1e-6
+
+
+@pytest.mark.parametrize('impl', ['oracle', 'ref'])
+def test_pinned_bar_cpu(impl):
+    """The reference's tests/pinned-bar.py: a bar hinged by two FIX_POINT
+    constraints, released at 30 degrees, GAUSS_SEIDEL_SOLVER (1E-3, 1000,
+    failure = 'EXIT'); the angular velocity about y as the mass centre passes
+    x = 0 within 1% of 2.121 rad/s; the hinge points do not move."""
+    if impl == 'ref' and not oracle.ref_available():
+        pytest.skip('compiled reference solver not built')
+    sc, J, mass, kinds, Z = scenes.pinned_bar()
+    cb = PinnedBarSwing()
+    drift = []
+
+    def watch(k, t, bd):
+        for p in sc.mpnt:
+            q = ro.cur_point(bd, 0, [float(v) for v in p])
+            drift.append(max(abs(q[i] - p[i]) for i in range(3)))
+        return cb(k, t, bd)
+    run_constrained_cpu(sc, J, mass, kinds, Z, (0.0, 0.0, -scenes.PINNED_BAR_GRAVITY), 500, watch, impl,
+                        epsilon=1e-3, maxiter=1000, failure='EXIT')
+    ref = pin('pinned_bar_ref.json')
+    assert cb.omega is not None and abs(cb.omega - ref['value']) / ref['value'] < ref['tolerance'], cb.omega
+    assert max(drift) < 1e-6, max(drift)
+
+
 def test_expmap_rotation():
     rng = np.random.default_rng(5)
     for scale in (1e-6, 1e-2, 0.17, 0.18, 1.0, 3.0):
