@@ -126,6 +126,23 @@ int b2dev_rigid_get(b2dev_ctx* ctx, double* rot, double* x, double* velo, double
  * before b2dev_set_kinds has given bilateral rows. */
 int b2dev_update_constraints(b2dev_ctx* ctx);
 
+/* Bilateral constraints of a scene with contact detection (the reference's
+ * FIX_POINT, FIX_DIRECTION, SET_VELOCITY, PUT_RIGID_LINK: dom.c:3272-3427),
+ * n of them with kind 1-5 (dom.h:98), master and slave body (slave -1: none,
+ * spnt then a spatial point), referential points mpnt[3]/spnt[3], base[9]
+ * (FIXPNT the identity, FIXDIR and VELODIR the frame of the direction,
+ * VELODIR3 the caller's frame; RIGLNK and FIXDIR with a slave are refreshed
+ * by b2dev_update_constraints) and Z[4] as b2dev_set_kinds takes it (RIGLNK:
+ * Z[3] the link length; FIXDIR with a slave: Z[0..2] the master's
+ * referential direction). Host arrays. Every b2dev_detect_spheres lists them
+ * after the detected contacts (rows ncon .. ncon + n - 1 of the local
+ * dynamics, ncon as it reports), with their kinds set and their reactions
+ * carried from the previous detection; b2dev_get_contacts and
+ * b2dev_get_contact_area list the contacts only. Calling it again replaces
+ * them (n = 0 removes them); uploading a scene removes them. */
+int b2dev_constraints_setup(b2dev_ctx* ctx, int n, const int* kind, const int* master, const int* slave,
+                            const double* mpnt, const double* spnt, const double* base, const double* Z);
+
 /* Contact update and detection between spheres held by the uploaded bodies:
  * the contact part of DOM_Update_Begin (dom.c:3700-3790) for sphere pairs, on
  * the device bodies (rotation of b2dev_upload_scene, mass centre of

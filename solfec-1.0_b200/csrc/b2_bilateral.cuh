@@ -27,13 +27,17 @@
 
 namespace b2 {
 
-__global__ void k_constraints_update(int n, const int* kind, const int* master, const int* slave, const double* rot,
-                                     const double* x, const double* x0, double* mpnt, const double* spnt,
-                                     double* base, double* gap, double* Z) {
+__global__ void k_constraints_update(int n, int nbod, const int* kind, const int* master, const int* slave,
+                                     const double* rot, const double* x, const double* x0, double* mpnt,
+                                     const double* spnt, double* base, double* gap, double* Z, int* bad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int k = kind[i];
   const int m = master[i], s = slave[i];
+  if ((k == CON_RIGLNK || k == CON_FIXDIR) && (m < 0 || m >= nbod || s < -1 || s >= nbod)) {
+    atomicExch(bad, 1);  // invalid body index: the row is left as it is
+    return;
+  }
   if (k == CON_RIGLNK) {
     double pm[3], ps[3];
     cur_point(rot + 9 * (size_t)m, x + 3 * (size_t)m, x0 + 3 * (size_t)m, mpnt + 3 * (size_t)i, pm);
@@ -70,6 +74,41 @@ __global__ void k_constraints_update(int n, const int* kind, const int* master, 
 #pragma unroll
     for (int q = 0; q < 9; q++) base[9 * (size_t)i + q] = b[q];
   }
+}
+
+// The bilateral constraints kept across detections as rows n0 .. n0+nc-1 of
+// the detection's output, after its contacts: bodies, points and frame as
+// set up, gap 0 until b2dev_update_constraints, no material, key -1 (never
+// matched by the next detection), kind and Z into the caller-order kind
+// planes; R, U carried from the previous detection's constraint rows when
+// pR is given (the same constraints), else zero.
+__global__ void k_constraints_append(int n0, int nc, const int* kind, const int* master, const int* slave,
+                                     const double* mpnt, const double* spnt, const double* base, const double* Z,
+                                     const double* pR, const double* pU, ContactOut o, int* kind_c, double* Z_c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nc) return;
+  const size_t i = (size_t)n0 + j;
+  o.master[i] = master[j];
+  o.slave[i] = slave[j];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    o.point[3 * i + q] = mpnt[3 * (size_t)j + q];
+    o.mpnt[3 * i + q] = mpnt[3 * (size_t)j + q];
+    o.spnt[3 * i + q] = spnt[3 * (size_t)j + q];
+    o.R0[3 * i + q] = pR ? pR[3 * (size_t)j + q] : 0.0;
+    o.U0[3 * i + q] = pU ? pU[3 * (size_t)j + q] : 0.0;
+  }
+#pragma unroll
+  for (int q = 0; q < 9; q++) o.base[9 * i + q] = base[9 * (size_t)j + q];
+  o.gap[i] = 0.0;
+  o.fric[i] = o.rest[i] = o.coh[i] = 0.0;
+  o.key[i] = -1;
+  o.slave_lo[i] = 0;
+  o.isnew[i] = 0;
+  o.area[i] = 0.0;
+  kind_c[i] = kind[j];
+#pragma unroll
+  for (int q = 0; q < 4; q++) Z_c[4 * i + q] = Z[4 * (size_t)j + q];
 }
 
 }  // namespace b2

@@ -216,6 +216,11 @@ struct b2dev_ctx {
   Buf st_master, st_slave, st_point, st_mpnt, st_spnt, st_base, st_gap, st_fric, st_rest, st_coh, st_R0, st_U0,
       st_key, st_slo, st_new, st_area;
   Buf det_point, det_R0, det_U0, det_key, det_slo, det_new, det_area;
+  // bilateral constraints listed after the detected contacts by every
+  // detection (b2dev_constraints_setup): kind, bodies, points, frame and Z of
+  // each; det_ncont counts the contacts among the last detection's rows
+  int cn_n = 0, det_ncont = 0;
+  Buf cn_kind, cn_master, cn_slave, cn_mpnt, cn_spnt, cn_base, cn_Z;
   // convexes of the detection (b2dev_convexes_setup): their data, the
   // adjacency of convexes of one body, and the convex-convex sweep
   int nconv = 0;
@@ -916,7 +921,8 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->cvx_surf, &c->cvx_ns, &c->cvx_cur, &c->cvx_pla, &c->cvx_box, &c->cvx_aptr, &c->cvx_adj,
                 &c->cc_lox, &c->cc_idx, &c->cc_sidx, &c->cc_cnt, &c->cc_off, &c->cc_keys, &c->cc_keys_s,
                 &c->cc_cell, &c->cc_hkey, &c->cc_hkey_s, &c->cc_large, &c->cc_bstart, &c->cc_bend, &c->cc_misc, &c->cc_keep, &c->cc_cls, &c->cc_order, &c->ex_bodies, &c->ex_surf,
-                &c->st_area, &c->det_area,
+                &c->st_area, &c->det_area, &c->cn_kind, &c->cn_master, &c->cn_slave, &c->cn_mpnt, &c->cn_spnt,
+                &c->cn_base, &c->cn_Z,
                 &c->topo_m, &c->topo_s, &c->topo_o, &c->topo_flag, &c->blkrow};
   for (Buf* b : all)
     if (b->p) cudaFree(b->p);
@@ -960,6 +966,8 @@ int b2dev_upload_scene(b2dev_ctx* c, int nbod, const double* rot, const double* 
   c->det_valid = c->det_assembled = false;
   c->ready = false;
   c->has_kinds = false;   // new constraints: all contacts until b2dev_set_kinds
+  c->cn_n = 0;            // constraints kept across detections refer to the old bodies
+  c->det_ncont = 0;
   return B2DEV_OK;
 }
 
@@ -1342,13 +1350,50 @@ int b2dev_update_constraints(b2dev_ctx* c) {
   if (!c || !c->have_rigid) { set_err("update_constraints: no rigid bodies set up"); return B2DEV_ESTATE; }
   if (!c->has_kinds || c->ncon == 0) return B2DEV_OK;  // contacts only: nothing to update
   DeviceGuard g(c->device);
+  B2_TRY(ensure(c->bad, sizeof(int)));
+  B2_CK(cudaMemsetAsync(c->bad.p, 0, sizeof(int), c->stream));
   c->launches++;
   k_constraints_update<<<blocks_for(c->ncon, 128), 128, 0, c->stream>>>(
-      c->ncon, ptr<int>(c->kind_c), ptr<int>(c->master), ptr<int>(c->slave), ptr<double>(c->rot),
+      c->ncon, c->nbod, ptr<int>(c->kind_c), ptr<int>(c->master), ptr<int>(c->slave), ptr<double>(c->rot),
       ptr<double>(c->rb_x), ptr<double>(c->x0), ptr<double>(c->mpnt), ptr<double>(c->spnt), ptr<double>(c->base),
-      ptr<double>(c->gap_c), ptr<double>(c->Z_c));
+      ptr<double>(c->gap_c), ptr<double>(c->Z_c), ptr<int>(c->bad));
   B2_CK(cudaGetLastError());
+  int bad = 0;
+  B2_CK(cudaMemcpyAsync(&bad, c->bad.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  B2_CK(cudaStreamSynchronize(c->stream));
+  if (bad) { set_err("update_constraints: a constraint's body index is out of range"); return B2DEV_EINVAL; }
   c->ready = false;  // frames and gaps changed: the local dynamics must be assembled again
+  return B2DEV_OK;
+}
+
+int b2dev_constraints_setup(b2dev_ctx* c, int n, const int* kind, const int* master, const int* slave,
+                            const double* mpnt, const double* spnt, const double* base, const double* Z) {
+  if (!c || !c->have_scene) { set_err("constraints_setup: no scene uploaded"); return B2DEV_ESTATE; }
+  if (n < 0 || (n > 0 && (!kind || !master || !slave || !mpnt || !spnt || !base || !Z))) {
+    set_err("constraints_setup: %d constraints need kind, bodies, points, base and Z", n);
+    return B2DEV_EINVAL;
+  }
+  for (int j = 0; j < n; j++) {
+    if (kind[j] < CON_FIXPNT || kind[j] > CON_RIGLNK) {
+      set_err("constraints_setup: constraint %d: kind %d is not FIXPNT, FIXDIR, VELODIR, VELODIR3 or RIGLNK (1-5)",
+              j, kind[j]);
+      return B2DEV_EUNSUPPORTED;
+    }
+    if (master[j] < 0 || master[j] >= c->nbod || slave[j] < -1 || slave[j] >= c->nbod || slave[j] == master[j]) {
+      set_err("constraints_setup: constraint %d: bodies %d, %d out of range or equal", j, master[j], slave[j]);
+      return B2DEV_EINVAL;
+    }
+  }
+  DeviceGuard g(c->device);
+  B2_TRY(upload(c, c->cn_kind, kind, (size_t)n, 0));
+  B2_TRY(upload(c, c->cn_master, master, (size_t)n, 0));
+  B2_TRY(upload(c, c->cn_slave, slave, (size_t)n, 0));
+  B2_TRY(upload(c, c->cn_mpnt, mpnt, (size_t)3 * n, 0));
+  B2_TRY(upload(c, c->cn_spnt, spnt, (size_t)3 * n, 0));
+  B2_TRY(upload(c, c->cn_base, base, (size_t)9 * n, 0));
+  B2_TRY(upload(c, c->cn_Z, Z, (size_t)4 * n, 0));
+  B2_CK(cudaStreamSynchronize(c->stream));
+  c->cn_n = n;
   return B2DEV_OK;
 }
 
@@ -1575,22 +1620,29 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
 
   // the previous step's contacts: keys, roles and their R, U (the last solve's
   // state when it was assembled from them, else the values they were given)
-  int nprev = c->det_valid ? c->ncon : 0;
+  // (rows: the contacts, then the constraints kept across detections; only
+  // the contacts' keys are matched, the constraints carry by position)
+  const int nrow_prev = c->det_valid ? c->ncon : 0;
+  const int nprev = c->det_valid ? c->det_ncont : 0;
+  const bool carry_cn = c->cn_n > 0 && c->det_valid && nrow_prev - nprev == c->cn_n;
   B2_TRY(ensure(c->sph_pkey, sizeof(long long) * (nprev + 1)));
   B2_TRY(ensure(c->sph_pslo, sizeof(int) * (nprev + 1)));
-  B2_TRY(ensure(c->sph_pR, sizeof(double) * 3 * (nprev + 1)));
-  B2_TRY(ensure(c->sph_pU, sizeof(double) * 3 * (nprev + 1)));
+  B2_TRY(ensure(c->sph_pR, sizeof(double) * 3 * (nrow_prev + 1)));
+  B2_TRY(ensure(c->sph_pU, sizeof(double) * 3 * (nrow_prev + 1)));
   if (nprev > 0) {
     B2_CK(cudaMemcpyAsync(c->sph_pkey.p, c->det_key.p, sizeof(long long) * nprev, cudaMemcpyDeviceToDevice, st));
     B2_CK(cudaMemcpyAsync(c->sph_pslo.p, c->det_slo.p, sizeof(int) * nprev, cudaMemcpyDeviceToDevice, st));
-    if (c->det_assembled && c->n == nprev && c->state_u) {
+  }
+  if (nrow_prev > 0) {
+    if (c->det_assembled && c->n == nrow_prev && c->state_u) {
       c->launches++;
-      k_state_out<<<blocks_for(nprev, T), T, 0, st>>>(nprev, ptr<int>(c->perm), ptr<double4>(c->R64[c->state_r]),
-                                                       ptr<double4>(*c->state_u), nullptr, 1.0,
-                                                       ptr<double>(c->sph_pR), ptr<double>(c->sph_pU), nullptr);
+      k_state_out<<<blocks_for(nrow_prev, T), T, 0, st>>>(nrow_prev, ptr<int>(c->perm),
+                                                           ptr<double4>(c->R64[c->state_r]), ptr<double4>(*c->state_u),
+                                                           nullptr, 1.0, ptr<double>(c->sph_pR),
+                                                           ptr<double>(c->sph_pU), nullptr);
     } else {
-      B2_CK(cudaMemcpyAsync(c->sph_pR.p, c->det_R0.p, sizeof(double) * 3 * nprev, cudaMemcpyDeviceToDevice, st));
-      B2_CK(cudaMemcpyAsync(c->sph_pU.p, c->det_U0.p, sizeof(double) * 3 * nprev, cudaMemcpyDeviceToDevice, st));
+      B2_CK(cudaMemcpyAsync(c->sph_pR.p, c->det_R0.p, sizeof(double) * 3 * nrow_prev, cudaMemcpyDeviceToDevice, st));
+      B2_CK(cudaMemcpyAsync(c->sph_pU.p, c->det_U0.p, sizeof(double) * 3 * nrow_prev, cudaMemcpyDeviceToDevice, st));
     }
   }
 
@@ -1809,26 +1861,28 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
   }
   npair = nps + ncc;
 
-  // contacts of the pairs, in pair order
+  // contacts of the pairs, in pair order (row arrays with room for the
+  // constraints that follow them)
   const size_t np1 = (size_t)npair + 1;
+  const size_t nr1 = np1 + (size_t)c->cn_n;
   B2_TRY(ensure(c->sph_pi, sizeof(int) * np1));
   B2_TRY(ensure(c->sph_pj, sizeof(int) * np1));
-  B2_TRY(ensure(c->st_master, sizeof(int) * np1));
-  B2_TRY(ensure(c->st_slave, sizeof(int) * np1));
-  B2_TRY(ensure(c->st_point, sizeof(double) * 3 * np1));
-  B2_TRY(ensure(c->st_mpnt, sizeof(double) * 3 * np1));
-  B2_TRY(ensure(c->st_spnt, sizeof(double) * 3 * np1));
-  B2_TRY(ensure(c->st_base, sizeof(double) * 9 * np1));
-  B2_TRY(ensure(c->st_gap, sizeof(double) * np1));
-  B2_TRY(ensure(c->st_fric, sizeof(double) * np1));
-  B2_TRY(ensure(c->st_rest, sizeof(double) * np1));
-  B2_TRY(ensure(c->st_coh, sizeof(double) * np1));
-  B2_TRY(ensure(c->st_R0, sizeof(double) * 3 * np1));
-  B2_TRY(ensure(c->st_U0, sizeof(double) * 3 * np1));
-  B2_TRY(ensure(c->st_key, sizeof(long long) * np1));
-  B2_TRY(ensure(c->st_slo, sizeof(int) * np1));
-  B2_TRY(ensure(c->st_new, sizeof(int) * np1));
-  B2_TRY(ensure(c->st_area, sizeof(double) * np1));
+  B2_TRY(ensure(c->st_master, sizeof(int) * nr1));
+  B2_TRY(ensure(c->st_slave, sizeof(int) * nr1));
+  B2_TRY(ensure(c->st_point, sizeof(double) * 3 * nr1));
+  B2_TRY(ensure(c->st_mpnt, sizeof(double) * 3 * nr1));
+  B2_TRY(ensure(c->st_spnt, sizeof(double) * 3 * nr1));
+  B2_TRY(ensure(c->st_base, sizeof(double) * 9 * nr1));
+  B2_TRY(ensure(c->st_gap, sizeof(double) * nr1));
+  B2_TRY(ensure(c->st_fric, sizeof(double) * nr1));
+  B2_TRY(ensure(c->st_rest, sizeof(double) * nr1));
+  B2_TRY(ensure(c->st_coh, sizeof(double) * nr1));
+  B2_TRY(ensure(c->st_R0, sizeof(double) * 3 * nr1));
+  B2_TRY(ensure(c->st_U0, sizeof(double) * 3 * nr1));
+  B2_TRY(ensure(c->st_key, sizeof(long long) * nr1));
+  B2_TRY(ensure(c->st_slo, sizeof(int) * nr1));
+  B2_TRY(ensure(c->st_new, sizeof(int) * nr1));
+  B2_TRY(ensure(c->st_area, sizeof(double) * nr1));
   B2_TRY(ensure(c->sph_keep, sizeof(int) * np1));
   B2_TRY(ensure(c->sph_pos, sizeof(int) * np1));
   B2_TRY(ensure(c->sph_bcnt, sizeof(int) * (nb + 1)));
@@ -1890,7 +1944,7 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
   // the kept contacts become the scene's contacts: when nothing was removed
   // (the common case) the staged arrays are taken over as they are, else the
   // kept ones are compacted into the scene's arrays
-  const size_t nk1 = (size_t)nkeep + 1;
+  const size_t nk1 = (size_t)nkeep + 1 + (size_t)c->cn_n;
   if (npair > 0 && nkeep == npair) {
     std::swap(c->master, c->st_master); std::swap(c->slave, c->st_slave); std::swap(c->det_point, c->st_point);
     std::swap(c->mpnt, c->st_mpnt); std::swap(c->spnt, c->st_spnt); std::swap(c->base, c->st_base);
@@ -1928,6 +1982,27 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
                                                          d);
     }
   }
+  if (c->cn_n > 0) {  // the constraints kept across detections follow the contacts
+    ContactOut d;
+    d.master = ptr<int>(c->master); d.slave = ptr<int>(c->slave); d.point = ptr<double>(c->det_point);
+    d.mpnt = ptr<double>(c->mpnt); d.spnt = ptr<double>(c->spnt); d.base = ptr<double>(c->base);
+    d.gap = ptr<double>(c->gap_c); d.fric = ptr<double>(c->fric_c); d.rest = ptr<double>(c->rest_c);
+    d.coh = ptr<double>(c->coh_c); d.R0 = ptr<double>(c->det_R0); d.U0 = ptr<double>(c->det_U0);
+    d.key = ptr<long long>(c->det_key); d.slave_lo = ptr<int>(c->det_slo); d.isnew = ptr<int>(c->det_new);
+    d.area = ptr<double>(c->det_area);
+    B2_TRY(ensure(c->kind_c, sizeof(int) * nk1));
+    B2_TRY(ensure(c->Z_c, sizeof(double) * 4 * nk1));
+    if (nkeep > 0) {
+      B2_CK(cudaMemsetAsync(c->kind_c.p, 0, sizeof(int) * nkeep, st));
+      B2_CK(cudaMemsetAsync(c->Z_c.p, 0, sizeof(double) * 4 * nkeep, st));
+    }
+    c->launches++;
+    k_constraints_append<<<blocks_for(c->cn_n, 128), 128, 0, st>>>(
+        nkeep, c->cn_n, ptr<int>(c->cn_kind), ptr<int>(c->cn_master), ptr<int>(c->cn_slave), ptr<double>(c->cn_mpnt),
+        ptr<double>(c->cn_spnt), ptr<double>(c->cn_base), ptr<double>(c->cn_Z),
+        carry_cn ? ptr<double>(c->sph_pR) + 3 * (size_t)nprev : nullptr,
+        carry_cn ? ptr<double>(c->sph_pU) + 3 * (size_t)nprev : nullptr, d, ptr<int>(c->kind_c), ptr<double>(c->Z_c));
+  }
   if (npair > 0) {  // new contacts kept
     B2_TRY(ensure(c->sph_cnt, sizeof(int) * nk1));
     size_t bytes = 0;
@@ -1938,8 +2013,9 @@ int b2dev_detect_spheres(b2dev_ctx* c, int* ncon, int* nnew) {
   }
   B2_CK(cudaGetLastError());
   B2_CK(cudaStreamSynchronize(st));
-  c->ncon = nkeep;
-  c->has_kinds = false;
+  c->ncon = nkeep + c->cn_n;
+  c->det_ncont = nkeep;
+  c->has_kinds = c->cn_n > 0;
   c->det_valid = true;
   c->det_assembled = false;
   c->ready = false;  // the local dynamics must be assembled for the new contacts
@@ -1962,7 +2038,7 @@ int b2dev_get_contacts(b2dev_ctx* c, int* master, int* slave, double* point, dou
   if (!c || !c->det_valid) { set_err("get_contacts: no detection"); return B2DEV_ESTATE; }
   DeviceGuard g(c->device);
   cudaStream_t st = c->stream;
-  const size_t n = (size_t)c->ncon;
+  const size_t n = (size_t)c->det_ncont;  // the contacts (constraint rows follow them)
   const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   if (n > 0) {
     if (master) B2_CK(cudaMemcpyAsync(master, c->master.p, sizeof(int) * n, kd, st));
@@ -1988,8 +2064,8 @@ int b2dev_get_contact_area(b2dev_ctx* c, double* area, int on_device) {
   if (!c || !c->det_valid) { set_err("get_contact_area: no detection"); return B2DEV_ESTATE; }
   if (!area) { set_err("get_contact_area: null output"); return B2DEV_EINVAL; }
   DeviceGuard g(c->device);
-  if (c->ncon > 0)
-    B2_CK(cudaMemcpyAsync(area, c->det_area.p, sizeof(double) * c->ncon,
+  if (c->det_ncont > 0)
+    B2_CK(cudaMemcpyAsync(area, c->det_area.p, sizeof(double) * c->det_ncont,
                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
   B2_CK(cudaStreamSynchronize(c->stream));
   return B2DEV_OK;

@@ -79,6 +79,7 @@ _SIGNATURES = {
     'b2dev_rigid_step_end': (C.c_int, [C.c_void_p, C.c_double]),
     'b2dev_rigid_get': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     'b2dev_update_constraints': (C.c_int, [C.c_void_p]),
+    'b2dev_constraints_setup': (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 7),
     'b2dev_spheres_setup': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                       C.c_void_p, C.c_int]),
     'b2dev_detect_spheres': (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),

@@ -92,6 +92,7 @@ class SPHERES:
         self._mat = material_table(material)
         self.ncon = 0
         self.nnew = 0
+        self.ncons = 0
         _check(lib().b2dev_spheres_setup(ldy.device_context, n, ptr(self._body), ptr(self._centre),
                                          ptr(self._radius), ptr(self._surface), int(self._mat.shape[0]),
                                          ptr(self._mat), 0), 'b2dev_spheres_setup')
@@ -113,6 +114,20 @@ class SPHERES:
         _check(lib().b2dev_convexes_setup(self.ldy.device_context, nc, *[ptr(a) for a in self._cvx]),
                'b2dev_convexes_setup')
         self.nconv = nc
+
+    def set_constraints(self, kinds, master, slave, mpnt, spnt, base, Z):
+        """Bilateral constraints kept across detections (b2dev_constraints_setup):
+        per constraint its kind (1-5, dom.h:98), master and slave body (-1:
+        none, spnt then a spatial point), referential points, base (column-major
+        9) and Z (4; RIGLNK: Z[3] the link length). Every detect() lists them
+        after its contacts; RIGID_DYNAMICS.update_constraints refreshes RIGLNK
+        and two-body FIXDIR frames from the moved bodies."""
+        n = int(np.asarray(kinds).reshape(-1).shape[0])
+        self._cons = [_i32(kinds, n), _i32(master, n), _i32(slave, n), _f64(mpnt, 3 * n), _f64(spnt, 3 * n),
+                      _f64(base, 9 * n), _f64(Z, 4 * n)]
+        _check(lib().b2dev_constraints_setup(self.ldy.device_context, n, *[ptr(a) for a in self._cons]),
+               'b2dev_constraints_setup')
+        self.ncons = n
 
     def sparsify(self, threshold=0.01, minarea=0.0, mindist=1e-6):
         """CONTACT_SPARSIFY (lng.c:8875-8899) for the sparsification of new
@@ -212,25 +227,31 @@ def bodies_only(scene):
 
 
 def run_spheres(scene, spheres: dict, gs, nsteps: int, J, mass, gravity=(0.0, 0.0, 0.0), callback=None,
-                scheme=None, ldy: LOCDYN = None):
+                scheme=None, ldy: LOCDYN = None, constraints: dict = None):
     """Time loop of a sphere scene with contact detection on the device.
 
     scene: bodies (its contacts are ignored); spheres: keyword arguments of
-    SPHERES (body, centre, radius, surface, material, convex). Every step: bodies to
-    t + h/2 and free velocities, contact update and detection, local dynamics,
-    R and U carried over, GAUSS_SEIDEL solve, reactions and second half step.
-    callback(k, dyn, sph, ldy) after step k (from 1); False stops the loop.
-    Returns (RIGID_DYNAMICS, SPHERES, LOCDYN)."""
+    SPHERES (body, centre, radius, surface, material, convex); constraints:
+    None or the keyword arguments of SPHERES.set_constraints. Every step:
+    bodies to t + h/2 and free velocities, contact update and detection, the
+    constraints' frames, local dynamics, R and U carried over, GAUSS_SEIDEL
+    solve, reactions and second half step. callback(k, dyn, sph, ldy) after
+    step k (from 1); False stops the loop. Returns (RIGID_DYNAMICS, SPHERES,
+    LOCDYN)."""
     if ldy is None:
         ldy = LOCDYN()
     ldy.update_begin(bodies_only(scene))
     dyn = RIGID_DYNAMICS(ldy, J, mass, scene.x, scheme)
     sph = SPHERES(ldy, **spheres)
+    if constraints is not None:
+        sph.set_constraints(**constraints)
     h = float(scene.step)
     for k in range(1, int(nsteps) + 1):
         dyn.step_begin(h, gravity)
         nc, _ = sph.detect()
-        if nc > 0:
+        if sph.ncons > 0:
+            dyn.update_constraints()
+        if nc + sph.ncons > 0:
             _check(lib().b2gs_locdyn_update_begin_resident(ldy.handle, h, int(scene.dynamic)),
                    'LOCDYN_Update_Begin')
             sph.carry_state()

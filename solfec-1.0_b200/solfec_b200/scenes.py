@@ -643,6 +643,57 @@ def math_pendulum(step: float = 1e-3):
                           [[1.0, 0.0, 1.0]], [[0.0, 0.0, 1.0]], base, [0.0], [[link[0], link[1], link[2], 1.0]])
 
 
+DOUBLE_PENDULUM_GRAVITY = 9.81
+
+
+def _length(v) -> float:
+    """LEN of alg.h: sqrt of the dot product summed left to right."""
+    return math.sqrt(float(v[0]) * float(v[0]) + float(v[1]) * float(v[1]) + float(v[2]) * float(v[2]))
+
+
+def double_pendulum(step: float = 1e-3):
+    """The scene of the reference's tests/double-pendulum.py: two rigid balls
+    (SPHERE radius 0.05, surface 1, mass 1, unit inertia) hanging from the
+    fixed point a = (0, 0, 2) by two rigid links of length 1: ball 1 at
+    b = a + (sin 60, 0, -cos 60) linked to a, ball 2 at c = b + (sin 36, 0,
+    -cos 36) linked to ball 1 (PUT_RIGID_LINK (bod2, bod1, c, b)); a fixed
+    0.05 x 0.4 x 2 box (HEX obstacle, surfaces 0) at x in [-0.1, -0.05] that
+    the balls strike; SIGNORINI_COULOMB with restitution 0.1, no friction;
+    gravity 9.81 (DOUBLE_PENDULUM_GRAVITY). The test sets GEOMETRIC_EPSILON to
+    1e-5; the device detection keeps the default 1e-6.
+    Returns (scene without contacts, SPHERES arguments with the box as
+    `convex`, SPHERES.set_constraints arguments, J, mass)."""
+    x1, z1 = math.sin(math.pi / 3.0), -math.cos(math.pi / 3.0)
+    x2, z2 = x1 + math.sin(math.pi / 5.0), z1 - math.cos(math.pi / 5.0)
+    a = np.array([0.0, 0.0, 2.0])
+    b = np.array([x1, 0.0, 2.0 + z1])
+    c = np.array([x2, 0.0, 2.0 + z2])
+    lo, hi = np.array([-0.10, -0.2, 0.0]), np.array([-0.05, 0.2, 2.0])
+    x = np.stack([b, c, 0.5 * (lo + hi)])
+    nb = 3
+    jinv = np.zeros((nb, 9)); jinv[:2] = np.eye(3).reshape(9)
+    mass = np.ones(nb)
+    z = np.zeros((nb, 6)); e = np.zeros(0)
+    sc = Scene(name='double-pendulum', step=step, dynamic=1, rot=np.tile(np.eye(3).reshape(9), (nb, 1)), x=x.copy(),
+               x0=x.copy(), jinv=jinv, minv=np.array([1.0, 1.0, 0.0]), velo=z.copy(), velo0=z.copy(),
+               obstacle=np.array([0, 0, 1], np.int32), master=np.zeros(0, np.int32), slave=np.zeros(0, np.int32),
+               mpnt=np.zeros((0, 3)), spnt=np.zeros((0, 3)), base=np.zeros((0, 9)), gap=e, friction=e,
+               restitution=e, cohesion=e, mass=mass, radius=np.array([0.05, 0.05, 0.0]))
+    v, f = box_convex(lo, hi)
+    convex = dict(body=np.array([2], np.int32), vptr=np.array([0, 8], np.int32), vert=v,
+                  fptr=np.array([0, f.shape[0]], np.int32), fac=f, sptr=np.array([0, 6], np.int32),
+                  surf=np.zeros(6, np.int32))
+    mat = np.zeros((2, 2, 2)); mat[:, :, 1] = 0.1
+    spheres = dict(body=np.array([0, 1], np.int32), centre=np.stack([b, c]), radius=np.array([0.05, 0.05]),
+                   surface=np.array([1, 1], np.int32), material=mat, convex=convex)
+    base = np.tile(np.eye(3).reshape(9), (2, 1))  # replaced by the first update_riglnk
+    constraints = dict(kinds=np.array([5, 5], np.int32), master=np.array([0, 1], np.int32),
+                       slave=np.array([-1, 0], np.int32), mpnt=np.stack([b, c]), spnt=np.stack([a, b]), base=base,
+                       Z=np.array([[0.0, 0.0, 1.0, _length(b - a)], [0.0, 0.0, 1.0, _length(c - b)]]))
+    J = np.tile(np.eye(3).reshape(9), (nb, 1))
+    return sc, spheres, constraints, J, mass
+
+
 PINNED_BAR_GRAVITY = 9.8
 
 

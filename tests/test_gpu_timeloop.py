@@ -228,3 +228,53 @@ def test_math_pendulum_through_run_fixed_contacts():
     ldy.close()
     ref = pin('math_pendulum_ref.json')
     assert state['period'] is not None and abs(state['period'] - ref['value']) / ref['value'] < ref['tolerance']
+
+
+def test_double_pendulum_energy():
+    """The reference's tests/double-pendulum.py on the device: two RIGLNK rows
+    kept across detections (b2dev_constraints_setup) after the sphere-box
+    contacts of every step's detection, the links' frames refreshed on the
+    device, 2500 steps; detection, reactions, iterations and bodies bitwise
+    with the CPU restatements at every step, and the total energy at the
+    test's five pinned indices within its 1e-3."""
+    from solfec_b200.detect import SPHERES, bodies_only
+    from test_rigid_cpu import (check_double_pendulum_pins, double_pendulum_energy, double_pendulum_state,
+                                double_pendulum_step_cpu)
+    sc, sph, cons, J, mass = scenes.double_pendulum()
+    h = sc.step
+    g = (0.0, 0.0, -scenes.DOUBLE_PENDULUM_GRAVITY)
+    ldy = LOCDYN()
+    ldy.update_begin(bodies_only(sc))
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    s = SPHERES(ldy, **sph)
+    s.set_constraints(**cons)
+    gs = GAUSS_SEIDEL_SOLVER(1e-3, 1000, failure='EXIT')
+    bd = ro.Bodies(sc.rot, sc.x, sc.velo, J, sc.jinv, mass, sc.minv, sc.x0, sc.obstacle)
+    state = double_pendulum_state(cons)
+    tot, hits = [double_pendulum_energy(bd)], 0
+    for k in range(2500):
+        dyn.step_begin(h, g)
+        nc, _ = s.detect()
+        dyn.update_constraints()
+        assert lib().b2gs_locdyn_update_begin_resident(ldy.handle, h, 1) == 0
+        s.carry_state()
+        gs.solve(ldy)
+        R, U, _ = ldy.get_state()
+        det, _, Ro, Uo, out = double_pendulum_step_cpu(bd, sc, sph, cons, state, order=ldy.order(), epsilon=1e-3,
+                                                       maxiter=1000, failure='EXIT')
+        assert nc == det['key'].shape[0], k
+        if nc:
+            dev = s.contacts()
+            for key in ('key', 'master', 'slave', 'mpnt', 'spnt', 'base', 'gap'):
+                assert same_bits(dev[key], det[key]), (k, key)
+            hits += 1
+        assert gs.iters == out['iters'], (k, gs.iters, out['iters'])
+        assert same_bits(R, Ro) and same_bits(U, Uo), k
+        dyn.step_end(h)
+        st = dyn.state()
+        for key in ('rot', 'x', 'velo'):
+            assert same_bits(st[key], np.array(getattr(bd, key))), (k, key)
+        tot.append(double_pendulum_energy(bd))
+    ldy.close()
+    assert hits > 5
+    check_double_pendulum_pins(tot)

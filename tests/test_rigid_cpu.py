@@ -207,6 +207,93 @@ def test_pinned_bar_cpu(impl):
     assert max(drift) < 1e-6, max(drift)
 
 
+def double_pendulum_energy(bd):
+    """Total energy as tests/double-pendulum.py:93-97 forms it: the kinetic
+    energy plus m g max(z, 0) of both balls."""
+    g = scenes.DOUBLE_PENDULUM_GRAVITY
+    return sum(ro.kinetic_energy(bd, b) + bd.mass[b] * g * max(bd.x[b][2], 0.0) for b in range(2))
+
+
+def double_pendulum_step_cpu(bd, sc, sph, cons, state, impl='oracle', **kw):
+    """One step of the double pendulum on the CPU restatements: step begin,
+    the links' update, contact update and detection (oracle_detect.c, carried
+    R, U by pair key), the rows (contacts, then the links), assembly, solve
+    with the kinds, step end. state: the carried detection, link frames and
+    link reactions (updated in place). Returns (detection, rows, R, U, out)."""
+    h = sc.step
+    ro.step_begin(bd, h, (0.0, 0.0, -scenes.DOUBLE_PENDULUM_GRAVITY))
+    cm, cb, cg, cZ = state['mpnt'], state['base'], state['gap'], state['Z']
+    ro.update_constraints(bd, cons['kinds'], cons['master'], cons['slave'], cm, cons['spnt'], cb, cg, cZ)
+    det = oracle.detect_spheres(sph['body'], sph['centre'], sph['radius'], sph['surface'], np.array(bd.rot),
+                                np.array(bd.x), sc.x0, sc.obstacle, sph['material'], state['prev'],
+                                convex=sph['convex'])
+    n1, nc = det['key'].shape[0], cons['kinds'].shape[0]
+    rows = dataclasses.replace(
+        sc, rot=np.array(bd.rot), x=np.array(bd.x), velo=np.array(bd.velo), velo0=np.array(bd.velo0),
+        master=np.concatenate([det['master'], cons['master']]).astype(np.int32),
+        slave=np.concatenate([det['slave'], cons['slave']]).astype(np.int32),
+        mpnt=np.concatenate([det['mpnt'].reshape(-1, 3), cm]), spnt=np.concatenate([det['spnt'].reshape(-1, 3),
+                                                                                     cons['spnt']]),
+        base=np.concatenate([det['base'].reshape(-1, 9), cb]), gap=np.concatenate([det['gap'], cg]),
+        friction=np.concatenate([det['friction'], np.zeros(nc)]),
+        restitution=np.concatenate([det['restitution'], np.zeros(nc)]), cohesion=np.zeros(n1 + nc))
+    kinds = np.concatenate([np.zeros(n1, np.int32), cons['kinds']])
+    Z = np.concatenate([np.zeros((n1, 4)), cZ])
+    R0 = np.concatenate([det['R'].reshape(-1, 3), state['R']])
+    U0 = np.concatenate([det['U'].reshape(-1, 3), state['U']])
+    order = kw.pop('order', None)
+    ld = oracle.assemble(rows)
+    if order is None:
+        order = np.arange(n1 + nc)
+    out = oracle.solve(ld.permuted(order), R0[order].ravel(), U0[order].ravel(), kinds=kinds[order], Z=Z[order],
+                       impl=impl, **kw)
+    R = np.empty((n1 + nc, 3)); U = np.empty((n1 + nc, 3))
+    R[order] = out['R'].reshape(-1, 3); U[order] = out['U'].reshape(-1, 3)
+    state['R'], state['U'] = R[n1:], U[n1:]
+    state['prev'] = dict(key=det['key'], slave_lo=det['slave_lo'], R=R[:n1], U=U[:n1])
+    ro.step_end(bd, h, rows.master, rows.slave, rows.mpnt, rows.spnt, rows.base, R)
+    return det, rows, R, U, out
+
+
+def double_pendulum_state(cons):
+    n = cons['kinds'].shape[0]
+    return dict(prev=None, mpnt=np.array(cons['mpnt'], float).reshape(n, 3).copy(),
+                base=np.array(cons['base'], float).reshape(n, 9).copy(), gap=np.zeros(n),
+                Z=np.array(cons['Z'], float).reshape(n, 4).copy(), R=np.zeros((n, 3)), U=np.zeros((n, 3)))
+
+
+def check_double_pendulum_pins(tot):
+    """tests/double-pendulum.py:93-115: the total energy shifted by its last
+    value, at the pinned indices, within 1e-3 relative to max(1, value)."""
+    ref = pin('double_pendulum_ref.json')
+    tot = np.asarray(tot) - tot[-1]
+    for p in ref['pins']:
+        err = abs(tot[p['index']] - p['value']) / max(1.0, p['value'])
+        assert err <= ref['tolerance'], (p, tot[p['index']], err)
+
+
+@pytest.mark.parametrize('impl', ['oracle', 'ref'])
+def test_double_pendulum_energy_cpu(impl):
+    """The reference's tests/double-pendulum.py: two balls on rigid links
+    (RIGLNK to a fixed point and between the balls) strike a fixed box
+    (sphere-convex contacts, restitution 0.1) over 2.5 s of 1 ms steps,
+    GAUSS_SEIDEL_SOLVER (1E-3, 1000, failure = 'EXIT'); the total energy at
+    the five pinned indices within the test's 1e-3."""
+    if impl == 'ref' and not oracle.ref_available():
+        pytest.skip('compiled reference solver not built')
+    sc, sph, cons, J, mass = scenes.double_pendulum()
+    bd = ro.Bodies(sc.rot, sc.x, sc.velo, J, sc.jinv, mass, sc.minv, sc.x0, sc.obstacle)
+    state = double_pendulum_state(cons)
+    tot, hits = [double_pendulum_energy(bd)], 0
+    for _ in range(2500):
+        det, _, _, _, _ = double_pendulum_step_cpu(bd, sc, sph, cons, state, impl, epsilon=1e-3, maxiter=1000,
+                                                   failure='EXIT')
+        hits += int(det['key'].shape[0] > 0)
+        tot.append(double_pendulum_energy(bd))
+    assert hits > 5  # the balls strike the box
+    check_double_pendulum_pins(tot)
+
+
 def test_expmap_rotation():
     rng = np.random.default_rng(5)
     for scale in (1e-6, 1e-2, 0.17, 0.18, 1.0, 3.0):
