@@ -21,9 +21,11 @@ struct ContactParams {
 
 // Solve A x = b (3x3, column-major, one right-hand side). Returns 0, or k > 0
 // when U(k,k) is exactly zero (b untouched), as LAPACK dgesv reports.
+template <bool RECIP = false>
 __device__ __forceinline__ int lu3_solve(double* a, double* b) {
   int ipiv[3];
   int info = 0;
+  double rpiv[3] = {0.0, 0.0, 0.0};  // RECIP: 1/U(j,j) where dgetf2 formed it (0: divide)
 #pragma unroll
   for (int j = 0; j < 3; j++) {
     int p = j;
@@ -49,6 +51,7 @@ __device__ __forceinline__ int lu3_solve(double* a, double* b) {
       double piv = a[j + 3 * j];
       if (fabs(piv) >= 2.2250738585072014e-308) {
         double r = 1.0 / piv;
+        if constexpr (RECIP) rpiv[j] = r;
 #pragma unroll
         for (int i = j + 1; i < 3; i++) a[i + 3 * j] *= r;
       } else {
@@ -89,7 +92,8 @@ __device__ __forceinline__ int lu3_solve(double* a, double* b) {
 #pragma unroll
   for (int k = 2; k >= 0; k--) {
     if (b[k] != 0.0) {
-      b[k] /= a[k + 3 * k];
+      if (RECIP && rpiv[k] != 0.0) b[k] *= rpiv[k];
+      else b[k] /= a[k + 3 * k];
 #pragma unroll
       for (int i = 0; i < k; i++) b[i] -= b[k] * a[i + 3 * k];
     }
@@ -246,7 +250,14 @@ static __device__ __noinline__ int de_saxce_feng(const ContactParams& cp, double
   return iter;
 }
 
-// semismooth_newton (dbs.c:142-303): the default diagonal solver.
+// semismooth_newton (dbs.c:142-303): the default diagonal solver. RECIP (the
+// FP32 sweeps of mixed precision only, which are not bitwise the reference's
+// anyway) shortens the solve's dependent chain of divisions: one reciprocal
+// where the reference divides several values by the same divisor (the slip
+// branch's norm and den, the stick branch's d2, the LU's pivots), the slip
+// branch's alfa delta as (R.d)/den (the same quantity), and the error test
+// squared; the results then differ from the reference's in the last bits.
+template <bool RECIP = false>
 __device__ __forceinline__ int semismooth_newton(const ContactParams& cp, double epsilon, int maxiter, double rho,
                                                  const double* W, const double* B, const double* V, double* U,
                                                  double* R) {
@@ -256,7 +267,8 @@ __device__ __forceinline__ int semismooth_newton(const ContactParams& cp, double
     return 0;
   }
   const double friction = cp.friction, cohesion = cp.cohesion;
-  int divi = maxiter / 10;
+  const int divi = maxiter / 10;
+  int until = divi;  // iterations left until rho grows (iter % divi == 0 without an integer division)
   int iter = 0;
   double error;
   do {
@@ -276,15 +288,29 @@ __device__ __forceinline__ int semismooth_newton(const ContactParams& cp, double
         if (lim > 0.0) {
           double len = sqrt(R[0] * R[0] + R[1] * R[1]);
           double den = B2_MAX(lim, len) * norm;
-          double e = lim / norm;
+          double rnorm = 0.0, rden = 0.0;
+          if constexpr (RECIP) { rnorm = 1.0 / norm; rden = 1.0 / den; }
+          double e = RECIP ? lim * rnorm : lim / norm;
           double beta;
-          if (len == 0.0) beta = 1.0;
-          else {
+          if constexpr (RECIP) {
+            // alfa delta = (R.d) / (len norm) min(len / lim, 1) = (R.d) / (max(lim, len) norm) = (R.d) / den,
+            // and alfa has the sign of R.d (0 when len = 0, where beta = 1)
+            const double rd = R[0] * d0 + R[1] * d1;
+            beta = (len != 0.0 && rd < 0.0) ? 1.0 / (1.0 - rd * rden) : 1.0;
+          } else if (len == 0.0) {
+            beta = 1.0;
+          } else {
             double alfa = (R[0] * d0 + R[1] * d1) / (len * norm);
             double delta = B2_MIN(len / lim, 1.0);
             beta = (alfa < 0.0 ? 1.0 / (1.0 - alfa * delta) : 1.0);
           }
-          double F0 = (R[0] * d0) / den, F1 = (R[1] * d0) / den, F2 = (R[0] * d1) / den, F3 = (R[1] * d1) / den;
+          double F0, F1, F2, F3;
+          if constexpr (RECIP) {
+            F0 = (R[0] * d0) * rden; F1 = (R[1] * d0) * rden; F2 = (R[0] * d1) * rden; F3 = (R[1] * d1) * rden;
+          } else {
+            F0 = (R[0] * d0) / den; F1 = (R[1] * d0) / den; F2 = (R[0] * d1) / den; F3 = (R[1] * d1) / den;
+          }
+          const double n0 = RECIP ? d0 * rnorm : d0 / norm, n1 = RECIP ? d1 * rnorm : d1 / norm;
           double M0 = e * (1.0 - F0), M1 = -e * F1, M2 = -e * F2, M3 = e * (1.0 - F3);
           double H0 = 1.0 - beta * M0, H1 = -beta * M1, H2 = -beta * M2, H3 = 1.0 - beta * M3;
           a[0] = H0 + rho * (M0 * W[0] + M2 * W[1]);
@@ -293,11 +319,11 @@ __device__ __forceinline__ int semismooth_newton(const ContactParams& cp, double
           a[3] = H2 + rho * (M0 * W[3] + M2 * W[4]);
           a[4] = H3 + rho * (M1 * W[3] + M3 * W[4]);
           a[5] = W[5];
-          a[6] = rho * (M0 * W[6] + M2 * W[7]) - friction * (d0 / norm);
-          a[7] = rho * (M1 * W[6] + M3 * W[7]) - friction * (d1 / norm);
+          a[6] = rho * (M0 * W[6] + M2 * W[7]) - friction * n0;
+          a[7] = rho * (M1 * W[6] + M3 * W[7]) - friction * n1;
           a[8] = W[8];
-          b[0] = friction * (d0 / norm) * (R[2] + cohesion) - R[0] - rho * (M0 * RES[0] + M2 * RES[1]);
-          b[1] = friction * (d1 / norm) * (R[2] + cohesion) - R[1] - rho * (M1 * RES[0] + M3 * RES[1]);
+          b[0] = friction * n0 * (R[2] + cohesion) - R[0] - rho * (M0 * RES[0] + M2 * RES[1]);
+          b[1] = friction * n1 * (R[2] + cohesion) - R[1] - rho * (M1 * RES[0] + M3 * RES[1]);
           b[2] = -UN - RES[2];
         } else {  // degenerate: homogeneous tangential tractions
           a[0] = 1.0; a[1] = 0.0; a[2] = W[2];
@@ -310,11 +336,20 @@ __device__ __forceinline__ int semismooth_newton(const ContactParams& cp, double
       } else {  // stick
         a[0] = W[0]; a[1] = W[1]; a[2] = W[2];
         a[3] = W[3]; a[4] = W[4]; a[5] = W[5];
-        a[6] = W[6] + U[0] / d2;
-        a[7] = W[7] + U[1] / d2;
         a[8] = W[8];
-        b[0] = -(1.0 + rho * U[2] / d2) * U[0] - RES[0];
-        b[1] = -(1.0 + rho * U[2] / d2) * U[1] - RES[1];
+        if constexpr (RECIP) {
+          const double rd2 = 1.0 / d2;
+          a[6] = W[6] + U[0] * rd2;
+          a[7] = W[7] + U[1] * rd2;
+          const double f = 1.0 + (rho * U[2]) * rd2;
+          b[0] = -f * U[0] - RES[0];
+          b[1] = -f * U[1] - RES[1];
+        } else {
+          a[6] = W[6] + U[0] / d2;
+          a[7] = W[7] + U[1] / d2;
+          b[0] = -(1.0 + rho * U[2] / d2) * U[0] - RES[0];
+          b[1] = -(1.0 + rho * U[2] / d2) * U[1] - RES[1];
+        }
         b[2] = -UN - RES[2];
       }
     } else {  // separation
@@ -323,7 +358,7 @@ __device__ __forceinline__ int semismooth_newton(const ContactParams& cp, double
       a[6] = 0.0; a[7] = 0.0; a[8] = 1.0;
       b[0] = -R[0]; b[1] = -R[1]; b[2] = -R[2];
     }
-    if (lu3_solve(a, b)) return -1;
+    if (lu3_solve<RECIP>(a, b)) return -1;
     if (!isfinite(b[0] + b[1] + b[2])) return -1;
     double c[3];
     nvaddmul(RES, W, b, c);
@@ -331,9 +366,15 @@ __device__ __forceinline__ int semismooth_newton(const ContactParams& cp, double
     U[0] += c[0]; U[1] += c[1]; U[2] += c[2];
     double e0 = R[0] - R00, e1 = R[1] - R01, e2 = R[2] - R02;
     error = dot3(R, R);
-    error = sqrt((e0 * e0 + e1 * e1 + e2 * e2) / B2_MAX(error, 1.0));
+    if (RECIP && epsilon * epsilon > 0.0) {  // error > epsilon compared squared: no division or root
+      const double d = e0 * e0 + e1 * e1 + e2 * e2, q = epsilon * epsilon * B2_MAX(error, 1.0);
+      error = d > q ? 2.0 * epsilon : 0.0;
+    } else {
+      error = sqrt((e0 * e0 + e1 * e1 + e2 * e2) / B2_MAX(error, 1.0));
+    }
     iter++;
-    if ((iter % divi) == 0) {
+    if (--until == 0) {
+      until = divi;
       rho *= 10.0;
       if (isinf(rho)) return -1;
     }
@@ -416,13 +457,14 @@ static __device__ __noinline__ int diagonal_solve_row_slow(int solver, int failu
 // Diagonal solve of one row with the reference's failure handling
 // (bgs.c:969-1013). Returns the failure kind of the first attempt: 0 none,
 // 1 diverged (iterations >= maxiter), 2 failed (< 0).
+template <bool RECIP = false>
 __device__ __forceinline__ int diagonal_solve_row(int solver, int failure, const ContactParams& cp, double epsilon,
                                                   int maxiter, double rho, const double* W, const double* B,
                                                   const double* V, double* U, double* R) {
   const double r0 = R[0], r1 = R[1], r2 = R[2];
   int it = -1;
   if (solver == DS_SEMISMOOTH_NEWTON) {
-    it = semismooth_newton(cp, epsilon, maxiter, rho, W, B, V, U, R);
+    it = semismooth_newton<RECIP>(cp, epsilon, maxiter, rho, W, B, V, U, R);
     if (it < maxiter && it >= 0) return 0;
   }
   RowState st;

@@ -659,8 +659,8 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
         kind = bilateral_solve_row(ckind, Zr, a.step, a.dynamic, a.failure, a.diagepsilon, a.diagmaxiter, W, ag, V, U,
                                    R);
       else
-        kind = diagonal_solve_row(a.diagsolver, a.failure, cp, a.diagepsilon, a.diagmaxiter, rho_row, W, ag, V, U,
-                                  R);
+        kind = diagonal_solve_row<MIXED>(a.diagsolver, a.failure, cp, a.diagepsilon, a.diagmaxiter, rho_row, W, ag, V,
+                                         U, R);
       if (tr) {
 #pragma unroll
         for (int q = 0; q < 3; q++) { tr[9 + q] = U[q]; tr[12 + q] = R[q]; }
