@@ -21,11 +21,9 @@ struct ContactParams {
 
 // Solve A x = b (3x3, column-major, one right-hand side). Returns 0, or k > 0
 // when U(k,k) is exactly zero (b untouched), as LAPACK dgesv reports.
-template <bool RECIP = false>
 __device__ __forceinline__ int lu3_solve(double* a, double* b) {
   int ipiv[3];
   int info = 0;
-  double rpiv[3] = {0.0, 0.0, 0.0};  // RECIP: 1/U(j,j) where dgetf2 formed it (0: divide)
 #pragma unroll
   for (int j = 0; j < 3; j++) {
     int p = j;
@@ -51,7 +49,6 @@ __device__ __forceinline__ int lu3_solve(double* a, double* b) {
       double piv = a[j + 3 * j];
       if (fabs(piv) >= 2.2250738585072014e-308) {
         double r = 1.0 / piv;
-        if constexpr (RECIP) rpiv[j] = r;
 #pragma unroll
         for (int i = j + 1; i < 3; i++) a[i + 3 * j] *= r;
       } else {
@@ -92,12 +89,29 @@ __device__ __forceinline__ int lu3_solve(double* a, double* b) {
 #pragma unroll
   for (int k = 2; k >= 0; k--) {
     if (b[k] != 0.0) {
-      if (RECIP && rpiv[k] != 0.0) b[k] *= rpiv[k];
-      else b[k] /= a[k + 3 * k];
+      b[k] /= a[k + 3 * k];
 #pragma unroll
       for (int i = 0; i < k; i++) b[i] -= b[k] * a[i + 3 * k];
     }
   }
+  return 0;
+}
+
+// A x = b for a 3x3 A (column-major) by the adjugate and one reciprocal of
+// the determinant (Cramer's rule): a shorter dependent chain than the pivoted
+// LU, for the FP32 sweeps' Newton steps only (not the reference's
+// arithmetic). Returns 0, or 1 for a zero or non-finite determinant.
+__device__ __forceinline__ int cramer3_solve(const double* a, double* b) {
+  const double c00 = a[4] * a[8] - a[7] * a[5], c01 = a[7] * a[2] - a[1] * a[8], c02 = a[1] * a[5] - a[4] * a[2];
+  const double det = a[0] * c00 + a[3] * c01 + a[6] * c02;
+  if (det == 0.0 || !isfinite(det)) return 1;
+  const double c10 = a[6] * a[5] - a[3] * a[8], c11 = a[0] * a[8] - a[6] * a[2], c12 = a[3] * a[2] - a[0] * a[5];
+  const double c20 = a[3] * a[7] - a[6] * a[4], c21 = a[6] * a[1] - a[0] * a[7], c22 = a[0] * a[4] - a[3] * a[1];
+  const double r = 1.0 / det;
+  const double x0 = (c00 * b[0] + c10 * b[1] + c20 * b[2]) * r;
+  const double x1 = (c01 * b[0] + c11 * b[1] + c21 * b[2]) * r;
+  const double x2 = (c02 * b[0] + c12 * b[1] + c22 * b[2]) * r;
+  b[0] = x0; b[1] = x1; b[2] = x2;
   return 0;
 }
 
@@ -133,8 +147,11 @@ __device__ __forceinline__ void scf_project(double fri, double coh, double* S, d
 }
 
 // SCF_Linearize (scf.c:28-133) with UT = -1 and zero smoothing, the values
-// every caller on the path passes. X, Y (Jacobians) only when WITHXY.
-template <bool WITHXY>
+// every caller on the path passes. X, Y (Jacobians) only when WITHXY. FAST
+// (the merit terms of the FP32 sweeps of mixed precision, which are not
+// bitwise the reference's anyway): one reciprocal per shared divisor and
+// |l| for sqrt(l l).
+template <bool WITHXY, bool FAST = false>
 __device__ __forceinline__ void scf_linearize(const ContactParams& cp, const double* V, const double* U,
                                               const double* R, double* C, double* X, double* Y) {
   const double fri = cp.friction;
@@ -146,17 +163,30 @@ __device__ __forceinline__ void scf_linearize(const ContactParams& cp, const dou
   S[2] += cp.cohesion;
   double sdot = S[0] * S[0] + S[1] * S[1];
   double slen = sqrt(sdot);
-  double l1 = -(S[2] + fri * slen) / onefri2;
-  double l2 = (slen - fri * S[2]) / onefri2;
+  double l1, l2;
+  if constexpr (FAST) {
+    const double r = 1.0 / onefri2;
+    l1 = -(S[2] + fri * slen) * r;
+    l2 = (slen - fri * S[2]) * r;
+  } else {
+    l1 = -(S[2] + fri * slen) / onefri2;
+    l2 = (slen - fri * S[2]) / onefri2;
+  }
   double u1[3], u2[3];
   if (slen != 0.0) {
-    u2[0] = S[0] / slen; u2[1] = S[1] / slen; u2[2] = -fri;
+    if constexpr (FAST) {
+      const double r = 1.0 / slen;
+      u2[0] = S[0] * r; u2[1] = S[1] * r;
+    } else {
+      u2[0] = S[0] / slen; u2[1] = S[1] / slen;
+    }
+    u2[2] = -fri;
     u1[0] = -fri * u2[0]; u1[1] = -fri * u2[1]; u1[2] = -1.0;
   } else {
     u2[0] = 1.0; u2[1] = 0.0; u2[2] = -fri;
     u1[0] = -fri; u1[1] = 0.0; u1[2] = -1.0;
   }
-  double sq1 = sqrt(l1 * l1), sq2 = sqrt(l2 * l2);
+  double sq1 = FAST ? fabs(l1) : sqrt(l1 * l1), sq2 = FAST ? fabs(l2) : sqrt(l2 * l2);
   double g1 = 0.5 * (sq1 + l1), g2 = 0.5 * (sq2 + l2);
   C[0] = F0 + (g1 * u1[0] + g2 * u2[0]);
   C[1] = F1 + (g1 * u1[1] + g2 * u2[1]);
@@ -254,9 +284,10 @@ static __device__ __noinline__ int de_saxce_feng(const ContactParams& cp, double
 // FP32 sweeps of mixed precision only, which are not bitwise the reference's
 // anyway) shortens the solve's dependent chain of divisions: one reciprocal
 // where the reference divides several values by the same divisor (the slip
-// branch's norm and den, the stick branch's d2, the LU's pivots), the slip
-// branch's alfa delta as (R.d)/den (the same quantity), and the error test
-// squared; the results then differ from the reference's in the last bits.
+// branch's norm and den, the stick branch's d2), the slip branch's alfa delta
+// as (R.d)/den (the same quantity), the Newton step by Cramer's rule instead
+// of the pivoted LU, and the error test squared; the results then differ from
+// the reference's in the last bits.
 template <bool RECIP = false>
 __device__ __forceinline__ int semismooth_newton(const ContactParams& cp, double epsilon, int maxiter, double rho,
                                                  const double* W, const double* B, const double* V, double* U,
@@ -358,7 +389,7 @@ __device__ __forceinline__ int semismooth_newton(const ContactParams& cp, double
       a[6] = 0.0; a[7] = 0.0; a[8] = 1.0;
       b[0] = -R[0]; b[1] = -R[1]; b[2] = -R[2];
     }
-    if (lu3_solve<RECIP>(a, b)) return -1;
+    if (RECIP ? cramer3_solve(a, b) : lu3_solve(a, b)) return -1;
     if (!isfinite(b[0] + b[1] + b[2])) return -1;
     double c[3];
     nvaddmul(RES, W, b, c);
@@ -482,10 +513,11 @@ __device__ __forceinline__ int diagonal_solve_row(int solver, int failure, const
 
 // Merit numerator of one CONTACT row (mrf.c:81-87): C = SCF_Linearize(U, R),
 // up = <A C, C>.
+template <bool FAST = false>
 __device__ __forceinline__ double merit_row(const ContactParams& cp, const double* A, const double* V,
                                             const double* U, const double* R) {
   double P[3];
-  scf_linearize<false>(cp, V, U, R, P, nullptr, nullptr);
+  scf_linearize<false, FAST>(cp, V, U, R, P, nullptr, nullptr);
   double Q0 = A[0] * P[0] + A[3] * P[1] + A[6] * P[2];
   double Q1 = A[1] * P[0] + A[4] * P[1] + A[7] * P[2];
   double Q2 = A[2] * P[0] + A[5] * P[1] + A[8] * P[2];

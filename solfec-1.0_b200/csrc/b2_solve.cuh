@@ -570,7 +570,7 @@ __device__ __forceinline__ bool solve_tile(const SolveArgs& a, const SweepFlags&
       for (int q = 0; q < 9; q++) A[q] = __ldg(a.Ad + (size_t)q * n + p);
       double up;
       if (KINDS && ckind != CON_CONTACT) up = merit_row_bilateral(ckind, Zr, cp.gap, a.step, a.dynamic, A, V, am);
-      else up = merit_row(cp, A, V, am, Rold);
+      else up = merit_row<MIXED>(cp, A, V, am, Rold);
       mnum += up;
       a.Um[s & 1][p] = make_double4(am[0], am[1], am[2], 0.0);
       if (a.conmerit[0]) a.conmerit[s & 1][p] = up;
