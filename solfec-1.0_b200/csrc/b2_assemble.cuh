@@ -224,14 +224,20 @@ __global__ void k_row_factors(SceneDev sc, double step, double* factors, double*
 #include "b2_diag.cuh"
 
 namespace b2 {
+// (one factorisation applied to the three unit vectors: the same arithmetic
+// as three dgesv calls, which factorise the same matrix identically; a
+// singular W leaves the unit vectors in A, as the three calls do)
 __device__ __forceinline__ void inv3(const double* W, double* A) {
+  double a[9];
+  int ipiv[3];
+#pragma unroll
+  for (int q = 0; q < 9; q++) a[q] = W[q];
+  const int info = lu3_factor(a, ipiv);
 #pragma unroll
   for (int j = 0; j < 3; j++) {
-    double a[9], b[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int q = 0; q < 9; q++) a[q] = W[q];
+    double b[3] = {0.0, 0.0, 0.0};
     b[j] = 1.0;
-    lu3_solve(a, b);
+    if (!info) lu3_apply(a, ipiv, b);
     A[3 * j] = b[0]; A[3 * j + 1] = b[1]; A[3 * j + 2] = b[2];
   }
 }

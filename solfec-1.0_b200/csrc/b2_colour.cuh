@@ -196,6 +196,78 @@ __global__ void k_offdiag_assembled(int n, long long K, const int* perm, const i
   }
 }
 
+// Body-pair table of the off-diagonal blocks, built once per layout while
+// the contact topology holds. Every non-obstacle body b with contacts
+// c_0 < c_1 < ... < c_{d-1} (its ascending body list) couples each pair
+// a < e: the block of row c_a, column c_e through b and its transpose
+// (row c_e, column c_a). Row i lists its neighbours through its master body,
+// then through its slave body, each ascending (k_adj_fill), so the pair's
+// slot in row c_a is that row's offset of body b plus e - 1, and in row c_e
+// its offset plus a. A record holds the two factor offsets (lo = c_a's H
+// through b, hi = c_e's M^-1 H^T through b) and the two sorted slots.
+__device__ __forceinline__ int pair_row_offset(int i, int b, const int* master, const int* obstacle,
+                                               const int* bptr) {
+  const int m = master[i];
+  if (m == b) return 0;
+  return (m >= 0 && !obstacle[m]) ? bptr[m + 1] - bptr[m] - 1 : 0;
+}
+
+__global__ void k_pair_count(int nbod, const int* obstacle, const int* bptr, long long* cnt) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbod) return;
+  const long long d = obstacle[b] ? 0 : (long long)(bptr[b + 1] - bptr[b]);
+  cnt[b] = d * (d - 1) / 2;
+}
+
+__global__ void k_pair_fill(int nbod, const int* obstacle, const int* master, const int* bptr, const int* brow,
+                            const long long* pptr, const int* iperm, const int* rowptr, int4* rec) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbod || obstacle[b]) return;
+  const int b0 = bptr[b], d = bptr[b + 1] - b0;
+  long long k = pptr[b];
+  for (int a = 0; a < d; a++) {
+    const int i = brow[b0 + a];
+    const int qi = rowptr[iperm[i]] + pair_row_offset(i, b, master, obstacle, bptr);
+    const int fl = i * kFactorStride + (master[i] == b ? 0 : 36);
+    for (int e = a + 1; e < d; e++) {
+      const int j = brow[b0 + e];
+      const int qj = rowptr[iperm[j]] + pair_row_offset(j, b, master, obstacle, bptr);
+      rec[k++] = make_int4(fl, j * kFactorStride + (master[j] == b ? 18 : 54), qi + e - 1, qj + a);
+    }
+  }
+}
+
+// The off-diagonal blocks from the body-pair table (thread per pair): the
+// product of k_offdiag_assembled for the pair (lo, hi) through b, computed
+// once and written as the block (lo, hi) and its transpose (hi, lo); bitwise
+// the blocks k_offdiag_assembled writes. The pairs of one body are
+// neighbours in the table, so their factors are read from L1.
+__global__ void k_offdiag_pairs(long long npairs, const int4* __restrict__ rec, const double* __restrict__ factors,
+                                double step, double* W64, float* W32, long long kstride) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= npairs) return;
+  const int4 r = rec[g];
+  const double* left = factors + r.x;
+  const double* right = factors + r.y;
+  double Lr[18], Pr[18], W[9];
+#pragma unroll
+  for (int q = 0; q < 18; q++) { Lr[q] = left[q]; Pr[q] = right[q]; }
+#pragma unroll
+  for (int q = 0; q < 9; q++) W[q] = 0.0;
+  hp_add(Lr, Pr, W);
+#pragma unroll
+  for (int q = 0; q < 9; q++) W[q] *= step;
+#pragma unroll
+  for (int rr = 0; rr < 3; rr++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      W64[(3 * c + rr) * kstride + r.z] = W[3 * c + rr];   // row lo, column hi: W as computed
+      W32[(3 * c + rr) * kstride + r.z] = (float)W[3 * c + rr];
+      W64[(3 * c + rr) * kstride + r.w] = W[3 * rr + c];   // row hi, column lo: the transpose
+      W32[(3 * c + rr) * kstride + r.w] = (float)W[3 * rr + c];
+    }
+}
+
 // Sorted row of every off-diagonal block of the colour-sorted CSR (thread per
 // row), kept with the layout so the per-step block kernel needs no search.
 __global__ void k_block_rows(int n, const int* rowptr, int* brow) {

@@ -249,6 +249,11 @@ struct b2dev_ctx {
   int topo_n = -1, topo_nb = -1;
   bool topo_valid = false;
   Buf blkrow;  // sorted row of every off-diagonal block (with the layout)
+  // body-pair table of the off-diagonal blocks (k_pair_fill), valid for the
+  // layout and contact topology it was built on
+  Buf pr_cnt, pr_ptr, pr_rec;
+  long long npairs = 0;
+  bool pairs_valid = false;
 
   int n = 0;
   long long K = 0, kstride = 0;
@@ -418,6 +423,42 @@ static int permute_kinds(b2dev_ctx* c) {
   return B2DEV_OK;
 }
 
+// The body-pair table of the current layout and contact topology (body lists
+// bptr/brow, sorted rows rowptr/iperm, roles master/obstacle). Left invalid
+// (the block kernel then runs) when the pair count or the factor offsets
+// would not fit an int.
+static int build_pairs(b2dev_ctx* c) {
+  const int nb = c->nbod, n = c->n;
+  cudaStream_t st = c->stream;
+  c->pairs_valid = false;
+  if ((long long)n * kFactorStride + kFactorStride > INT_MAX || c->K % 2 != 0) return B2DEV_OK;
+  B2_TRY(ensure(c->pr_cnt, sizeof(long long) * (nb + 1)));
+  B2_TRY(ensure(c->pr_ptr, sizeof(long long) * (nb + 1)));
+  B2_CK(cudaMemsetAsync(c->pr_cnt.p, 0, sizeof(long long) * (nb + 1), st));
+  c->launches++;
+  k_pair_count<<<blocks_for(nb, 256), 256, 0, st>>>(nb, ptr<int>(c->obst), ptr<int>(c->bptr),
+                                                   ptr<long long>(c->pr_cnt));
+  size_t bytes = 0;
+  B2_CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, ptr<long long>(c->pr_cnt), ptr<long long>(c->pr_ptr), nb + 1,
+                                      st));
+  B2_TRY(ensure(c->cub_tmp, bytes));
+  B2_CK(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, bytes, ptr<long long>(c->pr_cnt), ptr<long long>(c->pr_ptr),
+                                      nb + 1, st));
+  long long np = 0;
+  B2_CK(cudaMemcpyAsync(&np, ptr<long long>(c->pr_ptr) + nb, sizeof(long long), cudaMemcpyDeviceToHost, st));
+  B2_CK(cudaStreamSynchronize(st));
+  if (2 * np != c->K) return B2DEV_OK;  // every block is one side of one pair
+  B2_TRY(ensure(c->pr_rec, sizeof(int4) * (size_t)(np + 1)));
+  c->launches++;
+  k_pair_fill<<<blocks_for(nb, 128), 128, 0, st>>>(nb, ptr<int>(c->obst), ptr<int>(c->master), ptr<int>(c->bptr),
+                                                  ptr<int>(c->brow), ptr<long long>(c->pr_ptr), ptr<int>(c->iperm),
+                                                  ptr<int>(c->rowptr), ptr<int4>(c->pr_rec));
+  B2_CK(cudaGetLastError());
+  c->npairs = np;
+  c->pairs_valid = true;
+  return B2DEV_OK;
+}
+
 int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled, bool same_graph) {
   const int n = c->n;
   cudaStream_t st = c->stream;
@@ -538,8 +579,16 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled, bool same_graph)
   B2_TRY(ensure(c->W64, sizeof(double) * 9 * (c->kstride + 1)));
   B2_TRY(ensure(c->W32, sizeof(float) * 9 * (c->kstride + 1)));
   const int wpb = 8;
+  if (!same_layout || !same_graph) c->pairs_valid = false;
+  if (n > 0 && K > 0 && assembled && same_layout && same_graph && !c->pairs_valid)
+    B2_TRY(build_pairs(c));  // the second assembly on this layout and topology: the body-pair table
   if (n > 0 && K > 0) {
-    if (assembled) {
+    if (assembled && c->pairs_valid) {
+      c->launches++;
+      k_offdiag_pairs<<<(unsigned)((c->npairs + 255) / 256), 256, 0, st>>>(
+          c->npairs, ptr<int4>(c->pr_rec), ptr<double>(c->factors), c->step, ptr<double>(c->W64), ptr<float>(c->W32),
+          c->kstride);
+    } else if (assembled) {
       c->launches++;
       k_offdiag_assembled<<<blocks_for(K, 256), 256, 0, st>>>(
           n, K, ptr<int>(c->perm), ptr<int>(c->iperm), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<int>(c->adjbod),
@@ -923,7 +972,8 @@ void b2dev_destroy(b2dev_ctx* c) {
                 &c->cc_cell, &c->cc_hkey, &c->cc_hkey_s, &c->cc_large, &c->cc_bstart, &c->cc_bend, &c->cc_misc, &c->cc_keep, &c->cc_cls, &c->cc_order, &c->ex_bodies, &c->ex_surf,
                 &c->st_area, &c->det_area, &c->cn_kind, &c->cn_master, &c->cn_slave, &c->cn_mpnt, &c->cn_spnt,
                 &c->cn_base, &c->cn_Z,
-                &c->topo_m, &c->topo_s, &c->topo_o, &c->topo_flag, &c->blkrow};
+                &c->topo_m, &c->topo_s, &c->topo_o, &c->topo_flag, &c->blkrow, &c->pr_cnt, &c->pr_ptr,
+                &c->pr_rec};
   for (Buf* b : all)
     if (b->p) cudaFree(b->p);
   if (c->graph) cudaGraphExecDestroy(c->graph);

@@ -19,10 +19,10 @@ struct ContactParams {
   int dynamic;
 };
 
-// Solve A x = b (3x3, column-major, one right-hand side). Returns 0, or k > 0
-// when U(k,k) is exactly zero (b untouched), as LAPACK dgesv reports.
-__device__ __forceinline__ int lu3_solve(double* a, double* b) {
-  int ipiv[3];
+// LU factorisation with partial pivoting of a 3x3 A (column-major, in place)
+// in the arithmetic of LAPACK dgetf2. Returns 0, or k > 0 when U(k,k) is
+// exactly zero.
+__device__ __forceinline__ int lu3_factor(double* a, int* ipiv) {
   int info = 0;
 #pragma unroll
   for (int j = 0; j < 3; j++) {
@@ -68,7 +68,11 @@ __device__ __forceinline__ int lu3_solve(double* a, double* b) {
       }
     }
   }
-  if (info) return info;
+  return info;
+}
+
+// x = A^-1 b from lu3_factor's factors (dgetrs, one right-hand side, in place).
+__device__ __forceinline__ void lu3_apply(const double* a, const int* ipiv, double* b) {
 #pragma unroll
   for (int i = 0; i < 3; i++) {
     int p = ipiv[i];
@@ -94,6 +98,15 @@ __device__ __forceinline__ int lu3_solve(double* a, double* b) {
       for (int i = 0; i < k; i++) b[i] -= b[k] * a[i + 3 * k];
     }
   }
+}
+
+// Solve A x = b (3x3, column-major, one right-hand side). Returns 0, or k > 0
+// when U(k,k) is exactly zero (b untouched), as LAPACK dgesv reports.
+__device__ __forceinline__ int lu3_solve(double* a, double* b) {
+  int ipiv[3];
+  const int info = lu3_factor(a, ipiv);
+  if (info) return info;
+  lu3_apply(a, ipiv, b);
   return 0;
 }
 

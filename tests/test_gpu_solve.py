@@ -252,6 +252,40 @@ def test_assembly_parity(scene_cache):
     assert np.array_equal(ldy.colours(), col)
 
 
+@pytest.mark.parametrize('scene', ['spheres_lattice', 'hexahedra_small'])
+def test_assembly_parity_on_a_kept_layout(scene_cache, scene):
+    """Assemblies after the first on an unchanged contact topology (the
+    second builds the body-pair table, later ones reuse it) write W_ij from
+    the body pairs instead of per block: bitwise the oracle's blocks, on moved
+    bodies too."""
+    import dataclasses
+    from solfec_b200._lib import lib
+    from solfec_b200.dynamics import RIGID_DYNAMICS
+    sc = scene_cache('spheres_lattice') if scene == 'spheres_lattice' else \
+        scene_cache('hexahedra_lattice', nx=12, ny=12, nz=4)
+    J = np.stack([np.eye(3).reshape(9) if o else np.linalg.inv(j.reshape(3, 3).T).T.reshape(9)
+                  for j, o in zip(sc.jinv, sc.obstacle != 0)])
+    mass = np.where(sc.obstacle != 0, 1.0, 1.0 / np.where(sc.obstacle != 0, 1.0, sc.minv))
+    ldy = LOCDYN()
+    ldy.update_begin(sc)
+    dyn = RIGID_DYNAMICS(ldy, J, mass, sc.x)
+    for step in range(3):
+        dyn.step_begin(sc.step, (0.0, 0.0, -9.81))
+        assert lib().b2gs_locdyn_update_begin_resident(ldy.handle, sc.step, int(sc.dynamic)) == 0
+        st = dyn.state()
+        cur = dataclasses.replace(sc, rot=st['rot'], x=st['x'], velo=st['velo'], velo0=st['velo0'])
+        ld = O.assemble(cur)
+        d = ldy.download()
+        assert np.array_equal(d['adjcol'], ld.adjcol)
+        for k in ('W', 'Woff', 'B', 'V'):
+            assert same_bits(d[k], getattr(ld, k)), (step, k, rel(d[k], getattr(ld, k)))
+        ldy.set_state(np.zeros((sc.ncon, 3)), np.zeros((sc.ncon, 3)))
+        gs = GAUSS_SEIDEL_SOLVER(1e-4, 5)
+        gs.solve(ldy)
+        dyn.step_end(sc.step)
+    ldy.close()
+
+
 def test_hexahedra_assembly_and_solve(scene_cache):
     sc = scene_cache('hexahedra_lattice', nx=12, ny=12, nz=4)
     ld = O.assemble(sc)
