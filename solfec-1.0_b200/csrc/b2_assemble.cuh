@@ -19,6 +19,18 @@ namespace b2 {
 // P = M^-1 H^T (6x3). Zero for an obstacle side.
 constexpr int kFactorStride = 72;  // Hm[18] Pm[18] Hs[18] Ps[18]
 
+// 16-byte store and load of two doubles (p 16-byte aligned: a row's factors
+// start at a multiple of 72 doubles and each part at an even offset)
+__device__ __forceinline__ void st2(double* p, double a, double b) {
+  *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+__device__ __forceinline__ double2 ld2(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
+// the six velocity components of a body (6 doubles a body: 16-byte aligned)
+__device__ __forceinline__ void ld6(const double* p, double* u) {
+  const double2 a = ld2(p), b = ld2(p + 2), c = ld2(p + 4);
+  u[0] = a.x; u[1] = a.y; u[2] = b.x; u[3] = b.y; u[4] = c.x; u[5] = c.y;
+}
+
 struct SceneDev {
   int nbod, ncon;
   const double* rot;    // [nbod][9]
@@ -160,25 +172,31 @@ __global__ void k_row_factors(SceneDev sc, double step, double* factors, double*
 #pragma unroll
       for (int q = 0; q < 3; q++) X[q] = sc.mpnt[(size_t)3 * i + q];
       rig_H(sc.rot + (size_t)9 * m, sc.x0 + (size_t)3 * m, base, X, H);
-      h_times(H, sc.velo0 + (size_t)6 * m, y); V[0] += y[0]; V[1] += y[1]; V[2] += y[2];
-      h_times(H, sc.velo + (size_t)6 * m, y); B[0] += y[0]; B[1] += y[1]; B[2] += y[2];
+      double u[6];
+      ld6(sc.velo0 + (size_t)6 * m, u);
+      h_times(H, u, y); V[0] += y[0]; V[1] += y[1]; V[2] += y[2];
+      ld6(sc.velo + (size_t)6 * m, u);
+      h_times(H, u, y); B[0] += y[0]; B[1] += y[1]; B[2] += y[2];
       if (!sc.obstacle[m]) {
         double P[18];
         minv_ht(sc.jinv + (size_t)9 * m, sc.minv[m], H, P);
 #pragma unroll
-        for (int q = 0; q < 18; q++) { F[q] = H[q]; F[18 + q] = P[q]; }
+        for (int q = 0; q < 18; q += 2) { st2(F + q, H[q], H[q + 1]); st2(F + 18 + q, P[q], P[q + 1]); }
         hp_add(H, P, W);
       } else {
 #pragma unroll
-        for (int q = 0; q < 36; q++) F[q] = 0.0;
+        for (int q = 0; q < 36; q += 2) st2(F + q, 0.0, 0.0);
       }
       // slave side, subtracted (ldy.c:383-393), H negated for W (ldy.c:685)
       if (s >= 0) {
 #pragma unroll
         for (int q = 0; q < 3; q++) X[q] = sc.spnt[(size_t)3 * i + q];
         rig_H(sc.rot + (size_t)9 * s, sc.x0 + (size_t)3 * s, base, X, H);
-        h_times(H, sc.velo0 + (size_t)6 * s, y); V[0] -= y[0]; V[1] -= y[1]; V[2] -= y[2];
-        h_times(H, sc.velo + (size_t)6 * s, y); B[0] -= y[0]; B[1] -= y[1]; B[2] -= y[2];
+        double u[6];
+        ld6(sc.velo0 + (size_t)6 * s, u);
+        h_times(H, u, y); V[0] -= y[0]; V[1] -= y[1]; V[2] -= y[2];
+        ld6(sc.velo + (size_t)6 * s, u);
+        h_times(H, u, y); B[0] -= y[0]; B[1] -= y[1]; B[2] -= y[2];
       }
       if (s >= 0 && !sc.obstacle[s]) {
         double P[18];
@@ -186,11 +204,11 @@ __global__ void k_row_factors(SceneDev sc, double step, double* factors, double*
         for (int q = 0; q < 18; q++) H[q] = -H[q];
         minv_ht(sc.jinv + (size_t)9 * s, sc.minv[s], H, P);
 #pragma unroll
-        for (int q = 0; q < 18; q++) { F[36 + q] = H[q]; F[54 + q] = P[q]; }
+        for (int q = 0; q < 18; q += 2) { st2(F + 36 + q, H[q], H[q + 1]); st2(F + 54 + q, P[q], P[q + 1]); }
         hp_add(H, P, W);
       } else {
 #pragma unroll
-        for (int q = 0; q < 36; q++) F[36 + q] = 0.0;
+        for (int q = 0; q < 36; q += 2) st2(F + 36 + q, 0.0, 0.0);
       }
     }
 #pragma unroll

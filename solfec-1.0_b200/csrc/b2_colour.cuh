@@ -178,7 +178,10 @@ __global__ void k_offdiag_assembled(int n, long long K, const int* perm, const i
     const double* right = factors + (size_t)hi * kFactorStride + (master[hi] == b ? 18 : 54);
     double Lr[18], Pr[18], W[9];
 #pragma unroll
-    for (int q = 0; q < 18; q++) { Lr[q] = left[q]; Pr[q] = right[q]; }
+    for (int q = 0; q < 18; q += 2) {
+      const double2 l = ld2(left + q), p = ld2(right + q);
+      Lr[q] = l.x; Lr[q + 1] = l.y; Pr[q] = p.x; Pr[q + 1] = p.y;
+    }
 #pragma unroll
     for (int q = 0; q < 9; q++) W[q] = 0.0;
     hp_add(Lr, Pr, W);
@@ -251,7 +254,10 @@ __global__ void k_offdiag_pairs(long long npairs, const int4* __restrict__ rec, 
   const double* right = factors + r.y;
   double Lr[18], Pr[18], W[9];
 #pragma unroll
-  for (int q = 0; q < 18; q++) { Lr[q] = left[q]; Pr[q] = right[q]; }
+  for (int q = 0; q < 18; q += 2) {
+    const double2 l = ld2(left + q), p = ld2(right + q);
+    Lr[q] = l.x; Lr[q + 1] = l.y; Pr[q] = p.x; Pr[q + 1] = p.y;
+  }
 #pragma unroll
   for (int q = 0; q < 9; q++) W[q] = 0.0;
   hp_add(Lr, Pr, W);
