@@ -152,7 +152,7 @@ __device__ __forceinline__ void inv3(const double* W, double* A);
 // Row pass (thread per contact, caller order): H/P factors, W_ii, rho, A, B, V
 // and the per-block partial of the free energy sum_i B_i^T A_i B_i.
 __global__ void k_row_factors(SceneDev sc, double step, double* factors, double* Wii, double* Aii, double* rho,
-                              double* Bo, double* Vo, double* fe_part, int* bad) {
+                              double* Bo, double* Vo, double* fe_part, int* bad, int write_factors) {
   __shared__ double red[256 / kWarp];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double fe = 0.0;
@@ -181,11 +181,13 @@ __global__ void k_row_factors(SceneDev sc, double step, double* factors, double*
         double P[18];
         minv_ht(sc.jinv + (size_t)9 * m, sc.minv[m], H, P);
 #pragma unroll
-        for (int q = 0; q < 18; q += 2) { st2(F + q, H[q], H[q + 1]); st2(F + 18 + q, P[q], P[q + 1]); }
+        if (write_factors)
+          for (int q = 0; q < 18; q += 2) { st2(F + q, H[q], H[q + 1]); st2(F + 18 + q, P[q], P[q + 1]); }
         hp_add(H, P, W);
       } else {
 #pragma unroll
-        for (int q = 0; q < 36; q += 2) st2(F + q, 0.0, 0.0);
+        if (write_factors)
+          for (int q = 0; q < 36; q += 2) st2(F + q, 0.0, 0.0);
       }
       // slave side, subtracted (ldy.c:383-393), H negated for W (ldy.c:685)
       if (s >= 0) {
@@ -204,11 +206,13 @@ __global__ void k_row_factors(SceneDev sc, double step, double* factors, double*
         for (int q = 0; q < 18; q++) H[q] = -H[q];
         minv_ht(sc.jinv + (size_t)9 * s, sc.minv[s], H, P);
 #pragma unroll
-        for (int q = 0; q < 18; q += 2) { st2(F + 36 + q, H[q], H[q + 1]); st2(F + 54 + q, P[q], P[q + 1]); }
+        if (write_factors)
+          for (int q = 0; q < 18; q += 2) { st2(F + 36 + q, H[q], H[q + 1]); st2(F + 54 + q, P[q], P[q + 1]); }
         hp_add(H, P, W);
       } else {
 #pragma unroll
-        for (int q = 0; q < 36; q += 2) st2(F + 36 + q, 0.0, 0.0);
+        if (write_factors)
+          for (int q = 0; q < 36; q += 2) st2(F + 36 + q, 0.0, 0.0);
       }
     }
 #pragma unroll

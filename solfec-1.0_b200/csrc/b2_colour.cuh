@@ -274,6 +274,54 @@ __global__ void k_offdiag_pairs(long long npairs, const int4* __restrict__ rec, 
     }
 }
 
+// The contact's factor through one of its bodies, as k_row_factors forms it:
+// side 0 (master) or 1 (slave, H negated, ldy.c:685); P = M^-1 H^T when want_p.
+__device__ __forceinline__ void contact_factor(const SceneDev& sc, int i, int slave_side, bool want_p, double* H,
+                                               double* P) {
+  const int b = slave_side ? sc.slave[i] : sc.master[i];
+  double base[9], X[3];
+#pragma unroll
+  for (int q = 0; q < 9; q++) base[q] = sc.base[(size_t)9 * i + q];
+  const double* Xp = slave_side ? sc.spnt : sc.mpnt;
+#pragma unroll
+  for (int q = 0; q < 3; q++) X[q] = Xp[(size_t)3 * i + q];
+  rig_H(sc.rot + (size_t)9 * b, sc.x0 + (size_t)3 * b, base, X, H);
+  if (slave_side) {
+#pragma unroll
+    for (int q = 0; q < 18; q++) H[q] = -H[q];
+  }
+  if (want_p) minv_ht(sc.jinv + (size_t)9 * b, sc.minv[b], H, P);
+}
+
+// k_offdiag_pairs without the stored factors: each pair forms its two
+// factors from the bodies (the same operations as k_row_factors, so the
+// blocks are bitwise the same), which saves the factor array's write and
+// read-back. The pair record's factor offsets give the contacts and sides.
+__global__ void k_offdiag_pairs_formed(long long npairs, const int4* __restrict__ rec, SceneDev sc, double step,
+                                       double* W64, float* W32, long long kstride) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= npairs) return;
+  const int4 r = rec[g];
+  const int lo = r.x / kFactorStride, hi = r.y / kFactorStride;
+  double Lr[18], Hh[18], Pr[18], W[9];
+  contact_factor(sc, lo, r.x - lo * kFactorStride != 0, false, Lr, nullptr);
+  contact_factor(sc, hi, r.y - hi * kFactorStride != 18, true, Hh, Pr);
+#pragma unroll
+  for (int q = 0; q < 9; q++) W[q] = 0.0;
+  hp_add(Lr, Pr, W);
+#pragma unroll
+  for (int q = 0; q < 9; q++) W[q] *= step;
+#pragma unroll
+  for (int rr = 0; rr < 3; rr++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      W64[(3 * c + rr) * kstride + r.z] = W[3 * c + rr];
+      W32[(3 * c + rr) * kstride + r.z] = (float)W[3 * c + rr];
+      W64[(3 * c + rr) * kstride + r.w] = W[3 * rr + c];
+      W32[(3 * c + rr) * kstride + r.w] = (float)W[3 * rr + c];
+    }
+}
+
 // Sorted row of every off-diagonal block of the colour-sorted CSR (thread per
 // row), kept with the layout so the per-step block kernel needs no search.
 __global__ void k_block_rows(int n, const int* rowptr, int* brow) {

@@ -254,6 +254,7 @@ struct b2dev_ctx {
   Buf pr_cnt, pr_ptr, pr_rec;
   long long npairs = 0;
   bool pairs_valid = false;
+  bool factors_stored = true;  // the last row pass wrote the factor array
 
   int n = 0;
   long long K = 0, kstride = 0;
@@ -423,6 +424,17 @@ static int permute_kinds(b2dev_ctx* c) {
   return B2DEV_OK;
 }
 
+// Device view of the uploaded scene (bodies and contacts) for the assembly kernels.
+static SceneDev scene_view(b2dev_ctx* c) {
+  SceneDev sc;
+  sc.nbod = c->nbod; sc.ncon = c->ncon;
+  sc.rot = ptr<double>(c->rot); sc.x0 = ptr<double>(c->x0); sc.jinv = ptr<double>(c->jinv);
+  sc.minv = ptr<double>(c->minv); sc.velo = ptr<double>(c->velo); sc.velo0 = ptr<double>(c->velo0);
+  sc.obstacle = ptr<int>(c->obst); sc.master = ptr<int>(c->master); sc.slave = ptr<int>(c->slave);
+  sc.mpnt = ptr<double>(c->mpnt); sc.spnt = ptr<double>(c->spnt); sc.base = ptr<double>(c->base);
+  return sc;
+}
+
 // The body-pair table of the current layout and contact topology (body lists
 // bptr/brow, sorted rows rowptr/iperm, roles master/obstacle). Left invalid
 // (the block kernel then runs) when the pair count or the factor offsets
@@ -583,12 +595,26 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled, bool same_graph)
   if (n > 0 && K > 0 && assembled && same_layout && same_graph && !c->pairs_valid)
     B2_TRY(build_pairs(c));  // the second assembly on this layout and topology: the body-pair table
   if (n > 0 && K > 0) {
-    if (assembled && c->pairs_valid) {
+    if (assembled && c->pairs_valid && !c->factors_stored) {
+      c->launches++;
+      k_offdiag_pairs_formed<<<(unsigned)((c->npairs + 255) / 256), 256, 0, st>>>(
+          c->npairs, ptr<int4>(c->pr_rec), scene_view(c), c->step, ptr<double>(c->W64), ptr<float>(c->W32),
+          c->kstride);
+    } else if (assembled && c->pairs_valid) {
       c->launches++;
       k_offdiag_pairs<<<(unsigned)((c->npairs + 255) / 256), 256, 0, st>>>(
           c->npairs, ptr<int4>(c->pr_rec), ptr<double>(c->factors), c->step, ptr<double>(c->W64), ptr<float>(c->W32),
           c->kstride);
     } else if (assembled) {
+      if (!c->factors_stored) {  // the row pass left the factors out expecting the pair kernel: the same pass with them
+        c->launches++;
+        k_row_factors<<<blocks_for(n, 256), 256, 0, st>>>(scene_view(c), c->step, ptr<double>(c->factors),
+                                                          ptr<double>(c->Wii), ptr<double>(c->Aii),
+                                                          ptr<double>(c->rho_c), ptr<double>(c->B_c),
+                                                          ptr<double>(c->V_c), ptr<double>(c->fe_part),
+                                                          ptr<int>(c->bad), 1);
+        c->factors_stored = true;
+      }
       c->launches++;
       k_offdiag_assembled<<<blocks_for(K, 256), 256, 0, st>>>(
           n, K, ptr<int>(c->perm), ptr<int>(c->iperm), ptr<int>(c->adjptr), ptr<int>(c->adjcol), ptr<int>(c->adjbod),
@@ -1097,10 +1123,14 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
   sc.minv = ptr<double>(c->minv); sc.velo = ptr<double>(c->velo); sc.velo0 = ptr<double>(c->velo0);
   sc.obstacle = ptr<int>(c->obst); sc.master = ptr<int>(c->master); sc.slave = ptr<int>(c->slave);
   sc.mpnt = ptr<double>(c->mpnt); sc.spnt = ptr<double>(c->spnt); sc.base = ptr<double>(c->base);
+  // a kept layout whose body-pair table is valid forms the factors in the
+  // pair kernel: none are stored (if the topology check below fails, the rows
+  // are assembled again with the factors)
+  const bool formed = c->pairs_valid && topo_cand;
   c->launches++;
   k_row_factors<<<rb, T, 0, st>>>(sc, step, ptr<double>(c->factors), ptr<double>(c->Wii), ptr<double>(c->Aii),
                                   ptr<double>(c->rho_c), ptr<double>(c->B_c), ptr<double>(c->V_c),
-                                  ptr<double>(c->fe_part), ptr<int>(c->bad));
+                                  ptr<double>(c->fe_part), ptr<int>(c->bad), formed ? 0 : 1);
   c->launches++;
   k_sum_partials<<<1, 1024, 0, st>>>(ptr<double>(c->fe_part), rb, ptr<double>(c->fe_dev));
   B2_TRY(ensure(c->pfe, sizeof(double) * (c->nprob + 1)));
@@ -1123,6 +1153,7 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
     if (flags[0]) { set_err("assemble: self-contact or invalid body index (outside the rigid contact path)"); return B2DEV_EUNSUPPORTED; }
     same_topo = topo_cand && flags[1] == 0;
   }
+  c->factors_stored = !formed;  // prepare_layout writes them after all if the per-block kernel runs
   if (same_topo) {  // the contact graph of the last assembly holds (adjptr, adjcol, adjbod, K)
     B2_TRY(prepare_layout(c, colour_seed, true, true));
     B2_CK(cudaEventRecord(c->ev[1], st));

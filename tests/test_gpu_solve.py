@@ -283,6 +283,19 @@ def test_assembly_parity_on_a_kept_layout(scene_cache, scene):
         gs = GAUSS_SEIDEL_SOLVER(1e-4, 5)
         gs.solve(ldy)
         dyn.step_end(sc.step)
+    # another topology of the same sizes (roles swapped where both bodies move):
+    # the row pass expected the pair kernel, the per-block kernel runs instead
+    swap = (sc.slave >= 0) & (sc.obstacle[np.maximum(sc.slave, 0)] == 0)
+    sc2 = dataclasses.replace(sc, master=np.where(swap, sc.slave, sc.master).astype(np.int32),
+                              slave=np.where(swap, sc.master, sc.slave).astype(np.int32),
+                              mpnt=np.where(swap[:, None], sc.spnt, sc.mpnt),
+                              spnt=np.where(swap[:, None], sc.mpnt, sc.spnt))
+    assert swap.any()
+    ldy.update_begin(sc2)
+    ld = O.assemble(sc2)
+    d = ldy.download()
+    for k in ('W', 'Woff', 'B', 'V'):
+        assert same_bits(d[k], getattr(ld, k)), ('swapped', k, rel(d[k], getattr(ld, k)))
     ldy.close()
 
 
