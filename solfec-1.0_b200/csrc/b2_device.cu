@@ -268,6 +268,7 @@ struct b2dev_ctx {
   cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   long long launches = 0;  // kernels of this library launched on this context
   float assemble_ms = 0.f;
+  bool assemble_ms_pending = false;  // ev[0], ev[1] of the last assembly not yet read
 
   // CUDA graph of the batched solve (rebuilt when its captured arguments change)
   cudaGraphExec_t graph = nullptr;
@@ -422,6 +423,13 @@ static int permute_kinds(b2dev_ctx* c) {
                                                              ptr<double>(c->Z_s));
   B2_CK(cudaGetLastError());
   return B2DEV_OK;
+}
+
+// Duration of the last assembly from its events, once they have completed.
+static void assemble_time(b2dev_ctx* c) {
+  if (!c->assemble_ms_pending) return;
+  if (cudaEventSynchronize(c->ev[1]) == cudaSuccess) cudaEventElapsedTime(&c->assemble_ms, c->ev[0], c->ev[1]);
+  c->assemble_ms_pending = false;
 }
 
 // Device view of the uploaded scene (bodies and contacts) for the assembly kernels.
@@ -1094,6 +1102,7 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
   c->dynamic = dynamic ? 1 : 0;
   c->assembled_mode = true;
   c->det_assembled = c->det_valid;
+  assemble_time(c);  // the previous assembly's events before they are recorded again
   B2_CK(cudaEventRecord(c->ev[0], st));
 
   B2_TRY(ensure(c->factors, sizeof(double) * kFactorStride * (n + 1)));
@@ -1156,9 +1165,8 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
   c->factors_stored = !formed;  // prepare_layout writes them after all if the per-block kernel runs
   if (same_topo) {  // the contact graph of the last assembly holds (adjptr, adjcol, adjbod, K)
     B2_TRY(prepare_layout(c, colour_seed, true, true));
-    B2_CK(cudaEventRecord(c->ev[1], st));
-    B2_CK(cudaEventSynchronize(c->ev[1]));
-    cudaEventElapsedTime(&c->assemble_ms, c->ev[0], c->ev[1]);
+    B2_CK(cudaEventRecord(c->ev[1], st));  // read when asked (b2dev_last_assemble_ms): no synchronisation here
+    c->assemble_ms_pending = true;
     return B2DEV_OK;
   }
   c->topo_valid = false;
@@ -1213,8 +1221,7 @@ int b2dev_assemble(b2dev_ctx* c, double step, int dynamic, uint64_t colour_seed)
   c->topo_valid = true;
   B2_TRY(prepare_layout(c, colour_seed, true, false));
   B2_CK(cudaEventRecord(c->ev[1], st));
-  B2_CK(cudaEventSynchronize(c->ev[1]));
-  cudaEventElapsedTime(&c->assemble_ms, c->ev[0], c->ev[1]);
+  c->assemble_ms_pending = true;
   return B2DEV_OK;
 }
 
@@ -2188,7 +2195,7 @@ int b2dev_get_state(b2dev_ctx* c, double* R, double* U, double* conmerit, int on
     else if (on_device) B2_CK(cudaMemsetAsync(conmerit, 0, sizeof(double) * n, st));
     else memset(conmerit, 0, sizeof(double) * n);
   }
-  B2_CK(cudaStreamSynchronize(st));
+  if (!on_device) B2_CK(cudaStreamSynchronize(st));  // device outputs are ordered on the library's stream
   return B2DEV_OK;
 }
 
@@ -2334,6 +2341,7 @@ int b2dev_set_problems(b2dev_ctx* c, int nprob, const int* row_offsets) {
 int b2dev_problem_free_energy(b2dev_ctx* c, double* out) {
   if (!c || !c->ready || !out) { set_err("problem_free_energy: no local dynamics"); return B2DEV_ESTATE; }
   DeviceGuard g(c->device);
+  B2_CK(cudaStreamSynchronize(c->stream));  // the library's work on its stream first
   B2_CK(cudaMemcpy(out, c->pfe.p, sizeof(double) * c->nprob, cudaMemcpyDeviceToHost));
   return B2DEV_OK;
 }
@@ -2595,6 +2603,7 @@ int b2dev_sizes(b2dev_ctx* c, int* n, long long* nblocks, int* ncolours, double*
 int b2dev_get_order(b2dev_ctx* c, int* order) {
   if (!c || !c->ready) { set_err("get_order: no local dynamics"); return B2DEV_ESTATE; }
   DeviceGuard g(c->device);
+  B2_CK(cudaStreamSynchronize(c->stream));  // the library's work on its stream first
   if (c->n) B2_CK(cudaMemcpy(order, c->perm.p, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
   return B2DEV_OK;
 }
@@ -2602,6 +2611,7 @@ int b2dev_get_order(b2dev_ctx* c, int* order) {
 int b2dev_get_colours(b2dev_ctx* c, int* colour) {
   if (!c || !c->ready) { set_err("get_colours: no local dynamics"); return B2DEV_ESTATE; }
   DeviceGuard g(c->device);
+  B2_CK(cudaStreamSynchronize(c->stream));  // the library's work on its stream first
   if (c->n) B2_CK(cudaMemcpy(colour, c->colour.p, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
   return B2DEV_OK;
 }
@@ -2610,6 +2620,7 @@ int b2dev_get_locdyn(b2dev_ctx* c, double* W, double* A, double* rho, double* B,
                      double* Woff, double* free_energy) {
   if (!c || !c->ready) { set_err("get_locdyn: no local dynamics"); return B2DEV_ESTATE; }
   DeviceGuard g(c->device);
+  B2_CK(cudaStreamSynchronize(c->stream));  // the library's work on its stream first
   const int n = c->n;
   const long long K = c->K;
   if (W) B2_CK(cudaMemcpy(W, c->Wii.p, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost));
@@ -2632,7 +2643,12 @@ int b2dev_get_locdyn(b2dev_ctx* c, double* W, double* A, double* rho, double* B,
   return B2DEV_OK;
 }
 
-float b2dev_last_assemble_ms(b2dev_ctx* c) { return c ? c->assemble_ms : 0.f; }
+float b2dev_last_assemble_ms(b2dev_ctx* c) {
+  if (!c) return 0.f;
+  DeviceGuard g(c->device);
+  assemble_time(c);
+  return c->assemble_ms;
+}
 
 long long b2dev_launch_count(b2dev_ctx* c) { return c ? c->launches : 0; }
 
@@ -2667,6 +2683,7 @@ int b2dev_trace_sweep(b2dev_ctx* c, int sweep) {
 int b2dev_get_trace(b2dev_ctx* c, double* out) {
   if (!c || !c->ready || !c->trace.p) { set_err("get_trace: no trace recorded"); return B2DEV_ESTATE; }
   DeviceGuard g(c->device);
+  B2_CK(cudaStreamSynchronize(c->stream));  // the library's work on its stream first
   const int n = c->n;
   std::vector<double> tmp((size_t)kTraceStride * n);
   std::vector<int> perm(n);
