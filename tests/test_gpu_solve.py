@@ -220,6 +220,25 @@ def test_diagonal_failure_exit():
     assert same_bits(c['R'], oc['R'])
 
 
+def test_diagonal_failure_mixed_precision():
+    """The same singular row in mixed precision: the FP32 sweeps' Newton step
+    (Cramer's rule) meets a zero determinant, the failure is reported as in
+    FP64 (FAILURE_EXIT raises the diagonal code; CONTINUE runs the fallback
+    chain and ends with the same error code and reactions within 1e-6)."""
+    n = 2
+    W = np.tile(np.eye(3).ravel(), n); W[0:9] = 0.0
+    A = np.tile(np.eye(3).ravel(), n)
+    ld = O.LocalDynamics(W, A, np.ones(n), np.tile([0.1, 0.0, -1.0], n), np.zeros(3 * n), -np.ones(n) * 1e-3,
+                         np.full(n, 0.3), np.zeros(n), np.zeros(n), np.zeros(n + 1, np.int32), np.zeros(0, np.int32),
+                         np.zeros(0), 1.0, 1e-3, 1)
+    g = gpu_solve(ld, epsilon=1e-4, maxiter=10, failure='EXIT', precision='MIXED')
+    assert g['exc'] is not None and g['exc'].code == 44
+    m = gpu_solve(ld, epsilon=1e-4, maxiter=10, precision='MIXED')
+    f = gpu_solve(ld, epsilon=1e-4, maxiter=10)
+    assert m['gs'].error == f['gs'].error
+    assert np.all(np.isfinite(m['R'])) and np.abs(m['R'] - f['R']).max() <= 1e-6 * max(1.0, np.abs(f['R']).max())
+
+
 def test_empty_and_single():
     ld0 = O.LocalDynamics(np.zeros(0), np.zeros(0), np.zeros(0), np.zeros(0), np.zeros(0), np.zeros(0), np.zeros(0),
                           np.zeros(0), np.zeros(0), np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0), 0.0,
