@@ -346,7 +346,9 @@ int b2dev_set_problems(b2dev_ctx* ctx, int nprob, const int* row_offsets);
 /* free energy of every problem (ldy.c:739), nprob doubles */
 int b2dev_problem_free_energy(b2dev_ctx* ctx, double* out);
 /* Rows per tile (1..32) of the current layout: smaller tiles give more
- * parallel work to small problems; the autotuner chooses it. */
+ * parallel work to small problems. Until it is set here (or by the batch
+ * autotuner, which keeps its choice), a single problem of at most 16,384
+ * rows gets 8 rows per tile and a larger one 32. Results do not depend on it. */
 int b2dev_set_tile_rows(b2dev_ctx* ctx, int rows);
 int b2dev_tile_rows(b2dev_ctx* ctx);
 /* Limit, in seconds, of every bounded wait of the solver kernels on a flag

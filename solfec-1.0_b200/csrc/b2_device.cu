@@ -189,6 +189,7 @@ struct b2dev_ctx {
   int ntiles = 0;
   int max_tile_blocks = 0;  // most off-diagonal blocks of one tile
   int tile_rows = kWarp;    // rows per tile (at most one warp)
+  bool tile_rows_auto = true;  // chosen from the problem size until set (b2dev_set_tile_rows, the autotuner)
 
   // independent problems solved together (one GAUSS_SEIDEL_Solve each); rows
   // of problem k are caller rows prob_off[k] .. prob_off[k+1]-1
@@ -479,6 +480,8 @@ static int build_pairs(b2dev_ctx* c) {
   return B2DEV_OK;
 }
 
+constexpr int kSmallProblemRows = 16384;  // at most this many rows: 8 rows per tile (tile_rows_auto)
+
 int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled, bool same_graph) {
   const int n = c->n;
   cudaStream_t st = c->stream;
@@ -512,6 +515,13 @@ int prepare_layout(b2dev_ctx* c, uint64_t seed, bool assembled, bool same_graph)
     B2_CK(cudaStreamSynchronize(st));
     reuse = diff == 0;
   }
+  // rows per tile by size unless set: a small single problem has far fewer
+  // tiles per colour level than resident warps, and its sweep is the chain of
+  // colour levels, each as long as its slowest tile; 8-row tiles (a tile's
+  // diagonal solves wait for the slowest of 8 lanes, not of 32) shortened the
+  // sweep of a 2,163-row pile from 91 to 73 us and of a 375-row one from 39 to
+  // 36 us, while large problems, whose levels fill the machine, keep 32
+  if (c->tile_rows_auto && c->nprob == 1) c->tile_rows = n <= kSmallProblemRows ? 8 : kWarp;
   // same graph, same colours: the sorted layout and the tile table are those of
   // the last layout, unless the problems or the rows per tile changed since
   const bool same_layout = reuse && c->layout_valid && c->layout_nprob == c->nprob &&
@@ -2349,6 +2359,7 @@ int b2dev_problem_free_energy(b2dev_ctx* c, double* out) {
 int b2dev_set_tile_rows(b2dev_ctx* c, int rows) {
   if (!c || !c->ready || rows < 1 || rows > kWarp) { set_err("set_tile_rows: invalid arguments or no layout"); return B2DEV_EINVAL; }
   DeviceGuard g(c->device);
+  c->tile_rows_auto = false;
   return build_tiles(c, rows);
 }
 
@@ -2580,8 +2591,11 @@ int b2dev_autotune_batch(b2dev_ctx* c, const b2dev_solve_opts* o, b2dev_tune_res
     }
   }
   res->ntrials = std::min(nt, 32);
-  // the chosen tile rows and the initial state back in place
-  if (rc == B2DEV_OK) rc = build_tiles(c, res->tile_rows);
+  // the chosen tile rows (kept from now on) and the initial state back in place
+  if (rc == B2DEV_OK) {
+    c->tile_rows_auto = false;
+    rc = build_tiles(c, res->tile_rows);
+  }
   cudaMemcpyAsync(c->R64[0].p, sv, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(c->Us[0].p, sv + n, sizeof(double4) * n, cudaMemcpyDeviceToDevice, st);
   cudaStreamSynchronize(st);
