@@ -961,20 +961,30 @@ def roofline(mode, reps, n, K, peak):
 # rank 0), as the product arm measures them (its line's fp64_iters_from_rest).
 # The FP64 GPU path reproduces, bit for bit, the reference solver run on the
 # same rows in the GPU's colour order, so these are also that run's counts; the
-# reference's per-iteration cost does not depend on the row order, so the
-# reference arm scales its sample to the mean over the same W warm-up and K
-# timed steps as the product arm's. Past step 60 the loop has settled at one
-# iteration per step.
+# reference's per-iteration cost does not depend on the row order or the
+# state, so the reference arm runs these counts for the product arm's timed
+# steps (or, when they add up to many iterations, scales a sample to their
+# mean). Past step 60 the loop has settled at one iteration per step.
 FP64_ITERS_FROM_REST = [45, 196, 173, 76, 48, 30, 20, 14, 11, 8, 7, 5, 5, 3, 4, 3, 3, 4, 2, 3, 2, 3, 2, 2, 3, 2, 1,
                         3, 1, 2, 2, 1, 1, 2, 1, 1, 2, 1, 1, 2, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1,
                         1, 1, 1]
 
 
+def step_iters(warmup, steps):
+    """FP64 iterations of each timed step warmup+1 .. warmup+steps."""
+    seq = FP64_ITERS_FROM_REST
+    return [seq[k] if k < len(seq) else 1 for k in range(warmup, warmup + steps)]
+
+
 def workload_iters(warmup, steps):
     """Mean FP64 iterations of the timed steps warmup+1 .. warmup+steps."""
-    seq = FP64_ITERS_FROM_REST
-    window = [seq[k] if k < len(seq) else 1 for k in range(warmup, warmup + steps)]
-    return float(np.mean(window))
+    return float(np.mean(step_iters(warmup, steps)))
+
+
+# the reference arm runs every timed step's own iteration count in full when
+# the timed steps add up to at most this many iterations (about 0.27 s each on
+# one host core); past it, it times a sample per step and scales it
+REF_EXACT_MAX_ITERS = 600
 
 
 CPU_SAMPLE_ITERS = 10
@@ -983,10 +993,11 @@ CPU_SAMPLE_ITERS = 10
 def cpu_reference_step(sc, R0, U0, iters_full, sample_iters=CPU_SAMPLE_ITERS, seed=0x5EEDC0105):
     """One step on the host: the restated LOCDYN_Update_Begin (oracle_ldy.c,
     timed in full) and the reference's own serial GAUSS_SEIDEL_Solve
-    (oracle/_ref, compiled from bgs.c etc.) timed over a bounded sample of
-    `sample_iters` iterations from the step's warm start (R0/U0 may be None:
-    cold start) and scaled to `iters_full` iterations; the reference spends
-    the same work on every iteration (one sweep plus one merit pass)."""
+    (oracle/_ref, compiled from bgs.c etc.) timed over `sample_iters`
+    iterations from the step's warm start (R0/U0 may be None: cold start) and
+    scaled to `iters_full` iterations; the reference spends the same work on
+    every iteration (one sweep plus one merit pass). With sample_iters equal
+    to iters_full nothing is scaled: the step is measured in full."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     import oracle as O
     t0 = time.perf_counter()
@@ -1015,16 +1026,29 @@ def run_reference(args, ws, rank):
     from solfec_b200 import scenes
     sc = scenes.hexahedra_lattice(seed=replica_seed(0), **SCENE)
     iters = workload_iters(args.warmup, args.steps)
-    for _ in range(args.warmup):
-        cpu_reference_step(sc, None, None, iters)
-    times = [cpu_reference_step(sc, None, None, iters) for _ in range(args.steps)]
+    per_step = step_iters(args.warmup, args.steps)
+    exact = sum(per_step) <= REF_EXACT_MAX_ITERS
+    for _ in range(args.warmup):  # untimed: the assembly and one iteration
+        cpu_reference_step(sc, None, None, 1, sample_iters=1)
+    if exact:  # every timed step runs its own iteration count in full
+        times = [cpu_reference_step(sc, None, None, k, sample_iters=k) for k in per_step]
+    else:
+        times = [cpu_reference_step(sc, None, None, iters) for _ in range(args.steps)]
     ms = statistics.mean(t['ms'] for t in times)
     kind = 'reference' if times[-1]['impl'] == 'ref' else 'port'
-    sample = ('per step: the restated assembly of all %d contacts (oracle/oracle_ldy.c) timed in full, plus %d '
-              'iterations of the reference serial GAUSS_SEIDEL_Solve (bgs.c, compiled unmodified) timed and scaled '
-              'to %.2f iterations, the mean FP64 count of time-loop steps %d .. %d from rest (the product arm\'s '
-              'timed steps); the rigid integrator is not timed' % (times[-1]['n'], CPU_SAMPLE_ITERS, iters,
-                                                                  args.warmup + 1, args.warmup + args.steps))
+    if exact:
+        sample = ('per step: the restated assembly of all %d contacts (oracle/oracle_ldy.c) and the reference serial '
+                  'GAUSS_SEIDEL_Solve (bgs.c, compiled unmodified) run for the FP64 iteration count of that '
+                  'time-loop step from rest (steps %d .. %d, the product arm\'s timed steps; %d iterations in all, '
+                  'mean %.2f), both timed in full from the scene at rest (the work of an iteration does not depend '
+                  'on the state); the rigid integrator is not timed'
+                  % (times[-1]['n'], args.warmup + 1, args.warmup + args.steps, sum(per_step), iters))
+    else:
+        sample = ('per step: the restated assembly of all %d contacts (oracle/oracle_ldy.c) timed in full, plus %d '
+                  'iterations of the reference serial GAUSS_SEIDEL_Solve (bgs.c, compiled unmodified) timed and '
+                  'scaled to %.2f iterations, the mean FP64 count of time-loop steps %d .. %d from rest (the product '
+                  'arm\'s timed steps); the rigid integrator is not timed'
+                  % (times[-1]['n'], CPU_SAMPLE_ITERS, iters, args.warmup + 1, args.warmup + args.steps))
     line = {'metric': METRIC, 'value': round(ms, 3), 'unit': 'ms', 'n_gpus': ws, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': round(ms, 3), 'higher_is_better': False, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded scene generator)',
